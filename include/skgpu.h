@@ -1,0 +1,214 @@
+/* skgpu.h -- C ABI of the B200 (sm_100a) photon-packet life-cycle tracer for SKIRT 9.
+ *
+ * The boundary is segment level: the SKIRT host (C++) flattens its grid, medium state,
+ * dust-mix tables, sources and instruments once, hands them over through the upload calls
+ * below, and then replaces the per-thread Parallel::call over performLifeCycle with one
+ * skgpu_run_primary call per primary-emission segment. Tallies are added into the caller's
+ * arrays afterwards. All pointers are plain host pointers owned by the caller; the library
+ * copies what it needs into HBM during the call.
+ *
+ * Every function returns SKGPU_OK (0) or a positive error code; skgpu_last_error() gives the
+ * message. There is no CPU fallback: a non-zero status means the caller must stop (the SKIRT
+ * bridge turns it into a FatalError). Functions are not re-entrant per context.
+ *
+ * Reference interfaces replaced (paths relative to the SKIRT9-GPU source tree):
+ *   the whole family of GpuAcceleration static bool wrappers, SKIRT/core/GpuAcceleration.hpp:30-607,
+ *   and the per-chunk hook MonteCarloSimulation::performLifeCycle, SKIRT/core/MonteCarloSimulation.cpp:614-694.
+ */
+#ifndef SKGPU_H
+#define SKGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SKGPU_ABI_VERSION 1
+
+/* status codes */
+#define SKGPU_OK 0
+#define SKGPU_ERR_ARG 1       /* invalid argument or size */
+#define SKGPU_ERR_CUDA 2      /* CUDA runtime error (message holds the CUDA error string) */
+#define SKGPU_ERR_STATE 3     /* call made in the wrong order (e.g. run before uploads) */
+#define SKGPU_ERR_TIMEOUT 4   /* a bounded device-side loop gave up (guard exceeded) */
+#define SKGPU_ERR_DEVICE 5    /* device-side consistency check failed (bad index, NaN weight) */
+#define SKGPU_ERR_UNSUPPORTED 6
+
+/* grid kinds */
+#define SKGPU_GRID_CARTESIAN 0
+#define SKGPU_GRID_OCTREE 1
+#define SKGPU_GRID_VORONOI 2
+#define SKGPU_GRID_TETRA 3
+
+/* traversal precision (path kernels and life cycle) */
+#define SKGPU_PREC_FP64_EXACT 0 /* FP64 with the reference generators' operation order, no FMA contraction */
+#define SKGPU_PREC_FP32 1       /* FP32 traversal (positions relative to the ray origin / cell site) */
+
+/* source position models */
+#define SKGPU_SRC_POINT 0   /* PointSource: fixed position */
+#define SKGPU_SRC_EXPDISK 1 /* GeometricSource + ExpDiskGeometry: params hR, hz, Rmin, Rmax, zmax */
+#define SKGPU_SRC_RADIAL 2  /* GeometricSource with a spherical geometry (Sersic, Shell, ...): tabulated radial CDF */
+
+/* source spectral models */
+#define SKGPU_SPEC_DISCRETE 0 /* oligochromatic: pick one of n wavelengths uniformly, weight per wavelength */
+#define SKGPU_SPEC_TABLE 1    /* panchromatic: log-log tabulated CDF + log-uniform bias distribution */
+
+/* instrument kinds */
+#define SKGPU_INSTR_FRAME 0
+#define SKGPU_INSTR_SED 1
+
+typedef struct skgpu_ctx skgpu_ctx;
+
+/* One primary source, already normalised by the SourceSystem (SourceSystem.cpp setupSelfAfter /
+ * prepareForLaunch): histories [first_history, first_history+num_histories) of the segment
+ * launch from this source, each with base luminosity `packet_luminosity` (= Lpp * Lv[h]/Wv[h]). */
+typedef struct skgpu_source {
+    int32_t position_model;     /* SKGPU_SRC_* */
+    int32_t spectral_model;     /* SKGPU_SPEC_* */
+    double position[3];         /* point source position, or the centre of the geometry */
+    double geometry[6];         /* EXPDISK: hR, hz, Rmin, Rmax (0 = none), zmax (0 = none) */
+    uint64_t first_history;     /* _Iv[h] */
+    uint64_t num_histories;     /* _Iv[h+1] - _Iv[h] */
+    double packet_luminosity;   /* _Lpp * _Lv[h] / _Wv[h] */
+    double wavelength_bias;     /* xi of NormalizedSource (0 for unbiased, ignored for DISCRETE) */
+    double bias_lambda_min;     /* log-uniform bias distribution range (SPEC_TABLE) */
+    double bias_lambda_max;
+    int32_t table_offset;       /* offset into the shared table arrays (see skgpu_upload_sources) */
+    int32_t table_size;         /* number of entries used by this source */
+    int32_t radial_offset;      /* RADIAL: offset into the radial CDF arrays */
+    int32_t radial_size;
+} skgpu_source;
+
+/* One instrument of the InstrumentSystem, in instrument order. Instruments that share the
+ * observer of the preceding one (DistantInstrument::determineSameObserverAsPreceding) reuse its
+ * peel-off direction and observed optical depth, as FluxRecorder::detect does. */
+typedef struct skgpu_instrument {
+    int32_t kind;               /* SKGPU_INSTR_* */
+    int32_t same_observer;      /* 1 if same observer as the preceding instrument */
+    int32_t record_statistics;  /* accumulate sum_w^k, k=0..4, per history (FluxRecorder.cpp:1355-1409) */
+    int32_t record_components;  /* also record transparent / direct / scattered planes (FluxRecorder.cpp:412-440) */
+    int32_t num_pixels_x;       /* FRAME only */
+    int32_t num_pixels_y;
+    int32_t num_wavelength_bins;/* number of instrument wavelength bins */
+    int32_t wlg_offset;         /* offset into the wavelength-grid arrays (borders, ellv) */
+    int32_t wlg_num_borders;    /* K border points; ellv has K+1 entries */
+    double kobs[3];             /* DistantInstrument::bfkobs */
+    double cos_theta, sin_theta, cos_phi, sin_phi, cos_omega, sin_omega; /* FrameInstrument setup */
+    double xp_min, xp_size, yp_min, yp_size;                             /* FrameInstrument setup */
+} skgpu_instrument;
+
+/* Photon-packet options and run configuration (PhotonPacketOptions + Configuration flags). */
+typedef struct skgpu_options {
+    int32_t force_scattering;      /* 1: forced-scattering loop; 0: free (non-forced) propagation */
+    int32_t min_scatt_events;
+    double min_weight_reduction;   /* terminate when L <= L0 / reduction and nscatt >= min_scatt_events */
+    double path_length_bias;       /* xi of the forced-scattering composite distribution */
+    int32_t store_radiation_field; /* accumulate L*lnmean*ds per (cell, RF bin) on forced paths */
+    int32_t peel_off;              /* emission and scattering peel-off towards the instruments */
+    int32_t precision;             /* SKGPU_PREC_* */
+    int32_t reserved;
+    uint64_t seed;                 /* Philox key; packets draw from counter streams keyed by history index */
+} skgpu_options;
+
+/* device counters of the last run (all per segment) */
+typedef struct skgpu_counters {
+    uint64_t histories;
+    uint64_t crossings;        /* cell crossings over all traversals */
+    uint64_t scatterings;      /* scattering events */
+    uint64_t peel_detections;  /* instrument detections (per instrument) */
+    uint64_t rf_stores;        /* radiation-field updates */
+    uint64_t stats_overflows;  /* histories whose statistics buffer overflowed (partial grouping) */
+    uint64_t kernel_launches;
+    uint64_t reserved;
+} skgpu_counters;
+
+/* ---- context ---- */
+int skgpu_create(int device, skgpu_ctx** out);
+void skgpu_destroy(skgpu_ctx* ctx);
+const char* skgpu_last_error(const skgpu_ctx* ctx);
+int skgpu_abi_version(void);
+
+/* ---- grids (one per context; a new upload replaces the previous grid) ---- */
+/* CartesianSpatialGrid: border arrays _xv,_yv,_zv (CartesianSpatialGrid.hpp:95-97). */
+int skgpu_upload_grid_cartesian(skgpu_ctx* ctx, const double* xb, int32_t nxb, const double* yb, int32_t nyb,
+                                const double* zb, int32_t nzb);
+/* TreeSpatialGrid (octree): per node bounds xmin,ymin,zmin,xmax,ymax,zmax; cell index (-1 for
+ * non-leaf); children (8 per subdivided node, in OctTreeNode::createChildren order); per node and
+ * wall (BACK,FRONT,LEFT,RIGHT,BOTTOM,TOP) the overlap-sorted neighbour lists of TreeNode
+ * (TreeNode.cpp:103-112, :200-209) as CSR with nb_begin[6*num_nodes+1]. */
+int skgpu_upload_grid_octree(skgpu_ctx* ctx, int32_t num_nodes, const double* bounds, const int32_t* cell_index,
+                             const int32_t* child_begin, const int32_t* child_count, const int32_t* child_index,
+                             int32_t num_child_index, const int32_t* nb_begin, const int32_t* nb_index,
+                             int32_t num_nb_index, double eps);
+/* VoronoiMeshSnapshot: sites (x,y,z) and neighbour CSR with wall ids -1..-6
+ * (VoronoiMeshSnapshot.cpp:725-740); extent xmin..zmax; eps = 1e-12 * diagonal. */
+int skgpu_upload_grid_voronoi(skgpu_ctx* ctx, int32_t num_sites, const double* sites, const int32_t* nb_begin,
+                              const int32_t* nb_index, int32_t num_nb_index, const double* extent, double eps);
+/* TetraMeshSpatialGrid: vertices, per tetrahedron its 4 vertex indices, and per face the outward
+ * normal, the neighbouring tetrahedron (-1 on the hull) and its face index
+ * (TetraMeshSpatialGrid.hpp:107-133). */
+int skgpu_upload_grid_tetra(skgpu_ctx* ctx, int32_t num_vertices, const double* vertices, int32_t num_tetra,
+                            const int32_t* tetra_vertices, const double* face_normals, const int32_t* face_ntetra,
+                            const int32_t* face_nface, const double* extent, double eps);
+
+/* ---- medium ---- */
+/* MediumState number density per cell for a single dust medium (MediumState.hpp:251). */
+int skgpu_upload_medium(skgpu_ctx* ctx, int32_t num_cells, const double* number_density);
+/* DustMix tables: wavelength-index borders _lambdav (DustMix.cpp:92-97) and per entry the
+ * extinction / scattering cross sections and the HG asymmetry parameter. */
+int skgpu_upload_dust_mix(skgpu_ctx* ctx, int32_t num_lambda, const double* lambda_borders, const double* sigma_ext,
+                          const double* sigma_sca, const double* asymmpar);
+/* Radiation-field wavelength grid (DisjointWavelengthGrid borders + ellv map, as the instruments). */
+int skgpu_upload_rf_grid(skgpu_ctx* ctx, int32_t num_bins, int32_t num_borders, const double* borders,
+                         const int32_t* ellv);
+
+/* ---- sources ----
+ * table_lambda/table_a/table_b hold, per source at [table_offset, +table_size):
+ *   SPEC_DISCRETE: wavelengths, luminosity weights w_j (= s/b), unused;
+ *   SPEC_TABLE:    wavelength grid, normalised pdf p (per m), normalised cdf P.
+ * radial_r/radial_P hold the radial CDFs of SKGPU_SRC_RADIAL sources. */
+int skgpu_upload_sources(skgpu_ctx* ctx, int32_t num_sources, const skgpu_source* sources, int32_t table_len,
+                         const double* table_lambda, const double* table_a, const double* table_b,
+                         int32_t radial_len, const double* radial_r, const double* radial_P);
+
+/* ---- instruments ---- */
+int skgpu_upload_instruments(skgpu_ctx* ctx, int32_t num_instruments, const skgpu_instrument* instruments,
+                             int32_t wlg_len, const double* wlg_borders, const int32_t* wlg_ellv);
+
+/* ---- run ---- */
+int skgpu_set_options(skgpu_ctx* ctx, const skgpu_options* options);
+/* Runs the life cycle (launch, emission peel-off, forced or free propagation, radiation-field
+ * storage, scattering peel-off, HG scattering) of histories [first, first+count) of a segment
+ * of total_packets packets, adding into the device tallies. */
+int skgpu_run_primary(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t total_packets);
+/* Adds the device tallies of one instrument into the caller's arrays and leaves the device
+ * tallies untouched. ifu: num_wavelength_bins*npix (index l + ell*npix), sed: num_wavelength_bins,
+ * stats (may be NULL): 5 planes of ifu size then 5 planes of sed size (sum w^k, k=0..4). */
+int skgpu_fetch_instrument(skgpu_ctx* ctx, int32_t instrument, double* ifu, double* sed, double* ifu_stats,
+                           double* sed_stats);
+/* Adds the component planes (transparent, direct, scattered) of an instrument with
+ * record_components set: ifu3 holds 3 planes of ifu size, sed3 3 planes of sed size (either may be NULL). */
+int skgpu_fetch_instrument_components(skgpu_ctx* ctx, int32_t instrument, double* ifu3, double* sed3);
+/* Adds the radiation-field tally (num_cells * num_rf_bins, index m*num_rf_bins + ell) into rf. */
+int skgpu_fetch_radiation_field(skgpu_ctx* ctx, double* rf);
+int skgpu_clear_tallies(skgpu_ctx* ctx);
+int skgpu_get_counters(skgpu_ctx* ctx, skgpu_counters* out);
+/* Milliseconds of device time of the last skgpu_run_primary (CUDA events on the launch stream). */
+int skgpu_last_run_ms(skgpu_ctx* ctx, double* ms);
+
+/* ---- path segments (replaces GpuAcceleration::set*SpatialGridPath, GpuAcceleration.hpp) ----
+ * For each ray (x,y,z,kx,ky,kz) the segments (m, ds) the grid's PathSegmentGenerator returns,
+ * up to max_segments per ray; count[i] < 0 flags truncation (-n segments generated). */
+int skgpu_trace_paths(skgpu_ctx* ctx, int32_t num_rays, const double* rays, int32_t max_segments, int32_t precision,
+                      int32_t* count, int32_t* m, double* ds);
+/* Optical depth to the domain edge (MediumSystem::getExtinctionOpticalDepth, distance = inf)
+ * at wavelength lambda for each ray. */
+int skgpu_optical_depths(skgpu_ctx* ctx, int32_t num_rays, const double* rays, double lambda, int32_t precision,
+                         double* tau);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SKGPU_H */

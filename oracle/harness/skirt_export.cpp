@@ -1,0 +1,494 @@
+// Test infrastructure (oracle side): an export harness linked against the reference SKIRT 9
+// libraries built from source by oracle/ref.mk. It is never part of the product path.
+//
+//   skirt_export <file.ski> <outdir> [rays.npy [maxSegments [lambda_m]]]
+//
+// The harness reads a ski file through the reference's own SimulationItem machinery
+// (XmlHierarchyCreator + MonteCarloSimulation::setupSimulation, as SkirtCommandLineHandler.cpp
+// does at SKIRT/main/SkirtCommandLineHandler.cpp:315-380), then writes the flattened state that
+// the GPU tracer consumes as .npy files in <outdir>:
+//   - the spatial grid (Cartesian borders, octree nodes + overlap-sorted neighbour lists,
+//     Voronoi sites + neighbour lists, tetrahedra + faces);
+//   - the medium state (number density per cell and medium) and dust-mix tables;
+//   - instrument and source parameters;
+//   - optionally, for each ray (x,y,z,kx,ky,kz) in rays.npy, the reference path segments
+//     (m, ds) produced by SpatialGrid::createPathSegmentGenerator() -> next(), i.e. by the
+//     reference's own CPU generators (CartesianSpatialGrid.cpp:77-155, TreeSpatialGrid.cpp:143-228,
+//     VoronoiMeshSnapshot.cpp:1089-1222, TetraMeshSpatialGrid.cpp:688-831), and the optical depth
+//     to the domain edge from MediumSystem::getExtinctionOpticalDepth (MediumSystem.cpp:2328-2443).
+//
+// Members that the reference keeps private (octree neighbour lists, tetra faces, dust tables)
+// are read by compiling the reference headers with private/protected access opened; the
+// reference sources themselves are compiled unchanged.
+
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <memory>
+#include <sstream>
+#include <string>
+#include <vector>
+#include <array>
+#include <algorithm>
+#include <functional>
+#include <mutex>
+#include <atomic>
+#include <thread>
+#include <condition_variable>
+#include <unordered_map>
+#include <limits>
+#include <cmath>
+
+#define private public
+#define protected public
+#include "BuildInfo.hpp"
+#include "CartesianSpatialGrid.hpp"
+#include "Configuration.hpp"
+#include "DisjointWavelengthGrid.hpp"
+#include "DustMix.hpp"
+#include "FatalError.hpp"
+#include "FilePaths.hpp"
+#include "FluxRecorder.hpp"
+#include "FrameInstrument.hpp"
+#include "Instrument.hpp"
+#include "InstrumentSystem.hpp"
+#include "Log.hpp"
+#include "MediumSystem.hpp"
+#include "MonteCarloSimulation.hpp"
+#include "PathSegmentGenerator.hpp"
+#include "PhotonPacket.hpp"
+#include "ProcessManager.hpp"
+#include "SEDInstrument.hpp"
+#include "SimulationItemRegistry.hpp"
+#include "SourceSystem.hpp"
+#include "SpatialGrid.hpp"
+#include "SpatialGridPath.hpp"
+#include "System.hpp"
+#include "TetraMeshSpatialGrid.hpp"
+#include "TreeNode.hpp"
+#include "TreeSpatialGrid.hpp"
+#include "VoronoiMeshSnapshot.hpp"
+#include "VoronoiMeshSpatialGrid.hpp"
+#include "WavelengthGrid.hpp"
+#include "XmlHierarchyCreator.hpp"
+#undef private
+#undef protected
+
+namespace
+{
+    // ---- minimal .npy writer (format version 1.0) ----
+    template<typename T> const char* npyDescr();
+    template<> const char* npyDescr<double>() { return "<f8"; }
+    template<> const char* npyDescr<int32_t>() { return "<i4"; }
+    template<> const char* npyDescr<int64_t>() { return "<i8"; }
+
+    template<typename T>
+    void writeNpy(const std::string& path, const T* data, const std::vector<size_t>& shape)
+    {
+        std::ostringstream hdr;
+        hdr << "{'descr': '" << npyDescr<T>() << "', 'fortran_order': False, 'shape': (";
+        size_t n = 1;
+        for (size_t i = 0; i < shape.size(); ++i)
+        {
+            hdr << shape[i] << (shape.size() == 1 ? "," : (i + 1 < shape.size() ? ", " : ""));
+            n *= shape[i];
+        }
+        hdr << "), }";
+        std::string h = hdr.str();
+        size_t total = 10 + h.size() + 1;
+        size_t pad = (64 - total % 64) % 64;
+        h += std::string(pad, ' ');
+        h += '\n';
+        std::ofstream out(path, std::ios::binary);
+        const char magic[] = "\x93NUMPY";
+        out.write(magic, 6);
+        char ver[2] = {1, 0};
+        out.write(ver, 2);
+        uint16_t hl = static_cast<uint16_t>(h.size());
+        out.write(reinterpret_cast<const char*>(&hl), 2);
+        out.write(h.data(), h.size());
+        out.write(reinterpret_cast<const char*>(data), n * sizeof(T));
+    }
+
+    template<typename T> void writeVec(const std::string& path, const std::vector<T>& v)
+    {
+        writeNpy(path, v.data(), {v.size()});
+    }
+
+    // ---- minimal .npy reader for a contiguous little-endian f8 array ----
+    std::vector<double> readNpyDoubles(const std::string& path, size_t& rows, size_t& cols)
+    {
+        std::ifstream in(path, std::ios::binary);
+        if (!in) throw std::runtime_error("cannot open " + path);
+        char pre[10];
+        in.read(pre, 10);
+        uint16_t hl;
+        std::memcpy(&hl, pre + 8, 2);
+        std::string h(hl, ' ');
+        in.read(&h[0], hl);
+        if (h.find("<f8") == std::string::npos) throw std::runtime_error("rays must be float64");
+        auto p = h.find("shape");
+        auto a = h.find('(', p), b = h.find(')', p);
+        std::string s = h.substr(a + 1, b - a - 1);
+        std::vector<size_t> dims;
+        std::stringstream ss(s);
+        std::string tok;
+        while (std::getline(ss, tok, ','))
+        {
+            if (tok.find_first_not_of(' ') == std::string::npos) continue;
+            dims.push_back(std::stoul(tok));
+        }
+        rows = dims.size() > 0 ? dims[0] : 0;
+        cols = dims.size() > 1 ? dims[1] : 1;
+        std::vector<double> v(rows * cols);
+        in.read(reinterpret_cast<char*>(v.data()), v.size() * sizeof(double));
+        return v;
+    }
+
+    struct Meta
+    {
+        std::ostringstream s;
+        void kv(const std::string& k, const std::string& v) { s << k << " " << v << "\n"; }
+        void kv(const std::string& k, double v)
+        {
+            char buf[64];
+            std::snprintf(buf, sizeof buf, "%.17g", v);
+            s << k << " " << buf << "\n";
+        }
+    };
+
+    void exportGrid(SpatialGrid* grid, const std::string& out, Meta& meta)
+    {
+        Box ext = dynamic_cast<BoxSpatialGrid*>(grid) ? dynamic_cast<BoxSpatialGrid*>(grid)->extent() : Box();
+        std::vector<double> extent = {ext.xmin(), ext.ymin(), ext.zmin(), ext.xmax(), ext.ymax(), ext.zmax()};
+        writeVec(out + "/grid_extent.npy", extent);
+
+        if (auto g = dynamic_cast<CartesianSpatialGrid*>(grid))
+        {
+            meta.kv("grid", "cartesian");
+            std::vector<double> xb(begin(g->_xv), end(g->_xv)), yb(begin(g->_yv), end(g->_yv)),
+                zb(begin(g->_zv), end(g->_zv));
+            writeVec(out + "/grid_xb.npy", xb);
+            writeVec(out + "/grid_yb.npy", yb);
+            writeVec(out + "/grid_zb.npy", zb);
+            return;
+        }
+        if (auto g = dynamic_cast<TreeSpatialGrid*>(grid))
+        {
+            meta.kv("grid", "octree");
+            meta.kv("eps", g->_eps);
+            int numNodes = g->_nodev.size();
+            std::vector<double> bounds(6 * static_cast<size_t>(numNodes));
+            std::vector<int32_t> cellIndex(numNodes), childBegin(numNodes), childCount(numNodes), childIndex;
+            std::vector<int32_t> nbBegin(6 * static_cast<size_t>(numNodes) + 1), nbIndex;
+            for (int l = 0; l != numNodes; ++l)
+            {
+                TreeNode* node = g->_nodev[l];
+                if (node->id() != l) throw std::runtime_error("octree node id mismatch");
+                bounds[6 * l + 0] = node->xmin();
+                bounds[6 * l + 1] = node->ymin();
+                bounds[6 * l + 2] = node->zmin();
+                bounds[6 * l + 3] = node->xmax();
+                bounds[6 * l + 4] = node->ymax();
+                bounds[6 * l + 5] = node->zmax();
+                cellIndex[l] = g->_cellindexv[l];
+                childBegin[l] = childIndex.size();
+                childCount[l] = node->children().size();
+                for (auto c : node->children()) childIndex.push_back(c->id());
+                for (int w = 0; w != 6; ++w)
+                {
+                    nbBegin[6 * l + w] = nbIndex.size();
+                    for (auto nb : node->_neighbors[w]) nbIndex.push_back(nb->id());
+                }
+            }
+            nbBegin[6 * static_cast<size_t>(numNodes)] = nbIndex.size();
+            writeNpy(out + "/tree_bounds.npy", bounds.data(), {static_cast<size_t>(numNodes), 6});
+            writeVec(out + "/tree_cell_index.npy", cellIndex);
+            writeVec(out + "/tree_child_begin.npy", childBegin);
+            writeVec(out + "/tree_child_count.npy", childCount);
+            writeVec(out + "/tree_child_index.npy", childIndex);
+            writeVec(out + "/tree_nb_begin.npy", nbBegin);
+            writeVec(out + "/tree_nb_index.npy", nbIndex);
+            return;
+        }
+        if (auto vg = dynamic_cast<VoronoiMeshSpatialGrid*>(grid))
+        {
+            meta.kv("grid", "voronoi");
+            auto g = vg->_mesh;
+            meta.kv("eps", g->_eps);
+            int n = g->_traversalNeighborBegin.size();
+            writeNpy(out + "/vor_sites.npy", g->_traversalSiteCoordinates.data(), {static_cast<size_t>(n), 3});
+            std::vector<int32_t> nbBegin(n + 1);
+            for (int m = 0; m != n; ++m) nbBegin[m] = g->_traversalNeighborBegin[m];
+            nbBegin[n] = g->_traversalNeighborIndex.size();
+            std::vector<int32_t> nbIndex(g->_traversalNeighborIndex.begin(), g->_traversalNeighborIndex.end());
+            writeVec(out + "/vor_nb_begin.npy", nbBegin);
+            writeVec(out + "/vor_nb_index.npy", nbIndex);
+            return;
+        }
+        if (auto g = dynamic_cast<TetraMeshSpatialGrid*>(grid))
+        {
+            meta.kv("grid", "tetra");
+            meta.kv("eps", g->_eps);
+            int nv = g->_vertices.size();
+            std::vector<double> verts(3 * static_cast<size_t>(nv));
+            for (int i = 0; i != nv; ++i)
+            {
+                verts[3 * i] = g->_vertices[i].x();
+                verts[3 * i + 1] = g->_vertices[i].y();
+                verts[3 * i + 2] = g->_vertices[i].z();
+            }
+            int nt = g->_tetrahedra.size();
+            std::vector<int32_t> tv(4 * static_cast<size_t>(nt)), ntet(4 * static_cast<size_t>(nt)),
+                nface(4 * static_cast<size_t>(nt));
+            std::vector<double> normals(12 * static_cast<size_t>(nt));
+            for (int t = 0; t != nt; ++t)
+            {
+                const auto& tet = g->_tetrahedra[t];
+                for (int f = 0; f != 4; ++f)
+                {
+                    tv[4 * t + f] = tet._vertexIndices[f];
+                    ntet[4 * t + f] = tet._faces[f]._ntetra;
+                    nface[4 * t + f] = tet._faces[f]._nface;
+                    normals[12 * t + 3 * f] = tet._faces[f]._normal.x();
+                    normals[12 * t + 3 * f + 1] = tet._faces[f]._normal.y();
+                    normals[12 * t + 3 * f + 2] = tet._faces[f]._normal.z();
+                }
+            }
+            writeNpy(out + "/tet_vertices.npy", verts.data(), {static_cast<size_t>(nv), 3});
+            writeNpy(out + "/tet_tetra.npy", tv.data(), {static_cast<size_t>(nt), 4});
+            writeNpy(out + "/tet_ntetra.npy", ntet.data(), {static_cast<size_t>(nt), 4});
+            writeNpy(out + "/tet_nface.npy", nface.data(), {static_cast<size_t>(nt), 4});
+            writeNpy(out + "/tet_normals.npy", normals.data(), {static_cast<size_t>(nt), 4, 3});
+            return;
+        }
+        meta.kv("grid", "unsupported");
+    }
+
+    void exportMedium(MediumSystem* ms, const std::string& out, Meta& meta)
+    {
+        int numCells = ms->_state._numCells;
+        int numMedia = ms->_numMedia;
+        meta.kv("num_cells", numCells);
+        meta.kv("num_media", numMedia);
+        std::vector<double> dens(static_cast<size_t>(numCells) * numMedia);
+        for (int m = 0; m != numCells; ++m)
+            for (int h = 0; h != numMedia; ++h) dens[static_cast<size_t>(m) * numMedia + h] = ms->_state.numberDensity(m, h);
+        writeNpy(out + "/medium_density.npy", dens.data(), {static_cast<size_t>(numCells), static_cast<size_t>(numMedia)});
+        for (int h = 0; h != numMedia; ++h)
+        {
+            auto mix = dynamic_cast<const DustMix*>(ms->mix(0, h));
+            if (!mix) continue;
+            std::string p = out + "/mix" + std::to_string(h);
+            std::vector<double> lb(begin(mix->_lambdav), end(mix->_lambdav));
+            std::vector<double> se(begin(mix->_sigmaextv), end(mix->_sigmaextv));
+            std::vector<double> ss(begin(mix->_sigmascav), end(mix->_sigmascav));
+            std::vector<double> g(begin(mix->_asymmparv), end(mix->_asymmparv));
+            writeVec(p + "_lambda_borders.npy", lb);
+            writeVec(p + "_sigma_ext.npy", se);
+            writeVec(p + "_sigma_sca.npy", ss);
+            writeVec(p + "_asymmpar.npy", g);
+        }
+    }
+
+    // writes <prefix>_borders.npy and <prefix>_ellv.npy: the border list and the phantom-bin to
+    // bin-index map that DisjointWavelengthGrid::bin uses (DisjointWavelengthGrid.cpp:333-342)
+    void exportWLG(const WavelengthGrid* wlg, const std::string& prefix)
+    {
+        auto d = dynamic_cast<const DisjointWavelengthGrid*>(wlg);
+        if (!d) return;
+        std::vector<double> borders(begin(d->_borderv), end(d->_borderv));
+        std::vector<int32_t> ellv(d->_ellv.begin(), d->_ellv.end());
+        writeVec(prefix + "_borders.npy", borders);
+        writeVec(prefix + "_ellv.npy", ellv);
+    }
+
+    void exportInstruments(MonteCarloSimulation* sim, const std::string& out, Meta& meta)
+    {
+        int i = 0;
+        for (Instrument* instr : sim->instrumentSystem()->instruments())
+        {
+            std::string key = "instr" + std::to_string(i);
+            auto rec = instr->instrumentFluxRecorder();
+            meta.kv(key + "_same_observer", instr->isSameObserverAsPreceding() ? 1 : 0);
+            meta.kv(key + "_record_statistics", rec->_recordStatistics ? 1 : 0);
+            meta.kv(key + "_inclination", rec->_inclination);
+            meta.kv(key + "_azimuth", rec->_azimuth);
+            meta.kv(key + "_roll", rec->_roll);
+            if (auto d = dynamic_cast<DistantInstrument*>(instr))
+            {
+                Direction k = d->bfkobs(Position());
+                meta.kv(key + "_kobs_x", k.x());
+                meta.kv(key + "_kobs_y", k.y());
+                meta.kv(key + "_kobs_z", k.z());
+                meta.kv(key + "_distance", d->distance());
+            }
+            if (auto f = dynamic_cast<FrameInstrument*>(instr))
+            {
+                meta.kv(key + "_kind", "frame");
+                meta.kv(key + "_costheta", f->_costheta);
+                meta.kv(key + "_sintheta", f->_sintheta);
+                meta.kv(key + "_cosphi", f->_cosphi);
+                meta.kv(key + "_sinphi", f->_sinphi);
+                meta.kv(key + "_cosomega", f->_cosomega);
+                meta.kv(key + "_sinomega", f->_sinomega);
+                meta.kv(key + "_nxp", f->_Nxp);
+                meta.kv(key + "_nyp", f->_Nyp);
+                meta.kv(key + "_xpmin", f->_xpmin);
+                meta.kv(key + "_xpsiz", f->_xpsiz);
+                meta.kv(key + "_ypmin", f->_ypmin);
+                meta.kv(key + "_ypsiz", f->_ypsiz);
+            }
+            else if (dynamic_cast<SEDInstrument*>(instr))
+            {
+                meta.kv(key + "_kind", "sed");
+            }
+            else
+            {
+                meta.kv(key + "_kind", "other");
+            }
+            exportWLG(rec->_lambdagrid, out + "/" + key + "_wlg");
+            ++i;
+        }
+        meta.kv("num_instruments", i);
+    }
+
+    // launches the first `num` primary packets of a segment of `npp` packets through
+    // SourceSystem::launch and records (lambda, L*npp, x, y, z, kx, ky, kz) per packet
+    void probeLaunch(MonteCarloSimulation* sim, const std::string& out, size_t npp, size_t num)
+    {
+        auto ss = sim->sourceSystem();
+        ss->prepareForLaunch(npp);
+        std::vector<double> v;
+        PhotonPacket pp;
+        for (size_t i = 0; i != num; ++i)
+        {
+            ss->launch(&pp, i);
+            double x, y, z, kx, ky, kz;
+            pp.position().cartesian(x, y, z);
+            pp.direction().cartesian(kx, ky, kz);
+            double row[8] = {pp.wavelength(), pp.luminosity() * npp, x, y, z, kx, ky, kz};
+            v.insert(v.end(), row, row + 8);
+        }
+        writeNpy(out + "/src_probe.npy", v.data(), {num, 8});
+    }
+
+    void exportSources(MonteCarloSimulation* sim, Meta& meta)
+    {
+        auto ss = sim->sourceSystem();
+        meta.kv("source_total_luminosity", ss->_L);
+        meta.kv("num_sources", static_cast<int>(ss->_sources.size()));
+        for (size_t h = 0; h != ss->_sources.size(); ++h)
+        {
+            std::string key = "source" + std::to_string(h);
+            meta.kv(key + "_type", ss->_sources[h]->type());
+            meta.kv(key + "_lfrac", ss->_Lv[h]);
+            meta.kv(key + "_weight", ss->_Wv[h]);
+        }
+    }
+
+    void dumpRays(MonteCarloSimulation* sim, const std::string& raysPath, int maxSeg, double lambda,
+                  const std::string& out)
+    {
+        size_t rows, cols;
+        auto rays = readNpyDoubles(raysPath, rows, cols);
+        if (cols != 6) throw std::runtime_error("rays must be (N,6)");
+        SpatialGrid* grid = sim->mediumSystem()->grid();
+        auto gen = grid->createPathSegmentGenerator();
+        std::vector<int32_t> count(rows), segm(rows * maxSeg, -2);
+        std::vector<double> segds(rows * maxSeg, 0.), tau(rows, 0.);
+        for (size_t r = 0; r != rows; ++r)
+        {
+            const double* q = &rays[6 * r];
+            Position bfr(q[0], q[1], q[2]);
+            Direction bfk(q[3], q[4], q[5], false);
+            gen->start(bfr, bfk);
+            int n = 0;
+            bool overflow = false;
+            while (gen->next())
+            {
+                if (n < maxSeg)
+                {
+                    segm[r * maxSeg + n] = gen->m();
+                    segds[r * maxSeg + n] = gen->ds();
+                }
+                else
+                    overflow = true;
+                ++n;
+            }
+            count[r] = overflow ? -n : n;
+            // optical depth to the domain edge through the reference's MediumSystem routine
+            PhotonPacket pp;
+            pp.launch(r, lambda, 1.0, bfr, bfk);
+            tau[r] = sim->mediumSystem()->getExtinctionOpticalDepth(&pp, std::numeric_limits<double>::infinity());
+        }
+        writeVec(out + "/ray_count.npy", count);
+        writeNpy(out + "/ray_m.npy", segm.data(), {rows, static_cast<size_t>(maxSeg)});
+        writeNpy(out + "/ray_ds.npy", segds.data(), {rows, static_cast<size_t>(maxSeg)});
+        writeVec(out + "/ray_tau.npy", tau);
+    }
+}
+
+int main(int argc, char** argv)
+{
+    if (argc < 3)
+    {
+        std::fprintf(stderr, "usage: skirt_export <file.ski> <outdir> [rays.npy [maxSegments]]\n");
+        return 2;
+    }
+    ProcessManager pm(&argc, &argv);
+    System system(argc, argv);
+    SimulationItemRegistry registry(BuildInfo::projectVersion(), "9");
+    std::string ski = argv[1], out = argv[2];
+    try
+    {
+        auto schema = SimulationItemRegistry::getSchemaDef();
+        auto topitem = XmlHierarchyCreator::readFile(schema, ski);
+        auto sim = dynamic_cast<MonteCarloSimulation*>(topitem.get());
+        if (!sim) throw std::runtime_error("not a MonteCarloSimulation");
+        sim->filePaths()->setOutputPrefix("export");
+        sim->filePaths()->setOutputPath(out);
+        sim->parallelFactory()->setMaxThreadCount(1);
+        sim->log()->setLowestLevel(Log::Level::Warning);
+        sim->parallelFactory()->setup();
+        sim->log()->setup();
+        sim->setupSimulation();
+
+        Meta meta;
+        meta.kv("oligochromatic", sim->config()->oligochromatic() ? 1 : 0);
+        meta.kv("force_scattering", sim->config()->forceScattering() ? 1 : 0);
+        meta.kv("min_weight_reduction", sim->config()->minWeightReduction());
+        meta.kv("min_scatt_events", sim->config()->minScattEvents());
+        meta.kv("path_length_bias", sim->config()->pathLengthBias());
+        meta.kv("has_medium", sim->config()->hasMedium() ? 1 : 0);
+        if (sim->config()->hasMedium())
+        {
+            exportGrid(sim->mediumSystem()->grid(), out, meta);
+            exportMedium(sim->mediumSystem(), out, meta);
+            exportWLG(sim->config()->radiationFieldWLG(), out + "/rf_wlg");
+        }
+        exportInstruments(sim, out, meta);
+        exportSources(sim, meta);
+        probeLaunch(sim, out, 1000, 1000);
+        if (argc >= 4)
+        {
+            int maxSeg = argc >= 5 ? std::atoi(argv[4]) : 4096;
+            double lambda = argc >= 6 ? std::atof(argv[5]) : 0.55e-6;
+            dumpRays(sim, argv[3], maxSeg, lambda, out);
+        }
+        std::ofstream(out + "/meta.txt") << meta.s.str();
+    }
+    catch (FatalError& error)
+    {
+        for (const string& line : error.message()) std::fprintf(stderr, "%s\n", line.c_str());
+        return 1;
+    }
+    catch (std::exception& e)
+    {
+        std::fprintf(stderr, "error: %s\n", e.what());
+        return 1;
+    }
+    return 0;
+}

@@ -1,0 +1,148 @@
+# Test infrastructure: builds the reference SKIRT 9 CPU code from its own sources into
+# oracle/_ref/ with a plain Makefile (the reference's CMake project is not used).
+#
+#   make -f oracle/ref.mk -j8            # from the repository root
+#
+# Products (all under oracle/_ref/, git-ignored):
+#   lib/lib*.a                      the reference libraries (SMILE + SKIRT core/utils/...)
+#   exe/skirt/bin/skirt             the reference command-line program (CPU path, `-t N`)
+#   exe/skirt/bin/skirt_export      harness: loads a ski file through the reference's own
+#                                   SimulationItem tree and exports grids, medium state,
+#                                   mix tables and reference path segments as .npy files
+#   git/SKIRT/resources/            placeholder so FilePaths (SKIRT/core/FilePaths.cpp:33)
+#                                   finds its built-in resource directory relative to the
+#                                   executable (../../../git/SKIRT/resources)
+#
+# The only configure-time inputs of the reference build are SMILE/build/version_in.h and a
+# timestamp header; this recipe writes its own two-line stand-ins for both. Nothing on the
+# photon-packet path reads them.
+
+REF     ?= /root/reference
+HERE    := $(patsubst %/,%,$(dir $(lastword $(MAKEFILE_LIST))))
+OUT     := $(HERE)/_ref
+OBJ     := $(OUT)/obj
+LIB     := $(OUT)/lib
+GEN     := $(OUT)/gen
+BIN     := $(OUT)/exe/skirt/bin
+RES     := $(OUT)/git/SKIRT/resources
+
+CXX     ?= g++
+CC      ?= gcc
+# Release flags of the reference (CMake Release default for GNU): -O3 -DNDEBUG, C++14.
+CXXFLAGS_REF := -O3 -DNDEBUG -std=c++14 -w -pthread
+CFLAGS_REF   := -O3 -DNDEBUG -w -DFF_NO_UNISTD_H=1
+
+S_FUND  := $(REF)/SMILE/fundamentals
+S_SCH   := $(REF)/SMILE/schema
+S_SER   := $(REF)/SMILE/serialize
+S_BLD   := $(REF)/SMILE/build
+K_CORE  := $(REF)/SKIRT/core
+K_UTIL  := $(REF)/SKIRT/utils
+K_MPI   := $(REF)/SKIRT/mpi
+K_FITS  := $(REF)/SKIRT/fitsio
+K_VORO  := $(REF)/SKIRT/voro
+K_TET   := $(REF)/SKIRT/tetgen
+K_MAIN  := $(REF)/SKIRT/main
+
+INC_CORE := -I$(S_SCH) -I$(S_FUND) -I$(K_FITS) -I$(K_VORO) -I$(K_MPI) -I$(K_UTIL) -isystem $(K_TET)
+INC_MAIN := -I$(S_SER) -I$(S_SCH) -I$(S_FUND) -I$(S_BLD) -I$(GEN) -I$(K_CORE) -I$(K_MPI) -I$(K_UTIL)
+
+define objs_of
+$(patsubst $(1)/%,$(OBJ)/$(2)/%.o,$(wildcard $(1)/*.$(3)))
+endef
+
+O_FUND := $(call objs_of,$(S_FUND),fundamentals,cpp)
+O_SCH  := $(call objs_of,$(S_SCH),schema,cpp)
+O_SER  := $(call objs_of,$(S_SER),serialize,cpp)
+O_BLD  := $(OBJ)/build/BuildInfo.cpp.o
+O_CORE := $(call objs_of,$(K_CORE),skirtcore,cpp)
+O_UTIL := $(call objs_of,$(K_UTIL),utils,cpp)
+O_MPI  := $(call objs_of,$(K_MPI),mpi,cpp)
+O_FITS := $(call objs_of,$(K_FITS),fitsio,c)
+O_VORO := $(call objs_of,$(K_VORO),voro,cc)
+O_TET  := $(call objs_of,$(K_TET),tetgen,cxx)
+O_MAIN := $(call objs_of,$(K_MAIN),main,cpp)
+O_MAINLIB := $(OBJ)/main/SkirtCommandLineHandler.cpp.o
+
+LIBS := $(LIB)/libserialize.a $(LIB)/libschema.a $(LIB)/libfundamentals.a $(LIB)/libbuild.a \
+        $(LIB)/libskirtcore.a $(LIB)/libfitsio.a $(LIB)/libvoro.a $(LIB)/libmpi.a $(LIB)/libutils.a \
+        $(LIB)/libtetgen.a
+LINK_LIBS := -Wl,--start-group $(LIBS) -Wl,--end-group -pthread -ldl
+
+all: $(BIN)/skirt $(BIN)/skirt_export $(RES)/placeholder.txt
+
+$(RES)/placeholder.txt:
+	@mkdir -p $(RES)
+	@echo "built-in resource directory marker for the reference build in oracle/_ref" > $@
+
+$(GEN)/version.h:
+	@mkdir -p $(GEN)
+	@printf '#ifndef VERSION_HPP\n#define VERSION_HPP\n#define PROJECT_VERSION "v9.0"\n#endif\n' > $@
+
+$(GEN)/timestamp.h:
+	@mkdir -p $(GEN)
+	@printf '#ifndef TIMESTAMP_H\n#define TIMESTAMP_H\n#define BUILD_DATE "oracle"\n#define BUILD_TIME "oracle"\n#define COMMIT_HASH "reference"\n#endif\n' > $@
+
+$(OBJ)/fundamentals/%.o: $(S_FUND)/%
+	@mkdir -p $(dir $@)
+	$(CXX) $(CXXFLAGS_REF) -I$(S_FUND) -c $< -o $@
+$(OBJ)/schema/%.o: $(S_SCH)/%
+	@mkdir -p $(dir $@)
+	$(CXX) $(CXXFLAGS_REF) -I$(S_FUND) -c $< -o $@
+$(OBJ)/serialize/%.o: $(S_SER)/%
+	@mkdir -p $(dir $@)
+	$(CXX) $(CXXFLAGS_REF) -I$(S_SCH) -I$(S_FUND) -c $< -o $@
+$(OBJ)/build/%.o: $(S_BLD)/% $(GEN)/version.h $(GEN)/timestamp.h
+	@mkdir -p $(dir $@)
+	$(CXX) $(CXXFLAGS_REF) -I$(S_FUND) -I$(GEN) -c $< -o $@
+$(OBJ)/skirtcore/%.o: $(K_CORE)/%
+	@mkdir -p $(dir $@)
+	$(CXX) $(CXXFLAGS_REF) $(INC_CORE) -c $< -o $@
+$(OBJ)/utils/%.o: $(K_UTIL)/%
+	@mkdir -p $(dir $@)
+	$(CXX) $(CXXFLAGS_REF) -I$(S_FUND) -c $< -o $@
+$(OBJ)/mpi/%.o: $(K_MPI)/%
+	@mkdir -p $(dir $@)
+	$(CXX) $(CXXFLAGS_REF) -I$(S_FUND) -c $< -o $@
+$(OBJ)/fitsio/%.o: $(K_FITS)/%
+	@mkdir -p $(dir $@)
+	$(CC) $(CFLAGS_REF) -c $< -o $@
+$(OBJ)/voro/%.o: $(K_VORO)/%
+	@mkdir -p $(dir $@)
+	$(CXX) $(CXXFLAGS_REF) -c $< -o $@
+$(OBJ)/tetgen/%.o: $(K_TET)/%
+	@mkdir -p $(dir $@)
+	$(CXX) $(CXXFLAGS_REF) -DTETLIBRARY -c $< -o $@
+$(OBJ)/main/%.o: $(K_MAIN)/% $(GEN)/version.h
+	@mkdir -p $(dir $@)
+	$(CXX) $(CXXFLAGS_REF) $(INC_MAIN) -c $< -o $@
+
+$(LIB)/libfundamentals.a: $(O_FUND)
+$(LIB)/libschema.a: $(O_SCH)
+$(LIB)/libserialize.a: $(O_SER)
+$(LIB)/libbuild.a: $(O_BLD)
+$(LIB)/libskirtcore.a: $(O_CORE)
+$(LIB)/libutils.a: $(O_UTIL)
+$(LIB)/libmpi.a: $(O_MPI)
+$(LIB)/libfitsio.a: $(O_FITS)
+$(LIB)/libvoro.a: $(O_VORO)
+$(LIB)/libtetgen.a: $(O_TET)
+$(LIB)/%.a:
+	@mkdir -p $(LIB)
+	@rm -f $@
+	ar rcs $@ $^
+
+$(BIN)/skirt: $(O_MAIN) $(LIBS)
+	@mkdir -p $(BIN)
+	$(CXX) -o $@ $(O_MAIN) $(LINK_LIBS)
+
+# the export harness: reference libraries + the command-line handler object + our harness TU
+$(OBJ)/harness/skirt_export.o: $(HERE)/harness/skirt_export.cpp $(GEN)/version.h
+	@mkdir -p $(dir $@)
+	$(CXX) $(CXXFLAGS_REF) $(INC_MAIN) $(INC_CORE) -c $< -o $@
+
+$(BIN)/skirt_export: $(OBJ)/harness/skirt_export.o $(O_MAINLIB) $(LIBS)
+	@mkdir -p $(BIN)
+	$(CXX) -o $@ $(OBJ)/harness/skirt_export.o $(O_MAINLIB) $(LINK_LIBS)
+
+.PHONY: all

@@ -1,0 +1,1587 @@
+/* skoracle.c -- TEST INFRASTRUCTURE ONLY: CPU oracle of the photon-packet life cycle.
+ *
+ * A sequential restatement of the reference algorithm, written from the reference CPU classes
+ * (paths relative to the SKIRT9-GPU source tree):
+ *   path generators   CartesianSpatialGrid.cpp:77-155, TreeSpatialGrid.cpp:143-228 (TreeNode.cpp:66-112,
+ *                     OctTreeNode.cpp:37-42), VoronoiMeshSnapshot.cpp:1037-1222,
+ *                     TetraMeshSpatialGrid.cpp:87-138, 615-622, 688-831, PathSegmentGenerator.cpp:11-112
+ *   path + tau        SpatialGridPath.cpp:37-45, 161-203; MediumSystem.cpp:1785-1846, 2005-2150, 2328-2443
+ *   life cycle        MonteCarloSimulation.cpp:614-715, 888-957, 1492-1546, 1996-2092
+ *   scattering        MediumSystem.cpp:793-837, 1545-1655; DustMix.cpp:395-546
+ *   detection         FluxRecorder.cpp:372-538, 1355-1409; FrameInstrument.cpp:117-136
+ *   sources           SourceSystem.cpp (launch), NormalizedSource.cpp:73-110, SepAxGeometry.cpp:11-19,
+ *                     ExpDiskGeometry.cpp:46-69, SpheGeometry.cpp:25-32, Random.cpp:105-207
+ * Arithmetic is plain IEEE double with separate roundings (compiled without FMA contraction), as
+ * in the reference's x86-64 build. Random numbers are Philox4x32-10 streams keyed by history index
+ * instead of the reference's per-thread mt19937_64; histories draw in the reference's order.
+ * Mesh cell searches are brute force (nearest site; first containing tetrahedron by index).
+ */
+#define _GNU_SOURCE
+#include "skoracle.h"
+
+#include <float.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
+#ifndef M_E
+#define M_E 2.7182818284590452354
+#endif
+
+/* ------------------------------------------------------------------------------------------- */
+/* Philox4x32-10 (Salmon et al. 2011)                                                          */
+/* ------------------------------------------------------------------------------------------- */
+
+void or_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4])
+{
+    uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3], k0 = key[0], k1 = key[1];
+    for (int r = 0; r < 10; ++r)
+    {
+        uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0, hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        uint32_t n0 = hi1 ^ c1 ^ k0, n1 = lo1, n2 = hi0 ^ c3 ^ k1, n3 = lo0;
+        c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+typedef struct
+{
+    uint32_t key[2], hist[2], ctr;
+    int hasSpare;
+    double spare;
+} Rng;
+
+static double u01(uint32_t hi, uint32_t lo)
+{
+    uint64_t j = ((((uint64_t)hi) << 32) | lo) >> 12;
+    return ((double)j + 0.5) * 2.220446049250313080847e-16;
+}
+
+static void rng_start(Rng* r, uint64_t seed, uint64_t hist)
+{
+    r->key[0] = (uint32_t)seed;
+    r->key[1] = (uint32_t)(seed >> 32);
+    r->hist[0] = (uint32_t)hist;
+    r->hist[1] = (uint32_t)(hist >> 32);
+    r->ctr = 0;
+    r->hasSpare = 0;
+}
+
+static double uniform(Rng* r)
+{
+    if (r->hasSpare)
+    {
+        r->hasSpare = 0;
+        return r->spare;
+    }
+    uint32_t c[4] = {r->ctr++, 0u, r->hist[0], r->hist[1]}, o[4];
+    or_philox4x32_10(c, r->key, o);
+    r->spare = u01(o[2], o[3]);
+    r->hasSpare = 1;
+    return u01(o[0], o[1]);
+}
+
+/* ------------------------------------------------------------------------------------------- */
+/* context                                                                                     */
+/* ------------------------------------------------------------------------------------------- */
+
+typedef struct
+{
+    int kind;
+    double ext[6];
+    double eps;
+    int numCells;
+    /* cartesian */
+    double *xb, *yb, *zb;
+    int nx, ny, nz;
+    /* octree */
+    double* tb;
+    int *tcell, *tchild, *tnbb, *tnb;
+    int tnodes;
+    /* voronoi */
+    double* vs;
+    int *vnbb, *vnb;
+    int vn;
+    /* tetra */
+    double *tev, *ten, *tebox;
+    int *tet, *tent, *tenf;
+    int ten_n;
+} Grid;
+
+typedef struct
+{
+    skgpu_instrument d;
+    double *ifu, *sed, *comp, *stats;
+    size_t n;
+} Instr;
+
+struct or_ctx
+{
+    char err[256];
+    Grid g;
+    int hasGrid;
+    double* dens;
+    int numCells;
+    double *mixLb, *mixExt, *mixSca, *mixG;
+    int nmix;
+    double* rfB;
+    int *rfEll, nrf, rfNb;
+    double* rf;
+    size_t rfLen;
+    skgpu_source* src;
+    int nsrc;
+    double *tabL, *tabA, *tabB, *radR, *radP;
+    Instr* instr;
+    int ninstr;
+    double* wlgB;
+    int* wlgEll;
+    skgpu_options opt;
+    skgpu_counters cnt;
+    int errFlag;
+};
+
+static int fail(or_ctx* c, int code, const char* msg)
+{
+    if (c) snprintf(c->err, sizeof c->err, "%s", msg);
+    return code;
+}
+
+static void* dup(const void* p, size_t bytes)
+{
+    if (!p || !bytes) return NULL;
+    void* q = malloc(bytes);
+    memcpy(q, p, bytes);
+    return q;
+}
+
+static void free_grid(Grid* g)
+{
+    free(g->xb); free(g->yb); free(g->zb);
+    free(g->tb); free(g->tcell); free(g->tchild); free(g->tnbb); free(g->tnb);
+    free(g->vs); free(g->vnbb); free(g->vnb);
+    free(g->tev); free(g->ten); free(g->tebox); free(g->tet); free(g->tent); free(g->tenf);
+    memset(g, 0, sizeof *g);
+}
+
+static void free_instruments(or_ctx* c)
+{
+    for (int i = 0; i < c->ninstr; ++i)
+    {
+        free(c->instr[i].ifu); free(c->instr[i].sed); free(c->instr[i].comp); free(c->instr[i].stats);
+    }
+    free(c->instr);
+    c->instr = NULL;
+    c->ninstr = 0;
+    free(c->wlgB); free(c->wlgEll);
+    c->wlgB = NULL; c->wlgEll = NULL;
+}
+
+int or_create(int device, or_ctx** out)
+{
+    (void)device;
+    or_ctx* c = (or_ctx*)calloc(1, sizeof(or_ctx));
+    c->opt.force_scattering = 1;
+    c->opt.min_weight_reduction = 1e4;
+    c->opt.path_length_bias = 0.5;
+    c->opt.peel_off = 1;
+    *out = c;
+    return SKGPU_OK;
+}
+
+void or_destroy(or_ctx* c)
+{
+    if (!c) return;
+    free_grid(&c->g);
+    free_instruments(c);
+    free(c->dens); free(c->mixLb); free(c->mixExt); free(c->mixSca); free(c->mixG);
+    free(c->rfB); free(c->rfEll); free(c->rf);
+    free(c->src); free(c->tabL); free(c->tabA); free(c->tabB); free(c->radR); free(c->radP);
+    free(c);
+}
+
+const char* or_last_error(const or_ctx* c) { return c ? c->err : "null context"; }
+
+/* ------------------------------------------------------------------------------------------- */
+/* grid uploads                                                                                */
+/* ------------------------------------------------------------------------------------------- */
+
+int or_upload_grid_cartesian(or_ctx* c, const double* xb, int32_t nxb, const double* yb, int32_t nyb,
+                             const double* zb, int32_t nzb)
+{
+    if (nxb < 2 || nyb < 2 || nzb < 2) return fail(c, SKGPU_ERR_ARG, "cartesian: borders");
+    free_grid(&c->g);
+    Grid* g = &c->g;
+    g->kind = SKGPU_GRID_CARTESIAN;
+    g->xb = dup(xb, nxb * sizeof(double));
+    g->yb = dup(yb, nyb * sizeof(double));
+    g->zb = dup(zb, nzb * sizeof(double));
+    g->nx = nxb - 1; g->ny = nyb - 1; g->nz = nzb - 1;
+    g->ext[0] = xb[0]; g->ext[1] = yb[0]; g->ext[2] = zb[0];
+    g->ext[3] = xb[nxb - 1]; g->ext[4] = yb[nyb - 1]; g->ext[5] = zb[nzb - 1];
+    g->numCells = g->nx * g->ny * g->nz;
+    c->hasGrid = 1;
+    return SKGPU_OK;
+}
+
+int or_upload_grid_octree(or_ctx* c, int32_t num_nodes, const double* bounds, const int32_t* cell_index,
+                          const int32_t* child_begin, const int32_t* child_count, const int32_t* child_index,
+                          int32_t num_child_index, const int32_t* nb_begin, const int32_t* nb_index,
+                          int32_t num_nb_index, double eps)
+{
+    (void)num_child_index;
+    free_grid(&c->g);
+    Grid* g = &c->g;
+    g->kind = SKGPU_GRID_OCTREE;
+    g->tnodes = num_nodes;
+    g->tb = dup(bounds, 6 * (size_t)num_nodes * sizeof(double));
+    g->tcell = dup(cell_index, num_nodes * sizeof(int));
+    g->tchild = (int*)malloc(num_nodes * sizeof(int));
+    int numCells = 0;
+    for (int l = 0; l < num_nodes; ++l)
+    {
+        g->tchild[l] = child_count[l] > 0 ? child_index[child_begin[l]] : -1;
+        if (cell_index[l] + 1 > numCells) numCells = cell_index[l] + 1;
+    }
+    g->tnbb = dup(nb_begin, (6 * (size_t)num_nodes + 1) * sizeof(int));
+    g->tnb = dup(nb_index, (size_t)num_nb_index * sizeof(int));
+    memcpy(g->ext, bounds, 6 * sizeof(double));
+    g->eps = eps;
+    g->numCells = numCells;
+    c->hasGrid = 1;
+    return SKGPU_OK;
+}
+
+int or_upload_grid_voronoi(or_ctx* c, int32_t num_sites, const double* sites, const int32_t* nb_begin,
+                           const int32_t* nb_index, int32_t num_nb_index, const double* extent, double eps)
+{
+    free_grid(&c->g);
+    Grid* g = &c->g;
+    g->kind = SKGPU_GRID_VORONOI;
+    g->vn = num_sites;
+    g->vs = dup(sites, 3 * (size_t)num_sites * sizeof(double));
+    g->vnbb = dup(nb_begin, ((size_t)num_sites + 1) * sizeof(int));
+    g->vnb = dup(nb_index, (size_t)num_nb_index * sizeof(int));
+    memcpy(g->ext, extent, 6 * sizeof(double));
+    g->eps = eps;
+    g->numCells = num_sites;
+    c->hasGrid = 1;
+    return SKGPU_OK;
+}
+
+int or_upload_grid_tetra(or_ctx* c, int32_t num_vertices, const double* vertices, int32_t num_tetra,
+                         const int32_t* tetra_vertices, const double* face_normals, const int32_t* face_ntetra,
+                         const int32_t* face_nface, const double* extent, double eps)
+{
+    free_grid(&c->g);
+    Grid* g = &c->g;
+    g->kind = SKGPU_GRID_TETRA;
+    g->ten_n = num_tetra;
+    g->tev = dup(vertices, 3 * (size_t)num_vertices * sizeof(double));
+    g->tet = dup(tetra_vertices, 4 * (size_t)num_tetra * sizeof(int));
+    g->ten = dup(face_normals, 12 * (size_t)num_tetra * sizeof(double));
+    g->tent = dup(face_ntetra, 4 * (size_t)num_tetra * sizeof(int));
+    g->tenf = dup(face_nface, 4 * (size_t)num_tetra * sizeof(int));
+    g->tebox = (double*)malloc(6 * (size_t)num_tetra * sizeof(double));
+    for (int t = 0; t < num_tetra; ++t)
+    {
+        double* b = g->tebox + 6 * (size_t)t;
+        b[0] = b[1] = b[2] = DBL_MAX;
+        b[3] = b[4] = b[5] = -DBL_MAX;
+        for (int v = 0; v < 4; ++v)
+        {
+            const double* p = vertices + 3 * (size_t)tetra_vertices[4 * t + v];
+            for (int a = 0; a < 3; ++a)
+            {
+                if (p[a] < b[a]) b[a] = p[a];
+                if (p[a] > b[3 + a]) b[3 + a] = p[a];
+            }
+        }
+    }
+    memcpy(g->ext, extent, 6 * sizeof(double));
+    g->eps = eps;
+    g->numCells = num_tetra;
+    c->hasGrid = 1;
+    return SKGPU_OK;
+}
+
+/* ------------------------------------------------------------------------------------------- */
+/* path segment generators (restatements of the reference CPU generators)                     */
+/* ------------------------------------------------------------------------------------------- */
+
+enum { UNKNOWN = 0, INSIDE = 1, OUTSIDE = 2 };
+
+typedef struct
+{
+    double rx, ry, rz, kx, ky, kz, ds;
+    int m, state;
+    int i, j, k;  /* cartesian */
+    int node;     /* octree */
+    int mr, ef;   /* voronoi / tetra */
+} Gen;
+
+static int box_contains(const double* b, double x, double y, double z)
+{
+    return x >= b[0] && x <= b[3] && y >= b[1] && y <= b[4] && z >= b[2] && z <= b[5];
+}
+
+static void gen_start(Gen* s, const double* ray)
+{
+    memset(s, 0, sizeof *s);
+    s->state = UNKNOWN;
+    s->rx = ray[0]; s->ry = ray[1]; s->rz = ray[2];
+    s->kx = ray[3]; s->ky = ray[4]; s->kz = ray[5];
+    s->m = -1;
+    s->node = -1;
+    s->mr = -1;
+    s->ef = -1;
+}
+
+static void propagater(Gen* s, double d)
+{
+    s->rx += s->kx * d;
+    s->ry += s->ky * d;
+    s->rz += s->kz * d;
+}
+
+/* PathSegmentGenerator::moveInside */
+static int move_inside(Gen* s, const double* b, double eps)
+{
+    s->m = -1;
+    s->ds = 0.;
+    s->state = OUTSIDE;
+    double cumds = 0.;
+    if (s->rx <= b[0])
+    {
+        if (s->kx <= 0.0) return 0;
+        double d = (b[0] - s->rx) / s->kx;
+        s->rx = b[0] + eps; s->ry += s->ky * d; s->rz += s->kz * d; cumds += d;
+    }
+    else if (s->rx >= b[3])
+    {
+        if (s->kx >= 0.0) return 0;
+        double d = (b[3] - s->rx) / s->kx;
+        s->rx = b[3] - eps; s->ry += s->ky * d; s->rz += s->kz * d; cumds += d;
+    }
+    if (s->ry <= b[1])
+    {
+        if (s->ky <= 0.0) return 0;
+        double d = (b[1] - s->ry) / s->ky;
+        s->rx += s->kx * d; s->ry = b[1] + eps; s->rz += s->kz * d; cumds += d;
+    }
+    else if (s->ry >= b[4])
+    {
+        if (s->ky >= 0.0) return 0;
+        double d = (b[4] - s->ry) / s->ky;
+        s->rx += s->kx * d; s->ry = b[4] - eps; s->rz += s->kz * d; cumds += d;
+    }
+    if (s->rz <= b[2])
+    {
+        if (s->kz <= 0.0) return 0;
+        double d = (b[2] - s->rz) / s->kz;
+        s->rx += s->kx * d; s->ry += s->ky * d; s->rz = b[2] + eps; cumds += d;
+    }
+    else if (s->rz >= b[5])
+    {
+        if (s->kz >= 0.0) return 0;
+        double d = (b[5] - s->rz) / s->kz;
+        s->rx += s->kx * d; s->ry += s->ky * d; s->rz = b[5] - eps; cumds += d;
+    }
+    if (!box_contains(b, s->rx, s->ry, s->rz)) return 0;
+    s->m = -1;
+    s->ds = cumds;
+    s->state = INSIDE;
+    return 1;
+}
+
+/* NR::locateClip */
+static int locate_clip(const double* xv, int n, double x)
+{
+    if (x < xv[0]) return 0;
+    int jl = -1, ju = n - 1;
+    while (ju - jl > 1)
+    {
+        int jm = (ju + jl) >> 1;
+        if (x < xv[jm]) ju = jm; else jl = jm;
+    }
+    return jl;
+}
+
+static int cart_next(const Grid* g, Gen* s)
+{
+    if (s->state == OUTSIDE) return 0;
+    if (s->state == UNKNOWN)
+    {
+        double dx = g->ext[3] - g->ext[0], dy = g->ext[4] - g->ext[1], dz = g->ext[5] - g->ext[2];
+        if (!move_inside(s, g->ext, 1e-12 * sqrt(dx * dx + dy * dy + dz * dz))) return 0;
+        s->i = locate_clip(g->xb, g->nx + 1, s->rx);
+        s->j = locate_clip(g->yb, g->ny + 1, s->ry);
+        s->k = locate_clip(g->zb, g->nz + 1, s->rz);
+        if (s->ds > 0.) return 1;
+    }
+    int m = s->k + g->nz * s->j + g->nz * g->ny * s->i;
+    double xE = (s->kx < 0.0) ? g->xb[s->i] : g->xb[s->i + 1];
+    double yE = (s->ky < 0.0) ? g->yb[s->j] : g->yb[s->j + 1];
+    double zE = (s->kz < 0.0) ? g->zb[s->k] : g->zb[s->k + 1];
+    double dsx = (fabs(s->kx) > 1e-15) ? (xE - s->rx) / s->kx : DBL_MAX;
+    double dsy = (fabs(s->ky) > 1e-15) ? (yE - s->ry) / s->ky : DBL_MAX;
+    double dsz = (fabs(s->kz) > 1e-15) ? (zE - s->rz) / s->kz : DBL_MAX;
+    if (dsx <= dsy && dsx <= dsz)
+    {
+        s->m = m; s->ds = dsx;
+        s->rx = xE; s->ry += s->ky * dsx; s->rz += s->kz * dsx;
+        s->i += (s->kx < 0.0) ? -1 : 1;
+        if (s->i >= g->nx || s->i < 0) s->state = OUTSIDE;
+    }
+    else if (dsy < dsx && dsy <= dsz)
+    {
+        s->m = m; s->ds = dsy;
+        s->ry = yE; s->rx += s->kx * dsy; s->rz += s->kz * dsy;
+        s->j += (s->ky < 0.0) ? -1 : 1;
+        if (s->j >= g->ny || s->j < 0) s->state = OUTSIDE;
+    }
+    else
+    {
+        s->m = m; s->ds = dsz;
+        s->rz = zE; s->rx += s->kx * dsz; s->ry += s->ky * dsz;
+        s->k += (s->kz < 0.0) ? -1 : 1;
+        if (s->k >= g->nz || s->k < 0) s->state = OUTSIDE;
+    }
+    return 1;
+}
+
+/* TreeNode::leafChild from the root */
+static int leaf_child(const Grid* g, double x, double y, double z)
+{
+    if (!box_contains(g->tb, x, y, z)) return -1;
+    int node = 0;
+    while (g->tchild[node] >= 0)
+    {
+        int c0 = g->tchild[node];
+        const double* cb = g->tb + 6 * (size_t)c0;
+        node = c0 + (x < cb[3] ? 0 : 1) + (y < cb[4] ? 0 : 2) + (z < cb[5] ? 0 : 4);
+    }
+    return node;
+}
+
+static int tree_next(const Grid* g, Gen* s)
+{
+    if (s->state == OUTSIDE) return 0;
+    if (s->state == UNKNOWN)
+    {
+        if (!move_inside(s, g->ext, g->eps)) return 0;
+        s->node = leaf_child(g, s->rx, s->ry, s->rz);
+        if (s->node < 0)
+        {
+            s->state = OUTSIDE;
+            return 0;
+        }
+        if (s->ds > 0.) return 1;
+    }
+    const double* b = g->tb + 6 * (size_t)s->node;
+    double xnext = (s->kx < 0.0) ? b[0] : b[3];
+    double ynext = (s->ky < 0.0) ? b[1] : b[4];
+    double znext = (s->kz < 0.0) ? b[2] : b[5];
+    double dsx = (fabs(s->kx) > 1e-15) ? (xnext - s->rx) / s->kx : DBL_MAX;
+    double dsy = (fabs(s->ky) > 1e-15) ? (ynext - s->ry) / s->ky : DBL_MAX;
+    double dsz = (fabs(s->kz) > 1e-15) ? (znext - s->rz) / s->kz : DBL_MAX;
+    double ds;
+    int wall;
+    if (dsx <= dsy && dsx <= dsz) { ds = dsx; wall = (s->kx < 0.0) ? 0 : 1; }
+    else if (dsy <= dsx && dsy <= dsz) { ds = dsy; wall = (s->ky < 0.0) ? 2 : 3; }
+    else { ds = dsz; wall = (s->kz < 0.0) ? 4 : 5; }
+    propagater(s, ds + g->eps);
+    s->m = g->tcell[s->node];
+    s->ds = ds;
+    int old = s->node, nb = -1;
+    for (int e = g->tnbb[6 * old + wall]; e < g->tnbb[6 * old + wall + 1]; ++e)
+    {
+        int cand = g->tnb[e];
+        if (box_contains(g->tb + 6 * (size_t)cand, s->rx, s->ry, s->rz))
+        {
+            nb = cand;
+            break;
+        }
+    }
+    if (nb < 0) nb = leaf_child(g, s->rx, s->ry, s->rz);
+    if (nb == old)
+    {
+        s->rx = nextafter(s->rx, (s->kx < 0.) ? -DBL_MAX : DBL_MAX);
+        s->ry = nextafter(s->ry, (s->ky < 0.) ? -DBL_MAX : DBL_MAX);
+        s->rz = nextafter(s->rz, (s->kz < 0.) ? -DBL_MAX : DBL_MAX);
+        nb = leaf_child(g, s->rx, s->ry, s->rz);
+    }
+    s->node = nb;
+    if (nb < 0 || nb == old) s->state = OUTSIDE;
+    return 1;
+}
+
+/* nearest site by brute force (VoronoiMeshSnapshot::cellIndex up to equidistant ties) */
+static int vor_cell(const Grid* g, double x, double y, double z)
+{
+    if (!box_contains(g->ext, x, y, z)) return -1;
+    int best = -1;
+    double bd = DBL_MAX;
+    for (int s = 0; s < g->vn; ++s)
+    {
+        const double* p = g->vs + 3 * (size_t)s;
+        double dx = p[0] - x, dy = p[1] - y, dz = p[2] - z;
+        double d2 = dx * dx + dy * dy + dz * dz;
+        if (d2 < bd)
+        {
+            bd = d2;
+            best = s;
+        }
+    }
+    return best;
+}
+
+static int vor_next(const Grid* g, Gen* s)
+{
+    if (s->state == OUTSIDE) return 0;
+    if (s->state == UNKNOWN)
+    {
+        if (!move_inside(s, g->ext, g->eps)) return 0;
+        s->mr = vor_cell(g, s->rx, s->ry, s->rz);
+        if (s->mr < 0)
+        {
+            s->state = OUTSIDE;
+            return 0;
+        }
+        if (s->ds > 0.) return 1;
+    }
+    for (int guard = 0; guard < 1000; ++guard)
+    {
+        const double* pr = g->vs + 3 * (size_t)s->mr;
+        double sq = DBL_MAX;
+        int mq = -99;
+        for (int e = g->vnbb[s->mr]; e < g->vnbb[s->mr + 1]; ++e)
+        {
+            int mi = g->vnb[e];
+            double si = 0;
+            if (mi >= 0)
+            {
+                const double* pi = g->vs + 3 * (size_t)mi;
+                double nx = pi[0] - pr[0], ny = pi[1] - pr[1], nz = pi[2] - pr[2];
+                double ndotk = nx * s->kx + ny * s->ky + nz * s->kz;
+                if (ndotk > 0)
+                {
+                    double px = 0.5 * (pi[0] + pr[0]), py = 0.5 * (pi[1] + pr[1]), pz = 0.5 * (pi[2] + pr[2]);
+                    si = (nx * (px - s->rx) + ny * (py - s->ry) + nz * (pz - s->rz)) / ndotk;
+                }
+            }
+            else
+            {
+                switch (mi)
+                {
+                    case -1: si = (g->ext[0] - s->rx) / s->kx; break;
+                    case -2: si = (g->ext[3] - s->rx) / s->kx; break;
+                    case -3: si = (g->ext[1] - s->ry) / s->ky; break;
+                    case -4: si = (g->ext[4] - s->ry) / s->ky; break;
+                    case -5: si = (g->ext[2] - s->rz) / s->kz; break;
+                    case -6: si = (g->ext[5] - s->rz) / s->kz; break;
+                    default: si = 0; break;
+                }
+            }
+            if (si > 0 && si < sq)
+            {
+                sq = si;
+                mq = mi;
+            }
+        }
+        if (mq == -99)
+        {
+            propagater(s, g->eps);
+            s->mr = vor_cell(g, s->rx, s->ry, s->rz);
+            if (s->mr < 0)
+            {
+                s->state = OUTSIDE;
+                return 0;
+            }
+        }
+        else
+        {
+            propagater(s, sq + g->eps);
+            s->m = s->mr;
+            s->ds = sq;
+            s->mr = mq;
+            if (s->mr < 0) s->state = OUTSIDE;
+            return 1;
+        }
+    }
+    s->state = OUTSIDE;
+    return 0;
+}
+
+static const double* te_vertex(const Grid* g, int t, int v) { return g->tev + 3 * (size_t)g->tet[4 * (size_t)t + v]; }
+
+static int te_contains(const Grid* g, int t, double x, double y, double z)
+{
+    if (!box_contains(g->tebox + 6 * (size_t)t, x, y, z)) return 0;
+    const double* n = g->ten + 12 * (size_t)t;
+    const double* v = te_vertex(g, t, 3);
+    for (int f = 0; f <= 2; ++f)
+        if ((v[0] - x) * n[3 * f] + (v[1] - y) * n[3 * f + 1] + (v[2] - z) * n[3 * f + 2] < 0) return 0;
+    v = te_vertex(g, t, 0);
+    if ((v[0] - x) * n[9] + (v[1] - y) * n[10] + (v[2] - z) * n[11] < 0.) return 0;
+    return 1;
+}
+
+static int te_cell(const Grid* g, double x, double y, double z)
+{
+    if (!box_contains(g->ext, x, y, z)) return -1;
+    for (int t = 0; t < g->ten_n; ++t)
+        if (te_contains(g, t, x, y, z)) return t;
+    return -1;
+}
+
+static void cross3(const double* a, const double* b, double* c)
+{
+    c[0] = a[1] * b[2] - a[2] * b[1];
+    c[1] = a[2] * b[0] - a[0] * b[2];
+    c[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+static double dot3(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+static void cw_vertices(int face, int cv[3])
+{
+    cv[0] = (face + 3) % 4;
+    cv[1] = (face + 2) % 4;
+    cv[2] = (face + 1) % 4;
+    if (face % 2 == 0)
+    {
+        int t = cv[0]; cv[0] = cv[2]; cv[2] = t;
+    }
+}
+
+static int te_entering_face(const Grid* g, int t, const double* pos, const double* dir)
+{
+    static const int etable[6][2] = {{3, 2}, {1, 3}, {2, 1}, {3, 0}, {0, 2}, {1, 0}};
+    int e = 0;
+    for (int t1 = 0; t1 < 3; t1++)
+        for (int t2 = t1 + 1; t2 < 4; t2++)
+        {
+            const double* v1 = te_vertex(g, t, t1);
+            const double* v2 = te_vertex(g, t, t2);
+            double rel[3] = {pos[0] - v1[0], pos[1] - v1[1], pos[2] - v1[2]}, mom[3];
+            cross3(dir, rel, mom);
+            double edge[3] = {v2[0] - v1[0], v2[1] - v1[1], v2[2] - v1[2]};
+            double prod = dot3(mom, edge);
+            if (prod != 0.) return prod < 0 ? etable[e][0] : etable[e][1];
+            e++;
+        }
+    return -1;
+}
+
+static int tet_next(const Grid* g, Gen* s)
+{
+    if (s->state == OUTSIDE) return 0;
+    if (s->state == UNKNOWN)
+    {
+        if (!move_inside(s, g->ext, g->eps)) return 0;
+        s->mr = te_cell(g, s->rx, s->ry, s->rz);
+        s->ef = -1;
+        if (s->mr == -1)
+        {
+            s->state = OUTSIDE;
+            return 0;
+        }
+        if (s->ds > 0.) return 1;
+    }
+    for (int guard = 0; guard < 1000; ++guard)
+    {
+        double pos[3] = {s->rx, s->ry, s->rz}, dir[3] = {s->kx, s->ky, s->kz};
+        int leaving = -1;
+        double d = DBL_MAX;
+        if (s->ef == -1) s->ef = te_entering_face(g, s->mr, pos, dir);
+        if (s->ef < 0) s->ef = 0;
+        const double* ve = te_vertex(g, s->mr, s->ef);
+        double rel[3] = {pos[0] - ve[0], pos[1] - ve[1], pos[2] - ve[2]}, mom[3];
+        cross3(dir, rel, mom);
+        int cv[3];
+        cw_vertices(s->ef, cv);
+        const double* c0 = te_vertex(g, s->mr, cv[0]);
+        double e0[3] = {ve[0] - c0[0], ve[1] - c0[1], ve[2] - c0[2]};
+        double prod0 = dot3(mom, e0);
+        int clock0 = prod0 < 0;
+        int i = clock0 ? 1 : 2;
+        const double* ci = te_vertex(g, s->mr, cv[i]);
+        double ei[3] = {ve[0] - ci[0], ve[1] - ci[1], ve[2] - ci[2]};
+        double prodi = dot3(mom, ei);
+        int cclocki = prodi >= 0;
+        const double* nrm = g->ten + 12 * (size_t)s->mr;
+        double vp[3] = {ve[0] - pos[0], ve[1] - pos[1], ve[2] - pos[2]};
+        if (prod0 == 0. || prodi == 0.)
+        {
+            for (int q = 0; q < 3; ++q)
+            {
+                const double* n = nrm + 3 * cv[q];
+                double ndotk = dot3(n, dir);
+                if (ndotk > 0)
+                {
+                    double dq = dot3(n, vp) / ndotk;
+                    if (dq < d)
+                    {
+                        d = dq;
+                        leaving = cv[q];
+                    }
+                }
+            }
+        }
+        else
+        {
+            static const int dtable[2][2] = {{1, 0}, {0, 2}};
+            leaving = cv[dtable[clock0][cclocki]];
+            const double* n = nrm + 3 * leaving;
+            d = dot3(n, vp) / dot3(n, dir);
+        }
+        if (leaving == -1 || d < g->eps)
+        {
+            propagater(s, g->eps);
+            s->mr = te_cell(g, s->rx, s->ry, s->rz);
+            if (s->mr < 0)
+            {
+                s->state = OUTSIDE;
+                return 0;
+            }
+            s->ef = -1;
+        }
+        else
+        {
+            propagater(s, d);
+            s->m = s->mr;
+            s->ds = d;
+            int nt = g->tent[4 * (size_t)s->mr + leaving], nf = g->tenf[4 * (size_t)s->mr + leaving];
+            s->mr = nt;
+            if (s->mr < 0)
+            {
+                s->state = OUTSIDE;
+                return 0;
+            }
+            s->ef = nf;
+            return 1;
+        }
+    }
+    s->state = OUTSIDE;
+    return 0;
+}
+
+static int gen_next(const Grid* g, Gen* s)
+{
+    switch (g->kind)
+    {
+        case SKGPU_GRID_CARTESIAN: return cart_next(g, s);
+        case SKGPU_GRID_OCTREE: return tree_next(g, s);
+        case SKGPU_GRID_VORONOI: return vor_next(g, s);
+        case SKGPU_GRID_TETRA: return tet_next(g, s);
+    }
+    return 0;
+}
+
+int or_trace_paths(or_ctx* c, int32_t num_rays, const double* rays, int32_t max_segments, int32_t precision,
+                   int32_t* count, int32_t* m, double* ds)
+{
+    (void)precision;
+    if (!c->hasGrid) return fail(c, SKGPU_ERR_STATE, "trace: no grid");
+    for (int r = 0; r < num_rays; ++r)
+    {
+        Gen s;
+        gen_start(&s, rays + 6 * (size_t)r);
+        int n = 0, ovf = 0;
+        while (gen_next(&c->g, &s))
+        {
+            if (n < max_segments)
+            {
+                m[(size_t)r * max_segments + n] = s.m;
+                ds[(size_t)r * max_segments + n] = s.ds;
+            }
+            else
+                ovf = 1;
+            ++n;
+        }
+        count[r] = ovf ? -n : n;
+    }
+    return SKGPU_OK;
+}
+
+/* ------------------------------------------------------------------------------------------- */
+/* medium, sources, instruments, options                                                       */
+/* ------------------------------------------------------------------------------------------- */
+
+int or_upload_medium(or_ctx* c, int32_t num_cells, const double* number_density)
+{
+    free(c->dens);
+    c->dens = dup(number_density, num_cells * sizeof(double));
+    c->numCells = num_cells;
+    return SKGPU_OK;
+}
+
+int or_upload_dust_mix(or_ctx* c, int32_t num_lambda, const double* lb, const double* se, const double* ss,
+                       const double* g)
+{
+    free(c->mixLb); free(c->mixExt); free(c->mixSca); free(c->mixG);
+    c->mixLb = dup(lb, num_lambda * sizeof(double));
+    c->mixExt = dup(se, num_lambda * sizeof(double));
+    c->mixSca = dup(ss, num_lambda * sizeof(double));
+    c->mixG = dup(g, num_lambda * sizeof(double));
+    c->nmix = num_lambda;
+    return SKGPU_OK;
+}
+
+int or_upload_rf_grid(or_ctx* c, int32_t num_bins, int32_t num_borders, const double* borders, const int32_t* ellv)
+{
+    free(c->rfB); free(c->rfEll);
+    c->rfB = dup(borders, num_borders * sizeof(double));
+    c->rfEll = dup(ellv, (num_borders + 1) * sizeof(int));
+    c->nrf = num_bins;
+    c->rfNb = num_borders;
+    return SKGPU_OK;
+}
+
+int or_upload_sources(or_ctx* c, int32_t num_sources, const skgpu_source* sources, int32_t table_len,
+                      const double* table_lambda, const double* table_a, const double* table_b, int32_t radial_len,
+                      const double* radial_r, const double* radial_P)
+{
+    free(c->src); free(c->tabL); free(c->tabA); free(c->tabB); free(c->radR); free(c->radP);
+    c->src = dup(sources, num_sources * sizeof(skgpu_source));
+    c->nsrc = num_sources;
+    c->tabL = dup(table_lambda, table_len * sizeof(double));
+    c->tabA = dup(table_a, table_len * sizeof(double));
+    c->tabB = dup(table_b, table_len * sizeof(double));
+    c->radR = dup(radial_r, radial_len * sizeof(double));
+    c->radP = dup(radial_P, radial_len * sizeof(double));
+    return SKGPU_OK;
+}
+
+int or_upload_instruments(or_ctx* c, int32_t num_instruments, const skgpu_instrument* instruments, int32_t wlg_len,
+                          const double* wlg_borders, const int32_t* wlg_ellv)
+{
+    free_instruments(c);
+    c->ninstr = num_instruments;
+    c->instr = (Instr*)calloc(num_instruments > 0 ? num_instruments : 1, sizeof(Instr));
+    for (int i = 0; i < num_instruments; ++i)
+    {
+        Instr* in = &c->instr[i];
+        in->d = instruments[i];
+        size_t npix = in->d.kind == SKGPU_INSTR_FRAME ? (size_t)in->d.num_pixels_x * in->d.num_pixels_y : 1;
+        in->n = npix * in->d.num_wavelength_bins;
+        if (in->d.kind == SKGPU_INSTR_FRAME)
+            in->ifu = (double*)calloc(in->n, sizeof(double));
+        else
+            in->sed = (double*)calloc(in->n, sizeof(double));
+        if (in->d.record_components) in->comp = (double*)calloc(3 * in->n, sizeof(double));
+        if (in->d.record_statistics) in->stats = (double*)calloc(5 * in->n, sizeof(double));
+    }
+    c->wlgB = dup(wlg_borders, wlg_len * sizeof(double));
+    c->wlgEll = dup(wlg_ellv, wlg_len * sizeof(int));
+    return SKGPU_OK;
+}
+
+int or_set_options(or_ctx* c, const skgpu_options* o)
+{
+    c->opt = *o;
+    return SKGPU_OK;
+}
+
+/* ------------------------------------------------------------------------------------------- */
+/* life cycle                                                                                  */
+/* ------------------------------------------------------------------------------------------- */
+
+typedef struct
+{
+    int m;
+    double ds, s, tau;
+} Seg;
+
+typedef struct
+{
+    Seg* v;
+    int n, cap;
+} Path;
+
+typedef struct
+{
+    int instr, ell, l;
+    double w;
+} Contrib;
+
+typedef struct
+{
+    double rx, ry, rz, kx, ky, kz, L, lambda;
+    int nscatt, ellMix, ellRF;
+    double sext, ssca, g;
+    Contrib* contrib;
+    int ncontrib, capcontrib;
+} Packet;
+
+static int upper_bound(const double* xv, int n, double x)
+{
+    int lo = 0, hi = n;
+    while (lo < hi)
+    {
+        int mid = (lo + hi) >> 1;
+        if (x < xv[mid]) hi = mid; else lo = mid + 1;
+    }
+    return lo;
+}
+
+static int wlg_bin(const double* b, int nb, const int* ellv, double lambda) { return ellv[upper_bound(b, nb, lambda)]; }
+
+/* SpecialFunctions::gexp */
+static double gexp(double p, double x)
+{
+    const double q = 1.0 - p;
+    if (q == 0.0) return exp(x);
+    if (fabs(q) < 1e-3)
+    {
+        double x2 = x * x;
+        return exp(x) * (1.0 - 0.5 * x2 * q + 1.0 / 24.0 * x * x2 * (8.0 + 3.0 * x) * q * q
+                         - 1.0 / 48.0 * x2 * x2 * (12.0 + 8.0 * x + x2) * q * q * q);
+    }
+    return pow(1.0 + q * x, 1.0 / q);
+}
+
+/* SpecialFunctions::lnmean (4-argument flavour) */
+static double lnmean4(double x1, double x2, double lnx1, double lnx2)
+{
+    if (x1 > x2)
+    {
+        double t = x1; x1 = x2; x2 = t;
+        t = lnx1; lnx1 = lnx2; lnx2 = t;
+    }
+    if (x1 <= 0) return 0.;
+    double x = x2 / x1 - 1.;
+    if (x < 1e-3)
+        return x1 / (1. - 1. / 2. * x + 1. / 3. * x * x - 1. / 4. * x * x * x + 1. / 5. * x * x * x * x
+                     - 1. / 6. * x * x * x * x * x);
+    return (x2 - x1) / (lnx2 - lnx1);
+}
+
+/* Lambert W, branch -1 (Halley iteration), used by ExpDiskGeometry::randomCylRadius */
+static double lambert_wm1(double x)
+{
+    if (x >= 0.) return -INFINITY;
+    if (x <= -1. / M_E) return -1.;
+    double w;
+    if (x < -0.25)
+    {
+        double p = -sqrt(2. * (M_E * x + 1.));
+        w = -1. + p - p * p / 3. + 11. / 72. * p * p * p;
+    }
+    else
+    {
+        double l1 = log(-x), l2 = log(-l1);
+        w = l1 - l2 + l2 / l1;
+    }
+    for (int it = 0; it < 20; ++it)
+    {
+        double ew = exp(w), f = w * ew - x, wp1 = w + 1.;
+        if (wp1 == 0.) break;
+        double dw = f / (ew * wp1 - (w + 2.) * f / (2. * wp1));
+        w -= dw;
+        if (fabs(dw) <= 1e-15 * fabs(w)) break;
+    }
+    return w;
+}
+
+static void iso_direction(Rng* r, double* kx, double* ky, double* kz)
+{
+    double theta = acos(2.0 * uniform(r) - 1.0);
+    double phi = 2.0 * M_PI * uniform(r);
+    const double eps = 1e-8;
+    if (theta <= eps) { *kx = 0.; *ky = 0.; *kz = 1.; }
+    else if (theta >= M_PI - eps) { *kx = 0.; *ky = 0.; *kz = -1.; }
+    else
+    {
+        double st = sin(theta);
+        *kx = st * cos(phi);
+        *ky = st * sin(phi);
+        *kz = cos(theta);
+    }
+}
+
+static double expon_cutoff(Rng* r, double xmax)
+{
+    if (xmax == 0.0) return 0.0;
+    if (xmax < 1e-10) return uniform(r) * xmax;
+    double c = 1.0 - exp(-xmax);
+    for (int guard = 0; guard < 64; ++guard)
+    {
+        double x = -log(1.0 - uniform(r) * c);
+        if (x <= xmax) return x;
+    }
+    return xmax;
+}
+
+static double value_hg(double g, double ct)
+{
+    double t = 1. + g * g - 2. * g * ct;
+    return (1. - g) * (1. + g) / sqrt(t * t * t);
+}
+
+static double integral_hg(double g, double ca, double cb)
+{
+    double ta = sqrt(1. + g * g - 2. * g * ca), tb = sqrt(1. + g * g - 2. * g * cb);
+    return (1. - g) * (1. + g) / g * ((tb - ta) / (tb * ta));
+}
+
+static double mean_hg(double g, double ct)
+{
+    const double delta = 4. * M_PI / 180.;
+    double theta = acos(fmin(1., fmax(-1., ct)));
+    double ca = cos(theta - delta), cb = cos(theta + delta);
+    if (theta < delta) return (integral_hg(g, 1., ca) + integral_hg(g, 1., cb)) / (2. - ca - cb);
+    if (theta > M_PI - delta) return (integral_hg(g, ca, -1.) + integral_hg(g, cb, -1.)) / (2. + ca + cb);
+    return integral_hg(g, ca, cb) / (ca - cb);
+}
+
+static void add_contrib(Packet* pk, int i, int ell, int l, double w)
+{
+    if (pk->ncontrib == pk->capcontrib)
+    {
+        pk->capcontrib = pk->capcontrib ? 2 * pk->capcontrib : 64;
+        pk->contrib = (Contrib*)realloc(pk->contrib, pk->capcontrib * sizeof(Contrib));
+    }
+    Contrib ct = {i, ell, l, w};
+    pk->contrib[pk->ncontrib++] = ct;
+}
+
+/* FluxRecorder::recordContributions: group the history's contributions per bin, add w^k */
+static void record_contributions(or_ctx* c, Packet* pk)
+{
+    for (int a = 0; a < pk->ncontrib; ++a)
+    {
+        if (pk->contrib[a].instr < 0) continue;
+        Contrib ca = pk->contrib[a];
+        double w = ca.w;
+        for (int b = a + 1; b < pk->ncontrib; ++b)
+        {
+            Contrib* cb = &pk->contrib[b];
+            if (cb->instr == ca.instr && cb->ell == ca.ell && cb->l == ca.l)
+            {
+                w += cb->w;
+                cb->instr = -1;
+            }
+        }
+        Instr* in = &c->instr[ca.instr];
+        size_t idx = ca.l < 0 ? (size_t)ca.ell
+                              : (size_t)ca.l + (size_t)ca.ell * in->d.num_pixels_x * in->d.num_pixels_y;
+        double wn = 1.;
+        for (int k = 0; k <= 4; ++k)
+        {
+            in->stats[k * in->n + idx] += wn;
+            wn *= w;
+        }
+    }
+    pk->ncontrib = 0;
+}
+
+/* MediumSystem::getExtinctionOpticalDepth(pp, inf) for the peel-off packet */
+static double observed_tau(or_ctx* c, const Packet* pk, const double* kobs, double Lp)
+{
+    double taumax = log(Lp) + 745;
+    double ray[6] = {pk->rx, pk->ry, pk->rz, kobs[0], kobs[1], kobs[2]};
+    Gen s;
+    gen_start(&s, ray);
+    double tau = 0.;
+    while (gen_next(&c->g, &s))
+    {
+        c->cnt.crossings++;
+        if (s.m >= 0)
+        {
+            tau += pk->sext * c->dens[s.m] * s.ds;
+            if (tau >= taumax) return INFINITY;
+        }
+    }
+    return tau;
+}
+
+static int frame_pixel(const skgpu_instrument* d, const Packet* pk)
+{
+    double x = pk->rx, y = pk->ry, z = pk->rz;
+    double xpp = -d->sin_phi * x + d->cos_phi * y;
+    double ypp = -d->cos_phi * d->cos_theta * x - d->sin_phi * d->cos_theta * y + d->sin_theta * z;
+    double xp = d->cos_omega * xpp - d->sin_omega * ypp;
+    double yp = d->sin_omega * xpp + d->cos_omega * ypp;
+    int i = (int)floor((xp - d->xp_min) / d->xp_size);
+    int j = (int)floor((yp - d->yp_min) / d->yp_size);
+    if (i < 0 || i >= d->num_pixels_x || j < 0 || j >= d->num_pixels_y) return -1;
+    return i + d->num_pixels_x * j;
+}
+
+/* peelOffEmission / peelOffScattering + Instrument::detect + FluxRecorder::detect */
+static void peel_off(or_ctx* c, Packet* pk, int scattering)
+{
+    double Lp = 0., tau = 0.;
+    int tauKnown = 0;
+    const double* kobs = NULL;
+    int numScatt = pk->nscatt + (scattering ? 1 : 0);
+    for (int i = 0; i < c->ninstr; ++i)
+    {
+        Instr* in = &c->instr[i];
+        if (!in->d.same_observer)
+        {
+            kobs = in->d.kobs;
+            if (scattering)
+            {
+                double ct = pk->kx * kobs[0] + pk->ky * kobs[1] + pk->kz * kobs[2];
+                Lp = pk->L * (fabs(pk->g) > 0.95 ? mean_hg(pk->g, ct) : value_hg(pk->g, ct));
+            }
+            else
+                Lp = pk->L;
+            tauKnown = 0;
+        }
+        int l = in->d.kind == SKGPU_INSTR_FRAME ? frame_pixel(&in->d, pk) : -1;
+        if (in->d.kind == SKGPU_INSTR_FRAME && l < 0) continue;
+        int ell = wlg_bin(c->wlgB + in->d.wlg_offset, in->d.wlg_num_borders, c->wlgEll + in->d.wlg_offset, pk->lambda);
+        if (ell < 0) continue;
+        if (!tauKnown)
+        {
+            tau = observed_tau(c, pk, kobs, Lp);
+            tauKnown = 1;
+        }
+        double Lext = Lp * exp(-tau);
+        c->cnt.peel_detections++;
+        size_t idx = in->d.kind == SKGPU_INSTR_FRAME ? (size_t)l + (size_t)ell * in->d.num_pixels_x * in->d.num_pixels_y
+                                                     : (size_t)ell;
+        double* total = in->d.kind == SKGPU_INSTR_FRAME ? in->ifu : in->sed;
+        total[idx] += Lext;
+        if (in->d.record_components)
+        {
+            if (numScatt == 0)
+            {
+                in->comp[idx] += Lp;
+                in->comp[in->n + idx] += Lext;
+            }
+            else
+                in->comp[2 * in->n + idx] += Lext;
+        }
+        if (in->d.record_statistics) add_contrib(pk, i, ell, l, Lext);
+    }
+}
+
+static void path_build(or_ctx* c, const Packet* pk, Path* path)
+{
+    double ray[6] = {pk->rx, pk->ry, pk->rz, pk->kx, pk->ky, pk->kz};
+    Gen s;
+    gen_start(&s, ray);
+    path->n = 0;
+    double scum = 0., tau = 0.;
+    while (gen_next(&c->g, &s))
+    {
+        c->cnt.crossings++;
+        if (s.ds > 0.)
+        {
+            if (path->n == path->cap)
+            {
+                path->cap = path->cap ? 2 * path->cap : 1024;
+                path->v = (Seg*)realloc(path->v, path->cap * sizeof(Seg));
+            }
+            scum += s.ds;
+            if (s.m >= 0) tau += pk->sext * c->dens[s.m] * s.ds;
+            Seg sg = {s.m, s.ds, scum, tau};
+            path->v[path->n++] = sg;
+        }
+    }
+}
+
+static void launch(or_ctx* c, Rng* r, uint64_t hist, Packet* pk)
+{
+    int h = 0;
+    for (int q = 1; q < c->nsrc; ++q)
+        if (c->src[q].first_history <= hist) h = q;
+    const skgpu_source* S = &c->src[h];
+    rng_start(r, c->opt.seed, hist);
+    pk->nscatt = 0;
+    double L = S->packet_luminosity, lambda;
+    if (S->spectral_model == SKGPU_SPEC_DISCRETE)
+    {
+        int j = (int)(uniform(r) * S->table_size);
+        if (j > S->table_size - 1) j = S->table_size - 1;
+        lambda = c->tabL[S->table_offset + j];
+        L *= c->tabA[S->table_offset + j];
+    }
+    else
+    {
+        const double* lv = c->tabL + S->table_offset;
+        const double* pv = c->tabA + S->table_offset;
+        const double* Pv = c->tabB + S->table_offset;
+        int n = S->table_size;
+        double xi = S->wavelength_bias;
+        int fromSed = (xi <= 0.) || (uniform(r) > xi);
+        if (fromSed)
+        {
+            double X = uniform(r);
+            int i = locate_clip(Pv, n, X);
+            double alpha = log(pv[i + 1] / pv[i]) / log(lv[i + 1] / lv[i]);
+            lambda = lv[i] * gexp(-alpha, (X - Pv[i]) / (pv[i] * lv[i]));
+        }
+        else
+        {
+            double lmin = log(S->bias_lambda_min), lw = log(S->bias_lambda_max) - log(S->bias_lambda_min);
+            lambda = exp(lmin + lw * uniform(r));
+        }
+        if (xi > 0.)
+        {
+            double s = 0.;
+            if (lambda >= lv[0] && lambda <= lv[n - 1])
+            {
+                int i = upper_bound(lv, n, lambda) - 1;
+                if (i > n - 2) i = n - 2;
+                if (i < 0) i = 0;
+                double a = log(pv[i + 1] / pv[i]) / log(lv[i + 1] / lv[i]);
+                s = pv[i] * pow(lambda / lv[i], a);
+            }
+            double b = (lambda >= S->bias_lambda_min && lambda <= S->bias_lambda_max)
+                           ? 1. / ((log(S->bias_lambda_max) - log(S->bias_lambda_min)) * lambda)
+                           : 0.;
+            L *= (s > 0.) ? s / ((1 - xi) * s + xi * b) : 0.;
+        }
+    }
+    pk->lambda = lambda;
+    pk->L = L;
+    if (S->position_model == SKGPU_SRC_POINT)
+    {
+        pk->rx = S->position[0]; pk->ry = S->position[1]; pk->rz = S->position[2];
+    }
+    else if (S->position_model == SKGPU_SRC_EXPDISK)
+    {
+        double hR = S->geometry[0], hz = S->geometry[1], Rmin = S->geometry[2], Rmax = S->geometry[3], zmax = S->geometry[4];
+        double R = 0., z = 0.;
+        for (int t = 0; t < 1000; ++t)
+        {
+            double X = uniform(r);
+            R = hR * (-1.0 - lambert_wm1((X - 1.0) / M_E));
+            if (!((Rmax > 0.0 && R >= Rmax) || R <= Rmin)) break;
+        }
+        double phi = 2.0 * M_PI * uniform(r);
+        for (int t = 0; t < 1000; ++t)
+        {
+            double X = uniform(r);
+            z = (X <= 0.5) ? hz * log(2.0 * X) : -hz * log(2.0 * (1.0 - X));
+            if (!(zmax > 0.0 && fabs(z) >= zmax)) break;
+        }
+        pk->rx = S->position[0] + R * cos(phi);
+        pk->ry = S->position[1] + R * sin(phi);
+        pk->rz = S->position[2] + z;
+    }
+    else
+    {
+        double X = uniform(r);
+        const double* rv = c->radR + S->radial_offset;
+        const double* Pv = c->radP + S->radial_offset;
+        int i = locate_clip(Pv, S->radial_size, X);
+        double rr = rv[i] + (X - Pv[i]) / (Pv[i + 1] - Pv[i]) * (rv[i + 1] - rv[i]);
+        double ux, uy, uz;
+        iso_direction(r, &ux, &uy, &uz);
+        pk->rx = S->position[0] + rr * ux;
+        pk->ry = S->position[1] + rr * uy;
+        pk->rz = S->position[2] + rr * uz;
+    }
+    iso_direction(r, &pk->kx, &pk->ky, &pk->kz);
+    pk->ellMix = locate_clip(c->mixLb, c->nmix, lambda);
+    pk->sext = c->mixExt[pk->ellMix];
+    pk->ssca = c->mixSca[pk->ellMix];
+    pk->g = c->mixG[pk->ellMix];
+    pk->ellRF = c->opt.store_radiation_field ? wlg_bin(c->rfB, c->rfNb, c->rfEll, lambda) : -1;
+}
+
+static double albedo(or_ctx* c, const Packet* pk, int m)
+{
+    double n = c->dens[m];
+    double ksca = n > 0. ? n * pk->ssca : 0.;
+    double kext = n > 0. ? n * pk->sext : 0.;
+    return kext > 0. ? ksca / kext : 0.;
+}
+
+static void scatter(or_ctx* c, Rng* r, Packet* pk)
+{
+    double g = pk->g;
+    if (fabs(g) < 1e-6)
+        iso_direction(r, &pk->kx, &pk->ky, &pk->kz);
+    else
+    {
+        double f = ((1.0 - g) * (1.0 + g)) / (1.0 - g + 2.0 * g * uniform(r));
+        double costheta = (1.0 + g * g - f * f) / (2.0 * g);
+        /* Random::direction(bfk, costheta) */
+        double phi = 2.0 * M_PI * uniform(r);
+        double cosphi = cos(phi), sinphi = sin(phi);
+        double sintheta = sqrt(fabs((1.0 - costheta) * (1.0 + costheta)));
+        double kx = pk->kx, ky = pk->ky, kz = pk->kz, nx, ny, nz;
+        if (kz > 0.99999)
+        {
+            nx = cosphi * sintheta; ny = sinphi * sintheta; nz = costheta;
+        }
+        else if (kz < -0.99999)
+        {
+            nx = cosphi * sintheta; ny = sinphi * sintheta; nz = -costheta;
+        }
+        else
+        {
+            double root = sqrt((1.0 - kz) * (1.0 + kz));
+            nx = sintheta / root * (-kx * kz * cosphi + ky * sinphi) + kx * costheta;
+            ny = -sintheta / root * (ky * kz * cosphi + kx * sinphi) + ky * costheta;
+            nz = root * sintheta * cosphi + kz * costheta;
+        }
+        pk->kx = nx; pk->ky = ny; pk->kz = nz;
+    }
+    pk->nscatt++;
+    c->cnt.scatterings++;
+}
+
+static void life_cycle(or_ctx* c, uint64_t hist, Path* path, Packet* pk)
+{
+    Rng rng;
+    launch(c, &rng, hist, pk);
+    c->cnt.histories++;
+    pk->ncontrib = 0;
+    if (!(pk->L > 0)) return;
+    int peel = c->opt.peel_off && c->ninstr > 0;
+    if (peel) peel_off(c, pk, 0);
+    if (c->opt.force_scattering)
+    {
+        double Lthreshold = pk->L / c->opt.min_weight_reduction;
+        while (1)
+        {
+            path_build(c, pk, path);
+            /* storeRadiationField */
+            if (c->opt.store_radiation_field && pk->ellRF >= 0)
+            {
+                double lnExtBeg = 0., extBeg = 1.;
+                for (int q = 0; q < path->n; ++q)
+                {
+                    double lnExtEnd = -path->v[q].tau, extEnd = exp(lnExtEnd);
+                    int m = path->v[q].m;
+                    if (m >= 0)
+                    {
+                        double extMean = lnmean4(extEnd, extBeg, lnExtEnd, lnExtBeg);
+                        c->rf[(size_t)m * c->nrf + pk->ellRF] += pk->L * extMean * path->v[q].ds;
+                        c->cnt.rf_stores++;
+                    }
+                    lnExtBeg = lnExtEnd;
+                    extBeg = extEnd;
+                }
+            }
+            /* simulateForcedPropagation */
+            double taupath = path->n ? path->v[path->n - 1].tau : 0.;
+            if (taupath <= 0.)
+            {
+                pk->L *= 0.;
+            }
+            else
+            {
+                double xi = c->opt.path_length_bias, tau;
+                if (xi == 0.)
+                    tau = expon_cutoff(&rng, taupath);
+                else
+                {
+                    tau = uniform(&rng) < xi ? uniform(&rng) * taupath : expon_cutoff(&rng, taupath);
+                    double p = -exp(-tau) / expm1(-taupath);
+                    double q = (1.0 - xi) * p + xi / taupath;
+                    pk->L *= p / q;
+                }
+                /* SpatialGridPath::findInteractionPoint */
+                int lo = 0, hi = path->n;
+                while (lo < hi)
+                {
+                    int mid = (lo + hi) >> 1;
+                    if (tau < path->v[mid].tau) hi = mid; else lo = mid + 1;
+                }
+                int m;
+                double s;
+                if (lo < path->n)
+                {
+                    double t0 = lo ? path->v[lo - 1].tau : 0., s0 = lo ? path->v[lo - 1].s : 0.;
+                    m = path->v[lo].m;
+                    s = s0 + ((tau - t0) / (path->v[lo].tau - t0)) * (path->v[lo].s - s0);
+                }
+                else
+                {
+                    m = path->v[path->n - 1].m;
+                    s = path->v[path->n - 1].s;
+                }
+                if (m < 0)
+                {
+                    c->errFlag |= 2;
+                    break;
+                }
+                pk->L *= -expm1(-taupath) * albedo(c, pk, m);
+                pk->rx += s * pk->kx;
+                pk->ry += s * pk->ky;
+                pk->rz += s * pk->kz;
+            }
+            if (pk->L <= 0 || (pk->L <= Lthreshold && pk->nscatt >= c->opt.min_scatt_events)) break;
+            if (peel) peel_off(c, pk, 1);
+            scatter(c, &rng, pk);
+        }
+    }
+    else
+    {
+        while (1)
+        {
+            /* simulateNonForcedPropagation with setInteractionPointUsingExtinction */
+            double tauinteract = -log(uniform(&rng));
+            double ray[6] = {pk->rx, pk->ry, pk->rz, pk->kx, pk->ky, pk->kz};
+            Gen s;
+            gen_start(&s, ray);
+            double tau = 0., sc = 0.;
+            int found = 0, m = -1;
+            double sInt = 0.;
+            while (gen_next(&c->g, &s))
+            {
+                c->cnt.crossings++;
+                double t0 = tau, s0 = sc;
+                if (s.m >= 0) tau += pk->sext * c->dens[s.m] * s.ds;
+                sc += s.ds;
+                if (tauinteract < tau)
+                {
+                    m = s.m;
+                    sInt = s0 + ((tauinteract - t0) / (tau - t0)) * (sc - s0);
+                    found = 1;
+                    break;
+                }
+            }
+            if (!found) break;
+            if (m < 0)
+            {
+                c->errFlag |= 2;
+                break;
+            }
+            pk->L *= albedo(c, pk, m);
+            pk->rx += sInt * pk->kx;
+            pk->ry += sInt * pk->ky;
+            pk->rz += sInt * pk->kz;
+            if (pk->L <= 0) break;
+            if (peel) peel_off(c, pk, 1);
+            scatter(c, &rng, pk);
+        }
+    }
+    if (pk->ncontrib) record_contributions(c, pk);
+}
+
+int or_run_primary(or_ctx* c, uint64_t first, uint64_t count, uint64_t total_packets)
+{
+    if (!c->hasGrid || !c->dens || !c->nmix || !c->nsrc) return fail(c, SKGPU_ERR_STATE, "run: incomplete scene");
+    if (first + count > total_packets) return fail(c, SKGPU_ERR_ARG, "run: history range outside the segment");
+    if (c->opt.store_radiation_field)
+    {
+        size_t len = (size_t)c->numCells * c->nrf;
+        if (c->rfLen != len)
+        {
+            free(c->rf);
+            c->rf = (double*)calloc(len, sizeof(double));
+            c->rfLen = len;
+        }
+    }
+    memset(&c->cnt, 0, sizeof c->cnt);
+    c->errFlag = 0;
+    Path path = {NULL, 0, 0};
+    Packet pk;
+    memset(&pk, 0, sizeof pk);
+    for (uint64_t h = first; h < first + count; ++h) life_cycle(c, h, &path, &pk);
+    free(path.v);
+    free(pk.contrib);
+    c->cnt.kernel_launches = 0;
+    if (c->errFlag) return fail(c, SKGPU_ERR_DEVICE, "run: interaction point outside the grid");
+    return SKGPU_OK;
+}
+
+static void add_into(const double* src, size_t n, double* dst)
+{
+    if (!src || !dst) return;
+    for (size_t i = 0; i < n; ++i) dst[i] += src[i];
+}
+
+int or_fetch_instrument(or_ctx* c, int32_t i, double* ifu, double* sed, double* ifu_stats, double* sed_stats)
+{
+    if (i < 0 || i >= c->ninstr) return fail(c, SKGPU_ERR_ARG, "fetch: bad instrument index");
+    Instr* in = &c->instr[i];
+    if (in->d.kind == SKGPU_INSTR_FRAME)
+    {
+        add_into(in->ifu, in->n, ifu);
+        add_into(in->stats, 5 * in->n, ifu_stats);
+    }
+    else
+    {
+        add_into(in->sed, in->n, sed);
+        add_into(in->stats, 5 * in->n, sed_stats);
+    }
+    return SKGPU_OK;
+}
+
+int or_fetch_instrument_components(or_ctx* c, int32_t i, double* ifu3, double* sed3)
+{
+    if (i < 0 || i >= c->ninstr) return fail(c, SKGPU_ERR_ARG, "fetch: bad instrument index");
+    Instr* in = &c->instr[i];
+    if (!in->comp) return fail(c, SKGPU_ERR_STATE, "fetch: instrument does not record components");
+    add_into(in->comp, 3 * in->n, in->d.kind == SKGPU_INSTR_FRAME ? ifu3 : sed3);
+    return SKGPU_OK;
+}
+
+int or_fetch_radiation_field(or_ctx* c, double* rf)
+{
+    if (!c->rf) return fail(c, SKGPU_ERR_STATE, "fetch: no radiation field recorded");
+    add_into(c->rf, c->rfLen, rf);
+    return SKGPU_OK;
+}
+
+int or_clear_tallies(or_ctx* c)
+{
+    for (int i = 0; i < c->ninstr; ++i)
+    {
+        Instr* in = &c->instr[i];
+        if (in->ifu) memset(in->ifu, 0, in->n * sizeof(double));
+        if (in->sed) memset(in->sed, 0, in->n * sizeof(double));
+        if (in->comp) memset(in->comp, 0, 3 * in->n * sizeof(double));
+        if (in->stats) memset(in->stats, 0, 5 * in->n * sizeof(double));
+    }
+    if (c->rf) memset(c->rf, 0, c->rfLen * sizeof(double));
+    return SKGPU_OK;
+}
+
+int or_get_counters(or_ctx* c, skgpu_counters* out)
+{
+    *out = c->cnt;
+    return SKGPU_OK;
+}
+
+int or_last_run_ms(or_ctx* c, double* ms)
+{
+    (void)c;
+    *ms = 0.;
+    return SKGPU_OK;
+}
+
+int or_optical_depths(or_ctx* c, int32_t num_rays, const double* rays, double lambda, int32_t precision, double* tau)
+{
+    (void)precision;
+    if (!c->hasGrid || !c->dens || !c->nmix) return fail(c, SKGPU_ERR_STATE, "optical depths: incomplete scene");
+    double section = c->mixExt[locate_clip(c->mixLb, c->nmix, lambda)];
+    for (int r = 0; r < num_rays; ++r)
+    {
+        Gen s;
+        gen_start(&s, rays + 6 * (size_t)r);
+        double t = 0.;
+        while (gen_next(&c->g, &s))
+        {
+            if (s.m >= 0)
+            {
+                t += section * c->dens[s.m] * s.ds;
+                if (t >= 745.)
+                {
+                    t = INFINITY;
+                    break;
+                }
+            }
+        }
+        tau[r] = t;
+    }
+    return SKGPU_OK;
+}

@@ -1,0 +1,256 @@
+// Shared device helpers of the sm_100a photon-packet tracer: exact FP64 arithmetic without FMA
+// contraction (used where results must match the reference CPU generators bit for bit), the
+// Philox4x32-10 counter-based generator (one stream per history index), and the small sampling
+// routines of the life cycle.
+#pragma once
+
+#include <cstdint>
+#include <cfloat>
+#include <cmath>
+
+#define SKG_HD __host__ __device__ __forceinline__
+#define SKG_D __device__ __forceinline__
+
+namespace skg {
+
+// ---------------------------------------------------------------------------------------------
+// Exact IEEE double operations. The reference is compiled for x86-64 with SSE2 (no FMA), so
+// every multiply and add is rounded separately; __dmul_rn/__dadd_rn are never fused by nvcc.
+// ---------------------------------------------------------------------------------------------
+SKG_D double xmul(double a, double b) { return __dmul_rn(a, b); }
+SKG_D double xadd(double a, double b) { return __dadd_rn(a, b); }
+SKG_D double xsub(double a, double b) { return __dsub_rn(a, b); }
+// a*b + c*d + e*f evaluated left to right with separate roundings (Vec::dot, SKIRT/utils/Vec.hpp:70)
+SKG_D double xdot3(double a, double b, double c, double d, double e, double f)
+{
+    return xadd(xadd(xmul(a, b), xmul(c, d)), xmul(e, f));
+}
+
+// ---------------------------------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror & Shaw 2011, "Parallel random numbers: as easy as 1, 2, 3").
+// Each history draws from its own counter stream: key = seed, counter = (draw, 0, hist_lo, hist_hi).
+// ---------------------------------------------------------------------------------------------
+struct U4 { uint32_t x, y, z, w; };
+
+SKG_HD void mulhilo32(uint32_t a, uint32_t b, uint32_t& hi, uint32_t& lo)
+{
+    uint64_t p = static_cast<uint64_t>(a) * static_cast<uint64_t>(b);
+    hi = static_cast<uint32_t>(p >> 32);
+    lo = static_cast<uint32_t>(p);
+}
+
+SKG_HD U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1)
+{
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+    for (int r = 0; r < 10; ++r)
+    {
+        uint32_t hi0, lo0, hi1, lo1;
+        mulhilo32(M0, c.x, hi0, lo0);
+        mulhilo32(M1, c.z, hi1, lo1);
+        U4 n;
+        n.x = hi1 ^ c.y ^ k0;
+        n.y = lo1;
+        n.z = hi0 ^ c.w ^ k1;
+        n.w = lo0;
+        c = n;
+        k0 += W0;
+        k1 += W1;
+    }
+    return c;
+}
+
+// uniform deviate in the open interval (0,1) from 52 random bits: (j + 1/2) * 2^-52
+SKG_HD double u01_from_bits(uint32_t hi, uint32_t lo)
+{
+    uint64_t j = ((static_cast<uint64_t>(hi) << 32) | lo) >> 12;  // 52 bits
+    return (static_cast<double>(j) + 0.5) * 2.220446049250313080847e-16;
+}
+
+struct Rng
+{
+    uint32_t k0, k1;     // key (seed)
+    uint32_t c2, c3;     // history index
+    uint32_t ctr;        // draw block counter
+    int hasSpare;
+    double spare;
+
+    SKG_HD void start(uint64_t seed, uint64_t history)
+    {
+        k0 = static_cast<uint32_t>(seed);
+        k1 = static_cast<uint32_t>(seed >> 32);
+        c2 = static_cast<uint32_t>(history);
+        c3 = static_cast<uint32_t>(history >> 32);
+        ctr = 0;
+        hasSpare = 0;
+        spare = 0.;
+    }
+    SKG_HD double uniform()
+    {
+        if (hasSpare)
+        {
+            hasSpare = 0;
+            return spare;
+        }
+        U4 c{ctr++, 0u, c2, c3};
+        U4 r = philox4x32_10(c, k0, k1);
+        spare = u01_from_bits(r.z, r.w);
+        hasSpare = 1;
+        return u01_from_bits(r.x, r.y);
+    }
+};
+
+// ---------------------------------------------------------------------------------------------
+// Sampling helpers (restated from SKIRT/core/Random.cpp and DustMix.cpp)
+// ---------------------------------------------------------------------------------------------
+
+// Random::direction() (Random.cpp:121-128) with Direction(theta, phi) (Direction.cpp:11-37)
+SKG_D void isotropicDirection(Rng& rng, double& kx, double& ky, double& kz)
+{
+    double theta = acos(2.0 * rng.uniform() - 1.0);
+    double phi = 2.0 * M_PI * rng.uniform();
+    const double eps = 1e-8;
+    if (theta <= eps)
+    {
+        kx = 0.; ky = 0.; kz = 1.;
+    }
+    else if (theta >= M_PI - eps)
+    {
+        kx = 0.; ky = 0.; kz = -1.;
+    }
+    else
+    {
+        double st = sin(theta);
+        kx = st * cos(phi);
+        ky = st * sin(phi);
+        kz = cos(theta);
+    }
+}
+
+// Random::direction(bfk, costheta) (Random.cpp:130-163): rotate about the old direction
+SKG_D void rotateDirection(Rng& rng, double costheta, double& kx, double& ky, double& kz)
+{
+    double phi = 2.0 * M_PI * rng.uniform();
+    double cosphi = cos(phi);
+    double sinphi = sin(phi);
+    double sintheta = sqrt(fabs((1.0 - costheta) * (1.0 + costheta)));
+    double nx, ny, nz;
+    if (kz > 0.99999)
+    {
+        nx = cosphi * sintheta;
+        ny = sinphi * sintheta;
+        nz = costheta;
+    }
+    else if (kz < -0.99999)
+    {
+        nx = cosphi * sintheta;
+        ny = sinphi * sintheta;
+        nz = -costheta;
+    }
+    else
+    {
+        double root = sqrt((1.0 - kz) * (1.0 + kz));
+        nx = sintheta / root * (-kx * kz * cosphi + ky * sinphi) + kx * costheta;
+        ny = -sintheta / root * (ky * kz * cosphi + kx * sinphi) + ky * costheta;
+        nz = root * sintheta * cosphi + kz * costheta;
+    }
+    kx = nx;
+    ky = ny;
+    kz = nz;
+}
+
+// Random::exponCutoff (Random.cpp:105-121): exponential deviate truncated at xmax, by rejection
+SKG_D double exponCutoff(Rng& rng, double xmax)
+{
+    if (xmax == 0.0) return 0.0;
+    if (xmax < 1e-10) return rng.uniform() * xmax;
+    double c = 1.0 - exp(-xmax);
+    for (int guard = 0; guard < 64; ++guard)
+    {
+        double x = -log(1.0 - rng.uniform() * c);
+        if (x <= xmax) return x;
+    }
+    return xmax;
+}
+
+// Henyey-Greenstein phase function value and its 4-degree average for |g| > 0.95 (DustMix.cpp:395-428)
+SKG_D double valueHG(double g, double costheta)
+{
+    double t = 1. + g * g - 2. * g * costheta;
+    return (1. - g) * (1. + g) / sqrt(t * t * t);
+}
+SKG_D double integralHG(double g, double cosalpha, double cosbeta)
+{
+    double ta = sqrt(1. + g * g - 2. * g * cosalpha);
+    double tb = sqrt(1. + g * g - 2. * g * cosbeta);
+    double f1 = (1. - g) * (1. + g) / g;
+    double f2 = (tb - ta) / (tb * ta);
+    return f1 * f2;
+}
+SKG_D double meanHG(double g, double costheta)
+{
+    const double delta = 4. * M_PI / 180.;
+    double theta = acos(fmin(1., fmax(-1., costheta)));
+    double cosalpha = cos(theta - delta);
+    double cosbeta = cos(theta + delta);
+    if (theta < delta)
+        return (integralHG(g, 1., cosalpha) + integralHG(g, 1., cosbeta)) / (2. - cosalpha - cosbeta);
+    if (theta > M_PI - delta)
+        return (integralHG(g, cosalpha, -1.) + integralHG(g, cosbeta, -1.)) / (2. + cosalpha + cosbeta);
+    return integralHG(g, cosalpha, cosbeta) / (cosalpha - cosbeta);
+}
+SKG_D double phaseHG(double g, double costheta)
+{
+    return fabs(g) > 0.95 ? meanHG(g, costheta) : valueHG(g, costheta);
+}
+
+// SpecialFunctions::lnmean(x1, x2, lnx1, lnx2) (SKIRT/utils/SpecialFunctions.cpp:860-880)
+SKG_D double lnmean4(double x1, double x2, double lnx1, double lnx2)
+{
+    if (x1 > x2)
+    {
+        double t = x1; x1 = x2; x2 = t;
+        t = lnx1; lnx1 = lnx2; lnx2 = t;
+    }
+    if (x1 <= 0) return 0.;
+    double x = x2 / x1 - 1.;
+    if (x < 1e-3)
+        return x1 / (1. - 1. / 2. * x + 1. / 3. * x * x - 1. / 4. * x * x * x + 1. / 5. * x * x * x * x
+                     - 1. / 6. * x * x * x * x * x);
+    return (x2 - x1) / (lnx2 - lnx1);
+}
+
+// NR::locateClip on an ascending border array of n entries (SKIRT/utils/NR.hpp:177-182)
+template<typename T>
+SKG_HD int locateClip(const T* xv, int n, T x)
+{
+    if (x < xv[0]) return 0;
+    int jl = -1, ju = n - 1;
+    while (ju - jl > 1)
+    {
+        int jm = (ju + jl) >> 1;
+        if (x < xv[jm])
+            ju = jm;
+        else
+            jl = jm;
+    }
+    return jl;
+}
+
+// std::upper_bound index on an ascending array
+template<typename T>
+SKG_HD int upperBound(const T* xv, int n, T x)
+{
+    int lo = 0, hi = n;
+    while (lo < hi)
+    {
+        int mid = (lo + hi) >> 1;
+        if (x < xv[mid])
+            hi = mid;
+        else
+            lo = mid + 1;
+    }
+    return lo;
+}
+
+}  // namespace skg

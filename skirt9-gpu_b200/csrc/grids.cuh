@@ -1,0 +1,664 @@
+// Spatial-grid walkers of the tracer. Each walker is a device-side path segment generator with
+// the interface of SKIRT's PathSegmentGenerator (start / next / m / ds). The *Exact walkers keep
+// the reference generators' FP64 operation order with separate roundings, so that for identical
+// rays they return the same cell sequences and segment lengths as the CPU code:
+//   CartesianExact  <- CartesianSpatialGrid::MySegmentGenerator::next   (CartesianSpatialGrid.cpp:77-155)
+//   OctreeExact     <- TreeSpatialGrid::MySegmentGenerator::next        (TreeSpatialGrid.cpp:143-228)
+//   VoronoiExact    <- VoronoiMeshSnapshot::MySegmentGenerator::next    (VoronoiMeshSnapshot.cpp:1089-1222)
+//   TetraExact      <- TetraMeshSpatialGrid::MySegmentGenerator::next   (TetraMeshSpatialGrid.cpp:688-831)
+// and PathSegmentGenerator::moveInside (SKIRT/utils/PathSegmentGenerator.cpp:11-112).
+#pragma once
+
+#include "common.cuh"
+
+namespace skg {
+
+enum GenState { GS_UNKNOWN = 0, GS_INSIDE = 1, GS_OUTSIDE = 2 };
+
+// All device-resident grid data. Only the members of the uploaded grid kind are set.
+struct GridDev
+{
+    int kind;
+    double ext[6];  // xmin, ymin, zmin, xmax, ymax, zmax
+    double eps;
+    int numCells;
+
+    // Cartesian: borders (nx+1, ny+1, nz+1 entries)
+    const double* xb;
+    const double* yb;
+    const double* zb;
+    int nx, ny, nz;
+
+    // octree: per node bounds (6 doubles), cell index (-1 non-leaf), first child (-1 leaf),
+    // neighbour CSR per (node, wall)
+    const double* tBounds;
+    const int* tCell;
+    const int* tChild;
+    const int* tNbBegin;
+    const int* tNb;
+    int tNodes;
+
+    // Voronoi: sites, neighbour CSR (negative = wall), uniform site-search grid
+    const double* vSites;
+    const int* vNbBegin;
+    const int* vNb;
+    int vN;
+    int vGridN;            // blocks per dimension of the site search grid
+    const int* vBlkBegin;  // vGridN^3 + 1
+    const int* vBlkSites;  // site indices per block
+
+    // tetra: vertices, vertex indices (4 per tet), face normals (12 per tet), neighbour tet and
+    // face per face, tet bounding boxes, uniform tet-search grid
+    const double* teVerts;
+    const int* teTet;
+    const double* teNormals;
+    const int* teNTet;
+    const int* teNFace;
+    const double* teBox;
+    int teN;
+    int teGridN;
+    const int* teBlkBegin;
+    const int* teBlkTets;
+};
+
+// ---------------------------------------------------------------------------------------------
+// common generator state (PathSegmentGenerator)
+// ---------------------------------------------------------------------------------------------
+struct GenBase
+{
+    double rx, ry, rz, kx, ky, kz;
+    double ds;
+    int m;
+    int state;
+
+    SKG_D void startRay(double x, double y, double z, double ux, double uy, double uz)
+    {
+        state = GS_UNKNOWN;
+        rx = x; ry = y; rz = z;
+        kx = ux; ky = uy; kz = uz;
+        m = -1;
+        ds = 0.;
+    }
+    SKG_D void propagater(double d)
+    {
+        rx = xadd(rx, xmul(kx, d));
+        ry = xadd(ry, xmul(ky, d));
+        rz = xadd(rz, xmul(kz, d));
+    }
+    SKG_D static bool boxContains(const double* b, double x, double y, double z)
+    {
+        return x >= b[0] && x <= b[3] && y >= b[1] && y <= b[4] && z >= b[2] && z <= b[5];
+    }
+    // PathSegmentGenerator::moveInside (PathSegmentGenerator.cpp:11-112)
+    SKG_D bool moveInside(const double* b, double eps)
+    {
+        m = -1;
+        ds = 0.;
+        state = GS_OUTSIDE;
+        double cumds = 0.;
+        if (rx <= b[0])
+        {
+            if (kx <= 0.0) return false;
+            double d = (b[0] - rx) / kx;
+            rx = xadd(b[0], eps);
+            ry = xadd(ry, xmul(ky, d));
+            rz = xadd(rz, xmul(kz, d));
+            cumds = xadd(cumds, d);
+        }
+        else if (rx >= b[3])
+        {
+            if (kx >= 0.0) return false;
+            double d = (b[3] - rx) / kx;
+            rx = xsub(b[3], eps);
+            ry = xadd(ry, xmul(ky, d));
+            rz = xadd(rz, xmul(kz, d));
+            cumds = xadd(cumds, d);
+        }
+        if (ry <= b[1])
+        {
+            if (ky <= 0.0) return false;
+            double d = (b[1] - ry) / ky;
+            rx = xadd(rx, xmul(kx, d));
+            ry = xadd(b[1], eps);
+            rz = xadd(rz, xmul(kz, d));
+            cumds = xadd(cumds, d);
+        }
+        else if (ry >= b[4])
+        {
+            if (ky >= 0.0) return false;
+            double d = (b[4] - ry) / ky;
+            rx = xadd(rx, xmul(kx, d));
+            ry = xsub(b[4], eps);
+            rz = xadd(rz, xmul(kz, d));
+            cumds = xadd(cumds, d);
+        }
+        if (rz <= b[2])
+        {
+            if (kz <= 0.0) return false;
+            double d = (b[2] - rz) / kz;
+            rx = xadd(rx, xmul(kx, d));
+            ry = xadd(ry, xmul(ky, d));
+            rz = xadd(b[2], eps);
+            cumds = xadd(cumds, d);
+        }
+        else if (rz >= b[5])
+        {
+            if (kz >= 0.0) return false;
+            double d = (b[5] - rz) / kz;
+            rx = xadd(rx, xmul(kx, d));
+            ry = xadd(ry, xmul(ky, d));
+            rz = xsub(b[5], eps);
+            cumds = xadd(cumds, d);
+        }
+        if (!boxContains(b, rx, ry, rz)) return false;
+        m = -1;
+        ds = cumds;
+        state = GS_INSIDE;
+        return true;
+    }
+};
+
+// Box::diagonal (SKIRT/utils/Box.hpp:125-129) with separate roundings
+SKG_D double boxDiagonal(const double* b)
+{
+    double dx = xsub(b[3], b[0]), dy = xsub(b[4], b[1]), dz = xsub(b[5], b[2]);
+    return sqrt(xadd(xadd(xmul(dx, dx), xmul(dy, dy)), xmul(dz, dz)));
+}
+
+// ---------------------------------------------------------------------------------------------
+// Cartesian
+// ---------------------------------------------------------------------------------------------
+struct CartesianExact : GenBase
+{
+    int i, j, k;
+
+    SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz)
+    {
+        startRay(x, y, z, ux, uy, uz);
+    }
+
+    SKG_D bool next(const GridDev& g)
+    {
+        if (state == GS_OUTSIDE) return false;
+        if (state == GS_UNKNOWN)
+        {
+            if (!moveInside(g.ext, xmul(1e-12, boxDiagonal(g.ext)))) return false;
+            i = locateClip(g.xb, g.nx + 1, rx);
+            j = locateClip(g.yb, g.ny + 1, ry);
+            k = locateClip(g.zb, g.nz + 1, rz);
+            if (ds > 0.) return true;
+        }
+        // state == inside
+        int mm = k + g.nz * j + g.nz * g.ny * i;
+        double xE = (kx < 0.0) ? g.xb[i] : g.xb[i + 1];
+        double yE = (ky < 0.0) ? g.yb[j] : g.yb[j + 1];
+        double zE = (kz < 0.0) ? g.zb[k] : g.zb[k + 1];
+        double dsx = (fabs(kx) > 1e-15) ? xsub(xE, rx) / kx : DBL_MAX;
+        double dsy = (fabs(ky) > 1e-15) ? xsub(yE, ry) / ky : DBL_MAX;
+        double dsz = (fabs(kz) > 1e-15) ? xsub(zE, rz) / kz : DBL_MAX;
+        if (dsx <= dsy && dsx <= dsz)
+        {
+            m = mm; ds = dsx;
+            rx = xE;
+            ry = xadd(ry, xmul(ky, dsx));
+            rz = xadd(rz, xmul(kz, dsx));
+            i += (kx < 0.0) ? -1 : 1;
+            if (i >= g.nx || i < 0) state = GS_OUTSIDE;
+        }
+        else if (dsy < dsx && dsy <= dsz)
+        {
+            m = mm; ds = dsy;
+            ry = yE;
+            rx = xadd(rx, xmul(kx, dsy));
+            rz = xadd(rz, xmul(kz, dsy));
+            j += (ky < 0.0) ? -1 : 1;
+            if (j >= g.ny || j < 0) state = GS_OUTSIDE;
+        }
+        else
+        {
+            m = mm; ds = dsz;
+            rz = zE;
+            rx = xadd(rx, xmul(kx, dsz));
+            ry = xadd(ry, xmul(ky, dsz));
+            k += (kz < 0.0) ? -1 : 1;
+            if (k >= g.nz || k < 0) state = GS_OUTSIDE;
+        }
+        return true;
+    }
+};
+
+// ---------------------------------------------------------------------------------------------
+// Octree
+// ---------------------------------------------------------------------------------------------
+// TreeNode::leafChild from the root with OctTreeNode::child (TreeNode.cpp:66-76, OctTreeNode.cpp:37-42)
+SKG_D int octreeLeafChild(const GridDev& g, double x, double y, double z)
+{
+    const double* b = g.tBounds;
+    if (!GenBase::boxContains(b, x, y, z)) return -1;
+    int node = 0;
+    for (int guard = 0; guard < 64; ++guard)
+    {
+        int c0 = g.tChild[node];
+        if (c0 < 0) return node;
+        const double* cb = g.tBounds + 6 * static_cast<size_t>(c0);  // first child's rmax is the split point
+        int l = (x < cb[3] ? 0 : 1) + (y < cb[4] ? 0 : 2) + (z < cb[5] ? 0 : 4);
+        node = c0 + l;
+    }
+    return -1;
+}
+
+struct OctreeExact : GenBase
+{
+    int node;
+
+    SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz)
+    {
+        startRay(x, y, z, ux, uy, uz);
+        node = -1;
+    }
+
+    SKG_D bool next(const GridDev& g)
+    {
+        if (state == GS_OUTSIDE) return false;
+        if (state == GS_UNKNOWN)
+        {
+            if (!moveInside(g.ext, g.eps)) return false;
+            node = octreeLeafChild(g, rx, ry, rz);
+            if (node < 0)
+            {
+                state = GS_OUTSIDE;
+                return false;
+            }
+            if (ds > 0.) return true;
+        }
+        const double* b = g.tBounds + 6 * static_cast<size_t>(node);
+        double xnext = (kx < 0.0) ? b[0] : b[3];
+        double ynext = (ky < 0.0) ? b[1] : b[4];
+        double znext = (kz < 0.0) ? b[2] : b[5];
+        double dsx = (fabs(kx) > 1e-15) ? xsub(xnext, rx) / kx : DBL_MAX;
+        double dsy = (fabs(ky) > 1e-15) ? xsub(ynext, ry) / ky : DBL_MAX;
+        double dsz = (fabs(kz) > 1e-15) ? xsub(znext, rz) / kz : DBL_MAX;
+        double d;
+        int wall;
+        if (dsx <= dsy && dsx <= dsz)
+        {
+            d = dsx;
+            wall = (kx < 0.0) ? 0 : 1;
+        }
+        else if (dsy <= dsx && dsy <= dsz)
+        {
+            d = dsy;
+            wall = (ky < 0.0) ? 2 : 3;
+        }
+        else
+        {
+            d = dsz;
+            wall = (kz < 0.0) ? 4 : 5;
+        }
+        propagater(xadd(d, g.eps));
+        m = g.tCell[node];
+        ds = d;
+        int old = node;
+        // TreeNode::neighbor: first neighbour across the wall (overlap-sorted) containing r
+        int nb = -1;
+        int e0 = g.tNbBegin[6 * node + wall], e1 = g.tNbBegin[6 * node + wall + 1];
+        for (int e = e0; e < e1; ++e)
+        {
+            int cand = g.tNb[e];
+            if (boxContains(g.tBounds + 6 * static_cast<size_t>(cand), rx, ry, rz))
+            {
+                nb = cand;
+                break;
+            }
+        }
+        if (nb < 0) nb = octreeLeafChild(g, rx, ry, rz);
+        if (nb == old)
+        {
+            rx = nextafter(rx, (kx < 0.) ? -DBL_MAX : DBL_MAX);
+            ry = nextafter(ry, (ky < 0.) ? -DBL_MAX : DBL_MAX);
+            rz = nextafter(rz, (kz < 0.) ? -DBL_MAX : DBL_MAX);
+            nb = octreeLeafChild(g, rx, ry, rz);
+        }
+        node = nb;
+        if (nb < 0 || nb == old) state = GS_OUTSIDE;
+        return true;
+    }
+};
+
+// ---------------------------------------------------------------------------------------------
+// Voronoi
+// ---------------------------------------------------------------------------------------------
+// Nearest site by an expanding search over a uniform block grid of sites. Returns the site with
+// the smallest squared distance (VoronoiMeshSnapshot::cellIndex, VoronoiMeshSnapshot.cpp:1037-1067,
+// selects the same site except for exactly equidistant ties).
+SKG_D int voronoiCellIndex(const GridDev& g, double x, double y, double z)
+{
+    if (!GenBase::boxContains(g.ext, x, y, z)) return -1;
+    const int n = g.vGridN;
+    double wx = (g.ext[3] - g.ext[0]) / n, wy = (g.ext[4] - g.ext[1]) / n, wz = (g.ext[5] - g.ext[2]) / n;
+    int bi = min(n - 1, max(0, static_cast<int>((x - g.ext[0]) / wx)));
+    int bj = min(n - 1, max(0, static_cast<int>((y - g.ext[1]) / wy)));
+    int bk = min(n - 1, max(0, static_cast<int>((z - g.ext[2]) / wz)));
+    int best = -1;
+    double bestd = DBL_MAX;
+    double wmin = fmin(wx, fmin(wy, wz));
+    for (int ring = 0; ring <= n; ++ring)
+    {
+        int i0 = bi - ring, i1 = bi + ring, j0 = bj - ring, j1 = bj + ring, k0 = bk - ring, k1 = bk + ring;
+        for (int i = max(0, i0); i <= min(n - 1, i1); ++i)
+            for (int j = max(0, j0); j <= min(n - 1, j1); ++j)
+                for (int k = max(0, k0); k <= min(n - 1, k1); ++k)
+                {
+                    // only the shell of this ring
+                    if (i != i0 && i != i1 && j != j0 && j != j1 && k != k0 && k != k1) continue;
+                    int blk = (i * n + j) * n + k;
+                    for (int e = g.vBlkBegin[blk]; e < g.vBlkBegin[blk + 1]; ++e)
+                    {
+                        int s = g.vBlkSites[e];
+                        const double* p = g.vSites + 3 * static_cast<size_t>(s);
+                        double dx = xsub(p[0], x), dy = xsub(p[1], y), dz = xsub(p[2], z);
+                        double d2 = xadd(xadd(xmul(dx, dx), xmul(dy, dy)), xmul(dz, dz));
+                        if (d2 < bestd || (d2 == bestd && s < best))
+                        {
+                            bestd = d2;
+                            best = s;
+                        }
+                    }
+                }
+        // every unsearched site is at least ring*wmin away from the query point
+        if (best >= 0)
+        {
+            double reach = ring * wmin;
+            if (reach * reach > bestd) break;
+        }
+    }
+    return best;
+}
+
+struct VoronoiExact : GenBase
+{
+    int mr;
+
+    SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz)
+    {
+        startRay(x, y, z, ux, uy, uz);
+        mr = -1;
+    }
+
+    SKG_D bool next(const GridDev& g)
+    {
+        if (state == GS_OUTSIDE) return false;
+        if (state == GS_UNKNOWN)
+        {
+            if (!moveInside(g.ext, g.eps)) return false;
+            mr = voronoiCellIndex(g, rx, ry, rz);
+            if (mr < 0)
+            {
+                state = GS_OUTSIDE;
+                return false;
+            }
+            if (ds > 0.) return true;
+        }
+        for (int guard = 0; guard < 1000; ++guard)
+        {
+            const double* pr = g.vSites + 3 * static_cast<size_t>(mr);
+            double sq = DBL_MAX;
+            const int NO_INDEX = -99;
+            int mq = NO_INDEX;
+            for (int e = g.vNbBegin[mr]; e < g.vNbBegin[mr + 1]; ++e)
+            {
+                int mi = g.vNb[e];
+                double si = 0;
+                if (mi >= 0)
+                {
+                    const double* pi = g.vSites + 3 * static_cast<size_t>(mi);
+                    double nx = xsub(pi[0], pr[0]), ny = xsub(pi[1], pr[1]), nz = xsub(pi[2], pr[2]);
+                    double ndotk = xdot3(nx, kx, ny, ky, nz, kz);
+                    if (ndotk > 0)
+                    {
+                        double px = xmul(0.5, xadd(pi[0], pr[0]));
+                        double py = xmul(0.5, xadd(pi[1], pr[1]));
+                        double pz = xmul(0.5, xadd(pi[2], pr[2]));
+                        si = xdot3(nx, xsub(px, rx), ny, xsub(py, ry), nz, xsub(pz, rz)) / ndotk;
+                    }
+                }
+                else
+                {
+                    switch (mi)
+                    {
+                        case -1: si = xsub(g.ext[0], rx) / kx; break;
+                        case -2: si = xsub(g.ext[3], rx) / kx; break;
+                        case -3: si = xsub(g.ext[1], ry) / ky; break;
+                        case -4: si = xsub(g.ext[4], ry) / ky; break;
+                        case -5: si = xsub(g.ext[2], rz) / kz; break;
+                        case -6: si = xsub(g.ext[5], rz) / kz; break;
+                        default: si = 0; break;
+                    }
+                }
+                if (si > 0 && si < sq)
+                {
+                    sq = si;
+                    mq = mi;
+                }
+            }
+            if (mq == NO_INDEX)
+            {
+                propagater(g.eps);
+                mr = voronoiCellIndex(g, rx, ry, rz);
+                if (mr < 0)
+                {
+                    state = GS_OUTSIDE;
+                    return false;
+                }
+            }
+            else
+            {
+                propagater(xadd(sq, g.eps));
+                m = mr;
+                ds = sq;
+                mr = mq;
+                if (mr < 0) state = GS_OUTSIDE;
+                return true;
+            }
+        }
+        state = GS_OUTSIDE;
+        return false;
+    }
+};
+
+// ---------------------------------------------------------------------------------------------
+// Tetrahedral mesh
+// ---------------------------------------------------------------------------------------------
+SKG_D void teVertex(const GridDev& g, int t, int v, double& x, double& y, double& z)
+{
+    const double* p = g.teVerts + 3 * static_cast<size_t>(g.teTet[4 * static_cast<size_t>(t) + v]);
+    x = p[0]; y = p[1]; z = p[2];
+}
+
+// Tetra::contains (TetraMeshSpatialGrid.cpp:114-138)
+SKG_D bool teContains(const GridDev& g, int t, double x, double y, double z)
+{
+    if (!GenBase::boxContains(g.teBox + 6 * static_cast<size_t>(t), x, y, z)) return false;
+    const double* nrm = g.teNormals + 12 * static_cast<size_t>(t);
+    double vx, vy, vz;
+    teVertex(g, t, 3, vx, vy, vz);
+    for (int f = 0; f <= 2; ++f)
+    {
+        if (xdot3(xsub(vx, x), nrm[3 * f], xsub(vy, y), nrm[3 * f + 1], xsub(vz, z), nrm[3 * f + 2]) < 0) return false;
+    }
+    teVertex(g, t, 0, vx, vy, vz);
+    if (xdot3(xsub(vx, x), nrm[9], xsub(vy, y), nrm[10], xsub(vz, z), nrm[11]) < 0.) return false;
+    return true;
+}
+
+// TetraMeshSpatialGrid::cellIndex (TetraMeshSpatialGrid.cpp:615-622): first tetrahedron of the
+// position's search block that contains it
+SKG_D int tetraCellIndex(const GridDev& g, double x, double y, double z)
+{
+    if (!GenBase::boxContains(g.ext, x, y, z)) return -1;
+    const int n = g.teGridN;
+    int bi = min(n - 1, max(0, static_cast<int>(n * (x - g.ext[0]) / (g.ext[3] - g.ext[0]))));
+    int bj = min(n - 1, max(0, static_cast<int>(n * (y - g.ext[1]) / (g.ext[4] - g.ext[1]))));
+    int bk = min(n - 1, max(0, static_cast<int>(n * (z - g.ext[2]) / (g.ext[5] - g.ext[2]))));
+    int blk = (bi * n + bj) * n + bk;
+    for (int e = g.teBlkBegin[blk]; e < g.teBlkBegin[blk + 1]; ++e)
+    {
+        int t = g.teBlkTets[e];
+        if (teContains(g, t, x, y, z)) return t;
+    }
+    return -1;
+}
+
+// clockwiseVertices (TetraMeshSpatialGrid.cpp:44-50)
+SKG_D void clockwiseVertices(int face, int cv[3])
+{
+    cv[0] = (face + 3) % 4;
+    cv[1] = (face + 2) % 4;
+    cv[2] = (face + 1) % 4;
+    if (face % 2 == 0)
+    {
+        int t = cv[0]; cv[0] = cv[2]; cv[2] = t;
+    }
+}
+
+// Vec::cross (SKIRT/utils/Vec.hpp:73-76)
+SKG_D void xcross(double ax, double ay, double az, double bx, double by, double bz, double& cx, double& cy, double& cz)
+{
+    cx = xsub(xmul(ay, bz), xmul(az, by));
+    cy = xsub(xmul(az, bx), xmul(ax, bz));
+    cz = xsub(xmul(ax, by), xmul(ay, bx));
+}
+
+struct TetraExact : GenBase
+{
+    int mr;
+    int enteringFace;
+
+    SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz)
+    {
+        startRay(x, y, z, ux, uy, uz);
+        mr = -1;
+        enteringFace = -1;
+    }
+
+    // Tetra::findEnteringFace (TetraMeshSpatialGrid.cpp:87-112)
+    SKG_D int findEnteringFace(const GridDev& g, int t) const
+    {
+        const int etable[6][2] = {{3, 2}, {1, 3}, {2, 1}, {3, 0}, {0, 2}, {1, 0}};
+        int e = 0;
+        for (int t1 = 0; t1 < 3; t1++)
+        {
+            double v1x, v1y, v1z;
+            teVertex(g, t, t1, v1x, v1y, v1z);
+            for (int t2 = t1 + 1; t2 < 4; t2++)
+            {
+                double v2x, v2y, v2z;
+                teVertex(g, t, t2, v2x, v2y, v2z);
+                double mx, my, mz;
+                xcross(kx, ky, kz, xsub(rx, v1x), xsub(ry, v1y), xsub(rz, v1z), mx, my, mz);
+                double prod = xdot3(mx, xsub(v2x, v1x), my, xsub(v2y, v1y), mz, xsub(v2z, v1z));
+                if (prod != 0.) return prod < 0 ? etable[e][0] : etable[e][1];
+                e++;
+            }
+        }
+        return -1;
+    }
+
+    SKG_D bool next(const GridDev& g)
+    {
+        if (state == GS_OUTSIDE) return false;
+        if (state == GS_UNKNOWN)
+        {
+            if (!moveInside(g.ext, g.eps)) return false;
+            mr = tetraCellIndex(g, rx, ry, rz);
+            enteringFace = -1;
+            if (mr == -1)
+            {
+                state = GS_OUTSIDE;
+                return false;
+            }
+            if (ds > 0.) return true;
+        }
+        for (int guard = 0; guard < 1000; ++guard)
+        {
+            int leavingFace = -1;
+            double d = DBL_MAX;
+            if (enteringFace == -1) enteringFace = findEnteringFace(g, mr);
+            if (enteringFace < 0) enteringFace = 0;  // degenerate direction: the plane fallback below decides
+            double vex, vey, vez;
+            teVertex(g, mr, enteringFace, vex, vey, vez);
+            double mx, my, mz;
+            xcross(kx, ky, kz, xsub(rx, vex), xsub(ry, vey), xsub(rz, vez), mx, my, mz);
+            int cv[3];
+            clockwiseVertices(enteringFace, cv);
+            double c0x, c0y, c0z;
+            teVertex(g, mr, cv[0], c0x, c0y, c0z);
+            double prod0 = xdot3(mx, xsub(vex, c0x), my, xsub(vey, c0y), mz, xsub(vez, c0z));
+            int clock0 = prod0 < 0;
+            int i = clock0 ? 1 : 2;
+            double cix, ciy, ciz;
+            teVertex(g, mr, cv[i], cix, ciy, ciz);
+            double prodi = xdot3(mx, xsub(vex, cix), my, xsub(vey, ciy), mz, xsub(vez, ciz));
+            int cclocki = prodi >= 0;
+            const double* nrm = g.teNormals + 12 * static_cast<size_t>(mr);
+            if (prod0 == 0. || prodi == 0.)
+            {
+                for (int q = 0; q < 3; ++q)
+                {
+                    int face = cv[q];
+                    const double* n = nrm + 3 * face;
+                    double ndotk = xdot3(n[0], kx, n[1], ky, n[2], kz);
+                    if (ndotk > 0)
+                    {
+                        double dq = xdot3(n[0], xsub(vex, rx), n[1], xsub(vey, ry), n[2], xsub(vez, rz)) / ndotk;
+                        if (dq < d)
+                        {
+                            d = dq;
+                            leavingFace = face;
+                        }
+                    }
+                }
+            }
+            else
+            {
+                const int dtable[2][2] = {{1, 0}, {0, 2}};
+                leavingFace = cv[dtable[clock0][cclocki]];
+                const double* n = nrm + 3 * leavingFace;
+                double ndotk = xdot3(n[0], kx, n[1], ky, n[2], kz);
+                d = xdot3(n[0], xsub(vex, rx), n[1], xsub(vey, ry), n[2], xsub(vez, rz)) / ndotk;
+            }
+            if (leavingFace == -1 || d < g.eps)
+            {
+                propagater(g.eps);
+                mr = tetraCellIndex(g, rx, ry, rz);
+                if (mr < 0)
+                {
+                    state = GS_OUTSIDE;
+                    return false;
+                }
+                enteringFace = -1;
+            }
+            else
+            {
+                propagater(d);
+                m = mr;
+                ds = d;
+                int nt = g.teNTet[4 * static_cast<size_t>(mr) + leavingFace];
+                int nf = g.teNFace[4 * static_cast<size_t>(mr) + leavingFace];
+                mr = nt;
+                if (mr < 0)
+                {
+                    // the reference drops the final in-mesh segment when the path leaves the hull
+                    state = GS_OUTSIDE;
+                    return false;
+                }
+                enteringFace = nf;
+                return true;
+            }
+        }
+        state = GS_OUTSIDE;
+        return false;
+    }
+};
+
+}  // namespace skg

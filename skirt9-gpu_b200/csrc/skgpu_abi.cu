@@ -1,0 +1,847 @@
+// The C ABI of include/skgpu.h: context, uploads into HBM, the life-cycle launch, tallies.
+//
+// Host data layouts follow what SKIRT's objects already hold (border arrays, CSR neighbour lists,
+// MediumState densities, DustMix tables), so the SKIRT-side bridge only copies flat arrays. The
+// library builds two search structures of its own at upload time: a uniform site grid for the
+// Voronoi nearest-site search and a uniform grid of tetrahedron bounding boxes for the tetra
+// cell search.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/skgpu.h"
+#include "internal.hpp"
+
+using namespace skg;
+
+namespace {
+
+struct DevArray
+{
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace
+
+struct skgpu_ctx
+{
+    int device = 0;
+    int numSMs = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string err;
+    double lastMs = 0.;
+
+    GridDev g{};
+    bool hasGrid = false;
+    std::vector<void*> gridBufs;
+
+    double* dens = nullptr;
+    int numCells = 0;
+
+    double *mixLb = nullptr, *mixExt = nullptr, *mixSca = nullptr, *mixG = nullptr;
+    int nmix = 0;
+
+    int nrf = 0, rfNb = 0;
+    double* rfB = nullptr;
+    int* rfEll = nullptr;
+    double* rf = nullptr;
+    size_t rfLen = 0;
+
+    std::vector<SourceDev> srcHost;
+    SourceDev* src = nullptr;
+    double *tabL = nullptr, *tabA = nullptr, *tabB = nullptr, *radR = nullptr, *radP = nullptr;
+
+    std::vector<InstrDev> instrHost;
+    InstrDev* instr = nullptr;
+    std::vector<void*> instrBufs;
+    double* wlgB = nullptr;
+    int* wlgEll = nullptr;
+
+    skgpu_options opt{};
+    bool hasOptions = false;
+
+    unsigned long long* work = nullptr;
+    unsigned long long* counters = nullptr;
+    int* errFlag = nullptr;
+    skgpu_counters lastCounters{};
+};
+
+namespace {
+
+int fail(skgpu_ctx* c, int code, const std::string& msg)
+{
+    if (c) c->err = msg;
+    return code;
+}
+
+#define CK(call)                                                                                   \
+    do                                                                                             \
+    {                                                                                              \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return fail(ctx, SKGPU_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+template<typename T>
+cudaError_t devAlloc(T** p, size_t n)
+{
+    *p = nullptr;
+    if (n == 0) n = 1;
+    return cudaMalloc(reinterpret_cast<void**>(p), n * sizeof(T));
+}
+
+template<typename T>
+cudaError_t devUpload(T** p, const T* host, size_t n)
+{
+    cudaError_t e = devAlloc(p, n);
+    if (e != cudaSuccess) return e;
+    if (n && host) e = cudaMemcpy(*p, host, n * sizeof(T), cudaMemcpyHostToDevice);
+    return e;
+}
+
+template<typename T>
+void devFree(T*& p)
+{
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+void freeGrid(skgpu_ctx* ctx)
+{
+    for (void* p : ctx->gridBufs) cudaFree(p);
+    ctx->gridBufs.clear();
+    ctx->g = GridDev{};
+    ctx->hasGrid = false;
+}
+
+template<typename T>
+int gridUpload(skgpu_ctx* ctx, const T** dst, const T* host, size_t n)
+{
+    T* d = nullptr;
+    CK(devUpload(&d, host, n));
+    ctx->gridBufs.push_back(d);
+    *dst = d;
+    return SKGPU_OK;
+}
+
+void freeInstruments(skgpu_ctx* ctx)
+{
+    for (void* p : ctx->instrBufs) cudaFree(p);
+    ctx->instrBufs.clear();
+    ctx->instrHost.clear();
+    devFree(ctx->instr);
+    devFree(ctx->wlgB);
+    devFree(ctx->wlgEll);
+}
+
+bool finiteAll(const double* v, size_t n)
+{
+    for (size_t i = 0; i < n; ++i)
+        if (!std::isfinite(v[i])) return false;
+    return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+int skgpu_abi_version(void) { return SKGPU_ABI_VERSION; }
+
+int skgpu_create(int device, skgpu_ctx** out)
+{
+    if (!out) return SKGPU_ERR_ARG;
+    *out = nullptr;
+    skgpu_ctx* ctx = new skgpu_ctx();
+    ctx->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->numSMs, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev1);
+    if (e == cudaSuccess) e = devAlloc(&ctx->work, 1);
+    if (e == cudaSuccess) e = devAlloc(&ctx->counters, 8);
+    if (e == cudaSuccess) e = devAlloc(&ctx->errFlag, 1);
+    if (e != cudaSuccess)
+    {
+        // keep the context so the caller can read the message; the handle must still be destroyed
+        ctx->err = std::string("skgpu_create: ") + cudaGetErrorString(e);
+        *out = ctx;
+        return SKGPU_ERR_CUDA;
+    }
+    ctx->opt.force_scattering = 1;
+    ctx->opt.min_weight_reduction = 1e4;
+    ctx->opt.path_length_bias = 0.5;
+    ctx->opt.peel_off = 1;
+    *out = ctx;
+    return SKGPU_OK;
+}
+
+void skgpu_destroy(skgpu_ctx* ctx)
+{
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    freeGrid(ctx);
+    freeInstruments(ctx);
+    devFree(ctx->dens);
+    devFree(ctx->mixLb);
+    devFree(ctx->mixExt);
+    devFree(ctx->mixSca);
+    devFree(ctx->mixG);
+    devFree(ctx->rfB);
+    devFree(ctx->rfEll);
+    devFree(ctx->rf);
+    devFree(ctx->src);
+    devFree(ctx->tabL);
+    devFree(ctx->tabA);
+    devFree(ctx->tabB);
+    devFree(ctx->radR);
+    devFree(ctx->radP);
+    devFree(ctx->work);
+    devFree(ctx->counters);
+    devFree(ctx->errFlag);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char* skgpu_last_error(const skgpu_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+// ------------------------------------------------------------------------------------------------
+// grids
+// ------------------------------------------------------------------------------------------------
+
+int skgpu_upload_grid_cartesian(skgpu_ctx* ctx, const double* xb, int32_t nxb, const double* yb, int32_t nyb,
+                                const double* zb, int32_t nzb)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (!xb || !yb || !zb || nxb < 2 || nyb < 2 || nzb < 2)
+        return fail(ctx, SKGPU_ERR_ARG, "cartesian grid needs at least 2 borders per axis");
+    auto ascending = [](const double* v, int n) {
+        for (int i = 1; i < n; ++i)
+            if (!(v[i] > v[i - 1])) return false;
+        return true;
+    };
+    if (!ascending(xb, nxb) || !ascending(yb, nyb) || !ascending(zb, nzb))
+        return fail(ctx, SKGPU_ERR_ARG, "cartesian borders must be strictly ascending");
+    CK(cudaSetDevice(ctx->device));
+    freeGrid(ctx);
+    GridDev& g = ctx->g;
+    g.kind = SKGPU_GRID_CARTESIAN;
+    g.nx = nxb - 1;
+    g.ny = nyb - 1;
+    g.nz = nzb - 1;
+    g.ext[0] = xb[0]; g.ext[1] = yb[0]; g.ext[2] = zb[0];
+    g.ext[3] = xb[nxb - 1]; g.ext[4] = yb[nyb - 1]; g.ext[5] = zb[nzb - 1];
+    long long nc = 1LL * g.nx * g.ny * g.nz;
+    if (nc > 2147483647LL) return fail(ctx, SKGPU_ERR_ARG, "too many cells");
+    g.numCells = static_cast<int>(nc);
+    int rc;
+    if ((rc = gridUpload(ctx, &g.xb, xb, nxb))) return rc;
+    if ((rc = gridUpload(ctx, &g.yb, yb, nyb))) return rc;
+    if ((rc = gridUpload(ctx, &g.zb, zb, nzb))) return rc;
+    ctx->hasGrid = true;
+    return SKGPU_OK;
+}
+
+int skgpu_upload_grid_octree(skgpu_ctx* ctx, int32_t num_nodes, const double* bounds, const int32_t* cell_index,
+                             const int32_t* child_begin, const int32_t* child_count, const int32_t* child_index,
+                             int32_t num_child_index, const int32_t* nb_begin, const int32_t* nb_index,
+                             int32_t num_nb_index, double eps)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (num_nodes < 1 || !bounds || !cell_index || !child_begin || !child_count || !nb_begin)
+        return fail(ctx, SKGPU_ERR_ARG, "octree: missing arrays");
+    if (num_child_index < 0 || num_nb_index < 0) return fail(ctx, SKGPU_ERR_ARG, "octree: negative sizes");
+    // first-child table; OctTreeNode children are created with consecutive ids (OctTreeNode.cpp:15-25)
+    std::vector<int> firstChild(num_nodes, -1);
+    int numCells = 0;
+    for (int l = 0; l < num_nodes; ++l)
+    {
+        int cnt = child_count[l];
+        if (cnt == 0)
+        {
+            if (cell_index[l] < 0) return fail(ctx, SKGPU_ERR_ARG, "octree: leaf without cell index");
+            numCells = std::max(numCells, cell_index[l] + 1);
+            continue;
+        }
+        if (cnt != 8) return fail(ctx, SKGPU_ERR_UNSUPPORTED, "octree: only 8-way subdivision is supported");
+        int b = child_begin[l];
+        if (b < 0 || b + 8 > num_child_index) return fail(ctx, SKGPU_ERR_ARG, "octree: child index out of range");
+        int c0 = child_index[b];
+        for (int q = 0; q < 8; ++q)
+            if (child_index[b + q] != c0 + q || c0 + q >= num_nodes)
+                return fail(ctx, SKGPU_ERR_ARG, "octree: children must have consecutive node ids");
+        firstChild[l] = c0;
+    }
+    if (nb_begin[0] != 0 || nb_begin[6 * static_cast<size_t>(num_nodes)] != num_nb_index)
+        return fail(ctx, SKGPU_ERR_ARG, "octree: neighbour CSR inconsistent");
+    for (int e = 0; e < num_nb_index; ++e)
+        if (nb_index[e] < 0 || nb_index[e] >= num_nodes) return fail(ctx, SKGPU_ERR_ARG, "octree: neighbour id out of range");
+    if (!finiteAll(bounds, 6 * static_cast<size_t>(num_nodes))) return fail(ctx, SKGPU_ERR_ARG, "octree: non-finite bounds");
+    CK(cudaSetDevice(ctx->device));
+    freeGrid(ctx);
+    GridDev& g = ctx->g;
+    g.kind = SKGPU_GRID_OCTREE;
+    for (int q = 0; q < 6; ++q) g.ext[q] = bounds[q];
+    g.eps = eps;
+    g.tNodes = num_nodes;
+    g.numCells = numCells;
+    int rc;
+    if ((rc = gridUpload(ctx, &g.tBounds, bounds, 6 * static_cast<size_t>(num_nodes)))) return rc;
+    if ((rc = gridUpload<int>(ctx, &g.tCell, cell_index, num_nodes))) return rc;
+    if ((rc = gridUpload<int>(ctx, &g.tChild, firstChild.data(), num_nodes))) return rc;
+    if ((rc = gridUpload<int>(ctx, &g.tNbBegin, nb_begin, 6 * static_cast<size_t>(num_nodes) + 1))) return rc;
+    if ((rc = gridUpload<int>(ctx, &g.tNb, nb_index, num_nb_index))) return rc;
+    ctx->hasGrid = true;
+    return SKGPU_OK;
+}
+
+int skgpu_upload_grid_voronoi(skgpu_ctx* ctx, int32_t num_sites, const double* sites, const int32_t* nb_begin,
+                              const int32_t* nb_index, int32_t num_nb_index, const double* extent, double eps)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (num_sites < 1 || !sites || !nb_begin || !extent) return fail(ctx, SKGPU_ERR_ARG, "voronoi: missing arrays");
+    if (nb_begin[0] != 0 || nb_begin[num_sites] != num_nb_index) return fail(ctx, SKGPU_ERR_ARG, "voronoi: neighbour CSR inconsistent");
+    for (int e = 0; e < num_nb_index; ++e)
+        if (nb_index[e] >= num_sites || nb_index[e] < -6) return fail(ctx, SKGPU_ERR_ARG, "voronoi: neighbour id out of range");
+    if (!finiteAll(sites, 3 * static_cast<size_t>(num_sites))) return fail(ctx, SKGPU_ERR_ARG, "voronoi: non-finite sites");
+    // uniform site-search grid, about two sites per block
+    int n = static_cast<int>(std::cbrt(num_sites / 2.0));
+    n = std::max(1, std::min(256, n));
+    std::vector<int> cnt(static_cast<size_t>(n) * n * n + 1, 0), blk(num_sites);
+    for (int s = 0; s < num_sites; ++s)
+    {
+        auto idx = [&](double x, double lo, double hi) {
+            return std::min(n - 1, std::max(0, static_cast<int>((x - lo) / ((hi - lo) / n))));
+        };
+        int i = idx(sites[3 * s], extent[0], extent[3]);
+        int j = idx(sites[3 * s + 1], extent[1], extent[4]);
+        int k = idx(sites[3 * s + 2], extent[2], extent[5]);
+        blk[s] = (i * n + j) * n + k;
+        cnt[blk[s] + 1]++;
+    }
+    for (size_t b = 1; b < cnt.size(); ++b) cnt[b] += cnt[b - 1];
+    std::vector<int> fill(cnt.begin(), cnt.end() - 1), list(num_sites);
+    for (int s = 0; s < num_sites; ++s) list[fill[blk[s]]++] = s;
+    CK(cudaSetDevice(ctx->device));
+    freeGrid(ctx);
+    GridDev& g = ctx->g;
+    g.kind = SKGPU_GRID_VORONOI;
+    for (int q = 0; q < 6; ++q) g.ext[q] = extent[q];
+    g.eps = eps;
+    g.vN = num_sites;
+    g.numCells = num_sites;
+    g.vGridN = n;
+    int rc;
+    if ((rc = gridUpload(ctx, &g.vSites, sites, 3 * static_cast<size_t>(num_sites)))) return rc;
+    if ((rc = gridUpload<int>(ctx, &g.vNbBegin, nb_begin, num_sites + 1))) return rc;
+    if ((rc = gridUpload<int>(ctx, &g.vNb, nb_index, num_nb_index))) return rc;
+    if ((rc = gridUpload<int>(ctx, &g.vBlkBegin, cnt.data(), cnt.size()))) return rc;
+    if ((rc = gridUpload<int>(ctx, &g.vBlkSites, list.data(), list.size()))) return rc;
+    ctx->hasGrid = true;
+    return SKGPU_OK;
+}
+
+int skgpu_upload_grid_tetra(skgpu_ctx* ctx, int32_t num_vertices, const double* vertices, int32_t num_tetra,
+                            const int32_t* tetra_vertices, const double* face_normals, const int32_t* face_ntetra,
+                            const int32_t* face_nface, const double* extent, double eps)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (num_vertices < 4 || num_tetra < 1 || !vertices || !tetra_vertices || !face_normals || !face_ntetra
+        || !face_nface || !extent)
+        return fail(ctx, SKGPU_ERR_ARG, "tetra: missing arrays");
+    size_t nt = static_cast<size_t>(num_tetra);
+    for (size_t q = 0; q < 4 * nt; ++q)
+    {
+        if (tetra_vertices[q] < 0 || tetra_vertices[q] >= num_vertices) return fail(ctx, SKGPU_ERR_ARG, "tetra: vertex index out of range");
+        if (face_ntetra[q] >= num_tetra || face_ntetra[q] < -1) return fail(ctx, SKGPU_ERR_ARG, "tetra: neighbour out of range");
+        if (face_nface[q] < -1 || face_nface[q] > 3) return fail(ctx, SKGPU_ERR_ARG, "tetra: face index out of range");
+    }
+    // bounding boxes (Tetra constructor, TetraMeshSpatialGrid.cpp:54-81) and a uniform box grid
+    std::vector<double> box(6 * nt);
+    for (size_t t = 0; t < nt; ++t)
+    {
+        double b[6] = {DBL_MAX, DBL_MAX, DBL_MAX, -DBL_MAX, -DBL_MAX, -DBL_MAX};
+        for (int v = 0; v < 4; ++v)
+        {
+            const double* p = vertices + 3 * static_cast<size_t>(tetra_vertices[4 * t + v]);
+            for (int a = 0; a < 3; ++a)
+            {
+                b[a] = std::min(b[a], p[a]);
+                b[3 + a] = std::max(b[3 + a], p[a]);
+            }
+        }
+        std::memcpy(&box[6 * t], b, sizeof b);
+    }
+    int n = static_cast<int>(std::cbrt(num_tetra / 2.0));
+    n = std::max(1, std::min(192, n));
+    auto bidx = [&](double x, int a) {
+        return std::min(n - 1, std::max(0, static_cast<int>(n * (x - extent[a]) / (extent[3 + a] - extent[a]))));
+    };
+    std::vector<long long> cnt(static_cast<size_t>(n) * n * n + 1, 0);
+    for (size_t t = 0; t < nt; ++t)
+    {
+        int i0 = bidx(box[6 * t], 0), i1 = bidx(box[6 * t + 3], 0);
+        int j0 = bidx(box[6 * t + 1], 1), j1 = bidx(box[6 * t + 4], 1);
+        int k0 = bidx(box[6 * t + 2], 2), k1 = bidx(box[6 * t + 5], 2);
+        for (int i = i0; i <= i1; ++i)
+            for (int j = j0; j <= j1; ++j)
+                for (int k = k0; k <= k1; ++k) cnt[(static_cast<size_t>(i) * n + j) * n + k + 1]++;
+    }
+    for (size_t b = 1; b < cnt.size(); ++b) cnt[b] += cnt[b - 1];
+    if (cnt.back() > 2147483647LL) return fail(ctx, SKGPU_ERR_ARG, "tetra: search grid too large");
+    std::vector<int> begin(cnt.size()), list(static_cast<size_t>(cnt.back()));
+    std::vector<long long> fill(cnt.begin(), cnt.end() - 1);
+    for (size_t b = 0; b < cnt.size(); ++b) begin[b] = static_cast<int>(cnt[b]);
+    for (size_t t = 0; t < nt; ++t)
+    {
+        int i0 = bidx(box[6 * t], 0), i1 = bidx(box[6 * t + 3], 0);
+        int j0 = bidx(box[6 * t + 1], 1), j1 = bidx(box[6 * t + 4], 1);
+        int k0 = bidx(box[6 * t + 2], 2), k1 = bidx(box[6 * t + 5], 2);
+        for (int i = i0; i <= i1; ++i)
+            for (int j = j0; j <= j1; ++j)
+                for (int k = k0; k <= k1; ++k) list[fill[(static_cast<size_t>(i) * n + j) * n + k]++] = static_cast<int>(t);
+    }
+    CK(cudaSetDevice(ctx->device));
+    freeGrid(ctx);
+    GridDev& g = ctx->g;
+    g.kind = SKGPU_GRID_TETRA;
+    for (int q = 0; q < 6; ++q) g.ext[q] = extent[q];
+    g.eps = eps;
+    g.teN = num_tetra;
+    g.numCells = num_tetra;
+    g.teGridN = n;
+    int rc;
+    if ((rc = gridUpload(ctx, &g.teVerts, vertices, 3 * static_cast<size_t>(num_vertices)))) return rc;
+    if ((rc = gridUpload<int>(ctx, &g.teTet, tetra_vertices, 4 * nt))) return rc;
+    if ((rc = gridUpload(ctx, &g.teNormals, face_normals, 12 * nt))) return rc;
+    if ((rc = gridUpload<int>(ctx, &g.teNTet, face_ntetra, 4 * nt))) return rc;
+    if ((rc = gridUpload<int>(ctx, &g.teNFace, face_nface, 4 * nt))) return rc;
+    if ((rc = gridUpload(ctx, &g.teBox, box.data(), box.size()))) return rc;
+    if ((rc = gridUpload<int>(ctx, &g.teBlkBegin, begin.data(), begin.size()))) return rc;
+    if ((rc = gridUpload<int>(ctx, &g.teBlkTets, list.data(), list.size()))) return rc;
+    ctx->hasGrid = true;
+    return SKGPU_OK;
+}
+
+// ------------------------------------------------------------------------------------------------
+// medium
+// ------------------------------------------------------------------------------------------------
+
+int skgpu_upload_medium(skgpu_ctx* ctx, int32_t num_cells, const double* number_density)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (num_cells < 1 || !number_density) return fail(ctx, SKGPU_ERR_ARG, "medium: missing densities");
+    if (!finiteAll(number_density, num_cells)) return fail(ctx, SKGPU_ERR_ARG, "medium: non-finite density");
+    CK(cudaSetDevice(ctx->device));
+    if (ctx->numCells != num_cells)
+    {
+        devFree(ctx->dens);
+        CK(devAlloc(&ctx->dens, num_cells));
+        ctx->numCells = num_cells;
+    }
+    CK(cudaMemcpy(ctx->dens, number_density, num_cells * sizeof(double), cudaMemcpyHostToDevice));
+    return SKGPU_OK;
+}
+
+int skgpu_upload_dust_mix(skgpu_ctx* ctx, int32_t num_lambda, const double* lambda_borders, const double* sigma_ext,
+                          const double* sigma_sca, const double* asymmpar)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (num_lambda < 1 || !lambda_borders || !sigma_ext || !sigma_sca || !asymmpar)
+        return fail(ctx, SKGPU_ERR_ARG, "dust mix: missing tables");
+    CK(cudaSetDevice(ctx->device));
+    devFree(ctx->mixLb);
+    devFree(ctx->mixExt);
+    devFree(ctx->mixSca);
+    devFree(ctx->mixG);
+    CK(devUpload(&ctx->mixLb, lambda_borders, num_lambda));
+    CK(devUpload(&ctx->mixExt, sigma_ext, num_lambda));
+    CK(devUpload(&ctx->mixSca, sigma_sca, num_lambda));
+    CK(devUpload(&ctx->mixG, asymmpar, num_lambda));
+    ctx->nmix = num_lambda;
+    return SKGPU_OK;
+}
+
+int skgpu_upload_rf_grid(skgpu_ctx* ctx, int32_t num_bins, int32_t num_borders, const double* borders, const int32_t* ellv)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (num_bins < 1 || num_borders < 1 || !borders || !ellv) return fail(ctx, SKGPU_ERR_ARG, "rf grid: missing arrays");
+    for (int q = 0; q <= num_borders; ++q)
+        if (ellv[q] < -1 || ellv[q] >= num_bins) return fail(ctx, SKGPU_ERR_ARG, "rf grid: bin map out of range");
+    CK(cudaSetDevice(ctx->device));
+    devFree(ctx->rfB);
+    devFree(ctx->rfEll);
+    CK(devUpload(&ctx->rfB, borders, num_borders));
+    CK(devUpload<int>(&ctx->rfEll, ellv, num_borders + 1));
+    ctx->nrf = num_bins;
+    ctx->rfNb = num_borders;
+    return SKGPU_OK;
+}
+
+// ------------------------------------------------------------------------------------------------
+// sources and instruments
+// ------------------------------------------------------------------------------------------------
+
+int skgpu_upload_sources(skgpu_ctx* ctx, int32_t num_sources, const skgpu_source* sources, int32_t table_len,
+                         const double* table_lambda, const double* table_a, const double* table_b, int32_t radial_len,
+                         const double* radial_r, const double* radial_P)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (num_sources < 1 || !sources) return fail(ctx, SKGPU_ERR_ARG, "sources: none given");
+    std::vector<SourceDev> v(num_sources);
+    for (int h = 0; h < num_sources; ++h)
+    {
+        const skgpu_source& s = sources[h];
+        SourceDev& d = v[h];
+        if (s.position_model < 0 || s.position_model > 2) return fail(ctx, SKGPU_ERR_ARG, "sources: bad position model");
+        if (s.spectral_model < 0 || s.spectral_model > 1) return fail(ctx, SKGPU_ERR_ARG, "sources: bad spectral model");
+        if (s.table_size < 1 || s.table_offset < 0 || s.table_offset + s.table_size > table_len)
+            return fail(ctx, SKGPU_ERR_ARG, "sources: spectral table out of range");
+        if (s.spectral_model == 1 && s.table_size < 2) return fail(ctx, SKGPU_ERR_ARG, "sources: SED table needs 2 points");
+        if (s.position_model == 2 && (s.radial_size < 2 || s.radial_offset < 0 || s.radial_offset + s.radial_size > radial_len))
+            return fail(ctx, SKGPU_ERR_ARG, "sources: radial table out of range");
+        if (h > 0 && s.first_history < sources[h - 1].first_history)
+            return fail(ctx, SKGPU_ERR_ARG, "sources: first_history must be ascending");
+        d.posModel = s.position_model;
+        d.specModel = s.spectral_model;
+        for (int a = 0; a < 3; ++a) d.pos[a] = s.position[a];
+        for (int a = 0; a < 6; ++a) d.geom[a] = s.geometry[a];
+        d.first = s.first_history;
+        d.num = s.num_histories;
+        d.Lpk = s.packet_luminosity;
+        d.xi = s.wavelength_bias;
+        d.bmin = s.bias_lambda_min;
+        d.bmax = s.bias_lambda_max;
+        d.toff = s.table_offset;
+        d.tsize = s.table_size;
+        d.roff = s.radial_offset;
+        d.rsize = s.radial_size;
+    }
+    CK(cudaSetDevice(ctx->device));
+    devFree(ctx->src);
+    devFree(ctx->tabL);
+    devFree(ctx->tabA);
+    devFree(ctx->tabB);
+    devFree(ctx->radR);
+    devFree(ctx->radP);
+    CK(devUpload(&ctx->src, v.data(), v.size()));
+    CK(devUpload(&ctx->tabL, table_lambda, table_len));
+    CK(devUpload(&ctx->tabA, table_a, table_len));
+    CK(devUpload(&ctx->tabB, table_b, table_b ? table_len : 0));
+    CK(devUpload(&ctx->radR, radial_r, radial_r ? radial_len : 0));
+    CK(devUpload(&ctx->radP, radial_P, radial_P ? radial_len : 0));
+    ctx->srcHost = v;
+    return SKGPU_OK;
+}
+
+int skgpu_upload_instruments(skgpu_ctx* ctx, int32_t num_instruments, const skgpu_instrument* instruments,
+                             int32_t wlg_len, const double* wlg_borders, const int32_t* wlg_ellv)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (num_instruments < 0 || num_instruments > MAX_INSTR) return fail(ctx, SKGPU_ERR_ARG, "instruments: count out of range");
+    if (num_instruments > 0 && instruments[0].same_observer) return fail(ctx, SKGPU_ERR_ARG, "instruments: first cannot share an observer");
+    CK(cudaSetDevice(ctx->device));
+    freeInstruments(ctx);
+    std::vector<InstrDev> v(num_instruments);
+    for (int i = 0; i < num_instruments; ++i)
+    {
+        const skgpu_instrument& s = instruments[i];
+        InstrDev& d = v[i];
+        if (s.kind != SKGPU_INSTR_FRAME && s.kind != SKGPU_INSTR_SED) return fail(ctx, SKGPU_ERR_ARG, "instruments: bad kind");
+        if (s.num_wavelength_bins < 1 || s.wlg_num_borders < 1 || s.wlg_offset < 0
+            || s.wlg_offset + s.wlg_num_borders + 1 > wlg_len)
+            return fail(ctx, SKGPU_ERR_ARG, "instruments: wavelength grid out of range");
+        if (s.kind == SKGPU_INSTR_FRAME && (s.num_pixels_x < 1 || s.num_pixels_y < 1 || !(s.xp_size > 0) || !(s.yp_size > 0)))
+            return fail(ctx, SKGPU_ERR_ARG, "instruments: bad frame geometry");
+        for (int q = 0; q <= s.wlg_num_borders; ++q)
+            if (wlg_ellv[s.wlg_offset + q] < -1 || wlg_ellv[s.wlg_offset + q] >= s.num_wavelength_bins)
+                return fail(ctx, SKGPU_ERR_ARG, "instruments: bin map out of range");
+        d.kind = s.kind;
+        d.same = s.same_observer;
+        d.stats = s.record_statistics;
+        d.comps = s.record_components;
+        d.npx = s.kind == SKGPU_INSTR_FRAME ? s.num_pixels_x : 1;
+        d.npy = s.kind == SKGPU_INSTR_FRAME ? s.num_pixels_y : 1;
+        d.nbins = s.num_wavelength_bins;
+        d.woff = s.wlg_offset;
+        d.wnb = s.wlg_num_borders;
+        for (int a = 0; a < 3; ++a) d.kobs[a] = s.kobs[a];
+        d.ct = s.cos_theta; d.st = s.sin_theta; d.cp = s.cos_phi; d.sp = s.sin_phi; d.co = s.cos_omega; d.so = s.sin_omega;
+        d.xpmin = s.xp_min; d.xpsiz = s.xp_size; d.ypmin = s.yp_min; d.ypsiz = s.yp_size;
+        d.ifu = d.sed = d.ifuComp = d.sedComp = d.ifuStats = d.sedStats = nullptr;
+        size_t n = static_cast<size_t>(d.nbins) * (d.kind == SKGPU_INSTR_FRAME ? static_cast<size_t>(d.npx) * d.npy : 1);
+        auto alloc = [&](double** p, size_t cnt) -> int {
+            CK(devAlloc(p, cnt));
+            CK(cudaMemset(*p, 0, cnt * sizeof(double)));
+            ctx->instrBufs.push_back(*p);
+            return SKGPU_OK;
+        };
+        int rc;
+        double** total = d.kind == SKGPU_INSTR_FRAME ? &d.ifu : &d.sed;
+        double** comp = d.kind == SKGPU_INSTR_FRAME ? &d.ifuComp : &d.sedComp;
+        double** stats = d.kind == SKGPU_INSTR_FRAME ? &d.ifuStats : &d.sedStats;
+        if ((rc = alloc(total, n))) return rc;
+        if (d.comps && (rc = alloc(comp, 3 * n))) return rc;
+        if (d.stats && (rc = alloc(stats, 5 * n))) return rc;
+    }
+    CK(devUpload(&ctx->instr, v.data(), v.size()));
+    CK(devUpload(&ctx->wlgB, wlg_borders, wlg_len));
+    CK(devUpload<int>(&ctx->wlgEll, wlg_ellv, wlg_len));
+    ctx->instrHost = v;
+    return SKGPU_OK;
+}
+
+int skgpu_set_options(skgpu_ctx* ctx, const skgpu_options* options)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (!options) return fail(ctx, SKGPU_ERR_ARG, "options: null");
+    if (!(options->min_weight_reduction > 0)) return fail(ctx, SKGPU_ERR_ARG, "options: min_weight_reduction must be > 0");
+    if (options->path_length_bias < 0 || options->path_length_bias >= 1) return fail(ctx, SKGPU_ERR_ARG, "options: path_length_bias must be in [0,1)");
+    if (options->precision != SKGPU_PREC_FP64_EXACT && options->precision != SKGPU_PREC_FP32)
+        return fail(ctx, SKGPU_ERR_ARG, "options: bad precision");
+    ctx->opt = *options;
+    ctx->hasOptions = true;
+    return SKGPU_OK;
+}
+
+// ------------------------------------------------------------------------------------------------
+// run and tallies
+// ------------------------------------------------------------------------------------------------
+
+int skgpu_run_primary(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t total_packets)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (!ctx->hasGrid) return fail(ctx, SKGPU_ERR_STATE, "run: no grid uploaded");
+    if (!ctx->dens || ctx->numCells != ctx->g.numCells) return fail(ctx, SKGPU_ERR_STATE, "run: medium does not match the grid");
+    if (!ctx->nmix) return fail(ctx, SKGPU_ERR_STATE, "run: no dust mix uploaded");
+    if (ctx->srcHost.empty()) return fail(ctx, SKGPU_ERR_STATE, "run: no sources uploaded");
+    if (ctx->opt.store_radiation_field && !ctx->nrf) return fail(ctx, SKGPU_ERR_STATE, "run: radiation field requested without RF grid");
+    if (total_packets == 0 || first + count > total_packets) return fail(ctx, SKGPU_ERR_ARG, "run: history range outside the segment");
+    CK(cudaSetDevice(ctx->device));
+    if (ctx->opt.store_radiation_field)
+    {
+        size_t len = static_cast<size_t>(ctx->numCells) * ctx->nrf;
+        if (ctx->rfLen != len)
+        {
+            devFree(ctx->rf);
+            CK(devAlloc(&ctx->rf, len));
+            CK(cudaMemset(ctx->rf, 0, len * sizeof(double)));
+            ctx->rfLen = len;
+        }
+    }
+    LCParams p{};
+    p.g = ctx->g;
+    p.dens = ctx->dens;
+    p.mixLb = ctx->mixLb; p.mixExt = ctx->mixExt; p.mixSca = ctx->mixSca; p.mixG = ctx->mixG; p.nmix = ctx->nmix;
+    p.nsrc = static_cast<int>(ctx->srcHost.size());
+    p.src = ctx->src;
+    p.tabL = ctx->tabL; p.tabA = ctx->tabA; p.tabB = ctx->tabB; p.radR = ctx->radR; p.radP = ctx->radP;
+    p.ninstr = static_cast<int>(ctx->instrHost.size());
+    p.instr = ctx->instr;
+    p.wlgB = ctx->wlgB; p.wlgEll = ctx->wlgEll;
+    p.rfOn = ctx->opt.store_radiation_field ? 1 : 0;
+    p.nrf = ctx->nrf; p.rfNb = ctx->rfNb; p.rfB = ctx->rfB; p.rfEll = ctx->rfEll; p.rf = ctx->rf;
+    p.forced = ctx->opt.force_scattering ? 1 : 0;
+    p.minScatt = ctx->opt.min_scatt_events;
+    p.peel = ctx->opt.peel_off ? 1 : 0;
+    p.minWeightRed = ctx->opt.min_weight_reduction;
+    p.pathLengthBias = ctx->opt.path_length_bias;
+    p.seed = ctx->opt.seed;
+    p.first = first;
+    p.count = count;
+    p.npp = total_packets;
+    p.workCounter = ctx->work;
+    p.counters = ctx->counters;
+    p.errFlag = ctx->errFlag;
+    CK(cudaMemsetAsync(ctx->work, 0, sizeof(unsigned long long), ctx->stream));
+    CK(cudaMemsetAsync(ctx->counters, 0, 8 * sizeof(unsigned long long), ctx->stream));
+    CK(cudaMemsetAsync(ctx->errFlag, 0, sizeof(int), ctx->stream));
+    const int threads = 256;
+    int prec = ctx->opt.precision;
+    int perSM = prec == SKGPU_PREC_FP64_EXACT ? lifecycleBlocksPerSMFP64(ctx->g.kind, threads)
+                                              : lifecycleBlocksPerSMFP32(ctx->g.kind, threads);
+    long long want = (static_cast<long long>(count) + threads - 1) / threads;
+    int blocks = static_cast<int>(std::max(1LL, std::min(want, static_cast<long long>(perSM) * ctx->numSMs)));
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    if (count > 0)
+    {
+        cudaError_t e = prec == SKGPU_PREC_FP64_EXACT ? launchLifecycleFP64(ctx->g.kind, p, blocks, threads, ctx->stream)
+                                                      : launchLifecycleFP32(ctx->g.kind, p, blocks, threads, ctx->stream);
+        if (e != cudaSuccess) return fail(ctx, SKGPU_ERR_CUDA, std::string("life-cycle launch: ") + cudaGetErrorString(e));
+    }
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    ctx->lastMs = ms;
+    unsigned long long cnt[8];
+    int errFlag = 0;
+    CK(cudaMemcpy(cnt, ctx->counters, sizeof cnt, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&errFlag, ctx->errFlag, sizeof errFlag, cudaMemcpyDeviceToHost));
+    ctx->lastCounters.histories = cnt[0];
+    ctx->lastCounters.crossings = cnt[1];
+    ctx->lastCounters.scatterings = cnt[2];
+    ctx->lastCounters.peel_detections = cnt[3];
+    ctx->lastCounters.rf_stores = cnt[4];
+    ctx->lastCounters.stats_overflows = cnt[5];
+    ctx->lastCounters.kernel_launches = count > 0 ? 1 : 0;
+    if (errFlag & 4) return fail(ctx, SKGPU_ERR_TIMEOUT, "run: a traversal exceeded its segment guard");
+    if (errFlag) return fail(ctx, SKGPU_ERR_DEVICE, "run: interaction point outside the grid (device check)");
+    return SKGPU_OK;
+}
+
+static int addInto(skgpu_ctx* ctx, const double* dev, size_t n, double* host)
+{
+    if (!host || !dev || n == 0) return SKGPU_OK;
+    std::vector<double> tmp(n);
+    CK(cudaMemcpy(tmp.data(), dev, n * sizeof(double), cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < n; ++i) host[i] += tmp[i];
+    return SKGPU_OK;
+}
+
+int skgpu_fetch_instrument(skgpu_ctx* ctx, int32_t instrument, double* ifu, double* sed, double* ifu_stats,
+                           double* sed_stats)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (instrument < 0 || instrument >= static_cast<int>(ctx->instrHost.size())) return fail(ctx, SKGPU_ERR_ARG, "fetch: bad instrument index");
+    CK(cudaSetDevice(ctx->device));
+    const InstrDev& d = ctx->instrHost[instrument];
+    size_t n = static_cast<size_t>(d.nbins) * d.npx * d.npy;
+    int rc;
+    if (d.kind == SKGPU_INSTR_FRAME)
+    {
+        if ((rc = addInto(ctx, d.ifu, n, ifu))) return rc;
+        if (d.stats && (rc = addInto(ctx, d.ifuStats, 5 * n, ifu_stats))) return rc;
+    }
+    else
+    {
+        if ((rc = addInto(ctx, d.sed, n, sed))) return rc;
+        if (d.stats && (rc = addInto(ctx, d.sedStats, 5 * n, sed_stats))) return rc;
+    }
+    return SKGPU_OK;
+}
+
+int skgpu_fetch_instrument_components(skgpu_ctx* ctx, int32_t instrument, double* ifu3, double* sed3)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (instrument < 0 || instrument >= static_cast<int>(ctx->instrHost.size())) return fail(ctx, SKGPU_ERR_ARG, "fetch: bad instrument index");
+    const InstrDev& d = ctx->instrHost[instrument];
+    if (!d.comps) return fail(ctx, SKGPU_ERR_STATE, "fetch: instrument does not record components");
+    CK(cudaSetDevice(ctx->device));
+    size_t n = static_cast<size_t>(d.nbins) * d.npx * d.npy;
+    return d.kind == SKGPU_INSTR_FRAME ? addInto(ctx, d.ifuComp, 3 * n, ifu3) : addInto(ctx, d.sedComp, 3 * n, sed3);
+}
+
+int skgpu_fetch_radiation_field(skgpu_ctx* ctx, double* rf)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (!ctx->rf) return fail(ctx, SKGPU_ERR_STATE, "fetch: no radiation field recorded");
+    CK(cudaSetDevice(ctx->device));
+    return addInto(ctx, ctx->rf, ctx->rfLen, rf);
+}
+
+int skgpu_clear_tallies(skgpu_ctx* ctx)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    for (const InstrDev& d : ctx->instrHost)
+    {
+        size_t n = static_cast<size_t>(d.nbins) * d.npx * d.npy;
+        double* t = d.kind == SKGPU_INSTR_FRAME ? d.ifu : d.sed;
+        double* c = d.kind == SKGPU_INSTR_FRAME ? d.ifuComp : d.sedComp;
+        double* s = d.kind == SKGPU_INSTR_FRAME ? d.ifuStats : d.sedStats;
+        CK(cudaMemsetAsync(t, 0, n * sizeof(double), ctx->stream));
+        if (c) CK(cudaMemsetAsync(c, 0, 3 * n * sizeof(double), ctx->stream));
+        if (s) CK(cudaMemsetAsync(s, 0, 5 * n * sizeof(double), ctx->stream));
+    }
+    if (ctx->rf) CK(cudaMemsetAsync(ctx->rf, 0, ctx->rfLen * sizeof(double), ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return SKGPU_OK;
+}
+
+int skgpu_get_counters(skgpu_ctx* ctx, skgpu_counters* out)
+{
+    if (!ctx || !out) return SKGPU_ERR_ARG;
+    *out = ctx->lastCounters;
+    return SKGPU_OK;
+}
+
+int skgpu_last_run_ms(skgpu_ctx* ctx, double* ms)
+{
+    if (!ctx || !ms) return SKGPU_ERR_ARG;
+    *ms = ctx->lastMs;
+    return SKGPU_OK;
+}
+
+// ------------------------------------------------------------------------------------------------
+// path segments
+// ------------------------------------------------------------------------------------------------
+
+int skgpu_trace_paths(skgpu_ctx* ctx, int32_t num_rays, const double* rays, int32_t max_segments, int32_t precision,
+                      int32_t* count, int32_t* m, double* ds)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (!ctx->hasGrid) return fail(ctx, SKGPU_ERR_STATE, "trace: no grid uploaded");
+    if (num_rays < 0 || max_segments < 1 || (num_rays > 0 && (!rays || !count || !m || !ds)))
+        return fail(ctx, SKGPU_ERR_ARG, "trace: bad arguments");
+    if (precision != SKGPU_PREC_FP64_EXACT) return fail(ctx, SKGPU_ERR_UNSUPPORTED, "trace: only FP64 exact path dumps");
+    if (num_rays == 0) return SKGPU_OK;
+    CK(cudaSetDevice(ctx->device));
+    size_t n = num_rays, ns = n * static_cast<size_t>(max_segments);
+    double *dRays = nullptr, *dDs = nullptr;
+    int *dCount = nullptr, *dM = nullptr;
+    auto cleanup = [&]() { devFree(dRays); devFree(dDs); devFree(dCount); devFree(dM); };
+    cudaError_t e = devUpload(&dRays, rays, 6 * n);
+    if (e == cudaSuccess) e = devAlloc(&dDs, ns);
+    if (e == cudaSuccess) e = devAlloc(&dCount, n);
+    if (e == cudaSuccess) e = devAlloc(&dM, ns);
+    if (e == cudaSuccess) e = cudaMemsetAsync(ctx->errFlag, 0, sizeof(int), ctx->stream);
+    if (e == cudaSuccess) e = launchTracePaths(precision, ctx->g, num_rays, dRays, max_segments, dCount, dM, dDs, ctx->errFlag, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    int errFlag = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&errFlag, ctx->errFlag, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(count, dCount, n * sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(m, dM, ns * sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(ds, dDs, ns * sizeof(double), cudaMemcpyDeviceToHost);
+    cleanup();
+    if (e != cudaSuccess) return fail(ctx, SKGPU_ERR_CUDA, std::string("trace: ") + cudaGetErrorString(e));
+    if (errFlag) return fail(ctx, SKGPU_ERR_TIMEOUT, "trace: a path exceeded its segment guard");
+    return SKGPU_OK;
+}
+
+int skgpu_optical_depths(skgpu_ctx* ctx, int32_t num_rays, const double* rays, double lambda, int32_t precision,
+                         double* tau)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (!ctx->hasGrid || !ctx->dens || !ctx->nmix) return fail(ctx, SKGPU_ERR_STATE, "optical depths: grid, medium and mix required");
+    if (ctx->numCells != ctx->g.numCells) return fail(ctx, SKGPU_ERR_STATE, "optical depths: medium does not match the grid");
+    if (num_rays < 0 || (num_rays > 0 && (!rays || !tau))) return fail(ctx, SKGPU_ERR_ARG, "optical depths: bad arguments");
+    if (precision != SKGPU_PREC_FP64_EXACT) return fail(ctx, SKGPU_ERR_UNSUPPORTED, "optical depths: only FP64 exact");
+    if (num_rays == 0) return SKGPU_OK;
+    // DustMix::sectionExt(lambda) = sigma_ext[locateClip(lambda borders, lambda)]
+    std::vector<double> lb(ctx->nmix), se(ctx->nmix);
+    CK(cudaMemcpy(lb.data(), ctx->mixLb, ctx->nmix * sizeof(double), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(se.data(), ctx->mixExt, ctx->nmix * sizeof(double), cudaMemcpyDeviceToHost));
+    double section = se[skg::locateClip(lb.data(), ctx->nmix, lambda)];
+    size_t n = num_rays;
+    double *dRays = nullptr, *dTau = nullptr;
+    cudaError_t e = devUpload(&dRays, rays, 6 * n);
+    if (e == cudaSuccess) e = devAlloc(&dTau, n);
+    if (e == cudaSuccess) e = cudaMemsetAsync(ctx->errFlag, 0, sizeof(int), ctx->stream);
+    if (e == cudaSuccess) e = launchOpticalDepths(precision, ctx->g, ctx->dens, section, num_rays, dRays, dTau, ctx->errFlag, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpy(tau, dTau, n * sizeof(double), cudaMemcpyDeviceToHost);
+    devFree(dRays);
+    devFree(dTau);
+    if (e != cudaSuccess) return fail(ctx, SKGPU_ERR_CUDA, std::string("optical depths: ") + cudaGetErrorString(e));
+    return SKGPU_OK;
+}
+
+}  // extern "C"

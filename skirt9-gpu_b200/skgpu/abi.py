@@ -1,0 +1,293 @@
+"""ctypes binding of the C ABI in include/skgpu.h.
+
+`Backend` wraps one shared library whose entry points follow the skgpu.h signatures, given the
+function-name prefix. The product uses the CUDA library (`lib/libskgpu.so`, prefix ``skgpu_``);
+the test suite also drives the CPU oracle through the same class (prefix ``or_``), so that the
+GPU tracer and the oracle receive byte-identical inputs.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG_ROOT = os.path.dirname(HERE)
+LIB_PATH = os.path.join(PKG_ROOT, "lib", "libskgpu.so")
+
+# status codes
+OK, ERR_ARG, ERR_CUDA, ERR_STATE, ERR_TIMEOUT, ERR_DEVICE, ERR_UNSUPPORTED = range(7)
+GRID_CARTESIAN, GRID_OCTREE, GRID_VORONOI, GRID_TETRA = range(4)
+PREC_FP64_EXACT, PREC_FP32 = 0, 1
+SRC_POINT, SRC_EXPDISK, SRC_RADIAL = 0, 1, 2
+SPEC_DISCRETE, SPEC_TABLE = 0, 1
+INSTR_FRAME, INSTR_SED = 0, 1
+
+
+class SkgpuError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__(f"skgpu error {code}: {message}")
+        self.code = code
+
+
+class Source(C.Structure):
+    _fields_ = [
+        ("position_model", C.c_int32),
+        ("spectral_model", C.c_int32),
+        ("position", C.c_double * 3),
+        ("geometry", C.c_double * 6),
+        ("first_history", C.c_uint64),
+        ("num_histories", C.c_uint64),
+        ("packet_luminosity", C.c_double),
+        ("wavelength_bias", C.c_double),
+        ("bias_lambda_min", C.c_double),
+        ("bias_lambda_max", C.c_double),
+        ("table_offset", C.c_int32),
+        ("table_size", C.c_int32),
+        ("radial_offset", C.c_int32),
+        ("radial_size", C.c_int32),
+    ]
+
+
+class Instrument(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32),
+        ("same_observer", C.c_int32),
+        ("record_statistics", C.c_int32),
+        ("record_components", C.c_int32),
+        ("num_pixels_x", C.c_int32),
+        ("num_pixels_y", C.c_int32),
+        ("num_wavelength_bins", C.c_int32),
+        ("wlg_offset", C.c_int32),
+        ("wlg_num_borders", C.c_int32),
+        ("kobs", C.c_double * 3),
+        ("cos_theta", C.c_double),
+        ("sin_theta", C.c_double),
+        ("cos_phi", C.c_double),
+        ("sin_phi", C.c_double),
+        ("cos_omega", C.c_double),
+        ("sin_omega", C.c_double),
+        ("xp_min", C.c_double),
+        ("xp_size", C.c_double),
+        ("yp_min", C.c_double),
+        ("yp_size", C.c_double),
+    ]
+
+
+class Options(C.Structure):
+    _fields_ = [
+        ("force_scattering", C.c_int32),
+        ("min_scatt_events", C.c_int32),
+        ("min_weight_reduction", C.c_double),
+        ("path_length_bias", C.c_double),
+        ("store_radiation_field", C.c_int32),
+        ("peel_off", C.c_int32),
+        ("precision", C.c_int32),
+        ("reserved", C.c_int32),
+        ("seed", C.c_uint64),
+    ]
+
+
+class Counters(C.Structure):
+    _fields_ = [
+        ("histories", C.c_uint64),
+        ("crossings", C.c_uint64),
+        ("scatterings", C.c_uint64),
+        ("peel_detections", C.c_uint64),
+        ("rf_stores", C.c_uint64),
+        ("stats_overflows", C.c_uint64),
+        ("kernel_launches", C.c_uint64),
+        ("reserved", C.c_uint64),
+    ]
+
+
+_P = C.c_void_p
+_I = C.c_int32
+_D = C.c_double
+_U = C.c_uint64
+
+# name -> argtypes (restype int unless noted); the exported C-ABI of include/skgpu.h
+SIGNATURES = {
+    "create": [C.c_int, C.POINTER(_P)],
+    "destroy": [_P],
+    "last_error": [_P],
+    "upload_grid_cartesian": [_P, _P, _I, _P, _I, _P, _I],
+    "upload_grid_octree": [_P, _I, _P, _P, _P, _P, _P, _I, _P, _P, _I, _D],
+    "upload_grid_voronoi": [_P, _I, _P, _P, _P, _I, _P, _D],
+    "upload_grid_tetra": [_P, _I, _P, _I, _P, _P, _P, _P, _P, _D],
+    "upload_medium": [_P, _I, _P],
+    "upload_dust_mix": [_P, _I, _P, _P, _P, _P],
+    "upload_rf_grid": [_P, _I, _I, _P, _P],
+    "upload_sources": [_P, _I, _P, _I, _P, _P, _P, _I, _P, _P],
+    "upload_instruments": [_P, _I, _P, _I, _P, _P],
+    "set_options": [_P, _P],
+    "run_primary": [_P, _U, _U, _U],
+    "fetch_instrument": [_P, _I, _P, _P, _P, _P],
+    "fetch_instrument_components": [_P, _I, _P, _P],
+    "fetch_radiation_field": [_P, _P],
+    "clear_tallies": [_P],
+    "get_counters": [_P, _P],
+    "last_run_ms": [_P, _P],
+    "trace_paths": [_P, _I, _P, _I, _I, _P, _P, _P],
+    "optical_depths": [_P, _I, _P, _D, _I, _P],
+}
+
+# symbols of include/skgpu.h (the CUDA library must export every one)
+EXPORTED = ["skgpu_abi_version"] + ["skgpu_" + n for n in SIGNATURES]
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+_LIBS = {}
+
+
+def load_library(path=LIB_PATH):
+    """Load the CUDA tracer library. Raises if it is missing: there is no fallback path."""
+    if path not in _LIBS:
+        if not os.path.exists(path):
+            raise SkgpuError(ERR_STATE, f"CUDA tracer library not built: {path} (run __graft_entry__.build())")
+        _LIBS[path] = C.CDLL(path)
+    return _LIBS[path]
+
+
+class Backend:
+    """One context of a library with skgpu.h-shaped entry points."""
+
+    def __init__(self, lib=None, prefix="skgpu_", device=0):
+        self.lib = lib if lib is not None else load_library()
+        self.prefix = prefix
+        self.fn = {}
+        for name, args in SIGNATURES.items():
+            f = getattr(self.lib, prefix + name)
+            f.argtypes = args
+            f.restype = None if name == "destroy" else (C.c_char_p if name == "last_error" else C.c_int)
+            self.fn[name] = f
+        self.ctx = C.c_void_p()
+        rc = self.fn["create"](device, C.byref(self.ctx))
+        if rc != OK:
+            msg = self.fn["last_error"](self.ctx).decode() if self.ctx else "create failed"
+            self.close()
+            raise SkgpuError(rc, msg)
+
+    def close(self):
+        if self.ctx:
+            self.fn["destroy"](self.ctx)
+            self.ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def call(self, name, *args):
+        rc = self.fn[name](self.ctx, *args)
+        if rc != OK:
+            raise SkgpuError(rc, self.fn["last_error"](self.ctx).decode())
+        return rc
+
+    # ---- typed helpers ----
+    def upload_grid_cartesian(self, xb, yb, zb):
+        xb, yb, zb = f64(xb), f64(yb), f64(zb)
+        self.call("upload_grid_cartesian", _ptr(xb), len(xb), _ptr(yb), len(yb), _ptr(zb), len(zb))
+
+    def upload_grid_octree(self, bounds, cell_index, child_begin, child_count, child_index, nb_begin, nb_index, eps):
+        b, ci, cb, cc, cx, nbb, nbi = (f64(bounds), i32(cell_index), i32(child_begin), i32(child_count),
+                                       i32(child_index), i32(nb_begin), i32(nb_index))
+        self.call("upload_grid_octree", len(ci), _ptr(b), _ptr(ci), _ptr(cb), _ptr(cc), _ptr(cx), len(cx),
+                  _ptr(nbb), _ptr(nbi), len(nbi), float(eps))
+
+    def upload_grid_voronoi(self, sites, nb_begin, nb_index, extent, eps):
+        s, nbb, nbi, ext = f64(sites), i32(nb_begin), i32(nb_index), f64(extent)
+        self.call("upload_grid_voronoi", len(nbb) - 1, _ptr(s), _ptr(nbb), _ptr(nbi), len(nbi), _ptr(ext), float(eps))
+
+    def upload_grid_tetra(self, vertices, tetra, normals, ntetra, nface, extent, eps):
+        v, t, n, nt, nf, ext = f64(vertices), i32(tetra), f64(normals), i32(ntetra), i32(nface), f64(extent)
+        self.call("upload_grid_tetra", len(v) // 3 if v.ndim == 1 else v.shape[0], _ptr(v), t.size // 4, _ptr(t),
+                  _ptr(n), _ptr(nt), _ptr(nf), _ptr(ext), float(eps))
+
+    def upload_medium(self, density):
+        d = f64(density).ravel()
+        self.call("upload_medium", len(d), _ptr(d))
+
+    def upload_dust_mix(self, lambda_borders, sigma_ext, sigma_sca, asymmpar):
+        a, b, c, d = f64(lambda_borders), f64(sigma_ext), f64(sigma_sca), f64(asymmpar)
+        self.call("upload_dust_mix", len(a), _ptr(a), _ptr(b), _ptr(c), _ptr(d))
+
+    def upload_rf_grid(self, num_bins, borders, ellv):
+        b, e = f64(borders), i32(ellv)
+        self.call("upload_rf_grid", int(num_bins), len(b), _ptr(b), _ptr(e))
+
+    def upload_sources(self, sources, table_lambda, table_a, table_b=None, radial_r=None, radial_P=None):
+        arr = (Source * len(sources))(*sources)
+        tl, ta = f64(table_lambda), f64(table_a)
+        tb = f64(table_b) if table_b is not None else np.zeros_like(tl)
+        rr = f64(radial_r) if radial_r is not None else np.zeros(1)
+        rp = f64(radial_P) if radial_P is not None else np.zeros(1)
+        self._keep = (arr, tl, ta, tb, rr, rp)
+        self.call("upload_sources", len(sources), C.cast(arr, C.c_void_p), len(tl), _ptr(tl), _ptr(ta), _ptr(tb),
+                  len(rr), _ptr(rr), _ptr(rp))
+
+    def upload_instruments(self, instruments, wlg_borders, wlg_ellv):
+        arr = (Instrument * max(1, len(instruments)))(*instruments)
+        b, e = f64(wlg_borders), i32(wlg_ellv)
+        self.call("upload_instruments", len(instruments), C.cast(arr, C.c_void_p), len(e), _ptr(b), _ptr(e))
+
+    def set_options(self, opt):
+        self.call("set_options", C.cast(C.pointer(opt), C.c_void_p))
+
+    def run_primary(self, first, count, total):
+        self.call("run_primary", int(first), int(count), int(total))
+
+    def fetch_instrument(self, i, n, stats=False):
+        total = np.zeros(n)
+        st = np.zeros(5 * n) if stats else None
+        self.call("fetch_instrument", i, _ptr(total), _ptr(total), _ptr(st), _ptr(st))
+        return total, (st.reshape(5, n) if stats else None)
+
+    def fetch_instrument_components(self, i, n):
+        comp = np.zeros(3 * n)
+        self.call("fetch_instrument_components", i, _ptr(comp), _ptr(comp))
+        return comp.reshape(3, n)
+
+    def fetch_radiation_field(self, n):
+        rf = np.zeros(n)
+        self.call("fetch_radiation_field", _ptr(rf))
+        return rf
+
+    def clear_tallies(self):
+        self.call("clear_tallies")
+
+    def counters(self):
+        c = Counters()
+        self.call("get_counters", C.cast(C.pointer(c), C.c_void_p))
+        return {k: getattr(c, k) for k, _ in Counters._fields_}
+
+    def last_run_ms(self):
+        v = C.c_double()
+        self.call("last_run_ms", C.cast(C.pointer(v), C.c_void_p))
+        return v.value
+
+    def trace_paths(self, rays, max_segments, precision=PREC_FP64_EXACT):
+        r = f64(rays).reshape(-1, 6)
+        n = len(r)
+        count = np.zeros(n, np.int32)
+        m = np.full((n, max_segments), -2, np.int32)
+        ds = np.zeros((n, max_segments))
+        self.call("trace_paths", n, _ptr(r), int(max_segments), int(precision), _ptr(count), _ptr(m), _ptr(ds))
+        return count, m, ds
+
+    def optical_depths(self, rays, lam, precision=PREC_FP64_EXACT):
+        r = f64(rays).reshape(-1, 6)
+        tau = np.zeros(len(r))
+        self.call("optical_depths", len(r), _ptr(r), float(lam), int(precision), _ptr(tau))
+        return tau

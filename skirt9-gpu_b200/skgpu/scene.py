@@ -1,0 +1,246 @@
+"""Host-side scene description: the flattened state SKIRT hands to the tracer.
+
+A `Scene` holds exactly the arrays of the C ABI (grid, medium state, dust-mix tables, sources,
+instruments, options). It is filled either from the export of a reference simulation (the
+`skirt_export` harness writes the SimulationItem tree's flattened arrays as .npy files) or by the
+workload builders in `skgpu.workloads`. `Scene.upload` sends it through a `Backend`;
+`Scene.run` performs one primary-emission segment and returns the tallies.
+"""
+import os
+
+import numpy as np
+
+from . import abi
+
+
+class Results:
+    """Tallies of one segment, per instrument in instrument order, plus the radiation field."""
+
+    def __init__(self):
+        self.instruments = []
+        self.rf = None
+        self.counters = None
+        self.ms = None
+
+    def __getitem__(self, i):
+        return self.instruments[i]
+
+
+class Scene:
+    def __init__(self):
+        self.grid = None          # dict: kind + arrays in the ABI layout
+        self.density = None       # (num_cells,)
+        self.mix = None           # dict: lambda_borders, sigma_ext, sigma_sca, asymmpar
+        self.rf = None            # dict: num_bins, borders, ellv
+        self.total_luminosity = None
+        self.sources = []         # list of dicts (see add_* helpers)
+        self.instruments = []     # list of dicts
+        self.force_scattering = True
+        self.min_weight_reduction = 1e4
+        self.min_scatt_events = 0
+        self.path_length_bias = 0.5
+        self.store_rf = False
+        self.source_bias = 0.5
+
+    # ------------------------------------------------------------------ uploads
+    def upload(self, be):
+        g = self.grid
+        k = g["kind"]
+        if k == abi.GRID_CARTESIAN:
+            be.upload_grid_cartesian(g["xb"], g["yb"], g["zb"])
+        elif k == abi.GRID_OCTREE:
+            be.upload_grid_octree(g["bounds"], g["cell_index"], g["child_begin"], g["child_count"], g["child_index"],
+                                  g["nb_begin"], g["nb_index"], g["eps"])
+        elif k == abi.GRID_VORONOI:
+            be.upload_grid_voronoi(g["sites"], g["nb_begin"], g["nb_index"], g["extent"], g["eps"])
+        elif k == abi.GRID_TETRA:
+            be.upload_grid_tetra(g["vertices"], g["tetra"], g["normals"], g["ntetra"], g["nface"], g["extent"], g["eps"])
+        else:
+            raise ValueError(f"unknown grid kind {k}")
+        if self.density is not None:
+            be.upload_medium(self.density)
+        if self.mix is not None:
+            m = self.mix
+            be.upload_dust_mix(m["lambda_borders"], m["sigma_ext"], m["sigma_sca"], m["asymmpar"])
+        if self.rf is not None:
+            be.upload_rf_grid(self.rf["num_bins"], self.rf["borders"], self.rf["ellv"])
+        if self.instruments:
+            self._upload_instruments(be)
+
+    def _upload_instruments(self, be):
+        structs, borders, ellv = [], [], []
+        for ins in self.instruments:
+            s = abi.Instrument()
+            s.kind = ins["kind"]
+            s.same_observer = int(ins.get("same_observer", 0))
+            s.record_statistics = int(ins.get("stats", 0))
+            s.record_components = int(ins.get("comps", 0))
+            s.num_wavelength_bins = int(ins["num_bins"])
+            s.wlg_offset = len(ellv)
+            s.wlg_num_borders = len(ins["wlg_borders"])
+            borders.extend(list(ins["wlg_borders"]) + [0.0])
+            ellv.extend(list(ins["wlg_ellv"]))
+            s.kobs[:] = list(ins["kobs"])
+            if s.kind == abi.INSTR_FRAME:
+                s.num_pixels_x, s.num_pixels_y = int(ins["nx"]), int(ins["ny"])
+                (s.cos_theta, s.sin_theta, s.cos_phi, s.sin_phi, s.cos_omega, s.sin_omega) = ins["trig"]
+                s.xp_min, s.xp_size, s.yp_min, s.yp_size = ins["xp_min"], ins["xp_size"], ins["yp_min"], ins["yp_size"]
+            structs.append(s)
+        be.upload_instruments(structs, np.array(borders), np.array(ellv, np.int32))
+
+    def source_structs(self, npp):
+        """ABI source records for a segment of npp packets (SourceSystem::prepareForLaunch)."""
+        lv = np.array([s["lfrac"] for s in self.sources], float)
+        wv = np.array([s["weight"] for s in self.sources], float)
+        first = [0]
+        W = 0.0
+        for h in range(1, len(self.sources)):
+            W += wv[h - 1]
+            first.append(min(npp, int(np.floor(W * npp + 0.5))))  # std::round
+        first.append(npp)
+        structs, tl, ta, tb, rr, rp = [], [], [], [], [], []
+        for h, src in enumerate(self.sources):
+            s = abi.Source()
+            s.position_model = src["position_model"]
+            s.spectral_model = src["spectral_model"]
+            s.position[:] = list(src.get("position", (0.0, 0.0, 0.0)))
+            geo = list(src.get("geometry", ())) + [0.0] * 6
+            s.geometry[:] = geo[:6]
+            s.first_history = first[h]
+            s.num_histories = first[h + 1] - first[h]
+            s.packet_luminosity = self.total_luminosity / npp * lv[h] / wv[h]
+            s.wavelength_bias = src.get("wavelength_bias", 0.0)
+            s.bias_lambda_min, s.bias_lambda_max = src.get("bias_range", (0.0, 0.0))
+            s.table_offset = len(tl)
+            s.table_size = len(src["table_lambda"])
+            tl.extend(src["table_lambda"])
+            ta.extend(src["table_a"])
+            tb.extend(src.get("table_b", np.zeros(len(src["table_lambda"]))))
+            if s.position_model == abi.SRC_RADIAL:
+                s.radial_offset = len(rr)
+                s.radial_size = len(src["radial_r"])
+                rr.extend(src["radial_r"])
+                rp.extend(src["radial_P"])
+            structs.append(s)
+        if not rr:
+            rr, rp = [0.0], [0.0]
+        return structs, np.array(tl), np.array(ta), np.array(tb), np.array(rr), np.array(rp)
+
+    def options(self, seed=0, precision=abi.PREC_FP64_EXACT, peel=True):
+        o = abi.Options()
+        o.force_scattering = int(self.force_scattering)
+        o.min_scatt_events = int(self.min_scatt_events)
+        o.min_weight_reduction = float(self.min_weight_reduction)
+        o.path_length_bias = float(self.path_length_bias)
+        o.store_radiation_field = int(self.store_rf)
+        o.peel_off = int(peel)
+        o.precision = int(precision)
+        o.seed = int(seed)
+        return o
+
+    # ------------------------------------------------------------------ run
+    def instrument_size(self, i):
+        ins = self.instruments[i]
+        npix = ins["nx"] * ins["ny"] if ins["kind"] == abi.INSTR_FRAME else 1
+        return npix * ins["num_bins"]
+
+    def prepare(self, be, npp, seed=0, precision=abi.PREC_FP64_EXACT):
+        be.set_options(self.options(seed, precision))
+        structs, tl, ta, tb, rr, rp = self.source_structs(npp)
+        be.upload_sources(structs, tl, ta, tb, rr, rp)
+
+    def run(self, be, npp, seed=0, precision=abi.PREC_FP64_EXACT, first=0, count=None, clear=True):
+        """One primary-emission segment of npp packets (histories [first, first+count))."""
+        if clear:
+            be.clear_tallies()
+        self.prepare(be, npp, seed, precision)
+        be.run_primary(first, npp if count is None else count, npp)
+        return self.fetch(be)
+
+    def fetch(self, be):
+        res = Results()
+        for i, ins in enumerate(self.instruments):
+            n = self.instrument_size(i)
+            total, stats = be.fetch_instrument(i, n, stats=bool(ins.get("stats")))
+            d = {"total": total, "stats": stats}
+            if ins.get("comps"):
+                d["components"] = be.fetch_instrument_components(i, n)
+            if ins["kind"] == abi.INSTR_FRAME:
+                shape = (ins["num_bins"], ins["ny"], ins["nx"])
+                d["total"] = total.reshape(shape)
+                if stats is not None:
+                    d["stats"] = stats.reshape((5,) + shape)
+                if "components" in d:
+                    d["components"] = d["components"].reshape((3,) + shape)
+            res.instruments.append(d)
+        if self.store_rf:
+            res.rf = be.fetch_radiation_field(len(self.density) * self.rf["num_bins"]).reshape(len(self.density), -1)
+        res.counters = be.counters()
+        res.ms = be.last_run_ms()
+        return res
+
+    # ------------------------------------------------------------------ export loader
+    @classmethod
+    def from_export(cls, d, npp_probe=1000):
+        """Scene from the .npy files the reference export harness wrote into directory d."""
+        meta = {}
+        with open(os.path.join(d, "meta.txt")) as f:
+            for line in f:
+                k, _, v = line.strip().partition(" ")
+                meta[k] = v
+        L = lambda name: np.load(os.path.join(d, name + ".npy"))
+        sc = cls()
+        kind = meta["grid"]
+        ext = L("grid_extent")
+        if kind == "cartesian":
+            sc.grid = dict(kind=abi.GRID_CARTESIAN, xb=L("grid_xb"), yb=L("grid_yb"), zb=L("grid_zb"), extent=ext)
+        elif kind == "octree":
+            sc.grid = dict(kind=abi.GRID_OCTREE, bounds=L("tree_bounds"), cell_index=L("tree_cell_index"),
+                           child_begin=L("tree_child_begin"), child_count=L("tree_child_count"),
+                           child_index=L("tree_child_index"), nb_begin=L("tree_nb_begin"),
+                           nb_index=L("tree_nb_index"), eps=float(meta["eps"]), extent=ext)
+        elif kind == "voronoi":
+            sc.grid = dict(kind=abi.GRID_VORONOI, sites=L("vor_sites"), nb_begin=L("vor_nb_begin"),
+                           nb_index=L("vor_nb_index"), extent=ext, eps=float(meta["eps"]))
+        elif kind == "tetra":
+            sc.grid = dict(kind=abi.GRID_TETRA, vertices=L("tet_vertices"), tetra=L("tet_tetra"),
+                           normals=L("tet_normals"), ntetra=L("tet_ntetra"), nface=L("tet_nface"), extent=ext,
+                           eps=float(meta["eps"]))
+        else:
+            raise ValueError(f"unsupported grid in export: {kind}")
+        sc.density = L("medium_density")[:, 0].copy()
+        sc.mix = dict(lambda_borders=L("mix0_lambda_borders"), sigma_ext=L("mix0_sigma_ext"),
+                      sigma_sca=L("mix0_sigma_sca"), asymmpar=L("mix0_asymmpar"))
+        sc.force_scattering = bool(int(meta["force_scattering"]))
+        sc.min_weight_reduction = float(meta["min_weight_reduction"])
+        sc.min_scatt_events = int(float(meta["min_scatt_events"]))
+        sc.path_length_bias = float(meta["path_length_bias"])
+        if os.path.exists(os.path.join(d, "rf_wlg_borders.npy")):
+            ellv = L("rf_wlg_ellv")
+            sc.rf = dict(num_bins=int(ellv.max()) + 1, borders=L("rf_wlg_borders"), ellv=ellv)
+        # sources: the launch probe gives lambda and L*npp of the reference's own launches
+        sc.total_luminosity = float(meta["source_total_luminosity"])
+        probe = L("src_probe")
+        nsrc = int(meta["num_sources"])
+        if nsrc != 1 or meta["source0_type"] != "PointSource" or meta["oligochromatic"] != "1":
+            raise ValueError("export loader supports the oligochromatic single point source only")
+        lams = np.unique(probe[:, 0])
+        weights = np.array([probe[probe[:, 0] == l, 1][0] for l in lams]) / sc.total_luminosity
+        sc.sources = [dict(position_model=abi.SRC_POINT, spectral_model=abi.SPEC_DISCRETE,
+                           position=tuple(probe[0, 2:5]), lfrac=float(meta["source0_lfrac"]),
+                           weight=float(meta["source0_weight"]), table_lambda=lams, table_a=weights)]
+        for i in range(int(meta["num_instruments"])):
+            p = f"instr{i}_"
+            ellv = L(p + "wlg_ellv")
+            ins = dict(kind=abi.INSTR_FRAME if meta[p + "kind"] == "frame" else abi.INSTR_SED,
+                       same_observer=int(meta[p + "same_observer"]), stats=int(meta[p + "record_statistics"]),
+                       num_bins=int(ellv.max()) + 1, wlg_borders=L(p + "wlg_borders"), wlg_ellv=ellv,
+                       kobs=(float(meta[p + "kobs_x"]), float(meta[p + "kobs_y"]), float(meta[p + "kobs_z"])))
+            if ins["kind"] == abi.INSTR_FRAME:
+                ins.update(nx=int(meta[p + "nxp"]), ny=int(meta[p + "nyp"]),
+                           trig=tuple(float(meta[p + k]) for k in
+                                      ("costheta", "sintheta", "cosphi", "sinphi", "cosomega", "sinomega")),
+                           xp_min=float(meta[p + "xpmin"]), xp_size=float(meta[p + "xpsiz"]),
+                           yp_min=float(meta[p + "ypmin"]), yp_size=float(meta[p + "ypsiz"]))
+            sc.instruments.append(ins)
+        return sc

@@ -1,0 +1,144 @@
+"""Writers for SKIRT 9 ski files (the SimulationItem XML the reference reads).
+
+These produce the ski files of the named workloads (dust shell on a Cartesian grid, exponential
+disk galaxy on an octree, Voronoi and tetrahedral meshes, the edge-on thick disk) so that the
+reference CPU code and this tracer run the same configuration. Element and attribute names are
+those of the reference's schema (`skirt -x`, registered in SKIRT/core/SimulationItemRegistry.cpp).
+"""
+
+PC = 3.0856775814913673e16  # m, SKIRT Constants::pc()
+
+
+def _q(v, unit):
+    return f"{v:.17g} {unit}" if unit else f"{v:.17g}"
+
+
+def cartesian_grid(half_size_pc, nbins, points=None):
+    """CartesianSpatialGrid on +-half_size; LinMesh, or ListMesh with normalised border points."""
+    if points is None:
+        mesh = f'<LinMesh numBins="{nbins}"/>'
+        meshes = {a: mesh for a in "XYZ"}
+    else:
+        meshes = {a: '<ListMesh points="' + ", ".join(f"{p:.17g}" for p in points[a]) + '"/>' for a in "XYZ"}
+    h = half_size_pc
+    return (f'<CartesianSpatialGrid minX="{-h} pc" maxX="{h} pc" minY="{-h} pc" maxY="{h} pc" '
+            f'minZ="{-h} pc" maxZ="{h} pc">'
+            f'<meshX type="Mesh">{meshes["X"]}</meshX><meshY type="Mesh">{meshes["Y"]}</meshY>'
+            f'<meshZ type="Mesh">{meshes["Z"]}</meshZ></CartesianSpatialGrid>')
+
+
+def octree_grid(half_size, unit, max_level, max_dust_fraction, min_level=2):
+    h = half_size
+    return (f'<PolicyTreeSpatialGrid minX="{-h} {unit}" maxX="{h} {unit}" minY="{-h} {unit}" maxY="{h} {unit}" '
+            f'minZ="{-h} {unit}" maxZ="{h} {unit}" treeType="OctTree">'
+            f'<policy type="TreePolicy"><DensityTreePolicy minLevel="{min_level}" maxLevel="{max_level}" '
+            f'maxDustFraction="{max_dust_fraction:g}" maxDustOpticalDepth="0" wavelength="0.55 micron" '
+            f'maxDustDensityDispersion="0" maxElectronFraction="1e-6" maxGasFraction="1e-6"/></policy>'
+            f'</PolicyTreeSpatialGrid>')
+
+
+def voronoi_grid(half_size, unit, num_sites, policy="DustDensity"):
+    h = half_size
+    return (f'<VoronoiMeshSpatialGrid minX="{-h} {unit}" maxX="{h} {unit}" minY="{-h} {unit}" maxY="{h} {unit}" '
+            f'minZ="{-h} {unit}" maxZ="{h} {unit}" policy="{policy}" numSites="{num_sites}" relaxSites="false"/>')
+
+
+def tetra_grid(half_size, unit, num_samples, policy="DustDensity"):
+    h = half_size
+    return (f'<TetraMeshSpatialGrid minX="{-h} {unit}" maxX="{h} {unit}" minY="{-h} {unit}" maxY="{h} {unit}" '
+            f'minZ="{-h} {unit}" maxZ="{h} {unit}" policy="{policy}" numSamples="{num_samples}" refine="false"/>')
+
+
+def shell_medium(rmin_pc, rmax_pc, exponent, tau_x, mix):
+    return (f'<GeometricMedium velocityMagnitude="0 km/s" magneticFieldStrength="0 uG">'
+            f'<geometry type="Geometry"><ShellGeometry minRadius="{rmin_pc} pc" maxRadius="{rmax_pc} pc" '
+            f'exponent="{exponent}"/></geometry>'
+            f'<materialMix type="MaterialMix">{mix}</materialMix>'
+            f'<normalization type="MaterialNormalization"><OpticalDepthMaterialNormalization axis="X" '
+            f'wavelength="0.55 micron" opticalDepth="{tau_x}"/></normalization></GeometricMedium>')
+
+
+def expdisk_medium(hR, hz, unit, tau_z, mix):
+    return (f'<GeometricMedium velocityMagnitude="0 km/s" magneticFieldStrength="0 uG">'
+            f'<geometry type="Geometry"><ExpDiskGeometry scaleLength="{hR} {unit}" scaleHeight="{hz} {unit}" '
+            f'minRadius="0 {unit}" maxRadius="0 {unit}" maxZ="0 {unit}"/></geometry>'
+            f'<materialMix type="MaterialMix">{mix}</materialMix>'
+            f'<normalization type="MaterialNormalization"><OpticalDepthMaterialNormalization axis="Z" '
+            f'wavelength="0.55 micron" opticalDepth="{tau_z}"/></normalization></GeometricMedium>')
+
+
+def mean_list_mix(wavelengths_um, kappa, albedo, g):
+    j = lambda v, u="": ", ".join(f"{x:.17g}{(' ' + u) if u else ''}" for x in v)
+    return (f'<MeanListDustMix wavelengths="{j(wavelengths_um, "micron")}" '
+            f'extinctionCoefficients="{j(kappa, "m2/kg")}" albedos="{j(albedo)}" asymmetryParameters="{j(g)}"/>')
+
+
+def point_source(temperature=5800, luminosity_lsun=1.0):
+    return (f'<PointSource positionX="0 pc" positionY="0 pc" positionZ="0 pc" velocityX="0 km/s" velocityY="0 km/s" '
+            f'velocityZ="0 km/s" sourceWeight="1" wavelengthBias="0.5">'
+            f'<angularDistribution type="AngularDistribution"><IsotropicAngularDistribution/></angularDistribution>'
+            f'<polarizationProfile type="PolarizationProfile"><NoPolarizationProfile/></polarizationProfile>'
+            f'<sed type="SED"><BlackBodySED temperature="{temperature} K"/></sed>'
+            f'<normalization type="LuminosityNormalization"><IntegratedLuminosityNormalization wavelengthRange="All" '
+            f'integratedLuminosity="{luminosity_lsun} Lsun"/></normalization></PointSource>')
+
+
+def frame_instrument(name, inclination_deg, fov, unit, npix, stats=True, distance_mpc=10, comps=False):
+    return (f'<FrameInstrument instrumentName="{name}" distance="{distance_mpc} Mpc" inclination="{inclination_deg} deg" '
+            f'azimuth="0 deg" roll="0 deg" fieldOfViewX="{fov} {unit}" numPixelsX="{npix}" centerX="0 {unit}" '
+            f'fieldOfViewY="{fov} {unit}" numPixelsY="{npix}" centerY="0 {unit}" '
+            f'recordComponents="{"true" if comps else "false"}" numScatteringLevels="0" recordPolarization="false" '
+            f'recordStatistics="{"true" if stats else "false"}"/>')
+
+
+def sed_instrument(name, inclination_deg, stats=True, distance_mpc=10, comps=True):
+    return (f'<SEDInstrument instrumentName="{name}" distance="{distance_mpc} Mpc" inclination="{inclination_deg} deg" '
+            f'azimuth="0 deg" roll="0 deg" radius="0 pc" recordComponents="{"true" if comps else "false"}" '
+            f'numScatteringLevels="0" recordPolarization="false" recordStatistics="{"true" if stats else "false"}"/>')
+
+
+def simulation(mode, num_packets, sources, media, grid, instruments, source_wavelengths="0.55 micron",
+               instrument_wlg='<ListWavelengthGrid wavelengths="0.55 micron" relativeHalfWidth="0" log="false"/>',
+               force_scattering=True, store_rf=False, rf_wlg="", seed=0, num_density_samples=100,
+               min_weight_reduction=1e4, path_length_bias=0.5):
+    """A complete MonteCarloSimulation ski document."""
+    src_attr = f' wavelengths="{source_wavelengths}"' if mode.startswith("Oligo") else ' minWavelength="0.1 micron" maxWavelength="10 micron"'
+    rf = ""
+    if store_rf or rf_wlg:
+        rf = (f'<radiationFieldOptions type="RadiationFieldOptions"><RadiationFieldOptions '
+              f'storeRadiationField="{"true" if store_rf else "false"}">'
+              + (f'<radiationFieldWLG type="DisjointWavelengthGrid">{rf_wlg}</radiationFieldWLG>' if rf_wlg else "")
+              + '</RadiationFieldOptions></radiationFieldOptions>')
+    return f'''<?xml version="1.0" encoding="UTF-8"?>
+<skirt-simulation-hierarchy type="MonteCarloSimulation" format="9" producer="skgpu" time="2026-01-01T00:00:00">
+<MonteCarloSimulation userLevel="Expert" simulationMode="{mode}" iteratePrimaryEmission="false" iterateSecondaryEmission="false" numPackets="{num_packets:g}">
+<random type="Random"><Random seed="{seed}"/></random>
+<units type="Units"><ExtragalacticUnits wavelengthOutputStyle="Wavelength" fluxOutputStyle="Frequency"/></units>
+<cosmology type="Cosmology"><LocalUniverseCosmology/></cosmology>
+<sourceSystem type="SourceSystem"><SourceSystem{src_attr} sourceBias="0.5">
+<sources type="Source">{sources}</sources></SourceSystem></sourceSystem>
+<mediumSystem type="MediumSystem"><MediumSystem>
+<photonPacketOptions type="PhotonPacketOptions"><PhotonPacketOptions explicitAbsorption="false" forceScattering="{"true" if force_scattering else "false"}" minWeightReduction="{min_weight_reduction:g}" minScattEvents="0" pathLengthBias="{path_length_bias:g}"/></photonPacketOptions>
+{rf}
+<media type="Medium">{media}</media>
+<samplingOptions type="SamplingOptions"><SamplingOptions numDensitySamples="{num_density_samples}" numPropertySamples="1" aggregateVelocity="Average"/></samplingOptions>
+<grid type="SpatialGrid">{grid}</grid>
+</MediumSystem></mediumSystem>
+<instrumentSystem type="InstrumentSystem"><InstrumentSystem>
+<defaultWavelengthGrid type="WavelengthGrid">{instrument_wlg}</defaultWavelengthGrid>
+<instruments type="Instrument">{instruments}</instruments>
+</InstrumentSystem></instrumentSystem>
+<probeSystem type="ProbeSystem"><ProbeSystem/></probeSystem>
+</MonteCarloSimulation>
+</skirt-simulation-hierarchy>
+'''
+
+
+def shell_cartesian(num_packets=1e6, nbins=64, npix=256, stats=True, points=None):
+    """Dust shell (r^-2 between 0.1 and 1 pc, radial tau_V = 1, i.e. tau_X = 2 through the centre) on a
+    Cartesian grid of +-1 pc, isotropic point source at the centre, 0.55 micron, HG g = 0.6,
+    albedo 0.5, one frame at inclination 30 degrees plus one SED instrument."""
+    mix = mean_list_mix([0.5, 0.6], [1, 1], [0.5, 0.5], [0.6, 0.6])
+    return simulation("OligoExtinctionOnly", num_packets, point_source(),
+                      shell_medium(0.1, 1, 2, 2, mix), cartesian_grid(1, nbins, points),
+                      frame_instrument("i30", 30, 2, "pc", npix, stats) + sed_instrument("sed", 30, stats))
