@@ -1,0 +1,306 @@
+"""Throughput benchmark of the photon-packet life cycle: packets/s on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+One step = one primary-emission segment of the workload's packets through the C ABI
+(skgpu_run_primary): launch, emission peel-off, forced-scattering propagation, scattering
+peel-off and HG scattering for every history. `value` is device time (CUDA events on the launch
+stream, L2 flushed between steps); `e2e` is measured through the same C ABI with host buffers
+(medium state uploaded, tallies read back to the host every step). Under torchrun each rank
+traces its own contiguous range of history indices (weak scaling; no data-path collective).
+"""
+import argparse
+import json
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [os.path.join(ROOT, "skirt9-gpu_b200"), os.path.join(ROOT, "oracle")]
+
+REF_SKIRT = os.path.join(ROOT, "oracle", "_ref", "exe", "skirt", "bin", "skirt")
+
+WORKLOADS = {
+    # name: (description, packets per step per GPU)
+    "shell": ("dust shell r^-2 0.1-1 pc on a 64^3 CartesianSpatialGrid, tau_V=1, point source, 0.55 um, "
+              "HG g=0.6 albedo 0.5, 256^2 frame at 30 deg + SED, FP64 tallies with statistics", 1_000_000),
+}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p["hbm_gbs"], "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index=0):
+        self.samples = []
+        self.proc = None
+        self.index = index
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.index), "-lms", "100"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([s.strip() for s in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 5 + i and "Active" in s[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons}
+
+
+def build_scene(name):
+    from skgpu import workloads
+    if name == "shell":
+        return workloads.shell_cartesian(64, 256)
+    raise SystemExit(f"unknown workload {name}")
+
+
+def algorithmic_bytes(counters, grid_kind):
+    """Bytes per launch by the unit costs of the measurement plan: per cell crossing the grid's
+    record (Cartesian 4 B, octree 64 B, Voronoi 284 B, tetra 84 B), 128 B per interaction event
+    (packet state read + write), 16 B per peel-off detection and per radiation-field update."""
+    per_cross = {0: 4, 1: 64, 2: 284, 3: 84}[grid_kind]
+    return (per_cross * counters["crossings"] + 128 * counters["scatterings"]
+            + 16 * (counters["peel_detections"] + counters["rf_stores"]))
+
+
+def reference_run(scene_ski, npp, threads):
+    """Runs the reference CPU code on a ski file; returns (packets/s of the primary segment, secs)."""
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "bench.ski")
+        with open(path, "w") as f:
+            f.write(scene_ski)
+        out = subprocess.run([REF_SKIRT, "-t", str(threads), "bench.ski"], cwd=tmp, capture_output=True, text=True)
+        if out.returncode != 0:
+            raise RuntimeError("reference run failed: " + out.stdout[-500:] + out.stderr[-500:])
+        m = re.search(r"Finished primary emission in ([0-9.]+) s", out.stdout)
+        secs = float(m.group(1))
+        return npp / secs, secs
+
+
+def reference_ski(name, npp):
+    from skgpu import ski
+    if name == "shell":
+        return ski.shell_cartesian(npp, nbins=64, npix=256)
+    raise SystemExit(name)
+
+
+def cpu_baseline(name, budget_s=20.0):
+    """The reference's own multithreaded CPU path on the host cores, on a bounded sample."""
+    cores = os.cpu_count() or 1
+    if os.path.exists(REF_SKIRT):
+        probe = 20000
+        rate, secs = reference_run(reference_ski(name, probe), probe, cores)
+        npp = int(min(5e7, max(probe, rate * budget_s)))
+        rate, secs = reference_run(reference_ski(name, npp), npp, cores)
+        return {"value": rate, "unit": "packets/s", "cores": cores, "kind": "reference",
+                "sample": f"{npp} packets of the same workload, skirt -t {cores}, primary-emission segment "
+                          f"{secs:.2f} s (setup excluded)"}
+    import oracle
+    sc = build_scene(name)
+    be = oracle.backend()
+    sc.upload(be)
+    n = 20000
+    t = time.perf_counter()
+    sc.run(be, n, seed=1)
+    secs = time.perf_counter() - t
+    return {"value": n / secs, "unit": "packets/s", "cores": 1, "kind": "port",
+            "sample": f"{n} packets of the same workload through the single-threaded C oracle"}
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    name = args.workload
+    if not os.path.exists(REF_SKIRT):
+        print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref missing (build() compiles "
+                          "it where the reference sources are present)"}))
+        return
+    cores = os.cpu_count() or 1
+    probe = 20000
+    rate, _ = reference_run(reference_ski(name, probe), probe, cores)
+    npp = int(min(5e7, max(probe, rate * 8.0)))
+    vals = []
+    for _ in range(args.warmup):
+        reference_run(reference_ski(name, min(npp, probe)), min(npp, probe), cores)
+    for _ in range(args.steps):
+        r, _ = reference_run(reference_ski(name, npp), npp, cores)
+        vals.append(r)
+    value = statistics.median(vals)
+    line = {"metric": "packets/s on 1 B200", "value": value, "unit": "packets/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * npp / value,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": name, "description": WORKLOADS[name][0], "packets_per_step": npp,
+                       "l2": "n/a (CPU)"},
+            "cpu_baseline": {"value": value, "unit": "packets/s", "cores": cores, "kind": "reference",
+                             "sample": f"{npp} packets per step, skirt -t {cores}, primary-emission segment"},
+            "e2e": {"value": value, "unit": "packets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="shell", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl" if args.impl == "ours" else "gloo", timeout=datetime.timedelta(seconds=300))
+
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    import torch
+    from skgpu import Backend, abi
+
+    torch.cuda.set_device(local)
+    name = args.workload
+    sc = build_scene(name)
+    per_gpu = WORKLOADS[name][1]
+    npp_total = per_gpu * world
+    first = rank * per_gpu
+    prec = abi.PREC_FP64_EXACT if args.precision == "fp64" else abi.PREC_FP32
+    be = Backend(device=local)
+    sc.upload(be)
+    sc.prepare(be, npp_total, seed=12345, precision=prec)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")  # 256 MB > L2
+
+    def step():
+        be.run_primary(first, per_gpu, npp_total)
+        return be.last_run_ms()
+
+    for _ in range(args.warmup):
+        step()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms = []
+    counters = None
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            ms.append(step())
+            counters = be.counters()
+    torch.cuda.synchronize()
+    total_ms = float(sum(ms))
+    if dist:
+        t = torch.tensor([total_ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = npp_total * args.steps / (total_ms / 1e3)
+
+    # end to end through the C ABI with host buffers: medium state in, tallies out, every step
+    dens = np.ascontiguousarray(sc.density)
+    sizes = [sc.instrument_size(i) for i in range(len(sc.instruments))]
+    h2d = dens.nbytes
+    d2h = sum(8 * n for n in sizes) + sum(40 * n for i, n in enumerate(sizes) if sc.instruments[i].get("stats"))
+    be.clear_tallies()
+    e2e_times = []
+    for _ in range(max(1, min(args.steps, 3))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        be.upload_medium(dens)
+        be.run_primary(first, per_gpu, npp_total)
+        for i, n in enumerate(sizes):
+            be.fetch_instrument(i, n, stats=bool(sc.instruments[i].get("stats")))
+        torch.cuda.synchronize()
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_s = statistics.median(e2e_times)
+    if dist:
+        t = torch.tensor([e2e_s], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+
+    if rank == 0:
+        peak, peak_kind = peaks()
+        launch_ms = total_ms / args.steps
+        alg = algorithmic_bytes(counters, sc.grid["kind"])
+        achieved = alg / (launch_ms / 1e3) / 1e9
+        traffic = None
+        prof = os.path.join(ROOT, "profiles", f"lifecycle_{name}.json")
+        if os.path.exists(prof):
+            with open(prof) as f:
+                traffic = json.load(f).get("dram_bytes_per_launch")
+        line = {
+            "metric": "packets/s on 1 B200", "value": value, "unit": "packets/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": launch_ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == abi.PREC_FP64_EXACT else "f32+f64",
+            "data": "synthetic",
+            "config": {"workload": name, "description": WORKLOADS[name][0], "packets_per_step_per_gpu": per_gpu,
+                       "traversal": args.precision, "l2": "flushed between steps (256 MB write)",
+                       "parallelism": f"history ranges x{world}"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "skg::lifecycleKernel", "algorithmic_bytes_per_launch": alg},
+            "clocks": clk.summary(),
+            "e2e": {"value": npp_total / e2e_s, "unit": "packets/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": args.steps,
+            "counters_per_step": counters,
+        }
+        if not args.no_cpu_baseline:
+            try:
+                line["cpu_baseline"] = cpu_baseline(name)
+            except Exception as e:  # the baseline is reported, never required for the GPU number
+                line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+        print(json.dumps(line))
+    be.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

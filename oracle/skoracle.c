@@ -1287,6 +1287,7 @@ static void launch(or_ctx* c, Rng* r, uint64_t hist, Packet* pk)
     }
     iso_direction(r, &pk->kx, &pk->ky, &pk->kz);
     pk->ellMix = locate_clip(c->mixLb, c->nmix, lambda);
+    if (pk->ellMix < 0) pk->ellMix = 0;
     pk->sext = c->mixExt[pk->ellMix];
     pk->ssca = c->mixSca[pk->ellMix];
     pk->g = c->mixG[pk->ellMix];
@@ -1563,7 +1564,8 @@ int or_optical_depths(or_ctx* c, int32_t num_rays, const double* rays, double la
 {
     (void)precision;
     if (!c->hasGrid || !c->dens || !c->nmix) return fail(c, SKGPU_ERR_STATE, "optical depths: incomplete scene");
-    double section = c->mixExt[locate_clip(c->mixLb, c->nmix, lambda)];
+    int ell = locate_clip(c->mixLb, c->nmix, lambda);
+    double section = c->mixExt[ell < 0 ? 0 : ell];
     for (int r = 0; r < num_rays; ++r)
     {
         Gen s;
@@ -1585,3 +1587,9 @@ int or_optical_depths(or_ctx* c, int32_t num_rays, const double* rays, double la
     }
     return SKGPU_OK;
 }
+
+/* C struct sizes of the ABI records, for the binding layout test */
+int or_sizeof_source(void) { return (int)sizeof(skgpu_source); }
+int or_sizeof_instrument(void) { return (int)sizeof(skgpu_instrument); }
+int or_sizeof_options(void) { return (int)sizeof(skgpu_options); }
+int or_sizeof_counters(void) { return (int)sizeof(skgpu_counters); }

@@ -60,6 +60,12 @@ int or_trace_paths(or_ctx* ctx, int32_t num_rays, const double* rays, int32_t ma
 int or_optical_depths(or_ctx* ctx, int32_t num_rays, const double* rays, double lambda, int32_t precision,
                       double* tau);
 
+/* C sizes of the ABI records (binding layout test) */
+int or_sizeof_source(void);
+int or_sizeof_instrument(void);
+int or_sizeof_options(void);
+int or_sizeof_counters(void);
+
 /* Philox4x32-10 block, exported for known-answer tests */
 void or_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 

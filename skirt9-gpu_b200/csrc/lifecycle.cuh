@@ -29,6 +29,7 @@ namespace skg {
 
 constexpr int MAX_INSTR = 16;
 constexpr int STATS_CAP = 48;
+constexpr int MAX_SCATT_EVENTS = 1 << 20;
 
 struct SourceDev
 {
@@ -343,7 +344,7 @@ struct LifeCycle
         // wavelength-dependent quantities are constant during a history (no kinematics)
         if (p.nmix > 0)
         {
-            ln.ellMix = locateClip(p.mixLb, p.nmix, lambda);
+            ln.ellMix = max(0, locateClip(p.mixLb, p.nmix, lambda));  // a one-entry table has a single bin
             ln.sext = p.mixExt[ln.ellMix];
             ln.ssca = p.mixSca[ln.ellMix];
             ln.gHG = p.mixG[ln.ellMix];
@@ -520,6 +521,12 @@ struct LifeCycle
     // HG scattering (DustMix::performScattering, DustMix.cpp:490-546) and PhotonPacket::scatter
     SKG_D void scatter()
     {
+        if (ln.nscatt >= MAX_SCATT_EVENTS)
+        {
+            // a history that never meets its termination criterion (e.g. albedo 1 in a thick medium)
+            raiseError(8);
+            ln.L = 0.;
+        }
         double g = ln.gHG;
         if (fabs(g) < 1e-6)
         {

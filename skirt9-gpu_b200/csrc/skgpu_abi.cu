@@ -693,6 +693,7 @@ int skgpu_run_primary(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t t
     ctx->lastCounters.stats_overflows = cnt[5];
     ctx->lastCounters.kernel_launches = count > 0 ? 1 : 0;
     if (errFlag & 4) return fail(ctx, SKGPU_ERR_TIMEOUT, "run: a traversal exceeded its segment guard");
+    if (errFlag & 8) return fail(ctx, SKGPU_ERR_TIMEOUT, "run: a history exceeded the scattering-event guard");
     if (errFlag) return fail(ctx, SKGPU_ERR_DEVICE, "run: interaction point outside the grid (device check)");
     return SKGPU_OK;
 }
@@ -829,7 +830,7 @@ int skgpu_optical_depths(skgpu_ctx* ctx, int32_t num_rays, const double* rays, d
     std::vector<double> lb(ctx->nmix), se(ctx->nmix);
     CK(cudaMemcpy(lb.data(), ctx->mixLb, ctx->nmix * sizeof(double), cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(se.data(), ctx->mixExt, ctx->nmix * sizeof(double), cudaMemcpyDeviceToHost));
-    double section = se[skg::locateClip(lb.data(), ctx->nmix, lambda)];
+    double section = se[std::max(0, skg::locateClip(lb.data(), ctx->nmix, lambda))];
     size_t n = num_rays;
     double *dRays = nullptr, *dTau = nullptr;
     cudaError_t e = devUpload(&dRays, rays, 6 * n);

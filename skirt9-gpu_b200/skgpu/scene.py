@@ -180,15 +180,30 @@ class Scene:
         return res
 
     # ------------------------------------------------------------------ export loader
-    @classmethod
-    def from_export(cls, d, npp_probe=1000):
-        """Scene from the .npy files the reference export harness wrote into directory d."""
+    @staticmethod
+    def read_export(d):
+        """(meta dict, array loader) for an export directory or a mapping (e.g. an .npz) holding the
+        same arrays under their file stems plus the meta text under 'meta'."""
+        if isinstance(d, str):
+            with open(os.path.join(d, "meta.txt")) as f:
+                text = f.read()
+            load = lambda name: np.load(os.path.join(d, name + ".npy"))
+            has = lambda name: os.path.exists(os.path.join(d, name + ".npy"))
+        else:
+            text = str(d["meta"])
+            load = lambda name: np.asarray(d[name])
+            has = lambda name: name in d
         meta = {}
-        with open(os.path.join(d, "meta.txt")) as f:
-            for line in f:
-                k, _, v = line.strip().partition(" ")
+        for line in text.splitlines():
+            k, _, v = line.strip().partition(" ")
+            if k:
                 meta[k] = v
-        L = lambda name: np.load(os.path.join(d, name + ".npy"))
+        return meta, load, has
+
+    @classmethod
+    def from_export(cls, d):
+        """Scene from the arrays the reference export harness wrote (directory or mapping)."""
+        meta, L, has = cls.read_export(d)
         sc = cls()
         kind = meta["grid"]
         ext = L("grid_extent")
@@ -215,7 +230,7 @@ class Scene:
         sc.min_weight_reduction = float(meta["min_weight_reduction"])
         sc.min_scatt_events = int(float(meta["min_scatt_events"]))
         sc.path_length_bias = float(meta["path_length_bias"])
-        if os.path.exists(os.path.join(d, "rf_wlg_borders.npy")):
+        if has("rf_wlg_borders"):
             ellv = L("rf_wlg_ellv")
             sc.rf = dict(num_bins=int(ellv.max()) + 1, borders=L("rf_wlg_borders"), ellv=ellv)
         # sources: the launch probe gives lambda and L*npp of the reference's own launches

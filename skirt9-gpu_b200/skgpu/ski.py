@@ -134,6 +134,15 @@ def simulation(mode, num_packets, sources, media, grid, instruments, source_wave
 '''
 
 
+def disk_probe(grid_xml, num_packets=1e4, tau_z=1.0, hR=1.0, hz=0.2):
+    """Oligochromatic exponential dust disk (scale length hR pc, height hz pc) with a central
+    point source and one SED instrument, on the given grid; used to export grids and paths."""
+    mix = mean_list_mix([0.5, 0.6], [1, 1], [0.5, 0.5], [0.6, 0.6])
+    return simulation("OligoExtinctionOnly", num_packets, point_source(),
+                      expdisk_medium(hR, hz, "pc", tau_z, mix), grid_xml, sed_instrument("sed", 30, False),
+                      num_density_samples=10)
+
+
 def shell_cartesian(num_packets=1e6, nbins=64, npix=256, stats=True, points=None):
     """Dust shell (r^-2 between 0.1 and 1 pc, radial tau_V = 1, i.e. tau_X = 2 through the centre) on a
     Cartesian grid of +-1 pc, isotropic point source at the centre, 0.55 micron, HG g = 0.6,

@@ -1,0 +1,147 @@
+"""Generates the golden fixtures under tests/golden/ from the reference SKIRT 9 build.
+
+Runs only where the reference sources are present (it needs oracle/_ref, built by
+`make -f oracle/ref.mk`): the export harness (oracle/_ref/exe/skirt/bin/skirt_export) loads each
+ski file through the reference's own SimulationItem tree and dumps the flattened grid, medium and
+instrument state plus the path segments of the reference's CPU generators for a set of rays; the
+reference `skirt` program (single-threaded, so that its setup is reproducible) produces the image
+and SED statistics of the dust-shell run.
+
+    python tests/golden/make_fixtures.py
+
+Fixtures written:
+  paths_<name>.npz   grid + medium export, rays, reference (count, m, ds) per ray, reference tau
+  shell_c16.npz      export of the 16^3 dust-shell scene + reference SED/frame statistics of a
+                     2e5-packet run
+"""
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, os.path.join(ROOT, "skirt9-gpu_b200"))
+from skgpu import fits, ski  # noqa: E402
+
+BIN = os.path.join(ROOT, "oracle", "_ref", "exe", "skirt", "bin")
+OUT = os.path.dirname(os.path.abspath(__file__))
+PC = 3.08567758e16  # SKIRT's parsec in m
+
+
+def export(ski_text, tmp, rays=None, max_seg=512, lam=0.55e-6):
+    ski_path = os.path.join(tmp, "scene.ski")
+    with open(ski_path, "w") as f:
+        f.write(ski_text)
+    exp = os.path.join(tmp, "export")
+    os.makedirs(exp, exist_ok=True)
+    args = [os.path.join(BIN, "skirt_export"), ski_path, exp]
+    if rays is not None:
+        np.save(os.path.join(tmp, "rays.npy"), rays)
+        args += [os.path.join(tmp, "rays.npy"), str(max_seg), repr(lam)]
+    subprocess.run(args, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+    data = {}
+    for fn in os.listdir(exp):
+        if fn.endswith(".npy"):
+            data[fn[:-4]] = np.load(os.path.join(exp, fn))
+    with open(os.path.join(exp, "meta.txt")) as f:
+        data["meta"] = np.array(f.read())
+    return data
+
+
+def random_rays(rng, n, half, out_frac=0.3):
+    """Rays starting inside the box and (a fraction) outside it, isotropic directions, plus
+    rays along the axes and diagonals through the centre (exact ties with cell walls)."""
+    pos = rng.uniform(-half, half, (n, 3))
+    nout = int(out_frac * n)
+    pos[:nout] *= rng.uniform(1.05, 1.6, (nout, 1))
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    special = []
+    for k in ([1, 0, 0], [0, -1, 0], [0, 0, 1], [1, 1, 0], [1, 1, 1], [-1, 2, 0.5]):
+        k = np.array(k, float) / np.linalg.norm(k)
+        special.append(np.r_[0.0, 0.0, 0.0, k])
+        special.append(np.r_[0.1 * half, 0.0, -0.2 * half, k])
+    return np.vstack([np.hstack([pos, d]), np.array(special)])
+
+
+def path_fixture(name, ski_text, rays, max_seg=512):
+    with tempfile.TemporaryDirectory() as tmp:
+        data = export(ski_text, tmp, rays, max_seg)
+    data["rays"] = rays
+    # keep the segments ragged: ray r owns ray_m[off[r]:off[r+1]] (no truncated paths allowed)
+    cnt = data["ray_count"]
+    assert (cnt >= 0).all(), "a reference path was truncated; raise max_seg"
+    data["ray_offset"] = np.r_[0, np.cumsum(cnt)].astype(np.int64)
+    data["ray_m"] = np.concatenate([data["ray_m"][r, :c] for r, c in enumerate(cnt)]).astype(np.int32)
+    data["ray_ds"] = np.concatenate([data["ray_ds"][r, :c] for r, c in enumerate(cnt)])
+    np.savez_compressed(os.path.join(OUT, f"paths_{name}.npz"), **data)
+    print(f"paths_{name}: {len(rays)} rays, {np.abs(cnt).sum()} segments, max {np.abs(cnt).max()}")
+
+
+def main():
+    if not os.path.exists(os.path.join(BIN, "skirt_export")):
+        sys.exit("reference build missing: run `make -f oracle/ref.mk -j8` first")
+    rng = np.random.default_rng(20260101)
+
+    # Cartesian: the reference self-test grid (SKIRT/core/GpuAcceleration.cpp:12753-12755) with
+    # its rays (:12951-12953) and random rays, and the 16^3 shell grid
+    xb = np.array([-1.2, -0.5, 0.1, 0.7, 1.4, 2.0])
+    yb = np.array([-0.8, -0.2, 0.25, 0.9])
+    zb = np.array([-0.4, 0.0, 0.35, 0.8, 1.3])
+    norm = lambda b: (b - b[0]) / (b[-1] - b[0])
+    grid = (f'<CartesianSpatialGrid minX="{xb[0]} pc" maxX="{xb[-1]} pc" minY="{yb[0]} pc" maxY="{yb[-1]} pc" '
+            f'minZ="{zb[0]} pc" maxZ="{zb[-1]} pc">'
+            + "".join(f'<mesh{a} type="Mesh"><ListMesh points="' + ", ".join(f"{p:.17g}" for p in norm(b))
+                      + f'"/></mesh{a}>' for a, b in zip("XYZ", (xb, yb, zb)))
+            + '</CartesianSpatialGrid>')
+    st = []
+    for p, k in (((-2.1, -0.55, 0.2), (1.0, 0.26, 0.08)), ((0.1, -0.2, 0.0), (1.0, 1.0, 1.0))):
+        k = np.array(k) / np.linalg.norm(k)
+        st.append(np.r_[np.array(p) * PC, k])
+    rays = np.vstack([np.array(st), random_rays(rng, 300, 1.6 * PC)])
+    rays[2:, :3] += 0.4 * PC
+    path_fixture("cartesian_selftest", ski.disk_probe(grid), rays)
+    path_fixture("cartesian_c16", ski.shell_cartesian(1e4, nbins=16, npix=64), random_rays(rng, 300, PC))
+
+    # octree (DensityTreePolicy on a flattened exponential disk: many levels, uneven neighbours)
+    path_fixture("octree", ski.disk_probe(ski.octree_grid(4, "pc", 6, 1e-3)), random_rays(rng, 300, 4 * PC))
+    # Voronoi and tetrahedral meshes built by the reference (voro++ / TetGen) from disk-sampled sites
+    path_fixture("voronoi", ski.disk_probe(ski.voronoi_grid(4, "pc", 300)), random_rays(rng, 300, 4 * PC))
+    path_fixture("tetra", ski.disk_probe(ski.tetra_grid(4, "pc", 300)), random_rays(rng, 300, 4 * PC))
+
+    # dust shell, 16^3 grid, 64^2 frame + SED: scene export + reference statistics (2e5 packets)
+    npp = 200000
+    with tempfile.TemporaryDirectory() as tmp:
+        text = ski.shell_cartesian(npp, nbins=16, npix=64)
+        data = export(text, tmp)
+        run = os.path.join(tmp, "run")
+        os.makedirs(run)
+        with open(os.path.join(run, "c16.ski"), "w") as f:
+            f.write(text)
+        subprocess.run([os.path.join(BIN, "skirt"), "-t", "1", "c16.ski"], cwd=run, check=True,
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        sedstats = np.loadtxt(os.path.join(run, "c16_sed_sedstats.dat"))
+        sed = np.loadtxt(os.path.join(run, "c16_sed_sed.dat"))
+        stats = np.array([fits.read(os.path.join(run, f"c16_i30_stats{k}.fits"))[0][0] for k in range(5)])
+        total = fits.read(os.path.join(run, "c16_i30_total.fits"))[0][0]
+    # The stats files are scaled by c^k (FluxRecorder.cpp:1216-1236). Recover c from the
+    # transparent SED flux, whose raw value (total luminosity per packet summed) is known exactly:
+    # frame surface brightness per raw W = (SED Jy per raw W) * 1e-6 / pixel solid angle.
+    meta, load, _ = __import__("skgpu").Scene.read_export(data)
+    lum = load("src_probe")[0, 1]                     # L * npp of one packet = raw transparent SED sum
+    jy_per_w = sed[2] / lum
+    pix = float(meta["instr0_xpsiz"]) / float(meta["instr0_distance"])
+    mjysr_per_w = jy_per_w * 1e-6 / (pix * pix)
+    w1 = total / mjysr_per_w
+    c = stats[1].sum() / w1.sum()
+    data.update(ref_npp=npp, ref_sedstats=sedstats[1:], ref_sed_jy=sed[1:], ref_frame_w=np.array(
+        [stats[0], stats[1] / c, stats[2] / c ** 2]), ref_stats_scale=c, ref_jy_per_w=jy_per_w)
+    np.savez_compressed(os.path.join(OUT, "shell_c16.npz"), **data)
+    print("shell_c16: stats scale", c)
+
+
+if __name__ == "__main__":
+    main()
