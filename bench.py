@@ -79,7 +79,7 @@ class ClockSampler:
         sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
         mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 5 + i and "Active" in s[5 + i]})
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 5 + i and s[5 + i] == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons}
 
@@ -109,9 +109,15 @@ def reference_run(scene_ski, npp, threads):
         out = subprocess.run([REF_SKIRT, "-t", str(threads), "bench.ski"], cwd=tmp, capture_output=True, text=True)
         if out.returncode != 0:
             raise RuntimeError("reference run failed: " + out.stdout[-500:] + out.stderr[-500:])
-        m = re.search(r"Finished primary emission in ([0-9.]+) s", out.stdout)
-        secs = float(m.group(1))
-        return npp / secs, secs
+        # primary-emission segment from the log time stamps (millisecond resolution): from
+        # "Launching ... primary emission photon packets" to "Finished primary emission"
+        def stamp(pattern):
+            m = re.search(r"(\d\d):(\d\d):(\d\d\.\d+)[^\n]*" + pattern, out.stdout)
+            return 3600 * int(m.group(1)) + 60 * int(m.group(2)) + float(m.group(3))
+        secs = stamp(r"Finished primary emission") - stamp(r"Launching [^\n]* primary emission photon packets")
+        if secs < 0:
+            secs += 86400
+        return npp / max(secs, 1e-3), secs
 
 
 def reference_ski(name, npp):
@@ -184,6 +190,7 @@ def main():
     ap.add_argument("--workload", default="shell", choices=sorted(WORKLOADS))
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--packets", type=int, default=0, help="packets per step per GPU (default: the workload's)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -207,7 +214,7 @@ def main():
     torch.cuda.set_device(local)
     name = args.workload
     sc = build_scene(name)
-    per_gpu = WORKLOADS[name][1]
+    per_gpu = args.packets or WORKLOADS[name][1]
     npp_total = per_gpu * world
     first = rank * per_gpu
     prec = abi.PREC_FP64_EXACT if args.precision == "fp64" else abi.PREC_FP32
@@ -283,11 +290,11 @@ def main():
                        "parallelism": f"history ranges x{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "skg::lifecycleKernel", "algorithmic_bytes_per_launch": alg},
+                         "kernel": "skg::traceKernel", "algorithmic_bytes_per_launch": alg},
             "clocks": clk.summary(),
             "e2e": {"value": npp_total / e2e_s, "unit": "packets/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
-            "gpu_launches": args.steps,
+            "gpu_launches": int(counters["kernel_launches"]) * args.steps,
             "counters_per_step": counters,
         }
         if not args.no_cpu_baseline:

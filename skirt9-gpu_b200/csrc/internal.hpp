@@ -2,18 +2,18 @@
 #pragma once
 
 #include <cuda_runtime.h>
-#include "lifecycle.cuh"
+#include "wave_types.cuh"
 
 namespace skg {
 
-// life-cycle launchers, one per precision (separate translation units so the FP64 one can be
-// compiled without FMA contraction)
-cudaError_t launchLifecycleFP64(int gridKind, const LCParams& p, int blocks, int threads, cudaStream_t s);
-int lifecycleBlocksPerSMFP64(int gridKind, int threads);
-cudaError_t launchLifecycleFP32(int gridKind, const LCParams& p, int blocks, int threads, cudaStream_t s);
-int lifecycleBlocksPerSMFP32(int gridKind, int threads);
+// wavefront life cycle, one entry per traversal precision (separate translation units, so that
+// the FP64 one can be compiled without FMA contraction)
+cudaError_t runWaveFP64(int gridKind, const Wave& w, int numSMs, cudaStream_t s, unsigned long long* doneHost,
+                        long long* passes, long long maxPasses);
+cudaError_t runWaveFP32(int gridKind, const Wave& w, int numSMs, cudaStream_t s, unsigned long long* doneHost,
+                        long long* passes, long long maxPasses);
 
-// path-segment and optical-depth kernels (reference generators, FP64 exact or FP32)
+// path-segment and optical-depth kernels (reference generators, FP64)
 cudaError_t launchTracePaths(int precision, const GridDev& g, int n, const double* rays, int maxSeg, int* count,
                              int* m, double* ds, int* err, cudaStream_t s);
 cudaError_t launchOpticalDepths(int precision, const GridDev& g, const double* dens, double section, int n,

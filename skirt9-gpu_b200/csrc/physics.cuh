@@ -1,0 +1,300 @@
+// Device physics shared by the life-cycle stages: scene records, source launch, instrument
+// projection, wavelength bins, warp-aggregated FP64 atomics.
+#pragma once
+
+#include "grids.cuh"
+
+namespace skg {
+
+constexpr int MAX_INSTR = 16;
+constexpr int STATS_CAP = 48;
+constexpr int MAX_SCATT_EVENTS = 1 << 20;
+
+struct SourceDev
+{
+    int posModel, specModel;
+    double pos[3];
+    double geom[6];
+    unsigned long long first, num;
+    double Lpk;
+    double xi, bmin, bmax;
+    int toff, tsize, roff, rsize;
+};
+
+struct InstrDev
+{
+    int kind, same, stats, comps;
+    int npx, npy, nbins, woff, wnb;
+    double kobs[3];
+    double ct, st, cp, sp, co, so;
+    double xpmin, xpsiz, ypmin, ypsiz;
+    double* ifu;        // frame total, nbins*npix, index l + ell*npix
+    double* sed;        // SED total, nbins
+    double* ifuComp;    // 3 planes: transparent, direct, scattered
+    double* sedComp;
+    double* ifuStats;   // 5 planes: sum w^k, k = 0..4
+    double* sedStats;
+};
+
+// read-only scene data of a run
+struct Scene
+{
+    GridDev g;
+    const double* dens;
+    const double* mixLb;
+    const double* mixExt;
+    const double* mixSca;
+    const double* mixG;
+    int nmix;
+
+    int nsrc;
+    const SourceDev* src;
+    const double* tabL;
+    const double* tabA;
+    const double* tabB;
+    const double* radR;
+    const double* radP;
+
+    int ninstr;
+    const InstrDev* instr;
+    const double* wlgB;
+    const int* wlgEll;
+
+    int rfOn, nrf, rfNb;
+    const double* rfB;
+    const int* rfEll;
+    double* rf;
+
+    int forced, minScatt, peel;
+    double minWeightRed, pathLengthBias;
+    unsigned long long seed;
+};
+
+// atomicAdd after summing the contributions of the warp's active lanes that target the same address
+SKG_D void atomicAddAgg(double* addr, double v)
+{
+    unsigned active = __activemask();
+    unsigned peers = __match_any_sync(active, reinterpret_cast<unsigned long long>(addr));
+    int leader = __ffs(peers) - 1;
+    double sum = 0.;
+    unsigned rem = peers;
+    while (rem)
+    {
+        int j = __ffs(rem) - 1;
+        rem &= rem - 1;
+        sum += __shfl_sync(peers, v, j);
+    }
+    if ((threadIdx.x & 31) == leader) atomicAdd(addr, sum);
+}
+
+// DisjointWavelengthGrid::bin (DisjointWavelengthGrid.cpp:333-342)
+SKG_D int wlgBin(const double* borders, int nb, const int* ellv, double lambda)
+{
+    return ellv[upperBound(borders, nb, lambda)];
+}
+
+// SpecialFunctions::gexp(p, x) (SKIRT/utils/SpecialFunctions.cpp:822-836), the inverse of the
+// generalized logarithm used by Random::cdfLogLog (Random.cpp:200-207)
+SKG_D double gexp(double p, double x)
+{
+    const double q = 1.0 - p;
+    if (q == 0.0) return exp(x);
+    if (fabs(q) < 1e-3)
+    {
+        double x2 = x * x;
+        return exp(x)
+               * (1.0 - 0.5 * x2 * q + 1.0 / 24.0 * x * x2 * (8.0 + 3.0 * x) * q * q
+                  - 1.0 / 48.0 * x2 * x2 * (12.0 + 8.0 * x + x2) * q * q * q);
+    }
+    return pow(1.0 + q * x, 1.0 / q);
+}
+
+// Lambert W, branch -1, for x in [-1/e, 0): Halley iteration (Corless et al. 1996) from the
+// branch-point series or the asymptotic expansion
+SKG_D double lambertWm1(double x)
+{
+    if (x >= 0.) return -INFINITY;
+    if (x <= -1. / M_E) return -1.;
+    double w;
+    if (x < -0.25)
+    {
+        double pp = -sqrt(2. * (M_E * x + 1.));
+        w = -1. + pp - pp * pp / 3. + 11. / 72. * pp * pp * pp;
+    }
+    else
+    {
+        double l1 = log(-x), l2 = log(-l1);
+        w = l1 - l2 + l2 / l1;
+    }
+    for (int it = 0; it < 20; ++it)
+    {
+        double ew = exp(w);
+        double f = w * ew - x;
+        double wp1 = w + 1.;
+        if (wp1 == 0.) break;
+        double dw = f / (ew * wp1 - (w + 2.) * f / (2. * wp1));
+        w -= dw;
+        if (fabs(dw) <= 1e-15 * fabs(w)) break;
+    }
+    return w;
+}
+
+// launched packet state
+struct Launched
+{
+    double x, y, z, kx, ky, kz, L, lambda;
+};
+
+// SourceSystem::launch -> NormalizedSource::launch -> PointSource / GeometricSource
+// (SourceSystem.cpp, NormalizedSource.cpp:73-110, SepAxGeometry.cpp:11-19, SpheGeometry.cpp:25-32,
+// ExpDiskGeometry.cpp:46-69, LogWavelengthDistribution.cpp:31-34, Random.cpp:121-207)
+SKG_D Launched launchPacket(const Scene& p, unsigned long long hist, Rng& rng)
+{
+    int h = 0;
+    for (int q = 1; q < p.nsrc; ++q)
+        if (p.src[q].first <= hist) h = q;
+    const SourceDev& S = p.src[h];
+    Launched o;
+    double L = S.Lpk;
+    double lambda;
+    if (S.specModel == 0)
+    {
+        int j = min(S.tsize - 1, static_cast<int>(rng.uniform() * S.tsize));
+        lambda = p.tabL[S.toff + j];
+        L *= p.tabA[S.toff + j];
+    }
+    else
+    {
+        const double* lv = p.tabL + S.toff;
+        const double* pv = p.tabA + S.toff;
+        const double* Pv = p.tabB + S.toff;
+        int n = S.tsize;
+        double xi = S.xi;
+        bool fromSed = (xi <= 0.) || (rng.uniform() > xi);
+        if (fromSed)
+        {
+            double X = rng.uniform();
+            int i = locateClip(Pv, n, X);
+            double alpha = log(pv[i + 1] / pv[i]) / log(lv[i + 1] / lv[i]);
+            lambda = lv[i] * gexp(-alpha, (X - Pv[i]) / (pv[i] * lv[i]));
+        }
+        else
+        {
+            double lmin = log(S.bmin), lw = log(S.bmax) - log(S.bmin);
+            lambda = exp(lmin + lw * rng.uniform());
+        }
+        if (xi > 0.)
+        {
+            double s = 0.;
+            if (lambda >= lv[0] && lambda <= lv[n - 1])
+            {
+                int i = min(n - 2, max(0, upperBound(lv, n, lambda) - 1));
+                double a = log(pv[i + 1] / pv[i]) / log(lv[i + 1] / lv[i]);
+                s = pv[i] * pow(lambda / lv[i], a);
+            }
+            double b = (lambda >= S.bmin && lambda <= S.bmax) ? 1. / ((log(S.bmax) - log(S.bmin)) * lambda) : 0.;
+            L *= (s > 0.) ? s / ((1 - xi) * s + xi * b) : 0.;
+        }
+    }
+    o.lambda = lambda;
+    o.L = L;
+    if (S.posModel == 0)
+    {
+        o.x = S.pos[0]; o.y = S.pos[1]; o.z = S.pos[2];
+    }
+    else if (S.posModel == 1)
+    {
+        double hR = S.geom[0], hz = S.geom[1], Rmin = S.geom[2], Rmax = S.geom[3], zmax = S.geom[4];
+        double R = 0.;
+        for (int t = 0; t < 1000; ++t)
+        {
+            double X = rng.uniform();
+            R = hR * (-1.0 - lambertWm1((X - 1.0) / M_E));
+            if (!((Rmax > 0.0 && R >= Rmax) || R <= Rmin)) break;
+        }
+        double phi = 2.0 * M_PI * rng.uniform();
+        double z = 0.;
+        for (int t = 0; t < 1000; ++t)
+        {
+            double X = rng.uniform();
+            z = (X <= 0.5) ? hz * log(2.0 * X) : -hz * log(2.0 * (1.0 - X));
+            if (!(zmax > 0.0 && fabs(z) >= zmax)) break;
+        }
+        o.x = S.pos[0] + R * cos(phi);
+        o.y = S.pos[1] + R * sin(phi);
+        o.z = S.pos[2] + z;
+    }
+    else
+    {
+        double X = rng.uniform();
+        const double* rv = p.radR + S.roff;
+        const double* Pv = p.radP + S.roff;
+        int i = locateClip(Pv, S.rsize, X);
+        double r = rv[i] + (X - Pv[i]) / (Pv[i + 1] - Pv[i]) * (rv[i + 1] - rv[i]);
+        double ux, uy, uz;
+        isotropicDirection(rng, ux, uy, uz);
+        o.x = S.pos[0] + r * ux;
+        o.y = S.pos[1] + r * uy;
+        o.z = S.pos[2] + r * uz;
+    }
+    isotropicDirection(rng, o.kx, o.ky, o.kz);
+    return o;
+}
+
+// FrameInstrument::pixelOnDetector (FrameInstrument.cpp:117-136)
+SKG_D int framePixel(const InstrDev& in, double x, double y, double z)
+{
+    double xpp = -in.sp * x + in.cp * y;
+    double ypp = -in.cp * in.ct * x - in.sp * in.ct * y + in.st * z;
+    double xp = in.co * xpp - in.so * ypp;
+    double yp = in.so * xpp + in.co * ypp;
+    int i = static_cast<int>(floor((xp - in.xpmin) / in.xpsiz));
+    int j = static_cast<int>(floor((yp - in.ypmin) / in.ypsiz));
+    if (i < 0 || i >= in.npx || j < 0 || j >= in.npy) return -1;
+    return i + in.npx * j;
+}
+
+// does any instrument of the observer group starting at i0 record a packet at (x,y,z)?
+SKG_D bool groupNeedsTau(const Scene& p, int i0, double x, double y, double z)
+{
+    for (int i = i0; i < p.ninstr && (i == i0 || p.instr[i].same); ++i)
+    {
+        const InstrDev& in = p.instr[i];
+        if (in.kind == 1) return true;
+        if (framePixel(in, x, y, z) >= 0) return true;
+    }
+    return false;
+}
+
+SKG_D int nextGroup(const Scene& p, int i0)
+{
+    int j = i0 + 1;
+    while (j < p.ninstr && p.instr[j].same) ++j;
+    return j;
+}
+
+// the albedo of the interaction cell (MediumSystem::albedoForScattering, MediumSystem.cpp:793-837)
+SKG_D double albedoAt(const Scene& p, int m, double ssca, double sext)
+{
+    double n = p.dens[m];
+    double ksca = n > 0. ? n * ssca : 0.;
+    double kext = n > 0. ? n * sext : 0.;
+    return kext > 0. ? ksca / kext : 0.;
+}
+
+// HG scattering (DustMix::performScattering, DustMix.cpp:490-546)
+SKG_D void scatterHG(Rng& rng, double g, double& kx, double& ky, double& kz)
+{
+    if (fabs(g) < 1e-6)
+    {
+        isotropicDirection(rng, kx, ky, kz);
+    }
+    else
+    {
+        double f = ((1.0 - g) * (1.0 + g)) / (1.0 - g + 2.0 * g * rng.uniform());
+        double costheta = (1.0 + g * g - f * f) / (2.0 * g);
+        rotateDirection(rng, costheta, kx, ky, kz);
+    }
+}
+
+}  // namespace skg

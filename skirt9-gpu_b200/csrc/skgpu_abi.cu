@@ -65,10 +65,15 @@ struct skgpu_ctx
     skgpu_options opt{};
     bool hasOptions = false;
 
-    unsigned long long* work = nullptr;
-    unsigned long long* counters = nullptr;
     int* errFlag = nullptr;
     skgpu_counters lastCounters{};
+    long long lastPasses = 0;
+
+    // wavefront buffers (packet pool, task queues, control block), grown on demand
+    Wave wave{};
+    int waveP = 0, waveGroups = 0, waveStats = 0;
+    std::vector<void*> waveBufs;
+    unsigned long long* doneHost = nullptr;  // pinned progress word
 };
 
 namespace {
@@ -146,6 +151,82 @@ bool finiteAll(const double* v, size_t n)
     return true;
 }
 
+// histories in flight at most; a larger range streams through the pool
+constexpr uint64_t POOL_MAX = 1u << 20;
+// wavefront passes per run at most (each history needs about two passes per scattering event)
+constexpr long long MAX_PASSES = 2LL * MAX_SCATT_EVENTS + 64;
+
+void freeWave(skgpu_ctx* ctx)
+{
+    for (void* p : ctx->waveBufs) cudaFree(p);
+    ctx->waveBufs.clear();
+    ctx->wave = Wave{};
+    ctx->waveP = ctx->waveGroups = ctx->waveStats = 0;
+}
+
+template<typename T>
+int waveAlloc(skgpu_ctx* ctx, T** p, size_t n)
+{
+    CK(devAlloc(p, n));
+    ctx->waveBufs.push_back(*p);
+    return SKGPU_OK;
+}
+
+// packet pool of P slots (SoA), task buffers (peel: P per observer group; propagation: P per
+// kind), two parities each, and the control block
+int ensureWaveBuffers(skgpu_ctx* ctx, int P, int groups, int stats)
+{
+    if (ctx->waveP >= P && ctx->waveGroups >= groups && ctx->waveStats >= stats) return SKGPU_OK;
+    P = std::max(P, ctx->waveP);
+    groups = std::max(groups, ctx->waveGroups);
+    stats = std::max(stats, ctx->waveStats);
+    freeWave(ctx);
+    Wave& w = ctx->wave;
+    PacketPool& k = w.pk;
+    int rc = 0;
+    double** dbl[] = {&k.x, &k.y, &k.z, &k.kx, &k.ky, &k.kz, &k.L, &k.Lth, &k.lam, &k.tauPath, &k.rngSpare};
+    for (double** d : dbl)
+        if ((rc = waveAlloc(ctx, d, P))) return rc;
+    int** ints[] = {&k.rngHas, &k.nscatt, &k.ellMix, &k.ellRF, &k.nstat, &k.freeSlots};
+    for (int** d : ints)
+        if ((rc = waveAlloc(ctx, d, P))) return rc;
+    if ((rc = waveAlloc(ctx, &k.hist, P))) return rc;
+    if ((rc = waveAlloc(ctx, &k.rngCtr, P))) return rc;
+    size_t ns = stats ? static_cast<size_t>(P) * STATS_CAP : 1;
+    if ((rc = waveAlloc(ctx, &k.skey, ns))) return rc;
+    if ((rc = waveAlloc(ctx, &k.sw, ns))) return rc;
+    for (int b = 0; b < 2; ++b)
+        for (int kind = 0; kind < NUM_KINDS; ++kind)
+        {
+            TaskBuf& t = w.q[b][kind];
+            size_t cap = kind == K_PEEL ? static_cast<size_t>(P) * groups : static_cast<size_t>(P);
+            if ((rc = waveAlloc(ctx, &t.slot, cap))) return rc;
+            if ((rc = waveAlloc(ctx, &t.par, cap))) return rc;
+            if (kind == K_PEEL)
+            {
+                if ((rc = waveAlloc(ctx, &t.info, cap))) return rc;
+                if ((rc = waveAlloc(ctx, &t.x, cap))) return rc;
+                if ((rc = waveAlloc(ctx, &t.y, cap))) return rc;
+                if ((rc = waveAlloc(ctx, &t.z, cap))) return rc;
+            }
+            if (kind == K_PEEL || kind == K_PROP1)
+            {
+                if ((rc = waveAlloc(ctx, &t.tau, cap))) return rc;
+            }
+            else
+            {
+                if ((rc = waveAlloc(ctx, &t.m, cap))) return rc;
+                if ((rc = waveAlloc(ctx, &t.s, cap))) return rc;
+                if ((rc = waveAlloc(ctx, &t.found, cap))) return rc;
+            }
+        }
+    if ((rc = waveAlloc(ctx, &w.ctl, 1))) return rc;
+    ctx->waveP = P;
+    ctx->waveGroups = groups;
+    ctx->waveStats = stats;
+    return SKGPU_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -163,9 +244,8 @@ int skgpu_create(int device, skgpu_ctx** out)
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev1);
-    if (e == cudaSuccess) e = devAlloc(&ctx->work, 1);
-    if (e == cudaSuccess) e = devAlloc(&ctx->counters, 8);
     if (e == cudaSuccess) e = devAlloc(&ctx->errFlag, 1);
+    if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&ctx->doneHost), sizeof(unsigned long long));
     if (e != cudaSuccess)
     {
         // keep the context so the caller can read the message; the handle must still be destroyed
@@ -201,9 +281,9 @@ void skgpu_destroy(skgpu_ctx* ctx)
     devFree(ctx->tabB);
     devFree(ctx->radR);
     devFree(ctx->radP);
-    devFree(ctx->work);
-    devFree(ctx->counters);
+    freeWave(ctx);
     devFree(ctx->errFlag);
+    if (ctx->doneHost) cudaFreeHost(ctx->doneHost);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -636,7 +716,7 @@ int skgpu_run_primary(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t t
             ctx->rfLen = len;
         }
     }
-    LCParams p{};
+    Scene p{};
     p.g = ctx->g;
     p.dens = ctx->dens;
     p.mixLb = ctx->mixLb; p.mixExt = ctx->mixExt; p.mixSca = ctx->mixSca; p.mixG = ctx->mixG; p.nmix = ctx->nmix;
@@ -654,44 +734,47 @@ int skgpu_run_primary(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t t
     p.minWeightRed = ctx->opt.min_weight_reduction;
     p.pathLengthBias = ctx->opt.path_length_bias;
     p.seed = ctx->opt.seed;
-    p.first = first;
-    p.count = count;
-    p.npp = total_packets;
-    p.workCounter = ctx->work;
-    p.counters = ctx->counters;
-    p.errFlag = ctx->errFlag;
-    CK(cudaMemsetAsync(ctx->work, 0, sizeof(unsigned long long), ctx->stream));
-    CK(cudaMemsetAsync(ctx->counters, 0, 8 * sizeof(unsigned long long), ctx->stream));
-    CK(cudaMemsetAsync(ctx->errFlag, 0, sizeof(int), ctx->stream));
-    const int threads = 256;
+
+    // packet pool and task queues, sized for up to POOL_MAX histories in flight
+    int anyStats = 0;
+    for (const InstrDev& d : ctx->instrHost) anyStats |= d.stats;
+    int groups = 0;
+    for (const InstrDev& d : ctx->instrHost) groups += d.same ? 0 : 1;
+    int P = static_cast<int>(std::min<uint64_t>(std::max<uint64_t>(count, 1), POOL_MAX));
+    int rc = ensureWaveBuffers(ctx, P, std::max(groups, 1), anyStats);
+    if (rc) return rc;
+    Wave w = ctx->wave;
+    w.sc = p;
+    w.P = P;
+    w.first = first;
+    w.count = count;
+    w.anyStats = anyStats;
     int prec = ctx->opt.precision;
-    int perSM = prec == SKGPU_PREC_FP64_EXACT ? lifecycleBlocksPerSMFP64(ctx->g.kind, threads)
-                                              : lifecycleBlocksPerSMFP32(ctx->g.kind, threads);
-    long long want = (static_cast<long long>(count) + threads - 1) / threads;
-    int blocks = static_cast<int>(std::max(1LL, std::min(want, static_cast<long long>(perSM) * ctx->numSMs)));
+    long long passes = 0;
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
-    if (count > 0)
-    {
-        cudaError_t e = prec == SKGPU_PREC_FP64_EXACT ? launchLifecycleFP64(ctx->g.kind, p, blocks, threads, ctx->stream)
-                                                      : launchLifecycleFP32(ctx->g.kind, p, blocks, threads, ctx->stream);
-        if (e != cudaSuccess) return fail(ctx, SKGPU_ERR_CUDA, std::string("life-cycle launch: ") + cudaGetErrorString(e));
-    }
+    cudaError_t e = prec == SKGPU_PREC_FP64_EXACT
+                        ? runWaveFP64(ctx->g.kind, w, ctx->numSMs, ctx->stream, ctx->doneHost, &passes, MAX_PASSES)
+                        : runWaveFP32(ctx->g.kind, w, ctx->numSMs, ctx->stream, ctx->doneHost, &passes, MAX_PASSES);
+    if (e == cudaErrorNotSupported) return fail(ctx, SKGPU_ERR_UNSUPPORTED, "run: no FP32 walker for this grid kind");
+    if (e == cudaErrorLaunchTimeout) return fail(ctx, SKGPU_ERR_TIMEOUT, "run: pass limit reached before all histories finished");
+    if (e != cudaSuccess) return fail(ctx, SKGPU_ERR_CUDA, std::string("run: ") + cudaGetErrorString(e));
     CK(cudaEventRecord(ctx->ev1, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
     ctx->lastMs = ms;
-    unsigned long long cnt[8];
-    int errFlag = 0;
-    CK(cudaMemcpy(cnt, ctx->counters, sizeof cnt, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(&errFlag, ctx->errFlag, sizeof errFlag, cudaMemcpyDeviceToHost));
-    ctx->lastCounters.histories = cnt[0];
-    ctx->lastCounters.crossings = cnt[1];
-    ctx->lastCounters.scatterings = cnt[2];
-    ctx->lastCounters.peel_detections = cnt[3];
-    ctx->lastCounters.rf_stores = cnt[4];
-    ctx->lastCounters.stats_overflows = cnt[5];
-    ctx->lastCounters.kernel_launches = count > 0 ? 1 : 0;
+    Control ctl;
+    CK(cudaMemcpy(&ctl, ctx->wave.ctl, sizeof ctl, cudaMemcpyDeviceToHost));
+    int errFlag = ctl.err;
+    ctx->lastCounters.histories = ctl.counters[0];
+    ctx->lastCounters.crossings = ctl.counters[1];
+    ctx->lastCounters.scatterings = ctl.counters[2];
+    ctx->lastCounters.peel_detections = ctl.counters[3];
+    ctx->lastCounters.rf_stores = ctl.counters[4];
+    ctx->lastCounters.stats_overflows = ctl.counters[5];
+    ctx->lastCounters.kernel_launches = static_cast<uint64_t>(passes) * 7 + 1;
+    ctx->lastPasses = passes;
+    if (count > 0 && ctl.done != count) return fail(ctx, SKGPU_ERR_DEVICE, "run: not every history finished");
     if (errFlag & 4) return fail(ctx, SKGPU_ERR_TIMEOUT, "run: a traversal exceeded its segment guard");
     if (errFlag & 8) return fail(ctx, SKGPU_ERR_TIMEOUT, "run: a history exceeded the scattering-event guard");
     if (errFlag) return fail(ctx, SKGPU_ERR_DEVICE, "run: interaction point outside the grid (device check)");

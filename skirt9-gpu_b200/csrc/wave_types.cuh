@@ -1,0 +1,66 @@
+// Data layout of the wavefront life cycle: the packet pool (structure of arrays), the task
+// buffers of the four traversal kinds, and the control block of counters.
+#pragma once
+
+#include "physics.cuh"
+
+namespace skg {
+
+enum TaskKind { K_PEEL = 0, K_PROP1 = 1, K_PROP2 = 2, K_FREE = 3, NUM_KINDS = 4 };
+
+struct PacketPool
+{
+    double *x, *y, *z, *kx, *ky, *kz;
+    double *L, *Lth, *lam, *tauPath;
+    unsigned long long* hist;
+    unsigned* rngCtr;
+    double* rngSpare;
+    int* rngHas;
+    int *nscatt, *ellMix, *ellRF;
+    // per-history statistics buffer (only when an instrument records statistics)
+    unsigned long long* skey;  // P * STATS_CAP
+    double* sw;
+    int* nstat;
+    int* freeSlots;            // P
+};
+
+// one buffer of one task kind
+struct TaskBuf
+{
+    int* slot;
+    int* info;      // PEEL: first instrument of the observer group | numScatt << 8
+    double* par;    // PEEL: peel-off luminosity; PROP2/FREE: interaction optical depth
+    double *x, *y, *z;  // PEEL: origin (the packet position at the event)
+    // results written by the trace kernel
+    double* tau;    // PEEL / PROP1: optical depth (PROP1: of the complete path)
+    int* m;         // PROP2 / FREE: interaction cell (-1: none)
+    double* s;      // PROP2 / FREE: interaction distance
+    int* found;     // FREE: interaction point inside the path
+};
+
+struct Control
+{
+    unsigned qn[2][NUM_KINDS];  // task counts per buffer and kind
+    unsigned traceCursor;
+    int freeTop;
+    int nLaunch;
+    int launchBase;
+    unsigned long long launched;
+    unsigned long long done;
+    unsigned long long launchHist0;
+    unsigned long long counters[8];  // histories, crossings, scatterings, detections, rfStores, overflows
+    int err;
+};
+
+struct Wave
+{
+    Scene sc;
+    PacketPool pk;
+    TaskBuf q[2][NUM_KINDS];
+    Control* ctl;
+    int P;
+    unsigned long long first, count;
+    int anyStats;
+};
+
+}  // namespace skg

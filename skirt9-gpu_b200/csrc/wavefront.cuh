@@ -1,0 +1,609 @@
+// Wavefront form of the photon-packet life cycle (MonteCarloSimulation::performLifeCycle,
+// SKIRT/core/MonteCarloSimulation.cpp:614-694).
+//
+// Packet state lives in a structure-of-arrays pool of P slots. Every traversal of the life cycle
+// is a task in one of four queues:
+//   PEEL   optical depth from a packet position to the domain edge towards one observer
+//          (FluxRecorder::detect -> MediumSystem::getExtinctionOpticalDepth, MediumSystem.cpp:2328-2443)
+//   PROP1  forced scattering, complete path: cumulative optical depth + radiation-field storage
+//          (MediumSystem::setExtinctionOpticalDepths :1785-1846, MonteCarloSimulation::storeRadiationField :888-957)
+//   PROP2  forced scattering, interaction point of the sampled optical depth
+//          (MonteCarloSimulation::simulateForcedPropagation :1492-1546, SpatialGridPath::findInteractionPoint :161-203)
+//   FREE   non-forced propagation (simulateNonForcedPropagation :1996-2030,
+//          MediumSystem::setInteractionPointUsingExtinction :2005-2150)
+// One pass of the wavefront runs:
+//   trace    a persistent kernel: each lane takes a task, walks its ray to the end (one cell
+//            crossing per loop iteration, so the warp's lanes stay converged on the crossing code)
+//            and takes the next task index with a warp-aggregated atomic; no other work;
+//   shade    one coherent kernel per task kind: detection (peel-off tallies), forced sampling,
+//            interaction + scattering peel-off emission + HG scattering, free-path interaction;
+//            each emits the packet's next tasks into the other queue buffer;
+//   launch   refills free slots with new histories (SourceSystem::launch) and emits their
+//            emission peel-offs and first propagation.
+// Random numbers: each history draws from its own Philox stream in the reference's order
+// (launch, forced sampling, scattering), whatever pass the draws happen in.
+#pragma once
+
+#include "wave_types.cuh"
+
+namespace skg {
+
+// ---------------------------------------------------------------------------------------------
+// helpers
+// ---------------------------------------------------------------------------------------------
+
+// warp-aggregated append: one atomic per group of converged lanes
+SKG_D unsigned warpAppend(unsigned* counter)
+{
+    unsigned active = __activemask();
+    int lane = threadIdx.x & 31;
+    int leader = __ffs(active) - 1;
+    unsigned base = 0;
+    if (lane == leader) base = atomicAdd(counter, static_cast<unsigned>(__popc(active)));
+    base = __shfl_sync(active, base, leader);
+    return base + __popc(active & ((1u << lane) - 1));
+}
+
+SKG_D void loadRng(const Wave& w, int slot, Rng& r)
+{
+    r.start(w.sc.seed, w.pk.hist[slot]);
+    r.ctr = w.pk.rngCtr[slot];
+    r.hasSpare = w.pk.rngHas[slot];
+    r.spare = w.pk.rngSpare[slot];
+}
+
+SKG_D void storeRng(const Wave& w, int slot, const Rng& r)
+{
+    w.pk.rngCtr[slot] = r.ctr;
+    w.pk.rngHas[slot] = r.hasSpare;
+    w.pk.rngSpare[slot] = r.spare;
+}
+
+SKG_D void addMoments(double* base, size_t plane, size_t idx, double wsum)
+{
+    double wn = 1.;
+    for (int k = 0; k <= 4; ++k)
+    {
+        atomicAdd(base + k * plane + idx, wn);
+        wn *= wsum;
+    }
+}
+
+SKG_D void statMoments(const Scene& sc, unsigned long long key, double wsum)
+{
+    int i = static_cast<int>(key >> 48);
+    int ell = static_cast<int>((key >> 24) & 0xFFFFFF);
+    int l = static_cast<int>(key & 0xFFFFFF) - 1;
+    const InstrDev& in = sc.instr[i];
+    if (l < 0)
+        addMoments(in.sedStats, in.nbins, ell, wsum);
+    else
+    {
+        size_t npix = static_cast<size_t>(in.npx) * in.npy;
+        addMoments(in.ifuStats, npix * in.nbins, static_cast<size_t>(l) + static_cast<size_t>(ell) * npix, wsum);
+    }
+}
+
+// FluxRecorder::recordContributions (FluxRecorder.cpp:1355-1409): group the history's
+// contributions per (instrument, wavelength bin, pixel) and add w^0..w^4
+SKG_D void flushStats(const Wave& w, int slot)
+{
+    int n = min(w.pk.nstat[slot], STATS_CAP);
+    unsigned long long* key = w.pk.skey + static_cast<size_t>(slot) * STATS_CAP;
+    double* sw = w.pk.sw + static_cast<size_t>(slot) * STATS_CAP;
+    for (int a = 0; a < n; ++a)
+    {
+        unsigned long long ka = key[a];
+        if (ka == ~0ULL) continue;
+        double wsum = sw[a];
+        for (int b = a + 1; b < n; ++b)
+        {
+            if (key[b] == ka)
+            {
+                wsum += sw[b];
+                key[b] = ~0ULL;
+            }
+        }
+        statMoments(w.sc, ka, wsum);
+    }
+    w.pk.nstat[slot] = 0;
+}
+
+SKG_D void endHistory(const Wave& w, int slot)
+{
+    if (w.anyStats && w.pk.nstat[slot]) flushStats(w, slot);
+    int i = atomicAdd(&w.ctl->freeTop, 1);
+    w.pk.freeSlots[i] = slot;
+    atomicAdd(&w.ctl->done, 1ULL);
+}
+
+SKG_D void emitPeel(const Wave& w, int nxt, int slot, int group, int numScatt, double Lp, double x, double y,
+                    double z)
+{
+    const TaskBuf& b = w.q[nxt][K_PEEL];
+    unsigned i = warpAppend(&w.ctl->qn[nxt][K_PEEL]);
+    b.slot[i] = slot;
+    b.info[i] = group | (min(numScatt, (1 << 22)) << 8);
+    b.par[i] = Lp;
+    b.x[i] = x;
+    b.y[i] = y;
+    b.z[i] = z;
+}
+
+SKG_D void emitProp(const Wave& w, int nxt, int kind, int slot, double par)
+{
+    const TaskBuf& b = w.q[nxt][kind];
+    unsigned i = warpAppend(&w.ctl->qn[nxt][kind]);
+    b.slot[i] = slot;
+    b.par[i] = par;
+}
+
+// peel-off tasks for every observer group that records the packet at (x,y,z);
+// scattering peel-offs carry L * phase function (DustMix::peeloffScattering, DustMix.cpp:430-488)
+SKG_D void emitPeels(const Wave& w, int nxt, int slot, bool scattering, int numScatt, double L, double g, double x,
+                     double y, double z, double kx, double ky, double kz)
+{
+    const Scene& sc = w.sc;
+    for (int i = 0; i < sc.ninstr; i = nextGroup(sc, i))
+    {
+        if (!groupNeedsTau(sc, i, x, y, z)) continue;
+        const InstrDev& in = sc.instr[i];
+        double Lp = L;
+        if (scattering) Lp = L * phaseHG(g, kx * in.kobs[0] + ky * in.kobs[1] + kz * in.kobs[2]);
+        emitPeel(w, nxt, slot, i, numScatt, Lp, x, y, z);
+    }
+}
+
+// emits the first traversal of a propagation (forced: PROP1; free: FREE with its sampled tau)
+SKG_D void beginPropagation(const Wave& w, int nxt, int slot, Rng& rng)
+{
+    if (w.sc.forced)
+        emitProp(w, nxt, K_PROP1, slot, 0.);
+    else
+        emitProp(w, nxt, K_FREE, slot, -log(rng.uniform()));  // Random::expon
+}
+
+// ---------------------------------------------------------------------------------------------
+// trace: walk every queued ray; one crossing per iteration, lanes refill from the queues
+// ---------------------------------------------------------------------------------------------
+template<class Walker>
+__global__ void __launch_bounds__(256) traceKernel(Wave w, int cur)
+{
+    const Scene& sc = w.sc;
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    unsigned n0 = w.ctl->qn[cur][0], n1 = w.ctl->qn[cur][1], n2 = w.ctl->qn[cur][2], n3 = w.ctl->qn[cur][3];
+    unsigned total = n0 + n1 + n2 + n3;
+    if (total == 0) return;
+
+    Walker wk;
+    int kind = -1;  // -1: needs a task, -2: finished
+    unsigned idx = 0;
+    int slot = 0;
+    double tau = 0., s = 0., par = 0., lnExtBeg = 0., extBeg = 1., L = 0., sext = 0.;
+    int nseg = 0, lastM = -1, ellRF = -1;
+    double lastS = 0.;
+    unsigned long long cross = 0, rfStores = 0;
+    int guard = 0;
+
+    while (true)
+    {
+        unsigned need = __ballot_sync(FULL, kind == -1);
+        if (need)
+        {
+            int leader = __ffs(need) - 1;
+            unsigned base = 0;
+            if (lane == leader) base = atomicAdd(&w.ctl->traceCursor, static_cast<unsigned>(__popc(need)));
+            base = __shfl_sync(FULL, base, leader);
+            if (kind == -1)
+            {
+                unsigned t = base + __popc(need & ((1u << lane) - 1));
+                if (t >= total)
+                {
+                    kind = -2;
+                }
+                else
+                {
+                    if (t < n0) { kind = K_PEEL; idx = t; }
+                    else if (t < n0 + n1) { kind = K_PROP1; idx = t - n0; }
+                    else if (t < n0 + n1 + n2) { kind = K_PROP2; idx = t - n0 - n1; }
+                    else { kind = K_FREE; idx = t - n0 - n1 - n2; }
+                    const TaskBuf& b = w.q[cur][kind];
+                    slot = b.slot[idx];
+                    sext = sc.mixExt[w.pk.ellMix[slot]];
+                    tau = 0.;
+                    s = 0.;
+                    nseg = 0;
+                    lastM = -1;
+                    lastS = 0.;
+                    guard = 0;
+                    if (kind == K_PEEL)
+                    {
+                        const InstrDev& in = sc.instr[b.info[idx] & 0xFF];
+                        par = log(b.par[idx]) + 745.;  // taumax = log(L) + 745
+                        wk.start(sc.g, b.x[idx], b.y[idx], b.z[idx], in.kobs[0], in.kobs[1], in.kobs[2]);
+                    }
+                    else
+                    {
+                        par = b.par[idx];
+                        wk.start(sc.g, w.pk.x[slot], w.pk.y[slot], w.pk.z[slot], w.pk.kx[slot], w.pk.ky[slot],
+                                 w.pk.kz[slot]);
+                        if (kind == K_PROP1)
+                        {
+                            L = w.pk.L[slot];
+                            ellRF = sc.rfOn ? w.pk.ellRF[slot] : -1;
+                            lnExtBeg = 0.;
+                            extBeg = 1.;
+                        }
+                    }
+                }
+            }
+        }
+        if (__all_sync(FULL, kind == -2)) break;
+        if (kind < 0) continue;
+
+        bool got = wk.next(sc.g);
+        bool done = !got;
+        if (got)
+        {
+            cross++;
+            int m = wk.m;
+            double ds = wk.ds;
+            if (kind == K_PEEL)
+            {
+                if (m >= 0)
+                {
+                    tau = xadd(tau, xmul(xmul(sext, sc.dens[m]), ds));
+                    if (tau >= par)
+                    {
+                        tau = INFINITY;
+                        done = true;
+                    }
+                }
+            }
+            else if (kind == K_PROP1)
+            {
+                if (ds > 0.)
+                {
+                    if (m >= 0) tau = xadd(tau, xmul(xmul(sext, sc.dens[m]), ds));
+                    nseg++;
+                    if (ellRF >= 0)
+                    {
+                        double lnExtEnd = -tau;
+                        double extEnd = exp(lnExtEnd);
+                        if (m >= 0)
+                        {
+                            double Lds = L * lnmean4(extEnd, extBeg, lnExtEnd, lnExtBeg) * ds;
+                            atomicAdd(sc.rf + static_cast<size_t>(m) * sc.nrf + ellRF, Lds);
+                            rfStores++;
+                        }
+                        lnExtBeg = lnExtEnd;
+                        extBeg = extEnd;
+                    }
+                }
+            }
+            else
+            {
+                // PROP2 keeps segments with ds > 0 (SpatialGridPath::addSegment); FREE uses every segment
+                if (kind == K_FREE || ds > 0.)
+                {
+                    double tau0 = tau, s0 = s;
+                    if (m >= 0) tau = xadd(tau, xmul(xmul(sext, sc.dens[m]), ds));
+                    s = xadd(s, ds);
+                    lastM = m;
+                    lastS = s;
+                    if (par < tau)
+                    {
+                        // NR::interpolateLinLin (SKIRT/utils/NR.hpp:328-331)
+                        const TaskBuf& b = w.q[cur][kind];
+                        b.m[idx] = m;
+                        b.s[idx] = s0 + ((par - tau0) / (tau - tau0)) * (s - s0);
+                        b.found[idx] = 1;
+                        kind = -1;
+                        continue;
+                    }
+                }
+            }
+            if (++guard > (1 << 22))
+            {
+                atomicOr(&w.ctl->err, 4);
+                done = true;
+            }
+        }
+        if (done)
+        {
+            const TaskBuf& b = w.q[cur][kind];
+            if (kind == K_PEEL)
+                b.tau[idx] = tau;
+            else if (kind == K_PROP1)
+                b.tau[idx] = nseg ? tau : 0.;
+            else
+            {
+                // beyond the last segment: PROP2 uses the last segment, FREE escapes
+                b.m[idx] = lastM;
+                b.s[idx] = lastS;
+                b.found[idx] = 0;
+            }
+            kind = -1;
+        }
+    }
+
+    for (int off = 16; off > 0; off >>= 1)
+    {
+        cross += __shfl_down_sync(FULL, cross, off);
+        rfStores += __shfl_down_sync(FULL, rfStores, off);
+    }
+    if (lane == 0)
+    {
+        if (cross) atomicAdd(&w.ctl->counters[1], cross);
+        if (rfStores) atomicAdd(&w.ctl->counters[4], rfStores);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// shade kernels (one thread per completed task of one kind)
+// ---------------------------------------------------------------------------------------------
+
+// FluxRecorder::detect for the instruments of one observer group (FluxRecorder.cpp:372-538)
+static __global__ void __launch_bounds__(256) shadePeelKernel(Wave w, int cur)
+{
+    const Scene& sc = w.sc;
+    unsigned n = w.ctl->qn[cur][K_PEEL];
+    const TaskBuf& b = w.q[cur][K_PEEL];
+    unsigned long long det = 0, ovf = 0;
+    for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+    {
+        int slot = b.slot[t];
+        int group = b.info[t] & 0xFF;
+        int numScatt = b.info[t] >> 8;
+        double Lp = b.par[t];
+        double Lext = Lp * exp(-b.tau[t]);
+        double x = b.x[t], y = b.y[t], z = b.z[t];
+        double lambda = w.pk.lam[slot];
+        for (int i = group; i < sc.ninstr && (i == group || sc.instr[i].same); ++i)
+        {
+            const InstrDev& in = sc.instr[i];
+            int l = in.kind == 0 ? framePixel(in, x, y, z) : -1;
+            if (in.kind == 0 && l < 0) continue;
+            int ell = wlgBin(sc.wlgB + in.woff, in.wnb, sc.wlgEll + in.woff, lambda);
+            if (ell < 0) continue;
+            det++;
+            if (in.kind == 0)
+            {
+                size_t npix = static_cast<size_t>(in.npx) * in.npy;
+                size_t at = static_cast<size_t>(l) + static_cast<size_t>(ell) * npix;
+                atomicAddAgg(in.ifu + at, Lext);
+                if (in.comps)
+                {
+                    size_t plane = npix * in.nbins;
+                    if (numScatt == 0)
+                    {
+                        atomicAddAgg(in.ifuComp + at, Lp);
+                        atomicAddAgg(in.ifuComp + plane + at, Lext);
+                    }
+                    else
+                        atomicAddAgg(in.ifuComp + 2 * plane + at, Lext);
+                }
+            }
+            else
+            {
+                atomicAddAgg(in.sed + ell, Lext);
+                if (in.comps)
+                {
+                    if (numScatt == 0)
+                    {
+                        atomicAddAgg(in.sedComp + ell, Lp);
+                        atomicAddAgg(in.sedComp + in.nbins + ell, Lext);
+                    }
+                    else
+                        atomicAddAgg(in.sedComp + 2 * in.nbins + ell, Lext);
+                }
+            }
+            if (in.stats)
+            {
+                unsigned long long key = (static_cast<unsigned long long>(i) << 48)
+                                         | (static_cast<unsigned long long>(ell) << 24)
+                                         | static_cast<unsigned long long>(l + 1);
+                int k = atomicAdd(&w.pk.nstat[slot], 1);
+                if (k < STATS_CAP)
+                {
+                    w.pk.skey[static_cast<size_t>(slot) * STATS_CAP + k] = key;
+                    w.pk.sw[static_cast<size_t>(slot) * STATS_CAP + k] = Lext;
+                }
+                else
+                {
+                    // buffer full: this contribution forms its own group
+                    statMoments(sc, key, Lext);
+                    ovf++;
+                }
+            }
+        }
+    }
+    if (det) atomicAdd(&w.ctl->counters[3], det);
+    if (ovf) atomicAdd(&w.ctl->counters[5], ovf);
+}
+
+// forced scattering: sample the interaction optical depth (simulateForcedPropagation)
+static __global__ void __launch_bounds__(256) shadeProp1Kernel(Wave w, int cur, int nxt)
+{
+    unsigned n = w.ctl->qn[cur][K_PROP1];
+    const TaskBuf& b = w.q[cur][K_PROP1];
+    for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+    {
+        int slot = b.slot[t];
+        double taupath = b.tau[t];
+        if (taupath <= 0.)
+        {
+            w.pk.L[slot] *= 0.;
+            endHistory(w, slot);
+            continue;
+        }
+        Rng rng;
+        loadRng(w, slot, rng);
+        double xi = w.sc.pathLengthBias;
+        double tau;
+        if (xi == 0.)
+            tau = exponCutoff(rng, taupath);
+        else
+        {
+            tau = rng.uniform() < xi ? rng.uniform() * taupath : exponCutoff(rng, taupath);
+            double p = -exp(-tau) / expm1(-taupath);
+            double q = (1.0 - xi) * p + xi / taupath;
+            w.pk.L[slot] *= p / q;
+        }
+        storeRng(w, slot, rng);
+        w.pk.tauPath[slot] = taupath;
+        emitProp(w, nxt, K_PROP2, slot, tau);
+    }
+}
+
+// interaction point reached: weight, position, termination test, scattering peel-off and HG
+// scattering, next propagation (MonteCarloSimulation.cpp:645-665, 670-683)
+SKG_D void interact(const Wave& w, int nxt, int slot, int m, double sInt, bool forced)
+{
+    const Scene& sc = w.sc;
+    if (m < 0)
+    {
+        atomicOr(&w.ctl->err, 2);  // MediumSystem::albedoForScattering: cannot locate the interaction point
+        endHistory(w, slot);
+        return;
+    }
+    int ell = w.pk.ellMix[slot];
+    double albedo = albedoAt(sc, m, sc.mixSca[ell], sc.mixExt[ell]);
+    double L = w.pk.L[slot];
+    if (forced)
+        L *= -expm1(-w.pk.tauPath[slot]) * albedo;
+    else
+        L *= albedo;
+    w.pk.L[slot] = L;
+    double kx = w.pk.kx[slot], ky = w.pk.ky[slot], kz = w.pk.kz[slot];
+    double x = w.pk.x[slot] + sInt * kx;
+    double y = w.pk.y[slot] + sInt * ky;
+    double z = w.pk.z[slot] + sInt * kz;
+    w.pk.x[slot] = x;
+    w.pk.y[slot] = y;
+    w.pk.z[slot] = z;
+    int nscatt = w.pk.nscatt[slot];
+    if (L <= 0 || (forced && L <= w.pk.Lth[slot] && nscatt >= sc.minScatt))
+    {
+        endHistory(w, slot);
+        return;
+    }
+    double g = sc.mixG[ell];
+    if (sc.peel && sc.ninstr > 0) emitPeels(w, nxt, slot, true, nscatt + 1, L, g, x, y, z, kx, ky, kz);
+    Rng rng;
+    loadRng(w, slot, rng);
+    if (nscatt >= MAX_SCATT_EVENTS)
+    {
+        atomicOr(&w.ctl->err, 8);  // a history that never meets its termination criterion
+        endHistory(w, slot);
+        return;
+    }
+    scatterHG(rng, g, kx, ky, kz);
+    w.pk.kx[slot] = kx;
+    w.pk.ky[slot] = ky;
+    w.pk.kz[slot] = kz;
+    w.pk.nscatt[slot] = nscatt + 1;
+    atomicAdd(&w.ctl->counters[2], 1ULL);
+    beginPropagation(w, nxt, slot, rng);
+    storeRng(w, slot, rng);
+}
+
+static __global__ void __launch_bounds__(256) shadeProp2Kernel(Wave w, int cur, int nxt)
+{
+    unsigned n = w.ctl->qn[cur][K_PROP2];
+    const TaskBuf& b = w.q[cur][K_PROP2];
+    for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+        interact(w, nxt, b.slot[t], b.m[t], b.s[t], true);
+}
+
+static __global__ void __launch_bounds__(256) shadeFreeKernel(Wave w, int cur, int nxt)
+{
+    unsigned n = w.ctl->qn[cur][K_FREE];
+    const TaskBuf& b = w.q[cur][K_FREE];
+    for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+    {
+        if (!b.found[t])
+            endHistory(w, b.slot[t]);  // the interaction point is outside the path: the packet escapes
+        else
+            interact(w, nxt, b.slot[t], b.m[t], b.s[t], false);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// launch
+// ---------------------------------------------------------------------------------------------
+static __global__ void launchPrepKernel(Wave w, int nxt)
+{
+    Control* c = w.ctl;
+    unsigned long long remaining = w.count - c->launched;
+    int n = static_cast<int>(min(static_cast<unsigned long long>(c->freeTop), remaining));
+    c->nLaunch = n;
+    c->launchBase = c->freeTop - n;
+    c->freeTop -= n;
+    c->launchHist0 = w.first + c->launched;
+    c->launched += n;
+    c->traceCursor = 0;
+    for (int k = 0; k < NUM_KINDS; ++k) c->qn[1 - nxt][k] = 0;  // the buffer consumed by this pass
+}
+
+static __global__ void __launch_bounds__(256) launchKernel(Wave w, int nxt)
+{
+    const Scene& sc = w.sc;
+    int n = w.ctl->nLaunch;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+    {
+        int slot = w.pk.freeSlots[w.ctl->launchBase + t];
+        unsigned long long hist = w.ctl->launchHist0 + t;
+        Rng rng;
+        rng.start(sc.seed, hist);
+        Launched o = launchPacket(sc, hist, rng);
+        w.pk.hist[slot] = hist;
+        w.pk.x[slot] = o.x; w.pk.y[slot] = o.y; w.pk.z[slot] = o.z;
+        w.pk.kx[slot] = o.kx; w.pk.ky[slot] = o.ky; w.pk.kz[slot] = o.kz;
+        w.pk.L[slot] = o.L;
+        w.pk.Lth[slot] = o.L / sc.minWeightRed;
+        w.pk.lam[slot] = o.lambda;
+        w.pk.nscatt[slot] = 0;
+        int ell = sc.nmix > 0 ? max(0, locateClip(sc.mixLb, sc.nmix, o.lambda)) : 0;  // DustMix::indexForLambda
+        w.pk.ellMix[slot] = ell;
+        w.pk.ellRF[slot] = sc.rfOn ? wlgBin(sc.rfB, sc.rfNb, sc.rfEll, o.lambda) : -1;
+        if (w.anyStats) w.pk.nstat[slot] = 0;
+        atomicAdd(&w.ctl->counters[0], 1ULL);
+        if (!(o.L > 0))
+        {
+            storeRng(w, slot, rng);
+            endHistory(w, slot);
+            continue;
+        }
+        if (sc.peel && sc.ninstr > 0) emitPeels(w, nxt, slot, false, 0, o.L, 0., o.x, o.y, o.z, 0., 0., 0.);
+        beginPropagation(w, nxt, slot, rng);
+        storeRng(w, slot, rng);
+    }
+}
+
+static __global__ void initPoolKernel(Wave w)
+{
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < w.P; t += gridDim.x * blockDim.x)
+    {
+        w.pk.freeSlots[t] = t;
+        if (w.anyStats) w.pk.nstat[t] = 0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+    {
+        Control* c = w.ctl;
+        for (int b = 0; b < 2; ++b)
+            for (int k = 0; k < NUM_KINDS; ++k) c->qn[b][k] = 0;
+        c->traceCursor = 0;
+        c->freeTop = w.P;
+        c->nLaunch = 0;
+        c->launchBase = 0;
+        c->launched = 0;
+        c->done = 0;
+        c->launchHist0 = 0;
+        for (int k = 0; k < 8; ++k) c->counters[k] = 0;
+        c->err = 0;
+    }
+}
+
+}  // namespace skg

@@ -1,0 +1,99 @@
+// Host driver of the wavefront: pool initialisation, then two passes (buffer parities 0 and 1)
+// captured once into a CUDA graph and replayed until every history of the range is done.
+#pragma once
+
+#include <cuda_runtime.h>
+#include "wavefront.cuh"
+
+namespace skg {
+
+struct WaveLaunch
+{
+    int traceBlocks, shadeBlocks, threads;
+};
+
+template<class Walker>
+int traceBlocksPerSM()
+{
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, traceKernel<Walker>, 256, 0) != cudaSuccess) return 1;
+    return n > 0 ? n : 1;
+}
+
+template<class Walker>
+void enqueuePass(const Wave& w, int cur, const WaveLaunch& L, cudaStream_t s)
+{
+    int nxt = 1 - cur;
+    traceKernel<Walker><<<L.traceBlocks, L.threads, 0, s>>>(w, cur);
+    shadePeelKernel<<<L.shadeBlocks, L.threads, 0, s>>>(w, cur);
+    shadeProp1Kernel<<<L.shadeBlocks, L.threads, 0, s>>>(w, cur, nxt);
+    shadeProp2Kernel<<<L.shadeBlocks, L.threads, 0, s>>>(w, cur, nxt);
+    shadeFreeKernel<<<L.shadeBlocks, L.threads, 0, s>>>(w, cur, nxt);
+    launchPrepKernel<<<1, 1, 0, s>>>(w, nxt);
+    launchKernel<<<L.shadeBlocks, L.threads, 0, s>>>(w, nxt);
+}
+
+// Runs histories [w.first, w.first + w.count). `doneHost` is pinned host memory for the progress
+// word. Returns a CUDA error, or cudaErrorLaunchTimeout (mapped to SKGPU_ERR_TIMEOUT) when the pass
+// limit is reached without finishing. `passes` receives the number of passes run.
+template<class Walker>
+cudaError_t runWave(const Wave& w, int numSMs, cudaStream_t s, unsigned long long* doneHost, long long* passes,
+                    long long maxPasses)
+{
+    WaveLaunch L;
+    L.threads = 256;
+    L.traceBlocks = numSMs * traceBlocksPerSM<Walker>();
+    L.shadeBlocks = numSMs * 4;
+    *passes = 0;
+    initPoolKernel<<<L.shadeBlocks, L.threads, 0, s>>>(w);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (w.count == 0) return cudaStreamSynchronize(s);
+
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    const int passesPerGraph = 4;  // even: the buffer parity returns to 0 after every replay
+    for (int k = 0; k < passesPerGraph; ++k) enqueuePass<Walker>(w, k & 1, L, s);
+    e = cudaStreamEndCapture(s, &graph);
+    if (e != cudaSuccess) return e;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e != cudaSuccess)
+    {
+        cudaGraphDestroy(graph);
+        return e;
+    }
+    const size_t doneOffset = offsetof(Control, done);
+    unsigned long long lastDone = 0;
+    long long lastProgress = 0;
+    while (e == cudaSuccess)
+    {
+        e = cudaGraphLaunch(exec, s);
+        if (e != cudaSuccess) break;
+        *passes += passesPerGraph;
+        e = cudaMemcpyAsync(doneHost, reinterpret_cast<char*>(w.ctl) + doneOffset, sizeof(unsigned long long),
+                            cudaMemcpyDeviceToHost, s);
+        if (e != cudaSuccess) break;
+        e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) break;
+        if (*doneHost >= w.count) break;
+        if (*doneHost != lastDone)
+        {
+            lastDone = *doneHost;
+            lastProgress = *passes;
+        }
+        // no history finished for 65536 passes (more than 32768 scattering events of one history),
+        // or the overall pass limit: stop with a timeout status instead of looping on
+        if (*passes >= maxPasses || *passes - lastProgress > 65536)
+        {
+            e = cudaErrorLaunchTimeout;
+            break;
+        }
+    }
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    return e;
+}
+
+}  // namespace skg

@@ -1,0 +1,22 @@
+// Wavefront life cycle with the FP64 walkers that keep the reference generators' operation order.
+// Compiled with --fmad=false so that the FP64 physics outside the walkers (weights, directions,
+// positions) is rounded like the reference CPU build (x86-64 SSE2, no FMA).
+#include "internal.hpp"
+#include "wavefront_driver.cuh"
+
+namespace skg {
+
+cudaError_t runWaveFP64(int gridKind, const Wave& w, int numSMs, cudaStream_t s, unsigned long long* doneHost,
+                        long long* passes, long long maxPasses)
+{
+    switch (gridKind)
+    {
+        case 0: return runWave<CartesianExact>(w, numSMs, s, doneHost, passes, maxPasses);
+        case 1: return runWave<OctreeExact>(w, numSMs, s, doneHost, passes, maxPasses);
+        case 2: return runWave<VoronoiExact>(w, numSMs, s, doneHost, passes, maxPasses);
+        case 3: return runWave<TetraExact>(w, numSMs, s, doneHost, passes, maxPasses);
+    }
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace skg
