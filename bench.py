@@ -32,6 +32,10 @@ WORKLOADS = {
     # name: (description, packets per step per GPU)
     "shell": ("dust shell r^-2 0.1-1 pc on a 64^3 CartesianSpatialGrid, tau_V=1, point source, 0.55 um, "
               "HG g=0.6 albedo 0.5, 256^2 frame at 30 deg + SED, FP64 tallies with statistics", 1_000_000),
+    "galaxy": ("stellar exp. disk (hR 4 kpc, hz 0.35 kpc) + Sersic n=4 bulge (Re 1 kpc, B/T 0.2), dust exp. disk "
+               "(hR 6 kpc, hz 0.2 kpc, face-on tau_V=1) on a TreeSpatialGrid octree (max level 8, dust fraction 1e-6, "
+               "~5.1e5 leaves), 100 log wavelengths 0.1-10 um with power-law dust, three 512^2 frames at 0/60/90 deg, "
+               "radiation field stored on 100 bins; 1e8-packet run split into steps", 10_000_000),
 }
 
 
@@ -88,6 +92,8 @@ def build_scene(name):
     from skgpu import workloads
     if name == "shell":
         return workloads.shell_cartesian(64, 256)
+    if name == "galaxy":
+        return workloads.galaxy_octree()
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -124,6 +130,8 @@ def reference_ski(name, npp):
     from skgpu import ski
     if name == "shell":
         return ski.shell_cartesian(npp, nbins=64, npix=256)
+    if name == "galaxy":
+        return ski.galaxy_octree(npp)
     raise SystemExit(name)
 
 
@@ -187,7 +195,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="shell", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="galaxy", choices=sorted(WORKLOADS))
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--packets", type=int, default=0, help="packets per step per GPU (default: the workload's)")

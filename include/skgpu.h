@@ -207,6 +207,39 @@ int skgpu_trace_paths(skgpu_ctx* ctx, int32_t num_rays, const double* rays, int3
 int skgpu_optical_depths(skgpu_ctx* ctx, int32_t num_rays, const double* rays, double lambda, int32_t precision,
                          double* tau);
 
+/* ---- standalone octree construction ----
+ * For scenes not built by SKIRT itself: constructs a TreeSpatialGrid-like octree of an analytic
+ * dust geometry with the DensityTreePolicy criteria (SKIRT/core/DensityTreePolicy.cpp:88-245) and
+ * the overlap-sorted neighbour lists of OctTreeNode/TreeNode, and samples the mean normalised
+ * density per leaf. The exported arrays are exactly those skgpu_upload_grid_octree takes. No
+ * reference counterpart: in the drop-in case SKIRT's own tree is uploaded. */
+#define SKGPU_GEOM_EXPDISK 0 /* params: hR, hz, Rmin, Rmax (0 = none), zmax (0 = none) */
+#define SKGPU_GEOM_SHELL 1   /* params: rmin, rmax, power-law exponent */
+
+typedef struct skgpu_octree_spec {
+    int32_t geometry;                /* SKGPU_GEOM_* (unit total mass) */
+    int32_t min_level;
+    int32_t max_level;
+    int32_t num_subdivision_samples; /* random samples per node for the mass-fraction criterion */
+    int32_t num_density_samples;     /* random samples per leaf for the cell density */
+    int32_t reserved;
+    double params[6];
+    double extent[6];                /* xmin, ymin, zmin, xmax, ymax, zmax */
+    double max_dust_fraction;
+    uint64_t seed;
+} skgpu_octree_spec;
+
+typedef struct skgpu_octree skgpu_octree;
+int skgpu_octree_build(const skgpu_octree_spec* spec, skgpu_octree** out);
+int skgpu_octree_sizes(const skgpu_octree* tree, int32_t* num_nodes, int32_t* num_cells, int64_t* num_nb);
+/* arrays sized by skgpu_octree_sizes: bounds 6*num_nodes, cell_index/child_begin/child_count
+ * num_nodes, child_index 8*(subdivided nodes) (<= num_nodes), nb_begin 6*num_nodes+1, nb_index num_nb,
+ * cell_density num_cells (normalised geometry density, unit total mass); any may be NULL */
+int skgpu_octree_export(const skgpu_octree* tree, double* bounds, int32_t* cell_index, int32_t* child_begin,
+                        int32_t* child_count, int32_t* child_index, int32_t* nb_begin, int32_t* nb_index,
+                        double* cell_density);
+void skgpu_octree_free(skgpu_octree* tree);
+
 #ifdef __cplusplus
 }
 #endif

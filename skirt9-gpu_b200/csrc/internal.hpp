@@ -13,10 +13,14 @@ cudaError_t runWaveFP64(int gridKind, const Wave& w, int numSMs, cudaStream_t s,
 cudaError_t runWaveFP32(int gridKind, const Wave& w, int numSMs, cudaStream_t s, unsigned long long* doneHost,
                         long long* passes, long long maxPasses);
 
-// path-segment and optical-depth kernels (reference generators, FP64)
-cudaError_t launchTracePaths(int precision, const GridDev& g, int n, const double* rays, int maxSeg, int* count,
-                             int* m, double* ds, int* err, cudaStream_t s);
-cudaError_t launchOpticalDepths(int precision, const GridDev& g, const double* dens, double section, int n,
-                                const double* rays, double* tau, int* err, cudaStream_t s);
+// path-segment and optical-depth kernels, FP64 (reference operation order) and FP32-distance walkers
+cudaError_t launchTracePathsFP64(int precision, const GridDev& g, int n, const double* rays, int maxSeg, int* count,
+                                 int* m, double* ds, int* err, cudaStream_t s);
+cudaError_t launchOpticalDepthsFP64(int precision, const GridDev& g, const double* dens, double section, int n,
+                                    const double* rays, double* tau, int* err, cudaStream_t s);
+cudaError_t launchTracePathsFP32(int precision, const GridDev& g, int n, const double* rays, int maxSeg, int* count,
+                                 int* m, double* ds, int* err, cudaStream_t s);
+cudaError_t launchOpticalDepthsFP32(int precision, const GridDev& g, const double* dens, double section, int n,
+                                    const double* rays, double* tau, int* err, cudaStream_t s);
 
 }  // namespace skg

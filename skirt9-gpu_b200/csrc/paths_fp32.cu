@@ -1,0 +1,41 @@
+// Path-segment and optical-depth kernels with the FP32 walkers that keep the reference generators'
+// operation order. They back skgpu_trace_paths / skgpu_optical_depths, the replacements of the
+// reference's per-path GPU wrappers (GpuAcceleration::set*SpatialGridPath and the optical-depth
+// sums, GpuAcceleration.hpp), and they are what the cell-sequence parity tests call.
+#include "internal.hpp"
+#include "paths.cuh"
+#include "grids_fast.cuh"
+
+namespace skg {
+
+cudaError_t launchTracePathsFP32(int precision, const GridDev& g, int n, const double* rays, int maxSeg, int* count,
+                             int* m, double* ds, int* err, cudaStream_t s)
+{
+    if (n <= 0) return cudaSuccess;
+    int threads = 128, blocks = (n + threads - 1) / threads;
+    (void)precision;
+    switch (g.kind)
+    {
+        case 0: tracePathsKernel<CartesianFast<float>><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
+        case 1: tracePathsKernel<OctreeFast<float>><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
+        default: return cudaErrorNotSupported;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launchOpticalDepthsFP32(int precision, const GridDev& g, const double* dens, double section, int n,
+                                const double* rays, double* tau, int* err, cudaStream_t s)
+{
+    if (n <= 0) return cudaSuccess;
+    int threads = 128, blocks = (n + threads - 1) / threads;
+    (void)precision;
+    switch (g.kind)
+    {
+        case 0: opticalDepthKernel<CartesianFast<float>><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
+        case 1: opticalDepthKernel<OctreeFast<float>><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
+        default: return cudaErrorNotSupported;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace skg

@@ -875,7 +875,7 @@ int skgpu_trace_paths(skgpu_ctx* ctx, int32_t num_rays, const double* rays, int3
     if (!ctx->hasGrid) return fail(ctx, SKGPU_ERR_STATE, "trace: no grid uploaded");
     if (num_rays < 0 || max_segments < 1 || (num_rays > 0 && (!rays || !count || !m || !ds)))
         return fail(ctx, SKGPU_ERR_ARG, "trace: bad arguments");
-    if (precision != SKGPU_PREC_FP64_EXACT) return fail(ctx, SKGPU_ERR_UNSUPPORTED, "trace: only FP64 exact path dumps");
+    if (precision != SKGPU_PREC_FP64_EXACT && precision != SKGPU_PREC_FP32) return fail(ctx, SKGPU_ERR_ARG, "trace: bad precision");
     if (num_rays == 0) return SKGPU_OK;
     CK(cudaSetDevice(ctx->device));
     size_t n = num_rays, ns = n * static_cast<size_t>(max_segments);
@@ -887,7 +887,9 @@ int skgpu_trace_paths(skgpu_ctx* ctx, int32_t num_rays, const double* rays, int3
     if (e == cudaSuccess) e = devAlloc(&dCount, n);
     if (e == cudaSuccess) e = devAlloc(&dM, ns);
     if (e == cudaSuccess) e = cudaMemsetAsync(ctx->errFlag, 0, sizeof(int), ctx->stream);
-    if (e == cudaSuccess) e = launchTracePaths(precision, ctx->g, num_rays, dRays, max_segments, dCount, dM, dDs, ctx->errFlag, ctx->stream);
+    if (e == cudaSuccess)
+        e = (precision == SKGPU_PREC_FP32 ? launchTracePathsFP32 : launchTracePathsFP64)(
+            precision, ctx->g, num_rays, dRays, max_segments, dCount, dM, dDs, ctx->errFlag, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     int errFlag = 0;
     if (e == cudaSuccess) e = cudaMemcpy(&errFlag, ctx->errFlag, sizeof(int), cudaMemcpyDeviceToHost);
@@ -895,6 +897,7 @@ int skgpu_trace_paths(skgpu_ctx* ctx, int32_t num_rays, const double* rays, int3
     if (e == cudaSuccess) e = cudaMemcpy(m, dM, ns * sizeof(int), cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(ds, dDs, ns * sizeof(double), cudaMemcpyDeviceToHost);
     cleanup();
+    if (e == cudaErrorNotSupported) return fail(ctx, SKGPU_ERR_UNSUPPORTED, "trace: no walker of this precision for the grid kind");
     if (e != cudaSuccess) return fail(ctx, SKGPU_ERR_CUDA, std::string("trace: ") + cudaGetErrorString(e));
     if (errFlag) return fail(ctx, SKGPU_ERR_TIMEOUT, "trace: a path exceeded its segment guard");
     return SKGPU_OK;
@@ -907,7 +910,7 @@ int skgpu_optical_depths(skgpu_ctx* ctx, int32_t num_rays, const double* rays, d
     if (!ctx->hasGrid || !ctx->dens || !ctx->nmix) return fail(ctx, SKGPU_ERR_STATE, "optical depths: grid, medium and mix required");
     if (ctx->numCells != ctx->g.numCells) return fail(ctx, SKGPU_ERR_STATE, "optical depths: medium does not match the grid");
     if (num_rays < 0 || (num_rays > 0 && (!rays || !tau))) return fail(ctx, SKGPU_ERR_ARG, "optical depths: bad arguments");
-    if (precision != SKGPU_PREC_FP64_EXACT) return fail(ctx, SKGPU_ERR_UNSUPPORTED, "optical depths: only FP64 exact");
+    if (precision != SKGPU_PREC_FP64_EXACT && precision != SKGPU_PREC_FP32) return fail(ctx, SKGPU_ERR_ARG, "optical depths: bad precision");
     if (num_rays == 0) return SKGPU_OK;
     // DustMix::sectionExt(lambda) = sigma_ext[locateClip(lambda borders, lambda)]
     std::vector<double> lb(ctx->nmix), se(ctx->nmix);
@@ -919,7 +922,9 @@ int skgpu_optical_depths(skgpu_ctx* ctx, int32_t num_rays, const double* rays, d
     cudaError_t e = devUpload(&dRays, rays, 6 * n);
     if (e == cudaSuccess) e = devAlloc(&dTau, n);
     if (e == cudaSuccess) e = cudaMemsetAsync(ctx->errFlag, 0, sizeof(int), ctx->stream);
-    if (e == cudaSuccess) e = launchOpticalDepths(precision, ctx->g, ctx->dens, section, num_rays, dRays, dTau, ctx->errFlag, ctx->stream);
+    if (e == cudaSuccess)
+        e = (precision == SKGPU_PREC_FP32 ? launchOpticalDepthsFP32 : launchOpticalDepthsFP64)(
+            precision, ctx->g, ctx->dens, section, num_rays, dRays, dTau, ctx->errFlag, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e == cudaSuccess) e = cudaMemcpy(tau, dTau, n * sizeof(double), cudaMemcpyDeviceToHost);
     devFree(dRays);

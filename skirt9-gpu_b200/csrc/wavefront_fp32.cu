@@ -1,12 +1,19 @@
-// Wavefront life cycle with FP32 traversal walkers. A grid kind without an FP32 walker is
-// reported as unsupported; there is no silent substitution of the FP64 walkers.
+// Wavefront life cycle with the FP32-distance walkers (production path). Grid kinds without such a
+// walker are reported as unsupported; there is no silent substitution of the FP64 walkers.
 #include "internal.hpp"
-
+#include "grids_fast.cuh"
+#include "wavefront_driver.cuh"
 
 namespace skg {
 
-cudaError_t runWaveFP32(int, const Wave&, int, cudaStream_t, unsigned long long*, long long*, long long)
+cudaError_t runWaveFP32(int gridKind, const Wave& w, int numSMs, cudaStream_t s, unsigned long long* doneHost,
+                        long long* passes, long long maxPasses)
 {
+    switch (gridKind)
+    {
+        case 0: return runWave<CartesianFast<float>>(w, numSMs, s, doneHost, passes, maxPasses);
+        case 1: return runWave<OctreeFast<float>>(w, numSMs, s, doneHost, passes, maxPasses);
+    }
     return cudaErrorNotSupported;
 }
 

@@ -291,3 +291,65 @@ class Backend:
         tau = np.zeros(len(r))
         self.call("optical_depths", len(r), _ptr(r), float(lam), int(precision), _ptr(tau))
         return tau
+
+
+GEOM_EXPDISK, GEOM_SHELL = 0, 1
+
+
+class OctreeSpec(C.Structure):
+    _fields_ = [
+        ("geometry", C.c_int32),
+        ("min_level", C.c_int32),
+        ("max_level", C.c_int32),
+        ("num_subdivision_samples", C.c_int32),
+        ("num_density_samples", C.c_int32),
+        ("reserved", C.c_int32),
+        ("params", C.c_double * 6),
+        ("extent", C.c_double * 6),
+        ("max_dust_fraction", C.c_double),
+        ("seed", C.c_uint64),
+    ]
+
+
+EXPORTED += ["skgpu_octree_build", "skgpu_octree_sizes", "skgpu_octree_export", "skgpu_octree_free"]
+
+
+def build_octree(geometry, params, extent, min_level, max_level, max_dust_fraction, num_subdivision_samples=100,
+                 num_density_samples=100, seed=1, lib=None):
+    """Octree of an analytic unit-mass dust geometry (skgpu_octree_build); returns the arrays of
+    skgpu_upload_grid_octree plus the mean normalised density per cell."""
+    lib = lib if lib is not None else load_library()
+    spec = OctreeSpec()
+    spec.geometry = geometry
+    spec.min_level, spec.max_level = min_level, max_level
+    spec.num_subdivision_samples, spec.num_density_samples = num_subdivision_samples, num_density_samples
+    spec.params[:] = list(params) + [0.0] * (6 - len(params))
+    spec.extent[:] = list(extent)
+    spec.max_dust_fraction = max_dust_fraction
+    spec.seed = seed
+    lib.skgpu_octree_build.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
+    lib.skgpu_octree_sizes.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int64)]
+    lib.skgpu_octree_export.argtypes = [C.c_void_p] + [C.c_void_p] * 8
+    lib.skgpu_octree_free.argtypes = [C.c_void_p]
+    lib.skgpu_octree_free.restype = None
+    tree = C.c_void_p()
+    rc = lib.skgpu_octree_build(C.cast(C.pointer(spec), C.c_void_p), C.byref(tree))
+    if rc != OK:
+        raise SkgpuError(rc, "octree construction failed (bad specification)")
+    try:
+        nn, nc, nb = C.c_int32(), C.c_int32(), C.c_int64()
+        lib.skgpu_octree_sizes(tree, C.byref(nn), C.byref(nc), C.byref(nb))
+        nn, nc, nb = nn.value, nc.value, nb.value
+        out = dict(bounds=np.zeros((nn, 6)), cell_index=np.zeros(nn, np.int32), child_begin=np.zeros(nn, np.int32),
+                   child_count=np.zeros(nn, np.int32), child_index=np.zeros(max(nn, 1), np.int32),
+                   nb_begin=np.zeros(6 * nn + 1, np.int32), nb_index=np.zeros(max(nb, 1), np.int32),
+                   density=np.zeros(nc))
+        lib.skgpu_octree_export(tree, *[_ptr(out[k]) for k in ("bounds", "cell_index", "child_begin", "child_count",
+                                                             "child_index", "nb_begin", "nb_index", "density")])
+    finally:
+        lib.skgpu_octree_free(tree)
+    nsub = int((out["child_count"] > 0).sum())
+    out["child_index"] = out["child_index"][:8 * nsub]
+    out["nb_index"] = out["nb_index"][:nb]
+    out["extent"] = np.array(extent, float)
+    return out

@@ -143,6 +143,37 @@ def disk_probe(grid_xml, num_packets=1e4, tau_z=1.0, hR=1.0, hz=0.2):
                       num_density_samples=10)
 
 
+def geometric_source(geometry_xml, temperature, luminosity_lsun):
+    return (f'<GeometricSource velocityMagnitude="0 km/s" sourceWeight="1" wavelengthBias="0.5">'
+            f'<geometry type="Geometry">{geometry_xml}</geometry>'
+            f'<sed type="SED"><BlackBodySED temperature="{temperature} K"/></sed>'
+            f'<normalization type="LuminosityNormalization"><IntegratedLuminosityNormalization '
+            f'wavelengthRange="Source" integratedLuminosity="{luminosity_lsun:g} Lsun"/></normalization>'
+            f'</GeometricSource>')
+
+
+def galaxy_octree(num_packets=1e8, npix=512, nlambda=100, max_level=8, max_dust_fraction=1e-6, tau_v=1.0,
+                  half_size_kpc=25, store_rf=True):
+    """Stellar exponential disk (hR 4 kpc, hz 0.35 kpc) + Sersic n=4 bulge (Re 1 kpc), B/T = 0.2,
+    black bodies of 6000 K and 4000 K; dust exponential disk (hR 6 kpc, hz 0.2 kpc, face-on tau_V)
+    with power-law MeanListDustMix on 100 log wavelengths 0.1-10 micron; octree by the dust-mass
+    fraction policy; three frames at 0, 60 and 90 degrees; radiation field on the same grid."""
+    lam = [0.1 * (100.0 ** (i / (nlambda - 1))) for i in range(nlambda)]
+    kappa = [(l / 0.55) ** -1.0 for l in lam]
+    albedo = [min(0.9, max(0.05, 0.5 * (l / 0.55) ** -0.2)) for l in lam]
+    g = [min(0.9, max(0.0, 0.6 * (l / 0.55) ** -0.3)) for l in lam]
+    mix = mean_list_mix(lam, kappa, albedo, g)
+    sources = (geometric_source('<ExpDiskGeometry scaleLength="4 kpc" scaleHeight="0.35 kpc" minRadius="0 kpc" '
+                                'maxRadius="0 kpc" maxZ="0 kpc"/>', 6000, 8e9)
+               + geometric_source('<SersicGeometry effectiveRadius="1 kpc" index="4"/>', 4000, 2e9))
+    wlg = f'<LogWavelengthGrid minWavelength="0.1 micron" maxWavelength="10 micron" numWavelengths="{nlambda}"/>'
+    fov = 2 * half_size_kpc
+    instruments = "".join(frame_instrument(f"i{inc}", inc, fov, "kpc", npix, stats=False) for inc in (0, 60, 90))
+    return simulation("ExtinctionOnly", num_packets, sources, expdisk_medium(6, 0.2, "kpc", tau_v, mix),
+                      octree_grid(half_size_kpc, "kpc", max_level, max_dust_fraction), instruments,
+                      instrument_wlg=wlg, store_rf=store_rf, rf_wlg=wlg)
+
+
 def shell_cartesian(num_packets=1e6, nbins=64, npix=256, stats=True, points=None):
     """Dust shell (r^-2 between 0.1 and 1 pc, radial tau_V = 1, i.e. tau_X = 2 through the centre) on a
     Cartesian grid of +-1 pc, isotropic point source at the centre, 0.55 micron, HG g = 0.6,

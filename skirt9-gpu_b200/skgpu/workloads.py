@@ -45,6 +45,98 @@ def _cell_average(density, xb, yb, zb, samples=4, chunk=8):
     return out
 
 
+KPC = 1e3 * PC
+LSUN = 3.828e26  # W
+
+
+def log_wavelength_grid(lmin, lmax, n):
+    """LogWavelengthGrid: characteristic wavelengths, border list and bin map of
+    DisjointWavelengthGrid::setWavelengthRange (DisjointWavelengthGrid.cpp:22-84)."""
+    lam = np.exp(np.linspace(np.log(lmin), np.log(lmax), n))
+    borders = np.empty(n + 1)
+    borders[0] = np.sqrt(lam[0] ** 3 / lam[1])
+    borders[1:n] = np.sqrt(lam[:-1] * lam[1:])
+    borders[n] = np.sqrt(lam[-1] ** 3 / lam[-2])
+    ellv = np.r_[-1, np.arange(n), -1].astype(np.int32)
+    return lam, borders, ellv
+
+
+def planck_table(T, lmin, lmax, n=400):
+    """Normalised black-body pdf on a log grid with its cumulative distribution for log-log
+    sampling (Random::cdfLogLog): piecewise power laws between the grid points."""
+    h, c, k = 6.62607015e-34, 2.99792458e8, 1.380649e-23
+    lam = np.exp(np.linspace(np.log(lmin), np.log(lmax), n))
+    p = 1.0 / (lam ** 5 * np.expm1(h * c / (lam * k * T)))
+    alpha = np.log(p[1:] / p[:-1]) / np.log(lam[1:] / lam[:-1])
+    q = 1.0 + alpha
+    t = lam[1:] / lam[:-1]
+    seg = np.where(np.abs(q) > 1e-12, (t ** q - 1.0) / np.where(np.abs(q) > 1e-12, q, 1.0), np.log(t)) * p[:-1] * lam[:-1]
+    P = np.r_[0.0, np.cumsum(seg)]
+    return lam, p / P[-1], P / P[-1]
+
+
+def sersic_radial_cdf(reff, n, num=600):
+    """Cumulative mass of the deprojected Sersic profile (Abel inversion of the surface density
+    exp(-b_n ((R/Re)^(1/n) - 1))), on a log radius grid: the radius distribution of SersicGeometry."""
+    b = 2.0 * n - 1.0 / 3.0 + 0.009876 / n
+    r = np.exp(np.linspace(np.log(1e-5), np.log(200.0), num))   # in units of Re
+    u = np.linspace(0.0, 12.0, 3000)                              # R = r cosh(u)
+    ch = np.cosh(u)
+    R = r[:, None] * ch[None, :]
+    dS = -(b / n) * R ** (1.0 / n - 1.0) * np.exp(-b * (R ** (1.0 / n) - 1.0))
+    rho = -np.trapezoid(dS, u, axis=1) / np.pi                   # rho(r) = -1/pi int S'(r cosh u) du
+    dm = 4 * np.pi * r ** 2 * rho
+    M = np.r_[0.0, np.cumsum(0.5 * (dm[1:] + dm[:-1]) * np.diff(r))]
+    return np.r_[0.0, r * reff], np.r_[0.0, M / M[-1]]
+
+
+def galaxy_octree(npix=512, nlambda=100, max_level=8, max_dust_fraction=1e-6, tau_v=1.0, store_rf=True,
+                  seed=1, half_size_kpc=25.0, stats=False):
+    """Exponential-disk galaxy on an octree: stellar disk (hR 4 kpc, hz 0.35 kpc) + Sersic n=4
+    bulge (Re 1 kpc), B/T = 0.2; dust disk (hR 6 kpc, hz 0.2 kpc) with face-on tau_V; octree by
+    the dust-mass-fraction policy (max level 8, fraction 1e-6: ~5e5 leaves); 100 log wavelengths
+    0.1-10 micron with power-law dust properties; three 512^2 frames at 0, 60, 90 degrees; the
+    radiation field stored on the same wavelength grid."""
+    sc = Scene()
+    h = half_size_kpc * KPC
+    ext = [-h, -h, -h, h, h, h]
+    hRd, hzd = 6 * KPC, 0.2 * KPC
+    tree = abi.build_octree(abi.GEOM_EXPDISK, [hRd, hzd, 0, 0, 0], ext, 2, max_level, max_dust_fraction, seed=seed)
+    sc.grid = dict(kind=abi.GRID_OCTREE, bounds=tree["bounds"], cell_index=tree["cell_index"],
+                   child_begin=tree["child_begin"], child_count=tree["child_count"],
+                   child_index=tree["child_index"], nb_begin=tree["nb_begin"], nb_index=tree["nb_index"],
+                   eps=1e-12 * np.sqrt(3) * 2 * h, extent=np.array(ext))
+    # dust: power-law properties on the instrument wavelengths; kappa_V = 1 m2/kg
+    lam, borders, ellv = log_wavelength_grid(0.1e-6, 10e-6, nlambda)
+    kappa = (lam / LAMBDA_V) ** -1.0
+    albedo = np.clip(0.5 * (lam / LAMBDA_V) ** -0.2, 0.05, 0.9)
+    g = np.clip(0.6 * (lam / LAMBDA_V) ** -0.3, 0.0, 0.9)
+    mixb = np.r_[lam[0], np.sqrt(lam[1:] * lam[:-1])]  # DustMix wavelength-index borders (DustMix.cpp:92-97)
+    sc.mix = dict(lambda_borders=mixb, sigma_ext=kappa, sigma_sca=albedo * kappa, asymmpar=g)
+    # normalisation: face-on optical depth through the centre = tau_V (column 1/(2 pi hR^2) per unit mass)
+    mass = tau_v / (1.0 * 1.0 / (2 * np.pi * hRd ** 2))
+    sc.density = mass * tree["density"]
+    # sources: disk 80 %, bulge 20 %; black bodies; wavelength bias 0.5 with a log-uniform bias
+    sc.total_luminosity = 1e10 * LSUN
+    xi_src = 0.5
+    lf = np.array([0.8, 0.2])
+    wv = (1 - xi_src) * lf + xi_src * 0.5
+    ld, pd, Pd = planck_table(6000.0, 0.1e-6, 10e-6)
+    lb, pb, Pb = planck_table(4000.0, 0.1e-6, 10e-6)
+    rr, rP = sersic_radial_cdf(1.0 * KPC, 4.0)
+    common = dict(spectral_model=abi.SPEC_TABLE, wavelength_bias=0.5, bias_range=(0.1e-6, 10e-6))
+    sc.sources = [
+        dict(position_model=abi.SRC_EXPDISK, geometry=(4 * KPC, 0.35 * KPC, 0, 0, 0), lfrac=lf[0], weight=wv[0],
+             table_lambda=ld, table_a=pd, table_b=Pd, **common),
+        dict(position_model=abi.SRC_RADIAL, lfrac=lf[1], weight=wv[1], table_lambda=lb, table_a=pb, table_b=Pb,
+             radial_r=rr, radial_P=rP, **common),
+    ]
+    sc.instruments = [_frame(inc, 0, 0, 2 * h, npix, 10 * MPC, nlambda, borders, ellv, stats) for inc in (0, 60, 90)]
+    sc.rf = dict(num_bins=nlambda, borders=borders, ellv=ellv)
+    sc.store_rf = store_rf
+    return sc
+
+
 def shell_cartesian(nbins=64, npix=256, stats=True, luminosity=5.43959963e23):
     sc = Scene()
     b = np.linspace(-PC, PC, nbins + 1)
