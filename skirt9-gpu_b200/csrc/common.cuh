@@ -204,19 +204,21 @@ SKG_D double phaseHG(double g, double costheta)
     return fabs(g) > 0.95 ? meanHG(g, costheta) : valueHG(g, costheta);
 }
 
-// SpecialFunctions::lnmean(x1, x2, lnx1, lnx2) (SKIRT/utils/SpecialFunctions.cpp:860-880)
-SKG_D double lnmean4(double x1, double x2, double lnx1, double lnx2)
+// SpecialFunctions::lnmean(x1, x2, lnx1, lnx2) (SKIRT/utils/SpecialFunctions.cpp:860-880),
+// in the precision of the walk accumulators
+template<typename R>
+SKG_D R lnmean4(R x1, R x2, R lnx1, R lnx2)
 {
     if (x1 > x2)
     {
-        double t = x1; x1 = x2; x2 = t;
+        R t = x1; x1 = x2; x2 = t;
         t = lnx1; lnx1 = lnx2; lnx2 = t;
     }
-    if (x1 <= 0) return 0.;
-    double x = x2 / x1 - 1.;
-    if (x < 1e-3)
-        return x1 / (1. - 1. / 2. * x + 1. / 3. * x * x - 1. / 4. * x * x * x + 1. / 5. * x * x * x * x
-                     - 1. / 6. * x * x * x * x * x);
+    if (x1 <= R(0)) return R(0);
+    R x = x2 / x1 - R(1);
+    if (x < R(1e-3))
+        return x1 / (R(1) - R(1) / R(2) * x + R(1) / R(3) * x * x - R(1) / R(4) * x * x * x + R(1) / R(5) * x * x * x * x
+                     - R(1) / R(6) * x * x * x * x * x);
     return (x2 - x1) / (lnx2 - lnx1);
 }
 

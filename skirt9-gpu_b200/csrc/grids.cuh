@@ -37,6 +37,12 @@ struct GridDev
     const int* tNbBegin;
     const int* tNb;
     int tNodes;
+    // leaf-indexed records of the FP32 walker: per cell two float4 (FP32 bounds, FP32 number
+    // density, neighbour-list base), per cell the cumulative offsets of its 6 walls in its neighbour list (9 bits each), and
+    // the neighbour cells (positive overlap only, overlap-sorted) of every leaf wall
+    const float4* tLeaf;
+    const unsigned long long* tLeafCnt;
+    const int* tLeafNb;
 
     // Voronoi: sites, neighbour CSR (negative = wall), uniform site-search grid
     const double* vSites;
@@ -66,6 +72,7 @@ struct GridDev
 // ---------------------------------------------------------------------------------------------
 struct GenBase
 {
+    using Acc = double;  // accumulator type of optical depth and path length along the walk
     double rx, ry, rz, kx, ky, kz;
     double ds;
     int m;
@@ -79,6 +86,9 @@ struct GenBase
         m = -1;
         ds = 0.;
     }
+    // number density of the cell of the segment just returned
+    SKG_D double density(const double* dens) const { return dens[m]; }
+
     SKG_D void propagater(double d)
     {
         rx = xadd(rx, xmul(kx, d));
@@ -170,6 +180,7 @@ SKG_D double boxDiagonal(const double* b)
 // ---------------------------------------------------------------------------------------------
 struct CartesianExact : GenBase
 {
+    static constexpr int kMinBlocks = 3;
     int i, j, k;
 
     SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz)
@@ -249,6 +260,7 @@ SKG_D int octreeLeafChild(const GridDev& g, double x, double y, double z)
 
 struct OctreeExact : GenBase
 {
+    static constexpr int kMinBlocks = 3;
     int node;
 
     SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz)
@@ -377,6 +389,7 @@ SKG_D int voronoiCellIndex(const GridDev& g, double x, double y, double z)
 
 struct VoronoiExact : GenBase
 {
+    static constexpr int kMinBlocks = 3;
     int mr;
 
     SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz)
@@ -531,6 +544,7 @@ SKG_D void xcross(double ax, double ay, double az, double bx, double by, double 
 
 struct TetraExact : GenBase
 {
+    static constexpr int kMinBlocks = 3;
     int mr;
     int enteringFace;
 

@@ -70,6 +70,8 @@ struct FastBase : GenBase
 template<typename Real>
 struct CartesianFast : FastBase<Real>
 {
+    using Acc = Real;
+    static constexpr int kMinBlocks = 4;
     int i, j, k;
 
     SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz)
@@ -104,15 +106,40 @@ struct CartesianFast : FastBase<Real>
     }
 };
 
-template<typename Real>
-struct OctreeFast : FastBase<Real>
+// Octree walker on the leaf-indexed FP32 records. The current cell's record (bounds, density,
+// neighbour-list base) and wall counts are held in registers; a crossing loads the ids of the exit
+// wall's neighbours and their records until one contains the exit point, and that record becomes
+// the current one (two dependent loads per crossing, all from a working set that stays in L2).
+struct OctreeLeaf32 : FastBase<float>
 {
-    int node;
+    using Acc = float;
+    static constexpr int kMinBlocks = 4;
+    int cell;
+    float4 ra, rb;                 // record of the current cell
+    unsigned long long cnt;        // cumulative wall offsets of the neighbour list, 9 bits each
+    float segDens;                 // density of the cell of the segment just returned
 
     SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz)
     {
         this->startFast(x, y, z, ux, uy, uz);
-        node = -1;
+        cell = -1;
+    }
+
+    SKG_D double density(const double*) const { return static_cast<double>(segDens); }
+
+    SKG_D void enter(const GridDev& g, int c)
+    {
+        cell = c;
+        ra = g.tLeaf[2 * c];
+        rb = g.tLeaf[2 * c + 1];
+        cnt = g.tLeafCnt[c];
+    }
+
+    // top-down location of the leaf containing a point (FP64 bounds), as a cell index
+    SKG_D static int locate(const GridDev& g, double x, double y, double z)
+    {
+        int n = octreeLeafChild(g, x, y, z);
+        return n < 0 ? -1 : g.tCell[n];
     }
 
     SKG_D bool next(const GridDev& g)
@@ -121,56 +148,67 @@ struct OctreeFast : FastBase<Real>
         if (this->state == GS_UNKNOWN)
         {
             if (!this->moveInside(g.ext, g.eps)) return false;
-            node = octreeLeafChild(g, this->rx, this->ry, this->rz);
-            if (node < 0)
+            int c = locate(g, this->rx, this->ry, this->rz);
+            if (c < 0)
             {
                 this->state = GS_OUTSIDE;
                 return false;
             }
+            enter(g, c);
             if (this->ds > 0.) return true;
         }
-        const double* b = g.tBounds + 6 * static_cast<size_t>(node);
-        int sx = this->kx < 0.0 ? 0 : 3, sy = this->ky < 0.0 ? 1 : 4, sz = this->kz < 0.0 ? 2 : 5;
-        double xE = b[sx], yE = b[sy], zE = b[sz];
-        Real d;
+        double xE = this->kx < 0.0 ? ra.x : ra.w;
+        double yE = this->ky < 0.0 ? ra.y : rb.x;
+        double zE = this->kz < 0.0 ? ra.z : rb.y;
+        float d;
         int a = this->pickAxis(this->dist(xE, this->rx, this->ikx, this->kx), this->dist(yE, this->ry, this->iky, this->ky),
                                this->dist(zE, this->rz, this->ikz, this->kz), false, d);
         int wall = 2 * a + ((a == 0 ? this->kx : (a == 1 ? this->ky : this->kz)) < 0.0 ? 0 : 1);
-        this->m = g.tCell[node];
+        this->m = cell;
         this->ds = d;
+        segDens = rb.z;
         this->rebase(a, a == 0 ? xE : (a == 1 ? yE : zE), this->ds);
-        // first neighbour across the wall whose face contains the exit point (TreeNode::neighbor);
-        // the normal coordinate lies on the wall, so only the transverse ranges are tested
-        int nb = -1;
-        int e0 = g.tNbBegin[6 * node + wall], e1 = g.tNbBegin[6 * node + wall + 1];
-        for (int e = e0; e < e1; ++e)
+        // neighbour list of the exit wall: base + 9-bit cumulative offsets (all ones: no list)
+        int base = __float_as_int(rb.w);
+        bool listed = cnt != ~0ULL;
+        int e0 = base + static_cast<int>((cnt >> (9 * wall)) & 511);
+        int n = listed ? base + static_cast<int>((cnt >> (9 * (wall + 1))) & 511) - e0 : 0;
+        float pu = static_cast<float>(a == 0 ? this->ry : this->rx);
+        float pv = static_cast<float>(a == 2 ? this->ry : this->rz);
+        int old = cell, nb = -1;
         {
-            int cand = g.tNb[e];
-            const double* c = g.tBounds + 6 * static_cast<size_t>(cand);
-            bool in = (a == 0 || (this->rx >= c[0] && this->rx <= c[3])) && (a == 1 || (this->ry >= c[1] && this->ry <= c[4]))
-                      && (a == 2 || (this->rz >= c[2] && this->rz <= c[5]));
-            if (in)
+            for (int e = 0; e < n; ++e)
             {
-                nb = cand;
-                break;
+                int c = g.tLeafNb[e0 + e];
+                float4 qa = g.tLeaf[2 * c], qb = g.tLeaf[2 * c + 1];
+                float ulo = a == 0 ? qa.y : qa.x, uhi = a == 0 ? qb.x : qa.w;
+                float vlo = a == 2 ? qa.y : qa.z, vhi = a == 2 ? qb.x : qb.y;
+                if (pu >= ulo && pu <= uhi && pv >= vlo && pv <= vhi)
+                {
+                    nb = c;
+                    cell = c;
+                    ra = qa;
+                    rb = qb;
+                    cnt = g.tLeafCnt[c];
+                    break;
+                }
             }
         }
         if (nb < 0)
         {
-            // no neighbour (domain wall, or a corner exit): locate the point just beyond the wall
+            // no neighbour (domain wall, or an exit point on a cell edge): locate the point just beyond the wall
             double e = g.eps;
-            nb = octreeLeafChild(g, this->rx + this->kx * e, this->ry + this->ky * e, this->rz + this->kz * e);
+            nb = locate(g, this->rx + this->kx * e, this->ry + this->ky * e, this->rz + this->kz * e);
+            if (nb == old)
+            {
+                this->rx = nextafter(this->rx, (this->kx < 0.) ? -DBL_MAX : DBL_MAX);
+                this->ry = nextafter(this->ry, (this->ky < 0.) ? -DBL_MAX : DBL_MAX);
+                this->rz = nextafter(this->rz, (this->kz < 0.) ? -DBL_MAX : DBL_MAX);
+                nb = locate(g, this->rx, this->ry, this->rz);
+            }
+            if (nb >= 0 && nb != old) enter(g, nb);
         }
-        if (nb == node)
-        {
-            // still in the same node: escape to the next representable coordinates (as the reference)
-            this->rx = nextafter(this->rx, (this->kx < 0.) ? -DBL_MAX : DBL_MAX);
-            this->ry = nextafter(this->ry, (this->ky < 0.) ? -DBL_MAX : DBL_MAX);
-            this->rz = nextafter(this->rz, (this->kz < 0.) ? -DBL_MAX : DBL_MAX);
-            nb = octreeLeafChild(g, this->rx, this->ry, this->rz);
-        }
-        if (nb < 0 || nb == node) this->state = GS_OUTSIDE;
-        node = nb;
+        if (nb < 0 || nb == old) this->state = GS_OUTSIDE;
         return true;
     }
 };

@@ -55,7 +55,7 @@ __global__ void opticalDepthKernel(GridDev g, const double* dens, double section
     {
         if (w.m >= 0)
         {
-            t = xadd(t, xmul(xmul(section, dens[w.m]), w.ds));
+            t = xadd(t, xmul(xmul(section, w.density(dens)), w.ds));
             if (t >= taumax)
             {
                 t = INFINITY;

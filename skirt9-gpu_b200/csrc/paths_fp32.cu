@@ -17,7 +17,7 @@ cudaError_t launchTracePathsFP32(int precision, const GridDev& g, int n, const d
     switch (g.kind)
     {
         case 0: tracePathsKernel<CartesianFast<float>><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
-        case 1: tracePathsKernel<OctreeFast<float>><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
+        case 1: tracePathsKernel<OctreeLeaf32><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
         default: return cudaErrorNotSupported;
     }
     return cudaGetLastError();
@@ -32,7 +32,7 @@ cudaError_t launchOpticalDepthsFP32(int precision, const GridDev& g, const doubl
     switch (g.kind)
     {
         case 0: opticalDepthKernel<CartesianFast<float>><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
-        case 1: opticalDepthKernel<OctreeFast<float>><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
+        case 1: opticalDepthKernel<OctreeLeaf32><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
         default: return cudaErrorNotSupported;
     }
     return cudaGetLastError();

@@ -151,6 +151,24 @@ bool finiteAll(const double* v, size_t n)
     return true;
 }
 
+// copies the number densities into the FP32 leaf records of an octree grid
+__global__ void fillLeafDensityKernel(float4* leaf, const double* dens, int n)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < n) leaf[2 * c + 1].z = static_cast<float>(dens[c]);
+}
+
+int syncLeafDensity(skgpu_ctx* ctx)
+{
+    if (!ctx->hasGrid || ctx->g.kind != SKGPU_GRID_OCTREE || !ctx->g.tLeaf || !ctx->dens) return SKGPU_OK;
+    if (ctx->numCells != ctx->g.numCells) return SKGPU_OK;  // checked again at run time
+    int n = ctx->numCells;
+    fillLeafDensityKernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(const_cast<float4*>(ctx->g.tLeaf), ctx->dens, n);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->stream));
+    return SKGPU_OK;
+}
+
 // histories in flight at most; a larger range streams through the pool
 constexpr uint64_t POOL_MAX = 1u << 20;
 // wavefront passes per run at most (each history needs about two passes per scattering event)
@@ -378,8 +396,70 @@ int skgpu_upload_grid_octree(skgpu_ctx* ctx, int32_t num_nodes, const double* bo
     if ((rc = gridUpload<int>(ctx, &g.tChild, firstChild.data(), num_nodes))) return rc;
     if ((rc = gridUpload<int>(ctx, &g.tNbBegin, nb_begin, 6 * static_cast<size_t>(num_nodes) + 1))) return rc;
     if ((rc = gridUpload<int>(ctx, &g.tNb, nb_index, num_nb_index))) return rc;
+    // leaf-indexed FP32 records of the production walker (cell c <-> its leaf node): bounds, density
+    // (filled when the medium is uploaded), the base of the cell's neighbour list; per wall the
+    // positive-overlap neighbours in the reference's overlap order (zero-overlap entries, which only
+    // touch an edge, come last in the reference's lists and are left out: exit points on an edge
+    // are resolved by the top-down fallback)
+    std::vector<int> leafNode(numCells, -1);
+    for (int l = 0; l < num_nodes; ++l)
+        if (cell_index[l] >= 0) leafNode[cell_index[l]] = l;
+    std::vector<float4> leaf(2 * static_cast<size_t>(numCells));
+    std::vector<unsigned long long> cnt(numCells, 0);
+    std::vector<int> leafNb;
+    leafNb.reserve(static_cast<size_t>(numCells) * 8);
+    for (int c = 0; c < numCells; ++c)
+    {
+        int l = leafNode[c];
+        if (l < 0) return fail(ctx, SKGPU_ERR_ARG, "octree: cell index without leaf");
+        const double* b = bounds + 6 * static_cast<size_t>(l);
+        leaf[2 * c] = make_float4(static_cast<float>(b[0]), static_cast<float>(b[1]), static_cast<float>(b[2]),
+                                  static_cast<float>(b[3]));
+        int base = static_cast<int>(leafNb.size());
+        float baseBits;
+        std::memcpy(&baseBits, &base, sizeof base);
+        leaf[2 * c + 1] = make_float4(static_cast<float>(b[4]), static_cast<float>(b[5]), 0.f, baseBits);
+        // per wall the positive-overlap neighbours; 9-bit cumulative offsets of the 6 walls + end
+        // (a leaf with more than 511 such neighbours gets no list: its exits use the top-down search)
+        std::vector<int> lists[6];
+        size_t total = 0;
+        for (int w = 0; w < 6; ++w)
+        {
+            int a = w / 2, u = a == 0 ? 1 : 0, v = a == 2 ? 1 : 2;
+            for (int e = nb_begin[6 * static_cast<size_t>(l) + w]; e < nb_begin[6 * static_cast<size_t>(l) + w + 1]; ++e)
+            {
+                int nn = nb_index[e];
+                const double* q = bounds + 6 * static_cast<size_t>(nn);
+                double ou = std::min(b[3 + u], q[3 + u]) - std::max(b[u], q[u]);
+                double ov = std::min(b[3 + v], q[3 + v]) - std::max(b[v], q[v]);
+                if (!(ou > 0 && ov > 0) || cell_index[nn] < 0) continue;
+                lists[w].push_back(cell_index[nn]);
+            }
+            total += lists[w].size();
+        }
+        if (total > 511)
+        {
+            cnt[c] = ~0ULL;
+        }
+        else
+        {
+            unsigned long long off = 0;
+            for (int w = 0; w < 6; ++w)
+            {
+                cnt[c] |= off << (9 * w);
+                leafNb.insert(leafNb.end(), lists[w].begin(), lists[w].end());
+                off += lists[w].size();
+            }
+            cnt[c] |= off << 54;
+        }
+        if (leafNb.size() > 2147483647ULL) return fail(ctx, SKGPU_ERR_ARG, "octree: neighbour lists too long");
+    }
+    if (leafNb.empty()) leafNb.push_back(0);
+    if ((rc = gridUpload<float4>(ctx, &g.tLeaf, leaf.data(), leaf.size()))) return rc;
+    if ((rc = gridUpload<unsigned long long>(ctx, &g.tLeafCnt, cnt.data(), cnt.size()))) return rc;
+    if ((rc = gridUpload<int>(ctx, &g.tLeafNb, leafNb.data(), leafNb.size()))) return rc;
     ctx->hasGrid = true;
-    return SKGPU_OK;
+    return syncLeafDensity(ctx);
 }
 
 int skgpu_upload_grid_voronoi(skgpu_ctx* ctx, int32_t num_sites, const double* sites, const int32_t* nb_begin,
@@ -527,7 +607,7 @@ int skgpu_upload_medium(skgpu_ctx* ctx, int32_t num_cells, const double* number_
         ctx->numCells = num_cells;
     }
     CK(cudaMemcpy(ctx->dens, number_density, num_cells * sizeof(double), cudaMemcpyHostToDevice));
-    return SKGPU_OK;
+    return syncLeafDensity(ctx);
 }
 
 int skgpu_upload_dust_mix(skgpu_ctx* ctx, int32_t num_lambda, const double* lambda_borders, const double* sigma_ext,

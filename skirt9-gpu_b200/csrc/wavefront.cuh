@@ -166,8 +166,16 @@ SKG_D void beginPropagation(const Wave& w, int nxt, int slot, Rng& rng)
 // ---------------------------------------------------------------------------------------------
 // trace: walk every queued ray; one crossing per iteration, lanes refill from the queues
 // ---------------------------------------------------------------------------------------------
+// arithmetic of the walk accumulators: FP64 with separate roundings (reference order), or FP32
+SKG_D double aadd(double a, double b) { return xadd(a, b); }
+SKG_D double amul(double a, double b) { return xmul(a, b); }
+SKG_D double aexp(double x) { return exp(x); }
+SKG_D float aadd(float a, float b) { return a + b; }
+SKG_D float amul(float a, float b) { return a * b; }
+SKG_D float aexp(float x) { return __expf(x); }
+
 template<class Walker>
-__global__ void __launch_bounds__(256) traceKernel(Wave w, int cur)
+__global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(Wave w, int cur)
 {
     const Scene& sc = w.sc;
     const unsigned FULL = 0xffffffffu;
@@ -176,13 +184,14 @@ __global__ void __launch_bounds__(256) traceKernel(Wave w, int cur)
     unsigned total = n0 + n1 + n2 + n3;
     if (total == 0) return;
 
+    using Acc = typename Walker::Acc;  // FP64 (reference rounding) or FP32 optical depth and path length
     Walker wk;
     int kind = -1;  // -1: needs a task, -2: finished
     unsigned idx = 0;
     int slot = 0;
-    double tau = 0., s = 0., par = 0., lnExtBeg = 0., extBeg = 1., L = 0., sext = 0.;
+    Acc tau = 0, s = 0, par = 0, lnExtBeg = 0, extBeg = 1, L = 0, sext = 0;
     int nseg = 0, lastM = -1, ellRF = -1;
-    double lastS = 0.;
+    Acc lastS = 0;
     unsigned long long cross = 0, rfStores = 0;
     int guard = 0;
 
@@ -210,7 +219,7 @@ __global__ void __launch_bounds__(256) traceKernel(Wave w, int cur)
                     else { kind = K_FREE; idx = t - n0 - n1 - n2; }
                     const TaskBuf& b = w.q[cur][kind];
                     slot = b.slot[idx];
-                    sext = sc.mixExt[w.pk.ellMix[slot]];
+                    sext = static_cast<Acc>(sc.mixExt[w.pk.ellMix[slot]]);
                     tau = 0.;
                     s = 0.;
                     nseg = 0;
@@ -220,17 +229,17 @@ __global__ void __launch_bounds__(256) traceKernel(Wave w, int cur)
                     if (kind == K_PEEL)
                     {
                         const InstrDev& in = sc.instr[b.info[idx] & 0xFF];
-                        par = log(b.par[idx]) + 745.;  // taumax = log(L) + 745
+                        par = static_cast<Acc>(log(b.par[idx]) + 745.);  // taumax = log(L) + 745
                         wk.start(sc.g, b.x[idx], b.y[idx], b.z[idx], in.kobs[0], in.kobs[1], in.kobs[2]);
                     }
                     else
                     {
-                        par = b.par[idx];
+                        par = static_cast<Acc>(b.par[idx]);
                         wk.start(sc.g, w.pk.x[slot], w.pk.y[slot], w.pk.z[slot], w.pk.kx[slot], w.pk.ky[slot],
                                  w.pk.kz[slot]);
                         if (kind == K_PROP1)
                         {
-                            L = w.pk.L[slot];
+                            L = static_cast<Acc>(w.pk.L[slot]);
                             ellRF = sc.rfOn ? w.pk.ellRF[slot] : -1;
                             lnExtBeg = 0.;
                             extBeg = 1.;
@@ -248,15 +257,15 @@ __global__ void __launch_bounds__(256) traceKernel(Wave w, int cur)
         {
             cross++;
             int m = wk.m;
-            double ds = wk.ds;
+            Acc ds = static_cast<Acc>(wk.ds);
             if (kind == K_PEEL)
             {
                 if (m >= 0)
                 {
-                    tau = xadd(tau, xmul(xmul(sext, sc.dens[m]), ds));
+                    tau = aadd(tau, amul(amul(sext, static_cast<Acc>(wk.density(sc.dens))), ds));
                     if (tau >= par)
                     {
-                        tau = INFINITY;
+                        tau = static_cast<Acc>(INFINITY);
                         done = true;
                     }
                 }
@@ -265,16 +274,16 @@ __global__ void __launch_bounds__(256) traceKernel(Wave w, int cur)
             {
                 if (ds > 0.)
                 {
-                    if (m >= 0) tau = xadd(tau, xmul(xmul(sext, sc.dens[m]), ds));
+                    if (m >= 0) tau = aadd(tau, amul(amul(sext, static_cast<Acc>(wk.density(sc.dens))), ds));
                     nseg++;
                     if (ellRF >= 0)
                     {
-                        double lnExtEnd = -tau;
-                        double extEnd = exp(lnExtEnd);
+                        Acc lnExtEnd = -tau;
+                        Acc extEnd = aexp(lnExtEnd);
                         if (m >= 0)
                         {
-                            double Lds = L * lnmean4(extEnd, extBeg, lnExtEnd, lnExtBeg) * ds;
-                            atomicAdd(sc.rf + static_cast<size_t>(m) * sc.nrf + ellRF, Lds);
+                            Acc Lds = L * lnmean4(extEnd, extBeg, lnExtEnd, lnExtBeg) * ds;
+                            atomicAdd(sc.rf + static_cast<size_t>(m) * sc.nrf + ellRF, static_cast<double>(Lds));
                             rfStores++;
                         }
                         lnExtBeg = lnExtEnd;
@@ -287,9 +296,9 @@ __global__ void __launch_bounds__(256) traceKernel(Wave w, int cur)
                 // PROP2 keeps segments with ds > 0 (SpatialGridPath::addSegment); FREE uses every segment
                 if (kind == K_FREE || ds > 0.)
                 {
-                    double tau0 = tau, s0 = s;
-                    if (m >= 0) tau = xadd(tau, xmul(xmul(sext, sc.dens[m]), ds));
-                    s = xadd(s, ds);
+                    Acc tau0 = tau, s0 = s;
+                    if (m >= 0) tau = aadd(tau, amul(amul(sext, static_cast<Acc>(wk.density(sc.dens))), ds));
+                    s = aadd(s, ds);
                     lastM = m;
                     lastS = s;
                     if (par < tau)
@@ -297,7 +306,7 @@ __global__ void __launch_bounds__(256) traceKernel(Wave w, int cur)
                         // NR::interpolateLinLin (SKIRT/utils/NR.hpp:328-331)
                         const TaskBuf& b = w.q[cur][kind];
                         b.m[idx] = m;
-                        b.s[idx] = s0 + ((par - tau0) / (tau - tau0)) * (s - s0);
+                        b.s[idx] = static_cast<double>(s0 + ((par - tau0) / (tau - tau0)) * (s - s0));
                         b.found[idx] = 1;
                         kind = -1;
                         continue;
@@ -314,14 +323,14 @@ __global__ void __launch_bounds__(256) traceKernel(Wave w, int cur)
         {
             const TaskBuf& b = w.q[cur][kind];
             if (kind == K_PEEL)
-                b.tau[idx] = tau;
+                b.tau[idx] = static_cast<double>(tau);
             else if (kind == K_PROP1)
-                b.tau[idx] = nseg ? tau : 0.;
+                b.tau[idx] = nseg ? static_cast<double>(tau) : 0.;
             else
             {
                 // beyond the last segment: PROP2 uses the last segment, FREE escapes
                 b.m[idx] = lastM;
-                b.s[idx] = lastS;
+                b.s[idx] = static_cast<double>(lastS);
                 b.found[idx] = 0;
             }
             kind = -1;

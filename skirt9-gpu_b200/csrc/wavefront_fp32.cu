@@ -12,7 +12,7 @@ cudaError_t runWaveFP32(int gridKind, const Wave& w, int numSMs, cudaStream_t s,
     switch (gridKind)
     {
         case 0: return runWave<CartesianFast<float>>(w, numSMs, s, doneHost, passes, maxPasses);
-        case 1: return runWave<OctreeFast<float>>(w, numSMs, s, doneHost, passes, maxPasses);
+        case 1: return runWave<OctreeLeaf32>(w, numSMs, s, doneHost, passes, maxPasses);
     }
     return cudaErrorNotSupported;
 }
