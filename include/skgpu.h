@@ -182,6 +182,25 @@ int skgpu_set_options(skgpu_ctx* ctx, const skgpu_options* options);
  * storage, scattering peel-off, HG scattering) of histories [first, first+count) of a segment
  * of total_packets packets, adding into the device tallies. */
 int skgpu_run_primary(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t total_packets);
+/* Same life cycle as skgpu_run_primary for callers that must not allocate device memory while it
+ * runs: for example a host code that hands the GPU to this library between phases of its own
+ * memory manager, or that cannot afford the implicit device synchronisation of cudaMalloc/cudaFree
+ * in the middle of a segment. No counterpart in the reference (its GPU wrappers allocate per call).
+ * The call allocates nothing: its scratch (packet pool, task queues, per-history statistics
+ * buffers, control block) is a file-scope device array of SKGPU_NOALLOC_SCRATCH_BYTES that every
+ * GPU loading the library holds until exit, and it launches its passes directly instead of
+ * building a CUDA graph. Limits: at most SKGPU_NOALLOC_MAX_SLOTS histories in flight (larger ranges
+ * stream through them, only slower) and SKGPU_NOALLOC_MAX_GROUPS observer groups; scenes beyond
+ * that are rejected with SKGPU_ERR_ARG. Everything the run reads or writes besides the scratch
+ * (scene, tallies, radiation-field tally) must have been set up by the upload calls, skgpu_set_options
+ * and skgpu_clear_tallies beforehand. The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) with that device current; make that first call before any stream
+ * capture. Calls share the one array and the call re-initialises what must start at zero; calls that
+ * overlap on the GPU (other threads, other contexts on the same device) race on it. */
+#define SKGPU_NOALLOC_MAX_SLOTS 32768
+#define SKGPU_NOALLOC_MAX_GROUPS 4
+#define SKGPU_NOALLOC_SCRATCH_BYTES (48u * 1024u * 1024u)
+int skgpu_run_primary_noalloc(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t total_packets);
 /* Adds the device tallies of one instrument into the caller's arrays and leaves the device
  * tallies untouched. ifu: num_wavelength_bins*npix (index l + ell*npix), sed: num_wavelength_bins,
  * stats (may be NULL): 5 planes of ifu size then 5 planes of sed size (sum w^k, k=0..4). */

@@ -7,6 +7,8 @@
 // cell search.
 #include <algorithm>
 #include <cmath>
+#include <mutex>
+#include <type_traits>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -775,27 +777,9 @@ int skgpu_set_options(skgpu_ctx* ctx, const skgpu_options* options)
 // run and tallies
 // ------------------------------------------------------------------------------------------------
 
-int skgpu_run_primary(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t total_packets)
+// scene record of the kernels from the context's uploads
+static Scene sceneOf(const skgpu_ctx* ctx)
 {
-    if (!ctx) return SKGPU_ERR_ARG;
-    if (!ctx->hasGrid) return fail(ctx, SKGPU_ERR_STATE, "run: no grid uploaded");
-    if (!ctx->dens || ctx->numCells != ctx->g.numCells) return fail(ctx, SKGPU_ERR_STATE, "run: medium does not match the grid");
-    if (!ctx->nmix) return fail(ctx, SKGPU_ERR_STATE, "run: no dust mix uploaded");
-    if (ctx->srcHost.empty()) return fail(ctx, SKGPU_ERR_STATE, "run: no sources uploaded");
-    if (ctx->opt.store_radiation_field && !ctx->nrf) return fail(ctx, SKGPU_ERR_STATE, "run: radiation field requested without RF grid");
-    if (total_packets == 0 || first + count > total_packets) return fail(ctx, SKGPU_ERR_ARG, "run: history range outside the segment");
-    CK(cudaSetDevice(ctx->device));
-    if (ctx->opt.store_radiation_field)
-    {
-        size_t len = static_cast<size_t>(ctx->numCells) * ctx->nrf;
-        if (ctx->rfLen != len)
-        {
-            devFree(ctx->rf);
-            CK(devAlloc(&ctx->rf, len));
-            CK(cudaMemset(ctx->rf, 0, len * sizeof(double)));
-            ctx->rfLen = len;
-        }
-    }
     Scene p{};
     p.g = ctx->g;
     p.dens = ctx->dens;
@@ -814,27 +798,41 @@ int skgpu_run_primary(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t t
     p.minWeightRed = ctx->opt.min_weight_reduction;
     p.pathLengthBias = ctx->opt.path_length_bias;
     p.seed = ctx->opt.seed;
+    return p;
+}
 
-    // packet pool and task queues, sized for up to POOL_MAX histories in flight
-    int anyStats = 0;
-    for (const InstrDev& d : ctx->instrHost) anyStats |= d.stats;
-    int groups = 0;
-    for (const InstrDev& d : ctx->instrHost) groups += d.same ? 0 : 1;
-    int P = static_cast<int>(std::min<uint64_t>(std::max<uint64_t>(count, 1), POOL_MAX));
-    int rc = ensureWaveBuffers(ctx, P, std::max(groups, 1), anyStats);
-    if (rc) return rc;
-    Wave w = ctx->wave;
-    w.sc = p;
-    w.P = P;
-    w.first = first;
-    w.count = count;
-    w.anyStats = anyStats;
+static int checkRunnable(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t total_packets)
+{
+    if (!ctx->hasGrid) return fail(ctx, SKGPU_ERR_STATE, "run: no grid uploaded");
+    if (!ctx->dens || ctx->numCells != ctx->g.numCells) return fail(ctx, SKGPU_ERR_STATE, "run: medium does not match the grid");
+    if (!ctx->nmix) return fail(ctx, SKGPU_ERR_STATE, "run: no dust mix uploaded");
+    if (ctx->srcHost.empty()) return fail(ctx, SKGPU_ERR_STATE, "run: no sources uploaded");
+    if (ctx->opt.store_radiation_field && !ctx->nrf) return fail(ctx, SKGPU_ERR_STATE, "run: radiation field requested without RF grid");
+    if (total_packets == 0 || first + count > total_packets) return fail(ctx, SKGPU_ERR_ARG, "run: history range outside the segment");
+    return SKGPU_OK;
+}
+
+static void waveShape(const skgpu_ctx* ctx, int& groups, int& anyStats)
+{
+    anyStats = 0;
+    groups = 0;
+    for (const InstrDev& d : ctx->instrHost)
+    {
+        anyStats |= d.stats;
+        groups += d.same ? 0 : 1;
+    }
+    groups = std::max(groups, 1);
+}
+
+// runs the wavefront on prepared buffers and collects the counters and status of the run
+static int runAndCollect(skgpu_ctx* ctx, const Wave& w, bool useGraph)
+{
     int prec = ctx->opt.precision;
     long long passes = 0;
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
     cudaError_t e = prec == SKGPU_PREC_FP64_EXACT
-                        ? runWaveFP64(ctx->g.kind, w, ctx->numSMs, ctx->stream, ctx->doneHost, &passes, MAX_PASSES)
-                        : runWaveFP32(ctx->g.kind, w, ctx->numSMs, ctx->stream, ctx->doneHost, &passes, MAX_PASSES);
+                        ? runWaveFP64(ctx->g.kind, w, ctx->numSMs, ctx->stream, ctx->doneHost, &passes, MAX_PASSES, useGraph)
+                        : runWaveFP32(ctx->g.kind, w, ctx->numSMs, ctx->stream, ctx->doneHost, &passes, MAX_PASSES, useGraph);
     if (e == cudaErrorNotSupported) return fail(ctx, SKGPU_ERR_UNSUPPORTED, "run: no FP32 walker for this grid kind");
     if (e == cudaErrorLaunchTimeout) return fail(ctx, SKGPU_ERR_TIMEOUT, "run: pass limit reached before all histories finished");
     if (e != cudaSuccess) return fail(ctx, SKGPU_ERR_CUDA, std::string("run: ") + cudaGetErrorString(e));
@@ -844,7 +842,7 @@ int skgpu_run_primary(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t t
     CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
     ctx->lastMs = ms;
     Control ctl;
-    CK(cudaMemcpy(&ctl, ctx->wave.ctl, sizeof ctl, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&ctl, w.ctl, sizeof ctl, cudaMemcpyDeviceToHost));
     int errFlag = ctl.err;
     ctx->lastCounters.histories = ctl.counters[0];
     ctx->lastCounters.crossings = ctl.counters[1];
@@ -854,11 +852,144 @@ int skgpu_run_primary(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t t
     ctx->lastCounters.stats_overflows = ctl.counters[5];
     ctx->lastCounters.kernel_launches = static_cast<uint64_t>(passes) * 7 + 1;
     ctx->lastPasses = passes;
-    if (count > 0 && ctl.done != count) return fail(ctx, SKGPU_ERR_DEVICE, "run: not every history finished");
+    if (w.count > 0 && ctl.done != w.count) return fail(ctx, SKGPU_ERR_DEVICE, "run: not every history finished");
     if (errFlag & 4) return fail(ctx, SKGPU_ERR_TIMEOUT, "run: a traversal exceeded its segment guard");
     if (errFlag & 8) return fail(ctx, SKGPU_ERR_TIMEOUT, "run: a history exceeded the scattering-event guard");
     if (errFlag) return fail(ctx, SKGPU_ERR_DEVICE, "run: interaction point outside the grid (device check)");
     return SKGPU_OK;
+}
+
+// allocates the radiation-field tally for the current medium and RF grid if it does not exist yet
+static int ensureRadiationField(skgpu_ctx* ctx)
+{
+    if (!ctx->opt.store_radiation_field || !ctx->nrf || !ctx->numCells) return SKGPU_OK;
+    size_t len = static_cast<size_t>(ctx->numCells) * ctx->nrf;
+    if (ctx->rfLen == len) return SKGPU_OK;
+    devFree(ctx->rf);
+    CK(devAlloc(&ctx->rf, len));
+    CK(cudaMemset(ctx->rf, 0, len * sizeof(double)));
+    ctx->rfLen = len;
+    return SKGPU_OK;
+}
+
+int skgpu_run_primary(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t total_packets)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    int rc = checkRunnable(ctx, first, count, total_packets);
+    if (rc) return rc;
+    CK(cudaSetDevice(ctx->device));
+    if ((rc = ensureRadiationField(ctx))) return rc;
+    // packet pool and task queues, sized for up to POOL_MAX histories in flight
+    int groups, anyStats;
+    waveShape(ctx, groups, anyStats);
+    int P = static_cast<int>(std::min<uint64_t>(std::max<uint64_t>(count, 1), POOL_MAX));
+    if ((rc = ensureWaveBuffers(ctx, P, groups, anyStats))) return rc;
+    Wave w = ctx->wave;
+    w.sc = sceneOf(ctx);
+    w.P = P;
+    w.first = first;
+    w.count = count;
+    w.anyStats = anyStats;
+    return runAndCollect(ctx, w, true);
+}
+
+// ------------------------------------------------------------------------------------------------
+// run without allocations: the wavefront scratch comes from a file-scope device array
+// ------------------------------------------------------------------------------------------------
+
+// Scratch of skgpu_run_primary_noalloc: packet pool, task queues and control block of at most
+// NOALLOC_SLOTS histories in flight, NOALLOC_GROUPS observer groups, with statistics buffers. Every
+// GPU that loads this library holds it until the process exits.
+static __device__ __align__(256) unsigned char g_noallocScratch[SKGPU_NOALLOC_SCRATCH_BYTES];
+
+// lays the wavefront buffers for P slots out in a scratch area (base may be null: size only)
+static size_t carveWave(Wave& w, unsigned char* base, int P, int groups, int stats)
+{
+    size_t off = 0;
+    auto take = [&](auto** p, size_t count) {
+        using T = std::remove_pointer_t<std::remove_reference_t<decltype(*p)>>;
+        off = (off + 255) & ~static_cast<size_t>(255);
+        *p = base ? reinterpret_cast<T*>(base + off) : nullptr;
+        off += std::max<size_t>(count, 1) * sizeof(T);
+    };
+    PacketPool& k = w.pk;
+    double** dbl[] = {&k.x, &k.y, &k.z, &k.kx, &k.ky, &k.kz, &k.L, &k.Lth, &k.lam, &k.tauPath, &k.rngSpare};
+    for (double** d : dbl) take(d, P);
+    int** ints[] = {&k.rngHas, &k.nscatt, &k.ellMix, &k.ellRF, &k.nstat, &k.freeSlots};
+    for (int** d : ints) take(d, P);
+    take(&k.hist, P);
+    take(&k.rngCtr, P);
+    size_t ns = stats ? static_cast<size_t>(P) * STATS_CAP : 1;
+    take(&k.skey, ns);
+    take(&k.sw, ns);
+    for (int b = 0; b < 2; ++b)
+        for (int kind = 0; kind < NUM_KINDS; ++kind)
+        {
+            TaskBuf& t = w.q[b][kind];
+            t = TaskBuf{};
+            size_t cap = kind == K_PEEL ? static_cast<size_t>(P) * groups : static_cast<size_t>(P);
+            take(&t.slot, cap);
+            take(&t.par, cap);
+            if (kind == K_PEEL)
+            {
+                take(&t.info, cap);
+                take(&t.x, cap);
+                take(&t.y, cap);
+                take(&t.z, cap);
+            }
+            if (kind == K_PEEL || kind == K_PROP1)
+                take(&t.tau, cap);
+            else
+            {
+                take(&t.m, cap);
+                take(&t.s, cap);
+                take(&t.found, cap);
+            }
+        }
+    take(&w.ctl, 1);
+    return off;
+}
+
+int skgpu_run_primary_noalloc(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t total_packets)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    int rc = checkRunnable(ctx, first, count, total_packets);
+    if (rc) return rc;
+    int groups, anyStats;
+    waveShape(ctx, groups, anyStats);
+    if (groups > SKGPU_NOALLOC_MAX_GROUPS)
+        return fail(ctx, SKGPU_ERR_ARG, "run_noalloc: more than " + std::to_string(SKGPU_NOALLOC_MAX_GROUPS)
+                                            + " observer groups exceed the static scratch");
+    if (ctx->opt.store_radiation_field && ctx->rfLen != static_cast<size_t>(ctx->numCells) * ctx->nrf)
+        return fail(ctx, SKGPU_ERR_STATE, "run_noalloc: the radiation-field tally is not allocated yet "
+                                          "(call skgpu_clear_tallies after skgpu_set_options)");
+    Wave probe{};
+    if (carveWave(probe, nullptr, SKGPU_NOALLOC_MAX_SLOTS, groups, anyStats) > sizeof(g_noallocScratch))
+        return fail(ctx, SKGPU_ERR_ARG, "run_noalloc: scene needs more scratch than the static array holds");
+    CK(cudaSetDevice(ctx->device));
+    // the host-side name of the array is not a device address: ask the runtime once per device
+    static std::mutex mtx;
+    static void* addr[256] = {};
+    if (ctx->device < 0 || ctx->device >= 256) return fail(ctx, SKGPU_ERR_ARG, "run_noalloc: device index out of range");
+    {
+        std::lock_guard<std::mutex> lock(mtx);
+        if (!addr[ctx->device])
+        {
+            void* p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_noallocScratch);
+            if (e != cudaSuccess || !p)
+                return fail(ctx, SKGPU_ERR_CUDA, std::string("run_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+            addr[ctx->device] = p;
+        }
+    }
+    Wave w{};
+    carveWave(w, static_cast<unsigned char*>(addr[ctx->device]), SKGPU_NOALLOC_MAX_SLOTS, groups, anyStats);
+    w.sc = sceneOf(ctx);
+    w.P = static_cast<int>(std::min<uint64_t>(std::max<uint64_t>(count, 1), SKGPU_NOALLOC_MAX_SLOTS));
+    w.first = first;
+    w.count = count;
+    w.anyStats = anyStats;
+    return runAndCollect(ctx, w, false);
 }
 
 static int addInto(skgpu_ctx* ctx, const double* dev, size_t n, double* host)
@@ -915,6 +1046,8 @@ int skgpu_clear_tallies(skgpu_ctx* ctx)
 {
     if (!ctx) return SKGPU_ERR_ARG;
     CK(cudaSetDevice(ctx->device));
+    int rc = ensureRadiationField(ctx);
+    if (rc) return rc;
     for (const InstrDev& d : ctx->instrHost)
     {
         size_t n = static_cast<size_t>(d.nbins) * d.npx * d.npy;

@@ -33,12 +33,14 @@ void enqueuePass(const Wave& w, int cur, const WaveLaunch& L, cudaStream_t s)
     launchKernel<<<L.shadeBlocks, L.threads, 0, s>>>(w, nxt);
 }
 
-// Runs histories [w.first, w.first + w.count). `doneHost` is pinned host memory for the progress
-// word. Returns a CUDA error, or cudaErrorLaunchTimeout (mapped to SKGPU_ERR_TIMEOUT) when the pass
-// limit is reached without finishing. `passes` receives the number of passes run.
+// Runs histories [w.first, w.first + w.count). `doneHost` receives the progress word (pinned host
+// memory for the graph path). With `useGraph` the passes are captured once into a CUDA graph of
+// four passes and replayed; without it the same kernels are launched directly (no graph objects are
+// created). Returns a CUDA error, or cudaErrorLaunchTimeout (mapped to SKGPU_ERR_TIMEOUT) when the
+// pass limit is reached without finishing. `passes` receives the number of passes run.
 template<class Walker>
 cudaError_t runWave(const Wave& w, int numSMs, cudaStream_t s, unsigned long long* doneHost, long long* passes,
-                    long long maxPasses)
+                    long long maxPasses, bool useGraph)
 {
     WaveLaunch L;
     L.threads = 256;
@@ -50,28 +52,37 @@ cudaError_t runWave(const Wave& w, int numSMs, cudaStream_t s, unsigned long lon
     if (e != cudaSuccess) return e;
     if (w.count == 0) return cudaStreamSynchronize(s);
 
+    const int passesPerBatch = 4;  // even: the buffer parity returns to 0 after every batch
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
-    if (e != cudaSuccess) return e;
-    const int passesPerGraph = 4;  // even: the buffer parity returns to 0 after every replay
-    for (int k = 0; k < passesPerGraph; ++k) enqueuePass<Walker>(w, k & 1, L, s);
-    e = cudaStreamEndCapture(s, &graph);
-    if (e != cudaSuccess) return e;
-    e = cudaGraphInstantiate(&exec, graph, 0);
-    if (e != cudaSuccess)
+    if (useGraph)
     {
-        cudaGraphDestroy(graph);
-        return e;
+        e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return e;
+        for (int k = 0; k < passesPerBatch; ++k) enqueuePass<Walker>(w, k & 1, L, s);
+        e = cudaStreamEndCapture(s, &graph);
+        if (e != cudaSuccess) return e;
+        e = cudaGraphInstantiate(&exec, graph, 0);
+        if (e != cudaSuccess)
+        {
+            cudaGraphDestroy(graph);
+            return e;
+        }
     }
     const size_t doneOffset = offsetof(Control, done);
     unsigned long long lastDone = 0;
     long long lastProgress = 0;
     while (e == cudaSuccess)
     {
-        e = cudaGraphLaunch(exec, s);
+        if (useGraph)
+            e = cudaGraphLaunch(exec, s);
+        else
+        {
+            for (int k = 0; k < passesPerBatch; ++k) enqueuePass<Walker>(w, k & 1, L, s);
+            e = cudaGetLastError();
+        }
         if (e != cudaSuccess) break;
-        *passes += passesPerGraph;
+        *passes += passesPerBatch;
         e = cudaMemcpyAsync(doneHost, reinterpret_cast<char*>(w.ctl) + doneOffset, sizeof(unsigned long long),
                             cudaMemcpyDeviceToHost, s);
         if (e != cudaSuccess) break;
@@ -91,8 +102,8 @@ cudaError_t runWave(const Wave& w, int numSMs, cudaStream_t s, unsigned long lon
             break;
         }
     }
-    cudaGraphExecDestroy(exec);
-    cudaGraphDestroy(graph);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
     return e;
 }
 

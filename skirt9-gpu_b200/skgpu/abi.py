@@ -353,3 +353,17 @@ def build_octree(geometry, params, extent, min_level, max_level, max_dust_fracti
     out["nb_index"] = out["nb_index"][:nb]
     out["extent"] = np.array(extent, float)
     return out
+
+
+EXPORTED += ["skgpu_run_primary_noalloc"]
+
+
+def run_primary_noalloc(be, first, count, total):
+    """skgpu_run_primary_noalloc through a Backend of the CUDA library: the same segment as
+    run_primary, with its scratch in the library's static device array (no allocation)."""
+    f = be.lib.skgpu_run_primary_noalloc
+    f.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64]
+    f.restype = C.c_int
+    rc = f(be.ctx, int(first), int(count), int(total))
+    if rc != OK:
+        raise SkgpuError(rc, be.fn["last_error"](be.ctx).decode())
