@@ -3,11 +3,14 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
 
 One step = one primary-emission segment of the workload's packets through the C ABI
-(skgpu_run_primary): launch, emission peel-off, forced-scattering propagation, scattering
-peel-off and HG scattering for every history. `value` is device time (CUDA events on the launch
-stream, L2 flushed between steps); `e2e` is measured through the same C ABI with host buffers
-(medium state uploaded, tallies read back to the host every step). Under torchrun each rank
-traces its own contiguous range of history indices (weak scaling; no data-path collective).
+(skgpu_run_primary): launch, emission peel-off, forced-scattering propagation, radiation-field
+storage, scattering peel-off and HG scattering for every history. `value` is device time (CUDA
+events on the launch stream, L2 flushed between steps); `e2e` is measured through the same C ABI
+with host buffers (medium state uploaded from pinned memory, every instrument tally and the
+radiation field added into the caller's host arrays, every step). The roofline is that of the
+traversal kernel, whose launches are bracketed by CUDA events inside the timed steps. Under
+torchrun each rank traces its own contiguous range of history indices (weak scaling; no
+data-path collective).
 """
 import argparse
 import json
@@ -35,7 +38,7 @@ WORKLOADS = {
     "galaxy": ("stellar exp. disk (hR 4 kpc, hz 0.35 kpc) + Sersic n=4 bulge (Re 1 kpc, B/T 0.2), dust exp. disk "
                "(hR 6 kpc, hz 0.2 kpc, face-on tau_V=1) on a TreeSpatialGrid octree (max level 8, dust fraction 1e-6, "
                "~5.1e5 leaves), 100 log wavelengths 0.1-10 um with power-law dust, three 512^2 frames at 0/60/90 deg, "
-               "radiation field stored on 100 bins; 1e8-packet run split into steps", 10_000_000),
+               "radiation field stored on 100 bins; one step = the 1e8-packet primary-emission segment", 100_000_000),
 }
 
 
@@ -97,13 +100,20 @@ def build_scene(name):
     raise SystemExit(f"unknown workload {name}")
 
 
+BYTES_PER_CROSSING = {0: 4, 1: 64, 2: 284, 3: 84}  # Cartesian, octree, Voronoi, tetra
+
+
 def algorithmic_bytes(counters, grid_kind):
-    """Bytes per launch by the unit costs of the measurement plan: per cell crossing the grid's
+    """Bytes of one segment by the unit costs of the measurement plan: per cell crossing the grid's
     record (Cartesian 4 B, octree 64 B, Voronoi 284 B, tetra 84 B), 128 B per interaction event
     (packet state read + write), 16 B per peel-off detection and per radiation-field update."""
-    per_cross = {0: 4, 1: 64, 2: 284, 3: 84}[grid_kind]
-    return (per_cross * counters["crossings"] + 128 * counters["scatterings"]
+    return (BYTES_PER_CROSSING[grid_kind] * counters["crossings"] + 128 * counters["scatterings"]
             + 16 * (counters["peel_detections"] + counters["rf_stores"]))
+
+
+def trace_algorithmic_bytes(counters, grid_kind):
+    """The traversal kernel's share: cell crossings and radiation-field updates."""
+    return BYTES_PER_CROSSING[grid_kind] * counters["crossings"] + 16 * counters["rf_stores"]
 
 
 def reference_run(scene_ski, npp, threads):
@@ -196,8 +206,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="galaxy", choices=sorted(WORKLOADS))
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32"],
+                    help="traversal precision: fp32 (production) or fp64 (reference operation order)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--packets", type=int, default=0, help="packets per step per GPU (default: the workload's)")
     args = ap.parse_args()
 
@@ -237,10 +249,12 @@ def main():
 
     for _ in range(args.warmup):
         step()
+    abi.set_stage_timing(be, 1)  # CUDA events around every traversal-kernel launch
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     ms = []
+    trace_ms, trace_launches = 0.0, 0
     counters = None
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
@@ -248,7 +262,11 @@ def main():
             torch.cuda.synchronize()
             ms.append(step())
             counters = be.counters()
+            t_ms, t_n = abi.last_stage_times(be)["trace"]
+            trace_ms += t_ms
+            trace_launches += t_n
     torch.cuda.synchronize()
+    abi.set_stage_timing(be, 0)
     total_ms = float(sum(ms))
     if dist:
         t = torch.tensor([total_ms], device=f"cuda:{local}")
@@ -256,38 +274,55 @@ def main():
         total_ms = float(t.item())
     value = npp_total * args.steps / (total_ms / 1e3)
 
-    # end to end through the C ABI with host buffers: medium state in, tallies out, every step
-    dens = np.ascontiguousarray(sc.density)
-    sizes = [sc.instrument_size(i) for i in range(len(sc.instruments))]
-    h2d = dens.nbytes
-    d2h = sum(8 * n for n in sizes) + sum(40 * n for i, n in enumerate(sizes) if sc.instruments[i].get("stats"))
-    be.clear_tallies()
-    e2e_times = []
-    for _ in range(max(1, min(args.steps, 3))):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        be.upload_medium(dens)
-        be.run_primary(first, per_gpu, npp_total)
-        for i, n in enumerate(sizes):
-            be.fetch_instrument(i, n, stats=bool(sc.instruments[i].get("stats")))
-        torch.cuda.synchronize()
-        e2e_times.append(time.perf_counter() - t0)
-    e2e_s = statistics.median(e2e_times)
-    if dist:
-        t = torch.tensor([e2e_s], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    # end to end through the C ABI with host buffers, as the SKIRT bridge uses it: the medium state
+    # goes in from pinned host memory, every tally (instrument totals and statistics, radiation
+    # field) is added into the caller's preallocated host arrays, every step
+    e2e = None
+    if not args.no_e2e:
+        dens = torch.from_numpy(np.ascontiguousarray(sc.density)).pin_memory().numpy()
+        sizes = [sc.instrument_size(i) for i in range(len(sc.instruments))]
+        stats = [bool(sc.instruments[i].get("stats")) for i in range(len(sizes))]
+        host = [(np.zeros(n), np.zeros(5 * n) if st else None) for n, st in zip(sizes, stats)]
+        rf_len = sc.rf_length()
+        rf_host = np.zeros(rf_len) if rf_len else None
+        h2d = dens.nbytes
+        d2h = sum(8 * n + (40 * n if st else 0) for n, st in zip(sizes, stats)) + 8 * rf_len
+        e2e_times = []
+        for _ in range(max(1, min(args.steps, 2))):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            be.clear_tallies()
+            be.upload_medium(dens)
+            be.run_primary(first, per_gpu, npp_total)
+            for i, n in enumerate(sizes):
+                be.fetch_instrument(i, n, stats=stats[i], out=host[i][0], out_stats=host[i][1])
+            if rf_len:
+                be.fetch_radiation_field(rf_len, out=rf_host)
+            torch.cuda.synchronize()
+            e2e_times.append(time.perf_counter() - t0)
+        e2e_s = statistics.median(e2e_times)
+        if dist:
+            t = torch.tensor([e2e_s], device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e = {"value": npp_total / e2e_s, "unit": "packets/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
 
     if rank == 0:
         peak, peak_kind = peaks()
         launch_ms = total_ms / args.steps
-        alg = algorithmic_bytes(counters, sc.grid["kind"])
-        achieved = alg / (launch_ms / 1e3) / 1e9
+        # roofline of the dominant kernel: its algorithmic bytes per launch over its average launch
+        # duration (CUDA events on the launch stream, timed steps)
+        kind = sc.grid["kind"]
+        trace_bytes_per_launch = trace_algorithmic_bytes(counters, kind) / max(1, trace_launches / args.steps)
+        trace_avg_ms = trace_ms / max(1, trace_launches)
+        achieved = trace_bytes_per_launch / (trace_avg_ms / 1e3) / 1e9
         traffic = None
-        prof = os.path.join(ROOT, "profiles", f"lifecycle_{name}.json")
+        prof = os.path.join(ROOT, "profiles", f"trace_kernel_{name}_{args.precision}.json")
         if os.path.exists(prof):
             with open(prof) as f:
-                traffic = json.load(f).get("dram_bytes_per_launch")
+                ratio = json.load(f).get("dram_bytes_per_algorithmic_byte")
+            if ratio:
+                traffic = ratio * trace_bytes_per_launch
         line = {
             "metric": "packets/s on 1 B200", "value": value, "unit": "packets/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": launch_ms, "higher_is_better": True,
@@ -297,11 +332,12 @@ def main():
                        "traversal": args.precision, "l2": "flushed between steps (256 MB write)",
                        "parallelism": f"history ranges x{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "skg::traceKernel", "algorithmic_bytes_per_launch": alg},
+                         "traffic": traffic, "peak_kind": peak_kind, "kernel": "skg::traceKernel",
+                         "launches_per_step": trace_launches / args.steps, "avg_launch_ms": trace_avg_ms,
+                         "algorithmic_bytes_per_launch": trace_bytes_per_launch,
+                         "share_of_step": trace_ms / max(total_ms, 1e-9)},
             "clocks": clk.summary(),
-            "e2e": {"value": npp_total / e2e_s, "unit": "packets/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
+            "e2e": e2e,
             "gpu_launches": int(counters["kernel_launches"]) * args.steps,
             "counters_per_step": counters,
         }

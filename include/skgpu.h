@@ -216,6 +216,21 @@ int skgpu_get_counters(skgpu_ctx* ctx, skgpu_counters* out);
 /* Milliseconds of device time of the last skgpu_run_primary (CUDA events on the launch stream). */
 int skgpu_last_run_ms(skgpu_ctx* ctx, double* ms);
 
+/* ---- stage timing (measurement aid; no reference counterpart) ----
+ * Level 1 brackets every launch of the traversal kernel of skgpu_run_primary with CUDA events on the
+ * launch stream, level 2 every stage kernel; 0 (the default) records nothing. skgpu_last_stage_times
+ * returns, per stage of the last skgpu_run_primary, the summed device milliseconds and the number of
+ * launches (arrays of SKGPU_NUM_STAGES; either pointer may be NULL). */
+#define SKGPU_STAGE_TRACE 0  /* traversal of peel-off and propagation rays (+ radiation-field updates) */
+#define SKGPU_STAGE_PEEL 1   /* detection of finished peel-off rays */
+#define SKGPU_STAGE_PROP1 2  /* forced sampling of the interaction optical depth */
+#define SKGPU_STAGE_PROP2 3  /* forced interaction: weight, position, scattering, peel-off rays */
+#define SKGPU_STAGE_FREE 4   /* non-forced interaction */
+#define SKGPU_STAGE_LAUNCH 5 /* refill of free packet slots with new histories */
+#define SKGPU_NUM_STAGES 6
+int skgpu_set_stage_timing(skgpu_ctx* ctx, int32_t level);
+int skgpu_last_stage_times(skgpu_ctx* ctx, double* ms, uint64_t* launches);
+
 /* ---- path segments (replaces GpuAcceleration::set*SpatialGridPath, GpuAcceleration.hpp) ----
  * For each ray (x,y,z,kx,ky,kz) the segments (m, ds) the grid's PathSegmentGenerator returns,
  * up to max_segments per ray; count[i] < 0 flags truncation (-n segments generated). */

@@ -42,7 +42,9 @@ SKG_HD void mulhilo32(uint32_t a, uint32_t b, uint32_t& hi, uint32_t& lo)
 SKG_HD U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1)
 {
     const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#ifdef __CUDA_ARCH__
 #pragma unroll
+#endif
     for (int r = 0; r < 10; ++r)
     {
         uint32_t hi0, lo0, hi1, lo1;

@@ -40,9 +40,8 @@ struct GridDev
     // leaf-indexed records of the FP32 walker: per cell two float4 (FP32 bounds, FP32 number
     // density, neighbour-list base), per cell the cumulative offsets of its 6 walls in its neighbour list (9 bits each), and
     // the neighbour cells (positive overlap only, overlap-sorted) of every leaf wall
-    const float4* tLeaf;
-    const unsigned long long* tLeafCnt;
-    const int* tLeafNb;
+    const float4* tLeaf;   // 64-byte leaf records of the FP32 walker (4 float4 per cell)
+    const int* tLeafNb;    // their positive-overlap neighbour lists (cell indices)
 
     // Voronoi: sites, neighbour CSR (negative = wall), uniform site-search grid
     const double* vSites;

@@ -110,13 +110,17 @@ struct CartesianFast : FastBase<Real>
 // neighbour-list base) and wall counts are held in registers; a crossing loads the ids of the exit
 // wall's neighbours and their records until one contains the exit point, and that record becomes
 // the current one (two dependent loads per crossing, all from a working set that stays in L2).
+// resident 256-thread blocks per SM requested for the FP32 octree trace kernel (register budget)
+#ifndef SKG_OCTREE32_MIN_BLOCKS
+#define SKG_OCTREE32_MIN_BLOCKS 4
+#endif
+
 struct OctreeLeaf32 : FastBase<float>
 {
     using Acc = float;
-    static constexpr int kMinBlocks = 4;
+    static constexpr int kMinBlocks = SKG_OCTREE32_MIN_BLOCKS;
     int cell;
-    float4 ra, rb;                 // record of the current cell
-    unsigned long long cnt;        // cumulative wall offsets of the neighbour list, 9 bits each
+    float4 ra, rb;                 // bounds, density and list base of the current cell (record words 0-1)
     float segDens;                 // density of the cell of the segment just returned
 
     SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz)
@@ -130,9 +134,8 @@ struct OctreeLeaf32 : FastBase<float>
     SKG_D void enter(const GridDev& g, int c)
     {
         cell = c;
-        ra = g.tLeaf[2 * c];
-        rb = g.tLeaf[2 * c + 1];
-        cnt = g.tLeafCnt[c];
+        ra = __ldg(g.tLeaf + 4 * static_cast<size_t>(c));
+        rb = __ldg(g.tLeaf + 4 * static_cast<size_t>(c) + 1);
     }
 
     // top-down location of the leaf containing a point (FP64 bounds), as a cell index
@@ -140,6 +143,13 @@ struct OctreeLeaf32 : FastBase<float>
     {
         int n = octreeLeafChild(g, x, y, z);
         return n < 0 ? -1 : g.tCell[n];
+    }
+
+    // half-open interval test in the direction of travel: a point on the boundary belongs to the
+    // interval the ray moves into (closed on both ends for a zero direction component)
+    SKG_D static bool within(float p, float lo, float hi, double k)
+    {
+        return k > 0.0 ? (p >= lo && p < hi) : (k < 0.0 ? (p > lo && p <= hi) : (p >= lo && p <= hi));
     }
 
     SKG_D bool next(const GridDev& g)
@@ -163,49 +173,66 @@ struct OctreeLeaf32 : FastBase<float>
         float d;
         int a = this->pickAxis(this->dist(xE, this->rx, this->ikx, this->kx), this->dist(yE, this->ry, this->iky, this->ky),
                                this->dist(zE, this->rz, this->ikz, this->kz), false, d);
+        // the entry point may lie a rounding error beyond a wall of a cell entered through the
+        // fallback below: never step backwards, so that the walk advances monotonically
+        d = fmaxf(d, 0.f);
         int wall = 2 * a + ((a == 0 ? this->kx : (a == 1 ? this->ky : this->kz)) < 0.0 ? 0 : 1);
         this->m = cell;
         this->ds = d;
         segDens = rb.z;
         this->rebase(a, a == 0 ? xE : (a == 1 ? yE : zE), this->ds);
-        // neighbour list of the exit wall: base + 9-bit cumulative offsets (all ones: no list)
+        // words 2-3 of the record (same cache line as words 0-1): the list offsets and, per wall,
+        // the single neighbour across it (-1: domain wall, -2: several neighbours)
+        const int* w23 = reinterpret_cast<const int*>(g.tLeaf + 4 * static_cast<size_t>(cell) + 2);
+        int one = __ldg(w23 + 2 + wall);
+        int old = cell, nb = -1;
+        if (one >= 0)
+        {
+            enter(g, one);
+            return true;
+        }
+        if (one == -1)
+        {
+            this->state = GS_OUTSIDE;
+            return true;
+        }
+        unsigned long long cnt = (static_cast<unsigned long long>(static_cast<unsigned>(__ldg(w23 + 1))) << 32)
+                                 | static_cast<unsigned>(__ldg(w23));
         int base = __float_as_int(rb.w);
         bool listed = cnt != ~0ULL;
         int e0 = base + static_cast<int>((cnt >> (9 * wall)) & 511);
         int n = listed ? base + static_cast<int>((cnt >> (9 * (wall + 1))) & 511) - e0 : 0;
         float pu = static_cast<float>(a == 0 ? this->ry : this->rx);
         float pv = static_cast<float>(a == 2 ? this->ry : this->rz);
-        int old = cell, nb = -1;
+        double ku = a == 0 ? this->ky : this->kx;
+        double kv = a == 2 ? this->ky : this->kz;
+        for (int e = 0; e < n; ++e)
         {
-            for (int e = 0; e < n; ++e)
+            int c = __ldg(g.tLeafNb + e0 + e);
+            float4 qa = __ldg(g.tLeaf + 4 * static_cast<size_t>(c)), qb = __ldg(g.tLeaf + 4 * static_cast<size_t>(c) + 1);
+            float ulo = a == 0 ? qa.y : qa.x, uhi = a == 0 ? qb.x : qa.w;
+            float vlo = a == 2 ? qa.y : qa.z, vhi = a == 2 ? qb.x : qb.y;
+            if (within(pu, ulo, uhi, ku) && within(pv, vlo, vhi, kv))
             {
-                int c = g.tLeafNb[e0 + e];
-                float4 qa = g.tLeaf[2 * c], qb = g.tLeaf[2 * c + 1];
-                float ulo = a == 0 ? qa.y : qa.x, uhi = a == 0 ? qb.x : qa.w;
-                float vlo = a == 2 ? qa.y : qa.z, vhi = a == 2 ? qb.x : qb.y;
-                if (pu >= ulo && pu <= uhi && pv >= vlo && pv <= vhi)
-                {
-                    nb = c;
-                    cell = c;
-                    ra = qa;
-                    rb = qb;
-                    cnt = g.tLeafCnt[c];
-                    break;
-                }
+                nb = c;
+                cell = c;
+                ra = qa;
+                rb = qb;
+                break;
             }
         }
         if (nb < 0)
         {
-            // no neighbour (domain wall, or an exit point on a cell edge): locate the point just beyond the wall
-            double e = g.eps;
-            nb = locate(g, this->rx + this->kx * e, this->ry + this->ky * e, this->rz + this->kz * e);
-            if (nb == old)
-            {
-                this->rx = nextafter(this->rx, (this->kx < 0.) ? -DBL_MAX : DBL_MAX);
-                this->ry = nextafter(this->ry, (this->ky < 0.) ? -DBL_MAX : DBL_MAX);
-                this->rz = nextafter(this->rz, (this->kz < 0.) ? -DBL_MAX : DBL_MAX);
-                nb = locate(g, this->rx, this->ry, this->rz);
-            }
+            // No listed neighbour holds the exit point (a wall without list, or an exit point on a
+            // cell edge). Move the point forward along every axis by a few FP32 roundings of the
+            // coordinates (so that it lies beyond any FP32-rounded wall it sits on) and locate it
+            // top-down in the FP64 tree; a point outside the domain ends the path.
+            double big = fmax(fabs(this->rx), fmax(fabs(this->ry), fabs(this->rz)));
+            double e = fmax(g.eps, 4.8e-7 * big);
+            this->rx += this->kx > 0.0 ? e : (this->kx < 0.0 ? -e : 0.0);
+            this->ry += this->ky > 0.0 ? e : (this->ky < 0.0 ? -e : 0.0);
+            this->rz += this->kz > 0.0 ? e : (this->kz < 0.0 ? -e : 0.0);
+            nb = locate(g, this->rx, this->ry, this->rz);
             if (nb >= 0 && nb != old) enter(g, nb);
         }
         if (nb < 0 || nb == old) this->state = GS_OUTSIDE;

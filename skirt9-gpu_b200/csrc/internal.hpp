@@ -4,14 +4,16 @@
 #include <cuda_runtime.h>
 #include "wave_types.cuh"
 
+namespace skg { struct StageTimer; }
+
 namespace skg {
 
 // wavefront life cycle, one entry per traversal precision (separate translation units, so that
 // the FP64 one can be compiled without FMA contraction)
 cudaError_t runWaveFP64(int gridKind, const Wave& w, int numSMs, cudaStream_t s, unsigned long long* doneHost,
-                        long long* passes, long long maxPasses, bool useGraph);
+                        long long* passes, long long maxPasses, bool useGraph, StageTimer* timer);
 cudaError_t runWaveFP32(int gridKind, const Wave& w, int numSMs, cudaStream_t s, unsigned long long* doneHost,
-                        long long* passes, long long maxPasses, bool useGraph);
+                        long long* passes, long long maxPasses, bool useGraph, StageTimer* timer);
 
 // path-segment and optical-depth kernels, FP64 (reference operation order) and FP32-distance walkers
 cudaError_t launchTracePathsFP64(int precision, const GridDev& g, int n, const double* rays, int maxSeg, int* count,

@@ -9,7 +9,7 @@ namespace skg {
 constexpr int PATH_GUARD = 1 << 22;
 
 template<class W>
-__global__ void tracePathsKernel(GridDev g, int n, const double* rays, int maxSeg, int* count, int* mo, double* dso,
+__global__ void tracePathsKernel(const __grid_constant__ GridDev g, int n, const double* rays, int maxSeg, int* count, int* mo, double* dso,
                                  int* err)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -40,7 +40,7 @@ __global__ void tracePathsKernel(GridDev g, int n, const double* rays, int maxSe
 // MediumSystem::getExtinctionOpticalDepth for a single medium with spatially constant cross
 // section (MediumSystem.cpp:2328-2443), L = 1 so taumax = log(1) + 745
 template<class W>
-__global__ void opticalDepthKernel(GridDev g, const double* dens, double section, int n, const double* rays,
+__global__ void opticalDepthKernel(const __grid_constant__ GridDev g, const double* dens, double section, int n, const double* rays,
                                    double* tau, int* err)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;

@@ -12,10 +12,12 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/skgpu.h"
 #include "internal.hpp"
+#include "stage_timer.hpp"
 
 using namespace skg;
 
@@ -76,6 +78,14 @@ struct skgpu_ctx
     int waveP = 0, waveGroups = 0, waveStats = 0;
     std::vector<void*> waveBufs;
     unsigned long long* doneHost = nullptr;  // pinned progress word
+
+    // device timing of the stage kernels (skgpu_set_stage_timing)
+    StageTimer timer;
+    bool timerEvents = false;
+
+    // pinned staging of the tally read-back: the copy of one chunk overlaps the host add of the previous
+    double* pin[2] = {nullptr, nullptr};
+    cudaEvent_t pinEv[2] = {nullptr, nullptr};
 };
 
 namespace {
@@ -153,11 +163,11 @@ bool finiteAll(const double* v, size_t n)
     return true;
 }
 
-// copies the number densities into the FP32 leaf records of an octree grid
+// copies the number densities into the FP32 leaf records of an octree grid (4 float4 per leaf)
 __global__ void fillLeafDensityKernel(float4* leaf, const double* dens, int n)
 {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c < n) leaf[2 * c + 1].z = static_cast<float>(dens[c]);
+    if (c < n) leaf[4 * static_cast<size_t>(c) + 1].z = static_cast<float>(dens[c]);
 }
 
 int syncLeafDensity(skgpu_ctx* ctx)
@@ -304,6 +314,15 @@ void skgpu_destroy(skgpu_ctx* ctx)
     freeWave(ctx);
     devFree(ctx->errFlag);
     if (ctx->doneHost) cudaFreeHost(ctx->doneHost);
+    for (int i = 0; i < 2; ++i)
+    {
+        if (ctx->pin[i]) cudaFreeHost(ctx->pin[i]);
+        if (ctx->pinEv[i]) cudaEventDestroy(ctx->pinEv[i]);
+    }
+    if (ctx->timerEvents)
+        for (auto& row : ctx->timer.ev)
+            for (cudaEvent_t ev : row)
+                if (ev) cudaEventDestroy(ev);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -398,29 +417,33 @@ int skgpu_upload_grid_octree(skgpu_ctx* ctx, int32_t num_nodes, const double* bo
     if ((rc = gridUpload<int>(ctx, &g.tChild, firstChild.data(), num_nodes))) return rc;
     if ((rc = gridUpload<int>(ctx, &g.tNbBegin, nb_begin, 6 * static_cast<size_t>(num_nodes) + 1))) return rc;
     if ((rc = gridUpload<int>(ctx, &g.tNb, nb_index, num_nb_index))) return rc;
-    // leaf-indexed FP32 records of the production walker (cell c <-> its leaf node): bounds, density
-    // (filled when the medium is uploaded), the base of the cell's neighbour list; per wall the
-    // positive-overlap neighbours in the reference's overlap order (zero-overlap entries, which only
-    // touch an edge, come last in the reference's lists and are left out: exit points on an edge
-    // are resolved by the top-down fallback)
+    // Leaf-indexed 64-byte records of the production walker (cell c <-> its leaf node), four float4:
+    //   [0] lo.x lo.y lo.z hi.x   [1] hi.y hi.z density base   [2] cnt.lo cnt.hi one[0] one[1]
+    //   [3] one[2] one[3] one[4] one[5]
+    // FP32 bounds, FP32 density (filled when the medium is uploaded), the base of the cell's neighbour
+    // list, the 9-bit cumulative offsets of its 6 walls in the list (all ones: no list), and per wall
+    // the one neighbour across it when there is exactly one (-1: no neighbour, the domain wall;
+    // -2: several, scan the list). The lists hold per wall the positive-overlap neighbours in the
+    // reference's overlap order (zero-overlap entries, which only touch an edge, come last in the
+    // reference's lists and are left out: exit points on an edge are resolved by the top-down fallback).
     std::vector<int> leafNode(numCells, -1);
     for (int l = 0; l < num_nodes; ++l)
         if (cell_index[l] >= 0) leafNode[cell_index[l]] = l;
-    std::vector<float4> leaf(2 * static_cast<size_t>(numCells));
-    std::vector<unsigned long long> cnt(numCells, 0);
+    std::vector<float4> leaf(4 * static_cast<size_t>(numCells));
     std::vector<int> leafNb;
     leafNb.reserve(static_cast<size_t>(numCells) * 8);
+    auto bitsOf = [](auto v) {
+        float f;
+        static_assert(sizeof v == sizeof f, "32-bit field");
+        std::memcpy(&f, &v, sizeof f);
+        return f;
+    };
     for (int c = 0; c < numCells; ++c)
     {
         int l = leafNode[c];
         if (l < 0) return fail(ctx, SKGPU_ERR_ARG, "octree: cell index without leaf");
         const double* b = bounds + 6 * static_cast<size_t>(l);
-        leaf[2 * c] = make_float4(static_cast<float>(b[0]), static_cast<float>(b[1]), static_cast<float>(b[2]),
-                                  static_cast<float>(b[3]));
         int base = static_cast<int>(leafNb.size());
-        float baseBits;
-        std::memcpy(&baseBits, &base, sizeof base);
-        leaf[2 * c + 1] = make_float4(static_cast<float>(b[4]), static_cast<float>(b[5]), 0.f, baseBits);
         // per wall the positive-overlap neighbours; 9-bit cumulative offsets of the 6 walls + end
         // (a leaf with more than 511 such neighbours gets no list: its exits use the top-down search)
         std::vector<int> lists[6];
@@ -439,26 +462,36 @@ int skgpu_upload_grid_octree(skgpu_ctx* ctx, int32_t num_nodes, const double* bo
             }
             total += lists[w].size();
         }
+        unsigned long long cnt = 0;
         if (total > 511)
         {
-            cnt[c] = ~0ULL;
+            cnt = ~0ULL;
         }
         else
         {
             unsigned long long off = 0;
             for (int w = 0; w < 6; ++w)
             {
-                cnt[c] |= off << (9 * w);
+                cnt |= off << (9 * w);
                 leafNb.insert(leafNb.end(), lists[w].begin(), lists[w].end());
                 off += lists[w].size();
             }
-            cnt[c] |= off << 54;
+            cnt |= off << 54;
         }
+        int one[6];
+        for (int w = 0; w < 6; ++w)
+            one[w] = lists[w].size() == 1 ? lists[w][0] : (lists[w].empty() && total <= 511 ? -1 : -2);
+        float4* r = &leaf[4 * static_cast<size_t>(c)];
+        r[0] = make_float4(static_cast<float>(b[0]), static_cast<float>(b[1]), static_cast<float>(b[2]),
+                           static_cast<float>(b[3]));
+        r[1] = make_float4(static_cast<float>(b[4]), static_cast<float>(b[5]), 0.f, bitsOf(base));
+        r[2] = make_float4(bitsOf(static_cast<unsigned>(cnt)), bitsOf(static_cast<unsigned>(cnt >> 32)),
+                           bitsOf(one[0]), bitsOf(one[1]));
+        r[3] = make_float4(bitsOf(one[2]), bitsOf(one[3]), bitsOf(one[4]), bitsOf(one[5]));
         if (leafNb.size() > 2147483647ULL) return fail(ctx, SKGPU_ERR_ARG, "octree: neighbour lists too long");
     }
     if (leafNb.empty()) leafNb.push_back(0);
     if ((rc = gridUpload<float4>(ctx, &g.tLeaf, leaf.data(), leaf.size()))) return rc;
-    if ((rc = gridUpload<unsigned long long>(ctx, &g.tLeafCnt, cnt.data(), cnt.size()))) return rc;
     if ((rc = gridUpload<int>(ctx, &g.tLeafNb, leafNb.data(), leafNb.size()))) return rc;
     ctx->hasGrid = true;
     return syncLeafDensity(ctx);
@@ -825,14 +858,20 @@ static void waveShape(const skgpu_ctx* ctx, int& groups, int& anyStats)
 }
 
 // runs the wavefront on prepared buffers and collects the counters and status of the run
-static int runAndCollect(skgpu_ctx* ctx, const Wave& w, bool useGraph)
+static int runAndCollect(skgpu_ctx* ctx, const Wave& w, bool useGraph, bool timed)
 {
     int prec = ctx->opt.precision;
     long long passes = 0;
+    StageTimer* timer = timed && ctx->timer.level ? &ctx->timer : nullptr;
+    for (int i = 0; i < StageTimer::kStages; ++i)
+    {
+        ctx->timer.ms[i] = 0.;
+        ctx->timer.launches[i] = 0;
+    }
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
     cudaError_t e = prec == SKGPU_PREC_FP64_EXACT
-                        ? runWaveFP64(ctx->g.kind, w, ctx->numSMs, ctx->stream, ctx->doneHost, &passes, MAX_PASSES, useGraph)
-                        : runWaveFP32(ctx->g.kind, w, ctx->numSMs, ctx->stream, ctx->doneHost, &passes, MAX_PASSES, useGraph);
+                        ? runWaveFP64(ctx->g.kind, w, ctx->numSMs, ctx->stream, ctx->doneHost, &passes, MAX_PASSES, useGraph, timer)
+                        : runWaveFP32(ctx->g.kind, w, ctx->numSMs, ctx->stream, ctx->doneHost, &passes, MAX_PASSES, useGraph, timer);
     if (e == cudaErrorNotSupported) return fail(ctx, SKGPU_ERR_UNSUPPORTED, "run: no FP32 walker for this grid kind");
     if (e == cudaErrorLaunchTimeout) return fail(ctx, SKGPU_ERR_TIMEOUT, "run: pass limit reached before all histories finished");
     if (e != cudaSuccess) return fail(ctx, SKGPU_ERR_CUDA, std::string("run: ") + cudaGetErrorString(e));
@@ -890,7 +929,7 @@ int skgpu_run_primary(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t t
     w.first = first;
     w.count = count;
     w.anyStats = anyStats;
-    return runAndCollect(ctx, w, true);
+    return runAndCollect(ctx, w, true, true);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -989,15 +1028,57 @@ int skgpu_run_primary_noalloc(skgpu_ctx* ctx, uint64_t first, uint64_t count, ui
     w.first = first;
     w.count = count;
     w.anyStats = anyStats;
-    return runAndCollect(ctx, w, false);
+    return runAndCollect(ctx, w, false, false);
 }
 
+// host[i] += src[i] for i < n, split over the host cores for large n
+static void parallelAdd(double* host, const double* src, size_t n)
+{
+    const size_t perThread = size_t(1) << 18;
+    size_t hw = std::max(1u, std::min(std::thread::hardware_concurrency(), 16u));
+    size_t T = std::min(hw, (n + perThread - 1) / perThread);
+    if (T <= 1)
+    {
+        for (size_t i = 0; i < n; ++i) host[i] += src[i];
+        return;
+    }
+    std::vector<std::thread> pool;
+    size_t per = (n + T - 1) / T;
+    for (size_t t = 0; t < T; ++t)
+        pool.emplace_back([=] {
+            size_t a = t * per, b = std::min(n, a + per);
+            for (size_t i = a; i < b; ++i) host[i] += src[i];
+        });
+    for (std::thread& th : pool) th.join();
+}
+
+// Adds n doubles of device memory into a host array: chunked copies into two pinned buffers, the
+// copy of chunk c+1 in flight while the host cores add chunk c.
 static int addInto(skgpu_ctx* ctx, const double* dev, size_t n, double* host)
 {
     if (!host || !dev || n == 0) return SKGPU_OK;
-    std::vector<double> tmp(n);
-    CK(cudaMemcpy(tmp.data(), dev, n * sizeof(double), cudaMemcpyDeviceToHost));
-    for (size_t i = 0; i < n; ++i) host[i] += tmp[i];
+    const size_t chunk = size_t(8) << 20;  // doubles per staging buffer (64 MB)
+    for (int i = 0; i < 2; ++i)
+    {
+        if (!ctx->pin[i]) CK(cudaMallocHost(reinterpret_cast<void**>(&ctx->pin[i]), chunk * sizeof(double)));
+        if (!ctx->pinEv[i]) CK(cudaEventCreateWithFlags(&ctx->pinEv[i], cudaEventDisableTiming));
+    }
+    size_t chunks = (n + chunk - 1) / chunk;
+    auto issue = [&](size_t c) {
+        size_t a = c * chunk, len = std::min(chunk, n - a);
+        cudaError_t e = cudaMemcpyAsync(ctx->pin[c & 1], dev + a, len * sizeof(double), cudaMemcpyDeviceToHost,
+                                        ctx->stream);
+        return e == cudaSuccess ? cudaEventRecord(ctx->pinEv[c & 1], ctx->stream) : e;
+    };
+    CK(issue(0));
+    for (size_t c = 0; c < chunks; ++c)
+    {
+        // buffer (c+1)&1 held chunk c-1, whose add finished in the previous iteration
+        if (c + 1 < chunks) CK(issue(c + 1));
+        CK(cudaEventSynchronize(ctx->pinEv[c & 1]));
+        size_t a = c * chunk;
+        parallelAdd(host + a, ctx->pin[c & 1], std::min(chunk, n - a));
+    }
     return SKGPU_OK;
 }
 
@@ -1067,6 +1148,32 @@ int skgpu_get_counters(skgpu_ctx* ctx, skgpu_counters* out)
 {
     if (!ctx || !out) return SKGPU_ERR_ARG;
     *out = ctx->lastCounters;
+    return SKGPU_OK;
+}
+
+int skgpu_set_stage_timing(skgpu_ctx* ctx, int32_t level)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (level < 0 || level > 2) return fail(ctx, SKGPU_ERR_ARG, "stage timing: level must be 0, 1 or 2");
+    if (level && !ctx->timerEvents)
+    {
+        CK(cudaSetDevice(ctx->device));
+        for (auto& row : ctx->timer.ev)
+            for (cudaEvent_t& ev : row) CK(cudaEventCreate(&ev));
+        ctx->timerEvents = true;
+    }
+    ctx->timer.level = level;
+    return SKGPU_OK;
+}
+
+int skgpu_last_stage_times(skgpu_ctx* ctx, double* ms, uint64_t* launches)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    for (int i = 0; i < SKGPU_NUM_STAGES; ++i)
+    {
+        if (ms) ms[i] = ctx->timer.ms[i];
+        if (launches) launches[i] = ctx->timer.launches[i];
+    }
     return SKGPU_OK;
 }
 

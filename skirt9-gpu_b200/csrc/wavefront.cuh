@@ -24,6 +24,7 @@
 // (launch, forced sampling, scattering), whatever pass the draws happen in.
 #pragma once
 
+#include <cstdio>
 #include "wave_types.cuh"
 
 namespace skg {
@@ -175,7 +176,7 @@ SKG_D float amul(float a, float b) { return a * b; }
 SKG_D float aexp(float x) { return __expf(x); }
 
 template<class Walker>
-__global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(Wave w, int cur)
+__global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __grid_constant__ Wave w, int cur)
 {
     const Scene& sc = w.sc;
     const unsigned FULL = 0xffffffffu;
@@ -189,10 +190,14 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(Wave w, i
     int kind = -1;  // -1: needs a task, -2: finished
     unsigned idx = 0;
     int slot = 0;
-    Acc tau = 0, s = 0, par = 0, lnExtBeg = 0, extBeg = 1, L = 0, sext = 0;
-    int nseg = 0, lastM = -1, ellRF = -1;
-    Acc lastS = 0;
-    unsigned long long cross = 0, rfStores = 0;
+    // Per-task accumulators. The task kinds never share a lane at the same time, so their
+    // variables share registers (named per kind below):
+    //   PEEL:       fA = optical-depth cutoff log(L) + 745
+    //   PROP1:      fA = L, fB = ln(extinction) at the segment start, fC = extinction there, iA = RF bin
+    //   PROP2/FREE: fA = target optical depth, fB = path length, fC = path length at the last segment, iA = last cell
+    Acc tau = 0, fA = 0, fB = 0, fC = 0, sext = 0;
+    int iA = -1, nseg = 0;
+    unsigned cross = 0, rfStores = 0;  // flushed to the counters before they can overflow
     int guard = 0;
 
     while (true)
@@ -221,28 +226,31 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(Wave w, i
                     slot = b.slot[idx];
                     sext = static_cast<Acc>(sc.mixExt[w.pk.ellMix[slot]]);
                     tau = 0.;
-                    s = 0.;
                     nseg = 0;
-                    lastM = -1;
-                    lastS = 0.;
                     guard = 0;
                     if (kind == K_PEEL)
                     {
                         const InstrDev& in = sc.instr[b.info[idx] & 0xFF];
-                        par = static_cast<Acc>(log(b.par[idx]) + 745.);  // taumax = log(L) + 745
+                        fA = static_cast<Acc>(log(b.par[idx]) + 745.);  // taumax = log(L) + 745
                         wk.start(sc.g, b.x[idx], b.y[idx], b.z[idx], in.kobs[0], in.kobs[1], in.kobs[2]);
                     }
                     else
                     {
-                        par = static_cast<Acc>(b.par[idx]);
                         wk.start(sc.g, w.pk.x[slot], w.pk.y[slot], w.pk.z[slot], w.pk.kx[slot], w.pk.ky[slot],
                                  w.pk.kz[slot]);
                         if (kind == K_PROP1)
                         {
-                            L = static_cast<Acc>(w.pk.L[slot]);
-                            ellRF = sc.rfOn ? w.pk.ellRF[slot] : -1;
-                            lnExtBeg = 0.;
-                            extBeg = 1.;
+                            fA = static_cast<Acc>(w.pk.L[slot]);
+                            iA = sc.rfOn ? w.pk.ellRF[slot] : -1;
+                            fB = 0.;
+                            fC = 1.;
+                        }
+                        else
+                        {
+                            fA = static_cast<Acc>(b.par[idx]);
+                            fB = 0.;
+                            fC = 0.;
+                            iA = -1;
                         }
                     }
                 }
@@ -263,7 +271,7 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(Wave w, i
                 if (m >= 0)
                 {
                     tau = aadd(tau, amul(amul(sext, static_cast<Acc>(wk.density(sc.dens))), ds));
-                    if (tau >= par)
+                    if (tau >= fA)
                     {
                         tau = static_cast<Acc>(INFINITY);
                         done = true;
@@ -276,18 +284,18 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(Wave w, i
                 {
                     if (m >= 0) tau = aadd(tau, amul(amul(sext, static_cast<Acc>(wk.density(sc.dens))), ds));
                     nseg++;
-                    if (ellRF >= 0)
+                    if (iA >= 0)
                     {
                         Acc lnExtEnd = -tau;
                         Acc extEnd = aexp(lnExtEnd);
                         if (m >= 0)
                         {
-                            Acc Lds = L * lnmean4(extEnd, extBeg, lnExtEnd, lnExtBeg) * ds;
-                            atomicAdd(sc.rf + static_cast<size_t>(m) * sc.nrf + ellRF, static_cast<double>(Lds));
+                            Acc Lds = fA * lnmean4(extEnd, fC, lnExtEnd, fB) * ds;
+                            atomicAdd(sc.rf + static_cast<size_t>(m) * sc.nrf + iA, static_cast<double>(Lds));
                             rfStores++;
                         }
-                        lnExtBeg = lnExtEnd;
-                        extBeg = extEnd;
+                        fB = lnExtEnd;
+                        fC = extEnd;
                     }
                 }
             }
@@ -296,25 +304,37 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(Wave w, i
                 // PROP2 keeps segments with ds > 0 (SpatialGridPath::addSegment); FREE uses every segment
                 if (kind == K_FREE || ds > 0.)
                 {
-                    Acc tau0 = tau, s0 = s;
+                    Acc tau0 = tau, s0 = fB;
                     if (m >= 0) tau = aadd(tau, amul(amul(sext, static_cast<Acc>(wk.density(sc.dens))), ds));
-                    s = aadd(s, ds);
-                    lastM = m;
-                    lastS = s;
-                    if (par < tau)
+                    fB = aadd(fB, ds);
+                    iA = m;
+                    fC = fB;
+                    if (fA < tau)
                     {
                         // NR::interpolateLinLin (SKIRT/utils/NR.hpp:328-331)
                         const TaskBuf& b = w.q[cur][kind];
                         b.m[idx] = m;
-                        b.s[idx] = static_cast<double>(s0 + ((par - tau0) / (tau - tau0)) * (s - s0));
+                        b.s[idx] = static_cast<double>(s0 + ((fA - tau0) / (tau - tau0)) * (fB - s0));
                         b.found[idx] = 1;
                         kind = -1;
                         continue;
                     }
                 }
             }
-            if (++guard > (1 << 22))
+            if (++guard > (1 << 20))
             {
+                // a traversal that does not end: report the first few (task kind, start point and
+                // direction, last cell) and stop it; the run returns SKGPU_ERR_TIMEOUT
+                if (atomicAdd(&w.ctl->counters[7], 1ULL) < 4ULL)
+                {
+                    const TaskBuf& b = w.q[cur][kind];
+                    bool peel = kind == K_PEEL;
+                    const double* ko = peel ? sc.instr[b.info[idx] & 0xFF].kobs : nullptr;
+                    printf("skgpu: traversal guard: kind %d hist %llu start (%.17g %.17g %.17g) dir (%.17g %.17g %.17g) cell %d\n",
+                           kind, static_cast<unsigned long long>(w.pk.hist[slot]), peel ? b.x[idx] : w.pk.x[slot],
+                           peel ? b.y[idx] : w.pk.y[slot], peel ? b.z[idx] : w.pk.z[slot], peel ? ko[0] : w.pk.kx[slot],
+                           peel ? ko[1] : w.pk.ky[slot], peel ? ko[2] : w.pk.kz[slot], m);
+                }
                 atomicOr(&w.ctl->err, 4);
                 done = true;
             }
@@ -329,23 +349,30 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(Wave w, i
             else
             {
                 // beyond the last segment: PROP2 uses the last segment, FREE escapes
-                b.m[idx] = lastM;
-                b.s[idx] = static_cast<double>(lastS);
+                b.m[idx] = iA;
+                b.s[idx] = static_cast<double>(fC);
                 b.found[idx] = 0;
             }
             kind = -1;
+            if ((cross | rfStores) & 0x80000000u)
+            {
+                atomicAdd(&w.ctl->counters[1], static_cast<unsigned long long>(cross));
+                atomicAdd(&w.ctl->counters[4], static_cast<unsigned long long>(rfStores));
+                cross = rfStores = 0;
+            }
         }
     }
 
+    unsigned long long crossAll = cross, rfAll = rfStores;
     for (int off = 16; off > 0; off >>= 1)
     {
-        cross += __shfl_down_sync(FULL, cross, off);
-        rfStores += __shfl_down_sync(FULL, rfStores, off);
+        crossAll += __shfl_down_sync(FULL, crossAll, off);
+        rfAll += __shfl_down_sync(FULL, rfAll, off);
     }
     if (lane == 0)
     {
-        if (cross) atomicAdd(&w.ctl->counters[1], cross);
-        if (rfStores) atomicAdd(&w.ctl->counters[4], rfStores);
+        if (crossAll) atomicAdd(&w.ctl->counters[1], crossAll);
+        if (rfAll) atomicAdd(&w.ctl->counters[4], rfAll);
     }
 }
 
@@ -354,7 +381,7 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(Wave w, i
 // ---------------------------------------------------------------------------------------------
 
 // FluxRecorder::detect for the instruments of one observer group (FluxRecorder.cpp:372-538)
-static __global__ void __launch_bounds__(256) shadePeelKernel(Wave w, int cur)
+static __global__ void __launch_bounds__(256) shadePeelKernel(const __grid_constant__ Wave w, int cur)
 {
     const Scene& sc = w.sc;
     unsigned n = w.ctl->qn[cur][K_PEEL];
@@ -433,7 +460,7 @@ static __global__ void __launch_bounds__(256) shadePeelKernel(Wave w, int cur)
 }
 
 // forced scattering: sample the interaction optical depth (simulateForcedPropagation)
-static __global__ void __launch_bounds__(256) shadeProp1Kernel(Wave w, int cur, int nxt)
+static __global__ void __launch_bounds__(256) shadeProp1Kernel(const __grid_constant__ Wave w, int cur, int nxt)
 {
     unsigned n = w.ctl->qn[cur][K_PROP1];
     const TaskBuf& b = w.q[cur][K_PROP1];
@@ -518,7 +545,7 @@ SKG_D void interact(const Wave& w, int nxt, int slot, int m, double sInt, bool f
     storeRng(w, slot, rng);
 }
 
-static __global__ void __launch_bounds__(256) shadeProp2Kernel(Wave w, int cur, int nxt)
+static __global__ void __launch_bounds__(256) shadeProp2Kernel(const __grid_constant__ Wave w, int cur, int nxt)
 {
     unsigned n = w.ctl->qn[cur][K_PROP2];
     const TaskBuf& b = w.q[cur][K_PROP2];
@@ -526,7 +553,7 @@ static __global__ void __launch_bounds__(256) shadeProp2Kernel(Wave w, int cur, 
         interact(w, nxt, b.slot[t], b.m[t], b.s[t], true);
 }
 
-static __global__ void __launch_bounds__(256) shadeFreeKernel(Wave w, int cur, int nxt)
+static __global__ void __launch_bounds__(256) shadeFreeKernel(const __grid_constant__ Wave w, int cur, int nxt)
 {
     unsigned n = w.ctl->qn[cur][K_FREE];
     const TaskBuf& b = w.q[cur][K_FREE];
@@ -542,7 +569,7 @@ static __global__ void __launch_bounds__(256) shadeFreeKernel(Wave w, int cur, i
 // ---------------------------------------------------------------------------------------------
 // launch
 // ---------------------------------------------------------------------------------------------
-static __global__ void launchPrepKernel(Wave w, int nxt)
+static __global__ void launchPrepKernel(const __grid_constant__ Wave w, int nxt)
 {
     Control* c = w.ctl;
     unsigned long long remaining = w.count - c->launched;
@@ -556,7 +583,7 @@ static __global__ void launchPrepKernel(Wave w, int nxt)
     for (int k = 0; k < NUM_KINDS; ++k) c->qn[1 - nxt][k] = 0;  // the buffer consumed by this pass
 }
 
-static __global__ void __launch_bounds__(256) launchKernel(Wave w, int nxt)
+static __global__ void __launch_bounds__(256) launchKernel(const __grid_constant__ Wave w, int nxt)
 {
     const Scene& sc = w.sc;
     int n = w.ctl->nLaunch;
@@ -591,7 +618,7 @@ static __global__ void __launch_bounds__(256) launchKernel(Wave w, int nxt)
     }
 }
 
-static __global__ void initPoolKernel(Wave w)
+static __global__ void initPoolKernel(const __grid_constant__ Wave w)
 {
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < w.P; t += gridDim.x * blockDim.x)
     {

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include "stage_timer.hpp"
 #include "wavefront.cuh"
 
 namespace skg {
@@ -20,17 +21,27 @@ int traceBlocksPerSM()
     return n > 0 ? n : 1;
 }
 
+// `pass` is the index of the pass within its batch (selects the timer's events)
 template<class Walker>
-void enqueuePass(const Wave& w, int cur, const WaveLaunch& L, cudaStream_t s)
+cudaError_t enqueuePass(const Wave& w, int pass, const WaveLaunch& L, cudaStream_t s, StageTimer* t, bool capturing)
 {
-    int nxt = 1 - cur;
+    int cur = pass & 1, nxt = 1 - cur;
+    cudaError_t e;
+    if ((e = stageMark(t, pass, 0, s, capturing)) != cudaSuccess) return e;
     traceKernel<Walker><<<L.traceBlocks, L.threads, 0, s>>>(w, cur);
+    if ((e = stageMark(t, pass, 1, s, capturing)) != cudaSuccess) return e;
     shadePeelKernel<<<L.shadeBlocks, L.threads, 0, s>>>(w, cur);
+    if ((e = stageMark(t, pass, 2, s, capturing)) != cudaSuccess) return e;
     shadeProp1Kernel<<<L.shadeBlocks, L.threads, 0, s>>>(w, cur, nxt);
+    if ((e = stageMark(t, pass, 3, s, capturing)) != cudaSuccess) return e;
     shadeProp2Kernel<<<L.shadeBlocks, L.threads, 0, s>>>(w, cur, nxt);
+    if ((e = stageMark(t, pass, 4, s, capturing)) != cudaSuccess) return e;
     shadeFreeKernel<<<L.shadeBlocks, L.threads, 0, s>>>(w, cur, nxt);
+    if ((e = stageMark(t, pass, 5, s, capturing)) != cudaSuccess) return e;
     launchPrepKernel<<<1, 1, 0, s>>>(w, nxt);
     launchKernel<<<L.shadeBlocks, L.threads, 0, s>>>(w, nxt);
+    if ((e = stageMark(t, pass, 6, s, capturing)) != cudaSuccess) return e;
+    return cudaGetLastError();
 }
 
 // Runs histories [w.first, w.first + w.count). `doneHost` receives the progress word (pinned host
@@ -40,7 +51,7 @@ void enqueuePass(const Wave& w, int cur, const WaveLaunch& L, cudaStream_t s)
 // pass limit is reached without finishing. `passes` receives the number of passes run.
 template<class Walker>
 cudaError_t runWave(const Wave& w, int numSMs, cudaStream_t s, unsigned long long* doneHost, long long* passes,
-                    long long maxPasses, bool useGraph)
+                    long long maxPasses, bool useGraph, StageTimer* timer)
 {
     WaveLaunch L;
     L.threads = 256;
@@ -52,16 +63,21 @@ cudaError_t runWave(const Wave& w, int numSMs, cudaStream_t s, unsigned long lon
     if (e != cudaSuccess) return e;
     if (w.count == 0) return cudaStreamSynchronize(s);
 
-    const int passesPerBatch = 4;  // even: the buffer parity returns to 0 after every batch
+    const int passesPerBatch = StageTimer::kBatch;  // even: the buffer parity returns to 0 after every batch
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     if (useGraph)
     {
         e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
         if (e != cudaSuccess) return e;
-        for (int k = 0; k < passesPerBatch; ++k) enqueuePass<Walker>(w, k & 1, L, s);
-        e = cudaStreamEndCapture(s, &graph);
-        if (e != cudaSuccess) return e;
+        for (int k = 0; k < passesPerBatch && e == cudaSuccess; ++k) e = enqueuePass<Walker>(w, k, L, s, timer, true);
+        cudaError_t e2 = cudaStreamEndCapture(s, &graph);
+        if (e == cudaSuccess) e = e2;
+        if (e != cudaSuccess)
+        {
+            if (graph) cudaGraphDestroy(graph);
+            return e;
+        }
         e = cudaGraphInstantiate(&exec, graph, 0);
         if (e != cudaSuccess)
         {
@@ -77,16 +93,15 @@ cudaError_t runWave(const Wave& w, int numSMs, cudaStream_t s, unsigned long lon
         if (useGraph)
             e = cudaGraphLaunch(exec, s);
         else
-        {
-            for (int k = 0; k < passesPerBatch; ++k) enqueuePass<Walker>(w, k & 1, L, s);
-            e = cudaGetLastError();
-        }
+            for (int k = 0; k < passesPerBatch && e == cudaSuccess; ++k) e = enqueuePass<Walker>(w, k, L, s, timer, false);
         if (e != cudaSuccess) break;
         *passes += passesPerBatch;
         e = cudaMemcpyAsync(doneHost, reinterpret_cast<char*>(w.ctl) + doneOffset, sizeof(unsigned long long),
                             cudaMemcpyDeviceToHost, s);
         if (e != cudaSuccess) break;
         e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) break;
+        e = stageCollect(timer);
         if (e != cudaSuccess) break;
         if (*doneHost >= w.count) break;
         if (*doneHost != lastDone)

@@ -7,12 +7,13 @@
 namespace skg {
 
 cudaError_t runWaveFP32(int gridKind, const Wave& w, int numSMs, cudaStream_t s, unsigned long long* doneHost,
-                        long long* passes, long long maxPasses, bool useGraph)
+                        long long* passes, long long maxPasses, bool useGraph,
+                        StageTimer* timer)
 {
     switch (gridKind)
     {
-        case 0: return runWave<CartesianFast<float>>(w, numSMs, s, doneHost, passes, maxPasses, useGraph);
-        case 1: return runWave<OctreeLeaf32>(w, numSMs, s, doneHost, passes, maxPasses, useGraph);
+        case 0: return runWave<CartesianFast<float>>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer);
+        case 1: return runWave<OctreeLeaf32>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer);
     }
     return cudaErrorNotSupported;
 }

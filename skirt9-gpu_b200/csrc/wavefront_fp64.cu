@@ -7,14 +7,15 @@
 namespace skg {
 
 cudaError_t runWaveFP64(int gridKind, const Wave& w, int numSMs, cudaStream_t s, unsigned long long* doneHost,
-                        long long* passes, long long maxPasses, bool useGraph)
+                        long long* passes, long long maxPasses, bool useGraph,
+                        StageTimer* timer)
 {
     switch (gridKind)
     {
-        case 0: return runWave<CartesianExact>(w, numSMs, s, doneHost, passes, maxPasses, useGraph);
-        case 1: return runWave<OctreeExact>(w, numSMs, s, doneHost, passes, maxPasses, useGraph);
-        case 2: return runWave<VoronoiExact>(w, numSMs, s, doneHost, passes, maxPasses, useGraph);
-        case 3: return runWave<TetraExact>(w, numSMs, s, doneHost, passes, maxPasses, useGraph);
+        case 0: return runWave<CartesianExact>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer);
+        case 1: return runWave<OctreeExact>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer);
+        case 2: return runWave<VoronoiExact>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer);
+        case 3: return runWave<TetraExact>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer);
     }
     return cudaErrorInvalidValue;
 }

@@ -248,19 +248,29 @@ class Backend:
     def run_primary(self, first, count, total):
         self.call("run_primary", int(first), int(count), int(total))
 
-    def fetch_instrument(self, i, n, stats=False):
-        total = np.zeros(n)
-        st = np.zeros(5 * n) if stats else None
+    @staticmethod
+    def _into(out, n):
+        """The caller's accumulation array (float64, contiguous, n entries) or a new zeroed one."""
+        if out is None:
+            return np.zeros(n)
+        if out.dtype != np.float64 or not out.flags.c_contiguous or out.size != n:
+            raise ValueError(f"tally array must be contiguous float64 of {n} entries")
+        return out
+
+    def fetch_instrument(self, i, n, stats=False, out=None, out_stats=None):
+        """Adds instrument i's tallies into `out` (and `out_stats`, 5 planes) or into new arrays."""
+        total = self._into(out, n)
+        st = self._into(out_stats, 5 * n) if stats else None
         self.call("fetch_instrument", i, _ptr(total), _ptr(total), _ptr(st), _ptr(st))
         return total, (st.reshape(5, n) if stats else None)
 
-    def fetch_instrument_components(self, i, n):
-        comp = np.zeros(3 * n)
+    def fetch_instrument_components(self, i, n, out=None):
+        comp = self._into(out, 3 * n)
         self.call("fetch_instrument_components", i, _ptr(comp), _ptr(comp))
         return comp.reshape(3, n)
 
-    def fetch_radiation_field(self, n):
-        rf = np.zeros(n)
+    def fetch_radiation_field(self, n, out=None):
+        rf = self._into(out, n)
         self.call("fetch_radiation_field", _ptr(rf))
         return rf
 
@@ -367,3 +377,31 @@ def run_primary_noalloc(be, first, count, total):
     rc = f(be.ctx, int(first), int(count), int(total))
     if rc != OK:
         raise SkgpuError(rc, be.fn["last_error"](be.ctx).decode())
+
+
+EXPORTED += ["skgpu_set_stage_timing", "skgpu_last_stage_times"]
+
+STAGES = ("trace", "peel", "prop1", "prop2", "free", "launch")  # SKGPU_STAGE_* order
+
+
+def set_stage_timing(be, level):
+    """CUDA-event timing of the stage kernels of later runs: 0 off, 1 traversal kernel, 2 all stages."""
+    f = be.lib.skgpu_set_stage_timing
+    f.argtypes = [C.c_void_p, C.c_int32]
+    f.restype = C.c_int
+    rc = f(be.ctx, int(level))
+    if rc != OK:
+        raise SkgpuError(rc, be.fn["last_error"](be.ctx).decode())
+
+
+def last_stage_times(be):
+    """{stage: (device ms summed over the last run, launches)} of the stages that were timed."""
+    ms = np.zeros(len(STAGES))
+    n = np.zeros(len(STAGES), np.uint64)
+    f = be.lib.skgpu_last_stage_times
+    f.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    f.restype = C.c_int
+    rc = f(be.ctx, _ptr(ms), _ptr(n))
+    if rc != OK:
+        raise SkgpuError(rc, be.fn["last_error"](be.ctx).decode())
+    return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(STAGES) if n[i]}

@@ -144,6 +144,10 @@ class Scene:
         npix = ins["nx"] * ins["ny"] if ins["kind"] == abi.INSTR_FRAME else 1
         return npix * ins["num_bins"]
 
+    def rf_length(self):
+        """Entries of the radiation-field tally (cells x RF bins), 0 when it is not stored."""
+        return len(self.density) * self.rf["num_bins"] if self.store_rf and self.rf is not None else 0
+
     def prepare(self, be, npp, seed=0, precision=abi.PREC_FP64_EXACT):
         be.set_options(self.options(seed, precision))
         structs, tl, ta, tb, rr, rp = self.source_structs(npp)
