@@ -226,10 +226,55 @@ int skgpu_last_run_ms(skgpu_ctx* ctx, double* ms);
 #define SKGPU_STAGE_PROP1 2  /* forced sampling of the interaction optical depth */
 #define SKGPU_STAGE_PROP2 3  /* forced interaction: weight, position, scattering, peel-off rays */
 #define SKGPU_STAGE_FREE 4   /* non-forced interaction */
-#define SKGPU_STAGE_LAUNCH 5 /* refill of free packet slots with new histories */
-#define SKGPU_NUM_STAGES 6
+#define SKGPU_STAGE_GUIDE 5  /* guided scattering: network inference and direction sampling (guiding on) */
+#define SKGPU_STAGE_LAUNCH 6 /* refill of free packet slots with new histories */
+#define SKGPU_NUM_STAGES 7
 int skgpu_set_stage_timing(skgpu_ctx* ctx, int32_t level);
 int skgpu_last_stage_times(skgpu_ctx* ctx, double* ms, uint64_t* launches);
+
+/* ---- learned path guiding (no reference counterpart) ----
+ * A small network (8 inputs -> 4 x 64 ReLU -> 40 outputs: 8 von Mises-Fisher lobes over the outgoing
+ * direction) proposes scattering directions. Mode SKGPU_GUIDE_RECORD makes the next runs record a
+ * fraction of their scattering events (inputs, sampled direction, and the luminosity that the target
+ * instrument later detects from the history per unit packet luminosity, optionally weighted per
+ * pixel); skgpu_guide_train fits the network to them on the GPU (importance-weighted maximum
+ * likelihood, Adam). Mode SKGPU_GUIDE_SAMPLE makes the runs sample alpha * q_net + (1 - alpha) * p_HG
+ * and weight the packet by p_HG / (alpha * q_net + (1 - alpha) * p_HG): the estimator stays unbiased,
+ * and alpha = 0 is plain sampling. Inference runs as BF16 tensor-core layers with FP32 accumulation.
+ * Network inputs: position / domain half size (3), incoming direction (3), log10(lambda / 0.55 um),
+ * log(1 + tau) / 5 with tau the optical depth of the propagation path that ended at the event.
+ * Outputs per lobe j: [5j] weight logit, [5j+1..5j+3] direction (normalised), [5j+4] concentration
+ * (softplus + 0.05, at most 2000). Parameters: FP32, per layer W (out x in, row-major) then b.
+ * Guiding is not available through skgpu_run_primary_noalloc. */
+#define SKGPU_GUIDE_OFF 0
+#define SKGPU_GUIDE_RECORD 1
+#define SKGPU_GUIDE_SAMPLE 2
+#define SKGPU_GUIDE_NUM_INPUTS 8
+#define SKGPU_GUIDE_NUM_OUTPUTS 40
+#define SKGPU_GUIDE_RECORD_FLOATS 13 /* inputs[8], direction[3], downstream luminosity, packet luminosity */
+int skgpu_guide_num_params(void);
+/* creates the network with the given parameters, or a seeded random initialisation (params NULL) */
+int skgpu_guide_init(skgpu_ctx* ctx, const float* params, uint64_t seed);
+int skgpu_guide_get_params(skgpu_ctx* ctx, float* params);
+/* mode, target instrument, alpha (SAMPLE, in [0,1)), recorded fraction and record capacity (RECORD;
+ * switching to RECORD discards earlier records) */
+int skgpu_guide_set_mode(skgpu_ctx* ctx, int32_t mode, int32_t target_instrument, float alpha, float record_fraction,
+                         uint64_t record_capacity);
+/* per-pixel weights of the target frame's detections in the records (NULL: weight 1) */
+int skgpu_guide_set_importance(skgpu_ctx* ctx, int32_t n, const float* weights);
+/* training target: with position_bins > 0 each record's weight is its downstream luminosity over the
+ * mean of its position bin (position_bins^3 bins over the domain), so that every region of the
+ * domain weighs alike; with 0 (default) over the mean of all records */
+int skgpu_guide_set_training(skgpu_ctx* ctx, int32_t position_bins);
+int skgpu_guide_record_count(skgpu_ctx* ctx, uint64_t* n);
+int skgpu_guide_fetch_records(skgpu_ctx* ctx, uint64_t n, float* out);
+/* steps of Adam on random batches of the records; the loss of the last batch in final_loss */
+int skgpu_guide_train(skgpu_ctx* ctx, int32_t steps, int32_t batch, float learning_rate, uint64_t seed, float* final_loss);
+/* sum over n samples of -w log q(direction | inputs) and its gradient (FP32 forward / backward) */
+int skgpu_guide_loss_grad(skgpu_ctx* ctx, int32_t n, const float* inputs, const float* directions, const float* weights,
+                          float* loss, float* grad);
+/* raw outputs (n x 40) for n inputs: BF16 tensor cores (tensor_cores != 0) or FP32 CUDA cores */
+int skgpu_guide_infer(skgpu_ctx* ctx, int32_t n, const float* inputs, float* outputs, int32_t tensor_cores);
 
 /* ---- path segments (replaces GpuAcceleration::set*SpatialGridPath, GpuAcceleration.hpp) ----
  * For each ray (x,y,z,kx,ky,kz) the segments (m, ds) the grid's PathSegmentGenerator returns,

@@ -1,0 +1,80 @@
+// The state behind the opaque skgpu_ctx handle of include/skgpu.h (shared by the ABI translation
+// units).
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/skgpu.h"
+#include "internal.hpp"
+#include "stage_timer.hpp"
+
+namespace skg { struct GuideState; }
+
+using skg::GridDev;
+using skg::InstrDev;
+using skg::SourceDev;
+using skg::StageTimer;
+using skg::Wave;
+
+struct skgpu_ctx
+{
+    int device = 0;
+    int numSMs = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string err;
+    double lastMs = 0.;
+
+    GridDev g{};
+    bool hasGrid = false;
+    std::vector<void*> gridBufs;
+
+    double* dens = nullptr;
+    int numCells = 0;
+
+    double *mixLb = nullptr, *mixExt = nullptr, *mixSca = nullptr, *mixG = nullptr;
+    int nmix = 0;
+
+    int nrf = 0, rfNb = 0;
+    double* rfB = nullptr;
+    int* rfEll = nullptr;
+    double* rf = nullptr;
+    size_t rfLen = 0;
+
+    std::vector<SourceDev> srcHost;
+    SourceDev* src = nullptr;
+    double *tabL = nullptr, *tabA = nullptr, *tabB = nullptr, *radR = nullptr, *radP = nullptr;
+
+    std::vector<InstrDev> instrHost;
+    InstrDev* instr = nullptr;
+    std::vector<void*> instrBufs;
+    double* wlgB = nullptr;
+    int* wlgEll = nullptr;
+
+    skgpu_options opt{};
+    bool hasOptions = false;
+
+    int* errFlag = nullptr;
+    skgpu_counters lastCounters{};
+    long long lastPasses = 0;
+
+    // wavefront buffers (packet pool, task queues, control block), grown on demand
+    Wave wave{};
+    int waveP = 0, waveGroups = 0, waveStats = 0;
+    std::vector<void*> waveBufs;
+    unsigned long long* doneHost = nullptr;  // pinned progress word
+
+    // device timing of the stage kernels (skgpu_set_stage_timing)
+    StageTimer timer;
+    bool timerEvents = false;
+
+    // pinned staging of the tally read-back: the copy of one chunk overlaps the host add of the previous
+    double* pin[2] = {nullptr, nullptr};
+    cudaEvent_t pinEv[2] = {nullptr, nullptr};
+
+    // learned path guiding (network, pilot records, optimizer state); null until first used
+    skg::GuideState* guide = nullptr;
+};

@@ -3,6 +3,7 @@
 #pragma once
 
 #include "grids.cuh"
+#include "guide.cuh"
 
 namespace skg {
 
@@ -68,6 +69,18 @@ struct Scene
     int forced, minScatt, peel;
     double minWeightRed, pathLengthBias;
     unsigned long long seed;
+
+    // learned path guiding: 0 off, 1 pilot (record scattering events), 2 guided scattering
+    int guideMode;
+    int guideTarget;                 // instrument whose detections define the records' importance
+    float guideAlpha;                // probability of sampling the network's lobes (mode 2)
+    float guideRecFrac;              // fraction of scattering events recorded (mode 1)
+    GuideRecord* guideRec;
+    unsigned long long* guideRecCount;
+    unsigned long long guideRecCap;
+    const float* guideImportance;    // per-pixel weight of the target frame's detections (null: 1)
+    const unsigned char* guideBlob;  // packed BF16 network (mode 2)
+    int* guideErr;
 };
 
 // atomicAdd after summing the contributions of the warp's active lanes that target the same address

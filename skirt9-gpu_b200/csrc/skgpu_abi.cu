@@ -17,7 +17,8 @@
 
 #include "../../include/skgpu.h"
 #include "internal.hpp"
-#include "stage_timer.hpp"
+#include "ctx.hpp"
+#include "guide_internal.hpp"
 
 using namespace skg;
 
@@ -31,62 +32,6 @@ struct DevArray
 
 }  // namespace
 
-struct skgpu_ctx
-{
-    int device = 0;
-    int numSMs = 0;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    std::string err;
-    double lastMs = 0.;
-
-    GridDev g{};
-    bool hasGrid = false;
-    std::vector<void*> gridBufs;
-
-    double* dens = nullptr;
-    int numCells = 0;
-
-    double *mixLb = nullptr, *mixExt = nullptr, *mixSca = nullptr, *mixG = nullptr;
-    int nmix = 0;
-
-    int nrf = 0, rfNb = 0;
-    double* rfB = nullptr;
-    int* rfEll = nullptr;
-    double* rf = nullptr;
-    size_t rfLen = 0;
-
-    std::vector<SourceDev> srcHost;
-    SourceDev* src = nullptr;
-    double *tabL = nullptr, *tabA = nullptr, *tabB = nullptr, *radR = nullptr, *radP = nullptr;
-
-    std::vector<InstrDev> instrHost;
-    InstrDev* instr = nullptr;
-    std::vector<void*> instrBufs;
-    double* wlgB = nullptr;
-    int* wlgEll = nullptr;
-
-    skgpu_options opt{};
-    bool hasOptions = false;
-
-    int* errFlag = nullptr;
-    skgpu_counters lastCounters{};
-    long long lastPasses = 0;
-
-    // wavefront buffers (packet pool, task queues, control block), grown on demand
-    Wave wave{};
-    int waveP = 0, waveGroups = 0, waveStats = 0;
-    std::vector<void*> waveBufs;
-    unsigned long long* doneHost = nullptr;  // pinned progress word
-
-    // device timing of the stage kernels (skgpu_set_stage_timing)
-    StageTimer timer;
-    bool timerEvents = false;
-
-    // pinned staging of the tally read-back: the copy of one chunk overlaps the host add of the previous
-    double* pin[2] = {nullptr, nullptr};
-    cudaEvent_t pinEv[2] = {nullptr, nullptr};
-};
 
 namespace {
 
@@ -225,12 +170,16 @@ int ensureWaveBuffers(skgpu_ctx* ctx, int P, int groups, int stats)
     size_t ns = stats ? static_cast<size_t>(P) * STATS_CAP : 1;
     if ((rc = waveAlloc(ctx, &k.skey, ns))) return rc;
     if ((rc = waveAlloc(ctx, &k.sw, ns))) return rc;
+    if ((rc = waveAlloc(ctx, &k.gD, P))) return rc;
+    if ((rc = waveAlloc(ctx, &k.gLast, P))) return rc;
+    if ((rc = waveAlloc(ctx, &k.gPend, P))) return rc;
     for (int b = 0; b < 2; ++b)
         for (int kind = 0; kind < NUM_KINDS; ++kind)
         {
             TaskBuf& t = w.q[b][kind];
             size_t cap = kind == K_PEEL ? static_cast<size_t>(P) * groups : static_cast<size_t>(P);
             if ((rc = waveAlloc(ctx, &t.slot, cap))) return rc;
+            if (kind == K_GUIDE) continue;  // the guided-scattering queue holds packet slots only
             if ((rc = waveAlloc(ctx, &t.par, cap))) return rc;
             if (kind == K_PEEL)
             {
@@ -312,6 +261,7 @@ void skgpu_destroy(skgpu_ctx* ctx)
     devFree(ctx->radR);
     devFree(ctx->radP);
     freeWave(ctx);
+    guideDestroy(ctx);
     devFree(ctx->errFlag);
     if (ctx->doneHost) cudaFreeHost(ctx->doneHost);
     for (int i = 0; i < 2; ++i)
@@ -831,6 +781,20 @@ static Scene sceneOf(const skgpu_ctx* ctx)
     p.minWeightRed = ctx->opt.min_weight_reduction;
     p.pathLengthBias = ctx->opt.path_length_bias;
     p.seed = ctx->opt.seed;
+    p.guideMode = 0;
+    if (const GuideState* gs = ctx->guide)
+    {
+        p.guideMode = gs->mode;
+        p.guideTarget = gs->target;
+        p.guideAlpha = gs->alpha;
+        p.guideRecFrac = gs->recordFraction;
+        p.guideRec = gs->records;
+        p.guideRecCount = gs->recCount;
+        p.guideRecCap = gs->recCapacity;
+        p.guideImportance = gs->importance;
+        p.guideBlob = gs->blob;
+        p.guideErr = gs->errFlag;
+    }
     return p;
 }
 
@@ -889,11 +853,13 @@ static int runAndCollect(skgpu_ctx* ctx, const Wave& w, bool useGraph, bool time
     ctx->lastCounters.peel_detections = ctl.counters[3];
     ctx->lastCounters.rf_stores = ctl.counters[4];
     ctx->lastCounters.stats_overflows = ctl.counters[5];
-    ctx->lastCounters.kernel_launches = static_cast<uint64_t>(passes) * 7 + 1;
+    ctx->lastCounters.kernel_launches = static_cast<uint64_t>(passes) * (w.sc.guideMode == 2 ? 8 : 7) + 1;
     ctx->lastPasses = passes;
     if (w.count > 0 && ctl.done != w.count) return fail(ctx, SKGPU_ERR_DEVICE, "run: not every history finished");
     if (errFlag & 4) return fail(ctx, SKGPU_ERR_TIMEOUT, "run: a traversal exceeded its segment guard");
     if (errFlag & 8) return fail(ctx, SKGPU_ERR_TIMEOUT, "run: a history exceeded the scattering-event guard");
+    if (errFlag & 16) return fail(ctx, SKGPU_ERR_TIMEOUT, "run: a tensor-core wait of the guided-scattering stage gave up");
+    if (errFlag & 32) return fail(ctx, SKGPU_ERR_DEVICE, "run: non-finite guided-scattering weight");
     if (errFlag) return fail(ctx, SKGPU_ERR_DEVICE, "run: interaction point outside the grid (device check)");
     return SKGPU_OK;
 }
@@ -966,6 +932,7 @@ static size_t carveWave(Wave& w, unsigned char* base, int P, int groups, int sta
         {
             TaskBuf& t = w.q[b][kind];
             t = TaskBuf{};
+            if (kind == K_GUIDE) continue;  // guiding is not available without allocation
             size_t cap = kind == K_PEEL ? static_cast<size_t>(P) * groups : static_cast<size_t>(P);
             take(&t.slot, cap);
             take(&t.par, cap);
@@ -996,6 +963,8 @@ int skgpu_run_primary_noalloc(skgpu_ctx* ctx, uint64_t first, uint64_t count, ui
     if (rc) return rc;
     int groups, anyStats;
     waveShape(ctx, groups, anyStats);
+    if (ctx->guide && ctx->guide->mode != 0)
+        return fail(ctx, SKGPU_ERR_STATE, "run_noalloc: learned path guiding is not available without allocation");
     if (groups > SKGPU_NOALLOC_MAX_GROUPS)
         return fail(ctx, SKGPU_ERR_ARG, "run_noalloc: more than " + std::to_string(SKGPU_NOALLOC_MAX_GROUPS)
                                             + " observer groups exceed the static scratch");
@@ -1250,6 +1219,215 @@ int skgpu_optical_depths(skgpu_ctx* ctx, int32_t num_rays, const double* rays, d
     devFree(dRays);
     devFree(dTau);
     if (e != cudaSuccess) return fail(ctx, SKGPU_ERR_CUDA, std::string("optical depths: ") + cudaGetErrorString(e));
+    return SKGPU_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------------
+// learned path guiding
+// ------------------------------------------------------------------------------------------------
+namespace {
+
+// He-uniform hidden layers, small output layer with broad initial lobes (softplus(1.85) ~ 2)
+void guideRandomParams(std::vector<float>& p, uint64_t seed)
+{
+    uint64_t st = seed ^ 0x9E3779B97F4A7C15ULL;
+    auto next = [&]() {
+        st += 0x9E3779B97F4A7C15ULL;
+        uint64_t z = st;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+        z ^= z >> 31;
+        return static_cast<double>(z >> 11) * (1.0 / 9007199254740992.0);
+    };
+    p.assign(GUIDE_NPARAMS, 0.f);
+    for (int l = 0; l < GUIDE_LAYERS; ++l)
+    {
+        int nin = guideDimIn(l), nout = guideDimOut(l);
+        float* W = p.data() + guideParamOffset(l);
+        float* b = W + nin * nout;
+        double lim = std::sqrt(6.0 / nin) * (l + 1 == GUIDE_LAYERS ? 0.1 : 1.0);
+        for (int i = 0; i < nin * nout; ++i) W[i] = static_cast<float>((2.0 * next() - 1.0) * lim);
+        for (int o = 0; o < nout; ++o) b[o] = 0.f;
+        if (l + 1 == GUIDE_LAYERS)
+            for (int j = 0; j < GUIDE_LOBES; ++j)
+            {
+                // lobe directions spread over the sphere, concentration ~2
+                double u = 2.0 * next() - 1.0, ph = 2.0 * M_PI * next(), sn = std::sqrt(1.0 - u * u);
+                b[5 * j + 1] = static_cast<float>(sn * std::cos(ph));
+                b[5 * j + 2] = static_cast<float>(sn * std::sin(ph));
+                b[5 * j + 3] = static_cast<float>(u);
+                b[5 * j + 4] = 1.85f;
+            }
+    }
+}
+
+int guideReady(skgpu_ctx* ctx)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (!ctx->guide) return fail(ctx, SKGPU_ERR_STATE, "guide: call skgpu_guide_init first");
+    return SKGPU_OK;
+}
+
+#define GCK(call)                                                                                  \
+    do                                                                                             \
+    {                                                                                              \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return fail(ctx, SKGPU_ERR_CUDA, std::string("guide: ") + cudaGetErrorString(e_));     \
+    } while (0)
+
+}  // namespace
+
+extern "C" {
+
+int skgpu_guide_num_params(void) { return GUIDE_NPARAMS; }
+
+int skgpu_guide_init(skgpu_ctx* ctx, const float* params, uint64_t seed)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    GCK(guideEnsure(ctx));
+    std::vector<float> p;
+    if (params)
+        p.assign(params, params + GUIDE_NPARAMS);
+    else
+        guideRandomParams(p, seed);
+    for (float v : p)
+        if (!std::isfinite(v)) return fail(ctx, SKGPU_ERR_ARG, "guide: non-finite parameter");
+    GCK(guideSetParams(ctx, p.data()));
+    return SKGPU_OK;
+}
+
+int skgpu_guide_get_params(skgpu_ctx* ctx, float* params)
+{
+    int rc = guideReady(ctx);
+    if (rc) return rc;
+    if (!params) return fail(ctx, SKGPU_ERR_ARG, "guide: null output");
+    CK(cudaSetDevice(ctx->device));
+    GCK(guideGetParams(ctx, params));
+    return SKGPU_OK;
+}
+
+int skgpu_guide_set_mode(skgpu_ctx* ctx, int32_t mode, int32_t target_instrument, float alpha, float record_fraction,
+                         uint64_t record_capacity)
+{
+    int rc = guideReady(ctx);
+    if (rc) return rc;
+    GuideState* g = ctx->guide;
+    if (mode < 0 || mode > 2) return fail(ctx, SKGPU_ERR_ARG, "guide: mode must be 0, 1 or 2");
+    if (mode != 0 && (target_instrument < 0 || target_instrument >= static_cast<int>(ctx->instrHost.size())))
+        return fail(ctx, SKGPU_ERR_ARG, "guide: target instrument out of range (upload the instruments first)");
+    if (mode == 2 && !(alpha >= 0.f && alpha < 1.f))
+        return fail(ctx, SKGPU_ERR_ARG, "guide: alpha must lie in [0, 1): plain sampling must keep a share");
+    if (mode == 1 && (!(record_fraction > 0.f && record_fraction <= 1.f) || record_capacity == 0
+                      || record_capacity > 0x7FFFFFFFULL))
+        return fail(ctx, SKGPU_ERR_ARG, "guide: record fraction in (0, 1] and capacity in [1, 2^31) required");
+    CK(cudaSetDevice(ctx->device));
+    if (mode == 1) GCK(guideEnsureRecords(ctx, record_capacity));
+    g->mode = mode;
+    g->target = target_instrument;
+    g->alpha = alpha;
+    g->recordFraction = record_fraction;
+    return SKGPU_OK;
+}
+
+int skgpu_guide_set_importance(skgpu_ctx* ctx, int32_t n, const float* weights)
+{
+    int rc = guideReady(ctx);
+    if (rc) return rc;
+    GuideState* g = ctx->guide;
+    CK(cudaSetDevice(ctx->device));
+    if (g->importance) cudaFree(g->importance);
+    g->importance = nullptr;
+    g->importanceLen = 0;
+    if (!weights || n <= 0) return SKGPU_OK;
+    if (ctx->instrHost.empty() || g->target < 0 || g->target >= static_cast<int>(ctx->instrHost.size()))
+        return fail(ctx, SKGPU_ERR_STATE, "guide: set a mode with a target instrument first");
+    const InstrDev& t = ctx->instrHost[g->target];
+    if (t.kind != SKGPU_INSTR_FRAME || n != t.npx * t.npy)
+        return fail(ctx, SKGPU_ERR_ARG, "guide: importance needs one weight per pixel of the target frame");
+    for (int i = 0; i < n; ++i)
+        if (!(weights[i] >= 0.f) || !std::isfinite(weights[i]))
+            return fail(ctx, SKGPU_ERR_ARG, "guide: importance weights must be finite and >= 0");
+    CK(cudaMalloc(reinterpret_cast<void**>(&g->importance), static_cast<size_t>(n) * sizeof(float)));
+    CK(cudaMemcpy(g->importance, weights, static_cast<size_t>(n) * sizeof(float), cudaMemcpyHostToDevice));
+    g->importanceLen = n;
+    return SKGPU_OK;
+}
+
+int skgpu_guide_set_training(skgpu_ctx* ctx, int32_t position_bins)
+{
+    int rc = guideReady(ctx);
+    if (rc) return rc;
+    if (position_bins < 0 || position_bins > 64) return fail(ctx, SKGPU_ERR_ARG, "guide: position bins in [0, 64]");
+    ctx->guide->positionBins = position_bins;
+    return SKGPU_OK;
+}
+
+int skgpu_guide_record_count(skgpu_ctx* ctx, uint64_t* n)
+{
+    int rc = guideReady(ctx);
+    if (rc) return rc;
+    if (!n) return SKGPU_ERR_ARG;
+    unsigned long long v = 0;
+    if (ctx->guide->records)
+    {
+        CK(cudaSetDevice(ctx->device));
+        GCK(guideRecordCount(ctx, &v));
+    }
+    *n = v;
+    return SKGPU_OK;
+}
+
+int skgpu_guide_fetch_records(skgpu_ctx* ctx, uint64_t n, float* out)
+{
+    int rc = guideReady(ctx);
+    if (rc) return rc;
+    CK(cudaSetDevice(ctx->device));
+    unsigned long long have = 0;
+    if (ctx->guide->records) GCK(guideRecordCount(ctx, &have));
+    if (!out || n > have) return fail(ctx, SKGPU_ERR_ARG, "guide: more records requested than recorded");
+    GCK(guideFetchRecords(ctx, n, out));
+    return SKGPU_OK;
+}
+
+int skgpu_guide_train(skgpu_ctx* ctx, int32_t steps, int32_t batch, float learning_rate, uint64_t seed, float* final_loss)
+{
+    int rc = guideReady(ctx);
+    if (rc) return rc;
+    if (steps < 0 || batch < 1 || batch > (1 << 20) || !(learning_rate > 0.f))
+        return fail(ctx, SKGPU_ERR_ARG, "guide: steps >= 0, batch in [1, 2^20] and a positive learning rate required");
+    if (!ctx->guide->records) return fail(ctx, SKGPU_ERR_STATE, "guide: no pilot records (run in mode 1 first)");
+    CK(cudaSetDevice(ctx->device));
+    cudaError_t e = guideTrain(ctx, steps, batch, learning_rate, seed, final_loss);
+    if (e == cudaErrorInvalidValue) return fail(ctx, SKGPU_ERR_STATE, "guide: the pilot recorded no downstream detections");
+    GCK(e);
+    return SKGPU_OK;
+}
+
+int skgpu_guide_loss_grad(skgpu_ctx* ctx, int32_t n, const float* inputs, const float* directions, const float* weights,
+                          float* loss, float* grad)
+{
+    int rc = guideReady(ctx);
+    if (rc) return rc;
+    if (n < 1 || n > (1 << 20) || !inputs || !directions || !weights || !loss || !grad)
+        return fail(ctx, SKGPU_ERR_ARG, "guide: loss_grad arguments");
+    CK(cudaSetDevice(ctx->device));
+    GCK(guideLossGrad(ctx, n, inputs, directions, weights, loss, grad));
+    return SKGPU_OK;
+}
+
+int skgpu_guide_infer(skgpu_ctx* ctx, int32_t n, const float* inputs, float* outputs, int32_t tensor_cores)
+{
+    int rc = guideReady(ctx);
+    if (rc) return rc;
+    if (n < 1 || n > (1 << 24) || !inputs || !outputs) return fail(ctx, SKGPU_ERR_ARG, "guide: infer arguments");
+    CK(cudaSetDevice(ctx->device));
+    int devErr = 0;
+    GCK(guideInfer(ctx, n, inputs, outputs, tensor_cores, &devErr));
+    if (devErr) return fail(ctx, SKGPU_ERR_TIMEOUT, "guide: a tensor-core wait gave up");
     return SKGPU_OK;
 }
 

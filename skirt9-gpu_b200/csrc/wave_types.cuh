@@ -1,12 +1,14 @@
 // Data layout of the wavefront life cycle: the packet pool (structure of arrays), the task
-// buffers of the four traversal kinds, and the control block of counters.
+// buffers of the four traversal kinds (plus the guided-scattering queue), and the control block.
 #pragma once
 
 #include "physics.cuh"
 
 namespace skg {
 
-enum TaskKind { K_PEEL = 0, K_PROP1 = 1, K_PROP2 = 2, K_FREE = 3, NUM_KINDS = 4 };
+// K_GUIDE is not traversed: it queues the scattering events whose new direction the guiding
+// network samples (filled and consumed within one pass)
+enum TaskKind { K_PEEL = 0, K_PROP1 = 1, K_PROP2 = 2, K_FREE = 3, K_GUIDE = 4, NUM_KINDS = 5 };
 
 struct PacketPool
 {
@@ -22,6 +24,10 @@ struct PacketPool
     double* sw;
     int* nstat;
     int* freeSlots;            // P
+    // pilot records of the guiding network: luminosity of the history detected by the target
+    // instrument so far, last recorded event, event whose start value is still open
+    double* gD;
+    int *gLast, *gPend;
 };
 
 // one buffer of one task kind

@@ -26,6 +26,7 @@
 
 #include <cstdio>
 #include "wave_types.cuh"
+#include "guide_mma.cuh"
 
 namespace skg {
 
@@ -110,9 +111,27 @@ SKG_D void flushStats(const Wave& w, int slot)
     w.pk.nstat[slot] = 0;
 }
 
+// end of a recorded pilot history: the downstream luminosity per unit packet luminosity of every
+// recorded event, from the history's final detected luminosity
+SKG_D void guideCloseHistory(const Wave& w, int slot)
+{
+    const Scene& sc = w.sc;
+    double D = w.pk.gD[slot];
+    int pend = w.pk.gPend[slot];
+    if (pend >= 0) sc.guideRec[pend].dStart = D;
+    int r = w.pk.gLast[slot];
+    for (int guard = 0; r >= 0 && guard < (1 << 20); ++guard)
+    {
+        GuideRecord& q = sc.guideRec[r];
+        q.I = q.L > 0.f ? static_cast<float>((D - q.dStart) / static_cast<double>(q.L)) : 0.f;
+        r = q.prev;
+    }
+}
+
 SKG_D void endHistory(const Wave& w, int slot)
 {
     if (w.anyStats && w.pk.nstat[slot]) flushStats(w, slot);
+    if (w.sc.guideMode == 1) guideCloseHistory(w, slot);
     int i = atomicAdd(&w.ctl->freeTop, 1);
     w.pk.freeSlots[i] = slot;
     atomicAdd(&w.ctl->done, 1ULL);
@@ -404,6 +423,12 @@ static __global__ void __launch_bounds__(256) shadePeelKernel(const __grid_const
             int ell = wlgBin(sc.wlgB + in.woff, in.wnb, sc.wlgEll + in.woff, lambda);
             if (ell < 0) continue;
             det++;
+            if (sc.guideMode == 1 && i == sc.guideTarget)
+            {
+                // pilot records: the history's detected luminosity in the target instrument
+                double wp = (sc.guideImportance && l >= 0) ? static_cast<double>(sc.guideImportance[l]) : 1.0;
+                atomicAdd(w.pk.gD + slot, Lext * wp);
+            }
             if (in.kind == 0)
             {
                 size_t npix = static_cast<size_t>(in.npx) * in.npy;
@@ -495,7 +520,40 @@ static __global__ void __launch_bounds__(256) shadeProp1Kernel(const __grid_cons
 
 // interaction point reached: weight, position, termination test, scattering peel-off and HG
 // scattering, next propagation (MonteCarloSimulation.cpp:645-665, 670-683)
-SKG_D void interact(const Wave& w, int nxt, int slot, int m, double sInt, bool forced)
+// pilot record of a scattering event (guiding mode 1): the open record of the previous event gets
+// its start value (its own peel-off has been detected by now), and this event is recorded with
+// probability guideRecFrac, decided by a hash of history and event index so that the packet's
+// random stream is untouched
+SKG_D void guideRecord(const Wave& w, int slot, int nscatt, double x, double y, double z, double kx0, double ky0,
+                       double kz0, double kx, double ky, double kz, double L)
+{
+    const Scene& sc = w.sc;
+    int pend = w.pk.gPend[slot];
+    if (pend >= 0)
+    {
+        sc.guideRec[pend].dStart = w.pk.gD[slot];
+        w.pk.gPend[slot] = -1;
+    }
+    unsigned long long h = w.pk.hist[slot];
+    U4 r = philox4x32_10(U4{static_cast<uint32_t>(nscatt), 0x67756964u, static_cast<uint32_t>(h), static_cast<uint32_t>(h >> 32)},
+                         static_cast<uint32_t>(sc.seed), static_cast<uint32_t>(sc.seed >> 32) ^ 0x5bd1e995u);
+    if (static_cast<float>(r.x) * 2.3283064e-10f >= sc.guideRecFrac) return;
+    unsigned long long idx = atomicAdd(sc.guideRecCount, 1ULL);
+    if (idx >= sc.guideRecCap) return;
+    GuideRecord& q = sc.guideRec[idx];
+    guideFeatures(q.f, x, y, z, kx0, ky0, kz0, w.pk.lam[slot], w.pk.tauPath[slot], sc.g.ext);
+    q.k[0] = static_cast<float>(kx);
+    q.k[1] = static_cast<float>(ky);
+    q.k[2] = static_cast<float>(kz);
+    q.I = 0.f;
+    q.dStart = 0.;
+    q.L = static_cast<float>(L);
+    q.prev = w.pk.gLast[slot];
+    w.pk.gLast[slot] = static_cast<int>(idx);
+    w.pk.gPend[slot] = static_cast<int>(idx);
+}
+
+SKG_D void interact(const Wave& w, int cur, int nxt, int slot, int m, double sInt, bool forced)
 {
     const Scene& sc = w.sc;
     if (m < 0)
@@ -535,14 +593,101 @@ SKG_D void interact(const Wave& w, int nxt, int slot, int m, double sInt, bool f
         endHistory(w, slot);
         return;
     }
+    if (sc.guideMode == 2)
+    {
+        // the guided-scattering stage of this pass samples the new direction (no draw made here)
+        const TaskBuf& gb = w.q[cur][K_GUIDE];
+        unsigned i = warpAppend(&w.ctl->qn[cur][K_GUIDE]);
+        gb.slot[i] = slot;
+        return;
+    }
+    double kx0 = kx, ky0 = ky, kz0 = kz;
     scatterHG(rng, g, kx, ky, kz);
     w.pk.kx[slot] = kx;
     w.pk.ky[slot] = ky;
     w.pk.kz[slot] = kz;
     w.pk.nscatt[slot] = nscatt + 1;
     atomicAdd(&w.ctl->counters[2], 1ULL);
+    if (sc.guideMode == 1) guideRecord(w, slot, nscatt, x, y, z, kx0, ky0, kz0, kx, ky, kz, L);
     beginPropagation(w, nxt, slot, rng);
     storeRng(w, slot, rng);
+}
+
+// Guided scattering of one packet from the network's raw outputs: the composite density
+// alpha * q_mix + (1 - alpha) * p_HG is sampled and the weight multiplied by p_HG / composite.
+SKG_D void guidedScatter(const Wave& w, int nxt, int slot, const float* o)
+{
+    const Scene& sc = w.sc;
+    GuideMixture mix;
+    guideMixture(o, mix);
+    Rng rng;
+    loadRng(w, slot, rng);
+    double g = sc.mixG[w.pk.ellMix[slot]];
+    double kx0 = w.pk.kx[slot], ky0 = w.pk.ky[slot], kz0 = w.pk.kz[slot];
+    double kx = kx0, ky = ky0, kz = kz0;
+    double alpha = sc.guideAlpha;
+    if (rng.uniform() < alpha)
+    {
+        double u0 = rng.uniform(), u1 = rng.uniform(), u2 = rng.uniform();
+        guideSample(mix, u0, u1, u2, kx, ky, kz);
+    }
+    else
+    {
+        scatterHG(rng, g, kx, ky, kz);
+    }
+    double p = pdfHG(g, kx * kx0 + ky * ky0 + kz * kz0);
+    double q = exp(static_cast<double>(guideLogDensity(mix, kx, ky, kz)));
+    double den = alpha * q + (1.0 - alpha) * p;
+    double wgt = den > 0. ? p / den : 0.;
+    if (!(wgt >= 0.) || !isfinite(wgt))
+    {
+        atomicOr(&w.ctl->err, 32);  // non-finite guiding weight: the packet is dropped and flagged
+        wgt = 0.;
+    }
+    w.pk.L[slot] *= wgt;
+    w.pk.kx[slot] = kx;
+    w.pk.ky[slot] = ky;
+    w.pk.kz[slot] = kz;
+    w.pk.nscatt[slot] += 1;
+    atomicAdd(&w.ctl->counters[2], 1ULL);
+    beginPropagation(w, nxt, slot, rng);
+    storeRng(w, slot, rng);
+}
+
+// guided-scattering stage: the network runs on the tensor cores for 128 queued events per tile
+static __global__ void __launch_bounds__(GM_TILE) guideScatterKernel(const __grid_constant__ Wave w, int cur, int nxt)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    const Scene& sc = w.sc;
+    unsigned n = w.ctl->qn[cur][K_GUIDE];
+    if (blockIdx.x * GM_TILE >= n) return;  // uniform per CTA, before any tensor memory is taken
+    const TaskBuf& b = w.q[cur][K_GUIDE];
+    GuideTile t;
+    guideTileBegin(t, smem, sc.guideBlob);
+    bool failed = false;  // uniform across the CTA
+    for (unsigned tile = blockIdx.x; tile * GM_TILE < n; tile += gridDim.x)
+    {
+        unsigned i = tile * GM_TILE + threadIdx.x;
+        bool valid = i < n;
+        int slot = valid ? b.slot[i] : 0;
+        float f[GUIDE_IN], o[GUIDE_OUT];
+        if (valid)
+            guideFeatures(f, w.pk.x[slot], w.pk.y[slot], w.pk.z[slot], w.pk.kx[slot], w.pk.ky[slot], w.pk.kz[slot],
+                          w.pk.lam[slot], w.pk.tauPath[slot], sc.g.ext);
+        else
+            for (int k = 0; k < GUIDE_IN; ++k) f[k] = 0.f;
+        if (!failed && !guideTileForward(t, f, o))
+        {
+            failed = true;
+            if (threadIdx.x == 0) atomicOr(&w.ctl->err, 16);
+        }
+        if (!valid) continue;
+        if (failed)
+            endHistory(w, slot);  // the run reports the error; the history is not continued
+        else
+            guidedScatter(w, nxt, slot, o);
+    }
+    guideTileEnd(t);
 }
 
 static __global__ void __launch_bounds__(256) shadeProp2Kernel(const __grid_constant__ Wave w, int cur, int nxt)
@@ -550,7 +695,7 @@ static __global__ void __launch_bounds__(256) shadeProp2Kernel(const __grid_cons
     unsigned n = w.ctl->qn[cur][K_PROP2];
     const TaskBuf& b = w.q[cur][K_PROP2];
     for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
-        interact(w, nxt, b.slot[t], b.m[t], b.s[t], true);
+        interact(w, cur, nxt, b.slot[t], b.m[t], b.s[t], true);
 }
 
 static __global__ void __launch_bounds__(256) shadeFreeKernel(const __grid_constant__ Wave w, int cur, int nxt)
@@ -562,7 +707,7 @@ static __global__ void __launch_bounds__(256) shadeFreeKernel(const __grid_const
         if (!b.found[t])
             endHistory(w, b.slot[t]);  // the interaction point is outside the path: the packet escapes
         else
-            interact(w, nxt, b.slot[t], b.m[t], b.s[t], false);
+            interact(w, cur, nxt, b.slot[t], b.m[t], b.s[t], false);
     }
 }
 
@@ -605,6 +750,12 @@ static __global__ void __launch_bounds__(256) launchKernel(const __grid_constant
         w.pk.ellMix[slot] = ell;
         w.pk.ellRF[slot] = sc.rfOn ? wlgBin(sc.rfB, sc.rfNb, sc.rfEll, o.lambda) : -1;
         if (w.anyStats) w.pk.nstat[slot] = 0;
+        if (sc.guideMode == 1)
+        {
+            w.pk.gD[slot] = 0.;
+            w.pk.gLast[slot] = -1;
+            w.pk.gPend[slot] = -1;
+        }
         atomicAdd(&w.ctl->counters[0], 1ULL);
         if (!(o.L > 0))
         {

@@ -10,7 +10,8 @@ namespace skg {
 
 struct WaveLaunch
 {
-    int traceBlocks, shadeBlocks, threads;
+    int traceBlocks, shadeBlocks, guideBlocks, threads;
+    bool guided;
 };
 
 template<class Walker>
@@ -38,9 +39,11 @@ cudaError_t enqueuePass(const Wave& w, int pass, const WaveLaunch& L, cudaStream
     if ((e = stageMark(t, pass, 4, s, capturing)) != cudaSuccess) return e;
     shadeFreeKernel<<<L.shadeBlocks, L.threads, 0, s>>>(w, cur, nxt);
     if ((e = stageMark(t, pass, 5, s, capturing)) != cudaSuccess) return e;
+    if (L.guided) guideScatterKernel<<<L.guideBlocks, GM_TILE, GM_SMEM_BYTES, s>>>(w, cur, nxt);
+    if ((e = stageMark(t, pass, 6, s, capturing)) != cudaSuccess) return e;
     launchPrepKernel<<<1, 1, 0, s>>>(w, nxt);
     launchKernel<<<L.shadeBlocks, L.threads, 0, s>>>(w, nxt);
-    if ((e = stageMark(t, pass, 6, s, capturing)) != cudaSuccess) return e;
+    if ((e = stageMark(t, pass, 7, s, capturing)) != cudaSuccess) return e;
     return cudaGetLastError();
 }
 
@@ -57,7 +60,16 @@ cudaError_t runWave(const Wave& w, int numSMs, cudaStream_t s, unsigned long lon
     L.threads = 256;
     L.traceBlocks = numSMs * traceBlocksPerSM<Walker>();
     L.shadeBlocks = numSMs * 4;
+    L.guideBlocks = numSMs * 2;
+    L.guided = w.sc.guideMode == 2;
     *passes = 0;
+    if (timer)
+        for (int i = 0; i < StageTimer::kStages; ++i) timer->active[i] = i != 5 || L.guided;
+    if (L.guided)
+    {
+        cudaError_t ea = cudaFuncSetAttribute(guideScatterKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, GM_SMEM_BYTES);
+        if (ea != cudaSuccess) return ea;
+    }
     initPoolKernel<<<L.shadeBlocks, L.threads, 0, s>>>(w);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;

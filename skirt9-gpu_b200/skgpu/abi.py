@@ -381,7 +381,7 @@ def run_primary_noalloc(be, first, count, total):
 
 EXPORTED += ["skgpu_set_stage_timing", "skgpu_last_stage_times"]
 
-STAGES = ("trace", "peel", "prop1", "prop2", "free", "launch")  # SKGPU_STAGE_* order
+STAGES = ("trace", "peel", "prop1", "prop2", "free", "guide", "launch")  # SKGPU_STAGE_* order
 
 
 def set_stage_timing(be, level):
@@ -405,3 +405,90 @@ def last_stage_times(be):
     if rc != OK:
         raise SkgpuError(rc, be.fn["last_error"](be.ctx).decode())
     return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(STAGES) if n[i]}
+
+
+# ---- learned path guiding ----
+GUIDE_OFF, GUIDE_RECORD, GUIDE_SAMPLE = 0, 1, 2
+GUIDE_NUM_INPUTS, GUIDE_NUM_OUTPUTS, GUIDE_RECORD_FLOATS = 8, 40, 13
+EXPORTED += ["skgpu_guide_num_params", "skgpu_guide_init", "skgpu_guide_get_params", "skgpu_guide_set_mode",
+             "skgpu_guide_set_training",
+             "skgpu_guide_set_importance", "skgpu_guide_record_count", "skgpu_guide_fetch_records",
+             "skgpu_guide_train", "skgpu_guide_loss_grad", "skgpu_guide_infer"]
+
+
+def _guide_call(be, name, argtypes, *args):
+    f = getattr(be.lib, "skgpu_" + name)
+    f.argtypes = [C.c_void_p] + argtypes
+    f.restype = C.c_int
+    rc = f(be.ctx, *args)
+    if rc != OK:
+        raise SkgpuError(rc, be.fn["last_error"](be.ctx).decode())
+
+
+def guide_num_params(be):
+    f = be.lib.skgpu_guide_num_params
+    f.restype = C.c_int
+    return int(f())
+
+
+def guide_init(be, params=None, seed=0):
+    """Creates the guiding network from FP32 parameters, or a seeded random initialisation."""
+    p = None if params is None else np.ascontiguousarray(params, dtype=np.float32)
+    _guide_call(be, "guide_init", [C.c_void_p, C.c_uint64], _ptr(p), int(seed))
+
+
+def guide_get_params(be):
+    p = np.zeros(guide_num_params(be), np.float32)
+    _guide_call(be, "guide_get_params", [C.c_void_p], _ptr(p))
+    return p
+
+
+def guide_set_mode(be, mode, target=0, alpha=0.5, record_fraction=1.0, record_capacity=1 << 20):
+    _guide_call(be, "guide_set_mode", [C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_uint64], int(mode),
+                int(target), float(alpha), float(record_fraction), int(record_capacity))
+
+
+def guide_set_training(be, position_bins=0):
+    """Training target: records weighted per position bin (position_bins^3) or globally (0)."""
+    _guide_call(be, "guide_set_training", [C.c_int32], int(position_bins))
+
+
+def guide_set_importance(be, weights=None):
+    w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float32).ravel()
+    _guide_call(be, "guide_set_importance", [C.c_int32, C.c_void_p], 0 if w is None else len(w), _ptr(w))
+
+
+def guide_records(be):
+    """Recorded pilot events as an (n, 13) array: inputs[8], direction[3], downstream luminosity, L."""
+    n = C.c_uint64()
+    _guide_call(be, "guide_record_count", [C.c_void_p], C.cast(C.pointer(n), C.c_void_p))
+    out = np.zeros((n.value, GUIDE_RECORD_FLOATS), np.float32)
+    if n.value:
+        _guide_call(be, "guide_fetch_records", [C.c_uint64, C.c_void_p], n.value, _ptr(out))
+    return out
+
+
+def guide_train(be, steps, batch=8192, lr=1e-3, seed=1):
+    loss = C.c_float()
+    _guide_call(be, "guide_train", [C.c_int32, C.c_int32, C.c_float, C.c_uint64, C.c_void_p], int(steps), int(batch),
+                float(lr), int(seed), C.cast(C.pointer(loss), C.c_void_p))
+    return loss.value
+
+
+def guide_loss_grad(be, inputs, directions, weights):
+    x = np.ascontiguousarray(inputs, dtype=np.float32)
+    k = np.ascontiguousarray(directions, dtype=np.float32)
+    w = np.ascontiguousarray(weights, dtype=np.float32)
+    loss = C.c_float()
+    grad = np.zeros(guide_num_params(be), np.float32)
+    _guide_call(be, "guide_loss_grad", [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
+                len(w), _ptr(x), _ptr(k), _ptr(w), C.cast(C.pointer(loss), C.c_void_p), _ptr(grad))
+    return loss.value, grad
+
+
+def guide_infer(be, inputs, tensor_cores=True):
+    x = np.ascontiguousarray(inputs, dtype=np.float32)
+    out = np.zeros((len(x), GUIDE_NUM_OUTPUTS), np.float32)
+    _guide_call(be, "guide_infer", [C.c_int32, C.c_void_p, C.c_void_p, C.c_int32], len(x), _ptr(x), _ptr(out),
+                1 if tensor_cores else 0)
+    return out

@@ -164,3 +164,40 @@ def shell_cartesian(nbins=64, npix=256, stats=True, luminosity=5.43959963e23):
                wlg_ellv=ellv, kobs=frame["kobs"])
     sc.instruments = [frame, sed]
     return sc
+
+
+def guided_disk(npix=512, max_level=9, max_dust_fraction=2.5e-6, tau_v=50.0, seed=1, half_size_kpc=25.0,
+                stats=True, store_rf=True):
+    """Hard case of the learned path guiding: the stellar disk + bulge of `galaxy_octree` inside a
+    dust exponential disk (hR 6 kpc, hz 0.2 kpc) with face-on tau_V = 50, oligochromatic at 0.55
+    micron (kappa 1 m2/kg, albedo 0.6, g = 0.6), on an octree of about 1e6 leaves (max level 9, dust
+    fraction 2.5e-6), seen edge-on by one 512^2 frame with statistics; the radiation field is
+    stored on one bin."""
+    sc = Scene()
+    h = half_size_kpc * KPC
+    ext = [-h, -h, -h, h, h, h]
+    hRd, hzd = 6 * KPC, 0.2 * KPC
+    tree = abi.build_octree(abi.GEOM_EXPDISK, [hRd, hzd, 0, 0, 0], ext, 2, max_level, max_dust_fraction, seed=seed)
+    sc.grid = dict(kind=abi.GRID_OCTREE, bounds=tree["bounds"], cell_index=tree["cell_index"],
+                   child_begin=tree["child_begin"], child_count=tree["child_count"],
+                   child_index=tree["child_index"], nb_begin=tree["nb_begin"], nb_index=tree["nb_index"],
+                   eps=1e-12 * np.sqrt(3) * 2 * h, extent=np.array(ext))
+    kappa = 1.0
+    sc.mix = dict(lambda_borders=np.array([0.3e-6, 0.9e-6]), sigma_ext=np.array([kappa, kappa]),
+                  sigma_sca=np.array([0.6 * kappa, 0.6 * kappa]), asymmpar=np.array([0.6, 0.6]))
+    mass = tau_v / (kappa / (2 * np.pi * hRd ** 2))
+    sc.density = mass * tree["density"]
+    sc.total_luminosity = 1e10 * LSUN
+    lf = np.array([0.8, 0.2])
+    rr, rP = sersic_radial_cdf(1.0 * KPC, 4.0)
+    oligo = dict(spectral_model=abi.SPEC_DISCRETE, table_lambda=np.array([LAMBDA_V]), table_a=np.array([1.0]))
+    sc.sources = [
+        dict(position_model=abi.SRC_EXPDISK, geometry=(4 * KPC, 0.35 * KPC, 0, 0, 0), lfrac=lf[0], weight=lf[0], **oligo),
+        dict(position_model=abi.SRC_RADIAL, lfrac=lf[1], weight=lf[1], radial_r=rr, radial_P=rP, **oligo),
+    ]
+    borders = np.array([LAMBDA_V * 0.999, LAMBDA_V * 1.001])
+    ellv = np.array([-1, 0, -1], np.int32)
+    sc.instruments = [_frame(90, 0, 0, 2 * h, npix, 10 * MPC, 1, borders, ellv, stats)]
+    sc.rf = dict(num_bins=1, borders=borders, ellv=ellv)
+    sc.store_rf = store_rf
+    return sc

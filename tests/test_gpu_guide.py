@@ -1,0 +1,121 @@
+"""GPU tests of the learned path guiding, through the C ABI.
+
+- The FP32 training pass (forward, importance-weighted NLL, back-propagation) equals the float64
+  oracle's loss and gradient to FP32 accuracy.
+- The BF16 tensor-core inference (tcgen05, FP32 accumulation in tensor memory) equals the oracle's
+  forward pass with BF16-rounded weights and layer inputs, within a few BF16 roundings; the FP32
+  CUDA-core inference equals the unrounded oracle.
+- Recording a pilot leaves the packets' random streams and tallies untouched.
+- Guided sampling is unbiased: with any network (here an untrained one) the images agree with plain
+  sampling within Monte Carlo noise.
+- Training on pilot records lowers the loss on the records.
+"""
+import numpy as np
+import pytest
+
+import guide_oracle as go
+from helpers import zscores
+from skgpu import Scene, abi
+
+pytestmark = pytest.mark.gpu
+
+
+def _batch(n, seed):
+    rng = np.random.default_rng(seed)
+    x = rng.normal(size=(n, go.N_IN)).astype(np.float32)
+    x[:, 3:6] /= np.linalg.norm(x[:, 3:6], axis=1, keepdims=True)
+    k = rng.normal(size=(n, 3))
+    k = (k / np.linalg.norm(k, axis=1, keepdims=True)).astype(np.float32)
+    w = rng.uniform(0.1, 1.0, n).astype(np.float32)
+    return x, k, w
+
+
+def test_guide_gradient_matches_oracle(gpu_backend):
+    p = go.random_params(3).astype(np.float32)
+    abi.guide_init(gpu_backend, p)
+    np.testing.assert_array_equal(abi.guide_get_params(gpu_backend), p)
+    x, k, w = _batch(600, 1)
+    loss, grad = abi.guide_loss_grad(gpu_backend, x, k, w)
+    lo, gr = go.loss_grad(p.astype(np.float64), x.astype(np.float64), k.astype(np.float64), w.astype(np.float64))
+    assert loss == pytest.approx(lo, rel=1e-4)
+    scale = np.abs(gr).max()
+    assert np.abs(grad - gr).max() <= 2e-3 * scale
+    assert np.abs(grad - gr).mean() <= 1e-4 * scale
+
+
+def test_guide_inference_matches_oracle(gpu_backend):
+    p = go.random_params(8).astype(np.float32)
+    abi.guide_init(gpu_backend, p)
+    x, _, _ = _batch(1000, 2)  # not a multiple of the 128-sample tile
+    ref32 = go.forward(p.astype(np.float64), x.astype(np.float64))[0]
+    out32 = abi.guide_infer(gpu_backend, x, tensor_cores=False)
+    assert np.abs(out32 - ref32).max() <= 1e-4 * np.abs(ref32).max()
+    refq = go.forward(p.astype(np.float64), x.astype(np.float64), quantize=True)[0]
+    outtc = abi.guide_infer(gpu_backend, x, tensor_cores=True)
+    err = np.abs(outtc - refq)
+    scale = np.abs(refq).max()
+    assert err.max() <= 3e-2 * scale, err.max() / scale
+    assert err.mean() <= 3e-3 * scale, err.mean() / scale
+    # and the BF16 pass stays close to the exact network
+    assert np.abs(outtc - ref32).mean() <= 1e-2 * np.abs(ref32).max()
+
+
+def test_pilot_recording_leaves_results_unchanged(golden, gpu_backend):
+    sc = Scene.from_export(golden("shell_c16.npz"))
+    sc.upload(gpu_backend)
+    n = 20000
+    plain = sc.run(gpu_backend, n, seed=3, precision=abi.PREC_FP32)
+    abi.guide_init(gpu_backend, None, 1)
+    abi.guide_set_mode(gpu_backend, abi.GUIDE_RECORD, 0, 0.0, 1.0, 1 << 20)
+    try:
+        rec_run = sc.run(gpu_backend, n, seed=3, precision=abi.PREC_FP32)
+    finally:
+        abi.guide_set_mode(gpu_backend, abi.GUIDE_OFF)
+    for a, b in zip(plain.instruments, rec_run.instruments):
+        np.testing.assert_allclose(b["total"], a["total"], rtol=1e-9, atol=0)
+    rec = abi.guide_records(gpu_backend)
+    assert len(rec) == plain.counters["scatterings"]  # every event recorded (fraction 1)
+    assert np.all(np.isfinite(rec)) and np.all(rec[:, 11] >= -1e-6 * np.abs(rec[:, 11]).max())
+    assert np.allclose(np.linalg.norm(rec[:, 8:11], axis=1), 1.0, atol=1e-5)
+    assert (rec[:, 11] > 0).mean() > 0.1  # many events are followed by detected peel-offs
+
+
+def test_guided_sampling_is_unbiased(golden, gpu_backend):
+    sc = Scene.from_export(golden("shell_c16.npz"))
+    sc.upload(gpu_backend)
+    n = 200000
+    plain = sc.run(gpu_backend, n, seed=21, precision=abi.PREC_FP32)
+    abi.guide_init(gpu_backend, None, 5)  # an untrained network: any proposal must stay unbiased
+    abi.guide_set_mode(gpu_backend, abi.GUIDE_SAMPLE, 0, 0.5)
+    try:
+        guided = sc.run(gpu_backend, n, seed=22, precision=abi.PREC_FP32)
+    finally:
+        abi.guide_set_mode(gpu_backend, abi.GUIDE_OFF)
+    assert guided.counters["scatterings"] > 0
+    sp, sg = plain[0]["stats"][:, 0], guided[0]["stats"][:, 0]
+    lit = (sp[1] > 0) & (sg[1] > 0)
+    z = zscores(sg[1][lit], sg[2][lit], n, sp[1][lit], sp[2][lit], n)
+    assert abs(z.mean()) < 0.1
+    assert 0.8 < np.mean(z * z) < 1.25
+    # SED totals
+    ep, eg = plain[1]["stats"], guided[1]["stats"]
+    zt = zscores(eg[1], eg[2], n, ep[1], ep[2], n)
+    assert np.all(np.abs(zt) < 4)
+
+
+def test_training_lowers_the_loss(golden, gpu_backend):
+    sc = Scene.from_export(golden("shell_c16.npz"))
+    sc.upload(gpu_backend)
+    abi.guide_init(gpu_backend, None, 9)
+    abi.guide_set_mode(gpu_backend, abi.GUIDE_RECORD, 0, 0.0, 1.0, 1 << 20)
+    try:
+        sc.run(gpu_backend, 50000, seed=4, precision=abi.PREC_FP32)
+    finally:
+        abi.guide_set_mode(gpu_backend, abi.GUIDE_OFF)
+    rec = abi.guide_records(gpu_backend)
+    sel = rec[rec[:, 11] > 0][:4096]
+    w = (sel[:, 11] / sel[:, 11].mean() / len(sel)).astype(np.float32)
+    before, _ = abi.guide_loss_grad(gpu_backend, sel[:, :8], sel[:, 8:11], w)
+    abi.guide_train(gpu_backend, 400, batch=4096, lr=2e-3, seed=3)
+    after, _ = abi.guide_loss_grad(gpu_backend, sel[:, :8], sel[:, 8:11], w)
+    assert after < before - 0.05 * abs(before)
