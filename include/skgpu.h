@@ -266,6 +266,9 @@ int skgpu_guide_set_importance(skgpu_ctx* ctx, int32_t n, const float* weights);
  * mean of its position bin (position_bins^3 bins over the domain), so that every region of the
  * domain weighs alike; with 0 (default) over the mean of all records */
 int skgpu_guide_set_training(skgpu_ctx* ctx, int32_t position_bins);
+/* guided events of the last run and the mean of their weight factors (1 in expectation: a mean far
+ * from 1 over many events means the network's density and its sampling disagree) */
+int skgpu_guide_last_weights(skgpu_ctx* ctx, uint64_t* events, double* mean_weight);
 int skgpu_guide_record_count(skgpu_ctx* ctx, uint64_t* n);
 int skgpu_guide_fetch_records(skgpu_ctx* ctx, uint64_t n, float* out);
 /* steps of Adam on random batches of the records; the loss of the last batch in final_loss */

@@ -60,6 +60,8 @@ struct skgpu_ctx
     int* errFlag = nullptr;
     skgpu_counters lastCounters{};
     long long lastPasses = 0;
+    double lastGuideWeightSum = 0.;
+    unsigned long long lastGuideEvents = 0;
 
     // wavefront buffers (packet pool, task queues, control block), grown on demand
     Wave wave{};

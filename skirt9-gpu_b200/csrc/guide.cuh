@@ -34,6 +34,12 @@ SKG_HD constexpr int guideParamOffset(int layer)
 constexpr int GUIDE_NPARAMS = guideParamOffset(GUIDE_LAYERS);  // 15656
 constexpr float GUIDE_KAPPA_MIN = 0.05f;
 constexpr float GUIDE_KAPPA_MAX = 2000.f;
+// A packet whose accumulated guiding weight ratio (product of p_HG / composite over its guided
+// events) exceeds this bound scatters plainly until the ratio falls back below it. The choice
+// depends on past events only, so the estimator stays unbiased, and the ratio stays below
+// GUIDE_RATIO_MAX / (1 - alpha): without the bound the product over many scatterings is heavy-tailed
+// and finite runs miss the rare large weights (their means come out low).
+constexpr double GUIDE_RATIO_MAX = 4.0;
 
 // one recorded scattering event of a pilot run
 struct GuideRecord

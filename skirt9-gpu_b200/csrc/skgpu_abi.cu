@@ -173,6 +173,7 @@ int ensureWaveBuffers(skgpu_ctx* ctx, int P, int groups, int stats)
     if ((rc = waveAlloc(ctx, &k.gD, P))) return rc;
     if ((rc = waveAlloc(ctx, &k.gLast, P))) return rc;
     if ((rc = waveAlloc(ctx, &k.gPend, P))) return rc;
+    if ((rc = waveAlloc(ctx, &k.gRatio, P))) return rc;
     for (int b = 0; b < 2; ++b)
         for (int kind = 0; kind < NUM_KINDS; ++kind)
         {
@@ -855,6 +856,8 @@ static int runAndCollect(skgpu_ctx* ctx, const Wave& w, bool useGraph, bool time
     ctx->lastCounters.stats_overflows = ctl.counters[5];
     ctx->lastCounters.kernel_launches = static_cast<uint64_t>(passes) * (w.sc.guideMode == 2 ? 8 : 7) + 1;
     ctx->lastPasses = passes;
+    ctx->lastGuideWeightSum = ctl.guideWeightSum;
+    ctx->lastGuideEvents = ctl.guideEvents;
     if (w.count > 0 && ctl.done != w.count) return fail(ctx, SKGPU_ERR_DEVICE, "run: not every history finished");
     if (errFlag & 4) return fail(ctx, SKGPU_ERR_TIMEOUT, "run: a traversal exceeded its segment guard");
     if (errFlag & 8) return fail(ctx, SKGPU_ERR_TIMEOUT, "run: a history exceeded the scattering-event guard");
@@ -1363,6 +1366,14 @@ int skgpu_guide_set_training(skgpu_ctx* ctx, int32_t position_bins)
     if (rc) return rc;
     if (position_bins < 0 || position_bins > 64) return fail(ctx, SKGPU_ERR_ARG, "guide: position bins in [0, 64]");
     ctx->guide->positionBins = position_bins;
+    return SKGPU_OK;
+}
+
+int skgpu_guide_last_weights(skgpu_ctx* ctx, uint64_t* events, double* mean_weight)
+{
+    if (!ctx || !events || !mean_weight) return SKGPU_ERR_ARG;
+    *events = ctx->lastGuideEvents;
+    *mean_weight = ctx->lastGuideEvents ? ctx->lastGuideWeightSum / static_cast<double>(ctx->lastGuideEvents) : 0.;
     return SKGPU_OK;
 }
 

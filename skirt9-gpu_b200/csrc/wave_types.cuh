@@ -28,6 +28,8 @@ struct PacketPool
     // instrument so far, last recorded event, event whose start value is still open
     double* gD;
     int *gLast, *gPend;
+    // guided scattering: product of the packet's guiding weight factors so far
+    float* gRatio;
 };
 
 // one buffer of one task kind
@@ -55,6 +57,8 @@ struct Control
     unsigned long long done;
     unsigned long long launchHist0;
     unsigned long long counters[8];  // histories, crossings, scatterings, detections, rfStores, overflows
+    double guideWeightSum;           // guided scattering: sum of the weight factors (mean 1 in expectation)
+    unsigned long long guideEvents;  // guided scattering events
     int err;
 };
 

@@ -578,7 +578,13 @@ SKG_D void interact(const Wave& w, int cur, int nxt, int slot, int m, double sIn
     w.pk.y[slot] = y;
     w.pk.z[slot] = z;
     int nscatt = w.pk.nscatt[slot];
-    if (L <= 0 || (forced && L <= w.pk.Lth[slot] && nscatt >= sc.minScatt))
+    // termination (performLifeCycle, MonteCarloSimulation.cpp:643-660). Under guided scattering the
+    // test applies to the weight without the guiding factors, so that termination depends on the
+    // path alone and the guided runs estimate the same quantity as plain ones (in optically thick
+    // media the threshold L0/minWeightReduction is not small against the emergent flux)
+    double Lterm = L;
+    if (sc.guideMode == 2 && w.pk.gRatio[slot] > 0.f) Lterm = L / static_cast<double>(w.pk.gRatio[slot]);
+    if (L <= 0 || (forced && Lterm <= w.pk.Lth[slot] && nscatt >= sc.minScatt))
     {
         endHistory(w, slot);
         return;
@@ -614,8 +620,9 @@ SKG_D void interact(const Wave& w, int cur, int nxt, int slot, int m, double sIn
 }
 
 // Guided scattering of one packet from the network's raw outputs: the composite density
-// alpha * q_mix + (1 - alpha) * p_HG is sampled and the weight multiplied by p_HG / composite.
-SKG_D void guidedScatter(const Wave& w, int nxt, int slot, const float* o)
+// alpha * q_mix + (1 - alpha) * p_HG is sampled and the weight multiplied by p_HG / composite,
+// which is returned.
+SKG_D double guidedScatter(const Wave& w, int nxt, int slot, const float* o)
 {
     const Scene& sc = w.sc;
     GuideMixture mix;
@@ -625,8 +632,9 @@ SKG_D void guidedScatter(const Wave& w, int nxt, int slot, const float* o)
     double g = sc.mixG[w.pk.ellMix[slot]];
     double kx0 = w.pk.kx[slot], ky0 = w.pk.ky[slot], kz0 = w.pk.kz[slot];
     double kx = kx0, ky = ky0, kz = kz0;
-    double alpha = sc.guideAlpha;
-    if (rng.uniform() < alpha)
+    float ratio = w.pk.gRatio[slot];
+    double alpha = ratio <= GUIDE_RATIO_MAX ? static_cast<double>(sc.guideAlpha) : 0.0;
+    if (alpha > 0.0 && rng.uniform() < alpha)
     {
         double u0 = rng.uniform(), u1 = rng.uniform(), u2 = rng.uniform();
         guideSample(mix, u0, u1, u2, kx, ky, kz);
@@ -638,13 +646,14 @@ SKG_D void guidedScatter(const Wave& w, int nxt, int slot, const float* o)
     double p = pdfHG(g, kx * kx0 + ky * ky0 + kz * kz0);
     double q = exp(static_cast<double>(guideLogDensity(mix, kx, ky, kz)));
     double den = alpha * q + (1.0 - alpha) * p;
-    double wgt = den > 0. ? p / den : 0.;
-    if (!(wgt >= 0.) || !isfinite(wgt))
+    double wgt = p / den;
+    if (!(den > 0.) || !isfinite(den) || !(wgt >= 0.) || !isfinite(wgt))
     {
-        atomicOr(&w.ctl->err, 32);  // non-finite guiding weight: the packet is dropped and flagged
+        atomicOr(&w.ctl->err, 32);  // non-finite guiding density or weight: the packet is dropped and flagged
         wgt = 0.;
     }
     w.pk.L[slot] *= wgt;
+    w.pk.gRatio[slot] = static_cast<float>(ratio * wgt);
     w.pk.kx[slot] = kx;
     w.pk.ky[slot] = ky;
     w.pk.kz[slot] = kz;
@@ -652,6 +661,7 @@ SKG_D void guidedScatter(const Wave& w, int nxt, int slot, const float* o)
     atomicAdd(&w.ctl->counters[2], 1ULL);
     beginPropagation(w, nxt, slot, rng);
     storeRng(w, slot, rng);
+    return wgt;
 }
 
 // guided-scattering stage: the network runs on the tensor cores for 128 queued events per tile
@@ -665,6 +675,8 @@ static __global__ void __launch_bounds__(GM_TILE) guideScatterKernel(const __gri
     GuideTile t;
     guideTileBegin(t, smem, sc.guideBlob);
     bool failed = false;  // uniform across the CTA
+    double wsum = 0.;
+    unsigned wcount = 0;
     for (unsigned tile = blockIdx.x; tile * GM_TILE < n; tile += gridDim.x)
     {
         unsigned i = tile * GM_TILE + threadIdx.x;
@@ -683,11 +695,27 @@ static __global__ void __launch_bounds__(GM_TILE) guideScatterKernel(const __gri
         }
         if (!valid) continue;
         if (failed)
+        {
             endHistory(w, slot);  // the run reports the error; the history is not continued
+        }
         else
-            guidedScatter(w, nxt, slot, o);
+        {
+            wsum += guidedScatter(w, nxt, slot, o);
+            wcount++;
+        }
     }
     guideTileEnd(t);
+    // mean weight factor diagnostics: one atomic per warp
+    for (int off = 16; off > 0; off >>= 1)
+    {
+        wsum += __shfl_down_sync(0xffffffffu, wsum, off);
+        wcount += __shfl_down_sync(0xffffffffu, wcount, off);
+    }
+    if ((threadIdx.x & 31) == 0 && wcount)
+    {
+        atomicAdd(&w.ctl->guideWeightSum, wsum);
+        atomicAdd(&w.ctl->guideEvents, static_cast<unsigned long long>(wcount));
+    }
 }
 
 static __global__ void __launch_bounds__(256) shadeProp2Kernel(const __grid_constant__ Wave w, int cur, int nxt)
@@ -750,6 +778,7 @@ static __global__ void __launch_bounds__(256) launchKernel(const __grid_constant
         w.pk.ellMix[slot] = ell;
         w.pk.ellRF[slot] = sc.rfOn ? wlgBin(sc.rfB, sc.rfNb, sc.rfEll, o.lambda) : -1;
         if (w.anyStats) w.pk.nstat[slot] = 0;
+        if (sc.guideMode == 2) w.pk.gRatio[slot] = 1.f;
         if (sc.guideMode == 1)
         {
             w.pk.gD[slot] = 0.;
@@ -789,6 +818,8 @@ static __global__ void initPoolKernel(const __grid_constant__ Wave w)
         c->done = 0;
         c->launchHist0 = 0;
         for (int k = 0; k < 8; ++k) c->counters[k] = 0;
+        c->guideWeightSum = 0.;
+        c->guideEvents = 0;
         c->err = 0;
     }
 }

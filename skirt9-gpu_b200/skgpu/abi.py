@@ -411,7 +411,7 @@ def last_stage_times(be):
 GUIDE_OFF, GUIDE_RECORD, GUIDE_SAMPLE = 0, 1, 2
 GUIDE_NUM_INPUTS, GUIDE_NUM_OUTPUTS, GUIDE_RECORD_FLOATS = 8, 40, 13
 EXPORTED += ["skgpu_guide_num_params", "skgpu_guide_init", "skgpu_guide_get_params", "skgpu_guide_set_mode",
-             "skgpu_guide_set_training",
+             "skgpu_guide_set_training", "skgpu_guide_last_weights",
              "skgpu_guide_set_importance", "skgpu_guide_record_count", "skgpu_guide_fetch_records",
              "skgpu_guide_train", "skgpu_guide_loss_grad", "skgpu_guide_infer"]
 
@@ -446,6 +446,14 @@ def guide_get_params(be):
 def guide_set_mode(be, mode, target=0, alpha=0.5, record_fraction=1.0, record_capacity=1 << 20):
     _guide_call(be, "guide_set_mode", [C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_uint64], int(mode),
                 int(target), float(alpha), float(record_fraction), int(record_capacity))
+
+
+def guide_last_weights(be):
+    """(guided events, mean weight factor) of the last run."""
+    n, m = C.c_uint64(), C.c_double()
+    _guide_call(be, "guide_last_weights", [C.c_void_p, C.c_void_p], C.cast(C.pointer(n), C.c_void_p),
+                C.cast(C.pointer(m), C.c_void_p))
+    return n.value, m.value
 
 
 def guide_set_training(be, position_bins=0):
