@@ -39,6 +39,9 @@ WORKLOADS = {
                "(hR 6 kpc, hz 0.2 kpc, face-on tau_V=1) on a TreeSpatialGrid octree (max level 8, dust fraction 1e-6, "
                "~5.1e5 leaves), 100 log wavelengths 0.1-10 um with power-law dust, three 512^2 frames at 0/60/90 deg, "
                "radiation field stored on 100 bins; one step = the 1e8-packet primary-emission segment", 100_000_000),
+    "voronoi": ("the galaxy's sources and 100 wavelengths on a Voronoi mesh of 1e6 sites drawn (seed 1234) from the "
+                "dust exp. disk, analytic density per cell, face-on tau_V=2, two 512^2 frames at 0/90 deg, radiation "
+                "field on 100 bins; one step = a 1e7-packet segment (a tenth of the 1e8-packet run)", 10_000_000),
 }
 
 
@@ -97,6 +100,8 @@ def build_scene(name):
         return workloads.shell_cartesian(64, 256)
     if name == "galaxy":
         return workloads.galaxy_octree()
+    if name == "voronoi":
+        return workloads.galaxy_voronoi()
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -142,6 +147,8 @@ def reference_ski(name, npp):
         return ski.shell_cartesian(npp, nbins=64, npix=256)
     if name == "galaxy":
         return ski.galaxy_octree(npp)
+    if name == "voronoi":
+        return ski.galaxy_voronoi(npp)
     raise SystemExit(name)
 
 

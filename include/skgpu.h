@@ -322,6 +322,19 @@ int skgpu_octree_export(const skgpu_octree* tree, double* bounds, int32_t* cell_
                         double* cell_density);
 void skgpu_octree_free(skgpu_octree* tree);
 
+/* ---- standalone Voronoi neighbour construction ----
+ * For scenes not built by SKIRT itself: the face neighbours of the Voronoi cells of n sites inside
+ * the domain box (extent xmin, ymin, zmin, xmax, ymax, zmax), with the domain walls as -1..-6 (xmin,
+ * xmax, ymin, ymax, zmin, zmax): exactly the CSR arrays skgpu_upload_grid_voronoi takes. Cells are
+ * built by clipping the box with bisector planes (threads <= 0: all host cores). No reference
+ * counterpart: in the drop-in case SKIRT's voro++ mesh is uploaded. */
+typedef struct skgpu_voronoi skgpu_voronoi;
+int skgpu_voronoi_build(const double* sites, int32_t n, const double* extent, int32_t threads, skgpu_voronoi** out);
+int skgpu_voronoi_sizes(const skgpu_voronoi* v, int64_t* num_nb);
+/* nb_begin: n + 1 entries, nb_index: num_nb entries */
+int skgpu_voronoi_export(const skgpu_voronoi* v, int32_t* nb_begin, int32_t* nb_index);
+void skgpu_voronoi_free(skgpu_voronoi* v);
+
 #ifdef __cplusplus
 }
 #endif

@@ -48,9 +48,11 @@ struct GridDev
     const int* vNbBegin;
     const int* vNb;
     int vN;
+    const float4* vEnt;    // FP32 walker: per neighbour entry the face's unit normal and its distance from the site
     int vGridN;            // blocks per dimension of the site search grid
     const int* vBlkBegin;  // vGridN^3 + 1
     const int* vBlkSites;  // site indices per block
+    const int* vBlkRep;    // vGridN^3: a site in or near each block (start of the greedy locate)
 
     // tetra: vertices, vertex indices (4 per tet), face normals (12 per tet), neighbour tet and
     // face per face, tet bounding boxes, uniform tet-search grid
@@ -182,7 +184,7 @@ struct CartesianExact : GenBase
     static constexpr int kMinBlocks = 3;
     int i, j, k;
 
-    SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz)
+    SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz, int = -1)
     {
         startRay(x, y, z, ux, uy, uz);
     }
@@ -262,7 +264,7 @@ struct OctreeExact : GenBase
     static constexpr int kMinBlocks = 3;
     int node;
 
-    SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz)
+    SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz, int = -1)
     {
         startRay(x, y, z, ux, uy, uz);
         node = -1;
@@ -391,7 +393,7 @@ struct VoronoiExact : GenBase
     static constexpr int kMinBlocks = 3;
     int mr;
 
-    SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz)
+    SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz, int = -1)
     {
         startRay(x, y, z, ux, uy, uz);
         mr = -1;
@@ -547,7 +549,7 @@ struct TetraExact : GenBase
     int mr;
     int enteringFace;
 
-    SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz)
+    SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz, int = -1)
     {
         startRay(x, y, z, ux, uy, uz);
         mr = -1;

@@ -74,7 +74,7 @@ struct CartesianFast : FastBase<Real>
     static constexpr int kMinBlocks = 4;
     int i, j, k;
 
-    SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz)
+    SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz, int = -1)
     {
         this->startFast(x, y, z, ux, uy, uz);
     }
@@ -123,7 +123,7 @@ struct OctreeLeaf32 : FastBase<float>
     float4 ra, rb;                 // bounds, density and list base of the current cell (record words 0-1)
     float segDens;                 // density of the cell of the segment just returned
 
-    SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz)
+    SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz, int = -1)
     {
         this->startFast(x, y, z, ux, uy, uz);
         cell = -1;
@@ -237,6 +237,190 @@ struct OctreeLeaf32 : FastBase<float>
         }
         if (nb < 0 || nb == old) this->state = GS_OUTSIDE;
         return true;
+    }
+};
+
+
+// Nearest site of a point by a greedy walk on the neighbour graph (the Delaunay graph of the sites,
+// on which the walk towards ever nearer sites ends at the nearest one), starting from the
+// representative site of the point's block in the site-search grid. -1 outside the domain.
+SKG_D int voronoiLocate(const GridDev& g, double x, double y, double z)
+{
+    if (!GenBase::boxContains(g.ext, x, y, z)) return -1;
+    const int n = g.vGridN;
+    auto blk = [&](double v, double lo, double hi) {
+        return min(n - 1, max(0, static_cast<int>((v - lo) / ((hi - lo) / n))));
+    };
+    int c = g.vBlkRep[(blk(x, g.ext[0], g.ext[3]) * n + blk(y, g.ext[1], g.ext[4])) * n + blk(z, g.ext[2], g.ext[5])];
+    for (int guard = 0; guard < 100000; ++guard)
+    {
+        const double* p = g.vSites + 3 * static_cast<size_t>(c);
+        double best = (p[0] - x) * (p[0] - x) + (p[1] - y) * (p[1] - y) + (p[2] - z) * (p[2] - z);
+        int next = -1;
+        for (int e = g.vNbBegin[c]; e < g.vNbBegin[c + 1]; ++e)
+        {
+            int j = __ldg(g.vNb + e);
+            if (j < 0) continue;
+            const double* q = g.vSites + 3 * static_cast<size_t>(j);
+            double d = (q[0] - x) * (q[0] - x) + (q[1] - y) * (q[1] - y) + (q[2] - z) * (q[2] - z);
+            if (d < best)
+            {
+                best = d;
+                next = j;
+            }
+        }
+        if (next < 0) return c;
+        c = next;
+    }
+    return c;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Voronoi mesh, production walker (VoronoiMeshSnapshot::MySegmentGenerator::next,
+// VoronoiMeshSnapshot.cpp:1089-1222). On entering a cell the FP64 position is rebased to FP32
+// coordinates l relative to the cell's site; each face entry holds the outward unit normal n and
+// the plane's distance d from the site (half the site distance, or the distance to a domain wall),
+// and the exit distance through the face is s = (d - n . l) / (n . k). The two
+// smallest exits are re-decided in FP64 from the exact sites when they lie within a near-tie
+// tolerance (FP32 would misorder near-degenerate faces). The face just crossed is skipped (a ray
+// cannot re-enter a convex cell), the position moves exactly onto the exit face, and a cell
+// without a positive exit falls back to the reference's eps step and FP64 nearest-site search.
+// ---------------------------------------------------------------------------------------------
+struct VoronoiLocal32 : GenBase
+{
+    using Acc = float;
+    static constexpr int kMinBlocks = 3;
+    static constexpr int kNone = -99;  // no previous cell (the wall ids -1..-6 are taken)
+    int mr, prev;
+    float kxf, kyf, kzf;
+
+    // the start cell when the caller knows it (a scattering event's interaction cell), else -1
+    int hint;
+
+    SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz, int h = -1)
+    {
+        startRay(x, y, z, ux, uy, uz);
+        hint = h;
+        mr = -1;
+        prev = kNone;
+        kxf = static_cast<float>(ux);
+        kyf = static_cast<float>(uy);
+        kzf = static_cast<float>(uz);
+    }
+
+    // FP64 exit distance through entry e of cell mr (0 when the face is not ahead)
+    SKG_D double exit64(const GridDev& g, int e) const
+    {
+        int mi = g.vNb[e];
+        const double* pr = g.vSites + 3 * static_cast<size_t>(mr);
+        if (mi >= 0)
+        {
+            const double* pi = g.vSites + 3 * static_cast<size_t>(mi);
+            double nx = pi[0] - pr[0], ny = pi[1] - pr[1], nz = pi[2] - pr[2];
+            double nk = nx * kx + ny * ky + nz * kz;
+            if (!(nk > 0)) return 0.;
+            return (nx * (0.5 * (pi[0] + pr[0]) - rx) + ny * (0.5 * (pi[1] + pr[1]) - ry) + nz * (0.5 * (pi[2] + pr[2]) - rz)) / nk;
+        }
+        switch (mi)
+        {
+            case -1: return (g.ext[0] - rx) / kx;
+            case -2: return (g.ext[3] - rx) / kx;
+            case -3: return (g.ext[1] - ry) / ky;
+            case -4: return (g.ext[4] - ry) / ky;
+            case -5: return (g.ext[2] - rz) / kz;
+            case -6: return (g.ext[5] - rz) / kz;
+        }
+        return 0.;
+    }
+
+    SKG_D bool next(const GridDev& g)
+    {
+        if (state == GS_OUTSIDE) return false;
+        if (state == GS_UNKNOWN)
+        {
+            if (!moveInside(g.ext, g.eps)) return false;
+            // a start inside the domain in a known cell needs no search; otherwise a greedy walk
+            mr = (hint >= 0 && ds == 0.) ? hint : voronoiLocate(g, rx, ry, rz);
+            prev = kNone;
+            if (mr < 0)
+            {
+                state = GS_OUTSIDE;
+                return false;
+            }
+            if (ds > 0.) return true;
+        }
+        for (int guard = 0; guard < 64; ++guard)
+        {
+            const double* pr = g.vSites + 3 * static_cast<size_t>(mr);
+            float lx = static_cast<float>(rx - pr[0]);
+            float ly = static_cast<float>(ry - pr[1]);
+            float lz = static_cast<float>(rz - pr[2]);
+            float best = FLT_MAX, second = FLT_MAX, scale = 0.f;
+            int ib = -1, is = -1;
+            int e1 = g.vNbBegin[mr + 1];
+            for (int e = g.vNbBegin[mr]; e < e1; ++e)
+            {
+                float4 q = __ldg(g.vEnt + e);  // unit normal, plane distance from the site
+                float nk = q.x * kxf + q.y * kyf + q.z * kzf;
+                if (!(nk > 0.f)) continue;
+                int mi = __ldg(g.vNb + e);
+                if (mi == prev) continue;
+                float s = (q.w - (q.x * lx + q.y * ly + q.z * lz)) / nk;
+                if (!(s > 0.f)) continue;
+                if (s < best)
+                {
+                    second = best;
+                    is = ib;
+                    best = s;
+                    ib = e;
+                    scale = q.w;
+                }
+                else if (s < second)
+                {
+                    second = s;
+                    is = e;
+                }
+            }
+            if (ib < 0)
+            {
+                // no exit ahead (the point sits on an edge or slightly outside the cell): the
+                // reference's eps step and a fresh nearest-site search
+                propagater(g.eps);
+                mr = voronoiLocate(g, rx, ry, rz);
+                prev = kNone;
+                if (mr < 0)
+                {
+                    state = GS_OUTSIDE;
+                    return false;
+                }
+                continue;
+            }
+            double sq = best;
+            if (is >= 0 && second - best <= 2e-5f * (best + scale))
+            {
+                // near tie: decide with the exact FP64 sites
+                double s1 = exit64(g, ib), s2 = exit64(g, is);
+                if (s2 > 0. && (s2 < s1 || !(s1 > 0.)))
+                {
+                    ib = is;
+                    sq = s2;
+                }
+                else if (s1 > 0.)
+                {
+                    sq = s1;
+                }
+            }
+            int mq = g.vNb[ib];
+            m = mr;
+            ds = sq;
+            propagater(sq);
+            prev = mr;
+            mr = mq;
+            if (mr < 0) state = GS_OUTSIDE;
+            return true;
+        }
+        state = GS_OUTSIDE;
+        return false;
     }
 };
 

@@ -174,6 +174,7 @@ int ensureWaveBuffers(skgpu_ctx* ctx, int P, int groups, int stats)
     if ((rc = waveAlloc(ctx, &k.gLast, P))) return rc;
     if ((rc = waveAlloc(ctx, &k.gPend, P))) return rc;
     if ((rc = waveAlloc(ctx, &k.gRatio, P))) return rc;
+    if ((rc = waveAlloc(ctx, &k.cell, P))) return rc;
     for (int b = 0; b < 2; ++b)
         for (int kind = 0; kind < NUM_KINDS; ++kind)
         {
@@ -490,6 +491,76 @@ int skgpu_upload_grid_voronoi(skgpu_ctx* ctx, int32_t num_sites, const double* s
     if ((rc = gridUpload<int>(ctx, &g.vNb, nb_index, num_nb_index))) return rc;
     if ((rc = gridUpload<int>(ctx, &g.vBlkBegin, cnt.data(), cnt.size()))) return rc;
     if ((rc = gridUpload<int>(ctx, &g.vBlkSites, list.data(), list.size()))) return rc;
+    // a representative site per block: its first site, or for an empty block that of the nearest
+    // filled block found by growing the filled region one block at a time
+    {
+        size_t nb3 = static_cast<size_t>(n) * n * n;
+        std::vector<int> rep(nb3, -1);
+        for (size_t b = 0; b < nb3; ++b)
+            if (cnt[b + 1] > cnt[b]) rep[b] = list[cnt[b]];
+        for (int pass = 0; pass < 3 * n; ++pass)
+        {
+            bool open = false;
+            std::vector<int> nxt = rep;
+            for (int i = 0; i < n; ++i)
+                for (int j = 0; j < n; ++j)
+                    for (int k = 0; k < n; ++k)
+                    {
+                        size_t b = (static_cast<size_t>(i) * n + j) * n + k;
+                        if (rep[b] >= 0) continue;
+                        open = true;
+                        const int di[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
+                        for (const auto& d : di)
+                        {
+                            int a = i + d[0], bb = j + d[1], c = k + d[2];
+                            if (a < 0 || bb < 0 || c < 0 || a >= n || bb >= n || c >= n) continue;
+                            int r = rep[(static_cast<size_t>(a) * n + bb) * n + c];
+                            if (r >= 0)
+                            {
+                                nxt[b] = r;
+                                break;
+                            }
+                        }
+                    }
+            rep.swap(nxt);
+            if (!open) break;
+        }
+        for (int& r : rep)
+            if (r < 0) r = 0;
+        if ((rc = gridUpload<int>(ctx, &g.vBlkRep, rep.data(), rep.size()))) return rc;
+    }
+    // entries of the FP32 walker: per face the outward unit normal and the distance of the face's
+    // plane from the site (half the site distance for a neighbour, the distance to the domain wall
+    // for a wall), so that s = (d - n . l) / (n . k) needs no squares of metre-scale coordinates
+    std::vector<float4> ent(std::max(num_nb_index, 1));
+    for (int c = 0; c < num_sites; ++c)
+    {
+        const double* pc = sites + 3 * static_cast<size_t>(c);
+        for (int e = nb_begin[c]; e < nb_begin[c + 1]; ++e)
+        {
+            int mi = nb_index[e];
+            double n[3] = {0, 0, 0}, d = 0;
+            if (mi >= 0)
+            {
+                const double* pi = sites + 3 * static_cast<size_t>(mi);
+                for (int a = 0; a < 3; ++a) n[a] = pi[a] - pc[a];
+                double len = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+                if (len > 0)
+                    for (int a = 0; a < 3; ++a) n[a] /= len;
+                d = 0.5 * len;
+            }
+            else
+            {
+                int a = (-mi - 1) >> 1;
+                bool upper = ((-mi - 1) & 1) != 0;
+                n[a] = upper ? 1.0 : -1.0;
+                d = upper ? extent[3 + a] - pc[a] : pc[a] - extent[a];
+            }
+            ent[e] = make_float4(static_cast<float>(n[0]), static_cast<float>(n[1]), static_cast<float>(n[2]),
+                                 static_cast<float>(d));
+        }
+    }
+    if ((rc = gridUpload<float4>(ctx, &g.vEnt, ent.data(), ent.size()))) return rc;
     ctx->hasGrid = true;
     return SKGPU_OK;
 }

@@ -19,6 +19,7 @@ struct PacketPool
     double* rngSpare;
     int* rngHas;
     int *nscatt, *ellMix, *ellRF;
+    int* cell;  // cell of the last interaction (-1 after launch): start-cell hint of the next rays
     // per-history statistics buffer (only when an instrument records statistics)
     unsigned long long* skey;  // P * STATS_CAP
     double* sw;

@@ -251,12 +251,13 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __g
                     {
                         const InstrDev& in = sc.instr[b.info[idx] & 0xFF];
                         fA = static_cast<Acc>(log(b.par[idx]) + 745.);  // taumax = log(L) + 745
-                        wk.start(sc.g, b.x[idx], b.y[idx], b.z[idx], in.kobs[0], in.kobs[1], in.kobs[2]);
+                        wk.start(sc.g, b.x[idx], b.y[idx], b.z[idx], in.kobs[0], in.kobs[1], in.kobs[2],
+                                 w.pk.cell ? w.pk.cell[slot] : -1);
                     }
                     else
                     {
                         wk.start(sc.g, w.pk.x[slot], w.pk.y[slot], w.pk.z[slot], w.pk.kx[slot], w.pk.ky[slot],
-                                 w.pk.kz[slot]);
+                                 w.pk.kz[slot], w.pk.cell ? w.pk.cell[slot] : -1);
                         if (kind == K_PROP1)
                         {
                             fA = static_cast<Acc>(w.pk.L[slot]);
@@ -309,8 +310,10 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __g
                         Acc extEnd = aexp(lnExtEnd);
                         if (m >= 0)
                         {
-                            Acc Lds = fA * lnmean4(extEnd, fC, lnExtEnd, fB) * ds;
-                            atomicAdd(sc.rf + static_cast<size_t>(m) * sc.nrf + iA, static_cast<double>(Lds));
+                            // L * ds exceeds the FP32 range (watts times metres): the product is FP64
+                            double Lds = static_cast<double>(fA) * static_cast<double>(lnmean4(extEnd, fC, lnExtEnd, fB))
+                                         * static_cast<double>(ds);
+                            atomicAdd(sc.rf + static_cast<size_t>(m) * sc.nrf + iA, Lds);
                             rfStores++;
                         }
                         fB = lnExtEnd;
@@ -577,6 +580,7 @@ SKG_D void interact(const Wave& w, int cur, int nxt, int slot, int m, double sIn
     w.pk.x[slot] = x;
     w.pk.y[slot] = y;
     w.pk.z[slot] = z;
+    if (w.pk.cell) w.pk.cell[slot] = m;
     int nscatt = w.pk.nscatt[slot];
     // termination (performLifeCycle, MonteCarloSimulation.cpp:643-660). Under guided scattering the
     // test applies to the weight without the guiding factors, so that termination depends on the
@@ -778,6 +782,7 @@ static __global__ void __launch_bounds__(256) launchKernel(const __grid_constant
         w.pk.ellMix[slot] = ell;
         w.pk.ellRF[slot] = sc.rfOn ? wlgBin(sc.rfB, sc.rfNb, sc.rfEll, o.lambda) : -1;
         if (w.anyStats) w.pk.nstat[slot] = 0;
+        if (w.pk.cell) w.pk.cell[slot] = -1;
         if (sc.guideMode == 2) w.pk.gRatio[slot] = 1.f;
         if (sc.guideMode == 1)
         {

@@ -500,3 +500,33 @@ def guide_infer(be, inputs, tensor_cores=True):
     _guide_call(be, "guide_infer", [C.c_int32, C.c_void_p, C.c_void_p, C.c_int32], len(x), _ptr(x), _ptr(out),
                 1 if tensor_cores else 0)
     return out
+
+
+EXPORTED += ["skgpu_voronoi_build", "skgpu_voronoi_sizes", "skgpu_voronoi_export", "skgpu_voronoi_free"]
+
+
+def build_voronoi(sites, extent, threads=0, lib=None):
+    """Face neighbours of the Voronoi cells of the sites in the domain box (walls -1..-6): the CSR
+    arrays (nb_begin, nb_index) that skgpu_upload_grid_voronoi takes."""
+    lib = lib if lib is not None else load_library()
+    s = f64(sites).reshape(-1, 3)
+    e = f64(extent)
+    v = C.c_void_p()
+    lib.skgpu_voronoi_build.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.POINTER(C.c_void_p)]
+    lib.skgpu_voronoi_build.restype = C.c_int
+    lib.skgpu_voronoi_sizes.argtypes = [C.c_void_p, C.c_void_p]
+    lib.skgpu_voronoi_export.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.skgpu_voronoi_free.argtypes = [C.c_void_p]
+    lib.skgpu_voronoi_free.restype = None
+    rc = lib.skgpu_voronoi_build(_ptr(s), len(s), _ptr(e), int(threads), C.byref(v))
+    if rc != OK:
+        raise SkgpuError(rc, "voronoi build failed")
+    try:
+        nb = C.c_int64()
+        lib.skgpu_voronoi_sizes(v, C.cast(C.pointer(nb), C.c_void_p))
+        begin = np.zeros(len(s) + 1, np.int32)
+        index = np.zeros(max(nb.value, 1), np.int32)
+        lib.skgpu_voronoi_export(v, _ptr(begin), _ptr(index))
+    finally:
+        lib.skgpu_voronoi_free(v)
+    return begin, index[:nb.value]

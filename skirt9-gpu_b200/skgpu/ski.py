@@ -174,6 +174,26 @@ def galaxy_octree(num_packets=1e8, npix=512, nlambda=100, max_level=8, max_dust_
                       instrument_wlg=wlg, store_rf=store_rf, rf_wlg=wlg)
 
 
+def galaxy_voronoi(num_packets=1e8, npix=512, nlambda=100, num_sites=1_000_000, tau_v=2.0, half_size_kpc=25,
+                   store_rf=True):
+    """The galaxy of galaxy_octree on a VoronoiMeshSpatialGrid whose sites the reference draws from
+    the dust density (1e6 sites), face-on tau_V = 2, two frames at 0 and 90 degrees."""
+    lam = [0.1 * (100.0 ** (i / (nlambda - 1))) for i in range(nlambda)]
+    kappa = [(l / 0.55) ** -1.0 for l in lam]
+    albedo = [min(0.9, max(0.05, 0.5 * (l / 0.55) ** -0.2)) for l in lam]
+    g = [min(0.9, max(0.0, 0.6 * (l / 0.55) ** -0.3)) for l in lam]
+    mix = mean_list_mix(lam, kappa, albedo, g)
+    sources = (geometric_source('<ExpDiskGeometry scaleLength="4 kpc" scaleHeight="0.35 kpc" minRadius="0 kpc" '
+                                'maxRadius="0 kpc" maxZ="0 kpc"/>', 6000, 8e9)
+               + geometric_source('<SersicGeometry effectiveRadius="1 kpc" index="4"/>', 4000, 2e9))
+    wlg = f'<LogWavelengthGrid minWavelength="0.1 micron" maxWavelength="10 micron" numWavelengths="{nlambda}"/>'
+    fov = 2 * half_size_kpc
+    instruments = "".join(frame_instrument(f"i{inc}", inc, fov, "kpc", npix, stats=False) for inc in (0, 90))
+    return simulation("ExtinctionOnly", num_packets, sources, expdisk_medium(6, 0.2, "kpc", tau_v, mix),
+                      voronoi_grid(half_size_kpc, "kpc", num_sites), instruments,
+                      instrument_wlg=wlg, store_rf=store_rf, rf_wlg=wlg)
+
+
 def shell_cartesian(num_packets=1e6, nbins=64, npix=256, stats=True, points=None):
     """Dust shell (r^-2 between 0.1 and 1 pc, radial tau_V = 1, i.e. tau_X = 2 through the centre) on a
     Cartesian grid of +-1 pc, isotropic point source at the centre, 0.55 micron, HG g = 0.6,

@@ -133,7 +133,7 @@ def test_gpu_edge_cases(golden, gpu_backend):
         gpu_backend.upload_grid_cartesian([0, 1], [1, 0], [0, 1])  # descending borders
 
 
-@pytest.mark.parametrize("name", ["cartesian_selftest", "cartesian_c16", "octree"])
+@pytest.mark.parametrize("name", ["cartesian_selftest", "cartesian_c16", "octree", "voronoi"])
 def test_gpu_fp32_paths_close_to_reference(golden, gpu_backend, name):
     """FP32-distance walkers: cell sequences equal the reference's except for rays grazing a cell
     edge; segment lengths within 1e-5 of the path length; optical depths within 1e-5."""
@@ -181,3 +181,37 @@ def test_gpu_galaxy_octree_matches_oracle(gpu_backend, oracle_backend):
     rg, ro = run_both(sc, gpu_backend, oracle_backend, 3000, seed=17)
     assert_close_runs(rg, ro, frac=0.99)
     assert rg.rf.sum() == pytest.approx(ro.rf.sum(), rel=1e-6)
+
+
+def test_gpu_fp32_voronoi_lifecycle_close_to_fp64(gpu_backend):
+    """Production Voronoi walker (FP32 local distances, FP64 near-tie predicate) on a panchromatic
+    galaxy mesh: the same histories as the FP64 reference-order walker, tallies far inside the noise."""
+    from skgpu import workloads
+    sc = workloads.galaxy_voronoi(n_sites=20000, npix=64, nlambda=20)
+    sc.upload(gpu_backend)
+    n = 40000
+    r64 = sc.run(gpu_backend, n, seed=13)
+    r32 = sc.run(gpu_backend, n, seed=13, precision=abi.PREC_FP32)
+    for a, b in zip(r64.instruments, r32.instruments):
+        assert b["total"].sum() == pytest.approx(a["total"].sum(), rel=2e-3)
+        assert np.mean(np.isclose(a["total"], b["total"], rtol=1e-3, atol=0)) > 0.9
+    assert r32.rf.sum() == pytest.approx(r64.rf.sum(), rel=2e-3)
+    assert r32.counters["crossings"] == pytest.approx(r64.counters["crossings"], rel=1e-3)
+
+
+def test_gpu_fp32_octree_lifecycle_close_to_fp64(gpu_backend):
+    """Production octree walker with FP32 accumulators on the panchromatic galaxy: images and the
+    radiation field (whose L * ds products exceed the FP32 range and are formed in FP64) follow the
+    FP64 reference-order walker on the same histories."""
+    from skgpu import workloads
+    sc = workloads.galaxy_octree(npix=64, nlambda=20, max_level=6, max_dust_fraction=1e-5)
+    sc.upload(gpu_backend)
+    n = 40000
+    r64 = sc.run(gpu_backend, n, seed=19)
+    r32 = sc.run(gpu_backend, n, seed=19, precision=abi.PREC_FP32)
+    for a, b in zip(r64.instruments, r32.instruments):
+        assert b["total"].sum() == pytest.approx(a["total"].sum(), rel=2e-3)
+    assert np.all(np.isfinite(r32.rf))
+    assert r32.rf.sum() == pytest.approx(r64.rf.sum(), rel=2e-3)
+    lit = r64.rf > 0
+    assert np.median(np.abs(r32.rf[lit] / r64.rf[lit] - 1)) < 1e-3
