@@ -335,6 +335,22 @@ int skgpu_voronoi_sizes(const skgpu_voronoi* v, int64_t* num_nb);
 int skgpu_voronoi_export(const skgpu_voronoi* v, int32_t* nb_begin, int32_t* nb_index);
 void skgpu_voronoi_free(skgpu_voronoi* v);
 
+/* ---- standalone Delaunay tetrahedralisation ----
+ * For scenes not built by SKIRT itself: the Delaunay tetrahedra of n points strictly inside the
+ * domain box, joined by the box's 8 corners (vertices n..n+7, as TetraMeshSpatialGrid adds them),
+ * in the form skgpu_upload_grid_tetra takes: positively oriented tetrahedra, face f opposite vertex
+ * f, per face the neighbouring tetrahedron (-1 on the hull) and its face index, outward unit
+ * normals. Built as the dual of the Voronoi cells. No reference counterpart: in the drop-in case
+ * SKIRT's TetGen mesh is uploaded. */
+typedef struct skgpu_tetra skgpu_tetra;
+int skgpu_tetra_build(const double* points, int32_t n, const double* extent, int32_t threads, skgpu_tetra** out);
+int skgpu_tetra_sizes(const skgpu_tetra* t, int32_t* num_vertices, int32_t* num_tetra);
+/* vertices 3 x num_vertices, tetra 4 x num_tetra, face_normals 12 x num_tetra, face_ntetra and
+ * face_nface 4 x num_tetra; any may be NULL */
+int skgpu_tetra_export(const skgpu_tetra* t, double* vertices, int32_t* tetra, double* face_normals,
+                       int32_t* face_ntetra, int32_t* face_nface);
+void skgpu_tetra_free(skgpu_tetra* t);
+
 #ifdef __cplusplus
 }
 #endif

@@ -424,4 +424,15 @@ struct VoronoiLocal32 : GenBase
     }
 };
 
+
+// ---------------------------------------------------------------------------------------------
+// Tetrahedral mesh, production walker: the face-crossing decision stays the reference's FP64
+// Plucker test (FP32 would misorder near-degenerate faces), while optical depth, path length and
+// the radiation-field factors accumulate in FP32 like the other production walkers.
+// ---------------------------------------------------------------------------------------------
+struct TetraFast : TetraExact
+{
+    using Acc = float;
+};
+
 }  // namespace skg

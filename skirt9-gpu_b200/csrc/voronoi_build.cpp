@@ -9,6 +9,7 @@
 // plane by the intersections of the new plane with the cut edges. The planes left with vertices are
 // the cell's faces; their owners are the neighbours, with the domain walls numbered -1..-6 (xmin,
 // xmax, ymin, ymax, zmin, zmax) as in VoronoiMeshSnapshot (VoronoiMeshSnapshot.cpp:725-740).
+
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -133,28 +134,13 @@ struct Cell
             if (count[i] >= 3) nb.push_back(planes[i].owner);
     }
 };
-
-}  // namespace
-
-struct skgpu_voronoi
+// Builds the Voronoi cell of every site (clipped by clipExt) on `threads` threads and hands each
+// finished cell to visit(site, cell, worker). The site-search grid spans searchExt. Returns false
+// if a cell degenerated.
+template<typename Visit>
+bool buildCells(const double* sites, int n, const double* searchExt, const double* clipExt, int threads, Visit visit)
 {
-    int n = 0;
-    std::vector<int32_t> begin;  // n + 1
-    std::vector<int32_t> index;
-};
-
-extern "C" {
-
-int skgpu_voronoi_build(const double* sites, int32_t n, const double* extent, int32_t threads, skgpu_voronoi** out)
-{
-    if (!out) return SKGPU_ERR_ARG;
-    *out = nullptr;
-    if (!sites || !extent || n < 1) return SKGPU_ERR_ARG;
-    const double* e = extent;
-    if (!(e[3] > e[0] && e[4] > e[1] && e[5] > e[2])) return SKGPU_ERR_ARG;
-    for (int64_t i = 0; i < 3 * static_cast<int64_t>(n); ++i)
-        if (!std::isfinite(sites[i])) return SKGPU_ERR_ARG;
-    // uniform site grid with about 2 sites per block
+    const double* e = searchExt;
     int g = std::max(1, static_cast<int>(std::cbrt(n / 2.0)));
     double sz[3] = {(e[3] - e[0]) / g, (e[4] - e[1]) / g, (e[5] - e[2]) / g};
     auto blockOf = [&](const double* p, int a) {
@@ -177,19 +163,17 @@ int skgpu_voronoi_build(const double* sites, int32_t n, const double* extent, in
         }
     }
     double minSz = std::min(sz[0], std::min(sz[1], sz[2]));
-
-    std::vector<std::vector<int32_t>> nbs(n);
     std::atomic<int> next{0};
     std::atomic<bool> bad{false};
-    auto work = [&]() {
+    auto work = [&](int worker) {
         Cell cell;
         std::vector<std::pair<double, int>> cand;
         for (;;)
         {
             int i = next.fetch_add(1);
-            if (i >= n) break;
+            if (i >= n || bad) break;
             const double* s = sites + 3 * static_cast<size_t>(i);
-            cell.box(e);
+            cell.box(clipExt);
             int bi[3] = {blockOf(s, 0), blockOf(s, 1), blockOf(s, 2)};
             // shells of blocks at Chebyshev distance r; sites in shell r are at least (r-1) * minSz away
             for (int r = 0; r <= g; ++r)
@@ -218,8 +202,8 @@ int skgpu_voronoi_build(const double* sites, int32_t n, const double* extent, in
                 for (const auto& cj : cand)
                 {
                     if (cj.first > 4.0 * cell.maxDist2(s)) break;
-                    const double* q = sites + 3 * static_cast<size_t>(cj.second);
                     if (cj.first == 0.0) continue;  // coincident sites share no face
+                    const double* q = sites + 3 * static_cast<size_t>(cj.second);
                     Plane pl;
                     for (int a = 0; a < 3; ++a) pl.n[a] = q[a] - s[a];
                     pl.c = 0.5 * (pl.n[0] * (q[0] + s[0]) + pl.n[1] * (q[1] + s[1]) + pl.n[2] * (q[2] + s[2]));
@@ -232,18 +216,44 @@ int skgpu_voronoi_build(const double* sites, int32_t n, const double* extent, in
                 }
                 if (bad) break;
             }
-            std::vector<int32_t>& nb = nbs[i];
-            std::vector<int> f;
-            cell.faces(f);
-            nb.assign(f.begin(), f.end());
+            if (!bad) visit(i, cell, worker);
         }
     };
     int T = threads > 0 ? threads : static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
     T = std::min(T, 64);
     std::vector<std::thread> pool;
-    for (int t = 0; t < T; ++t) pool.emplace_back(work);
+    for (int t = 0; t < T; ++t) pool.emplace_back(work, t);
     for (std::thread& t : pool) t.join();
-    if (bad) return SKGPU_ERR_DEVICE;
+    return !bad;
+}
+
+}  // namespace
+
+struct skgpu_voronoi
+{
+    int n = 0;
+    std::vector<int32_t> begin;  // n + 1
+    std::vector<int32_t> index;
+};
+
+extern "C" {
+
+int skgpu_voronoi_build(const double* sites, int32_t n, const double* extent, int32_t threads, skgpu_voronoi** out)
+{
+    if (!out) return SKGPU_ERR_ARG;
+    *out = nullptr;
+    if (!sites || !extent || n < 1) return SKGPU_ERR_ARG;
+    const double* e = extent;
+    if (!(e[3] > e[0] && e[4] > e[1] && e[5] > e[2])) return SKGPU_ERR_ARG;
+    for (int64_t i = 0; i < 3 * static_cast<int64_t>(n); ++i)
+        if (!std::isfinite(sites[i])) return SKGPU_ERR_ARG;
+    std::vector<std::vector<int32_t>> nbs(n);
+    bool ok = buildCells(sites, n, e, e, threads, [&](int i, const Cell& cell, int) {
+        std::vector<int> f;
+        cell.faces(f);
+        nbs[i].assign(f.begin(), f.end());
+    });
+    if (!ok) return SKGPU_ERR_DEVICE;
     skgpu_voronoi* v = new skgpu_voronoi();
     v->n = n;
     v->begin.resize(static_cast<size_t>(n) + 1, 0);
@@ -272,3 +282,4 @@ int skgpu_voronoi_export(const skgpu_voronoi* v, int32_t* nb_begin, int32_t* nb_
 void skgpu_voronoi_free(skgpu_voronoi* v) { delete v; }
 
 }  // extern "C"
+

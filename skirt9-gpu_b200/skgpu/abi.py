@@ -530,3 +530,34 @@ def build_voronoi(sites, extent, threads=0, lib=None):
     finally:
         lib.skgpu_voronoi_free(v)
     return begin, index[:nb.value]
+
+
+EXPORTED += ["skgpu_tetra_build", "skgpu_tetra_sizes", "skgpu_tetra_export", "skgpu_tetra_free"]
+
+
+def build_tetra(points, extent, threads=0, lib=None):
+    """Delaunay tetrahedra of the points and the domain's 8 corners, as the dict of arrays
+    skgpu_upload_grid_tetra takes (vertices, tetra, normals, ntetra, nface)."""
+    lib = lib if lib is not None else load_library()
+    p = f64(points).reshape(-1, 3)
+    e = f64(extent)
+    t = C.c_void_p()
+    lib.skgpu_tetra_build.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.POINTER(C.c_void_p)]
+    lib.skgpu_tetra_build.restype = C.c_int
+    lib.skgpu_tetra_sizes.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.skgpu_tetra_export.argtypes = [C.c_void_p] * 6
+    lib.skgpu_tetra_free.argtypes = [C.c_void_p]
+    lib.skgpu_tetra_free.restype = None
+    rc = lib.skgpu_tetra_build(_ptr(p), len(p), _ptr(e), int(threads), C.byref(t))
+    if rc != OK:
+        raise SkgpuError(rc, "tetra build failed")
+    try:
+        nv, nt = C.c_int32(), C.c_int32()
+        lib.skgpu_tetra_sizes(t, C.cast(C.pointer(nv), C.c_void_p), C.cast(C.pointer(nt), C.c_void_p))
+        out = dict(vertices=np.zeros((nv.value, 3)), tetra=np.zeros((nt.value, 4), np.int32),
+                   normals=np.zeros((nt.value, 4, 3)), ntetra=np.zeros((nt.value, 4), np.int32),
+                   nface=np.zeros((nt.value, 4), np.int32))
+        lib.skgpu_tetra_export(t, *[_ptr(out[k]) for k in ("vertices", "tetra", "normals", "ntetra", "nface")])
+    finally:
+        lib.skgpu_tetra_free(t)
+    return out

@@ -133,7 +133,7 @@ def test_gpu_edge_cases(golden, gpu_backend):
         gpu_backend.upload_grid_cartesian([0, 1], [1, 0], [0, 1])  # descending borders
 
 
-@pytest.mark.parametrize("name", ["cartesian_selftest", "cartesian_c16", "octree", "voronoi"])
+@pytest.mark.parametrize("name", ["cartesian_selftest", "cartesian_c16", "octree", "voronoi", "tetra"])
 def test_gpu_fp32_paths_close_to_reference(golden, gpu_backend, name):
     """FP32-distance walkers: cell sequences equal the reference's except for rays grazing a cell
     edge; segment lengths within 1e-5 of the path length; optical depths within 1e-5."""
