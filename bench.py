@@ -42,6 +42,11 @@ WORKLOADS = {
     "voronoi": ("the galaxy's sources and 100 wavelengths on a Voronoi mesh of 1e6 sites drawn (seed 1234) from the "
                 "dust exp. disk, analytic density per cell, face-on tau_V=2, two 512^2 frames at 0/90 deg, radiation "
                 "field on 100 bins; one step = a 1e7-packet segment (a tenth of the 1e8-packet run)", 10_000_000),
+    "batch": ("16 independent galaxies on Delaunay tetrahedral meshes (TetraMeshSpatialGrid), parameters from "
+              "default_rng(2024): vertex counts log-uniform 1e4-4e5 (half uniform in the box, half from the dust "
+              "disk), face-on tau_V log-uniform 0.1-10, packets log-uniform 1e6-1e7 (7.1e7 in all), 32 log "
+              "wavelengths, one 256^2 frame each; one step = every simulation's full primary-emission segment, "
+              "traced as one batched wavefront", 0),
 }
 
 
@@ -121,12 +126,16 @@ def trace_algorithmic_bytes(counters, grid_kind):
     return BYTES_PER_CROSSING[grid_kind] * counters["crossings"] + 16 * counters["rf_stores"]
 
 
-def reference_run(scene_ski, npp, threads):
-    """Runs the reference CPU code on a ski file; returns (packets/s of the primary segment, secs)."""
+def reference_run(scene_ski, npp, threads, files=None):
+    """Runs the reference CPU code on a ski file (plus input files {name: text} beside it); returns
+    (packets/s of the primary segment, secs)."""
     with tempfile.TemporaryDirectory() as tmp:
         path = os.path.join(tmp, "bench.ski")
         with open(path, "w") as f:
             f.write(scene_ski)
+        for fname, text in (files or {}).items():
+            with open(os.path.join(tmp, fname), "w") as f:
+                f.write(text)
         out = subprocess.run([REF_SKIRT, "-t", str(threads), "bench.ski"], cwd=tmp, capture_output=True, text=True)
         if out.returncode != 0:
             raise RuntimeError("reference run failed: " + out.stdout[-500:] + out.stderr[-500:])
@@ -152,9 +161,37 @@ def reference_ski(name, npp):
     raise SystemExit(name)
 
 
+def reference_batch(indices, fraction, cores):
+    """The reference on simulations `indices` of the batched workload, each with `fraction` of its
+    packets (one skirt run per simulation, as the reference would run the batch); returns (packets/s
+    over the primary segments, packets, secs)."""
+    from skgpu import ski, workloads
+    spec = workloads.tetra_batch_spec()
+    tot_n, tot_s = 0, 0.0
+    for i in indices:
+        sp = spec[i]
+        n = max(1000, int(sp["packets"] * fraction))
+        pts = workloads.tetra_points(sp["num_vertices"], sp["point_seed"])
+        _, secs = reference_run(ski.galaxy_tetra(n, "vertices.txt", sp["tau_v"]), n, cores,
+                                {"vertices.txt": ski.vertex_file_text(pts)})
+        tot_n += n
+        tot_s += secs
+    return tot_n / max(tot_s, 1e-3), tot_n, tot_s
+
+
 def cpu_baseline(name, budget_s=20.0):
     """The reference's own multithreaded CPU path on the host cores, on a bounded sample."""
     cores = os.cpu_count() or 1
+    if name == "batch":
+        if not os.path.exists(REF_SKIRT):
+            return {"value": None, "error": "reference build oracle/_ref missing"}
+        idx = [0, 4, 8, 12]
+        rate, _, _ = reference_batch(idx[:1], 0.0025, cores)
+        frac = min(1.0, rate * budget_s / 71e6 * 4)  # about budget_s of primary emission over 4 simulations
+        rate, n, secs = reference_batch(idx, frac, cores)
+        return {"value": rate, "unit": "packets/s", "cores": cores, "kind": "reference",
+                "sample": f"simulations {idx} of the batch, {frac:.4f} of their packets ({n} in all), one skirt -t "
+                          f"{cores} run each, primary-emission segments {secs:.2f} s (setup excluded)"}
     if os.path.exists(REF_SKIRT):
         probe = 20000
         rate, secs = reference_run(reference_ski(name, probe), probe, cores)
@@ -184,6 +221,8 @@ def run_reference_arm(args, rank, world):
                           "it where the reference sources are present)"}))
         return
     cores = os.cpu_count() or 1
+    if name == "batch":
+        return run_reference_batch_arm(args, cores)
     probe = 20000
     rate, _ = reference_run(reference_ski(name, probe), probe, cores)
     npp = int(min(5e7, max(probe, rate * 8.0)))
@@ -204,6 +243,161 @@ def run_reference_arm(args, rank, world):
                              "sample": f"{npp} packets per step, skirt -t {cores}, primary-emission segment"},
             "e2e": {"value": value, "unit": "packets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
+
+
+def run_reference_batch_arm(args, cores):
+    """The batch on the reference: 16 sequential skirt runs per step, each on a sample of its
+    packets sized so the primary segments of a step take about 8 s."""
+    rate, _, _ = reference_batch([0], 0.0025, cores)
+    frac = min(1.0, rate * 8.0 / 71e6)
+    reference_batch([1], 0.001, cores)  # warm-up: one small run
+    vals, npp = [], 0
+    for _ in range(args.steps):
+        r, npp, _ = reference_batch(range(16), frac, cores)
+        vals.append(r)
+    value = statistics.median(vals)
+    print(json.dumps({
+        "metric": "packets/s on 1 B200", "value": value, "unit": "packets/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": 1, "ms_per_step": 1e3 * npp / value, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": {"workload": "batch", "description": WORKLOADS["batch"][0], "packets_per_step": npp,
+                   "packet_fraction": frac, "l2": "n/a (CPU)"},
+        "cpu_baseline": {"value": value, "unit": "packets/s", "cores": cores, "kind": "reference",
+                         "sample": f"16 sequential skirt -t {cores} runs per step, {frac:.4f} of each simulation's "
+                                   f"packets ({npp} in all), primary-emission segments (setup excluded)"},
+        "e2e": {"value": value, "unit": "packets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+def run_batch_arm(args, rank, world, local):
+    """Our arm on the batched workload: the 16 simulations (one context each) traced as one
+    wavefront per step through skgpu_run_batch. Under torchrun every rank runs its own batch (the
+    same meshes, rank-dependent random seeds: weak scaling)."""
+    import torch
+    from skgpu import Backend, abi, workloads
+
+    torch.cuda.set_device(local)
+    scenes, spec = workloads.tetra_batch()
+    n = len(scenes)
+    packets = [s["packets"] for s in spec]
+    seeds = [s["seed"] + 1000003 * rank for s in spec]
+    prec = abi.PREC_FP64_EXACT if args.precision == "fp64" else abi.PREC_FP32
+    bes = [Backend(device=local) for _ in scenes]
+    for sc, be, npp, sd in zip(scenes, bes, packets, seeds):
+        sc.upload(be)
+        sc.prepare(be, npp, sd, prec)
+    be0 = bes[0]
+    zeros = [0] * n
+    per_gpu = sum(packets)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")
+
+    def step():
+        abi.run_batch(bes, zeros, packets, packets)
+        return be0.last_run_ms()
+
+    for _ in range(args.warmup):
+        step()
+    abi.set_stage_timing(be0, 1)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms, trace_ms, trace_launches, counters = [], 0.0, 0, None
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            ms.append(step())
+            counters = be0.counters()
+            t_ms, t_n = abi.last_stage_times(be0)["trace"]
+            trace_ms += t_ms
+            trace_launches += t_n
+    torch.cuda.synchronize()
+    abi.set_stage_timing(be0, 0)
+    total_ms = max_over_ranks(float(sum(ms)), world, local)
+    value = per_gpu * world * args.steps / (total_ms / 1e3)
+
+    e2e = None
+    if not args.no_e2e:
+        dens = [torch.from_numpy(np.ascontiguousarray(sc.density)).pin_memory().numpy() for sc in scenes]
+        sizes = [sc.instrument_size(0) for sc in scenes]
+        host = [np.zeros(k) for k in sizes]
+        h2d = sum(d.nbytes for d in dens)
+        d2h = 8 * sum(sizes)
+        times = []
+        for _ in range(max(1, min(args.steps, 2))):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for be, d in zip(bes, dens):
+                be.clear_tallies()
+                be.upload_medium(d)
+            abi.run_batch(bes, zeros, packets, packets)
+            for be, k, hbuf in zip(bes, sizes, host):
+                be.fetch_instrument(0, k, stats=False, out=hbuf)
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+        e2e_s = max_over_ranks(statistics.median(times), world, local)
+        e2e = {"value": per_gpu * world / e2e_s, "unit": "packets/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h}
+
+    if rank == 0:
+        line = result_line(args, "batch", world, value, total_ms, trace_ms, trace_launches, counters, abi.GRID_TETRA,
+                           prec, clk, e2e, per_gpu)
+        line["config"]["simulations"] = n
+        line["config"]["launch_shape"] = "default (pool 2^20 slots, resident traversal blocks, 4 stage blocks/SM)"
+        if not args.no_cpu_baseline:
+            try:
+                line["cpu_baseline"] = cpu_baseline("batch")
+            except Exception as e:
+                line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+        print(json.dumps(line))
+    for be in bes:
+        be.close()
+
+
+def max_over_ranks(x, world, local):
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def result_line(args, name, world, value, total_ms, trace_ms, trace_launches, counters, kind, prec, clk, e2e,
+                per_gpu):
+    """The JSON line of our arm; the roofline is that of the traversal kernel: its algorithmic bytes per
+    launch over its average launch duration (CUDA events on the launch stream, timed steps)."""
+    from skgpu import abi
+    peak, peak_kind = peaks()
+    trace_bytes_per_launch = trace_algorithmic_bytes(counters, kind) / max(1, trace_launches / args.steps)
+    trace_avg_ms = trace_ms / max(1, trace_launches)
+    achieved = trace_bytes_per_launch / (trace_avg_ms / 1e3) / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", f"trace_kernel_{name}_{args.precision}.json")
+    if os.path.exists(prof):
+        with open(prof) as f:
+            ratio = json.load(f).get("dram_bytes_per_algorithmic_byte")
+        if ratio:
+            traffic = ratio * trace_bytes_per_launch
+    return {
+        "metric": "packets/s on 1 B200", "value": value, "unit": "packets/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == abi.PREC_FP64_EXACT else "f32+f64",
+        "data": "synthetic",
+        "config": {"workload": name, "description": WORKLOADS[name][0], "packets_per_step_per_gpu": per_gpu,
+                   "traversal": args.precision, "l2": "flushed between steps (256 MB write)",
+                   "parallelism": f"history ranges x{world}" if name != "batch" else f"independent batches x{world}"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_kind": peak_kind, "kernel": "skg::traceKernel",
+                     "launches_per_step": trace_launches / args.steps, "avg_launch_ms": trace_avg_ms,
+                     "algorithmic_bytes_per_launch": trace_bytes_per_launch,
+                     "share_of_step": trace_ms / max(total_ms, 1e-9)},
+        "clocks": clk.summary(),
+        "e2e": e2e,
+        "gpu_launches": int(counters["kernel_launches"]) * args.steps,
+        "counters_per_step": counters,
+    }
 
 
 def main():
@@ -232,6 +426,13 @@ def main():
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
         if dist:
+            dist.destroy_process_group()
+        return
+
+    if args.workload == "batch":
+        run_batch_arm(args, rank, world, local)
+        if dist:
+            dist.barrier()
             dist.destroy_process_group()
         return
 
@@ -274,11 +475,7 @@ def main():
             trace_launches += t_n
     torch.cuda.synchronize()
     abi.set_stage_timing(be, 0)
-    total_ms = float(sum(ms))
-    if dist:
-        t = torch.tensor([total_ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(float(sum(ms)), world, local)
     value = npp_total * args.steps / (total_ms / 1e3)
 
     # end to end through the C ABI with host buffers, as the SKIRT bridge uses it: the medium state
@@ -307,47 +504,12 @@ def main():
                 be.fetch_radiation_field(rf_len, out=rf_host)
             torch.cuda.synchronize()
             e2e_times.append(time.perf_counter() - t0)
-        e2e_s = statistics.median(e2e_times)
-        if dist:
-            t = torch.tensor([e2e_s], device=f"cuda:{local}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
+        e2e_s = max_over_ranks(statistics.median(e2e_times), world, local)
         e2e = {"value": npp_total / e2e_s, "unit": "packets/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
 
     if rank == 0:
-        peak, peak_kind = peaks()
-        launch_ms = total_ms / args.steps
-        # roofline of the dominant kernel: its algorithmic bytes per launch over its average launch
-        # duration (CUDA events on the launch stream, timed steps)
-        kind = sc.grid["kind"]
-        trace_bytes_per_launch = trace_algorithmic_bytes(counters, kind) / max(1, trace_launches / args.steps)
-        trace_avg_ms = trace_ms / max(1, trace_launches)
-        achieved = trace_bytes_per_launch / (trace_avg_ms / 1e3) / 1e9
-        traffic = None
-        prof = os.path.join(ROOT, "profiles", f"trace_kernel_{name}_{args.precision}.json")
-        if os.path.exists(prof):
-            with open(prof) as f:
-                ratio = json.load(f).get("dram_bytes_per_algorithmic_byte")
-            if ratio:
-                traffic = ratio * trace_bytes_per_launch
-        line = {
-            "metric": "packets/s on 1 B200", "value": value, "unit": "packets/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": launch_ms, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == abi.PREC_FP64_EXACT else "f32+f64",
-            "data": "synthetic",
-            "config": {"workload": name, "description": WORKLOADS[name][0], "packets_per_step_per_gpu": per_gpu,
-                       "traversal": args.precision, "l2": "flushed between steps (256 MB write)",
-                       "parallelism": f"history ranges x{world}"},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "peak_kind": peak_kind, "kernel": "skg::traceKernel",
-                         "launches_per_step": trace_launches / args.steps, "avg_launch_ms": trace_avg_ms,
-                         "algorithmic_bytes_per_launch": trace_bytes_per_launch,
-                         "share_of_step": trace_ms / max(total_ms, 1e-9)},
-            "clocks": clk.summary(),
-            "e2e": e2e,
-            "gpu_launches": int(counters["kernel_launches"]) * args.steps,
-            "counters_per_step": counters,
-        }
+        line = result_line(args, name, world, value, total_ms, trace_ms, trace_launches, counters, sc.grid["kind"],
+                           prec, clk, e2e, per_gpu)
         if not args.no_cpu_baseline:
             try:
                 line["cpu_baseline"] = cpu_baseline(name)

@@ -201,6 +201,19 @@ int skgpu_run_primary(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t t
 #define SKGPU_NOALLOC_MAX_GROUPS 4
 #define SKGPU_NOALLOC_SCRATCH_BYTES (48u * 1024u * 1024u)
 int skgpu_run_primary_noalloc(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t total_packets);
+/* Launch shape of later runs (0 keeps a default): packet slots in flight (at most 2^20), resident
+ * traversal blocks per SM (capped by what fits) and stage-kernel blocks per SM. Set by an
+ * autotuner (skgpu/autotune.py); no reference counterpart. */
+int skgpu_set_launch_shape(skgpu_ctx* ctx, int32_t pool_slots, int32_t trace_blocks_per_sm, int32_t shade_blocks_per_sm);
+/* Batched run (no reference counterpart): the segments [first[i], first[i] + count[i]) of n
+ * independent simulations, one per context (each with its own uploads and options), traced as one
+ * wavefront on the first context's device and stream. The contexts must share the device, grid kind
+ * and traversal precision, and guiding must be off. Each history draws from its own simulation's
+ * random streams, so every simulation's tallies equal those of its own skgpu_run_primary; they land
+ * in each context's device tallies. Counters and device time of the batch are those of the first
+ * context (skgpu_get_counters, skgpu_last_run_ms). At most 64 contexts. */
+int skgpu_run_batch(skgpu_ctx* const* ctxs, int32_t n, const uint64_t* first, const uint64_t* count,
+                    const uint64_t* total_packets);
 /* Adds the device tallies of one instrument into the caller's arrays and leaves the device
  * tallies untouched. ifu: num_wavelength_bins*npix (index l + ell*npix), sed: num_wavelength_bins,
  * stats (may be NULL): 5 planes of ifu size then 5 planes of sed size (sum w^k, k=0..4). */
@@ -336,12 +349,15 @@ int skgpu_voronoi_export(const skgpu_voronoi* v, int32_t* nb_begin, int32_t* nb_
 void skgpu_voronoi_free(skgpu_voronoi* v);
 
 /* ---- standalone Delaunay tetrahedralisation ----
- * For scenes not built by SKIRT itself: the Delaunay tetrahedra of n points strictly inside the
- * domain box, joined by the box's 8 corners (vertices n..n+7, as TetraMeshSpatialGrid adds them),
- * in the form skgpu_upload_grid_tetra takes: positively oriented tetrahedra, face f opposite vertex
- * f, per face the neighbouring tetrahedron (-1 on the hull) and its face index, outward unit
- * normals. Built as the dual of the Voronoi cells. No reference counterpart: in the drop-in case
- * SKIRT's TetGen mesh is uploaded. */
+ * For scenes not built by SKIRT itself: the Delaunay tetrahedra of the points inside the domain
+ * box, joined by the box's 8 corners, in the form skgpu_upload_grid_tetra takes: positively
+ * oriented tetrahedra, face f opposite vertex f, per face the neighbouring tetrahedron (-1 on the
+ * hull) and its face index, outward unit normals. Coordinates are snapped to a lattice of 2^20 steps
+ * per box side; points on or outside the box surface and points on the lattice point of an earlier
+ * one are left out (as TetraMeshSpatialGrid::removeInvalid drops them), so the m vertices exported
+ * are the m - 8 kept points in input order followed by the corners. Incremental (Bowyer-Watson)
+ * with exact integer predicates. No reference counterpart: in the drop-in case SKIRT's TetGen mesh
+ * is uploaded. */
 typedef struct skgpu_tetra skgpu_tetra;
 int skgpu_tetra_build(const double* points, int32_t n, const double* extent, int32_t threads, skgpu_tetra** out);
 int skgpu_tetra_sizes(const skgpu_tetra* t, int32_t* num_vertices, int32_t* num_tetra);

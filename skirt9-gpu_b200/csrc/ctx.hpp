@@ -77,6 +77,11 @@ struct skgpu_ctx
     double* pin[2] = {nullptr, nullptr};
     cudaEvent_t pinEv[2] = {nullptr, nullptr};
 
+    // launch shape set by skgpu_set_launch_shape (0: defaults)
+    int shapePool = 0, shapeTraceBlocks = 0, shapeShadeBlocks = 0;
+    // device tables of the last batched run (scene table, history prefix, first histories)
+    std::vector<void*> batchBufs;
+
     // learned path guiding (network, pilot records, optimizer state); null until first used
     skg::GuideState* guide = nullptr;
 };

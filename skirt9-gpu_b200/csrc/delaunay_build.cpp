@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstdint>
 #include <unordered_map>
+#include <unordered_set>
 #include <vector>
 
 #include "../../include/skgpu.h"
@@ -124,9 +125,13 @@ int skgpu_tetra_build(const double* points, int32_t n, const double* extent, int
     const double* e = extent;
     if (!(e[3] > e[0] && e[4] > e[1] && e[5] > e[2])) return SKGPU_ERR_ARG;
     Mesh m;
-    // lattice coordinates; points must lie strictly inside (after quantisation) and be distinct
+    // lattice coordinates. As TetraMeshSpatialGrid::removeInvalid (TetraMeshSpatialGrid.cpp:324-363)
+    // drops vertices outside the domain and vertices too near another one, points that quantise onto
+    // or outside the box surface, or onto the lattice point of an earlier point, are left out.
     std::vector<int32_t> keep;
     keep.reserve(n);
+    std::unordered_set<uint64_t> used;
+    used.reserve(2 * static_cast<size_t>(n));
     m.P.reserve(3 * (static_cast<size_t>(n) + 8));
     for (int c = 0; c < 8; ++c)
     {
@@ -141,12 +146,19 @@ int skgpu_tetra_build(const double* points, int32_t n, const double* extent, int
         {
             double x = points[3 * static_cast<size_t>(i) + a];
             if (!std::isfinite(x)) return SKGPU_ERR_ARG;
-            q[a] = static_cast<int64_t>(std::llround((x - e[a]) / (e[3 + a] - e[a]) * QSTEPS));
-            if (q[a] <= 0 || q[a] >= QSTEPS) return SKGPU_ERR_ARG;
+            double u = (x - e[a]) / (e[3 + a] - e[a]) * QSTEPS;
+            q[a] = u > 0 && u < QSTEPS ? static_cast<int64_t>(std::llround(u)) : 0;
         }
+        bool inside = true;
+        for (int a = 0; a < 3; ++a) inside = inside && q[a] > 0 && q[a] < QSTEPS;
+        if (!inside) continue;
+        uint64_t code = (static_cast<uint64_t>(q[0]) << 40) | (static_cast<uint64_t>(q[1]) << 20) | static_cast<uint64_t>(q[2]);
+        if (!used.insert(code).second) continue;
         m.P.insert(m.P.end(), q, q + 3);
         keep.push_back(i);
     }
+    n = static_cast<int32_t>(keep.size());
+    if (n < 1) return SKGPU_ERR_ARG;
     int nv = n + 8;
     // insertion order: Morton order of the lattice coordinates (short walks)
     std::vector<std::pair<uint64_t, int>> order(n);
@@ -323,7 +335,7 @@ int skgpu_tetra_build(const double* points, int32_t n, const double* extent, int
     for (int v = 0; v < nv; ++v)
         for (int a = 0; a < 3; ++a)
         {
-            // vertices n..n+7 are the corners (lattice ids 0..7); the points keep their order
+            // vertices n..n+7 are the corners (lattice ids 0..7); the kept points keep their order
             int lat = v < n ? 8 + v : v - n;
             r->vertices[3 * static_cast<size_t>(v) + a] = e[a] + (e[3 + a] - e[a]) * static_cast<double>(m.p(lat)[a]) / QSTEPS;
         }

@@ -175,6 +175,7 @@ int ensureWaveBuffers(skgpu_ctx* ctx, int P, int groups, int stats)
     if ((rc = waveAlloc(ctx, &k.gPend, P))) return rc;
     if ((rc = waveAlloc(ctx, &k.gRatio, P))) return rc;
     if ((rc = waveAlloc(ctx, &k.cell, P))) return rc;
+    if ((rc = waveAlloc(ctx, &k.scene, P))) return rc;
     for (int b = 0; b < 2; ++b)
         for (int kind = 0; kind < NUM_KINDS; ++kind)
         {
@@ -263,6 +264,7 @@ void skgpu_destroy(skgpu_ctx* ctx)
     devFree(ctx->radR);
     devFree(ctx->radP);
     freeWave(ctx);
+    for (void* p : ctx->batchBufs) cudaFree(p);
     guideDestroy(ctx);
     devFree(ctx->errFlag);
     if (ctx->doneHost) cudaFreeHost(ctx->doneHost);
@@ -961,10 +963,13 @@ int skgpu_run_primary(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t t
     // packet pool and task queues, sized for up to POOL_MAX histories in flight
     int groups, anyStats;
     waveShape(ctx, groups, anyStats);
-    int P = static_cast<int>(std::min<uint64_t>(std::max<uint64_t>(count, 1), POOL_MAX));
+    uint64_t poolMax = ctx->shapePool > 0 ? static_cast<uint64_t>(ctx->shapePool) : POOL_MAX;
+    int P = static_cast<int>(std::min<uint64_t>(std::max<uint64_t>(count, 1), poolMax));
     if ((rc = ensureWaveBuffers(ctx, P, groups, anyStats))) return rc;
     Wave w = ctx->wave;
     w.sc = sceneOf(ctx);
+    w.traceBlocksPerSM = ctx->shapeTraceBlocks;
+    w.shadeBlocksPerSM = ctx->shapeShadeBlocks;
     w.P = P;
     w.first = first;
     w.count = count;
@@ -1511,6 +1516,93 @@ int skgpu_guide_infer(skgpu_ctx* ctx, int32_t n, const float* inputs, float* out
     GCK(guideInfer(ctx, n, inputs, outputs, tensor_cores, &devErr));
     if (devErr) return fail(ctx, SKGPU_ERR_TIMEOUT, "guide: a tensor-core wait gave up");
     return SKGPU_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------------
+// launch shape and batched runs
+// ------------------------------------------------------------------------------------------------
+extern "C" {
+
+int skgpu_set_launch_shape(skgpu_ctx* ctx, int32_t pool_slots, int32_t trace_blocks_per_sm, int32_t shade_blocks_per_sm)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (pool_slots < 0 || pool_slots > static_cast<int32_t>(POOL_MAX) || trace_blocks_per_sm < 0 || trace_blocks_per_sm > 32
+        || shade_blocks_per_sm < 0 || shade_blocks_per_sm > 64)
+        return fail(ctx, SKGPU_ERR_ARG, "launch shape: pool in [0, 2^20], trace blocks per SM in [0, 32], shade blocks per SM in [0, 64]");
+    ctx->shapePool = pool_slots;
+    ctx->shapeTraceBlocks = trace_blocks_per_sm;
+    ctx->shapeShadeBlocks = shade_blocks_per_sm;
+    return SKGPU_OK;
+}
+
+int skgpu_run_batch(skgpu_ctx* const* ctxs, int32_t n, const uint64_t* first, const uint64_t* count,
+                    const uint64_t* total_packets)
+{
+    if (!ctxs || n < 1 || !first || !count || !total_packets) return SKGPU_ERR_ARG;
+    skgpu_ctx* ctx = ctxs[0];
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (n > MAX_BATCH) return fail(ctx, SKGPU_ERR_ARG, "batch: at most " + std::to_string(MAX_BATCH) + " contexts");
+    int groups = 1, anyStats = 0;
+    uint64_t sum = 0;
+    for (int i = 0; i < n; ++i)
+    {
+        skgpu_ctx* c = ctxs[i];
+        if (!c) return fail(ctx, SKGPU_ERR_ARG, "batch: null context");
+        int rc = checkRunnable(c, first[i], count[i], total_packets[i]);
+        if (rc) return fail(ctx, rc, "batch: context " + std::to_string(i) + ": " + c->err);
+        if (c->device != ctx->device || c->g.kind != ctx->g.kind || c->opt.precision != ctx->opt.precision)
+            return fail(ctx, SKGPU_ERR_ARG, "batch: contexts must share the device, grid kind and precision");
+        if (c->guide && c->guide->mode != 0) return fail(ctx, SKGPU_ERR_STATE, "batch: learned path guiding is not offered in batches");
+        CK(cudaSetDevice(c->device));
+        if ((rc = ensureRadiationField(c))) return fail(ctx, rc, "batch: context " + std::to_string(i) + ": " + c->err);
+        CK(cudaStreamSynchronize(c->stream));  // the batch runs on the first context's stream
+        int g, st;
+        waveShape(c, g, st);
+        groups = std::max(groups, g);
+        anyStats |= st;
+        sum += count[i];
+    }
+    CK(cudaSetDevice(ctx->device));
+    uint64_t poolMax = ctx->shapePool > 0 ? static_cast<uint64_t>(ctx->shapePool) : POOL_MAX;
+    int P = static_cast<int>(std::min<uint64_t>(std::max<uint64_t>(sum, 1), poolMax));
+    int rc = ensureWaveBuffers(ctx, P, groups, anyStats);
+    if (rc) return rc;
+    std::vector<Scene> scenes(n);
+    std::vector<unsigned long long> prefix(n + 1, 0), sfirst(n);
+    for (int i = 0; i < n; ++i)
+    {
+        scenes[i] = sceneOf(ctxs[i]);
+        prefix[i + 1] = prefix[i] + count[i];
+        sfirst[i] = first[i];
+    }
+    for (void* p : ctx->batchBufs) cudaFree(p);
+    ctx->batchBufs.clear();
+    Scene* dScenes = nullptr;
+    unsigned long long *dPrefix = nullptr, *dFirst = nullptr;
+    CK(devAlloc(&dScenes, n));
+    ctx->batchBufs.push_back(dScenes);
+    CK(devAlloc(&dPrefix, n + 1));
+    ctx->batchBufs.push_back(dPrefix);
+    CK(devAlloc(&dFirst, n));
+    ctx->batchBufs.push_back(dFirst);
+    CK(cudaMemcpy(dScenes, scenes.data(), n * sizeof(Scene), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dPrefix, prefix.data(), (n + 1) * sizeof(unsigned long long), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dFirst, sfirst.data(), n * sizeof(unsigned long long), cudaMemcpyHostToDevice));
+    Wave w = ctx->wave;
+    w.sc = scenes[0];
+    w.scenes = dScenes;
+    w.nScenes = n;
+    w.prefix = dPrefix;
+    w.sfirst = dFirst;
+    w.P = P;
+    w.first = 0;
+    w.count = sum;
+    w.anyStats = anyStats;
+    w.traceBlocksPerSM = ctx->shapeTraceBlocks;
+    w.shadeBlocksPerSM = ctx->shapeShadeBlocks;
+    return runAndCollect(ctx, w, true, true);
 }
 
 }  // extern "C"

@@ -20,6 +20,7 @@ struct PacketPool
     int* rngHas;
     int *nscatt, *ellMix, *ellRF;
     int* cell;  // cell of the last interaction (-1 after launch): start-cell hint of the next rays
+    int* scene; // batched runs: the scene (simulation) of the slot's history
     // per-history statistics buffer (only when an instrument records statistics)
     unsigned long long* skey;  // P * STATS_CAP
     double* sw;
@@ -63,9 +64,20 @@ struct Control
     int err;
 };
 
+// Batched runs trace the histories of several independent scenes (simulations) through one
+// wavefront: scene s owns the batch histories [prefix[s], prefix[s+1]), which are its segment
+// histories first[s], first[s] + 1, ... With one scene, sc is that scene and scenes is null.
+constexpr int MAX_BATCH = 64;
+
 struct Wave
 {
     Scene sc;
+    const Scene* scenes;               // device table of nScenes scenes (batched runs)
+    int nScenes;
+    const unsigned long long* prefix;  // nScenes + 1
+    const unsigned long long* sfirst;  // nScenes: first segment history of each scene
+    // launch shape (0: defaults): resident trace blocks per SM, shade blocks per SM
+    int traceBlocksPerSM, shadeBlocksPerSM;
     PacketPool pk;
     TaskBuf q[2][NUM_KINDS];
     Control* ctl;

@@ -30,6 +30,10 @@
 
 namespace skg {
 
+// the scene of a packet slot (batched runs keep one per slot)
+SKG_D const Scene& slotScene(const Wave& w, int slot) { return w.nScenes > 1 ? w.scenes[w.pk.scene[slot]] : w.sc; }
+
+
 // ---------------------------------------------------------------------------------------------
 // helpers
 // ---------------------------------------------------------------------------------------------
@@ -48,7 +52,7 @@ SKG_D unsigned warpAppend(unsigned* counter)
 
 SKG_D void loadRng(const Wave& w, int slot, Rng& r)
 {
-    r.start(w.sc.seed, w.pk.hist[slot]);
+    r.start(slotScene(w, slot).seed, w.pk.hist[slot]);
     r.ctr = w.pk.rngCtr[slot];
     r.hasSpare = w.pk.rngHas[slot];
     r.spare = w.pk.rngSpare[slot];
@@ -106,7 +110,7 @@ SKG_D void flushStats(const Wave& w, int slot)
                 key[b] = ~0ULL;
             }
         }
-        statMoments(w.sc, ka, wsum);
+        statMoments(slotScene(w, slot), ka, wsum);
     }
     w.pk.nstat[slot] = 0;
 }
@@ -115,7 +119,7 @@ SKG_D void flushStats(const Wave& w, int slot)
 // recorded event, from the history's final detected luminosity
 SKG_D void guideCloseHistory(const Wave& w, int slot)
 {
-    const Scene& sc = w.sc;
+    const Scene& sc = slotScene(w, slot);
     double D = w.pk.gD[slot];
     int pend = w.pk.gPend[slot];
     if (pend >= 0) sc.guideRec[pend].dStart = D;
@@ -131,7 +135,7 @@ SKG_D void guideCloseHistory(const Wave& w, int slot)
 SKG_D void endHistory(const Wave& w, int slot)
 {
     if (w.anyStats && w.pk.nstat[slot]) flushStats(w, slot);
-    if (w.sc.guideMode == 1) guideCloseHistory(w, slot);
+    if (slotScene(w, slot).guideMode == 1) guideCloseHistory(w, slot);
     int i = atomicAdd(&w.ctl->freeTop, 1);
     w.pk.freeSlots[i] = slot;
     atomicAdd(&w.ctl->done, 1ULL);
@@ -163,7 +167,7 @@ SKG_D void emitProp(const Wave& w, int nxt, int kind, int slot, double par)
 SKG_D void emitPeels(const Wave& w, int nxt, int slot, bool scattering, int numScatt, double L, double g, double x,
                      double y, double z, double kx, double ky, double kz)
 {
-    const Scene& sc = w.sc;
+    const Scene& sc = slotScene(w, slot);
     for (int i = 0; i < sc.ninstr; i = nextGroup(sc, i))
     {
         if (!groupNeedsTau(sc, i, x, y, z)) continue;
@@ -177,7 +181,7 @@ SKG_D void emitPeels(const Wave& w, int nxt, int slot, bool scattering, int numS
 // emits the first traversal of a propagation (forced: PROP1; free: FREE with its sampled tau)
 SKG_D void beginPropagation(const Wave& w, int nxt, int slot, Rng& rng)
 {
-    if (w.sc.forced)
+    if (slotScene(w, slot).forced)
         emitProp(w, nxt, K_PROP1, slot, 0.);
     else
         emitProp(w, nxt, K_FREE, slot, -log(rng.uniform()));  // Random::expon
@@ -194,10 +198,17 @@ SKG_D float aadd(float a, float b) { return a + b; }
 SKG_D float amul(float a, float b) { return a * b; }
 SKG_D float aexp(float x) { return __expf(x); }
 
-template<class Walker>
+template<class Walker, bool Multi = false>
 __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __grid_constant__ Wave w, int cur)
 {
-    const Scene& sc = w.sc;
+    // the scene of the lane's task: the kernel parameter's for one scene, the batch table's otherwise
+    int sid = 0;
+    auto scn = [&]() -> const Scene& {
+        if constexpr (Multi)
+            return w.scenes[sid];
+        else
+            return w.sc;
+    };
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     unsigned n0 = w.ctl->qn[cur][0], n1 = w.ctl->qn[cur][1], n2 = w.ctl->qn[cur][2], n3 = w.ctl->qn[cur][3];
@@ -243,25 +254,26 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __g
                     else { kind = K_FREE; idx = t - n0 - n1 - n2; }
                     const TaskBuf& b = w.q[cur][kind];
                     slot = b.slot[idx];
-                    sext = static_cast<Acc>(sc.mixExt[w.pk.ellMix[slot]]);
+                    if constexpr (Multi) sid = w.pk.scene[slot];
+                    sext = static_cast<Acc>(scn().mixExt[w.pk.ellMix[slot]]);
                     tau = 0.;
                     nseg = 0;
                     guard = 0;
                     if (kind == K_PEEL)
                     {
-                        const InstrDev& in = sc.instr[b.info[idx] & 0xFF];
+                        const InstrDev& in = scn().instr[b.info[idx] & 0xFF];
                         fA = static_cast<Acc>(log(b.par[idx]) + 745.);  // taumax = log(L) + 745
-                        wk.start(sc.g, b.x[idx], b.y[idx], b.z[idx], in.kobs[0], in.kobs[1], in.kobs[2],
+                        wk.start(scn().g, b.x[idx], b.y[idx], b.z[idx], in.kobs[0], in.kobs[1], in.kobs[2],
                                  w.pk.cell ? w.pk.cell[slot] : -1);
                     }
                     else
                     {
-                        wk.start(sc.g, w.pk.x[slot], w.pk.y[slot], w.pk.z[slot], w.pk.kx[slot], w.pk.ky[slot],
+                        wk.start(scn().g, w.pk.x[slot], w.pk.y[slot], w.pk.z[slot], w.pk.kx[slot], w.pk.ky[slot],
                                  w.pk.kz[slot], w.pk.cell ? w.pk.cell[slot] : -1);
                         if (kind == K_PROP1)
                         {
                             fA = static_cast<Acc>(w.pk.L[slot]);
-                            iA = sc.rfOn ? w.pk.ellRF[slot] : -1;
+                            iA = scn().rfOn ? w.pk.ellRF[slot] : -1;
                             fB = 0.;
                             fC = 1.;
                         }
@@ -279,7 +291,7 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __g
         if (__all_sync(FULL, kind == -2)) break;
         if (kind < 0) continue;
 
-        bool got = wk.next(sc.g);
+        bool got = wk.next(scn().g);
         bool done = !got;
         if (got)
         {
@@ -290,7 +302,7 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __g
             {
                 if (m >= 0)
                 {
-                    tau = aadd(tau, amul(amul(sext, static_cast<Acc>(wk.density(sc.dens))), ds));
+                    tau = aadd(tau, amul(amul(sext, static_cast<Acc>(wk.density(scn().dens))), ds));
                     if (tau >= fA)
                     {
                         tau = static_cast<Acc>(INFINITY);
@@ -302,7 +314,7 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __g
             {
                 if (ds > 0.)
                 {
-                    if (m >= 0) tau = aadd(tau, amul(amul(sext, static_cast<Acc>(wk.density(sc.dens))), ds));
+                    if (m >= 0) tau = aadd(tau, amul(amul(sext, static_cast<Acc>(wk.density(scn().dens))), ds));
                     nseg++;
                     if (iA >= 0)
                     {
@@ -313,7 +325,7 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __g
                             // L * ds exceeds the FP32 range (watts times metres): the product is FP64
                             double Lds = static_cast<double>(fA) * static_cast<double>(lnmean4(extEnd, fC, lnExtEnd, fB))
                                          * static_cast<double>(ds);
-                            atomicAdd(sc.rf + static_cast<size_t>(m) * sc.nrf + iA, Lds);
+                            atomicAdd(scn().rf + static_cast<size_t>(m) * scn().nrf + iA, Lds);
                             rfStores++;
                         }
                         fB = lnExtEnd;
@@ -327,7 +339,7 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __g
                 if (kind == K_FREE || ds > 0.)
                 {
                     Acc tau0 = tau, s0 = fB;
-                    if (m >= 0) tau = aadd(tau, amul(amul(sext, static_cast<Acc>(wk.density(sc.dens))), ds));
+                    if (m >= 0) tau = aadd(tau, amul(amul(sext, static_cast<Acc>(wk.density(scn().dens))), ds));
                     fB = aadd(fB, ds);
                     iA = m;
                     fC = fB;
@@ -351,7 +363,7 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __g
                 {
                     const TaskBuf& b = w.q[cur][kind];
                     bool peel = kind == K_PEEL;
-                    const double* ko = peel ? sc.instr[b.info[idx] & 0xFF].kobs : nullptr;
+                    const double* ko = peel ? scn().instr[b.info[idx] & 0xFF].kobs : nullptr;
                     printf("skgpu: traversal guard: kind %d hist %llu start (%.17g %.17g %.17g) dir (%.17g %.17g %.17g) cell %d\n",
                            kind, static_cast<unsigned long long>(w.pk.hist[slot]), peel ? b.x[idx] : w.pk.x[slot],
                            peel ? b.y[idx] : w.pk.y[slot], peel ? b.z[idx] : w.pk.z[slot], peel ? ko[0] : w.pk.kx[slot],
@@ -405,13 +417,13 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __g
 // FluxRecorder::detect for the instruments of one observer group (FluxRecorder.cpp:372-538)
 static __global__ void __launch_bounds__(256) shadePeelKernel(const __grid_constant__ Wave w, int cur)
 {
-    const Scene& sc = w.sc;
     unsigned n = w.ctl->qn[cur][K_PEEL];
     const TaskBuf& b = w.q[cur][K_PEEL];
     unsigned long long det = 0, ovf = 0;
     for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
     {
         int slot = b.slot[t];
+        const Scene& sc = slotScene(w, slot);
         int group = b.info[t] & 0xFF;
         int numScatt = b.info[t] >> 8;
         double Lp = b.par[t];
@@ -504,7 +516,7 @@ static __global__ void __launch_bounds__(256) shadeProp1Kernel(const __grid_cons
         }
         Rng rng;
         loadRng(w, slot, rng);
-        double xi = w.sc.pathLengthBias;
+        double xi = slotScene(w, slot).pathLengthBias;
         double tau;
         if (xi == 0.)
             tau = exponCutoff(rng, taupath);
@@ -530,7 +542,7 @@ static __global__ void __launch_bounds__(256) shadeProp1Kernel(const __grid_cons
 SKG_D void guideRecord(const Wave& w, int slot, int nscatt, double x, double y, double z, double kx0, double ky0,
                        double kz0, double kx, double ky, double kz, double L)
 {
-    const Scene& sc = w.sc;
+    const Scene& sc = slotScene(w, slot);
     int pend = w.pk.gPend[slot];
     if (pend >= 0)
     {
@@ -558,7 +570,7 @@ SKG_D void guideRecord(const Wave& w, int slot, int nscatt, double x, double y, 
 
 SKG_D void interact(const Wave& w, int cur, int nxt, int slot, int m, double sInt, bool forced)
 {
-    const Scene& sc = w.sc;
+    const Scene& sc = slotScene(w, slot);
     if (m < 0)
     {
         atomicOr(&w.ctl->err, 2);  // MediumSystem::albedoForScattering: cannot locate the interaction point
@@ -628,7 +640,7 @@ SKG_D void interact(const Wave& w, int cur, int nxt, int slot, int m, double sIn
 // which is returned.
 SKG_D double guidedScatter(const Wave& w, int nxt, int slot, const float* o)
 {
-    const Scene& sc = w.sc;
+    const Scene& sc = slotScene(w, slot);
     GuideMixture mix;
     guideMixture(o, mix);
     Rng rng;
@@ -672,7 +684,7 @@ SKG_D double guidedScatter(const Wave& w, int nxt, int slot, const float* o)
 static __global__ void __launch_bounds__(GM_TILE) guideScatterKernel(const __grid_constant__ Wave w, int cur, int nxt)
 {
     extern __shared__ __align__(128) unsigned char smem[];
-    const Scene& sc = w.sc;
+    const Scene& sc = w.sc;  // the network (guiding is not offered in batched runs)
     unsigned n = w.ctl->qn[cur][K_GUIDE];
     if (blockIdx.x * GM_TILE >= n) return;  // uniform per CTA, before any tensor memory is taken
     const TaskBuf& b = w.q[cur][K_GUIDE];
@@ -689,7 +701,7 @@ static __global__ void __launch_bounds__(GM_TILE) guideScatterKernel(const __gri
         float f[GUIDE_IN], o[GUIDE_OUT];
         if (valid)
             guideFeatures(f, w.pk.x[slot], w.pk.y[slot], w.pk.z[slot], w.pk.kx[slot], w.pk.ky[slot], w.pk.kz[slot],
-                          w.pk.lam[slot], w.pk.tauPath[slot], sc.g.ext);
+                          w.pk.lam[slot], w.pk.tauPath[slot], slotScene(w, slot).g.ext);
         else
             for (int k = 0; k < GUIDE_IN; ++k) f[k] = 0.f;
         if (!failed && !guideTileForward(t, f, o))
@@ -762,12 +774,20 @@ static __global__ void launchPrepKernel(const __grid_constant__ Wave w, int nxt)
 
 static __global__ void __launch_bounds__(256) launchKernel(const __grid_constant__ Wave w, int nxt)
 {
-    const Scene& sc = w.sc;
     int n = w.ctl->nLaunch;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
     {
         int slot = w.pk.freeSlots[w.ctl->launchBase + t];
         unsigned long long hist = w.ctl->launchHist0 + t;
+        if (w.nScenes > 1)
+        {
+            // batch history -> (scene, segment history of that scene)
+            int sid = 0;
+            while (sid + 1 < w.nScenes && hist >= w.prefix[sid + 1]) ++sid;
+            w.pk.scene[slot] = sid;
+            hist = w.sfirst[sid] + (hist - w.prefix[sid]);
+        }
+        const Scene& sc = slotScene(w, slot);
         Rng rng;
         rng.start(sc.seed, hist);
         Launched o = launchPacket(sc, hist, rng);

@@ -2,6 +2,7 @@
 // captured once into a CUDA graph and replayed until every history of the range is done.
 #pragma once
 
+#include <algorithm>
 #include <cuda_runtime.h>
 #include "stage_timer.hpp"
 #include "wavefront.cuh"
@@ -11,14 +12,16 @@ namespace skg {
 struct WaveLaunch
 {
     int traceBlocks, shadeBlocks, guideBlocks, threads;
-    bool guided;
+    bool guided, multi;
 };
 
 template<class Walker>
-int traceBlocksPerSM()
+int traceBlocksPerSM(bool multi)
 {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, traceKernel<Walker>, 256, 0) != cudaSuccess) return 1;
+    cudaError_t e = multi ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, traceKernel<Walker, true>, 256, 0)
+                          : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, traceKernel<Walker, false>, 256, 0);
+    if (e != cudaSuccess) return 1;
     return n > 0 ? n : 1;
 }
 
@@ -29,7 +32,10 @@ cudaError_t enqueuePass(const Wave& w, int pass, const WaveLaunch& L, cudaStream
     int cur = pass & 1, nxt = 1 - cur;
     cudaError_t e;
     if ((e = stageMark(t, pass, 0, s, capturing)) != cudaSuccess) return e;
-    traceKernel<Walker><<<L.traceBlocks, L.threads, 0, s>>>(w, cur);
+    if (L.multi)
+        traceKernel<Walker, true><<<L.traceBlocks, L.threads, 0, s>>>(w, cur);
+    else
+        traceKernel<Walker, false><<<L.traceBlocks, L.threads, 0, s>>>(w, cur);
     if ((e = stageMark(t, pass, 1, s, capturing)) != cudaSuccess) return e;
     shadePeelKernel<<<L.shadeBlocks, L.threads, 0, s>>>(w, cur);
     if ((e = stageMark(t, pass, 2, s, capturing)) != cudaSuccess) return e;
@@ -58,8 +64,11 @@ cudaError_t runWave(const Wave& w, int numSMs, cudaStream_t s, unsigned long lon
 {
     WaveLaunch L;
     L.threads = 256;
-    L.traceBlocks = numSMs * traceBlocksPerSM<Walker>();
-    L.shadeBlocks = numSMs * 4;
+    L.multi = w.nScenes > 1;
+    int resident = traceBlocksPerSM<Walker>(L.multi);
+    // a tuned shape may ask for fewer resident trace blocks, never for more than fit
+    L.traceBlocks = numSMs * (w.traceBlocksPerSM > 0 ? std::min(w.traceBlocksPerSM, resident) : resident);
+    L.shadeBlocks = numSMs * (w.shadeBlocksPerSM > 0 ? w.shadeBlocksPerSM : 4);
     L.guideBlocks = numSMs * 2;
     L.guided = w.sc.guideMode == 2;
     *passes = 0;

@@ -561,3 +561,25 @@ def build_tetra(points, extent, threads=0, lib=None):
     finally:
         lib.skgpu_tetra_free(t)
     return out
+
+
+EXPORTED += ["skgpu_set_launch_shape", "skgpu_run_batch"]
+
+
+def set_launch_shape(be, pool_slots=0, trace_blocks_per_sm=0, shade_blocks_per_sm=0):
+    _guide_call(be, "set_launch_shape", [C.c_int32, C.c_int32, C.c_int32], int(pool_slots), int(trace_blocks_per_sm),
+                int(shade_blocks_per_sm))
+
+
+def run_batch(backends, first, count, total):
+    """skgpu_run_batch over the contexts of several Backends of the CUDA library (one simulation each)."""
+    n = len(backends)
+    ctxs = (C.c_void_p * n)(*[b.ctx.value for b in backends])
+    arr = lambda v: (C.c_uint64 * n)(*[int(x) for x in v])
+    f = backends[0].lib.skgpu_run_batch
+    f.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]
+    f.restype = C.c_int
+    rc = f(C.cast(ctxs, C.c_void_p), n, C.cast(arr(first), C.c_void_p), C.cast(arr(count), C.c_void_p),
+           C.cast(arr(total), C.c_void_p))
+    if rc != OK:
+        raise SkgpuError(rc, backends[0].fn["last_error"](backends[0].ctx).decode())

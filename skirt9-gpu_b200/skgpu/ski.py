@@ -43,10 +43,19 @@ def voronoi_grid(half_size, unit, num_sites, policy="DustDensity"):
             f'minZ="{-h} {unit}" maxZ="{h} {unit}" policy="{policy}" numSites="{num_sites}" relaxSites="false"/>')
 
 
-def tetra_grid(half_size, unit, num_samples, policy="DustDensity"):
+def tetra_grid(half_size, unit, num_samples, policy="DustDensity", filename=None):
     h = half_size
+    f = f' filename="{filename}"' if filename else ""
     return (f'<TetraMeshSpatialGrid minX="{-h} {unit}" maxX="{h} {unit}" minY="{-h} {unit}" maxY="{h} {unit}" '
-            f'minZ="{-h} {unit}" maxZ="{h} {unit}" policy="{policy}" numSamples="{num_samples}" refine="false"/>')
+            f'minZ="{-h} {unit}" maxZ="{h} {unit}" policy="{policy}" numSamples="{num_samples}"{f} refine="false"/>')
+
+
+def vertex_file_text(points_m):
+    """Text column file of vertex positions in pc, as TetraMeshSpatialGrid's File policy reads it
+    (TetraMeshSpatialGrid.cpp:303-312)."""
+    lines = ["# column 1: position x (pc)", "# column 2: position y (pc)", "# column 3: position z (pc)"]
+    lines += [f"{x / PC:.17g} {y / PC:.17g} {z / PC:.17g}" for x, y, z in points_m]
+    return "\n".join(lines) + "\n"
 
 
 def shell_medium(rmin_pc, rmax_pc, exponent, tau_x, mix):
@@ -202,3 +211,21 @@ def shell_cartesian(num_packets=1e6, nbins=64, npix=256, stats=True, points=None
     return simulation("OligoExtinctionOnly", num_packets, point_source(),
                       shell_medium(0.1, 1, 2, 2, mix), cartesian_grid(1, nbins, points),
                       frame_instrument("i30", 30, 2, "pc", npix, stats) + sed_instrument("sed", 30, stats))
+
+
+def galaxy_tetra(num_packets, vertex_filename, tau_v=1.0, npix=256, nlambda=32, half_size_kpc=25):
+    """The galaxy of galaxy_octree with `nlambda` wavelengths on a TetraMeshSpatialGrid whose vertices
+    are read from a text column file (policy File), face-on tau_V, one frame at 60 degrees."""
+    lam = [0.1 * (100.0 ** (i / (nlambda - 1))) for i in range(nlambda)]
+    kappa = [(l / 0.55) ** -1.0 for l in lam]
+    albedo = [min(0.9, max(0.05, 0.5 * (l / 0.55) ** -0.2)) for l in lam]
+    g = [min(0.9, max(0.0, 0.6 * (l / 0.55) ** -0.3)) for l in lam]
+    mix = mean_list_mix(lam, kappa, albedo, g)
+    sources = (geometric_source('<ExpDiskGeometry scaleLength="4 kpc" scaleHeight="0.35 kpc" minRadius="0 kpc" '
+                                'maxRadius="0 kpc" maxZ="0 kpc"/>', 6000, 8e9)
+               + geometric_source('<SersicGeometry effectiveRadius="1 kpc" index="4"/>', 4000, 2e9))
+    wlg = f'<LogWavelengthGrid minWavelength="0.1 micron" maxWavelength="10 micron" numWavelengths="{nlambda}"/>'
+    instruments = frame_instrument("i60", 60, 2 * half_size_kpc, "kpc", npix, stats=False)
+    return simulation("ExtinctionOnly", num_packets, sources, expdisk_medium(6, 0.2, "kpc", tau_v, mix),
+                      tetra_grid(half_size_kpc, "kpc", 100, policy="File", filename=vertex_filename), instruments,
+                      instrument_wlg=wlg, store_rf=False)

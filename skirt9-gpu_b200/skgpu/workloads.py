@@ -241,3 +241,64 @@ def galaxy_voronoi(n_sites=1_000_000, npix=512, nlambda=100, tau_v=2.0, store_rf
     lam, borders, ellv = log_wavelength_grid(0.1e-6, 10e-6, nlambda)
     sc.instruments = [_frame(inc, 0, 0, 2 * h, npix, 10 * MPC, nlambda, borders, ellv, stats) for inc in (0, 90)]
     return sc
+
+
+def tetra_points(num_vertices, seed, half_size_kpc=25.0):
+    """Mesh vertices of `galaxy_tetra`: half uniform in the box, half from the dust exponential disk
+    (hR 6 kpc, hz 0.2 kpc), from numpy default_rng(seed) and default_rng(seed + 1)."""
+    h = half_size_kpc * KPC
+    rng = np.random.default_rng(seed)
+    nu = num_vertices // 2
+    return np.concatenate([rng.uniform(-h, h, (nu, 3)), disk_sites(num_vertices - nu, 6 * KPC, 0.2 * KPC, h, seed=seed + 1)])
+
+
+def galaxy_tetra(num_vertices, tau_v=1.0, seed=1, npix=256, nlambda=32, half_size_kpc=25.0, store_rf=False,
+                 stats=False, threads=0):
+    """The galaxy of `galaxy_octree` (sources, power-law dust on `nlambda` log wavelengths) on a
+    Delaunay tetrahedral mesh of `num_vertices` points plus the box corners, half drawn uniformly in
+    the box and half from the dust exponential disk (hR 6 kpc, hz 0.2 kpc), each tetrahedron with the
+    analytic dust density at its centroid, normalised to face-on tau_V; one frame at 60 degrees."""
+    sc = galaxy_octree(npix=8, nlambda=nlambda, max_level=2, max_dust_fraction=1e-2, store_rf=store_rf,
+                       half_size_kpc=half_size_kpc, stats=stats)
+    h = half_size_kpc * KPC
+    ext = np.array([-h, -h, -h, h, h, h])
+    hRd, hzd = 6 * KPC, 0.2 * KPC
+    pts = tetra_points(num_vertices, seed, half_size_kpc)
+    t = abi.build_tetra(pts, ext, threads)
+    sc.grid = dict(kind=abi.GRID_TETRA, vertices=t["vertices"], tetra=t["tetra"], normals=t["normals"],
+                   ntetra=t["ntetra"], nface=t["nface"], extent=ext, eps=1e-12 * np.sqrt(3) * 2 * h)
+    c = t["vertices"][t["tetra"]].mean(axis=1)
+    mass = tau_v / (1.0 / (2 * np.pi * hRd ** 2))
+    R = np.hypot(c[:, 0], c[:, 1])
+    sc.density = mass * np.exp(-R / hRd - np.abs(c[:, 2]) / hzd) / (4 * np.pi * hRd ** 2 * hzd)
+    lam, borders, ellv = log_wavelength_grid(0.1e-6, 10e-6, nlambda)
+    sc.instruments = [_frame(60, 0, 0, 2 * h, npix, 10 * MPC, nlambda, borders, ellv, stats)]
+    sc.vertex_points = pts
+    return sc
+
+
+def tetra_batch_spec(num=16, seed=2024, min_vertices=1e4, max_vertices=4e5, min_packets=1e6, max_packets=1e7):
+    """Parameters of a batch of independent tetrahedral-mesh simulations, drawn with
+    numpy default_rng(seed): vertex counts, face-on tau_V (0.1-10) and packet counts, each
+    log-uniform; per simulation a point seed and a random-stream seed."""
+    rng = np.random.default_rng(seed)
+    lu = lambda lo, hi: np.exp(rng.uniform(np.log(lo), np.log(hi), num))
+    nv = lu(min_vertices, max_vertices).astype(np.int64)
+    tau = lu(0.1, 10.0)
+    npp = lu(min_packets, max_packets).astype(np.int64)
+    point_seeds = rng.integers(1, 2 ** 31, num)
+    run_seeds = rng.integers(1, 2 ** 31, num)
+    return [dict(num_vertices=int(nv[i]), tau_v=float(tau[i]), packets=int(npp[i]), point_seed=int(point_seeds[i]),
+                 seed=int(run_seeds[i])) for i in range(num)]
+
+
+def tetra_batch(num=16, seed=2024, npix=256, nlambda=32, min_vertices=1e4, max_vertices=4e5, min_packets=1e6,
+                max_packets=1e7, workers=8):
+    """The batched tetrahedral workload: `num` galaxies on Delaunay meshes (`galaxy_tetra`) with the
+    parameters of `tetra_batch_spec`, meshes built in parallel. Returns (scenes, spec)."""
+    from concurrent.futures import ThreadPoolExecutor
+    spec = tetra_batch_spec(num, seed, min_vertices, max_vertices, min_packets, max_packets)
+    make = lambda s: galaxy_tetra(s["num_vertices"], s["tau_v"], s["point_seed"], npix=npix, nlambda=nlambda, threads=1)
+    with ThreadPoolExecutor(max(1, workers)) as ex:
+        scenes = list(ex.map(make, spec))
+    return scenes, spec

@@ -1,0 +1,36 @@
+"""CPU tests of the batched-workload description and the batch entry points (no GPU work)."""
+import numpy as np
+import pytest
+
+from skgpu import abi, batch, workloads
+
+
+def test_tetra_batch_spec_is_seeded_and_in_range():
+    a = workloads.tetra_batch_spec()
+    b = workloads.tetra_batch_spec()
+    assert a == b and len(a) == 16
+    for s in a:
+        assert 1e4 <= s["num_vertices"] <= 4e5
+        assert 0.1 <= s["tau_v"] <= 10
+        assert 1e6 <= s["packets"] <= 1e7
+    assert len({s["seed"] for s in a}) == 16
+
+
+def test_galaxy_tetra_scene_is_consistent():
+    sc = workloads.galaxy_tetra(3000, tau_v=2.0, seed=4, npix=16, nlambda=8)
+    g = sc.grid
+    assert g["kind"] == abi.GRID_TETRA
+    assert len(sc.density) == len(g["tetra"]) and np.all(sc.density >= 0)
+    assert len(g["vertices"]) == 3000 + 8
+    assert sc.instruments[0]["num_bins"] == 8
+
+
+def test_run_batch_checks_its_arguments():
+    with pytest.raises(ValueError):
+        batch.run_batch([object()], [], [1], [1])
+
+
+def test_batch_symbols_exported():
+    lib = abi.load_library()
+    for name in ("skgpu_run_batch", "skgpu_set_launch_shape"):
+        assert hasattr(lib, name)

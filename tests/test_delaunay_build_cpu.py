@@ -56,3 +56,18 @@ def test_random_points_fill_the_box():
     assert 6.4 < len(t["tetra"]) / len(pts) < 6.9  # Poisson-Delaunay: 6.77 tetrahedra per point
     assert (t["ntetra"] < 0).sum() == 12
     _conventions(t)
+
+
+def test_points_outside_or_repeated_are_left_out():
+    """As TetraMeshSpatialGrid::removeInvalid: points outside the box (or on its surface) and repeated
+    points are dropped; the kept points come first, in input order, then the 8 corners."""
+    rng = np.random.default_rng(9)
+    pts = rng.uniform(-0.9, 0.9, size=(3000, 3))
+    bad = np.array([[1.5, 0, 0], [0, -1.0, 0], [0.2, 0.3, 1.0]])
+    allp = np.concatenate([pts[:1000], bad, pts[:10], pts[1000:]])
+    t = abi.build_tetra(allp, [-1, -1, -1, 1, 1, 1])
+    assert len(t["vertices"]) == len(pts) + 8
+    assert np.allclose(t["vertices"][:len(pts)], pts, atol=2.0 / 2 ** 20)
+    vol = _volumes(t)
+    assert vol.min() > 0 and np.isclose(vol.sum(), 8.0, rtol=1e-12)
+    _conventions(t)
