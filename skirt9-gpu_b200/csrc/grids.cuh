@@ -66,7 +66,23 @@ struct GridDev
     int teGridN;
     const int* teBlkBegin;
     const int* teBlkTets;
+    const struct TetRec* teRec;  // FP32 walker: one cache-line record per tetrahedron
+    const int* teBlkRep;         // teGridN^3: a tetrahedron overlapping each block (start of the walking locate)
 };
+
+// Per-tetrahedron record of the production walker, one 128-byte cache line: the four face planes
+// n_f . x = c_f (outward FP32 unit normal, FP64 offset in global coordinates) and the neighbour
+// across each face with the face index on its side. The two tetrahedra sharing a face hold exactly
+// negated copies of one plane, so a point is never inside both (or neither) of them.
+struct alignas(128) TetRec
+{
+    double c[4];
+    float n[12];
+    int nb[4];    // neighbour across face f, -1 on the hull
+    int nface;    // neighbour's face index for face f in bits 8f..8f+7
+    int pad[7];
+};
+static_assert(sizeof(TetRec) == 128, "one cache line per tetrahedron");
 
 // ---------------------------------------------------------------------------------------------
 // common generator state (PathSegmentGenerator)

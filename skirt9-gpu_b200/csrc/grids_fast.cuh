@@ -9,6 +9,8 @@
 // differ only where a ray passes within that distance of a cell edge or corner.
 #pragma once
 
+#include <type_traits>
+
 #include "grids.cuh"
 
 namespace skg {
@@ -426,13 +428,168 @@ struct VoronoiLocal32 : GenBase
 
 
 // ---------------------------------------------------------------------------------------------
-// Tetrahedral mesh, production walker: the face-crossing decision stays the reference's FP64
-// Plucker test (FP32 would misorder near-degenerate faces), while optical depth, path length and
-// the radiation-field factors accumulate in FP32 like the other production walkers.
+// Tetrahedral mesh, production walker (TetraMeshSpatialGrid::MySegmentGenerator::next,
+// TetraMeshSpatialGrid.cpp:688-831). Every step reads one 128-byte record (TetRec) of the current
+// tetrahedron: the exit is the nearest face plane ahead, s_f = (c_f - n_f . r) / (n_f . k) over the
+// faces with n_f . k > 0 other than the face just entered (a ray cannot re-enter a convex cell),
+// with the plane offset difference in FP64 and the division in FP32. Shared faces are one plane
+// seen from both sides, so the walk stays watertight: a point that rounding puts just past the exit
+// plane gives a zero-length step into the neighbour, which is taken without reporting a segment.
+// As the reference, the last in-mesh segment is dropped when the path leaves the hull. A start at a
+// known cell (a scattering event's interaction cell) needs no point location; otherwise a walk over
+// the face planes from the search block's representative finds the containing tetrahedron.
 // ---------------------------------------------------------------------------------------------
-struct TetraFast : TetraExact
+// a record in registers (the fields are picked with selects, never by a dynamic index, so that the
+// record stays out of local memory)
+struct TetRegs
+{
+    double c[4];
+    float n[12];
+    int nb[4];
+    int nface;
+
+    SKG_D static TetRegs load(const TetRec* rec)
+    {
+        const float4* q = reinterpret_cast<const float4*>(rec);
+        float4 a = __ldg(q), b = __ldg(q + 1), n0 = __ldg(q + 2), n1 = __ldg(q + 3), n2 = __ldg(q + 4), nb = __ldg(q + 5),
+               nf = __ldg(q + 6);
+        TetRegs t;
+        t.c[0] = __hiloint2double(__float_as_int(a.y), __float_as_int(a.x));
+        t.c[1] = __hiloint2double(__float_as_int(a.w), __float_as_int(a.z));
+        t.c[2] = __hiloint2double(__float_as_int(b.y), __float_as_int(b.x));
+        t.c[3] = __hiloint2double(__float_as_int(b.w), __float_as_int(b.z));
+        t.n[0] = n0.x; t.n[1] = n0.y; t.n[2] = n0.z; t.n[3] = n0.w;
+        t.n[4] = n1.x; t.n[5] = n1.y; t.n[6] = n1.z; t.n[7] = n1.w;
+        t.n[8] = n2.x; t.n[9] = n2.y; t.n[10] = n2.z; t.n[11] = n2.w;
+        t.nb[0] = __float_as_int(nb.x); t.nb[1] = __float_as_int(nb.y);
+        t.nb[2] = __float_as_int(nb.z); t.nb[3] = __float_as_int(nb.w);
+        t.nface = __float_as_int(nf.x);
+        return t;
+    }
+
+    SKG_D int neighbour(int f) const { return f == 0 ? nb[0] : f == 1 ? nb[1] : f == 2 ? nb[2] : nb[3]; }
+
+    // positive when (x, y, z) lies outside face F's plane
+    template<int F>
+    SKG_D double excess(double x, double y, double z) const
+    {
+        return static_cast<double>(n[3 * F]) * x + static_cast<double>(n[3 * F + 1]) * y + static_cast<double>(n[3 * F + 2]) * z - c[F];
+    }
+};
+
+SKG_D int tetraLocate(const GridDev& g, double x, double y, double z)
+{
+    if (!GenBase::boxContains(g.ext, x, y, z)) return -1;
+    const int n = g.teGridN;
+    auto blk = [&](double v, double lo, double hi) {
+        return min(n - 1, max(0, static_cast<int>(n * (v - lo) / (hi - lo))));
+    };
+    int t = g.teBlkRep[(blk(x, g.ext[0], g.ext[3]) * n + blk(y, g.ext[1], g.ext[4])) * n + blk(z, g.ext[2], g.ext[5])];
+    // visibility walk: cross the face whose plane the point is farthest outside of
+    for (int guard = 0; guard < 4096 && t >= 0; ++guard)
+    {
+        TetRegs r = TetRegs::load(g.teRec + t);
+        int f = -1;
+        double worst = 0., e;
+        if ((e = r.excess<0>(x, y, z)) > worst) { worst = e; f = 0; }
+        if ((e = r.excess<1>(x, y, z)) > worst) { worst = e; f = 1; }
+        if ((e = r.excess<2>(x, y, z)) > worst) { worst = e; f = 2; }
+        if ((e = r.excess<3>(x, y, z)) > worst) { worst = e; f = 3; }
+        if (f < 0) return t;
+        t = r.neighbour(f);
+    }
+    return tetraCellIndex(g, x, y, z);  // walk left the hull or did not settle: the reference's block scan
+}
+
+struct TetraPlane32 : GenBase
 {
     using Acc = float;
+    static constexpr int kMinBlocks = 3;
+    int mr, ef;  // current tetrahedron, face it was entered through (-1: none)
+    int hint;
+    float kxf, kyf, kzf;
+
+    SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz, int h = -1)
+    {
+        startRay(x, y, z, ux, uy, uz);
+        hint = h;
+        mr = -1;
+        ef = -1;
+        kxf = static_cast<float>(ux);
+        kyf = static_cast<float>(uy);
+        kzf = static_cast<float>(uz);
+    }
+
+    SKG_D bool next(const GridDev& g)
+    {
+        if (state == GS_OUTSIDE) return false;
+        if (state == GS_UNKNOWN)
+        {
+            if (!moveInside(g.ext, g.eps)) return false;
+            mr = (hint >= 0 && ds == 0.) ? hint : tetraLocate(g, rx, ry, rz);
+            ef = -1;
+            if (mr < 0)
+            {
+                state = GS_OUTSIDE;
+                return false;
+            }
+            if (ds > 0.) return true;
+        }
+        for (int guard = 0; guard < 256; ++guard)
+        {
+            TetRegs r = TetRegs::load(g.teRec + mr);
+            float best = FLT_MAX;
+            int lf = -1;
+            auto face = [&](auto F) {
+                constexpr int f = decltype(F)::value;
+                float nk = r.n[3 * f] * kxf + r.n[3 * f + 1] * kyf + r.n[3 * f + 2] * kzf;
+                if (f == ef || !(nk > 0.f)) return;
+                float s = static_cast<float>(-r.template excess<f>(rx, ry, rz)) / nk;
+                if (s < best)
+                {
+                    best = s;
+                    lf = f;
+                }
+            };
+            face(std::integral_constant<int, 0>());
+            face(std::integral_constant<int, 1>());
+            face(std::integral_constant<int, 2>());
+            face(std::integral_constant<int, 3>());
+            if (lf < 0)
+            {
+                // no face ahead (degenerate direction or position): the reference's eps step and a
+                // fresh point location
+                propagater(g.eps);
+                mr = tetraLocate(g, rx, ry, rz);
+                ef = -1;
+                if (mr < 0)
+                {
+                    state = GS_OUTSIDE;
+                    return false;
+                }
+                continue;
+            }
+            int nt = r.neighbour(lf);
+            int nf = (r.nface >> (8 * lf)) & 0xff;
+            if (best > 0.f)
+            {
+                m = mr;
+                ds = best;
+                propagater(ds);
+            }
+            mr = nt;
+            ef = nf;
+            if (mr < 0)
+            {
+                // the reference drops the final in-mesh segment when the path leaves the hull
+                state = GS_OUTSIDE;
+                return false;
+            }
+            if (best > 0.f) return true;
+        }
+        state = GS_OUTSIDE;
+        return false;
+    }
 };
 
 }  // namespace skg

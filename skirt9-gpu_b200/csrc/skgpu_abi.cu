@@ -627,6 +627,43 @@ int skgpu_upload_grid_tetra(skgpu_ctx* ctx, int32_t num_vertices, const double* 
             for (int j = j0; j <= j1; ++j)
                 for (int k = k0; k <= k1; ++k) list[fill[(static_cast<size_t>(i) * n + j) * n + k]++] = static_cast<int>(t);
     }
+    // production walker records: each shared face becomes one plane, taken from the side of the
+    // lower-numbered tetrahedron (its outward normal rounded to FP32, the offset through the face
+    // vertex with the lowest index, in FP64) and exactly negated for the other side
+    std::vector<TetRec> rec(nt);
+    for (size_t t = 0; t < nt; ++t)
+    {
+        TetRec& r = rec[t];
+        std::memset(&r, 0, sizeof r);
+        r.nface = 0;
+        for (int f = 0; f < 4; ++f)
+        {
+            int nb = face_ntetra[4 * t + f];
+            int nf = face_nface[4 * t + f];
+            r.nb[f] = nb;
+            r.nface |= (nb >= 0 ? (nf & 0xff) : 0) << (8 * f);
+            size_t owner = t;
+            int of = f;
+            double sign = 1.0;
+            if (nb >= 0 && static_cast<size_t>(nb) < t)
+            {
+                owner = static_cast<size_t>(nb);
+                of = nf;
+                sign = -1.0;
+            }
+            float n32[3];
+            for (int a = 0; a < 3; ++a) n32[a] = static_cast<float>(face_normals[12 * owner + 3 * of + a]);
+            int vmin = INT32_MAX;
+            for (int v = 0; v < 4; ++v)
+                if (v != of) vmin = std::min(vmin, tetra_vertices[4 * owner + v]);
+            const double* p = vertices + 3 * static_cast<size_t>(vmin);
+            double c = static_cast<double>(n32[0]) * p[0] + static_cast<double>(n32[1]) * p[1] + static_cast<double>(n32[2]) * p[2];
+            for (int a = 0; a < 3; ++a) r.n[3 * f + a] = static_cast<float>(sign) * n32[a];
+            r.c[f] = sign * c;
+        }
+    }
+    std::vector<int> rep(static_cast<size_t>(n) * n * n);
+    for (size_t b = 0; b < rep.size(); ++b) rep[b] = begin[b] < begin[b + 1] ? list[begin[b]] : 0;
     CK(cudaSetDevice(ctx->device));
     freeGrid(ctx);
     GridDev& g = ctx->g;
@@ -645,6 +682,8 @@ int skgpu_upload_grid_tetra(skgpu_ctx* ctx, int32_t num_vertices, const double* 
     if ((rc = gridUpload(ctx, &g.teBox, box.data(), box.size()))) return rc;
     if ((rc = gridUpload<int>(ctx, &g.teBlkBegin, begin.data(), begin.size()))) return rc;
     if ((rc = gridUpload<int>(ctx, &g.teBlkTets, list.data(), list.size()))) return rc;
+    if ((rc = gridUpload<TetRec>(ctx, &g.teRec, rec.data(), rec.size()))) return rc;
+    if ((rc = gridUpload<int>(ctx, &g.teBlkRep, rep.data(), rep.size()))) return rc;
     ctx->hasGrid = true;
     return SKGPU_OK;
 }

@@ -199,6 +199,26 @@ def test_gpu_fp32_voronoi_lifecycle_close_to_fp64(gpu_backend):
     assert r32.counters["crossings"] == pytest.approx(r64.counters["crossings"], rel=1e-3)
 
 
+def test_gpu_fp32_tetra_lifecycle_close_to_fp64(gpu_backend):
+    """Production tetrahedral walker (one plane record per tetrahedron, start-cell hints, walking
+    point location) on a panchromatic galaxy mesh: the same histories as the reference-order FP64
+    walker, tallies far inside the noise."""
+    from skgpu import workloads
+    sc = workloads.galaxy_tetra(20000, tau_v=3.0, seed=21, npix=64, nlambda=16, store_rf=True)
+    sc.upload(gpu_backend)
+    n = 40000
+    r64 = sc.run(gpu_backend, n, seed=17)
+    r32 = sc.run(gpu_backend, n, seed=17, precision=abi.PREC_FP32)
+    for a, b in zip(r64.instruments, r32.instruments):
+        assert b["total"].sum() == pytest.approx(a["total"].sum(), rel=2e-3)
+        assert np.mean(np.isclose(a["total"], b["total"], rtol=1e-3, atol=0)) > 0.9
+    assert r32.rf.sum() == pytest.approx(r64.rf.sum(), rel=2e-3)
+    c64, c32 = r64.counters, r32.counters
+    assert c32["histories"] == c64["histories"] == n
+    assert c32["scatterings"] == pytest.approx(c64["scatterings"], rel=1e-3)
+    assert c32["crossings"] == pytest.approx(c64["crossings"], rel=1e-3)
+
+
 def test_gpu_fp32_octree_lifecycle_close_to_fp64(gpu_backend):
     """Production octree walker with FP32 accumulators on the panchromatic galaxy: images and the
     radiation field (whose L * ds products exceed the FP32 range and are formed in FP64) follow the
