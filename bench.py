@@ -276,9 +276,9 @@ def run_batch_arm(args, rank, world, local):
     from skgpu import Backend, abi, workloads
 
     torch.cuda.set_device(local)
-    scenes, spec = workloads.tetra_batch()
+    scenes, spec = workloads.tetra_batch(num=16, first=args.sims)
     n = len(scenes)
-    packets = [s["packets"] for s in spec]
+    packets = [max(1, int(s["packets"] * args.packet_scale)) for s in spec]
     seeds = [s["seed"] + 1000003 * rank for s in spec]
     prec = abi.PREC_FP64_EXACT if args.precision == "fp64" else abi.PREC_FP32
     bes = [Backend(device=local) for _ in scenes]
@@ -343,6 +343,8 @@ def run_batch_arm(args, rank, world, local):
         line = result_line(args, "batch", world, value, total_ms, trace_ms, trace_launches, counters, abi.GRID_TETRA,
                            prec, clk, e2e, per_gpu)
         line["config"]["simulations"] = n
+        if n != 16 or args.packet_scale != 1.0:
+            line["config"]["subset"] = f"first {n} simulations, {args.packet_scale:g} of their packets (profiling case)"
         line["config"]["launch_shape"] = "default (pool 2^20 slots, resident traversal blocks, 4 stage blocks/SM)"
         if not args.no_cpu_baseline:
             try:
@@ -412,6 +414,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--packets", type=int, default=0, help="packets per step per GPU (default: the workload's)")
+    ap.add_argument("--sims", type=int, default=16, help="batch workload: the first K simulations (profiling cases)")
+    ap.add_argument("--packet-scale", type=float, default=1.0,
+                    help="batch workload: fraction of every simulation's packets (profiling cases)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))

@@ -501,10 +501,13 @@ SKG_D int tetraLocate(const GridDev& g, double x, double y, double z)
     return tetraCellIndex(g, x, y, z);  // walk left the hull or did not settle: the reference's block scan
 }
 
+#ifndef SKG_TETRA32_MIN_BLOCKS
+#define SKG_TETRA32_MIN_BLOCKS 3
+#endif
 struct TetraPlane32 : GenBase
 {
     using Acc = float;
-    static constexpr int kMinBlocks = 3;
+    static constexpr int kMinBlocks = SKG_TETRA32_MIN_BLOCKS;
     int mr, ef;  // current tetrahedron, face it was entered through (-1: none)
     int hint;
     float kxf, kyf, kzf;

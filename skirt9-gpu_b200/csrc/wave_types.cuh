@@ -68,6 +68,9 @@ struct Control
 // wavefront: scene s owns the batch histories [prefix[s], prefix[s+1]), which are its segment
 // histories first[s], first[s] + 1, ... With one scene, sc is that scene and scenes is null.
 constexpr int MAX_BATCH = 64;
+// a batch's scene table is staged in the traversal kernel's shared memory as int4 words, within the
+// 48 KB available without an opt-in
+static_assert(sizeof(Scene) % 16 == 0 && MAX_BATCH * sizeof(Scene) <= 48 * 1024, "scene table in shared memory");
 
 struct Wave
 {

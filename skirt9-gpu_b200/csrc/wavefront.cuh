@@ -201,11 +201,22 @@ SKG_D float aexp(float x) { return __expf(x); }
 template<class Walker, bool Multi = false>
 __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __grid_constant__ Wave w, int cur)
 {
-    // the scene of the lane's task: the kernel parameter's for one scene, the batch table's otherwise
+    // the scene of the lane's task: the kernel parameter's for one scene; for a batch, the scene
+    // table staged in shared memory (the walker reads its grid pointers there at every crossing)
     int sid = 0;
+    extern __shared__ __align__(16) unsigned char traceSmem[];
+    const Scene* table = reinterpret_cast<const Scene*>(traceSmem);
+    if constexpr (Multi)
+    {
+        const int4* src = reinterpret_cast<const int4*>(w.scenes);
+        int4* dst = reinterpret_cast<int4*>(traceSmem);
+        const int words = w.nScenes * static_cast<int>(sizeof(Scene) / sizeof(int4));
+        for (int i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
+        __syncthreads();
+    }
     auto scn = [&]() -> const Scene& {
         if constexpr (Multi)
-            return w.scenes[sid];
+            return table[sid];
         else
             return w.sc;
     };

@@ -15,11 +15,14 @@ struct WaveLaunch
     bool guided, multi;
 };
 
+// shared memory of the traversal kernel: the scene table of a batch
+inline size_t traceSmemBytes(const Wave& w) { return w.nScenes > 1 ? w.nScenes * sizeof(Scene) : 0; }
+
 template<class Walker>
-int traceBlocksPerSM(bool multi)
+int traceBlocksPerSM(bool multi, size_t smem)
 {
     int n = 0;
-    cudaError_t e = multi ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, traceKernel<Walker, true>, 256, 0)
+    cudaError_t e = multi ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, traceKernel<Walker, true>, 256, smem)
                           : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, traceKernel<Walker, false>, 256, 0);
     if (e != cudaSuccess) return 1;
     return n > 0 ? n : 1;
@@ -33,7 +36,7 @@ cudaError_t enqueuePass(const Wave& w, int pass, const WaveLaunch& L, cudaStream
     cudaError_t e;
     if ((e = stageMark(t, pass, 0, s, capturing)) != cudaSuccess) return e;
     if (L.multi)
-        traceKernel<Walker, true><<<L.traceBlocks, L.threads, 0, s>>>(w, cur);
+        traceKernel<Walker, true><<<L.traceBlocks, L.threads, traceSmemBytes(w), s>>>(w, cur);
     else
         traceKernel<Walker, false><<<L.traceBlocks, L.threads, 0, s>>>(w, cur);
     if ((e = stageMark(t, pass, 1, s, capturing)) != cudaSuccess) return e;
@@ -65,7 +68,7 @@ cudaError_t runWave(const Wave& w, int numSMs, cudaStream_t s, unsigned long lon
     WaveLaunch L;
     L.threads = 256;
     L.multi = w.nScenes > 1;
-    int resident = traceBlocksPerSM<Walker>(L.multi);
+    int resident = traceBlocksPerSM<Walker>(L.multi, traceSmemBytes(w));
     // a tuned shape may ask for fewer resident trace blocks, never for more than fit
     L.traceBlocks = numSMs * (w.traceBlocksPerSM > 0 ? std::min(w.traceBlocksPerSM, resident) : resident);
     L.shadeBlocks = numSMs * (w.shadeBlocksPerSM > 0 ? w.shadeBlocksPerSM : 4);

@@ -293,11 +293,12 @@ def tetra_batch_spec(num=16, seed=2024, min_vertices=1e4, max_vertices=4e5, min_
 
 
 def tetra_batch(num=16, seed=2024, npix=256, nlambda=32, min_vertices=1e4, max_vertices=4e5, min_packets=1e6,
-                max_packets=1e7, workers=8):
+                max_packets=1e7, workers=8, first=None):
     """The batched tetrahedral workload: `num` galaxies on Delaunay meshes (`galaxy_tetra`) with the
-    parameters of `tetra_batch_spec`, meshes built in parallel. Returns (scenes, spec)."""
+    parameters of `tetra_batch_spec` (only the first `first` of them when given), meshes built in
+    parallel. Returns (scenes, spec)."""
     from concurrent.futures import ThreadPoolExecutor
-    spec = tetra_batch_spec(num, seed, min_vertices, max_vertices, min_packets, max_packets)
+    spec = tetra_batch_spec(num, seed, min_vertices, max_vertices, min_packets, max_packets)[:first]
     make = lambda s: galaxy_tetra(s["num_vertices"], s["tau_v"], s["point_seed"], npix=npix, nlambda=nlambda, threads=1)
     with ThreadPoolExecutor(max(1, workers)) as ex:
         scenes = list(ex.map(make, spec))
