@@ -205,6 +205,15 @@ int skgpu_run_primary_noalloc(skgpu_ctx* ctx, uint64_t first, uint64_t count, ui
  * traversal blocks per SM (capped by what fits) and stage-kernel blocks per SM. Set by an
  * autotuner (skgpu/autotune.py); no reference counterpart. */
 int skgpu_set_launch_shape(skgpu_ctx* ctx, int32_t pool_slots, int32_t trace_blocks_per_sm, int32_t shade_blocks_per_sm);
+/* Launch order of the histories of later runs. SKGPU_ORDER_WAVELENGTH (default): histories are
+ * taken up in order of their launch wavelength (a counting sort at the start of every run whose
+ * range exceeds the pool; 6 bytes of device memory per history), so that the packets in flight
+ * update a few wavelength slices of the tallies at a time. SKGPU_ORDER_INDEX: in index order, as
+ * the reference's loop. Every history draws its own random stream either way, so the tallies are
+ * the same up to the order of floating-point additions. No reference counterpart. */
+#define SKGPU_ORDER_INDEX 0
+#define SKGPU_ORDER_WAVELENGTH 1
+int skgpu_set_history_order(skgpu_ctx* ctx, int32_t mode);
 /* Batched run (no reference counterpart): the segments [first[i], first[i] + count[i]) of n
  * independent simulations, one per context (each with its own uploads and options), traced as one
  * wavefront on the first context's device and stream. The contexts must share the device, grid kind

@@ -81,6 +81,12 @@ struct skgpu_ctx
     int shapePool = 0, shapeTraceBlocks = 0, shapeShadeBlocks = 0;
     // device tables of the last batched run (scene table, history prefix, first histories)
     std::vector<void*> batchBufs;
+    // wavelength-ordered launch (skgpu_set_history_order): mode, keys, order, bucket counts + cursors
+    int historyOrder = 1;
+    unsigned short* orderKeys = nullptr;
+    unsigned* orderIdx = nullptr;
+    unsigned* orderCounts = nullptr;
+    size_t orderCap = 0;
 
     // learned path guiding (network, pilot records, optimizer state); null until first used
     skg::GuideState* guide = nullptr;

@@ -124,11 +124,13 @@ struct OctreeLeaf32 : FastBase<float>
     int cell;
     float4 ra, rb;                 // bounds, density and list base of the current cell (record words 0-1)
     float segDens;                 // density of the cell of the segment just returned
+    int hint;                      // the start cell when the caller knows it (an interaction cell), else -1
 
-    SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz, int = -1)
+    SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz, int h = -1)
     {
         this->startFast(x, y, z, ux, uy, uz);
         cell = -1;
+        hint = h;
     }
 
     SKG_D double density(const double*) const { return static_cast<double>(segDens); }
@@ -160,7 +162,8 @@ struct OctreeLeaf32 : FastBase<float>
         if (this->state == GS_UNKNOWN)
         {
             if (!this->moveInside(g.ext, g.eps)) return false;
-            int c = locate(g, this->rx, this->ry, this->rz);
+            // a start inside the domain in a known cell needs no top-down search
+            int c = (hint >= 0 && this->ds == 0.) ? hint : locate(g, this->rx, this->ry, this->rz);
             if (c < 0)
             {
                 this->state = GS_OUTSIDE;

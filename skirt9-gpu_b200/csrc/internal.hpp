@@ -15,6 +15,11 @@ cudaError_t runWaveFP64(int gridKind, const Wave& w, int numSMs, cudaStream_t s,
 cudaError_t runWaveFP32(int gridKind, const Wave& w, int numSMs, cudaStream_t s, unsigned long long* doneHost,
                         long long* passes, long long maxPasses, bool useGraph, StageTimer* timer);
 
+// wavelength order of the histories of w's range into order[] (keys: count entries, counts and
+// cursor: ORDER_BUCKETS entries each, zeroed here)
+cudaError_t orderHistories(const Wave& w, unsigned short* keys, unsigned* counts, unsigned* cursor, unsigned* order,
+                           int numSMs, cudaStream_t s);
+
 // path-segment and optical-depth kernels, FP64 (reference operation order) and FP32-distance walkers
 cudaError_t launchTracePathsFP64(int precision, const GridDev& g, int n, const double* rays, int maxSeg, int* count,
                                  int* m, double* ds, int* err, cudaStream_t s);

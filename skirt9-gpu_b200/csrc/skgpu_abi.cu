@@ -265,6 +265,9 @@ void skgpu_destroy(skgpu_ctx* ctx)
     devFree(ctx->radP);
     freeWave(ctx);
     for (void* p : ctx->batchBufs) cudaFree(p);
+    cudaFree(ctx->orderKeys);
+    cudaFree(ctx->orderIdx);
+    cudaFree(ctx->orderCounts);
     guideDestroy(ctx);
     devFree(ctx->errFlag);
     if (ctx->doneHost) cudaFreeHost(ctx->doneHost);
@@ -934,6 +937,28 @@ static void waveShape(const skgpu_ctx* ctx, int& groups, int& anyStats)
     groups = std::max(groups, 1);
 }
 
+// Chooses the launch order of a run: wavelength order when it is on and the range is larger than
+// the pool (otherwise every history is in flight at once), index order otherwise.
+static int prepareOrder(skgpu_ctx* ctx, Wave& w)
+{
+    w.order = nullptr;
+    if (!ctx->historyOrder || w.count <= static_cast<unsigned long long>(w.P) || w.count >= (1ULL << 32)) return SKGPU_OK;
+    if (ctx->orderCap < w.count)
+    {
+        cudaFree(ctx->orderKeys);
+        cudaFree(ctx->orderIdx);
+        ctx->orderKeys = nullptr;
+        ctx->orderIdx = nullptr;
+        ctx->orderCap = 0;
+        CK(devAlloc(&ctx->orderKeys, w.count));
+        CK(devAlloc(&ctx->orderIdx, w.count));
+        ctx->orderCap = w.count;
+    }
+    if (!ctx->orderCounts) CK(devAlloc(&ctx->orderCounts, 2 * static_cast<size_t>(ORDER_BUCKETS)));
+    w.order = ctx->orderIdx;
+    return SKGPU_OK;
+}
+
 // runs the wavefront on prepared buffers and collects the counters and status of the run
 static int runAndCollect(skgpu_ctx* ctx, const Wave& w, bool useGraph, bool timed)
 {
@@ -946,6 +971,12 @@ static int runAndCollect(skgpu_ctx* ctx, const Wave& w, bool useGraph, bool time
         ctx->timer.launches[i] = 0;
     }
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    if (w.order)
+    {
+        cudaError_t eo = orderHistories(w, ctx->orderKeys, ctx->orderCounts, ctx->orderCounts + ORDER_BUCKETS,
+                                        ctx->orderIdx, ctx->numSMs, ctx->stream);
+        if (eo != cudaSuccess) return fail(ctx, SKGPU_ERR_CUDA, std::string("run: ordering: ") + cudaGetErrorString(eo));
+    }
     cudaError_t e = prec == SKGPU_PREC_FP64_EXACT
                         ? runWaveFP64(ctx->g.kind, w, ctx->numSMs, ctx->stream, ctx->doneHost, &passes, MAX_PASSES, useGraph, timer)
                         : runWaveFP32(ctx->g.kind, w, ctx->numSMs, ctx->stream, ctx->doneHost, &passes, MAX_PASSES, useGraph, timer);
@@ -966,7 +997,7 @@ static int runAndCollect(skgpu_ctx* ctx, const Wave& w, bool useGraph, bool time
     ctx->lastCounters.peel_detections = ctl.counters[3];
     ctx->lastCounters.rf_stores = ctl.counters[4];
     ctx->lastCounters.stats_overflows = ctl.counters[5];
-    ctx->lastCounters.kernel_launches = static_cast<uint64_t>(passes) * (w.sc.guideMode == 2 ? 8 : 7) + 1;
+    ctx->lastCounters.kernel_launches = static_cast<uint64_t>(passes) * (w.sc.guideMode == 2 ? 8 : 7) + 1 + (w.order ? 3 : 0);
     ctx->lastPasses = passes;
     ctx->lastGuideWeightSum = ctl.guideWeightSum;
     ctx->lastGuideEvents = ctl.guideEvents;
@@ -1013,6 +1044,7 @@ int skgpu_run_primary(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t t
     w.first = first;
     w.count = count;
     w.anyStats = anyStats;
+    if ((rc = prepareOrder(ctx, w))) return rc;
     return runAndCollect(ctx, w, true, true);
 }
 
@@ -1641,7 +1673,16 @@ int skgpu_run_batch(skgpu_ctx* const* ctxs, int32_t n, const uint64_t* first, co
     w.anyStats = anyStats;
     w.traceBlocksPerSM = ctx->shapeTraceBlocks;
     w.shadeBlocksPerSM = ctx->shapeShadeBlocks;
+    if ((rc = prepareOrder(ctx, w))) return rc;
     return runAndCollect(ctx, w, true, true);
+}
+
+int skgpu_set_history_order(skgpu_ctx* ctx, int32_t mode)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (mode != SKGPU_ORDER_INDEX && mode != SKGPU_ORDER_WAVELENGTH) return fail(ctx, SKGPU_ERR_ARG, "history order: 0 or 1");
+    ctx->historyOrder = mode;
+    return SKGPU_OK;
 }
 
 }  // extern "C"

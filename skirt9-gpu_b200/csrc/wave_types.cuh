@@ -68,6 +68,8 @@ struct Control
 // wavefront: scene s owns the batch histories [prefix[s], prefix[s+1]), which are its segment
 // histories first[s], first[s] + 1, ... With one scene, sc is that scene and scenes is null.
 constexpr int MAX_BATCH = 64;
+// buckets of the wavelength-ordered launch (top 14 bits of the FP32 wavelength)
+constexpr int ORDER_BUCKETS = 1 << 14;
 // a batch's scene table is staged in the traversal kernel's shared memory as int4 words, within the
 // 48 KB available without an opt-in
 static_assert(sizeof(Scene) % 16 == 0 && MAX_BATCH * sizeof(Scene) <= 48 * 1024, "scene table in shared memory");
@@ -81,6 +83,8 @@ struct Wave
     const unsigned long long* sfirst;  // nScenes: first segment history of each scene
     // launch shape (0: defaults): resident trace blocks per SM, shade blocks per SM
     int traceBlocksPerSM, shadeBlocksPerSM;
+    // launch order: histories first + order[i] for i = 0, 1, ... (null: index order)
+    const unsigned* order;
     PacketPool pk;
     TaskBuf q[2][NUM_KINDS];
     Control* ctl;

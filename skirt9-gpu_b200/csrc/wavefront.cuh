@@ -790,6 +790,7 @@ static __global__ void __launch_bounds__(256) launchKernel(const __grid_constant
     {
         int slot = w.pk.freeSlots[w.ctl->launchBase + t];
         unsigned long long hist = w.ctl->launchHist0 + t;
+        if (w.order) hist = w.first + w.order[hist - w.first];  // wavelength-ordered launch
         if (w.nScenes > 1)
         {
             // batch history -> (scene, segment history of that scene)
@@ -857,6 +858,98 @@ static __global__ void initPoolKernel(const __grid_constant__ Wave w)
         c->guideWeightSum = 0.;
         c->guideEvents = 0;
         c->err = 0;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Wavelength-ordered launch. Each history draws its own Philox stream, so the order in which the
+// pool takes up histories changes no history, only which histories are in flight together. Taking
+// them up in order of wavelength keeps the packets in flight on a few wavelength bins at a time, so
+// that the tallies they update (radiation field m*nbins + ell, frames l + ell*npix) and the dust
+// tables they read stay within a few L2-resident slices instead of spreading over the full arrays.
+// The order is a counting sort of the segment's histories by the top bits of their launch
+// wavelength as an FP32 number: 14 bits for one scene (32 buckets per octave). A batch keeps its
+// histories grouped by scene (its meshes are separate working sets) and sorts by wavelength within
+// each scene: the scene id takes the top sceneBits of the 14-bit key.
+// ---------------------------------------------------------------------------------------------
+SKG_D unsigned orderBucket(double lambda, int lambdaBits)
+{
+    // positive FP32: sign bit 0, the top lambdaBits of the remaining 31 bits
+    return __float_as_uint(static_cast<float>(lambda)) >> (31 - lambdaBits);
+}
+
+// the launch wavelength of every history of the range (the launch draws of launchKernel), its
+// bucket in keys[] and the bucket counts
+static __global__ void __launch_bounds__(256) orderKeyKernel(const __grid_constant__ Wave w, int sceneBits,
+                                                             unsigned short* keys, unsigned* counts)
+{
+    for (unsigned long long off = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x; off < w.count;
+         off += static_cast<unsigned long long>(gridDim.x) * blockDim.x)
+    {
+        unsigned long long hist = w.first + off;
+        const Scene* sc = &w.sc;
+        int sid = 0;
+        if (w.nScenes > 1)
+        {
+            while (sid + 1 < w.nScenes && hist >= w.prefix[sid + 1]) ++sid;
+            sc = w.scenes + sid;
+            hist = w.sfirst[sid] + (hist - w.prefix[sid]);
+        }
+        Rng rng;
+        rng.start(sc->seed, hist);
+        Launched o = launchPacket(*sc, hist, rng);
+        const int lambdaBits = 14 - sceneBits;
+        unsigned key = (static_cast<unsigned>(sid) << lambdaBits) | orderBucket(o.lambda, lambdaBits);
+        key = min(key, static_cast<unsigned>(ORDER_BUCKETS - 1));
+        keys[off] = static_cast<unsigned short>(key);
+        // one atomic per distinct key of the warp
+        unsigned active = __activemask();
+        unsigned peers = __match_any_sync(active, key);
+        if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(counts + key, static_cast<unsigned>(__popc(peers)));
+    }
+}
+
+// exclusive scan of the bucket counts into bucket cursors (one block of 1024 threads)
+static __global__ void __launch_bounds__(1024) orderScanKernel(const unsigned* counts, unsigned* cursor)
+{
+    constexpr int PER = ORDER_BUCKETS / 1024;
+    __shared__ unsigned part[1024];
+    unsigned local[PER];
+    unsigned sum = 0;
+    for (int i = 0; i < PER; ++i)
+    {
+        local[i] = sum;
+        sum += counts[threadIdx.x * PER + i];
+    }
+    part[threadIdx.x] = sum;
+    __syncthreads();
+    for (int d = 1; d < 1024; d <<= 1)
+    {
+        unsigned v = threadIdx.x >= d ? part[threadIdx.x - d] : 0;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    unsigned base = part[threadIdx.x] - sum;
+    for (int i = 0; i < PER; ++i) cursor[threadIdx.x * PER + i] = base + local[i];
+}
+
+// scatter: order[position] = history offset, positions taken per bucket
+static __global__ void __launch_bounds__(256) orderScatterKernel(unsigned long long count, const unsigned short* keys,
+                                                                 unsigned* cursor, unsigned* order)
+{
+    for (unsigned long long off = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x; off < count;
+         off += static_cast<unsigned long long>(gridDim.x) * blockDim.x)
+    {
+        unsigned key = keys[off];
+        unsigned active = __activemask();
+        unsigned peers = __match_any_sync(active, key);
+        int lane = threadIdx.x & 31;
+        int leader = __ffs(peers) - 1;
+        unsigned base = 0;
+        if (lane == leader) base = atomicAdd(cursor + key, static_cast<unsigned>(__popc(peers)));
+        base = __shfl_sync(peers, base, leader);
+        order[base + __popc(peers & ((1u << lane) - 1))] = static_cast<unsigned>(off);
     }
 }
 

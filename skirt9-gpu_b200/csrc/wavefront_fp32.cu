@@ -20,4 +20,17 @@ cudaError_t runWaveFP32(int gridKind, const Wave& w, int numSMs, cudaStream_t s,
     return cudaErrorNotSupported;
 }
 
+cudaError_t orderHistories(const Wave& w, unsigned short* keys, unsigned* counts, unsigned* cursor, unsigned* order,
+                           int numSMs, cudaStream_t s)
+{
+    cudaError_t e = cudaMemsetAsync(counts, 0, ORDER_BUCKETS * sizeof(unsigned), s);
+    if (e != cudaSuccess) return e;
+    int sceneBits = 0;
+    while ((1 << sceneBits) < w.nScenes) ++sceneBits;  // at most 6 (64 scenes)
+    orderKeyKernel<<<numSMs * 8, 256, 0, s>>>(w, sceneBits, keys, counts);
+    orderScanKernel<<<1, 1024, 0, s>>>(counts, cursor);
+    orderScatterKernel<<<numSMs * 8, 256, 0, s>>>(w.count, keys, cursor, order);
+    return cudaGetLastError();
+}
+
 }  // namespace skg

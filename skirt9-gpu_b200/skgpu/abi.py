@@ -583,3 +583,11 @@ def run_batch(backends, first, count, total):
            C.cast(arr(total), C.c_void_p))
     if rc != OK:
         raise SkgpuError(rc, backends[0].fn["last_error"](backends[0].ctx).decode())
+
+
+EXPORTED += ["skgpu_set_history_order"]
+ORDER_INDEX, ORDER_WAVELENGTH = 0, 1
+
+
+def set_history_order(be, mode):
+    _guide_call(be, "set_history_order", [C.c_int32], int(mode))
