@@ -265,6 +265,7 @@ void skgpu_destroy(skgpu_ctx* ctx)
     devFree(ctx->radP);
     freeWave(ctx);
     for (void* p : ctx->batchBufs) cudaFree(p);
+    cudaFree(ctx->rfT);
     cudaFree(ctx->orderKeys);
     cudaFree(ctx->orderIdx);
     cudaFree(ctx->orderCounts);
@@ -1017,6 +1018,7 @@ static int ensureRadiationField(skgpu_ctx* ctx)
     size_t len = static_cast<size_t>(ctx->numCells) * ctx->nrf;
     if (ctx->rfLen == len) return SKGPU_OK;
     devFree(ctx->rf);
+    devFree(ctx->rfT);
     CK(devAlloc(&ctx->rf, len));
     CK(cudaMemset(ctx->rf, 0, len * sizeof(double)));
     ctx->rfLen = len;
@@ -1234,12 +1236,37 @@ int skgpu_fetch_instrument_components(skgpu_ctx* ctx, int32_t instrument, double
     return d.kind == SKGPU_INSTR_FRAME ? addInto(ctx, d.ifuComp, 3 * n, ifu3) : addInto(ctx, d.sedComp, 3 * n, sed3);
 }
 
+// out[m * nbins + ell] = in[ell * cells + m], through 32 x 32 shared-memory tiles (both sides coalesced)
+static __global__ void rfTransposeKernel(const double* __restrict__ in, double* __restrict__ out, int cells, int nbins)
+{
+    __shared__ double tile[32][33];
+    int m0 = blockIdx.x * 32, e0 = blockIdx.y * 32;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y)
+    {
+        int e = e0 + j, m = m0 + threadIdx.x;
+        if (e < nbins && m < cells) tile[j][threadIdx.x] = in[static_cast<size_t>(e) * cells + m];
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += blockDim.y)
+    {
+        int m = m0 + j, e = e0 + threadIdx.x;
+        if (e < nbins && m < cells) out[static_cast<size_t>(m) * nbins + e] = tile[threadIdx.x][j];
+    }
+}
+
 int skgpu_fetch_radiation_field(skgpu_ctx* ctx, double* rf)
 {
     if (!ctx) return SKGPU_ERR_ARG;
     if (!ctx->rf) return fail(ctx, SKGPU_ERR_STATE, "fetch: no radiation field recorded");
     CK(cudaSetDevice(ctx->device));
-    return addInto(ctx, ctx->rf, ctx->rfLen, rf);
+    if (!rf) return SKGPU_OK;
+    // the device tally is wavelength-major (ell * cells + m); the caller's layout is cell-major
+    int cells = static_cast<int>(ctx->rfLen / ctx->nrf), nbins = ctx->nrf;
+    if (!ctx->rfT) CK(devAlloc(&ctx->rfT, ctx->rfLen));
+    dim3 grid((cells + 31) / 32, (nbins + 31) / 32);
+    rfTransposeKernel<<<grid, dim3(32, 8), 0, ctx->stream>>>(ctx->rf, ctx->rfT, cells, nbins);
+    CK(cudaGetLastError());
+    return addInto(ctx, ctx->rfT, ctx->rfLen, rf);
 }
 
 int skgpu_clear_tallies(skgpu_ctx* ctx)

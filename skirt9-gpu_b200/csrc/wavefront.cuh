@@ -336,7 +336,9 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __g
                             // L * ds exceeds the FP32 range (watts times metres): the product is FP64
                             double Lds = static_cast<double>(fA) * static_cast<double>(lnmean4(extEnd, fC, lnExtEnd, fB))
                                          * static_cast<double>(ds);
-                            atomicAdd(scn().rf + static_cast<size_t>(m) * scn().nrf + iA, Lds);
+                            // device layout ell * cells + m: the packets in flight (taken up in
+                            // wavelength order) update one contiguous slice; the fetch transposes
+                            atomicAdd(scn().rf + static_cast<size_t>(iA) * scn().g.numCells + m, Lds);
                             rfStores++;
                         }
                         fB = lnExtEnd;
