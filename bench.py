@@ -324,7 +324,7 @@ def run_batch_arm(args, rank, world, local):
         h2d = sum(d.nbytes for d in dens)
         d2h = 8 * sum(sizes)
         times = []
-        for _ in range(max(1, min(args.steps, 2))):
+        for it in range(1 + max(1, min(args.steps, 3))):  # the first call is untimed (pinned buffers)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             for be, d in zip(bes, dens):
@@ -334,7 +334,8 @@ def run_batch_arm(args, rank, world, local):
             for be, k, hbuf in zip(bes, sizes, host):
                 be.fetch_instrument(0, k, stats=False, out=hbuf)
             torch.cuda.synchronize()
-            times.append(time.perf_counter() - t0)
+            if it > 0:
+                times.append(time.perf_counter() - t0)
         e2e_s = max_over_ranks(statistics.median(times), world, local)
         e2e = {"value": per_gpu * world / e2e_s, "unit": "packets/s", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h}
@@ -497,7 +498,8 @@ def main():
         h2d = dens.nbytes
         d2h = sum(8 * n + (40 * n if st else 0) for n, st in zip(sizes, stats)) + 8 * rf_len
         e2e_times = []
-        for _ in range(max(1, min(args.steps, 2))):
+        # one untimed call first: the fetch's pinned staging buffers are allocated on first use
+        for it in range(1 + max(1, min(args.steps, 3))):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             be.clear_tallies()
@@ -508,7 +510,8 @@ def main():
             if rf_len:
                 be.fetch_radiation_field(rf_len, out=rf_host)
             torch.cuda.synchronize()
-            e2e_times.append(time.perf_counter() - t0)
+            if it > 0:
+                e2e_times.append(time.perf_counter() - t0)
         e2e_s = max_over_ranks(statistics.median(e2e_times), world, local)
         e2e = {"value": npp_total / e2e_s, "unit": "packets/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
 
