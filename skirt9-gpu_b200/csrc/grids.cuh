@@ -198,6 +198,7 @@ SKG_D double boxDiagonal(const double* b)
 struct CartesianExact : GenBase
 {
     static constexpr int kMinBlocks = 3;
+    static constexpr int kRefillMin = 16;  // waiting lanes before a warp takes new tasks
     int i, j, k;
 
     SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz, int = -1)
@@ -278,6 +279,7 @@ SKG_D int octreeLeafChild(const GridDev& g, double x, double y, double z)
 struct OctreeExact : GenBase
 {
     static constexpr int kMinBlocks = 3;
+    static constexpr int kRefillMin = 16;  // waiting lanes before a warp takes new tasks
     int node;
 
     SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz, int = -1)
@@ -407,6 +409,7 @@ SKG_D int voronoiCellIndex(const GridDev& g, double x, double y, double z)
 struct VoronoiExact : GenBase
 {
     static constexpr int kMinBlocks = 3;
+    static constexpr int kRefillMin = 4;  // waiting lanes before a warp takes new tasks
     int mr;
 
     SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz, int = -1)
@@ -562,6 +565,7 @@ SKG_D void xcross(double ax, double ay, double az, double bx, double by, double 
 struct TetraExact : GenBase
 {
     static constexpr int kMinBlocks = 3;
+    static constexpr int kRefillMin = 8;  // waiting lanes before a warp takes new tasks
     int mr;
     int enteringFace;
 

@@ -74,6 +74,7 @@ struct CartesianFast : FastBase<Real>
 {
     using Acc = Real;
     static constexpr int kMinBlocks = 4;
+    static constexpr int kRefillMin = 16;  // waiting lanes before a warp takes new tasks
     int i, j, k;
 
     SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz, int = -1)
@@ -121,6 +122,7 @@ struct OctreeLeaf32 : FastBase<float>
 {
     using Acc = float;
     static constexpr int kMinBlocks = SKG_OCTREE32_MIN_BLOCKS;
+    static constexpr int kRefillMin = 16;  // waiting lanes before a warp takes new tasks
     int cell;
     float4 ra, rb;                 // bounds, density and list base of the current cell (record words 0-1)
     float segDens;                 // density of the cell of the segment just returned
@@ -295,6 +297,7 @@ struct VoronoiLocal32 : GenBase
 {
     using Acc = float;
     static constexpr int kMinBlocks = 3;
+    static constexpr int kRefillMin = 4;  // waiting lanes before a warp takes new tasks
     static constexpr int kNone = -99;  // no previous cell (the wall ids -1..-6 are taken)
     int mr, prev;
     float kxf, kyf, kzf;
@@ -511,6 +514,7 @@ struct TetraPlane32 : GenBase
 {
     using Acc = float;
     static constexpr int kMinBlocks = SKG_TETRA32_MIN_BLOCKS;
+    static constexpr int kRefillMin = 8;  // waiting lanes before a warp takes new tasks
     int mr, ef;  // current tetrahedron, face it was entered through (-1: none)
     int hint;
     float kxf, kyf, kzf;
