@@ -48,7 +48,8 @@ struct GridDev
     const int* vNbBegin;
     const int* vNb;
     int vN;
-    const float4* vEnt;    // FP32 walker: per neighbour entry the face's unit normal and its distance from the site
+    const float4* vRec;    // FP32 walker: one record per cell (site, faces, neighbour record offsets)
+    const int* vRecOff;    // record offset of each cell (16-byte units)
     int vGridN;            // blocks per dimension of the site search grid
     const int* vBlkBegin;  // vGridN^3 + 1
     const int* vBlkSites;  // site indices per block

@@ -284,52 +284,66 @@ SKG_D int voronoiLocate(const GridDev& g, double x, double y, double z)
 
 // ---------------------------------------------------------------------------------------------
 // Voronoi mesh, production walker (VoronoiMeshSnapshot::MySegmentGenerator::next,
-// VoronoiMeshSnapshot.cpp:1089-1222). On entering a cell the FP64 position is rebased to FP32
-// coordinates l relative to the cell's site; each face entry holds the outward unit normal n and
-// the plane's distance d from the site (half the site distance, or the distance to a domain wall),
-// and the exit distance through the face is s = (d - n . l) / (n . k). The two
-// smallest exits are re-decided in FP64 from the exact sites when they lie within a near-tie
-// tolerance (FP32 would misorder near-degenerate faces). The face just crossed is skipped (a ray
-// cannot re-enter a convex cell), the position moves exactly onto the exit face, and a cell
-// without a positive exit falls back to the reference's eps step and FP64 nearest-site search.
+// VoronoiMeshSnapshot.cpp:1089-1222). Each cell is one contiguous record in 16-byte units:
+//   [0] site x, y (FP64)   [1] site z (FP64), cell index, face count n
+//   [2, 2 + n4)            per face the outward unit normal n and the distance d of the face's plane
+//                          from the site (half the site distance, or the distance to a domain wall)
+//   [2 + n4, 2 + n4 + n4/4) per face the neighbour's record offset (16-byte units), or the wall id
+//                          -1..-6, or kPad
+// with n4 = n rounded up to a multiple of 4 (padding faces have n = 0 and are never ahead). A
+// crossing reads one record and takes the next cell's offset from it: no index arrays between
+// cells. On entering a cell the FP64 position is rebased to FP32 coordinates l relative to the
+// site; the exit through a face is s = (d - n . l) / (n . k). The two smallest exits are
+// re-decided in FP64 from the exact sites when they lie within a near-tie tolerance (FP32 would
+// misorder near-degenerate faces). The face just crossed is skipped (a ray cannot re-enter a convex
+// cell), and a cell without a positive exit falls back to the reference's eps step and an FP64
+// nearest-site search. A start in a known cell (a scattering event's interaction cell) needs no
+// search; other starts walk greedily over the Delaunay neighbours from a site of the search block.
 // ---------------------------------------------------------------------------------------------
-struct VoronoiLocal32 : GenBase
+struct VoronoiRec32 : GenBase
 {
     using Acc = float;
     static constexpr int kMinBlocks = 3;
     static constexpr int kRefillMin = 4;  // waiting lanes before a warp takes new tasks
-    static constexpr int kNone = -99;  // no previous cell (the wall ids -1..-6 are taken)
-    int mr, prev;
+    static constexpr int kNone = -99;     // no previous cell (the wall ids -1..-6 are taken)
+    static constexpr int kPad = -100;     // padding face
+    int rec, prev;                        // record offsets of the current and the previous cell
     float kxf, kyf, kzf;
-
-    // the start cell when the caller knows it (a scattering event's interaction cell), else -1
-    int hint;
+    int hint;                             // the start cell when the caller knows it, else -1
 
     SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz, int h = -1)
     {
         startRay(x, y, z, ux, uy, uz);
         hint = h;
-        mr = -1;
+        rec = -1;
         prev = kNone;
         kxf = static_cast<float>(ux);
         kyf = static_cast<float>(uy);
         kzf = static_cast<float>(uz);
     }
 
-    // FP64 exit distance through entry e of cell mr (0 when the face is not ahead)
-    SKG_D double exit64(const GridDev& g, int e) const
+    SKG_D static void site(const GridDev& g, int r, double& x, double& y, double& z)
     {
-        int mi = g.vNb[e];
-        const double* pr = g.vSites + 3 * static_cast<size_t>(mr);
-        if (mi >= 0)
+        const double* h = reinterpret_cast<const double*>(g.vRec + r);
+        x = __ldg(h);
+        y = __ldg(h + 1);
+        z = __ldg(h + 2);
+    }
+
+    // FP64 exit distance from the current position through the face towards `to` (a record offset
+    // or a wall id) of the cell with site p (0 when the face is not ahead)
+    SKG_D double exit64(const GridDev& g, double px, double py, double pz, int to) const
+    {
+        if (to >= 0)
         {
-            const double* pi = g.vSites + 3 * static_cast<size_t>(mi);
-            double nx = pi[0] - pr[0], ny = pi[1] - pr[1], nz = pi[2] - pr[2];
+            double qx, qy, qz;
+            site(g, to, qx, qy, qz);
+            double nx = qx - px, ny = qy - py, nz = qz - pz;
             double nk = nx * kx + ny * ky + nz * kz;
             if (!(nk > 0)) return 0.;
-            return (nx * (0.5 * (pi[0] + pr[0]) - rx) + ny * (0.5 * (pi[1] + pr[1]) - ry) + nz * (0.5 * (pi[2] + pr[2]) - rz)) / nk;
+            return (nx * (0.5 * (qx + px) - rx) + ny * (0.5 * (qy + py) - ry) + nz * (0.5 * (qz + pz) - rz)) / nk;
         }
-        switch (mi)
+        switch (to)
         {
             case -1: return (g.ext[0] - rx) / kx;
             case -2: return (g.ext[3] - rx) / kx;
@@ -341,16 +355,21 @@ struct VoronoiLocal32 : GenBase
         return 0.;
     }
 
+    SKG_D bool locateRec(const GridDev& g, int cellHint)
+    {
+        int c = cellHint >= 0 ? cellHint : voronoiLocate(g, rx, ry, rz);
+        rec = c >= 0 ? __ldg(g.vRecOff + c) : -1;
+        prev = kNone;
+        return rec >= 0;
+    }
+
     SKG_D bool next(const GridDev& g)
     {
         if (state == GS_OUTSIDE) return false;
         if (state == GS_UNKNOWN)
         {
             if (!moveInside(g.ext, g.eps)) return false;
-            // a start inside the domain in a known cell needs no search; otherwise a greedy walk
-            mr = (hint >= 0 && ds == 0.) ? hint : voronoiLocate(g, rx, ry, rz);
-            prev = kNone;
-            if (mr < 0)
+            if (!locateRec(g, (hint >= 0 && ds == 0.) ? hint : -1))
             {
                 state = GS_OUTSIDE;
                 return false;
@@ -359,44 +378,54 @@ struct VoronoiLocal32 : GenBase
         }
         for (int guard = 0; guard < 64; ++guard)
         {
-            const double* pr = g.vSites + 3 * static_cast<size_t>(mr);
-            float lx = static_cast<float>(rx - pr[0]);
-            float ly = static_cast<float>(ry - pr[1]);
-            float lz = static_cast<float>(rz - pr[2]);
+            const float4* R = g.vRec + rec;
+            float4 h0 = __ldg(R), h1 = __ldg(R + 1);
+            double px = __hiloint2double(__float_as_int(h0.y), __float_as_int(h0.x));
+            double py = __hiloint2double(__float_as_int(h0.w), __float_as_int(h0.z));
+            double pz = __hiloint2double(__float_as_int(h1.y), __float_as_int(h1.x));
+            int cell = __float_as_int(h1.z);
+            int n4 = (__float_as_int(h1.w) + 3) & ~3;
+            float lx = static_cast<float>(rx - px);
+            float ly = static_cast<float>(ry - py);
+            float lz = static_cast<float>(rz - pz);
+            const float4* E = R + 2;
+            const int4* ids = reinterpret_cast<const int4*>(R + 2 + n4);
             float best = FLT_MAX, second = FLT_MAX, scale = 0.f;
-            int ib = -1, is = -1;
-            int e1 = g.vNbBegin[mr + 1];
-            for (int e = g.vNbBegin[mr]; e < e1; ++e)
+            int ib = kNone, is = kNone;
+            for (int c = 0; c < n4; c += 4)
             {
-                float4 q = __ldg(g.vEnt + e);  // unit normal, plane distance from the site
-                float nk = q.x * kxf + q.y * kyf + q.z * kzf;
-                if (!(nk > 0.f)) continue;
-                int mi = __ldg(g.vNb + e);
-                if (mi == prev) continue;
-                float s = (q.w - (q.x * lx + q.y * ly + q.z * lz)) / nk;
-                if (!(s > 0.f)) continue;
-                if (s < best)
+                // four faces per step: their loads are issued together
+                float4 q[4] = {__ldg(E + c), __ldg(E + c + 1), __ldg(E + c + 2), __ldg(E + c + 3)};
+                int4 id4 = __ldg(ids + (c >> 2));
+                int id[4] = {id4.x, id4.y, id4.z, id4.w};
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
                 {
-                    second = best;
-                    is = ib;
-                    best = s;
-                    ib = e;
-                    scale = q.w;
-                }
-                else if (s < second)
-                {
-                    second = s;
-                    is = e;
+                    float nk = q[j].x * kxf + q[j].y * kyf + q[j].z * kzf;
+                    if (!(nk > 0.f) || id[j] == prev) continue;
+                    float s = (q[j].w - (q[j].x * lx + q[j].y * ly + q[j].z * lz)) / nk;
+                    if (!(s > 0.f)) continue;
+                    if (s < best)
+                    {
+                        second = best;
+                        is = ib;
+                        best = s;
+                        ib = id[j];
+                        scale = q[j].w;
+                    }
+                    else if (s < second)
+                    {
+                        second = s;
+                        is = id[j];
+                    }
                 }
             }
-            if (ib < 0)
+            if (ib == kNone)
             {
                 // no exit ahead (the point sits on an edge or slightly outside the cell): the
                 // reference's eps step and a fresh nearest-site search
                 propagater(g.eps);
-                mr = voronoiLocate(g, rx, ry, rz);
-                prev = kNone;
-                if (mr < 0)
+                if (!locateRec(g, -1))
                 {
                     state = GS_OUTSIDE;
                     return false;
@@ -404,10 +433,10 @@ struct VoronoiLocal32 : GenBase
                 continue;
             }
             double sq = best;
-            if (is >= 0 && second - best <= 2e-5f * (best + scale))
+            if (is != kNone && second - best <= 2e-5f * (best + scale))
             {
                 // near tie: decide with the exact FP64 sites
-                double s1 = exit64(g, ib), s2 = exit64(g, is);
+                double s1 = exit64(g, px, py, pz, ib), s2 = exit64(g, px, py, pz, is);
                 if (s2 > 0. && (s2 < s1 || !(s1 > 0.)))
                 {
                     ib = is;
@@ -418,13 +447,12 @@ struct VoronoiLocal32 : GenBase
                     sq = s1;
                 }
             }
-            int mq = g.vNb[ib];
-            m = mr;
+            m = cell;
             ds = sq;
             propagater(sq);
-            prev = mr;
-            mr = mq;
-            if (mr < 0) state = GS_OUTSIDE;
+            prev = rec;
+            rec = ib;
+            if (rec < 0) state = GS_OUTSIDE;
             return true;
         }
         state = GS_OUTSIDE;

@@ -18,7 +18,7 @@ cudaError_t launchTracePathsFP32(int precision, const GridDev& g, int n, const d
     {
         case 0: tracePathsKernel<CartesianFast<float>><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
         case 1: tracePathsKernel<OctreeLeaf32><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
-        case 2: tracePathsKernel<VoronoiLocal32><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
+        case 2: tracePathsKernel<VoronoiRec32><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
         case 3: tracePathsKernel<TetraPlane32><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
         default: return cudaErrorNotSupported;
     }
@@ -35,7 +35,7 @@ cudaError_t launchOpticalDepthsFP32(int precision, const GridDev& g, const doubl
     {
         case 0: opticalDepthKernel<CartesianFast<float>><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
         case 1: opticalDepthKernel<OctreeLeaf32><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
-        case 2: opticalDepthKernel<VoronoiLocal32><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
+        case 2: opticalDepthKernel<VoronoiRec32><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
         case 3: opticalDepthKernel<TetraPlane32><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
         default: return cudaErrorNotSupported;
     }

@@ -38,7 +38,7 @@ struct InstrDev
 };
 
 // read-only scene data of a run
-struct Scene
+struct alignas(16) Scene  // 16-byte multiple: a batch stages its scene table as int4 words
 {
     GridDev g;
     const double* dens;

@@ -535,16 +535,44 @@ int skgpu_upload_grid_voronoi(skgpu_ctx* ctx, int32_t num_sites, const double* s
             if (r < 0) r = 0;
         if ((rc = gridUpload<int>(ctx, &g.vBlkRep, rep.data(), rep.size()))) return rc;
     }
-    // entries of the FP32 walker: per face the outward unit normal and the distance of the face's
-    // plane from the site (half the site distance for a neighbour, the distance to the domain wall
-    // for a wall), so that s = (d - n . l) / (n . k) needs no squares of metre-scale coordinates
-    std::vector<float4> ent(std::max(num_nb_index, 1));
+    // records of the FP32 walker, one per cell in 16-byte units: the FP64 site and the cell's face
+    // count, then per face the outward unit normal and the distance of the face's plane from the site
+    // (half the site distance for a neighbour, the distance to the domain wall for a wall), so that
+    // s = (d - n . l) / (n . k) needs no squares of metre-scale coordinates, then per face the
+    // neighbour's record offset (or the wall id); the faces are padded to a multiple of 4
+    std::vector<int> recOff(num_sites);
+    size_t units = 0;
+    for (int c = 0; c < num_sites; ++c)
+    {
+        size_t n4 = (static_cast<size_t>(nb_begin[c + 1] - nb_begin[c]) + 3) & ~static_cast<size_t>(3);
+        recOff[c] = static_cast<int>(units);
+        units += 2 + n4 + n4 / 4;
+        if (units > 2147483647ULL) return fail(ctx, SKGPU_ERR_ARG, "voronoi: mesh too large for 32-bit record offsets");
+    }
+    std::vector<float4> rec(units);
     for (int c = 0; c < num_sites; ++c)
     {
         const double* pc = sites + 3 * static_cast<size_t>(c);
-        for (int e = nb_begin[c]; e < nb_begin[c + 1]; ++e)
+        float4* R = rec.data() + recOff[c];
+        int nf = nb_begin[c + 1] - nb_begin[c];
+        int n4 = (nf + 3) & ~3;
+        double* hd = reinterpret_cast<double*>(R);
+        hd[0] = pc[0];
+        hd[1] = pc[1];
+        hd[2] = pc[2];
+        int* hi = reinterpret_cast<int*>(R + 1);
+        hi[2] = c;
+        hi[3] = nf;
+        int* ids = reinterpret_cast<int*>(R + 2 + n4);
+        for (int j = 0; j < n4; ++j)
         {
-            int mi = nb_index[e];
+            if (j >= nf)
+            {
+                R[2 + j] = make_float4(0.f, 0.f, 0.f, 0.f);
+                ids[j] = -100;  // padding face: never ahead
+                continue;
+            }
+            int mi = nb_index[nb_begin[c] + j];
             double n[3] = {0, 0, 0}, d = 0;
             if (mi >= 0)
             {
@@ -554,6 +582,7 @@ int skgpu_upload_grid_voronoi(skgpu_ctx* ctx, int32_t num_sites, const double* s
                 if (len > 0)
                     for (int a = 0; a < 3; ++a) n[a] /= len;
                 d = 0.5 * len;
+                ids[j] = recOff[mi];
             }
             else
             {
@@ -561,12 +590,14 @@ int skgpu_upload_grid_voronoi(skgpu_ctx* ctx, int32_t num_sites, const double* s
                 bool upper = ((-mi - 1) & 1) != 0;
                 n[a] = upper ? 1.0 : -1.0;
                 d = upper ? extent[3 + a] - pc[a] : pc[a] - extent[a];
+                ids[j] = mi;
             }
-            ent[e] = make_float4(static_cast<float>(n[0]), static_cast<float>(n[1]), static_cast<float>(n[2]),
-                                 static_cast<float>(d));
+            R[2 + j] = make_float4(static_cast<float>(n[0]), static_cast<float>(n[1]), static_cast<float>(n[2]),
+                                   static_cast<float>(d));
         }
     }
-    if ((rc = gridUpload<float4>(ctx, &g.vEnt, ent.data(), ent.size()))) return rc;
+    if ((rc = gridUpload<float4>(ctx, &g.vRec, rec.data(), rec.size()))) return rc;
+    if ((rc = gridUpload<int>(ctx, &g.vRecOff, recOff.data(), recOff.size()))) return rc;
     ctx->hasGrid = true;
     return SKGPU_OK;
 }

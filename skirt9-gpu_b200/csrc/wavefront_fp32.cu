@@ -14,7 +14,7 @@ cudaError_t runWaveFP32(int gridKind, const Wave& w, int numSMs, cudaStream_t s,
     {
         case 0: return runWave<CartesianFast<float>>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer);
         case 1: return runWave<OctreeLeaf32>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer);
-        case 2: return runWave<VoronoiLocal32>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer);
+        case 2: return runWave<VoronoiRec32>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer);
         case 3: return runWave<TetraPlane32>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer);
     }
     return cudaErrorNotSupported;
