@@ -410,7 +410,7 @@ SKG_D int voronoiCellIndex(const GridDev& g, double x, double y, double z)
 struct VoronoiExact : GenBase
 {
     static constexpr int kMinBlocks = 3;
-    static constexpr int kRefillMin = 4;  // waiting lanes before a warp takes new tasks
+    static constexpr int kRefillMin = 8;  // waiting lanes before a warp takes new tasks
     int mr;
 
     SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz, int = -1)

@@ -300,11 +300,17 @@ SKG_D int voronoiLocate(const GridDev& g, double x, double y, double z)
 // nearest-site search. A start in a known cell (a scattering event's interaction cell) needs no
 // search; other starts walk greedily over the Delaunay neighbours from a site of the search block.
 // ---------------------------------------------------------------------------------------------
+#ifndef SKG_VORONOI32_MIN_BLOCKS
+#define SKG_VORONOI32_MIN_BLOCKS 3
+#endif
+#ifndef SKG_VORONOI32_REFILL
+#define SKG_VORONOI32_REFILL 8
+#endif
 struct VoronoiRec32 : GenBase
 {
     using Acc = float;
-    static constexpr int kMinBlocks = 3;
-    static constexpr int kRefillMin = 4;  // waiting lanes before a warp takes new tasks
+    static constexpr int kMinBlocks = SKG_VORONOI32_MIN_BLOCKS;
+    static constexpr int kRefillMin = SKG_VORONOI32_REFILL;  // waiting lanes before a warp takes new tasks
     static constexpr int kNone = -99;     // no previous cell (the wall ids -1..-6 are taken)
     static constexpr int kPad = -100;     // padding face
     int rec, prev;                        // record offsets of the current and the previous cell

@@ -248,7 +248,7 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __g
         // lane that finishes: the refill (task-buffer and packet-state loads, walker start) then runs
         // once for several lanes instead of stalling the busy lanes at almost every crossing. The
         // best count depends on the cost of a crossing (measured: 16 for the Cartesian grid and the
-        // octree, 8 for tetrahedra, 4 for Voronoi cells).
+        // octree, 8 for tetrahedra and Voronoi cells).
         if (need && (__popc(need) >= Walker::kRefillMin || __ballot_sync(FULL, kind >= 0) == 0))
         {
             int leader = __ffs(need) - 1;
