@@ -107,7 +107,11 @@ typedef struct skgpu_options {
     int32_t store_radiation_field; /* accumulate L*lnmean*ds per (cell, RF bin) on forced paths */
     int32_t peel_off;              /* emission and scattering peel-off towards the instruments */
     int32_t precision;             /* SKGPU_PREC_* */
-    int32_t reserved;
+    /* 1: explicit absorption (PhotonPacketOptions::explicitAbsorption): interaction points are
+     * sampled on the scattering optical depth and the weight carries exp(-tau_abs) instead of the
+     * albedo (MonteCarloSimulation.cpp:1492-1546, 1996-2030; MediumSystem.cpp:1881-1915, 2152-2223);
+     * peel-off and radiation field still use extinction */
+    int32_t explicit_absorption;
     uint64_t seed;                 /* Philox key; packets draw from counter streams keyed by history index */
 } skgpu_options;
 

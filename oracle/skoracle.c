@@ -897,7 +897,8 @@ int or_set_options(or_ctx* c, const skgpu_options* o)
 typedef struct
 {
     int m;
-    double ds, s, tau;
+    double ds, s, tau;  /* tau: cumulative extinction, or scattering under explicit absorption */
+    double tauAbs;      /* cumulative absorption optical depth (explicit absorption), else 0 */
 } Seg;
 
 typedef struct
@@ -1173,7 +1174,8 @@ static void path_build(or_ctx* c, const Packet* pk, Path* path)
     Gen s;
     gen_start(&s, ray);
     path->n = 0;
-    double scum = 0., tau = 0.;
+    double scum = 0., tau = 0., tauAbs = 0.;
+    double sabs = pk->sext - pk->ssca;
     while (gen_next(&c->g, &s))
     {
         c->cnt.crossings++;
@@ -1185,8 +1187,19 @@ static void path_build(or_ctx* c, const Packet* pk, Path* path)
                 path->v = (Seg*)realloc(path->v, path->cap * sizeof(Seg));
             }
             scum += s.ds;
-            if (s.m >= 0) tau += pk->sext * c->dens[s.m] * s.ds;
-            Seg sg = {s.m, s.ds, scum, tau};
+            if (c->opt.explicit_absorption)
+            {
+                /* MediumSystem::setScatteringAndAbsorptionOpticalDepths (MediumSystem.cpp:1899-1913) */
+                if (s.m >= 0)
+                {
+                    double ns = c->dens[s.m] * s.ds;
+                    tau += pk->ssca * ns;
+                    tauAbs += sabs * ns;
+                }
+            }
+            else if (s.m >= 0)
+                tau += pk->sext * c->dens[s.m] * s.ds;
+            Seg sg = {s.m, s.ds, scum, tau, tauAbs};
             path->v[path->n++] = sg;
         }
     }
@@ -1358,7 +1371,8 @@ static void life_cycle(or_ctx* c, uint64_t hist, Path* path, Packet* pk)
                 double lnExtBeg = 0., extBeg = 1.;
                 for (int q = 0; q < path->n; ++q)
                 {
-                    double lnExtEnd = -path->v[q].tau, extEnd = exp(lnExtEnd);
+                    /* Segment::tauExt = tauExtOrSca + tauAbs (SpatialGridPath.hpp:108) */
+                    double lnExtEnd = -(path->v[q].tau + path->v[q].tauAbs), extEnd = exp(lnExtEnd);
                     int m = path->v[q].m;
                     if (m >= 0)
                     {
@@ -1396,24 +1410,31 @@ static void life_cycle(or_ctx* c, uint64_t hist, Path* path, Packet* pk)
                     if (tau < path->v[mid].tau) hi = mid; else lo = mid + 1;
                 }
                 int m;
-                double s;
+                double s, tauAbs;
                 if (lo < path->n)
                 {
                     double t0 = lo ? path->v[lo - 1].tau : 0., s0 = lo ? path->v[lo - 1].s : 0.;
+                    double a0 = lo ? path->v[lo - 1].tauAbs : 0.;
                     m = path->v[lo].m;
                     s = s0 + ((tau - t0) / (path->v[lo].tau - t0)) * (path->v[lo].s - s0);
+                    tauAbs = a0 + ((tau - t0) / (path->v[lo].tau - t0)) * (path->v[lo].tauAbs - a0);
                 }
                 else
                 {
                     m = path->v[path->n - 1].m;
                     s = path->v[path->n - 1].s;
+                    tauAbs = path->v[path->n - 1].tauAbs;
                 }
                 if (m < 0)
                 {
                     c->errFlag |= 2;
                     break;
                 }
-                pk->L *= -expm1(-taupath) * albedo(c, pk, m);
+                /* MonteCarloSimulation.cpp:1529-1540 */
+                if (c->opt.explicit_absorption)
+                    pk->L *= -expm1(-taupath) * exp(-tauAbs);
+                else
+                    pk->L *= -expm1(-taupath) * albedo(c, pk, m);
                 pk->rx += s * pk->kx;
                 pk->ry += s * pk->ky;
                 pk->rz += s * pk->kz;
@@ -1439,7 +1460,9 @@ static void life_cycle(or_ctx* c, uint64_t hist, Path* path, Packet* pk)
             {
                 c->cnt.crossings++;
                 double t0 = tau, s0 = sc;
-                if (s.m >= 0) tau += pk->sext * c->dens[s.m] * s.ds;
+                /* explicit absorption: MediumSystem::setInteractionPointUsingScatteringAndAbsorption
+                   (MediumSystem.cpp:2203-2222) walks on the scattering optical depth */
+                if (s.m >= 0) tau += (c->opt.explicit_absorption ? pk->ssca : pk->sext) * c->dens[s.m] * s.ds;
                 sc += s.ds;
                 if (tauinteract < tau)
                 {
@@ -1455,7 +1478,11 @@ static void life_cycle(or_ctx* c, uint64_t hist, Path* path, Packet* pk)
                 c->errFlag |= 2;
                 break;
             }
-            pk->L *= albedo(c, pk, m);
+            /* MonteCarloSimulation::simulateNonForcedPropagation (MonteCarloSimulation.cpp:2001-2022) */
+            if (c->opt.explicit_absorption)
+                pk->L *= exp(-(tauinteract * (pk->sext - pk->ssca) / pk->ssca));
+            else
+                pk->L *= albedo(c, pk, m);
             pk->rx += sInt * pk->kx;
             pk->ry += sInt * pk->ky;
             pk->rz += sInt * pk->kz;

@@ -67,6 +67,7 @@ struct alignas(16) Scene  // 16-byte multiple: a batch stages its scene table as
     double* rf;
 
     int forced, minScatt, peel;
+    int explicitAbs;  // explicit absorption: sampling on scattering optical depth, weight exp(-tau_abs)
     double minWeightRed, pathLengthBias;
     unsigned long long seed;
 

@@ -926,6 +926,7 @@ static Scene sceneOf(const skgpu_ctx* ctx)
     p.forced = ctx->opt.force_scattering ? 1 : 0;
     p.minScatt = ctx->opt.min_scatt_events;
     p.peel = ctx->opt.peel_off ? 1 : 0;
+    p.explicitAbs = ctx->opt.explicit_absorption ? 1 : 0;
     p.minWeightRed = ctx->opt.min_weight_reduction;
     p.pathLengthBias = ctx->opt.path_length_bias;
     p.seed = ctx->opt.seed;

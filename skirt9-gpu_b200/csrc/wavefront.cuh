@@ -271,7 +271,13 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __g
                     const TaskBuf& b = w.q[cur][kind];
                     slot = b.slot[idx];
                     if constexpr (Multi) sid = w.pk.scene[slot];
-                    sext = static_cast<Acc>(scn().mixExt[w.pk.ellMix[slot]]);
+                    // peel-off rays and complete forced paths (PROP1: radiation field) accumulate
+                    // extinction; under explicit absorption the interaction searches (PROP2, FREE)
+                    // walk on the scattering optical depth (setScatteringAndAbsorptionOpticalDepths)
+                    {
+                        int ell = w.pk.ellMix[slot];
+                        sext = static_cast<Acc>(scn().explicitAbs && kind >= K_PROP2 ? scn().mixSca[ell] : scn().mixExt[ell]);
+                    }
                     tau = 0.;
                     nseg = 0;
                     guard = 0;
@@ -526,6 +532,16 @@ static __global__ void __launch_bounds__(256) shadeProp1Kernel(const __grid_cons
     {
         int slot = b.slot[t];
         double taupath = b.tau[t];
+        const Scene& sc = slotScene(w, slot);
+        if (sc.explicitAbs)
+        {
+            // explicit absorption samples on the scattering optical depth of the path: for one medium
+            // with constant cross sections tau_sca = tau_ext * sca / ext (the trace accumulated
+            // extinction for the radiation field)
+            int ell = w.pk.ellMix[slot];
+            double ext = sc.mixExt[ell];
+            taupath = ext > 0. ? taupath * (sc.mixSca[ell] / ext) : 0.;
+        }
         if (taupath <= 0.)
         {
             w.pk.L[slot] *= 0.;
@@ -534,7 +550,7 @@ static __global__ void __launch_bounds__(256) shadeProp1Kernel(const __grid_cons
         }
         Rng rng;
         loadRng(w, slot, rng);
-        double xi = slotScene(w, slot).pathLengthBias;
+        double xi = sc.pathLengthBias;
         double tau;
         if (xi == 0.)
             tau = exponCutoff(rng, taupath);
@@ -586,7 +602,9 @@ SKG_D void guideRecord(const Wave& w, int slot, int nscatt, double x, double y, 
     w.pk.gPend[slot] = static_cast<int>(idx);
 }
 
-SKG_D void interact(const Wave& w, int cur, int nxt, int slot, int m, double sInt, bool forced)
+// tauInt: the interaction optical depth (PROP2: the sampled one within the path; FREE: the drawn
+// one), which under explicit absorption is a scattering optical depth
+SKG_D void interact(const Wave& w, int cur, int nxt, int slot, int m, double sInt, bool forced, double tauInt)
 {
     const Scene& sc = slotScene(w, slot);
     if (m < 0)
@@ -596,12 +614,27 @@ SKG_D void interact(const Wave& w, int cur, int nxt, int slot, int m, double sIn
         return;
     }
     int ell = w.pk.ellMix[slot];
-    double albedo = albedoAt(sc, m, sc.mixSca[ell], sc.mixExt[ell]);
     double L = w.pk.L[slot];
-    if (forced)
-        L *= -expm1(-w.pk.tauPath[slot]) * albedo;
+    if (sc.explicitAbs)
+    {
+        // absorption optical depth at the interaction point: tau_int * abs / sca for one medium with
+        // constant cross sections (MediumSystem.cpp:2216-2220); applied as exp(-tau_abs)
+        // (MonteCarloSimulation.cpp:1531-1535, 2001-2010)
+        double sca = sc.mixSca[ell];
+        double tauAbs = tauInt * (sc.mixExt[ell] - sca) / sca;
+        if (forced)
+            L *= -expm1(-w.pk.tauPath[slot]) * exp(-tauAbs);
+        else
+            L *= exp(-tauAbs);
+    }
     else
-        L *= albedo;
+    {
+        double albedo = albedoAt(sc, m, sc.mixSca[ell], sc.mixExt[ell]);
+        if (forced)
+            L *= -expm1(-w.pk.tauPath[slot]) * albedo;
+        else
+            L *= albedo;
+    }
     w.pk.L[slot] = L;
     double kx = w.pk.kx[slot], ky = w.pk.ky[slot], kz = w.pk.kz[slot];
     double x = w.pk.x[slot] + sInt * kx;
@@ -757,7 +790,7 @@ static __global__ void __launch_bounds__(256) shadeProp2Kernel(const __grid_cons
     unsigned n = w.ctl->qn[cur][K_PROP2];
     const TaskBuf& b = w.q[cur][K_PROP2];
     for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
-        interact(w, cur, nxt, b.slot[t], b.m[t], b.s[t], true);
+        interact(w, cur, nxt, b.slot[t], b.m[t], b.s[t], true, b.par[t]);
 }
 
 static __global__ void __launch_bounds__(256) shadeFreeKernel(const __grid_constant__ Wave w, int cur, int nxt)
@@ -769,7 +802,7 @@ static __global__ void __launch_bounds__(256) shadeFreeKernel(const __grid_const
         if (!b.found[t])
             endHistory(w, b.slot[t]);  // the interaction point is outside the path: the packet escapes
         else
-            interact(w, cur, nxt, b.slot[t], b.m[t], b.s[t], false);
+            interact(w, cur, nxt, b.slot[t], b.m[t], b.s[t], false, b.par[t]);
     }
 }
 

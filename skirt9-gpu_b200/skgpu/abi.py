@@ -82,7 +82,7 @@ class Options(C.Structure):
         ("store_radiation_field", C.c_int32),
         ("peel_off", C.c_int32),
         ("precision", C.c_int32),
-        ("reserved", C.c_int32),
+        ("explicit_absorption", C.c_int32),
         ("seed", C.c_uint64),
     ]
 

@@ -41,6 +41,7 @@ class Scene:
         self.path_length_bias = 0.5
         self.store_rf = False
         self.source_bias = 0.5
+        self.explicit_absorption = False
 
     # ------------------------------------------------------------------ uploads
     def upload(self, be):
@@ -135,6 +136,7 @@ class Scene:
         o.store_radiation_field = int(self.store_rf)
         o.peel_off = int(peel)
         o.precision = int(precision)
+        o.explicit_absorption = int(self.explicit_absorption)
         o.seed = int(seed)
         return o
 

@@ -109,7 +109,7 @@ def sed_instrument(name, inclination_deg, stats=True, distance_mpc=10, comps=Tru
 def simulation(mode, num_packets, sources, media, grid, instruments, source_wavelengths="0.55 micron",
                instrument_wlg='<ListWavelengthGrid wavelengths="0.55 micron" relativeHalfWidth="0" log="false"/>',
                force_scattering=True, store_rf=False, rf_wlg="", seed=0, num_density_samples=100,
-               min_weight_reduction=1e4, path_length_bias=0.5):
+               min_weight_reduction=1e4, path_length_bias=0.5, explicit_absorption=False):
     """A complete MonteCarloSimulation ski document."""
     src_attr = f' wavelengths="{source_wavelengths}"' if mode.startswith("Oligo") else ' minWavelength="0.1 micron" maxWavelength="10 micron"'
     rf = ""
@@ -127,7 +127,7 @@ def simulation(mode, num_packets, sources, media, grid, instruments, source_wave
 <sourceSystem type="SourceSystem"><SourceSystem{src_attr} sourceBias="0.5">
 <sources type="Source">{sources}</sources></SourceSystem></sourceSystem>
 <mediumSystem type="MediumSystem"><MediumSystem>
-<photonPacketOptions type="PhotonPacketOptions"><PhotonPacketOptions explicitAbsorption="false" forceScattering="{"true" if force_scattering else "false"}" minWeightReduction="{min_weight_reduction:g}" minScattEvents="0" pathLengthBias="{path_length_bias:g}"/></photonPacketOptions>
+<photonPacketOptions type="PhotonPacketOptions"><PhotonPacketOptions explicitAbsorption="{"true" if explicit_absorption else "false"}" forceScattering="{"true" if force_scattering else "false"}" minWeightReduction="{min_weight_reduction:g}" minScattEvents="0" pathLengthBias="{path_length_bias:g}"/></photonPacketOptions>
 {rf}
 <media type="Medium">{media}</media>
 <samplingOptions type="SamplingOptions"><SamplingOptions numDensitySamples="{num_density_samples}" numPropertySamples="1" aggregateVelocity="Average"/></samplingOptions>
@@ -203,14 +203,16 @@ def galaxy_voronoi(num_packets=1e8, npix=512, nlambda=100, num_sites=1_000_000, 
                       instrument_wlg=wlg, store_rf=store_rf, rf_wlg=wlg)
 
 
-def shell_cartesian(num_packets=1e6, nbins=64, npix=256, stats=True, points=None):
+def shell_cartesian(num_packets=1e6, nbins=64, npix=256, stats=True, points=None, explicit_absorption=False,
+                    force_scattering=True):
     """Dust shell (r^-2 between 0.1 and 1 pc, radial tau_V = 1, i.e. tau_X = 2 through the centre) on a
     Cartesian grid of +-1 pc, isotropic point source at the centre, 0.55 micron, HG g = 0.6,
     albedo 0.5, one frame at inclination 30 degrees plus one SED instrument."""
     mix = mean_list_mix([0.5, 0.6], [1, 1], [0.5, 0.5], [0.6, 0.6])
     return simulation("OligoExtinctionOnly", num_packets, point_source(),
                       shell_medium(0.1, 1, 2, 2, mix), cartesian_grid(1, nbins, points),
-                      frame_instrument("i30", 30, 2, "pc", npix, stats) + sed_instrument("sed", 30, stats))
+                      frame_instrument("i30", 30, 2, "pc", npix, stats) + sed_instrument("sed", 30, stats),
+                      explicit_absorption=explicit_absorption, force_scattering=force_scattering)
 
 
 def galaxy_tetra(num_packets, vertex_filename, tau_v=1.0, npix=256, nlambda=32, half_size_kpc=25):

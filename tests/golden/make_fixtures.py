@@ -13,6 +13,9 @@ Fixtures written:
   paths_<name>.npz   grid + medium export, rays, reference (count, m, ds) per ray, reference tau
   shell_c16.npz      export of the 16^3 dust-shell scene + reference SED/frame statistics of a
                      2e5-packet run
+  shell_c16_explicit.npz  reference frame/SED statistics of the same scene with explicit absorption
+                     (forced and free propagation), 2e5 packets each; `python
+                     tests/golden/make_fixtures.py explicit` writes only this one
 """
 import os
 import shutil
@@ -141,7 +144,36 @@ def main():
         [stats[0], stats[1] / c, stats[2] / c ** 2]), ref_stats_scale=c, ref_jy_per_w=jy_per_w)
     np.savez_compressed(os.path.join(OUT, "shell_c16.npz"), **data)
     print("shell_c16: stats scale", c)
+    explicit_fixture(mjysr_per_w, npp)
+
+
+def explicit_fixture(mjysr_per_w, npp):
+    """The 16^3 shell with explicit absorption (PhotonPacketOptions::explicitAbsorption), forced and
+    free propagation: reference frame and SED statistics of single-threaded runs of npp packets. Each
+    run scales its statistics files by its own c (from the largest sums); c is recovered per run from
+    its total image as for shell_c16 (same instruments, so the same MJy/sr per raw W)."""
+    out = {}
+    for tag, forced in (("forced", True), ("free", False)):
+        with tempfile.TemporaryDirectory() as tmp:
+            with open(os.path.join(tmp, "ea.ski"), "w") as f:
+                f.write(ski.shell_cartesian(npp, nbins=16, npix=64, explicit_absorption=True, force_scattering=forced))
+            subprocess.run([os.path.join(BIN, "skirt"), "-t", "1", "ea.ski"], cwd=tmp, check=True,
+                           stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+            st = np.array([fits.read(os.path.join(tmp, f"ea_i30_stats{k}.fits"))[0][0] for k in range(5)])
+            ss = np.loadtxt(os.path.join(tmp, "ea_sed_sedstats.dat"))
+            total = fits.read(os.path.join(tmp, "ea_i30_total.fits"))[0][0]
+        c = st[1].sum() / (total / mjysr_per_w).sum()
+        out[f"ref_{tag}_frame_w"] = np.array([st[0], st[1] / c, st[2] / c ** 2])
+        out[f"ref_{tag}_sedstats"] = ss[1:]
+    np.savez_compressed(os.path.join(OUT, "shell_c16_explicit.npz"), ref_npp=npp, **out)
+    print("shell_c16_explicit written")
 
 
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["explicit"]:
+        z = np.load(os.path.join(OUT, "shell_c16.npz"))
+        meta = __import__("skgpu").Scene.read_export(z)[0]
+        pix = float(meta["instr0_xpsiz"]) / float(meta["instr0_distance"])
+        explicit_fixture(float(z["ref_jy_per_w"]) * 1e-6 / (pix * pix), int(z["ref_npp"]))
+    else:
+        main()

@@ -98,3 +98,27 @@ def test_abi_struct_layouts():
         f = getattr(lib, f"or_sizeof_{name}")
         f.restype = C.c_int
         assert f() == C.sizeof(cls), name
+
+
+@pytest.mark.parametrize("forced", [True, False])
+def test_oracle_explicit_absorption_matches_reference_statistics(golden, oracle_backend, forced):
+    """Explicit absorption (PhotonPacketOptions::explicitAbsorption), forced and free propagation:
+    the oracle's frame and SED against the reference's own runs of the same scene (z-scores)."""
+    z = golden("shell_c16.npz")
+    e = golden("shell_c16_explicit.npz")
+    tag = "forced" if forced else "free"
+    sc = Scene.from_export(z)
+    sc.explicit_absorption = True
+    sc.force_scattering = forced
+    sc.upload(oracle_backend)
+    n = int(e["ref_npp"])
+    res = sc.run(oracle_backend, n, seed=11)
+    st = res[0]["stats"][:, 0]
+    ref = e[f"ref_{tag}_frame_w"]
+    zs = zscores(st[1], st[2], n, ref[1], ref[2], n)
+    assert len(zs) > 2000
+    assert abs(zs.mean()) < 0.1 and 0.85 < zs.std() < 1.15
+    sst = res[1]["stats"][:, 0]
+    rs = e[f"ref_{tag}_sedstats"]
+    zsed = zscores(sst[1:2], sst[2:3], n, rs[1:2], rs[2:3], n)
+    assert abs(zsed[0]) < 4
