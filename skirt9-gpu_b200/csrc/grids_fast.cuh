@@ -386,14 +386,12 @@ struct VoronoiRec32 : GenBase
         {
             const float4* R = g.vRec + rec;
             float4 h0 = __ldg(R), h1 = __ldg(R + 1);
-            double px = __hiloint2double(__float_as_int(h0.y), __float_as_int(h0.x));
-            double py = __hiloint2double(__float_as_int(h0.w), __float_as_int(h0.z));
-            double pz = __hiloint2double(__float_as_int(h1.y), __float_as_int(h1.x));
+            // the FP64 site only rebases the position here (the near-tie branch reloads it)
+            float lx = static_cast<float>(rx - __hiloint2double(__float_as_int(h0.y), __float_as_int(h0.x)));
+            float ly = static_cast<float>(ry - __hiloint2double(__float_as_int(h0.w), __float_as_int(h0.z)));
+            float lz = static_cast<float>(rz - __hiloint2double(__float_as_int(h1.y), __float_as_int(h1.x)));
             int cell = __float_as_int(h1.z);
             int n4 = (__float_as_int(h1.w) + 3) & ~3;
-            float lx = static_cast<float>(rx - px);
-            float ly = static_cast<float>(ry - py);
-            float lz = static_cast<float>(rz - pz);
             const float4* E = R + 2;
             const int4* ids = reinterpret_cast<const int4*>(R + 2 + n4);
             float best = FLT_MAX, second = FLT_MAX, scale = 0.f;
@@ -442,6 +440,8 @@ struct VoronoiRec32 : GenBase
             if (is != kNone && second - best <= 2e-5f * (best + scale))
             {
                 // near tie: decide with the exact FP64 sites
+                double px, py, pz;
+                site(g, rec, px, py, pz);
                 double s1 = exit64(g, px, py, pz, ib), s2 = exit64(g, px, py, pz, is);
                 if (s2 > 0. && (s2 < s1 || !(s1 > 0.)))
                 {
