@@ -147,7 +147,7 @@ int waveAlloc(skgpu_ctx* ctx, T** p, size_t n)
     return SKGPU_OK;
 }
 
-// packet pool of P slots (SoA), task buffers (peel: P per observer group; propagation: P per
+// packet pool of P slots (128-byte records), task buffers (peel: P per observer group; propagation: P per
 // kind), two parities each, and the control block
 int ensureWaveBuffers(skgpu_ctx* ctx, int P, int groups, int stats)
 {
@@ -159,14 +159,9 @@ int ensureWaveBuffers(skgpu_ctx* ctx, int P, int groups, int stats)
     Wave& w = ctx->wave;
     PacketPool& k = w.pk;
     int rc = 0;
-    double** dbl[] = {&k.x, &k.y, &k.z, &k.kx, &k.ky, &k.kz, &k.L, &k.Lth, &k.lam, &k.tauPath, &k.rngSpare};
-    for (double** d : dbl)
-        if ((rc = waveAlloc(ctx, d, P))) return rc;
-    int** ints[] = {&k.rngHas, &k.nscatt, &k.ellMix, &k.ellRF, &k.nstat, &k.freeSlots};
-    for (int** d : ints)
-        if ((rc = waveAlloc(ctx, d, P))) return rc;
-    if ((rc = waveAlloc(ctx, &k.hist, P))) return rc;
-    if ((rc = waveAlloc(ctx, &k.rngCtr, P))) return rc;
+    if ((rc = waveAlloc(ctx, &k.rec, P))) return rc;
+    if ((rc = waveAlloc(ctx, &k.nstat, P))) return rc;
+    if ((rc = waveAlloc(ctx, &k.freeSlots, P))) return rc;
     size_t ns = stats ? static_cast<size_t>(P) * STATS_CAP : 1;
     if ((rc = waveAlloc(ctx, &k.skey, ns))) return rc;
     if ((rc = waveAlloc(ctx, &k.sw, ns))) return rc;
@@ -174,8 +169,6 @@ int ensureWaveBuffers(skgpu_ctx* ctx, int P, int groups, int stats)
     if ((rc = waveAlloc(ctx, &k.gLast, P))) return rc;
     if ((rc = waveAlloc(ctx, &k.gPend, P))) return rc;
     if ((rc = waveAlloc(ctx, &k.gRatio, P))) return rc;
-    if ((rc = waveAlloc(ctx, &k.cell, P))) return rc;
-    if ((rc = waveAlloc(ctx, &k.scene, P))) return rc;
     for (int b = 0; b < 2; ++b)
         for (int kind = 0; kind < NUM_KINDS; ++kind)
         {
@@ -1102,12 +1095,9 @@ static size_t carveWave(Wave& w, unsigned char* base, int P, int groups, int sta
         off += std::max<size_t>(count, 1) * sizeof(T);
     };
     PacketPool& k = w.pk;
-    double** dbl[] = {&k.x, &k.y, &k.z, &k.kx, &k.ky, &k.kz, &k.L, &k.Lth, &k.lam, &k.tauPath, &k.rngSpare};
-    for (double** d : dbl) take(d, P);
-    int** ints[] = {&k.rngHas, &k.nscatt, &k.ellMix, &k.ellRF, &k.nstat, &k.freeSlots};
-    for (int** d : ints) take(d, P);
-    take(&k.hist, P);
-    take(&k.rngCtr, P);
+    take(&k.rec, P);
+    take(&k.nstat, P);
+    take(&k.freeSlots, P);
     size_t ns = stats ? static_cast<size_t>(P) * STATS_CAP : 1;
     take(&k.skey, ns);
     take(&k.sw, ns);

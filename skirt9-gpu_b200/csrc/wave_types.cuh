@@ -10,17 +10,27 @@ namespace skg {
 // network samples (filled and consumed within one pass)
 enum TaskKind { K_PEEL = 0, K_PROP1 = 1, K_PROP2 = 2, K_FREE = 3, K_GUIDE = 4, NUM_KINDS = 5 };
 
+// The state of one packet slot that the stage kernels and the traversal kernel's task start read:
+// one 128-byte line, so that a packet taken from a task queue (slots in no particular order) costs
+// one line instead of a sector from each of eighteen arrays.
+struct alignas(128) PacketRec
+{
+    double x, y, z, kx, ky, kz;
+    double L, Lth, lam, tauPath;
+    unsigned long long hist;
+    double rngSpare;
+    unsigned rngCtr;
+    int rngHas;
+    int nscatt, ellMix, ellRF;
+    int cell;   // cell of the last interaction (-1 after launch): start-cell hint of the next rays
+    int scene;  // batched runs: the scene (simulation) of the slot's history
+    int pad;
+};
+static_assert(sizeof(PacketRec) == 128, "one line per packet");
+
 struct PacketPool
 {
-    double *x, *y, *z, *kx, *ky, *kz;
-    double *L, *Lth, *lam, *tauPath;
-    unsigned long long* hist;
-    unsigned* rngCtr;
-    double* rngSpare;
-    int* rngHas;
-    int *nscatt, *ellMix, *ellRF;
-    int* cell;  // cell of the last interaction (-1 after launch): start-cell hint of the next rays
-    int* scene; // batched runs: the scene (simulation) of the slot's history
+    PacketRec* rec;  // P
     // per-history statistics buffer (only when an instrument records statistics)
     unsigned long long* skey;  // P * STATS_CAP
     double* sw;

@@ -31,7 +31,7 @@
 namespace skg {
 
 // the scene of a packet slot (batched runs keep one per slot)
-SKG_D const Scene& slotScene(const Wave& w, int slot) { return w.nScenes > 1 ? w.scenes[w.pk.scene[slot]] : w.sc; }
+SKG_D const Scene& slotScene(const Wave& w, int slot) { return w.nScenes > 1 ? w.scenes[w.pk.rec[slot].scene] : w.sc; }
 
 
 // ---------------------------------------------------------------------------------------------
@@ -52,17 +52,17 @@ SKG_D unsigned warpAppend(unsigned* counter)
 
 SKG_D void loadRng(const Wave& w, int slot, Rng& r)
 {
-    r.start(slotScene(w, slot).seed, w.pk.hist[slot]);
-    r.ctr = w.pk.rngCtr[slot];
-    r.hasSpare = w.pk.rngHas[slot];
-    r.spare = w.pk.rngSpare[slot];
+    r.start(slotScene(w, slot).seed, w.pk.rec[slot].hist);
+    r.ctr = w.pk.rec[slot].rngCtr;
+    r.hasSpare = w.pk.rec[slot].rngHas;
+    r.spare = w.pk.rec[slot].rngSpare;
 }
 
 SKG_D void storeRng(const Wave& w, int slot, const Rng& r)
 {
-    w.pk.rngCtr[slot] = r.ctr;
-    w.pk.rngHas[slot] = r.hasSpare;
-    w.pk.rngSpare[slot] = r.spare;
+    w.pk.rec[slot].rngCtr = r.ctr;
+    w.pk.rec[slot].rngHas = r.hasSpare;
+    w.pk.rec[slot].rngSpare = r.spare;
 }
 
 SKG_D void addMoments(double* base, size_t plane, size_t idx, double wsum)
@@ -270,12 +270,12 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __g
                     else { kind = K_FREE; idx = t - n0 - n1 - n2; }
                     const TaskBuf& b = w.q[cur][kind];
                     slot = b.slot[idx];
-                    if constexpr (Multi) sid = w.pk.scene[slot];
+                    if constexpr (Multi) sid = w.pk.rec[slot].scene;
                     // peel-off rays and complete forced paths (PROP1: radiation field) accumulate
                     // extinction; under explicit absorption the interaction searches (PROP2, FREE)
                     // walk on the scattering optical depth (setScatteringAndAbsorptionOpticalDepths)
                     {
-                        int ell = w.pk.ellMix[slot];
+                        int ell = w.pk.rec[slot].ellMix;
                         sext = static_cast<Acc>(scn().explicitAbs && kind >= K_PROP2 ? scn().mixSca[ell] : scn().mixExt[ell]);
                     }
                     tau = 0.;
@@ -286,16 +286,16 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __g
                         const InstrDev& in = scn().instr[b.info[idx] & 0xFF];
                         fA = static_cast<Acc>(log(b.par[idx]) + 745.);  // taumax = log(L) + 745
                         wk.start(scn().g, b.x[idx], b.y[idx], b.z[idx], in.kobs[0], in.kobs[1], in.kobs[2],
-                                 w.pk.cell ? w.pk.cell[slot] : -1);
+                                 w.pk.rec[slot].cell);
                     }
                     else
                     {
-                        wk.start(scn().g, w.pk.x[slot], w.pk.y[slot], w.pk.z[slot], w.pk.kx[slot], w.pk.ky[slot],
-                                 w.pk.kz[slot], w.pk.cell ? w.pk.cell[slot] : -1);
+                        wk.start(scn().g, w.pk.rec[slot].x, w.pk.rec[slot].y, w.pk.rec[slot].z, w.pk.rec[slot].kx, w.pk.rec[slot].ky,
+                                 w.pk.rec[slot].kz, w.pk.rec[slot].cell);
                         if (kind == K_PROP1)
                         {
-                            fA = static_cast<Acc>(w.pk.L[slot]);
-                            iA = scn().rfOn ? w.pk.ellRF[slot] : -1;
+                            fA = static_cast<Acc>(w.pk.rec[slot].L);
+                            iA = scn().rfOn ? w.pk.rec[slot].ellRF : -1;
                             fB = 0.;
                             fC = 1.;
                         }
@@ -389,9 +389,9 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __g
                     bool peel = kind == K_PEEL;
                     const double* ko = peel ? scn().instr[b.info[idx] & 0xFF].kobs : nullptr;
                     printf("skgpu: traversal guard: kind %d hist %llu start (%.17g %.17g %.17g) dir (%.17g %.17g %.17g) cell %d\n",
-                           kind, static_cast<unsigned long long>(w.pk.hist[slot]), peel ? b.x[idx] : w.pk.x[slot],
-                           peel ? b.y[idx] : w.pk.y[slot], peel ? b.z[idx] : w.pk.z[slot], peel ? ko[0] : w.pk.kx[slot],
-                           peel ? ko[1] : w.pk.ky[slot], peel ? ko[2] : w.pk.kz[slot], m);
+                           kind, static_cast<unsigned long long>(w.pk.rec[slot].hist), peel ? b.x[idx] : w.pk.rec[slot].x,
+                           peel ? b.y[idx] : w.pk.rec[slot].y, peel ? b.z[idx] : w.pk.rec[slot].z, peel ? ko[0] : w.pk.rec[slot].kx,
+                           peel ? ko[1] : w.pk.rec[slot].ky, peel ? ko[2] : w.pk.rec[slot].kz, m);
                 }
                 atomicOr(&w.ctl->err, 4);
                 done = true;
@@ -453,7 +453,7 @@ static __global__ void __launch_bounds__(256) shadePeelKernel(const __grid_const
         double Lp = b.par[t];
         double Lext = Lp * exp(-b.tau[t]);
         double x = b.x[t], y = b.y[t], z = b.z[t];
-        double lambda = w.pk.lam[slot];
+        double lambda = w.pk.rec[slot].lam;
         for (int i = group; i < sc.ninstr && (i == group || sc.instr[i].same); ++i)
         {
             const InstrDev& in = sc.instr[i];
@@ -538,13 +538,13 @@ static __global__ void __launch_bounds__(256) shadeProp1Kernel(const __grid_cons
             // explicit absorption samples on the scattering optical depth of the path: for one medium
             // with constant cross sections tau_sca = tau_ext * sca / ext (the trace accumulated
             // extinction for the radiation field)
-            int ell = w.pk.ellMix[slot];
+            int ell = w.pk.rec[slot].ellMix;
             double ext = sc.mixExt[ell];
             taupath = ext > 0. ? taupath * (sc.mixSca[ell] / ext) : 0.;
         }
         if (taupath <= 0.)
         {
-            w.pk.L[slot] *= 0.;
+            w.pk.rec[slot].L *= 0.;
             endHistory(w, slot);
             continue;
         }
@@ -559,10 +559,10 @@ static __global__ void __launch_bounds__(256) shadeProp1Kernel(const __grid_cons
             tau = rng.uniform() < xi ? rng.uniform() * taupath : exponCutoff(rng, taupath);
             double p = -exp(-tau) / expm1(-taupath);
             double q = (1.0 - xi) * p + xi / taupath;
-            w.pk.L[slot] *= p / q;
+            w.pk.rec[slot].L *= p / q;
         }
         storeRng(w, slot, rng);
-        w.pk.tauPath[slot] = taupath;
+        w.pk.rec[slot].tauPath = taupath;
         emitProp(w, nxt, K_PROP2, slot, tau);
     }
 }
@@ -583,14 +583,14 @@ SKG_D void guideRecord(const Wave& w, int slot, int nscatt, double x, double y, 
         sc.guideRec[pend].dStart = w.pk.gD[slot];
         w.pk.gPend[slot] = -1;
     }
-    unsigned long long h = w.pk.hist[slot];
+    unsigned long long h = w.pk.rec[slot].hist;
     U4 r = philox4x32_10(U4{static_cast<uint32_t>(nscatt), 0x67756964u, static_cast<uint32_t>(h), static_cast<uint32_t>(h >> 32)},
                          static_cast<uint32_t>(sc.seed), static_cast<uint32_t>(sc.seed >> 32) ^ 0x5bd1e995u);
     if (static_cast<float>(r.x) * 2.3283064e-10f >= sc.guideRecFrac) return;
     unsigned long long idx = atomicAdd(sc.guideRecCount, 1ULL);
     if (idx >= sc.guideRecCap) return;
     GuideRecord& q = sc.guideRec[idx];
-    guideFeatures(q.f, x, y, z, kx0, ky0, kz0, w.pk.lam[slot], w.pk.tauPath[slot], sc.g.ext);
+    guideFeatures(q.f, x, y, z, kx0, ky0, kz0, w.pk.rec[slot].lam, w.pk.rec[slot].tauPath, sc.g.ext);
     q.k[0] = static_cast<float>(kx);
     q.k[1] = static_cast<float>(ky);
     q.k[2] = static_cast<float>(kz);
@@ -613,8 +613,8 @@ SKG_D void interact(const Wave& w, int cur, int nxt, int slot, int m, double sIn
         endHistory(w, slot);
         return;
     }
-    int ell = w.pk.ellMix[slot];
-    double L = w.pk.L[slot];
+    int ell = w.pk.rec[slot].ellMix;
+    double L = w.pk.rec[slot].L;
     if (sc.explicitAbs)
     {
         // absorption optical depth at the interaction point: tau_int * abs / sca for one medium with
@@ -623,7 +623,7 @@ SKG_D void interact(const Wave& w, int cur, int nxt, int slot, int m, double sIn
         double sca = sc.mixSca[ell];
         double tauAbs = tauInt * (sc.mixExt[ell] - sca) / sca;
         if (forced)
-            L *= -expm1(-w.pk.tauPath[slot]) * exp(-tauAbs);
+            L *= -expm1(-w.pk.rec[slot].tauPath) * exp(-tauAbs);
         else
             L *= exp(-tauAbs);
     }
@@ -631,27 +631,27 @@ SKG_D void interact(const Wave& w, int cur, int nxt, int slot, int m, double sIn
     {
         double albedo = albedoAt(sc, m, sc.mixSca[ell], sc.mixExt[ell]);
         if (forced)
-            L *= -expm1(-w.pk.tauPath[slot]) * albedo;
+            L *= -expm1(-w.pk.rec[slot].tauPath) * albedo;
         else
             L *= albedo;
     }
-    w.pk.L[slot] = L;
-    double kx = w.pk.kx[slot], ky = w.pk.ky[slot], kz = w.pk.kz[slot];
-    double x = w.pk.x[slot] + sInt * kx;
-    double y = w.pk.y[slot] + sInt * ky;
-    double z = w.pk.z[slot] + sInt * kz;
-    w.pk.x[slot] = x;
-    w.pk.y[slot] = y;
-    w.pk.z[slot] = z;
-    if (w.pk.cell) w.pk.cell[slot] = m;
-    int nscatt = w.pk.nscatt[slot];
+    w.pk.rec[slot].L = L;
+    double kx = w.pk.rec[slot].kx, ky = w.pk.rec[slot].ky, kz = w.pk.rec[slot].kz;
+    double x = w.pk.rec[slot].x + sInt * kx;
+    double y = w.pk.rec[slot].y + sInt * ky;
+    double z = w.pk.rec[slot].z + sInt * kz;
+    w.pk.rec[slot].x = x;
+    w.pk.rec[slot].y = y;
+    w.pk.rec[slot].z = z;
+    w.pk.rec[slot].cell = m;
+    int nscatt = w.pk.rec[slot].nscatt;
     // termination (performLifeCycle, MonteCarloSimulation.cpp:643-660). Under guided scattering the
     // test applies to the weight without the guiding factors, so that termination depends on the
     // path alone and the guided runs estimate the same quantity as plain ones (in optically thick
     // media the threshold L0/minWeightReduction is not small against the emergent flux)
     double Lterm = L;
     if (sc.guideMode == 2 && w.pk.gRatio[slot] > 0.f) Lterm = L / static_cast<double>(w.pk.gRatio[slot]);
-    if (L <= 0 || (forced && Lterm <= w.pk.Lth[slot] && nscatt >= sc.minScatt))
+    if (L <= 0 || (forced && Lterm <= w.pk.rec[slot].Lth && nscatt >= sc.minScatt))
     {
         endHistory(w, slot);
         return;
@@ -676,10 +676,10 @@ SKG_D void interact(const Wave& w, int cur, int nxt, int slot, int m, double sIn
     }
     double kx0 = kx, ky0 = ky, kz0 = kz;
     scatterHG(rng, g, kx, ky, kz);
-    w.pk.kx[slot] = kx;
-    w.pk.ky[slot] = ky;
-    w.pk.kz[slot] = kz;
-    w.pk.nscatt[slot] = nscatt + 1;
+    w.pk.rec[slot].kx = kx;
+    w.pk.rec[slot].ky = ky;
+    w.pk.rec[slot].kz = kz;
+    w.pk.rec[slot].nscatt = nscatt + 1;
     atomicAdd(&w.ctl->counters[2], 1ULL);
     if (sc.guideMode == 1) guideRecord(w, slot, nscatt, x, y, z, kx0, ky0, kz0, kx, ky, kz, L);
     beginPropagation(w, nxt, slot, rng);
@@ -696,8 +696,8 @@ SKG_D double guidedScatter(const Wave& w, int nxt, int slot, const float* o)
     guideMixture(o, mix);
     Rng rng;
     loadRng(w, slot, rng);
-    double g = sc.mixG[w.pk.ellMix[slot]];
-    double kx0 = w.pk.kx[slot], ky0 = w.pk.ky[slot], kz0 = w.pk.kz[slot];
+    double g = sc.mixG[w.pk.rec[slot].ellMix];
+    double kx0 = w.pk.rec[slot].kx, ky0 = w.pk.rec[slot].ky, kz0 = w.pk.rec[slot].kz;
     double kx = kx0, ky = ky0, kz = kz0;
     float ratio = w.pk.gRatio[slot];
     double alpha = ratio <= GUIDE_RATIO_MAX ? static_cast<double>(sc.guideAlpha) : 0.0;
@@ -719,12 +719,12 @@ SKG_D double guidedScatter(const Wave& w, int nxt, int slot, const float* o)
         atomicOr(&w.ctl->err, 32);  // non-finite guiding density or weight: the packet is dropped and flagged
         wgt = 0.;
     }
-    w.pk.L[slot] *= wgt;
+    w.pk.rec[slot].L *= wgt;
     w.pk.gRatio[slot] = static_cast<float>(ratio * wgt);
-    w.pk.kx[slot] = kx;
-    w.pk.ky[slot] = ky;
-    w.pk.kz[slot] = kz;
-    w.pk.nscatt[slot] += 1;
+    w.pk.rec[slot].kx = kx;
+    w.pk.rec[slot].ky = ky;
+    w.pk.rec[slot].kz = kz;
+    w.pk.rec[slot].nscatt += 1;
     atomicAdd(&w.ctl->counters[2], 1ULL);
     beginPropagation(w, nxt, slot, rng);
     storeRng(w, slot, rng);
@@ -751,8 +751,8 @@ static __global__ void __launch_bounds__(GM_TILE) guideScatterKernel(const __gri
         int slot = valid ? b.slot[i] : 0;
         float f[GUIDE_IN], o[GUIDE_OUT];
         if (valid)
-            guideFeatures(f, w.pk.x[slot], w.pk.y[slot], w.pk.z[slot], w.pk.kx[slot], w.pk.ky[slot], w.pk.kz[slot],
-                          w.pk.lam[slot], w.pk.tauPath[slot], slotScene(w, slot).g.ext);
+            guideFeatures(f, w.pk.rec[slot].x, w.pk.rec[slot].y, w.pk.rec[slot].z, w.pk.rec[slot].kx, w.pk.rec[slot].ky, w.pk.rec[slot].kz,
+                          w.pk.rec[slot].lam, w.pk.rec[slot].tauPath, slotScene(w, slot).g.ext);
         else
             for (int k = 0; k < GUIDE_IN; ++k) f[k] = 0.f;
         if (!failed && !guideTileForward(t, f, o))
@@ -836,25 +836,25 @@ static __global__ void __launch_bounds__(256) launchKernel(const __grid_constant
             // batch history -> (scene, segment history of that scene)
             int sid = 0;
             while (sid + 1 < w.nScenes && hist >= w.prefix[sid + 1]) ++sid;
-            w.pk.scene[slot] = sid;
+            w.pk.rec[slot].scene = sid;
             hist = w.sfirst[sid] + (hist - w.prefix[sid]);
         }
         const Scene& sc = slotScene(w, slot);
         Rng rng;
         rng.start(sc.seed, hist);
         Launched o = launchPacket(sc, hist, rng);
-        w.pk.hist[slot] = hist;
-        w.pk.x[slot] = o.x; w.pk.y[slot] = o.y; w.pk.z[slot] = o.z;
-        w.pk.kx[slot] = o.kx; w.pk.ky[slot] = o.ky; w.pk.kz[slot] = o.kz;
-        w.pk.L[slot] = o.L;
-        w.pk.Lth[slot] = o.L / sc.minWeightRed;
-        w.pk.lam[slot] = o.lambda;
-        w.pk.nscatt[slot] = 0;
+        w.pk.rec[slot].hist = hist;
+        w.pk.rec[slot].x = o.x; w.pk.rec[slot].y = o.y; w.pk.rec[slot].z = o.z;
+        w.pk.rec[slot].kx = o.kx; w.pk.rec[slot].ky = o.ky; w.pk.rec[slot].kz = o.kz;
+        w.pk.rec[slot].L = o.L;
+        w.pk.rec[slot].Lth = o.L / sc.minWeightRed;
+        w.pk.rec[slot].lam = o.lambda;
+        w.pk.rec[slot].nscatt = 0;
         int ell = sc.nmix > 0 ? max(0, locateClip(sc.mixLb, sc.nmix, o.lambda)) : 0;  // DustMix::indexForLambda
-        w.pk.ellMix[slot] = ell;
-        w.pk.ellRF[slot] = sc.rfOn ? wlgBin(sc.rfB, sc.rfNb, sc.rfEll, o.lambda) : -1;
+        w.pk.rec[slot].ellMix = ell;
+        w.pk.rec[slot].ellRF = sc.rfOn ? wlgBin(sc.rfB, sc.rfNb, sc.rfEll, o.lambda) : -1;
         if (w.anyStats) w.pk.nstat[slot] = 0;
-        if (w.pk.cell) w.pk.cell[slot] = -1;
+        w.pk.rec[slot].cell = -1;
         if (sc.guideMode == 2) w.pk.gRatio[slot] = 1.f;
         if (sc.guideMode == 1)
         {
