@@ -346,7 +346,7 @@ def run_batch_arm(args, rank, world, local):
         line["config"]["simulations"] = n
         if n != 16 or args.packet_scale != 1.0:
             line["config"]["subset"] = f"first {n} simulations, {args.packet_scale:g} of their packets (profiling case)"
-        line["config"]["launch_shape"] = "default (pool 2^20 slots, resident traversal blocks, 4 stage blocks/SM)"
+        line["config"]["launch_shape"] = "default (pool 2^22 slots, resident traversal blocks, 4 stage blocks/SM)"
         if not args.no_cpu_baseline:
             try:
                 line["cpu_baseline"] = cpu_baseline("batch")

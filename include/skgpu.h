@@ -205,7 +205,7 @@ int skgpu_run_primary(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t t
 #define SKGPU_NOALLOC_MAX_GROUPS 4
 #define SKGPU_NOALLOC_SCRATCH_BYTES (48u * 1024u * 1024u)
 int skgpu_run_primary_noalloc(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t total_packets);
-/* Launch shape of later runs (0 keeps a default): packet slots in flight (at most 2^20), resident
+/* Launch shape of later runs (0 keeps a default): packet slots in flight (default and maximum 2^22), resident
  * traversal blocks per SM (capped by what fits) and stage-kernel blocks per SM. Set by an
  * autotuner (skgpu/autotune.py); no reference counterpart. */
 int skgpu_set_launch_shape(skgpu_ctx* ctx, int32_t pool_slots, int32_t trace_blocks_per_sm, int32_t shade_blocks_per_sm);

@@ -127,7 +127,8 @@ int syncLeafDensity(skgpu_ctx* ctx)
 }
 
 // histories in flight at most; a larger range streams through the pool
-constexpr uint64_t POOL_MAX = 1u << 20;
+constexpr uint64_t POOL_DEFAULT = 1u << 22;  // packet slots in flight unless a launch shape sets them
+constexpr uint64_t POOL_MAX = 1u << 22;
 // wavefront passes per run at most (each history needs about two passes per scattering event)
 constexpr long long MAX_PASSES = 2LL * MAX_SCATT_EVENTS + 64;
 
@@ -1060,7 +1061,7 @@ int skgpu_run_primary(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t t
     // packet pool and task queues, sized for up to POOL_MAX histories in flight
     int groups, anyStats;
     waveShape(ctx, groups, anyStats);
-    uint64_t poolMax = ctx->shapePool > 0 ? static_cast<uint64_t>(ctx->shapePool) : POOL_MAX;
+    uint64_t poolMax = ctx->shapePool > 0 ? static_cast<uint64_t>(ctx->shapePool) : POOL_DEFAULT;
     int P = static_cast<int>(std::min<uint64_t>(std::max<uint64_t>(count, 1), poolMax));
     if ((rc = ensureWaveBuffers(ctx, P, groups, anyStats))) return rc;
     Wave w = ctx->wave;
@@ -1650,7 +1651,7 @@ int skgpu_set_launch_shape(skgpu_ctx* ctx, int32_t pool_slots, int32_t trace_blo
     if (!ctx) return SKGPU_ERR_ARG;
     if (pool_slots < 0 || pool_slots > static_cast<int32_t>(POOL_MAX) || trace_blocks_per_sm < 0 || trace_blocks_per_sm > 32
         || shade_blocks_per_sm < 0 || shade_blocks_per_sm > 64)
-        return fail(ctx, SKGPU_ERR_ARG, "launch shape: pool in [0, 2^20], trace blocks per SM in [0, 32], shade blocks per SM in [0, 64]");
+        return fail(ctx, SKGPU_ERR_ARG, "launch shape: pool in [0, 2^22], trace blocks per SM in [0, 32], shade blocks per SM in [0, 64]");
     ctx->shapePool = pool_slots;
     ctx->shapeTraceBlocks = trace_blocks_per_sm;
     ctx->shapeShadeBlocks = shade_blocks_per_sm;
@@ -1685,7 +1686,7 @@ int skgpu_run_batch(skgpu_ctx* const* ctxs, int32_t n, const uint64_t* first, co
         sum += count[i];
     }
     CK(cudaSetDevice(ctx->device));
-    uint64_t poolMax = ctx->shapePool > 0 ? static_cast<uint64_t>(ctx->shapePool) : POOL_MAX;
+    uint64_t poolMax = ctx->shapePool > 0 ? static_cast<uint64_t>(ctx->shapePool) : POOL_DEFAULT;
     int P = static_cast<int>(std::min<uint64_t>(std::max<uint64_t>(sum, 1), poolMax));
     int rc = ensureWaveBuffers(ctx, P, groups, anyStats);
     if (rc) return rc;

@@ -34,7 +34,7 @@ def run_batch(scenes, backends, packets, seeds, precision=abi.PREC_FP32, clear=T
 
 
 DEFAULT_CANDIDATES = {
-    "pool_slots": [1 << 18, 1 << 19, 1 << 20],
+    "pool_slots": [1 << 20, 1 << 21, 1 << 22],
     "trace_blocks_per_sm": [1, 2, 3, 4, 6, 8],
     "shade_blocks_per_sm": [2, 4, 8, 16],
 }
