@@ -1058,7 +1058,7 @@ int skgpu_run_primary(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t t
     if (rc) return rc;
     CK(cudaSetDevice(ctx->device));
     if ((rc = ensureRadiationField(ctx))) return rc;
-    // packet pool and task queues, sized for up to POOL_MAX histories in flight
+    // packet pool and task queues, sized for up to POOL_DEFAULT histories in flight (or the launch shape's pool)
     int groups, anyStats;
     waveShape(ctx, groups, anyStats);
     uint64_t poolMax = ctx->shapePool > 0 ? static_cast<uint64_t>(ctx->shapePool) : POOL_DEFAULT;

@@ -1,8 +1,8 @@
 // Wavefront form of the photon-packet life cycle (MonteCarloSimulation::performLifeCycle,
 // SKIRT/core/MonteCarloSimulation.cpp:614-694).
 //
-// Packet state lives in a structure-of-arrays pool of P slots. Every traversal of the life cycle
-// is a task in one of four queues:
+// Packet state lives in a pool of P slots, one 128-byte record per slot. Every traversal of the
+// life cycle is a task in one of four queues (a fifth holds the events of guided scattering):
 //   PEEL   optical depth from a packet position to the domain edge towards one observer
 //          (FluxRecorder::detect -> MediumSystem::getExtinctionOpticalDepth, MediumSystem.cpp:2328-2443)
 //   PROP1  forced scattering, complete path: cumulative optical depth + radiation-field storage
@@ -13,13 +13,14 @@
 //          MediumSystem::setInteractionPointUsingExtinction :2005-2150)
 // One pass of the wavefront runs:
 //   trace    a persistent kernel: each lane takes a task, walks its ray to the end (one cell
-//            crossing per loop iteration, so the warp's lanes stay converged on the crossing code)
-//            and takes the next task index with a warp-aggregated atomic; no other work;
+//            crossing per loop iteration, so the warp's lanes stay converged on the crossing code);
+//            a warp takes new task indices with one atomic once enough of its lanes wait;
 //   shade    one coherent kernel per task kind: detection (peel-off tallies), forced sampling,
 //            interaction + scattering peel-off emission + HG scattering, free-path interaction;
 //            each emits the packet's next tasks into the other queue buffer;
-//   launch   refills free slots with new histories (SourceSystem::launch) and emits their
-//            emission peel-offs and first propagation.
+//   launch   refills free slots with new histories (SourceSystem::launch; in wavelength order
+//            when the range exceeds the pool) and emits their emission peel-offs and first
+//            propagation.
 // Random numbers: each history draws from its own Philox stream in the reference's order
 // (launch, forced sampling, scattering), whatever pass the draws happen in.
 #pragma once
