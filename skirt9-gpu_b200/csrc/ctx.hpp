@@ -81,6 +81,8 @@ struct skgpu_ctx
     int shapePool = 0, shapeTraceBlocks = 0, shapeShadeBlocks = 0;
     // device tables of the last batched run (scene table, history prefix, first histories)
     std::vector<void*> batchBufs;
+    // pass graph of the last run, replayed by the next run with the same parameters
+    skg::GraphCache graphCache;
     // radiation field in the caller's layout (m * nbins + ell), transposed from the device tally at fetch
     double* rfT = nullptr;
     // wavelength-ordered launch (skgpu_set_history_order): mode, keys, order, bucket counts + cursors

@@ -4,16 +4,33 @@
 #include <cuda_runtime.h>
 #include "wave_types.cuh"
 
+#include <vector>
+
 namespace skg { struct StageTimer; }
 
 namespace skg {
 
+// An instantiated graph of passes kept across runs of one context: replayed while the wave
+// parameters, launch shape, walker and timing it was captured with stay the same (repeated
+// segments), re-captured otherwise.
+struct GraphCache
+{
+    cudaGraphExec_t exec = nullptr;
+    std::vector<unsigned char> key;
+    void reset()
+    {
+        if (exec) cudaGraphExecDestroy(exec);
+        exec = nullptr;
+        key.clear();
+    }
+};
+
 // wavefront life cycle, one entry per traversal precision (separate translation units, so that
 // the FP64 one can be compiled without FMA contraction)
 cudaError_t runWaveFP64(int gridKind, const Wave& w, int numSMs, cudaStream_t s, unsigned long long* doneHost,
-                        long long* passes, long long maxPasses, bool useGraph, StageTimer* timer);
+                        long long* passes, long long maxPasses, bool useGraph, StageTimer* timer, GraphCache* cache);
 cudaError_t runWaveFP32(int gridKind, const Wave& w, int numSMs, cudaStream_t s, unsigned long long* doneHost,
-                        long long* passes, long long maxPasses, bool useGraph, StageTimer* timer);
+                        long long* passes, long long maxPasses, bool useGraph, StageTimer* timer, GraphCache* cache);
 
 // wavelength order of the histories of w's range into order[] (keys: count entries, counts and
 // cursor: ORDER_BUCKETS entries each, zeroed here)

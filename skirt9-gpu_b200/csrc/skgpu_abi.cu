@@ -134,6 +134,7 @@ constexpr long long MAX_PASSES = 2LL * MAX_SCATT_EVENTS + 64;
 
 void freeWave(skgpu_ctx* ctx)
 {
+    ctx->graphCache.reset();  // its kernel nodes point into the buffers freed here
     for (void* p : ctx->waveBufs) cudaFree(p);
     ctx->waveBufs.clear();
     ctx->wave = Wave{};
@@ -258,6 +259,7 @@ void skgpu_destroy(skgpu_ctx* ctx)
     devFree(ctx->radR);
     devFree(ctx->radP);
     freeWave(ctx);
+    ctx->graphCache.reset();
     for (void* p : ctx->batchBufs) cudaFree(p);
     cudaFree(ctx->rfT);
     cudaFree(ctx->orderKeys);
@@ -1005,8 +1007,10 @@ static int runAndCollect(skgpu_ctx* ctx, const Wave& w, bool useGraph, bool time
         if (eo != cudaSuccess) return fail(ctx, SKGPU_ERR_CUDA, std::string("run: ordering: ") + cudaGetErrorString(eo));
     }
     cudaError_t e = prec == SKGPU_PREC_FP64_EXACT
-                        ? runWaveFP64(ctx->g.kind, w, ctx->numSMs, ctx->stream, ctx->doneHost, &passes, MAX_PASSES, useGraph, timer)
-                        : runWaveFP32(ctx->g.kind, w, ctx->numSMs, ctx->stream, ctx->doneHost, &passes, MAX_PASSES, useGraph, timer);
+                        ? runWaveFP64(ctx->g.kind, w, ctx->numSMs, ctx->stream, ctx->doneHost, &passes, MAX_PASSES, useGraph, timer,
+                                      &ctx->graphCache)
+                        : runWaveFP32(ctx->g.kind, w, ctx->numSMs, ctx->stream, ctx->doneHost, &passes, MAX_PASSES, useGraph, timer,
+                                      &ctx->graphCache);
     if (e == cudaErrorNotSupported) return fail(ctx, SKGPU_ERR_UNSUPPORTED, "run: no FP32 walker for this grid kind");
     if (e == cudaErrorLaunchTimeout) return fail(ctx, SKGPU_ERR_TIMEOUT, "run: pass limit reached before all histories finished");
     if (e != cudaSuccess) return fail(ctx, SKGPU_ERR_CUDA, std::string("run: ") + cudaGetErrorString(e));

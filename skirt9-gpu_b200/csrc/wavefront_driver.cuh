@@ -3,7 +3,10 @@
 #pragma once
 
 #include <algorithm>
+#include <cstring>
+#include <vector>
 #include <cuda_runtime.h>
+#include "internal.hpp"
 #include "stage_timer.hpp"
 #include "wavefront.cuh"
 
@@ -61,9 +64,29 @@ cudaError_t enqueuePass(const Wave& w, int pass, const WaveLaunch& L, cudaStream
 // four passes and replayed; without it the same kernels are launched directly (no graph objects are
 // created). Returns a CUDA error, or cudaErrorLaunchTimeout (mapped to SKGPU_ERR_TIMEOUT) when the
 // pass limit is reached without finishing. `passes` receives the number of passes run.
+// the inputs a captured pass graph depends on: the wave parameters (by value in every kernel
+// node), the launch shape, the walker and the timing events recorded into it
+template<class Walker>
+std::vector<unsigned char> graphKey(const Wave& w, const WaveLaunch& L, const StageTimer* timer)
+{
+    std::vector<unsigned char> k(sizeof(Wave) + sizeof(WaveLaunch) + 2 * sizeof(void*) + StageTimer::kStages);
+    unsigned char* p = k.data();
+    std::memcpy(p, &w, sizeof(Wave));
+    p += sizeof(Wave);
+    std::memcpy(p, &L, sizeof(WaveLaunch));
+    p += sizeof(WaveLaunch);
+    const void* id = reinterpret_cast<const void*>(&traceKernel<Walker, false>);
+    std::memcpy(p, &id, sizeof(void*));
+    p += sizeof(void*);
+    std::memcpy(p, &timer, sizeof(void*));
+    p += sizeof(void*);
+    for (int i = 0; i < StageTimer::kStages; ++i) p[i] = timer && timer->active[i] ? 1 : 0;
+    return k;
+}
+
 template<class Walker>
 cudaError_t runWave(const Wave& w, int numSMs, cudaStream_t s, unsigned long long* doneHost, long long* passes,
-                    long long maxPasses, bool useGraph, StageTimer* timer)
+                    long long maxPasses, bool useGraph, StageTimer* timer, GraphCache* cache = nullptr)
 {
     WaveLaunch L;
     L.threads = 256;
@@ -90,7 +113,17 @@ cudaError_t runWave(const Wave& w, int numSMs, cudaStream_t s, unsigned long lon
     const int passesPerBatch = StageTimer::kBatch;  // even: the buffer parity returns to 0 after every batch
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    if (useGraph)
+    std::vector<unsigned char> key;
+    if (useGraph && cache)
+    {
+        // a repeated segment replays the graph captured for the previous one
+        key = graphKey<Walker>(w, L, timer);
+        if (cache->exec && cache->key == key)
+            exec = cache->exec;
+        else
+            cache->reset();
+    }
+    if (useGraph && !exec)
     {
         e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
         if (e != cudaSuccess) return e;
@@ -103,10 +136,13 @@ cudaError_t runWave(const Wave& w, int numSMs, cudaStream_t s, unsigned long lon
             return e;
         }
         e = cudaGraphInstantiate(&exec, graph, 0);
-        if (e != cudaSuccess)
+        cudaGraphDestroy(graph);  // the executable graph does not need it
+        graph = nullptr;
+        if (e != cudaSuccess) return e;
+        if (cache)
         {
-            cudaGraphDestroy(graph);
-            return e;
+            cache->exec = exec;
+            cache->key = key;
         }
     }
     const size_t doneOffset = offsetof(Control, done);
@@ -141,8 +177,8 @@ cudaError_t runWave(const Wave& w, int numSMs, cudaStream_t s, unsigned long lon
             break;
         }
     }
-    if (exec) cudaGraphExecDestroy(exec);
-    if (graph) cudaGraphDestroy(graph);
+    if (exec && !(cache && cache->exec == exec)) cudaGraphExecDestroy(exec);
+    if (cache && e != cudaSuccess) cache->reset();  // after an error the next run captures afresh
     return e;
 }
 

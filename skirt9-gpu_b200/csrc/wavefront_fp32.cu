@@ -8,14 +8,14 @@ namespace skg {
 
 cudaError_t runWaveFP32(int gridKind, const Wave& w, int numSMs, cudaStream_t s, unsigned long long* doneHost,
                         long long* passes, long long maxPasses, bool useGraph,
-                        StageTimer* timer)
+                        StageTimer* timer, GraphCache* cache)
 {
     switch (gridKind)
     {
-        case 0: return runWave<CartesianFast<float>>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer);
-        case 1: return runWave<OctreeLeaf32>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer);
-        case 2: return runWave<VoronoiRec32>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer);
-        case 3: return runWave<TetraPlane32>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer);
+        case 0: return runWave<CartesianFast<float>>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer, cache);
+        case 1: return runWave<OctreeLeaf32>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer, cache);
+        case 2: return runWave<VoronoiRec32>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer, cache);
+        case 3: return runWave<TetraPlane32>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer, cache);
     }
     return cudaErrorNotSupported;
 }
