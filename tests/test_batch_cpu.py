@@ -34,3 +34,27 @@ def test_batch_symbols_exported():
     lib = abi.load_library()
     for name in ("skgpu_run_batch", "skgpu_set_launch_shape"):
         assert hasattr(lib, name)
+
+
+def test_autotune_descends_to_the_fastest_shape(monkeypatch):
+    """The coordinate descent of skgpu.batch.autotune on a fake timing model: it visits every
+    candidate of each knob with the others fixed, keeps the fastest, and leaves that shape set."""
+    state = {"shape": (0, 0, 0)}
+    monkeypatch.setattr(abi, "set_launch_shape", lambda be, p, t, s: state.update(shape=(p, t, s)))
+
+    class Fake:
+        def last_run_ms(self):
+            p, t, s = state["shape"]
+            cost = 100.0
+            cost -= {0: 0, 1 << 20: 5, 1 << 21: 8, 1 << 22: 10}[p]
+            cost -= {0: 0, 1: -20, 2: 3, 3: 1}[t]
+            cost -= {0: 0, 2: 1, 4: 2, 8: -1}[s]
+            return cost
+
+    be = Fake()
+    cand = {"pool_slots": [1 << 20, 1 << 21, 1 << 22], "trace_blocks_per_sm": [1, 2, 3], "shade_blocks_per_sm": [2, 4, 8]}
+    shape, ms, trials = batch.autotune(be, lambda: None, cand, rounds=2)
+    assert shape == {"pool_slots": 1 << 22, "trace_blocks_per_sm": 2, "shade_blocks_per_sm": 4}
+    assert ms == 100.0 - 10 - 3 - 2
+    assert state["shape"] == (1 << 22, 2, 4)
+    assert len(trials) >= 1 + 3 + 3 + 3
