@@ -40,6 +40,7 @@ extern "C" {
 #define SKGPU_GRID_OCTREE 1
 #define SKGPU_GRID_VORONOI 2
 #define SKGPU_GRID_TETRA 3
+#define SKGPU_GRID_SPHERE1D 4
 
 /* traversal precision (path kernels and life cycle) */
 #define SKGPU_PREC_FP64_EXACT 0 /* FP64 with the reference generators' operation order, no FMA contraction */
@@ -149,6 +150,10 @@ int skgpu_upload_grid_octree(skgpu_ctx* ctx, int32_t num_nodes, const double* bo
  * (VoronoiMeshSnapshot.cpp:725-740); extent xmin..zmax; eps = 1e-12 * diagonal. */
 int skgpu_upload_grid_voronoi(skgpu_ctx* ctx, int32_t num_sites, const double* sites, const int32_t* nb_begin,
                               const int32_t* nb_index, int32_t num_nb_index, const double* extent, double eps);
+/* Sphere1DSpatialGrid: the num_borders ascending radial border positions r_0 >= 0 .. r_N of its N
+ * radial cells (Sphere1DSpatialGrid::radialBorderPositions, Sphere1DSpatialGrid.hpp:101); cell i is
+ * the shell r_i <= r < r_{i+1} around the origin. */
+int skgpu_upload_grid_sphere1d(skgpu_ctx* ctx, int32_t num_borders, const double* radial_borders);
 /* TetraMeshSpatialGrid: vertices, per tetrahedron its 4 vertex indices, and per face the outward
  * normal, the neighbouring tetrahedron (-1 on the hull) and its face index
  * (TetraMeshSpatialGrid.hpp:107-133). */

@@ -66,6 +66,7 @@
 #include "SpatialGrid.hpp"
 #include "SpatialGridPath.hpp"
 #include "System.hpp"
+#include "Sphere1DSpatialGrid.hpp"
 #include "TetraMeshSpatialGrid.hpp"
 #include "TreeNode.hpp"
 #include "TreeSpatialGrid.hpp"
@@ -173,6 +174,13 @@ namespace
             writeVec(out + "/grid_xb.npy", xb);
             writeVec(out + "/grid_yb.npy", yb);
             writeVec(out + "/grid_zb.npy", zb);
+            return;
+        }
+        if (auto g = dynamic_cast<Sphere1DSpatialGrid*>(grid))
+        {
+            meta.kv("grid", "sphere1d");
+            std::vector<double> rv(begin(g->radialBorderPositions()), end(g->radialBorderPositions()));
+            writeVec(out + "/grid_rv.npy", rv);
             return;
         }
         if (auto g = dynamic_cast<TreeSpatialGrid*>(grid))

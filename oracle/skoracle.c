@@ -113,6 +113,9 @@ typedef struct
     double *tev, *ten, *tebox;
     int *tet, *tent, *tenf;
     int ten_n;
+    /* sphere1d */
+    double* srv;
+    int snr;
 } Grid;
 
 typedef struct
@@ -167,6 +170,7 @@ static void free_grid(Grid* g)
     free(g->tb); free(g->tcell); free(g->tchild); free(g->tnbb); free(g->tnb);
     free(g->vs); free(g->vnbb); free(g->vnb);
     free(g->tev); free(g->ten); free(g->tebox); free(g->tet); free(g->tent); free(g->tenf);
+    free(g->srv);
     memset(g, 0, sizeof *g);
 }
 
@@ -275,6 +279,25 @@ int or_upload_grid_voronoi(or_ctx* c, int32_t num_sites, const double* sites, co
     return SKGPU_OK;
 }
 
+int or_upload_grid_sphere1d(or_ctx* c, int32_t num_borders, const double* rv)
+{
+    if (num_borders < 2 || !rv || !(rv[0] >= 0.)) return fail(c, SKGPU_ERR_ARG, "sphere1d: need >= 2 borders from r >= 0");
+    for (int i = 1; i < num_borders; ++i)
+        if (!(rv[i] > rv[i - 1])) return fail(c, SKGPU_ERR_ARG, "sphere1d: borders must ascend");
+    free_grid(&c->g);
+    Grid* g = &c->g;
+    g->kind = SKGPU_GRID_SPHERE1D;
+    g->snr = num_borders - 1;
+    g->srv = dup(rv, (size_t)num_borders * sizeof(double));
+    double r = rv[num_borders - 1];
+    double e[6] = {-r, -r, -r, r, r, r};
+    memcpy(g->ext, e, sizeof e);
+    g->eps = 1e-12 * sqrt(3.) * 2. * r;
+    g->numCells = g->snr;
+    c->hasGrid = 1;
+    return SKGPU_OK;
+}
+
 int or_upload_grid_tetra(or_ctx* c, int32_t num_vertices, const double* vertices, int32_t num_tetra,
                          const int32_t* tetra_vertices, const double* face_normals, const int32_t* face_ntetra,
                          const int32_t* face_nface, const double* extent, double eps)
@@ -324,6 +347,8 @@ typedef struct
     int i, j, k;  /* cartesian */
     int node;     /* octree */
     int mr, ef;   /* voronoi / tetra */
+    double sq, sp; /* sphere1d: projection of the position on the direction, impact parameter */
+    int simin, sinw;
 } Gen;
 
 static int box_contains(const double* b, double x, double y, double z)
@@ -773,6 +798,94 @@ static int tet_next(const Grid* g, Gen* s)
     return 0;
 }
 
+/* NR::locate on an ascending array of n entries (SKIRT/utils/NR.hpp:168-173): -1 below xv[0], n-2 at xv[n-1] */
+static int nr_locate(const double* xv, int n, double x)
+{
+    if (x == xv[n - 1]) return n - 2;
+    int jl = -1, ju = n;
+    while (ju - jl > 1)
+    {
+        int jm = (ju + jl) >> 1;
+        if (x < xv[jm]) ju = jm; else jl = jm;
+    }
+    return jl;
+}
+
+/* Sphere1DSpatialGrid::MySegmentGenerator::next (Sphere1DSpatialGrid.cpp): radial shells crossed
+   inwards down to the impact parameter's shell, then outwards; the position is not advanced (the
+   generator tracks q, the position's projection on the direction) */
+static int sph_next(const Grid* g, Gen* s)
+{
+    if (s->state == OUTSIDE) return 0;
+    const double* rv = g->srv;
+    int nr = g->snr;
+    if (s->state == UNKNOWN)
+    {
+        double rmax = rv[nr], rmin = rv[0];
+        double r = sqrt(s->rx * s->rx + s->ry * s->ry + s->rz * s->rz);
+        s->sq = s->rx * s->kx + s->ry * s->ky + s->rz * s->kz;
+        s->sp = sqrt((r - s->sq) * (r + s->sq));
+        if (r > rmax)
+        {
+            if (s->sq > 0. || s->sp > rmax)
+            {
+                s->state = OUTSIDE;
+                return 0;
+            }
+            double qmax = -sqrt((rmax - s->sp) * (rmax + s->sp));
+            s->m = -1;
+            s->ds = qmax - s->sq;
+            s->i = nr - 1;
+            s->sq = qmax;
+            s->state = INSIDE;
+            s->simin = nr_locate(rv, nr + 1, s->sp);
+            s->sinw = s->i > s->simin;
+            return 1;
+        }
+        else if (r < rmin)
+        {
+            double qmin = sqrt((rmin - s->sp) * (rmin + s->sp));
+            s->m = -1;
+            s->ds = qmin - s->sq;
+            s->i = 0;
+            s->sq = qmin;
+            s->state = INSIDE;
+            s->sinw = 0;
+            return 1;
+        }
+        else
+        {
+            s->i = locate_clip(rv, nr + 1, r);
+            s->state = INSIDE;
+            s->sinw = 0;
+            if (s->sq < 0.)
+            {
+                s->simin = nr_locate(rv, nr + 1, s->sp);
+                if (s->i > s->simin) s->sinw = 1;
+            }
+        }
+    }
+    if (s->sinw)
+    {
+        double rN = rv[s->i];
+        double qN = -sqrt((rN - s->sp) * (rN + s->sp));
+        s->m = s->i;
+        s->ds = qN - s->sq;
+        s->i--;
+        s->sq = qN;
+        if (s->i <= s->simin) s->sinw = 0;
+        return 1;
+    }
+    double rN = rv[s->i + 1];
+    double qN = sqrt((rN - s->sp) * (rN + s->sp));
+    s->m = s->i;
+    s->ds = qN - s->sq;
+    s->i++;
+    s->sq = qN;
+    if (s->i >= nr) s->state = OUTSIDE;
+    return 1;
+}
+
 static int gen_next(const Grid* g, Gen* s)
 {
     switch (g->kind)
@@ -781,6 +894,7 @@ static int gen_next(const Grid* g, Gen* s)
         case SKGPU_GRID_OCTREE: return tree_next(g, s);
         case SKGPU_GRID_VORONOI: return vor_next(g, s);
         case SKGPU_GRID_TETRA: return tet_next(g, s);
+        case SKGPU_GRID_SPHERE1D: return sph_next(g, s);
     }
     return 0;
 }

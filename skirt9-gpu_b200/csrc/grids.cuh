@@ -68,6 +68,9 @@ struct GridDev
     const int* teBlkBegin;
     const int* teBlkTets;
     const struct TetRec* teRec;  // FP32 walker: one cache-line record per tetrahedron
+    // 1D spherical: sNr radial cells between the sNr + 1 ascending border radii sRv
+    const double* sRv;
+    int sNr;
     const int* teBlkRep;         // teGridN^3: a tetrahedron overlapping each block (start of the walking locate)
 };
 
@@ -694,6 +697,111 @@ struct TetraExact : GenBase
         }
         state = GS_OUTSIDE;
         return false;
+    }
+};
+
+// ---------------------------------------------------------------------------------------------
+// 1D spherical grid (Sphere1DSpatialGrid::MySegmentGenerator::next, Sphere1DSpatialGrid.cpp):
+// the radial shells are crossed inwards down to the shell of the impact parameter p, then
+// outwards; each exit is at q_N = -/+ sqrt((r_N - p)(r_N + p)) along the ray, q measured from the
+// projection of the origin. The position is not advanced: the generator tracks q.
+// ---------------------------------------------------------------------------------------------
+// NR::locate (SKIRT/utils/NR.hpp:168-173): -1 below xv[0], n - 2 at xv[n - 1]
+SKG_D int locateNR(const double* xv, int n, double x)
+{
+    if (x == xv[n - 1]) return n - 2;
+    int jl = -1, ju = n;
+    while (ju - jl > 1)
+    {
+        int jm = (ju + jl) >> 1;
+        if (x < xv[jm])
+            ju = jm;
+        else
+            jl = jm;
+    }
+    return jl;
+}
+
+struct Sphere1DExact : GenBase
+{
+    static constexpr int kMinBlocks = 4;
+    static constexpr int kRefillMin = 16;  // waiting lanes before a warp takes new tasks
+    double q, p;
+    int i, imin;
+    bool inwards;
+
+    SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz, int = -1)
+    {
+        startRay(x, y, z, ux, uy, uz);
+    }
+
+    SKG_D bool next(const GridDev& g)
+    {
+        if (state == GS_OUTSIDE) return false;
+        const double* rv = g.sRv;
+        const int nr = g.sNr;
+        if (state == GS_UNKNOWN)
+        {
+            double rmax = rv[nr], rmin = rv[0];
+            double r = sqrt(xadd(xadd(xmul(rx, rx), xmul(ry, ry)), xmul(rz, rz)));
+            q = xadd(xadd(xmul(rx, kx), xmul(ry, ky)), xmul(rz, kz));
+            p = sqrt(xmul(xsub(r, q), xadd(r, q)));
+            if (r > rmax)
+            {
+                if (q > 0. || p > rmax)
+                {
+                    state = GS_OUTSIDE;
+                    return false;
+                }
+                double qmax = -sqrt(xmul(xsub(rmax, p), xadd(rmax, p)));
+                m = -1;
+                ds = xsub(qmax, q);
+                i = nr - 1;
+                q = qmax;
+                state = GS_INSIDE;
+                imin = locateNR(rv, nr + 1, p);
+                inwards = i > imin;
+                return true;
+            }
+            else if (r < rmin)
+            {
+                double qmin = sqrt(xmul(xsub(rmin, p), xadd(rmin, p)));
+                m = -1;
+                ds = xsub(qmin, q);
+                i = 0;
+                q = qmin;
+                state = GS_INSIDE;
+                inwards = false;
+                return true;
+            }
+            i = locateClip(rv, nr + 1, r);
+            state = GS_INSIDE;
+            inwards = false;
+            if (q < 0.)
+            {
+                imin = locateNR(rv, nr + 1, p);
+                if (i > imin) inwards = true;
+            }
+        }
+        if (inwards)
+        {
+            double rN = rv[i];
+            double qN = -sqrt(xmul(xsub(rN, p), xadd(rN, p)));
+            m = i;
+            ds = xsub(qN, q);
+            i--;
+            q = qN;
+            if (i <= imin) inwards = false;
+            return true;
+        }
+        double rN = rv[i + 1];
+        double qN = sqrt(xmul(xsub(rN, p), xadd(rN, p)));
+        m = i;
+        ds = xsub(qN, q);
+        i++;
+        q = qN;
+        if (i >= nr) state = GS_OUTSIDE;
+        return true;
     }
 };
 

@@ -636,4 +636,14 @@ struct TetraPlane32 : GenBase
     }
 };
 
+// ---------------------------------------------------------------------------------------------
+// 1D spherical grid, production: the reference-order FP64 shell crossings (a handful of square
+// roots per ray over a border table that stays in L1) with FP32 accumulators like the other
+// production walkers.
+// ---------------------------------------------------------------------------------------------
+struct Sphere1DFast : Sphere1DExact
+{
+    using Acc = float;
+};
+
 }  // namespace skg

@@ -598,6 +598,29 @@ int skgpu_upload_grid_voronoi(skgpu_ctx* ctx, int32_t num_sites, const double* s
     return SKGPU_OK;
 }
 
+int skgpu_upload_grid_sphere1d(skgpu_ctx* ctx, int32_t num_borders, const double* rv)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (num_borders < 2 || !rv || !(rv[0] >= 0.)) return fail(ctx, SKGPU_ERR_ARG, "sphere1d: need >= 2 borders from r >= 0");
+    if (!finiteAll(rv, num_borders)) return fail(ctx, SKGPU_ERR_ARG, "sphere1d: non-finite border");
+    for (int i = 1; i < num_borders; ++i)
+        if (!(rv[i] > rv[i - 1])) return fail(ctx, SKGPU_ERR_ARG, "sphere1d: borders must ascend");
+    CK(cudaSetDevice(ctx->device));
+    freeGrid(ctx);
+    GridDev& g = ctx->g;
+    g.kind = SKGPU_GRID_SPHERE1D;
+    double r = rv[num_borders - 1];
+    double e[6] = {-r, -r, -r, r, r, r};
+    for (int q = 0; q < 6; ++q) g.ext[q] = e[q];
+    g.eps = 1e-12 * std::sqrt(3.) * 2. * r;
+    g.sNr = num_borders - 1;
+    g.numCells = g.sNr;
+    int rc;
+    if ((rc = gridUpload(ctx, &g.sRv, rv, static_cast<size_t>(num_borders)))) return rc;
+    ctx->hasGrid = true;
+    return SKGPU_OK;
+}
+
 int skgpu_upload_grid_tetra(skgpu_ctx* ctx, int32_t num_vertices, const double* vertices, int32_t num_tetra,
                             const int32_t* tetra_vertices, const double* face_normals, const int32_t* face_ntetra,
                             const int32_t* face_nface, const double* extent, double eps)

@@ -56,6 +56,8 @@ class Scene:
             be.upload_grid_voronoi(g["sites"], g["nb_begin"], g["nb_index"], g["extent"], g["eps"])
         elif k == abi.GRID_TETRA:
             be.upload_grid_tetra(g["vertices"], g["tetra"], g["normals"], g["ntetra"], g["nface"], g["extent"], g["eps"])
+        elif k == abi.GRID_SPHERE1D:
+            be.upload_grid_sphere1d(g["rv"])
         else:
             raise ValueError(f"unknown grid kind {k}")
         if self.density is not None:
@@ -227,6 +229,8 @@ class Scene:
             sc.grid = dict(kind=abi.GRID_TETRA, vertices=L("tet_vertices"), tetra=L("tet_tetra"),
                            normals=L("tet_normals"), ntetra=L("tet_ntetra"), nface=L("tet_nface"), extent=ext,
                            eps=float(meta["eps"]))
+        elif kind == "sphere1d":
+            sc.grid = dict(kind=abi.GRID_SPHERE1D, rv=L("grid_rv"), extent=ext)
         else:
             raise ValueError(f"unsupported grid in export: {kind}")
         sc.density = L("medium_density")[:, 0].copy()

@@ -58,6 +58,21 @@ def vertex_file_text(points_m):
     return "\n".join(lines) + "\n"
 
 
+def sphere1d_grid(rmin_pc, rmax_pc, nbins, mesh="LinMesh"):
+    """Sphere1DSpatialGrid between rmin and rmax with nbins radial bins."""
+    return (f'<Sphere1DSpatialGrid minRadius="{rmin_pc} pc" maxRadius="{rmax_pc} pc">'
+            f'<meshRadial type="Mesh"><{mesh} numBins="{nbins}"/></meshRadial></Sphere1DSpatialGrid>')
+
+
+def shell_sphere1d(num_packets=1e5, nbins=24, npix=64, stats=True, rmin_pc=0.05):
+    """The dust shell of shell_cartesian on a Sphere1DSpatialGrid (rmin to 1 pc, nbins radial bins;
+    inside rmin no cell), one frame at 30 degrees with statistics plus one SED instrument."""
+    mix = mean_list_mix([0.5, 0.6], [1, 1], [0.5, 0.5], [0.6, 0.6])
+    return simulation("OligoExtinctionOnly", num_packets, point_source(),
+                      shell_medium(0.1, 1, 2, 2, mix), sphere1d_grid(rmin_pc, 1, nbins),
+                      frame_instrument("i30", 30, 2, "pc", npix, stats) + sed_instrument("sed", 30, stats))
+
+
 def shell_medium(rmin_pc, rmax_pc, exponent, tau_x, mix):
     return (f'<GeometricMedium velocityMagnitude="0 km/s" magneticFieldStrength="0 uG">'
             f'<geometry type="Geometry"><ShellGeometry minRadius="{rmin_pc} pc" maxRadius="{rmax_pc} pc" '

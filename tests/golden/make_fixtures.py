@@ -114,6 +114,7 @@ def main():
     # Voronoi and tetrahedral meshes built by the reference (voro++ / TetGen) from disk-sampled sites
     path_fixture("voronoi", ski.disk_probe(ski.voronoi_grid(4, "pc", 300)), random_rays(rng, 300, 4 * PC))
     path_fixture("tetra", ski.disk_probe(ski.tetra_grid(4, "pc", 300)), random_rays(rng, 300, 4 * PC))
+    sphere1d_fixture(rng)
 
     # dust shell, 16^3 grid, 64^2 frame + SED: scene export + reference statistics (2e5 packets)
     npp = 200000
@@ -147,6 +148,42 @@ def main():
     explicit_fixture(mjysr_per_w, npp)
 
 
+def sphere1d_fixture(rng=None):
+    """Sphere1DSpatialGrid (the dust shell, 24 radial bins between 0.05 and 1 pc, no cell inside
+    0.05 pc): scene export and path fixture with random rays plus radial and tangent rays (exact
+    shell borders, rays through the centre, rays starting inside and outside)."""
+    rng = rng if rng is not None else np.random.default_rng(20260102)
+    rays = random_rays(rng, 300, 1.2 * PC)
+    extra = []
+    for r0 in (0.0, 0.25, 0.5, 1.0 + 1e-9):
+        extra.append(np.r_[np.array([r0, 0.0, 0.0]) * PC, [1.0, 0.0, 0.0]])
+        extra.append(np.r_[np.array([r0, 0.0, 0.0]) * PC, [-1.0, 0.0, 0.0]])
+    for b in (0.1, 0.5, 1.0 / 24 * 7):
+        extra.append(np.r_[np.array([-2.0, b, 0.0]) * PC, [1.0, 0.0, 0.0]])
+    rays = np.vstack([rays, np.array(extra)])
+    path_fixture("sphere1d", ski.shell_sphere1d(1e4, nbins=24, npix=32), rays)
+    # reference statistics of the same scene: a single-threaded 2e5-packet run; its stats files are
+    # scaled by the run's own c, recovered from the total image (MJy/sr per raw W from the SED's
+    # Jy per raw W of the shell_c16 run, same distance, and this frame's pixel)
+    npp = 200000
+    path = os.path.join(OUT, "paths_sphere1d.npz")
+    data = dict(np.load(path))
+    meta = __import__("skgpu").Scene.read_export(data)[0]
+    pix = float(meta["instr0_xpsiz"]) / float(meta["instr0_distance"])
+    mjysr_per_w = float(np.load(os.path.join(OUT, "shell_c16.npz"))["ref_jy_per_w"]) * 1e-6 / (pix * pix)
+    with tempfile.TemporaryDirectory() as tmp:
+        with open(os.path.join(tmp, "s1.ski"), "w") as f:
+            f.write(ski.shell_sphere1d(npp, nbins=24, npix=32))
+        subprocess.run([os.path.join(BIN, "skirt"), "-t", "1", "s1.ski"], cwd=tmp, check=True,
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        st = np.array([fits.read(os.path.join(tmp, f"s1_i30_stats{k}.fits"))[0][0] for k in range(5)])
+        ss = np.loadtxt(os.path.join(tmp, "s1_sed_sedstats.dat"))
+        total = fits.read(os.path.join(tmp, "s1_i30_total.fits"))[0][0]
+    c = st[1].sum() / (total / mjysr_per_w).sum()
+    data.update(ref_npp=npp, ref_frame_w=np.array([st[0], st[1] / c, st[2] / c ** 2]), ref_sedstats=ss[1:])
+    np.savez_compressed(path, **data)
+
+
 def explicit_fixture(mjysr_per_w, npp):
     """The 16^3 shell with explicit absorption (PhotonPacketOptions::explicitAbsorption), forced and
     free propagation: reference frame and SED statistics of single-threaded runs of npp packets. Each
@@ -170,7 +207,9 @@ def explicit_fixture(mjysr_per_w, npp):
 
 
 if __name__ == "__main__":
-    if sys.argv[1:] == ["explicit"]:
+    if sys.argv[1:] == ["sphere1d"]:
+        sphere1d_fixture()
+    elif sys.argv[1:] == ["explicit"]:
         z = np.load(os.path.join(OUT, "shell_c16.npz"))
         meta = __import__("skgpu").Scene.read_export(z)[0]
         pix = float(meta["instr0_xpsiz"]) / float(meta["instr0_distance"])

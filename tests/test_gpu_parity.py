@@ -65,7 +65,7 @@ def test_gpu_free_propagation_matches_oracle(golden, gpu_backend, oracle_backend
     assert_close_runs(rg, ro)
 
 
-@pytest.mark.parametrize("name", ["octree", "voronoi", "tetra", "cartesian_selftest"])
+@pytest.mark.parametrize("name", ["octree", "voronoi", "tetra", "cartesian_selftest", "sphere1d"])
 def test_gpu_lifecycle_matches_oracle_grids(golden, gpu_backend, oracle_backend, name):
     sc = Scene.from_export(golden(f"paths_{name}.npz"))
     sc.instruments[0]["stats"] = 1
@@ -235,3 +235,23 @@ def test_gpu_fp32_octree_lifecycle_close_to_fp64(gpu_backend):
     assert r32.rf.sum() == pytest.approx(r64.rf.sum(), rel=2e-3)
     lit = r64.rf > 0
     assert np.median(np.abs(r32.rf[lit] / r64.rf[lit] - 1)) < 1e-3
+
+
+def test_gpu_sphere1d_lifecycle_matches_reference_statistics(golden, gpu_backend):
+    """The dust shell on a Sphere1DSpatialGrid, both traversal precisions: frame and SED against
+    the reference's own run of the same scene (z-scores)."""
+    z = golden("paths_sphere1d.npz")
+    sc = Scene.from_export(z)
+    sc.instruments[0]["stats"] = 1
+    sc.instruments[1]["stats"] = 1
+    sc.upload(gpu_backend)
+    n = int(z["ref_npp"])
+    for precision in (abi.PREC_FP64_EXACT, abi.PREC_FP32):
+        res = sc.run(gpu_backend, n, seed=29, precision=precision)
+        st = res[0]["stats"][:, 0]
+        ref = z["ref_frame_w"]
+        zs = zscores(st[1], st[2], n, ref[1], ref[2], n)
+        assert abs(zs.mean()) < 0.1 and 0.85 < zs.std() < 1.15
+        sst = res[1]["stats"][:, 0]
+        rs = z["ref_sedstats"]
+        assert abs(zscores(sst[1:2], sst[2:3], n, rs[1:2], rs[2:3], n)[0]) < 4

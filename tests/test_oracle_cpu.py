@@ -122,3 +122,23 @@ def test_oracle_explicit_absorption_matches_reference_statistics(golden, oracle_
     rs = e[f"ref_{tag}_sedstats"]
     zsed = zscores(sst[1:2], sst[2:3], n, rs[1:2], rs[2:3], n)
     assert abs(zsed[0]) < 4
+
+
+def test_oracle_sphere1d_lifecycle_matches_reference_statistics(golden, oracle_backend):
+    """The dust shell on a Sphere1DSpatialGrid: the oracle's frame and SED against the reference's
+    own run of the same scene (z-scores)."""
+    z = golden("paths_sphere1d.npz")
+    sc = Scene.from_export(z)
+    sc.instruments[0]["stats"] = 1
+    sc.instruments[1]["stats"] = 1
+    sc.upload(oracle_backend)
+    n = int(z["ref_npp"])
+    res = sc.run(oracle_backend, n, seed=23)
+    st = res[0]["stats"][:, 0]
+    ref = z["ref_frame_w"]
+    zs = zscores(st[1], st[2], n, ref[1], ref[2], n)
+    assert len(zs) > 500
+    assert abs(zs.mean()) < 0.1 and 0.85 < zs.std() < 1.15
+    sst = res[1]["stats"][:, 0]
+    rs = z["ref_sedstats"]
+    assert abs(zscores(sst[1:2], sst[2:3], n, rs[1:2], rs[2:3], n)[0]) < 4
