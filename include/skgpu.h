@@ -41,6 +41,7 @@ extern "C" {
 #define SKGPU_GRID_VORONOI 2
 #define SKGPU_GRID_TETRA 3
 #define SKGPU_GRID_SPHERE1D 4
+#define SKGPU_GRID_CYLINDER2D 5
 
 /* traversal precision (path kernels and life cycle) */
 #define SKGPU_PREC_FP64_EXACT 0 /* FP64 with the reference generators' operation order, no FMA contraction */
@@ -154,6 +155,11 @@ int skgpu_upload_grid_voronoi(skgpu_ctx* ctx, int32_t num_sites, const double* s
  * radial cells (Sphere1DSpatialGrid::radialBorderPositions, Sphere1DSpatialGrid.hpp:101); cell i is
  * the shell r_i <= r < r_{i+1} around the origin. */
 int skgpu_upload_grid_sphere1d(skgpu_ctx* ctx, int32_t num_borders, const double* radial_borders);
+/* Cylinder2DSpatialGrid: ascending radial borders R_0 >= 0 .. R_NR and vertical borders z_0 .. z_Nz
+ * (its _Rv and _zv); cell index k + Nz * i for radial bin i and vertical bin k
+ * (Cylinder2DSpatialGrid.cpp:433-437). */
+int skgpu_upload_grid_cylinder2d(skgpu_ctx* ctx, int32_t num_radial_borders, const double* radial_borders,
+                                 int32_t num_z_borders, const double* z_borders);
 /* TetraMeshSpatialGrid: vertices, per tetrahedron its 4 vertex indices, and per face the outward
  * normal, the neighbouring tetrahedron (-1 on the hull) and its face index
  * (TetraMeshSpatialGrid.hpp:107-133). */

@@ -66,6 +66,7 @@
 #include "SpatialGrid.hpp"
 #include "SpatialGridPath.hpp"
 #include "System.hpp"
+#include "Cylinder2DSpatialGrid.hpp"
 #include "Sphere1DSpatialGrid.hpp"
 #include "TetraMeshSpatialGrid.hpp"
 #include "TreeNode.hpp"
@@ -174,6 +175,14 @@ namespace
             writeVec(out + "/grid_xb.npy", xb);
             writeVec(out + "/grid_yb.npy", yb);
             writeVec(out + "/grid_zb.npy", zb);
+            return;
+        }
+        if (auto g = dynamic_cast<Cylinder2DSpatialGrid*>(grid))
+        {
+            meta.kv("grid", "cylinder2d");
+            std::vector<double> rv(begin(g->_Rv), end(g->_Rv)), zv(begin(g->_zv), end(g->_zv));
+            writeVec(out + "/grid_rv.npy", rv);
+            writeVec(out + "/grid_zv.npy", zv);
             return;
         }
         if (auto g = dynamic_cast<Sphere1DSpatialGrid*>(grid))

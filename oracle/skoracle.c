@@ -116,6 +116,9 @@ typedef struct
     /* sphere1d */
     double* srv;
     int snr;
+    /* cylinder2d */
+    double *crv, *czv;
+    int cnr, cnz;
 } Grid;
 
 typedef struct
@@ -171,6 +174,7 @@ static void free_grid(Grid* g)
     free(g->vs); free(g->vnbb); free(g->vnb);
     free(g->tev); free(g->ten); free(g->tebox); free(g->tet); free(g->tent); free(g->tenf);
     free(g->srv);
+    free(g->crv); free(g->czv);
     memset(g, 0, sizeof *g);
 }
 
@@ -298,6 +302,29 @@ int or_upload_grid_sphere1d(or_ctx* c, int32_t num_borders, const double* rv)
     return SKGPU_OK;
 }
 
+int or_upload_grid_cylinder2d(or_ctx* c, int32_t nrb, const double* rv, int32_t nzb, const double* zv)
+{
+    if (nrb < 2 || nzb < 2 || !rv || !zv || !(rv[0] >= 0.)) return fail(c, SKGPU_ERR_ARG, "cylinder2d: bad borders");
+    for (int i = 1; i < nrb; ++i)
+        if (!(rv[i] > rv[i - 1])) return fail(c, SKGPU_ERR_ARG, "cylinder2d: radial borders must ascend");
+    for (int i = 1; i < nzb; ++i)
+        if (!(zv[i] > zv[i - 1])) return fail(c, SKGPU_ERR_ARG, "cylinder2d: z borders must ascend");
+    free_grid(&c->g);
+    Grid* g = &c->g;
+    g->kind = SKGPU_GRID_CYLINDER2D;
+    g->cnr = nrb - 1;
+    g->cnz = nzb - 1;
+    g->crv = dup(rv, (size_t)nrb * sizeof(double));
+    g->czv = dup(zv, (size_t)nzb * sizeof(double));
+    double r = rv[nrb - 1];
+    double e[6] = {-r, -r, zv[0], r, r, zv[nzb - 1]};
+    memcpy(g->ext, e, sizeof e);
+    g->eps = 1e-12 * sqrt(2. * (2. * r) * (2. * r) + (zv[nzb - 1] - zv[0]) * (zv[nzb - 1] - zv[0]));
+    g->numCells = g->cnr * g->cnz;
+    c->hasGrid = 1;
+    return SKGPU_OK;
+}
+
 int or_upload_grid_tetra(or_ctx* c, int32_t num_vertices, const double* vertices, int32_t num_tetra,
                          const int32_t* tetra_vertices, const double* face_normals, const int32_t* face_ntetra,
                          const int32_t* face_nface, const double* extent, double eps)
@@ -349,6 +376,8 @@ typedef struct
     int mr, ef;   /* voronoi / tetra */
     double sq, sp; /* sphere1d: projection of the position on the direction, impact parameter */
     int simin, sinw;
+    double cR, cz, ckq, ckz, cp, cq; /* cylinder2d: meridional position and direction */
+    int cimin, cphase;
 } Gen;
 
 static int box_contains(const double* b, double x, double y, double z)
@@ -886,6 +915,145 @@ static int sph_next(const Grid* g, Gen* s)
     return 1;
 }
 
+/* Cylinder2DSpatialGrid::MySegmentGenerator::moveInside (Cylinder2DSpatialGrid.cpp:124-198) */
+static int cyl_move_inside(const Grid* g, Gen* s)
+{
+    const double* Rv = g->crv;
+    const double* zv = g->czv;
+    int NR = g->cnr, Nz = g->cnz;
+    s->cR = sqrt(s->rx * s->rx + s->ry * s->ry);
+    s->cz = s->rz;
+    s->ckq = sqrt(s->kx * s->kx + s->ky * s->ky);
+    s->ckz = s->kz;
+    if (s->ckq == 0.0) s->ckq = 1e-20;
+    if (s->ckz == 0.0) s->ckz = 1e-20;
+    s->cq = (s->rx * s->kx + s->ry * s->ky) / s->ckq;
+    double pp = (s->cR - s->cq) * (s->cR + s->cq);
+    s->cp = sqrt(0. < pp ? pp : 0.);  /* std::max(0., x) */
+    double Rmax = Rv[NR], zmin = zv[0], zmax = zv[Nz];
+    s->m = -1;
+    s->ds = 0.;
+    s->state = OUTSIDE;
+    double cumds = 0.;
+    if (s->cR >= Rmax)
+    {
+        if (s->cq > 0.0 || s->cp > Rmax) return 0;
+        double qmin = -sqrt((Rmax - s->cp) * (Rmax + s->cp));
+        double ds = (qmin - s->cq) / s->ckq;
+        s->cq = qmin;
+        s->cR = Rmax - 1e-8 * (Rv[NR] - Rv[NR - 1]);
+        s->cz += s->ckz * ds;
+        cumds += ds;
+    }
+    if (s->cz < zmin)
+    {
+        if (s->ckz <= 0.0) return 0;
+        double ds = (zmin - s->cz) / s->ckz;
+        s->cq += s->ckq * ds;
+        s->cR = sqrt(s->cp * s->cp + s->cq * s->cq);
+        s->cz = zmin + 1e-8 * (zv[1] - zv[0]);
+        cumds += ds;
+    }
+    else if (s->cz > zmax)
+    {
+        if (s->ckz >= 0.0) return 0;
+        double ds = (zmax - s->cz) / s->ckz;
+        s->cq += s->ckq * ds;
+        s->cR = sqrt(s->cp * s->cp + s->cq * s->cq);
+        s->cz = zmax - 1e-8 * (zv[Nz] - zv[Nz - 1]);
+        cumds += ds;
+    }
+    if (isinf(s->cR) || isnan(s->cR) || isinf(s->cz) || isnan(s->cz)) return 0;
+    if (s->cR >= Rmax || s->cz <= zmin || s->cz >= zmax) return 0;
+    s->m = -1;
+    s->ds = cumds;
+    s->state = INSIDE;
+    return 1;
+}
+
+enum { CYL_UP_IN = 0, CYL_UP_OUT = 1, CYL_DOWN_IN = 2, CYL_DOWN_OUT = 3 };
+
+/* Cylinder2DSpatialGrid::MySegmentGenerator::next (Cylinder2DSpatialGrid.cpp:200-391) */
+static int cyl_next(const Grid* g, Gen* s)
+{
+    const double* Rv = g->crv;
+    const double* zv = g->czv;
+    int NR = g->cnr, Nz = g->cnz;
+    if (s->state == OUTSIDE) return 0;
+    if (s->state == UNKNOWN)
+    {
+        if (!cyl_move_inside(g, s)) return 0;
+        s->i = nr_locate(Rv, NR + 1, s->cR);
+        s->k = locate_clip(zv, Nz + 1, s->cz);
+        if (s->ckz >= 0.)
+        {
+            s->cphase = CYL_UP_OUT;
+            if (s->cq < 0.)
+            {
+                s->cimin = nr_locate(Rv, NR + 1, s->cp);
+                if (s->i > s->cimin) s->cphase = CYL_UP_IN;
+            }
+        }
+        else
+        {
+            s->cphase = CYL_DOWN_OUT;
+            if (s->cq < 0.)
+            {
+                s->cimin = nr_locate(Rv, NR + 1, s->cp);
+                if (s->i > s->cimin) s->cphase = CYL_DOWN_IN;
+            }
+        }
+        if (s->ds > 0.) return 1;
+    }
+    int up = s->cphase == CYL_UP_IN || s->cphase == CYL_UP_OUT;
+    int in = s->cphase == CYL_UP_IN || s->cphase == CYL_DOWN_IN;
+    double RN = in ? Rv[s->i] : Rv[s->i + 1];
+    double qN = in ? -sqrt((RN - s->cp) * (RN + s->cp)) : sqrt((RN - s->cp) * (RN + s->cp));
+    double zN = up ? zv[s->k + 1] : zv[s->k];
+    int m = s->i < 0 ? -1 : s->k + Nz * s->i;  /* Cylinder2DSpatialGrid::index */
+    double dsq = (qN - s->cq) / s->ckq;
+    double dsz = (zN - s->cz) / s->ckz;
+    if (dsq < dsz)
+    {
+        double ds = dsq;
+        s->m = m;
+        s->ds = ds;
+        if (in)
+        {
+            s->i--;
+            s->cq = qN;
+            s->cz += s->ckz * ds;
+            if (s->i <= s->cimin) s->cphase = up ? CYL_UP_OUT : CYL_DOWN_OUT;
+        }
+        else
+        {
+            s->i++;
+            if (s->i >= NR)
+                s->state = OUTSIDE;
+            else
+            {
+                s->cq = qN;
+                s->cz += s->ckz * ds;
+            }
+        }
+    }
+    else
+    {
+        double ds = dsz;
+        s->m = m;
+        s->ds = ds;
+        if (up) s->k++; else s->k--;
+        if (up ? s->k >= Nz : s->k < 0)
+            s->state = OUTSIDE;
+        else
+        {
+            s->cq += s->ckq * ds;
+            s->cz = zN;
+        }
+    }
+    return 1;
+}
+
 static int gen_next(const Grid* g, Gen* s)
 {
     switch (g->kind)
@@ -895,6 +1063,7 @@ static int gen_next(const Grid* g, Gen* s)
         case SKGPU_GRID_VORONOI: return vor_next(g, s);
         case SKGPU_GRID_TETRA: return tet_next(g, s);
         case SKGPU_GRID_SPHERE1D: return sph_next(g, s);
+        case SKGPU_GRID_CYLINDER2D: return cyl_next(g, s);
     }
     return 0;
 }

@@ -71,6 +71,10 @@ struct GridDev
     // 1D spherical: sNr radial cells between the sNr + 1 ascending border radii sRv
     const double* sRv;
     int sNr;
+    // 2D cylindrical: cNR radial x cNz vertical cells between the borders cRv and czv
+    const double* cRv;
+    const double* czv;
+    int cNR, cNz;
     const int* teBlkRep;         // teGridN^3: a tetrahedron overlapping each block (start of the walking locate)
 };
 
@@ -801,6 +805,149 @@ struct Sphere1DExact : GenBase
         i++;
         q = qN;
         if (i >= nr) state = GS_OUTSIDE;
+        return true;
+    }
+};
+
+// ---------------------------------------------------------------------------------------------
+// 2D cylindrical grid (Cylinder2DSpatialGrid::MySegmentGenerator, Cylinder2DSpatialGrid.cpp:110-391):
+// the ray in the meridional plane, with q its projection on the horizontal direction and p the
+// horizontal impact parameter; each step exits either through the next cylinder (inwards down to the
+// impact parameter's shell, then outwards) or through the next horizontal plane, whichever is
+// nearer. Entry from outside by the generator's own moveInside (small inward nudges at the walls).
+// ---------------------------------------------------------------------------------------------
+struct Cylinder2DExact : GenBase
+{
+    static constexpr int kMinBlocks = 4;
+    static constexpr int kRefillMin = 16;  // waiting lanes before a warp takes new tasks
+    double cR, cz, kq, kzc, p, q;
+    int i, k, imin;
+    bool up, in;
+
+    SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz, int = -1)
+    {
+        startRay(x, y, z, ux, uy, uz);
+        imin = -1;
+    }
+
+    SKG_D bool moveInsideCyl(const GridDev& g)
+    {
+        const double* Rv = g.cRv;
+        const double* zv = g.czv;
+        const int NR = g.cNR, Nz = g.cNz;
+        cR = sqrt(xadd(xmul(rx, rx), xmul(ry, ry)));
+        cz = rz;
+        kq = sqrt(xadd(xmul(kx, kx), xmul(ky, ky)));
+        kzc = kz;
+        if (kq == 0.0) kq = 1e-20;
+        if (kzc == 0.0) kzc = 1e-20;
+        q = xadd(xmul(rx, kx), xmul(ry, ky)) / kq;
+        double pp = xmul(xsub(cR, q), xadd(cR, q));
+        p = sqrt(0. < pp ? pp : 0.);  // std::max(0., x)
+        double Rmax = Rv[NR], zmin = zv[0], zmax = zv[Nz];
+        m = -1;
+        ds = 0.;
+        state = GS_OUTSIDE;
+        double cumds = 0.;
+        if (cR >= Rmax)
+        {
+            if (q > 0.0 || p > Rmax) return false;
+            double qmin = -sqrt(xmul(xsub(Rmax, p), xadd(Rmax, p)));
+            double d = xsub(qmin, q) / kq;
+            q = qmin;
+            cR = xsub(Rmax, xmul(1e-8, xsub(Rv[NR], Rv[NR - 1])));
+            cz = xadd(cz, xmul(kzc, d));
+            cumds = xadd(cumds, d);
+        }
+        if (cz < zmin)
+        {
+            if (kzc <= 0.0) return false;
+            double d = xsub(zmin, cz) / kzc;
+            q = xadd(q, xmul(kq, d));
+            cR = sqrt(xadd(xmul(p, p), xmul(q, q)));
+            cz = xadd(zmin, xmul(1e-8, xsub(zv[1], zv[0])));
+            cumds = xadd(cumds, d);
+        }
+        else if (cz > zmax)
+        {
+            if (kzc >= 0.0) return false;
+            double d = xsub(zmax, cz) / kzc;
+            q = xadd(q, xmul(kq, d));
+            cR = sqrt(xadd(xmul(p, p), xmul(q, q)));
+            cz = xsub(zmax, xmul(1e-8, xsub(zv[Nz], zv[Nz - 1])));
+            cumds = xadd(cumds, d);
+        }
+        if (isinf(cR) || isnan(cR) || isinf(cz) || isnan(cz)) return false;
+        if (cR >= Rmax || cz <= zmin || cz >= zmax) return false;
+        m = -1;
+        ds = cumds;
+        state = GS_INSIDE;
+        return true;
+    }
+
+    SKG_D bool next(const GridDev& g)
+    {
+        if (state == GS_OUTSIDE) return false;
+        const double* Rv = g.cRv;
+        const double* zv = g.czv;
+        const int NR = g.cNR, Nz = g.cNz;
+        if (state == GS_UNKNOWN)
+        {
+            if (!moveInsideCyl(g)) return false;
+            i = locateNR(Rv, NR + 1, cR);
+            k = locateClip(zv, Nz + 1, cz);
+            up = kzc >= 0.;
+            in = false;
+            if (q < 0.)
+            {
+                imin = locateNR(Rv, NR + 1, p);
+                if (i > imin) in = true;
+            }
+            if (ds > 0.) return true;
+        }
+        double RN = in ? Rv[i] : Rv[i + 1];
+        double w = sqrt(xmul(xsub(RN, p), xadd(RN, p)));
+        double qN = in ? -w : w;
+        double zN = up ? zv[k + 1] : zv[k];
+        int mc = i < 0 ? -1 : k + Nz * i;  // Cylinder2DSpatialGrid::index
+        double dsq = xsub(qN, q) / kq;
+        double dsz = xsub(zN, cz) / kzc;
+        if (dsq < dsz)
+        {
+            m = mc;
+            ds = dsq;
+            if (in)
+            {
+                i--;
+                q = qN;
+                cz = xadd(cz, xmul(kzc, dsq));
+                if (i <= imin) in = false;
+            }
+            else
+            {
+                i++;
+                if (i >= NR)
+                    state = GS_OUTSIDE;
+                else
+                {
+                    q = qN;
+                    cz = xadd(cz, xmul(kzc, dsq));
+                }
+            }
+        }
+        else
+        {
+            m = mc;
+            ds = dsz;
+            k += up ? 1 : -1;
+            if (up ? k >= Nz : k < 0)
+                state = GS_OUTSIDE;
+            else
+            {
+                q = xadd(q, xmul(kq, dsz));
+                cz = zN;
+            }
+        }
         return true;
     }
 };

@@ -646,4 +646,10 @@ struct Sphere1DFast : Sphere1DExact
     using Acc = float;
 };
 
+// 2D cylindrical grid, production: the reference-order FP64 crossings with FP32 accumulators
+struct Cylinder2DFast : Cylinder2DExact
+{
+    using Acc = float;
+};
+
 }  // namespace skg

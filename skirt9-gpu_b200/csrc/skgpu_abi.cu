@@ -621,6 +621,34 @@ int skgpu_upload_grid_sphere1d(skgpu_ctx* ctx, int32_t num_borders, const double
     return SKGPU_OK;
 }
 
+int skgpu_upload_grid_cylinder2d(skgpu_ctx* ctx, int32_t nrb, const double* rv, int32_t nzb, const double* zv)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (nrb < 2 || nzb < 2 || !rv || !zv || !(rv[0] >= 0.)) return fail(ctx, SKGPU_ERR_ARG, "cylinder2d: need >= 2 radial borders from R >= 0 and >= 2 z borders");
+    if (!finiteAll(rv, nrb) || !finiteAll(zv, nzb)) return fail(ctx, SKGPU_ERR_ARG, "cylinder2d: non-finite border");
+    for (int i = 1; i < nrb; ++i)
+        if (!(rv[i] > rv[i - 1])) return fail(ctx, SKGPU_ERR_ARG, "cylinder2d: radial borders must ascend");
+    for (int i = 1; i < nzb; ++i)
+        if (!(zv[i] > zv[i - 1])) return fail(ctx, SKGPU_ERR_ARG, "cylinder2d: z borders must ascend");
+    if (static_cast<int64_t>(nrb - 1) * (nzb - 1) > 2147483647LL) return fail(ctx, SKGPU_ERR_ARG, "cylinder2d: too many cells");
+    CK(cudaSetDevice(ctx->device));
+    freeGrid(ctx);
+    GridDev& g = ctx->g;
+    g.kind = SKGPU_GRID_CYLINDER2D;
+    double r = rv[nrb - 1];
+    double e[6] = {-r, -r, zv[0], r, r, zv[nzb - 1]};
+    for (int q = 0; q < 6; ++q) g.ext[q] = e[q];
+    g.eps = 1e-12 * std::sqrt(2. * (2. * r) * (2. * r) + (zv[nzb - 1] - zv[0]) * (zv[nzb - 1] - zv[0]));
+    g.cNR = nrb - 1;
+    g.cNz = nzb - 1;
+    g.numCells = g.cNR * g.cNz;
+    int rc;
+    if ((rc = gridUpload(ctx, &g.cRv, rv, static_cast<size_t>(nrb)))) return rc;
+    if ((rc = gridUpload(ctx, &g.czv, zv, static_cast<size_t>(nzb)))) return rc;
+    ctx->hasGrid = true;
+    return SKGPU_OK;
+}
+
 int skgpu_upload_grid_tetra(skgpu_ctx* ctx, int32_t num_vertices, const double* vertices, int32_t num_tetra,
                             const int32_t* tetra_vertices, const double* face_normals, const int32_t* face_ntetra,
                             const int32_t* face_nface, const double* extent, double eps)

@@ -58,6 +58,8 @@ class Scene:
             be.upload_grid_tetra(g["vertices"], g["tetra"], g["normals"], g["ntetra"], g["nface"], g["extent"], g["eps"])
         elif k == abi.GRID_SPHERE1D:
             be.upload_grid_sphere1d(g["rv"])
+        elif k == abi.GRID_CYLINDER2D:
+            be.upload_grid_cylinder2d(g["rv"], g["zv"])
         else:
             raise ValueError(f"unknown grid kind {k}")
         if self.density is not None:
@@ -231,6 +233,8 @@ class Scene:
                            eps=float(meta["eps"]))
         elif kind == "sphere1d":
             sc.grid = dict(kind=abi.GRID_SPHERE1D, rv=L("grid_rv"), extent=ext)
+        elif kind == "cylinder2d":
+            sc.grid = dict(kind=abi.GRID_CYLINDER2D, rv=L("grid_rv"), zv=L("grid_zv"), extent=ext)
         else:
             raise ValueError(f"unsupported grid in export: {kind}")
         sc.density = L("medium_density")[:, 0].copy()

@@ -73,6 +73,24 @@ def shell_sphere1d(num_packets=1e5, nbins=24, npix=64, stats=True, rmin_pc=0.05)
                       frame_instrument("i30", 30, 2, "pc", npix, stats) + sed_instrument("sed", 30, stats))
 
 
+def cylinder2d_grid(rmin_pc, rmax_pc, zmin_pc, zmax_pc, nr, nz):
+    """Cylinder2DSpatialGrid with nr linear radial bins and nz linear vertical bins."""
+    return (f'<Cylinder2DSpatialGrid minRadius="{rmin_pc} pc" maxRadius="{rmax_pc} pc" minZ="{zmin_pc} pc" '
+            f'maxZ="{zmax_pc} pc"><meshRadial type="Mesh"><LinMesh numBins="{nr}"/></meshRadial>'
+            f'<meshZ type="Mesh"><LinMesh numBins="{nz}"/></meshZ></Cylinder2DSpatialGrid>')
+
+
+def disk_cylinder2d(num_packets=1e5, npix=32, stats=True):
+    """Oligochromatic exponential dust disk (hR 1 pc, hz 0.2 pc, face-on tau 1) with a central point
+    source on a Cylinder2DSpatialGrid (R 0.05-4 pc in 20 bins, z -1..1 pc in 16 bins), one frame at
+    60 degrees with statistics plus one SED instrument."""
+    mix = mean_list_mix([0.5, 0.6], [1, 1], [0.5, 0.5], [0.6, 0.6])
+    return simulation("OligoExtinctionOnly", num_packets, point_source(), expdisk_medium(1.0, 0.2, "pc", 1.0, mix),
+                      cylinder2d_grid(0.05, 4, -1, 1, 20, 16),
+                      frame_instrument("i60", 60, 8, "pc", npix, stats) + sed_instrument("sed", 60, stats),
+                      num_density_samples=10)
+
+
 def shell_medium(rmin_pc, rmax_pc, exponent, tau_x, mix):
     return (f'<GeometricMedium velocityMagnitude="0 km/s" magneticFieldStrength="0 uG">'
             f'<geometry type="Geometry"><ShellGeometry minRadius="{rmin_pc} pc" maxRadius="{rmax_pc} pc" '

@@ -16,6 +16,8 @@ Fixtures written:
   shell_c16_explicit.npz  reference frame/SED statistics of the same scene with explicit absorption
                      (forced and free propagation), 2e5 packets each; `python
                      tests/golden/make_fixtures.py explicit` writes only this one
+  paths_sphere1d.npz, paths_cylinder2d.npz  path fixtures that also hold reference frame/SED
+                     statistics of the same scene (arguments `sphere1d`, `cylinder2d` write only them)
 """
 import os
 import shutil
@@ -115,6 +117,7 @@ def main():
     path_fixture("voronoi", ski.disk_probe(ski.voronoi_grid(4, "pc", 300)), random_rays(rng, 300, 4 * PC))
     path_fixture("tetra", ski.disk_probe(ski.tetra_grid(4, "pc", 300)), random_rays(rng, 300, 4 * PC))
     sphere1d_fixture(rng)
+    cylinder2d_fixture()
 
     # dust shell, 16^3 grid, 64^2 frame + SED: scene export + reference statistics (2e5 packets)
     npp = 200000
@@ -184,6 +187,44 @@ def sphere1d_fixture(rng=None):
     np.savez_compressed(path, **data)
 
 
+def cylinder2d_fixture(rng=None):
+    """Cylinder2DSpatialGrid (exponential disk, R 0.05-4 pc in 20 bins, z -1..1 pc in 16 bins):
+    scene export and path fixture (random rays, many starting outside in z, plus vertical,
+    horizontal and radial rays), and reference statistics of a single-threaded 2e5-packet run."""
+    rng = rng if rng is not None else np.random.default_rng(20260103)
+    rays = random_rays(rng, 300, 4.5 * PC)
+    extra = []
+    for k in ((0, 0, 1), (0, 0, -1), (1, 0, 0), (0.6, 0.8, 0.0), (0.3, 0.0, 0.95)):
+        k = np.array(k, float) / np.linalg.norm(k)
+        for p in ((0.0, 0.0, 0.0), (1.0, 0.5, 0.3), (5.0, 0.0, 0.1), (0.0, 0.0, -2.0), (0.02, 0.0, 0.0)):
+            extra.append(np.r_[np.array(p) * PC, k])
+    rays = np.vstack([rays, np.array(extra)])
+    path_fixture("cylinder2d", ski.disk_cylinder2d(1e4), rays)
+    reference_stats("paths_cylinder2d.npz", ski.disk_cylinder2d(200000), "i60", 200000)
+
+
+def reference_stats(fixture, ski_text, frame_name, npp):
+    """Adds the frame and SED statistics of a single-threaded reference run of ski_text to a
+    fixture; the run's stats scale c is recovered from its total image (MJy/sr per raw W from the
+    SED's Jy per raw W of the shell_c16 run, same distance, and this frame's pixel)."""
+    path = os.path.join(OUT, fixture)
+    data = dict(np.load(path))
+    meta = __import__("skgpu").Scene.read_export(data)[0]
+    pix = float(meta["instr0_xpsiz"]) / float(meta["instr0_distance"])
+    mjysr_per_w = float(np.load(os.path.join(OUT, "shell_c16.npz"))["ref_jy_per_w"]) * 1e-6 / (pix * pix)
+    with tempfile.TemporaryDirectory() as tmp:
+        with open(os.path.join(tmp, "r.ski"), "w") as f:
+            f.write(ski_text)
+        subprocess.run([os.path.join(BIN, "skirt"), "-t", "1", "r.ski"], cwd=tmp, check=True,
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        st = np.array([fits.read(os.path.join(tmp, f"r_{frame_name}_stats{k}.fits"))[0][0] for k in range(5)])
+        ss = np.loadtxt(os.path.join(tmp, "r_sed_sedstats.dat"))
+        total = fits.read(os.path.join(tmp, f"r_{frame_name}_total.fits"))[0][0]
+    c = st[1].sum() / (total / mjysr_per_w).sum()
+    data.update(ref_npp=npp, ref_frame_w=np.array([st[0], st[1] / c, st[2] / c ** 2]), ref_sedstats=ss[1:])
+    np.savez_compressed(path, **data)
+
+
 def explicit_fixture(mjysr_per_w, npp):
     """The 16^3 shell with explicit absorption (PhotonPacketOptions::explicitAbsorption), forced and
     free propagation: reference frame and SED statistics of single-threaded runs of npp packets. Each
@@ -209,6 +250,8 @@ def explicit_fixture(mjysr_per_w, npp):
 if __name__ == "__main__":
     if sys.argv[1:] == ["sphere1d"]:
         sphere1d_fixture()
+    elif sys.argv[1:] == ["cylinder2d"]:
+        cylinder2d_fixture()
     elif sys.argv[1:] == ["explicit"]:
         z = np.load(os.path.join(OUT, "shell_c16.npz"))
         meta = __import__("skgpu").Scene.read_export(z)[0]
