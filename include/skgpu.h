@@ -42,6 +42,7 @@ extern "C" {
 #define SKGPU_GRID_TETRA 3
 #define SKGPU_GRID_SPHERE1D 4
 #define SKGPU_GRID_CYLINDER2D 5
+#define SKGPU_GRID_SPHERE2D 6
 
 /* traversal precision (path kernels and life cycle) */
 #define SKGPU_PREC_FP64_EXACT 0 /* FP64 with the reference generators' operation order, no FMA contraction */
@@ -160,6 +161,12 @@ int skgpu_upload_grid_sphere1d(skgpu_ctx* ctx, int32_t num_borders, const double
  * (Cylinder2DSpatialGrid.cpp:433-437). */
 int skgpu_upload_grid_cylinder2d(skgpu_ctx* ctx, int32_t num_radial_borders, const double* radial_borders,
                                  int32_t num_z_borders, const double* z_borders);
+/* Sphere2DSpatialGrid: ascending radial borders r_0 >= 0 .. r_Nr, polar borders theta_0 = 0 ..
+ * theta_Nt = pi and their cosines as the grid holds them (its _rv, _thetav, _cv:
+ * SphereSpatialGrid::initPolarGrid, SphereSpatialGrid.cpp:27-60); cell index j + Nt * i
+ * (Sphere2DSpatialGrid.cpp:326-329). */
+int skgpu_upload_grid_sphere2d(skgpu_ctx* ctx, int32_t num_radial_borders, const double* radial_borders,
+                               int32_t num_polar_borders, const double* polar_borders, const double* polar_cosines);
 /* TetraMeshSpatialGrid: vertices, per tetrahedron its 4 vertex indices, and per face the outward
  * normal, the neighbouring tetrahedron (-1 on the hull) and its face index
  * (TetraMeshSpatialGrid.hpp:107-133). */

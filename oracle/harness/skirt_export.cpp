@@ -68,6 +68,7 @@
 #include "System.hpp"
 #include "Cylinder2DSpatialGrid.hpp"
 #include "Sphere1DSpatialGrid.hpp"
+#include "Sphere2DSpatialGrid.hpp"
 #include "TetraMeshSpatialGrid.hpp"
 #include "TreeNode.hpp"
 #include "TreeSpatialGrid.hpp"
@@ -183,6 +184,16 @@ namespace
             std::vector<double> rv(begin(g->_Rv), end(g->_Rv)), zv(begin(g->_zv), end(g->_zv));
             writeVec(out + "/grid_rv.npy", rv);
             writeVec(out + "/grid_zv.npy", zv);
+            return;
+        }
+        if (auto g = dynamic_cast<Sphere2DSpatialGrid*>(grid))
+        {
+            meta.kv("grid", "sphere2d");
+            std::vector<double> rv(begin(g->_rv), end(g->_rv)), tv(begin(g->_thetav), end(g->_thetav)),
+                cv(begin(g->_cv), end(g->_cv));
+            writeVec(out + "/grid_rv.npy", rv);
+            writeVec(out + "/grid_thetav.npy", tv);
+            writeVec(out + "/grid_cv.npy", cv);
             return;
         }
         if (auto g = dynamic_cast<Sphere1DSpatialGrid*>(grid))

@@ -119,6 +119,9 @@ typedef struct
     /* cylinder2d */
     double *crv, *czv;
     int cnr, cnz;
+    /* sphere2d */
+    double *s2r, *s2t, *s2c;
+    int s2nr, s2nt;
 } Grid;
 
 typedef struct
@@ -175,6 +178,7 @@ static void free_grid(Grid* g)
     free(g->tev); free(g->ten); free(g->tebox); free(g->tet); free(g->tent); free(g->tenf);
     free(g->srv);
     free(g->crv); free(g->czv);
+    free(g->s2r); free(g->s2t); free(g->s2c);
     memset(g, 0, sizeof *g);
 }
 
@@ -321,6 +325,30 @@ int or_upload_grid_cylinder2d(or_ctx* c, int32_t nrb, const double* rv, int32_t 
     memcpy(g->ext, e, sizeof e);
     g->eps = 1e-12 * sqrt(2. * (2. * r) * (2. * r) + (zv[nzb - 1] - zv[0]) * (zv[nzb - 1] - zv[0]));
     g->numCells = g->cnr * g->cnz;
+    c->hasGrid = 1;
+    return SKGPU_OK;
+}
+
+int or_upload_grid_sphere2d(or_ctx* c, int32_t nrb, const double* rv, int32_t ntb, const double* tv, const double* cv)
+{
+    if (nrb < 2 || ntb < 2 || !rv || !tv || !cv || !(rv[0] >= 0.)) return fail(c, SKGPU_ERR_ARG, "sphere2d: bad borders");
+    for (int i = 1; i < nrb; ++i)
+        if (!(rv[i] > rv[i - 1])) return fail(c, SKGPU_ERR_ARG, "sphere2d: radial borders must ascend");
+    for (int i = 1; i < ntb; ++i)
+        if (!(tv[i] > tv[i - 1])) return fail(c, SKGPU_ERR_ARG, "sphere2d: polar borders must ascend");
+    free_grid(&c->g);
+    Grid* g = &c->g;
+    g->kind = SKGPU_GRID_SPHERE2D;
+    g->s2nr = nrb - 1;
+    g->s2nt = ntb - 1;
+    g->s2r = dup(rv, (size_t)nrb * sizeof(double));
+    g->s2t = dup(tv, (size_t)ntb * sizeof(double));
+    g->s2c = dup(cv, (size_t)ntb * sizeof(double));
+    double r = rv[nrb - 1];
+    double e[6] = {-r, -r, -r, r, r, r};
+    memcpy(g->ext, e, sizeof e);
+    g->eps = 1e-11 * r;
+    g->numCells = g->s2nr * g->s2nt;
     c->hasGrid = 1;
     return SKGPU_OK;
 }
@@ -915,6 +943,131 @@ static int sph_next(const Grid* g, Gen* s)
     return 1;
 }
 
+/* Quadratic::smallestPositiveSolution (SKIRT/utils/Quadratic.hpp:44-68): of x^2 + 2 b x + c = 0, or 0 */
+static double quad_sps(double b, double c)
+{
+    if (b * b > c)
+    {
+        if (b > 0.)
+        {
+            if (c < 0.)
+            {
+                double x1 = -b - sqrt(b * b - c);
+                return c / x1;
+            }
+        }
+        else
+        {
+            double x2 = -b + sqrt(b * b - c);
+            if (c > 0.)
+            {
+                double x1 = c / x2;
+                if (x1 < x2) return x1;
+            }
+            return x2;
+        }
+    }
+    return 0.;
+}
+
+/* smallestPositiveSolution of a x^2 + 2 b x + c = 0 (Sphere2DSpatialGrid.cpp:118-125) */
+static double quad_sps3(double a, double b, double c)
+{
+    if (fabs(a) > 1e-9) return quad_sps(b / a, c / a);
+    double x = -0.5 * c / b;
+    if (x > 0.) return x;
+    return 0.;
+}
+
+/* firstIntersectionSphere / firstIntersectionCone (Sphere2DSpatialGrid.cpp:130-142) */
+static double s2_sphere(const Gen* s, double r)
+{
+    double dot = s->rx * s->kx + s->ry * s->ky + s->rz * s->kz;
+    double n2 = s->rx * s->rx + s->ry * s->ry + s->rz * s->rz;
+    return quad_sps(dot, n2 - r * r);
+}
+static double s2_cone(const Gen* s, double c)
+{
+    if (c == 0.) return -s->rz / s->kz;
+    double dot = s->rx * s->kx + s->ry * s->ky + s->rz * s->kz;
+    double n2 = s->rx * s->rx + s->ry * s->ry + s->rz * s->rz;
+    return quad_sps3(c * c - s->kz * s->kz, c * c * dot - s->rz * s->kz, c * c * n2 - s->rz * s->rz);
+}
+
+/* setCellIndices (Sphere2DSpatialGrid.cpp:160-167, Position::spherical) */
+static int s2_indices(const Grid* g, Gen* s)
+{
+    double radius = sqrt(s->rx * s->rx + s->ry * s->ry + s->rz * s->rz);
+    double theta = radius == 0 ? 0. : acos(s->rz / radius);
+    s->i = nr_locate(g->s2r, g->s2nr + 1, radius);
+    s->j = locate_clip(g->s2t, g->s2nt + 1, theta);
+    return s->i < g->s2nr;
+}
+
+/* Sphere2DSpatialGrid::MySegmentGenerator::next (Sphere2DSpatialGrid.cpp:176-290) */
+static int sph2_next(const Grid* g, Gen* s)
+{
+    const double* rv = g->s2r;
+    const double* cv = g->s2c;
+    int Nr = g->s2nr, Nt = g->s2nt;
+    double eps = 1e-11 * rv[Nr];
+    if (s->state == OUTSIDE) return 0;
+    if (s->state == UNKNOWN)
+    {
+        double rn = sqrt(s->rx * s->rx + s->ry * s->ry + s->rz * s->rz);
+        if (rn > rv[Nr])
+        {
+            double ds = s2_sphere(s, rv[Nr]);
+            if (ds <= 0.) { s->state = OUTSIDE; return 0; }
+            propagater(s, ds + eps);
+            if (!s2_indices(g, s)) { s->state = OUTSIDE; return 0; }
+            s->m = -1;
+            s->ds = ds;
+            s->state = INSIDE;
+            return 1;
+        }
+        if (rn < eps) propagater(s, eps);
+        if (!s2_indices(g, s)) { s->state = OUTSIDE; return 0; }
+        s->state = INSIDE;
+    }
+    for (int guard = 0; guard < 1000; ++guard)
+    {
+        int icur = s->i, jcur = s->j;
+        double ds = DBL_MAX;
+        if (icur > 0 || (icur == 0 && rv[0] > 0.))
+        {
+            double t = s2_sphere(s, rv[icur]);
+            if (t > 0 && t < ds) { ds = t; s->i = icur - 1; s->j = jcur; }
+        }
+        {
+            double t = s2_sphere(s, rv[icur + 1]);
+            if (t > 0 && t < ds) { ds = t; s->i = icur + 1; s->j = jcur; }
+        }
+        if (jcur > 0)
+        {
+            double t = s2_cone(s, cv[jcur]);
+            if (t > 0 && t < ds) { ds = t; s->i = icur; s->j = jcur - 1; }
+        }
+        if (jcur < Nt - 1)
+        {
+            double t = s2_cone(s, cv[jcur + 1]);
+            if (t > 0 && t < ds) { ds = t; s->i = icur; s->j = jcur + 1; }
+        }
+        if (s->i != icur || s->j != jcur)
+        {
+            s->m = jcur + Nt * icur;  /* Sphere2DSpatialGrid::index */
+            s->ds = ds;
+            propagater(s, ds + eps);
+            if (s->i >= Nr) s->state = OUTSIDE;
+            return 1;
+        }
+        propagater(s, eps);
+        if (!s2_indices(g, s)) { s->state = OUTSIDE; return 0; }
+    }
+    s->state = OUTSIDE;
+    return 0;
+}
+
 /* Cylinder2DSpatialGrid::MySegmentGenerator::moveInside (Cylinder2DSpatialGrid.cpp:124-198) */
 static int cyl_move_inside(const Grid* g, Gen* s)
 {
@@ -1064,6 +1217,7 @@ static int gen_next(const Grid* g, Gen* s)
         case SKGPU_GRID_TETRA: return tet_next(g, s);
         case SKGPU_GRID_SPHERE1D: return sph_next(g, s);
         case SKGPU_GRID_CYLINDER2D: return cyl_next(g, s);
+        case SKGPU_GRID_SPHERE2D: return sph2_next(g, s);
     }
     return 0;
 }

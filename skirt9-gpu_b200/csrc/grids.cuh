@@ -75,6 +75,11 @@ struct GridDev
     const double* cRv;
     const double* czv;
     int cNR, cNz;
+    // 2D spherical: s2Nr radial x s2Nt polar cells; radial borders, polar borders and their cosines
+    const double* s2r;
+    const double* s2t;
+    const double* s2c;
+    int s2Nr, s2Nt;
     const int* teBlkRep;         // teGridN^3: a tetrahedron overlapping each block (start of the walking locate)
 };
 
@@ -949,6 +954,178 @@ struct Cylinder2DExact : GenBase
             }
         }
         return true;
+    }
+};
+
+// ---------------------------------------------------------------------------------------------
+// 2D spherical grid (Sphere2DSpatialGrid::MySegmentGenerator::next, Sphere2DSpatialGrid.cpp:147-290):
+// from the current position the nearest positive intersection with the cell's two spheres and two
+// cones wins; the position advances by the segment plus eps = 1e-11 r_max and the cell indices
+// follow the winning boundary. Sphere and cone intersections by the reference's quadratic
+// solvers (Quadratic.hpp:44-68, Sphere2DSpatialGrid.cpp:118-142).
+// ---------------------------------------------------------------------------------------------
+SKG_D double quadSps(double b, double c)
+{
+    if (xmul(b, b) > c)
+    {
+        if (b > 0.)
+        {
+            if (c < 0.)
+            {
+                double x1 = xsub(-b, sqrt(xsub(xmul(b, b), c)));
+                return c / x1;
+            }
+        }
+        else
+        {
+            double x2 = xadd(-b, sqrt(xsub(xmul(b, b), c)));
+            if (c > 0.)
+            {
+                double x1 = c / x2;
+                if (x1 < x2) return x1;
+            }
+            return x2;
+        }
+    }
+    return 0.;
+}
+
+SKG_D double quadSps3(double a, double b, double c)
+{
+    if (fabs(a) > 1e-9) return quadSps(b / a, c / a);
+    double x = xmul(-0.5, c) / b;
+    if (x > 0.) return x;
+    return 0.;
+}
+
+struct Sphere2DExact : GenBase
+{
+    static constexpr int kMinBlocks = 3;
+    static constexpr int kRefillMin = 16;  // waiting lanes before a warp takes new tasks
+    int i, j;
+
+    SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz, int = -1)
+    {
+        startRay(x, y, z, ux, uy, uz);
+    }
+
+    SKG_D double dotRK() const { return xadd(xadd(xmul(rx, kx), xmul(ry, ky)), xmul(rz, kz)); }
+    SKG_D double norm2R() const { return xadd(xadd(xmul(rx, rx), xmul(ry, ry)), xmul(rz, rz)); }
+    SKG_D double sphere(double r) const { return quadSps(dotRK(), xsub(norm2R(), xmul(r, r))); }
+    SKG_D double cone(double c) const
+    {
+        if (c == 0.) return -rz / kz;
+        double cc = xmul(c, c);
+        return quadSps3(xsub(cc, xmul(kz, kz)), xsub(xmul(cc, dotRK()), xmul(rz, kz)), xsub(xmul(cc, norm2R()), xmul(rz, rz)));
+    }
+
+    // setCellIndices (Sphere2DSpatialGrid.cpp:160-167) with Position::spherical
+    SKG_D bool indices(const GridDev& g)
+    {
+        double radius = sqrt(norm2R());
+        double theta = radius == 0 ? 0. : acos(rz / radius);
+        i = locateNR(g.s2r, g.s2Nr + 1, radius);
+        j = locateClip(g.s2t, g.s2Nt + 1, theta);
+        return i < g.s2Nr;
+    }
+
+    SKG_D bool next(const GridDev& g)
+    {
+        if (state == GS_OUTSIDE) return false;
+        const double* rv = g.s2r;
+        const double* cv = g.s2c;
+        const int Nr = g.s2Nr, Nt = g.s2Nt;
+        const double eps = xmul(1e-11, rv[Nr]);
+        if (state == GS_UNKNOWN)
+        {
+            double rn = sqrt(norm2R());
+            if (rn > rv[Nr])
+            {
+                double d = sphere(rv[Nr]);
+                if (d <= 0.)
+                {
+                    state = GS_OUTSIDE;
+                    return false;
+                }
+                propagater(xadd(d, eps));
+                if (!indices(g))
+                {
+                    state = GS_OUTSIDE;
+                    return false;
+                }
+                m = -1;
+                ds = d;
+                state = GS_INSIDE;
+                return true;
+            }
+            if (rn < eps) propagater(eps);
+            if (!indices(g))
+            {
+                state = GS_OUTSIDE;
+                return false;
+            }
+            state = GS_INSIDE;
+        }
+        for (int guard = 0; guard < 1000; ++guard)
+        {
+            int icur = i, jcur = j;
+            double d = DBL_MAX;
+            if (icur > 0 || (icur == 0 && rv[0] > 0.))
+            {
+                double t = sphere(rv[icur]);
+                if (t > 0 && t < d)
+                {
+                    d = t;
+                    i = icur - 1;
+                    j = jcur;
+                }
+            }
+            {
+                double t = sphere(rv[icur + 1]);
+                if (t > 0 && t < d)
+                {
+                    d = t;
+                    i = icur + 1;
+                    j = jcur;
+                }
+            }
+            if (jcur > 0)
+            {
+                double t = cone(cv[jcur]);
+                if (t > 0 && t < d)
+                {
+                    d = t;
+                    i = icur;
+                    j = jcur - 1;
+                }
+            }
+            if (jcur < Nt - 1)
+            {
+                double t = cone(cv[jcur + 1]);
+                if (t > 0 && t < d)
+                {
+                    d = t;
+                    i = icur;
+                    j = jcur + 1;
+                }
+            }
+            if (i != icur || j != jcur)
+            {
+                m = jcur + Nt * icur;  // Sphere2DSpatialGrid::index (negative inside r_0)
+                ds = d;
+                propagater(xadd(d, eps));
+                if (i >= Nr) state = GS_OUTSIDE;
+                return true;
+            }
+            propagater(eps);
+            if (!indices(g))
+            {
+                state = GS_OUTSIDE;
+                return false;
+            }
+        }
+        state = GS_OUTSIDE;
+        return false;
     }
 };
 

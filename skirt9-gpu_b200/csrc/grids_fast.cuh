@@ -652,4 +652,10 @@ struct Cylinder2DFast : Cylinder2DExact
     using Acc = float;
 };
 
+// 2D spherical grid, production: the reference-order FP64 crossings with FP32 accumulators
+struct Sphere2DFast : Sphere2DExact
+{
+    using Acc = float;
+};
+
 }  // namespace skg

@@ -21,6 +21,7 @@ cudaError_t launchTracePathsFP64(int precision, const GridDev& g, int n, const d
         case 3: tracePathsKernel<TetraExact><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
         case 4: tracePathsKernel<Sphere1DExact><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
         case 5: tracePathsKernel<Cylinder2DExact><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
+        case 6: tracePathsKernel<Sphere2DExact><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -40,6 +41,7 @@ cudaError_t launchOpticalDepthsFP64(int precision, const GridDev& g, const doubl
         case 3: opticalDepthKernel<TetraExact><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
         case 4: opticalDepthKernel<Sphere1DExact><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
         case 5: opticalDepthKernel<Cylinder2DExact><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
+        case 6: opticalDepthKernel<Sphere2DExact><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

@@ -649,6 +649,36 @@ int skgpu_upload_grid_cylinder2d(skgpu_ctx* ctx, int32_t nrb, const double* rv, 
     return SKGPU_OK;
 }
 
+int skgpu_upload_grid_sphere2d(skgpu_ctx* ctx, int32_t nrb, const double* rv, int32_t ntb, const double* tv,
+                               const double* cv)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (nrb < 2 || ntb < 2 || !rv || !tv || !cv || !(rv[0] >= 0.)) return fail(ctx, SKGPU_ERR_ARG, "sphere2d: need >= 2 radial borders from r >= 0 and >= 2 polar borders");
+    if (!finiteAll(rv, nrb) || !finiteAll(tv, ntb) || !finiteAll(cv, ntb)) return fail(ctx, SKGPU_ERR_ARG, "sphere2d: non-finite border");
+    for (int i = 1; i < nrb; ++i)
+        if (!(rv[i] > rv[i - 1])) return fail(ctx, SKGPU_ERR_ARG, "sphere2d: radial borders must ascend");
+    for (int i = 1; i < ntb; ++i)
+        if (!(tv[i] > tv[i - 1])) return fail(ctx, SKGPU_ERR_ARG, "sphere2d: polar borders must ascend");
+    if (static_cast<int64_t>(nrb - 1) * (ntb - 1) > 2147483647LL) return fail(ctx, SKGPU_ERR_ARG, "sphere2d: too many cells");
+    CK(cudaSetDevice(ctx->device));
+    freeGrid(ctx);
+    GridDev& g = ctx->g;
+    g.kind = SKGPU_GRID_SPHERE2D;
+    double r = rv[nrb - 1];
+    double e[6] = {-r, -r, -r, r, r, r};
+    for (int q = 0; q < 6; ++q) g.ext[q] = e[q];
+    g.eps = 1e-11 * r;
+    g.s2Nr = nrb - 1;
+    g.s2Nt = ntb - 1;
+    g.numCells = g.s2Nr * g.s2Nt;
+    int rc;
+    if ((rc = gridUpload(ctx, &g.s2r, rv, static_cast<size_t>(nrb)))) return rc;
+    if ((rc = gridUpload(ctx, &g.s2t, tv, static_cast<size_t>(ntb)))) return rc;
+    if ((rc = gridUpload(ctx, &g.s2c, cv, static_cast<size_t>(ntb)))) return rc;
+    ctx->hasGrid = true;
+    return SKGPU_OK;
+}
+
 int skgpu_upload_grid_tetra(skgpu_ctx* ctx, int32_t num_vertices, const double* vertices, int32_t num_tetra,
                             const int32_t* tetra_vertices, const double* face_normals, const int32_t* face_ntetra,
                             const int32_t* face_nface, const double* extent, double eps)

@@ -16,7 +16,7 @@ LIB_PATH = os.path.join(PKG_ROOT, "lib", "libskgpu.so")
 
 # status codes
 OK, ERR_ARG, ERR_CUDA, ERR_STATE, ERR_TIMEOUT, ERR_DEVICE, ERR_UNSUPPORTED = range(7)
-GRID_CARTESIAN, GRID_OCTREE, GRID_VORONOI, GRID_TETRA, GRID_SPHERE1D, GRID_CYLINDER2D = range(6)
+GRID_CARTESIAN, GRID_OCTREE, GRID_VORONOI, GRID_TETRA, GRID_SPHERE1D, GRID_CYLINDER2D, GRID_SPHERE2D = range(7)
 PREC_FP64_EXACT, PREC_FP32 = 0, 1
 SRC_POINT, SRC_EXPDISK, SRC_RADIAL = 0, 1, 2
 SPEC_DISCRETE, SPEC_TABLE = 0, 1
@@ -116,6 +116,7 @@ SIGNATURES = {
     "upload_grid_tetra": [_P, _I, _P, _I, _P, _P, _P, _P, _P, _D],
     "upload_grid_sphere1d": [_P, _I, _P],
     "upload_grid_cylinder2d": [_P, _I, _P, _I, _P],
+    "upload_grid_sphere2d": [_P, _I, _P, _I, _P, _P],
     "upload_medium": [_P, _I, _P],
     "upload_dust_mix": [_P, _I, _P, _P, _P, _P],
     "upload_rf_grid": [_P, _I, _I, _P, _P],
@@ -198,6 +199,10 @@ class Backend:
         return rc
 
     # ---- typed helpers ----
+    def upload_grid_sphere2d(self, rv, thetav, cv):
+        rv, tv, cv = f64(rv), f64(thetav), f64(cv)
+        self.call("upload_grid_sphere2d", len(rv), _ptr(rv), len(tv), _ptr(tv), _ptr(cv))
+
     def upload_grid_cylinder2d(self, rv, zv):
         rv, zv = f64(rv), f64(zv)
         self.call("upload_grid_cylinder2d", len(rv), _ptr(rv), len(zv), _ptr(zv))

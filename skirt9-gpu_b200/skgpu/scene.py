@@ -60,6 +60,8 @@ class Scene:
             be.upload_grid_sphere1d(g["rv"])
         elif k == abi.GRID_CYLINDER2D:
             be.upload_grid_cylinder2d(g["rv"], g["zv"])
+        elif k == abi.GRID_SPHERE2D:
+            be.upload_grid_sphere2d(g["rv"], g["thetav"], g["cv"])
         else:
             raise ValueError(f"unknown grid kind {k}")
         if self.density is not None:
@@ -235,6 +237,9 @@ class Scene:
             sc.grid = dict(kind=abi.GRID_SPHERE1D, rv=L("grid_rv"), extent=ext)
         elif kind == "cylinder2d":
             sc.grid = dict(kind=abi.GRID_CYLINDER2D, rv=L("grid_rv"), zv=L("grid_zv"), extent=ext)
+        elif kind == "sphere2d":
+            sc.grid = dict(kind=abi.GRID_SPHERE2D, rv=L("grid_rv"), thetav=L("grid_thetav"), cv=L("grid_cv"),
+                           extent=ext)
         else:
             raise ValueError(f"unsupported grid in export: {kind}")
         sc.density = L("medium_density")[:, 0].copy()

@@ -80,6 +80,23 @@ def cylinder2d_grid(rmin_pc, rmax_pc, zmin_pc, zmax_pc, nr, nz):
             f'<meshZ type="Mesh"><LinMesh numBins="{nz}"/></meshZ></Cylinder2DSpatialGrid>')
 
 
+def sphere2d_grid(rmin_pc, rmax_pc, nr, ntheta):
+    """Sphere2DSpatialGrid with nr linear radial bins and ntheta linear polar bins."""
+    return (f'<Sphere2DSpatialGrid minRadius="{rmin_pc} pc" maxRadius="{rmax_pc} pc">'
+            f'<meshRadial type="Mesh"><LinMesh numBins="{nr}"/></meshRadial>'
+            f'<meshPolar type="Mesh"><LinMesh numBins="{ntheta}"/></meshPolar></Sphere2DSpatialGrid>')
+
+
+def disk_sphere2d(num_packets=1e5, npix=32, stats=True):
+    """The disk scene of disk_cylinder2d on a Sphere2DSpatialGrid (r 0.05-4 pc in 20 bins, 15 polar
+    bins; the grid adds the equatorial border), one frame at 60 degrees with statistics plus one SED."""
+    mix = mean_list_mix([0.5, 0.6], [1, 1], [0.5, 0.5], [0.6, 0.6])
+    return simulation("OligoExtinctionOnly", num_packets, point_source(), expdisk_medium(1.0, 0.2, "pc", 1.0, mix),
+                      sphere2d_grid(0.05, 4, 20, 15),
+                      frame_instrument("i60", 60, 8, "pc", npix, stats) + sed_instrument("sed", 60, stats),
+                      num_density_samples=10)
+
+
 def disk_cylinder2d(num_packets=1e5, npix=32, stats=True):
     """Oligochromatic exponential dust disk (hR 1 pc, hz 0.2 pc, face-on tau 1) with a central point
     source on a Cylinder2DSpatialGrid (R 0.05-4 pc in 20 bins, z -1..1 pc in 16 bins), one frame at
