@@ -43,6 +43,7 @@ extern "C" {
 #define SKGPU_GRID_SPHERE1D 4
 #define SKGPU_GRID_CYLINDER2D 5
 #define SKGPU_GRID_SPHERE2D 6
+#define SKGPU_GRID_SPHERE3D 7
 
 /* traversal precision (path kernels and life cycle) */
 #define SKGPU_PREC_FP64_EXACT 0 /* FP64 with the reference generators' operation order, no FMA contraction */
@@ -167,6 +168,14 @@ int skgpu_upload_grid_cylinder2d(skgpu_ctx* ctx, int32_t num_radial_borders, con
  * (Sphere2DSpatialGrid.cpp:326-329). */
 int skgpu_upload_grid_sphere2d(skgpu_ctx* ctx, int32_t num_radial_borders, const double* radial_borders,
                                int32_t num_polar_borders, const double* polar_borders, const double* polar_cosines);
+/* Sphere3DSpatialGrid: radial borders (with the artificial inner hole the grid adds when r_min = 0),
+ * polar borders and cosines, azimuthal borders phi_0 = -pi .. phi_Nphi = pi with their sines and
+ * cosines, and the grid's path step eps, all as the grid holds them (its _rv, _thetav, _cv, _phiv,
+ * _sinv, _cosv, _eps: Sphere3DSpatialGrid.cpp:25-70); cell index k + (j + i * Ntheta) * Nphi. */
+int skgpu_upload_grid_sphere3d(skgpu_ctx* ctx, int32_t num_radial_borders, const double* radial_borders,
+                               int32_t num_polar_borders, const double* polar_borders, const double* polar_cosines,
+                               int32_t num_azimuth_borders, const double* azimuth_borders, const double* azimuth_sines,
+                               const double* azimuth_cosines, double eps);
 /* TetraMeshSpatialGrid: vertices, per tetrahedron its 4 vertex indices, and per face the outward
  * normal, the neighbouring tetrahedron (-1 on the hull) and its face index
  * (TetraMeshSpatialGrid.hpp:107-133). */

@@ -69,6 +69,7 @@
 #include "Cylinder2DSpatialGrid.hpp"
 #include "Sphere1DSpatialGrid.hpp"
 #include "Sphere2DSpatialGrid.hpp"
+#include "Sphere3DSpatialGrid.hpp"
 #include "TetraMeshSpatialGrid.hpp"
 #include "TreeNode.hpp"
 #include "TreeSpatialGrid.hpp"
@@ -184,6 +185,19 @@ namespace
             std::vector<double> rv(begin(g->_Rv), end(g->_Rv)), zv(begin(g->_zv), end(g->_zv));
             writeVec(out + "/grid_rv.npy", rv);
             writeVec(out + "/grid_zv.npy", zv);
+            return;
+        }
+        if (auto g = dynamic_cast<Sphere3DSpatialGrid*>(grid))
+        {
+            meta.kv("grid", "sphere3d");
+            meta.kv("eps", g->_eps);
+            auto vec = [](const Array& a) { return std::vector<double>(begin(a), end(a)); };
+            writeVec(out + "/grid_rv.npy", vec(g->_rv));
+            writeVec(out + "/grid_thetav.npy", vec(g->_thetav));
+            writeVec(out + "/grid_cv.npy", vec(g->_cv));
+            writeVec(out + "/grid_phiv.npy", vec(g->_phiv));
+            writeVec(out + "/grid_sinv.npy", vec(g->_sinv));
+            writeVec(out + "/grid_cosv.npy", vec(g->_cosv));
             return;
         }
         if (auto g = dynamic_cast<Sphere2DSpatialGrid*>(grid))

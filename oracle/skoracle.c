@@ -122,6 +122,10 @@ typedef struct
     /* sphere2d */
     double *s2r, *s2t, *s2c;
     int s2nr, s2nt;
+    /* sphere3d */
+    double *s3r, *s3t, *s3c, *s3p, *s3s, *s3k;
+    int s3nr, s3nt, s3np;
+    double s3eps;
 } Grid;
 
 typedef struct
@@ -179,6 +183,7 @@ static void free_grid(Grid* g)
     free(g->srv);
     free(g->crv); free(g->czv);
     free(g->s2r); free(g->s2t); free(g->s2c);
+    free(g->s3r); free(g->s3t); free(g->s3c); free(g->s3p); free(g->s3s); free(g->s3k);
     memset(g, 0, sizeof *g);
 }
 
@@ -349,6 +354,33 @@ int or_upload_grid_sphere2d(or_ctx* c, int32_t nrb, const double* rv, int32_t nt
     memcpy(g->ext, e, sizeof e);
     g->eps = 1e-11 * r;
     g->numCells = g->s2nr * g->s2nt;
+    c->hasGrid = 1;
+    return SKGPU_OK;
+}
+
+int or_upload_grid_sphere3d(or_ctx* c, int32_t nrb, const double* rv, int32_t ntb, const double* tv, const double* cv,
+                            int32_t npb, const double* pv, const double* sv, const double* kv, double eps)
+{
+    if (nrb < 2 || ntb < 2 || npb < 2 || !rv || !tv || !cv || !pv || !sv || !kv || !(rv[0] >= 0.) || !(eps > 0.))
+        return fail(c, SKGPU_ERR_ARG, "sphere3d: bad borders");
+    free_grid(&c->g);
+    Grid* g = &c->g;
+    g->kind = SKGPU_GRID_SPHERE3D;
+    g->s3nr = nrb - 1;
+    g->s3nt = ntb - 1;
+    g->s3np = npb - 1;
+    g->s3r = dup(rv, (size_t)nrb * sizeof(double));
+    g->s3t = dup(tv, (size_t)ntb * sizeof(double));
+    g->s3c = dup(cv, (size_t)ntb * sizeof(double));
+    g->s3p = dup(pv, (size_t)npb * sizeof(double));
+    g->s3s = dup(sv, (size_t)npb * sizeof(double));
+    g->s3k = dup(kv, (size_t)npb * sizeof(double));
+    g->s3eps = eps;
+    double r = rv[nrb - 1];
+    double e[6] = {-r, -r, -r, r, r, r};
+    memcpy(g->ext, e, sizeof e);
+    g->eps = eps;
+    g->numCells = g->s3nr * g->s3nt * g->s3np;
     c->hasGrid = 1;
     return SKGPU_OK;
 }
@@ -1068,6 +1100,118 @@ static int sph2_next(const Grid* g, Gen* s)
     return 0;
 }
 
+/* Sphere3DSpatialGrid::MySegmentGenerator (Sphere3DSpatialGrid.cpp:160-370); EPS = 1e-12 (:20) */
+static double s3_sps3(double a, double b, double c)
+{
+    if (fabs(a) > 1e-12) return quad_sps(b / a, c / a);
+    double x = -0.5 * c / b;
+    if (x > 0.) return x;
+    return 0.;
+}
+static double s3_sphere(const Gen* s, double r)
+{
+    double dot = s->rx * s->kx + s->ry * s->ky + s->rz * s->kz;
+    double n2 = s->rx * s->rx + s->ry * s->ry + s->rz * s->rz;
+    return quad_sps(dot, n2 - r * r);
+}
+static double s3_cone(const Gen* s, double c)
+{
+    if (c == 0.) return -s->rz / s->kz;
+    double dot = s->rx * s->kx + s->ry * s->ky + s->rz * s->kz;
+    double n2 = s->rx * s->rx + s->ry * s->ry + s->rz * s->rz;
+    return s3_sps3(c * c - s->kz * s->kz, c * c * dot - s->rz * s->kz, c * c * n2 - s->rz * s->rz);
+}
+static double s3_plane(const Gen* s, double sn, double cs)
+{
+    double q = s->kx * sn - s->ky * cs;
+    if (fabs(q) < 1e-12) return 0.;
+    return -(s->rx * sn - s->ry * cs) / q;
+}
+static int s3_indices(const Grid* g, Gen* s)
+{
+    double radius = sqrt(s->rx * s->rx + s->ry * s->ry + s->rz * s->rz);
+    double theta = 0., phi = 0.;
+    if (radius != 0)
+    {
+        theta = acos(s->rz / radius);
+        phi = atan2(s->ry, s->rx);
+    }
+    s->i = nr_locate(g->s3r, g->s3nr + 1, radius);
+    s->j = locate_clip(g->s3t, g->s3nt + 1, theta);
+    s->k = locate_clip(g->s3p, g->s3np + 1, phi);
+    return s->i < g->s3nr;
+}
+static int sph3_next(const Grid* g, Gen* s)
+{
+    const double* rv = g->s3r;
+    int Nr = g->s3nr, Nt = g->s3nt, Np = g->s3np;
+    double eps = g->s3eps;
+    if (s->state == OUTSIDE) return 0;
+    if (s->state == UNKNOWN)
+    {
+        double rn = sqrt(s->rx * s->rx + s->ry * s->ry + s->rz * s->rz);
+        if (rn > rv[Nr])
+        {
+            double ds = s3_sphere(s, rv[Nr]);
+            if (ds <= 0.) { s->state = OUTSIDE; return 0; }
+            propagater(s, ds + eps);
+            if (!s3_indices(g, s)) { s->state = OUTSIDE; return 0; }
+            s->m = -1;
+            s->ds = ds;
+            s->state = INSIDE;
+            return 1;
+        }
+        if (!s3_indices(g, s)) { s->state = OUTSIDE; return 0; }
+        s->state = INSIDE;
+    }
+    if (s->i >= 0)
+    {
+        int icur = s->i, jcur = s->j, kcur = s->k;
+        double ds = DBL_MAX;
+        {
+            double t = s3_sphere(s, rv[icur]);
+            if (t > 0 && t < ds) { ds = t; s->i = icur - 1; s->j = jcur; s->k = kcur; }
+        }
+        {
+            double t = s3_sphere(s, rv[icur + 1]);
+            if (t > 0 && t < ds) { ds = t; s->i = icur + 1; s->j = jcur; s->k = kcur; }
+        }
+        if (jcur > 0)
+        {
+            double t = s3_cone(s, g->s3c[jcur]);
+            if (t > 0 && t < ds) { ds = t; s->i = icur; s->j = jcur - 1; s->k = kcur; }
+        }
+        if (jcur < Nt - 1)
+        {
+            double t = s3_cone(s, g->s3c[jcur + 1]);
+            if (t > 0 && t < ds) { ds = t; s->i = icur; s->j = jcur + 1; s->k = kcur; }
+        }
+        {
+            double t = s3_plane(s, g->s3s[kcur], g->s3k[kcur]);
+            if (t > 0. && t < ds) { ds = t; s->i = icur; s->j = jcur; s->k = kcur > 0 ? kcur - 1 : Np - 1; }
+        }
+        {
+            double t = s3_plane(s, g->s3s[kcur + 1], g->s3k[kcur + 1]);
+            if (t > 0. && t < ds) { ds = t; s->i = icur; s->j = jcur; s->k = (kcur + 1) % Np; }
+        }
+        if (ds == DBL_MAX) { s->state = OUTSIDE; return 0; }
+        s->m = kcur + (jcur + icur * Nt) * Np;  /* Sphere3DSpatialGrid::index */
+        s->ds = ds;
+        propagater(s, ds + eps);
+        if (s->i >= Nr) s->state = OUTSIDE;
+    }
+    else
+    {
+        double ds = s3_sphere(s, rv[0]);
+        if (ds <= 0.) { s->state = OUTSIDE; return 0; }
+        s->m = -1;
+        s->ds = ds;
+        propagater(s, ds + eps);
+        if (!s3_indices(g, s)) { s->state = OUTSIDE; return 0; }
+    }
+    return 1;
+}
+
 /* Cylinder2DSpatialGrid::MySegmentGenerator::moveInside (Cylinder2DSpatialGrid.cpp:124-198) */
 static int cyl_move_inside(const Grid* g, Gen* s)
 {
@@ -1218,6 +1362,7 @@ static int gen_next(const Grid* g, Gen* s)
         case SKGPU_GRID_SPHERE1D: return sph_next(g, s);
         case SKGPU_GRID_CYLINDER2D: return cyl_next(g, s);
         case SKGPU_GRID_SPHERE2D: return sph2_next(g, s);
+        case SKGPU_GRID_SPHERE3D: return sph3_next(g, s);
     }
     return 0;
 }

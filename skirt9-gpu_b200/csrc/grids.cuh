@@ -80,6 +80,15 @@ struct GridDev
     const double* s2t;
     const double* s2c;
     int s2Nr, s2Nt;
+    // 3D spherical: radial, polar (+ cosines) and azimuthal (+ sines, cosines) borders, path step
+    const double* s3r;
+    const double* s3t;
+    const double* s3c;
+    const double* s3p;
+    const double* s3s;
+    const double* s3k;
+    int s3Nr, s3Nt, s3Np;
+    double s3eps;
     const int* teBlkRep;         // teGridN^3: a tetrahedron overlapping each block (start of the walking locate)
 };
 
@@ -1126,6 +1135,155 @@ struct Sphere2DExact : GenBase
         }
         state = GS_OUTSIDE;
         return false;
+    }
+};
+
+// ---------------------------------------------------------------------------------------------
+// 3D spherical grid (Sphere3DSpatialGrid::MySegmentGenerator, Sphere3DSpatialGrid.cpp:160-370):
+// the nearest positive intersection of the cell's two spheres, two cones and two meridional planes
+// (EPS = 1e-12, :20); inside the (possibly artificial) inner hole one empty step to the hole's
+// sphere, after which the azimuth bin is re-derived from the position.
+// ---------------------------------------------------------------------------------------------
+struct Sphere3DExact : GenBase
+{
+    static constexpr int kMinBlocks = 3;
+    static constexpr int kRefillMin = 16;  // waiting lanes before a warp takes new tasks
+    int i, j, k;
+
+    SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz, int = -1)
+    {
+        startRay(x, y, z, ux, uy, uz);
+    }
+
+    SKG_D double dotRK() const { return xadd(xadd(xmul(rx, kx), xmul(ry, ky)), xmul(rz, kz)); }
+    SKG_D double norm2R() const { return xadd(xadd(xmul(rx, rx), xmul(ry, ry)), xmul(rz, rz)); }
+    SKG_D double sphere(double r) const { return quadSps(dotRK(), xsub(norm2R(), xmul(r, r))); }
+    SKG_D static double sps3(double a, double b, double c)
+    {
+        if (fabs(a) > 1e-12) return quadSps(b / a, c / a);
+        double x = xmul(-0.5, c) / b;
+        if (x > 0.) return x;
+        return 0.;
+    }
+    SKG_D double cone(double c) const
+    {
+        if (c == 0.) return -rz / kz;
+        double cc = xmul(c, c);
+        return sps3(xsub(cc, xmul(kz, kz)), xsub(xmul(cc, dotRK()), xmul(rz, kz)), xsub(xmul(cc, norm2R()), xmul(rz, rz)));
+    }
+    SKG_D double plane(double sn, double cs) const
+    {
+        double q = xsub(xmul(kx, sn), xmul(ky, cs));
+        if (fabs(q) < 1e-12) return 0.;
+        return -xsub(xmul(rx, sn), xmul(ry, cs)) / q;
+    }
+    // setCellIndices with Position::spherical (Sphere3DSpatialGrid.cpp:175-183)
+    SKG_D bool indices(const GridDev& g)
+    {
+        double radius = sqrt(norm2R());
+        double theta = 0., phi = 0.;
+        if (radius != 0)
+        {
+            theta = acos(rz / radius);
+            phi = atan2(ry, rx);
+        }
+        i = locateNR(g.s3r, g.s3Nr + 1, radius);
+        j = locateClip(g.s3t, g.s3Nt + 1, theta);
+        k = locateClip(g.s3p, g.s3Np + 1, phi);
+        return i < g.s3Nr;
+    }
+
+    SKG_D bool next(const GridDev& g)
+    {
+        if (state == GS_OUTSIDE) return false;
+        const double* rv = g.s3r;
+        const int Nr = g.s3Nr, Nt = g.s3Nt, Np = g.s3Np;
+        const double eps = g.s3eps;
+        if (state == GS_UNKNOWN)
+        {
+            double rn = sqrt(norm2R());
+            if (rn > rv[Nr])
+            {
+                double d = sphere(rv[Nr]);
+                if (d <= 0.)
+                {
+                    state = GS_OUTSIDE;
+                    return false;
+                }
+                propagater(xadd(d, eps));
+                if (!indices(g))
+                {
+                    state = GS_OUTSIDE;
+                    return false;
+                }
+                m = -1;
+                ds = d;
+                state = GS_INSIDE;
+                return true;
+            }
+            if (!indices(g))
+            {
+                state = GS_OUTSIDE;
+                return false;
+            }
+            state = GS_INSIDE;
+        }
+        if (i >= 0)
+        {
+            int icur = i, jcur = j, kcur = k;
+            double d = DBL_MAX;
+            {
+                double t = sphere(rv[icur]);
+                if (t > 0 && t < d) { d = t; i = icur - 1; j = jcur; k = kcur; }
+            }
+            {
+                double t = sphere(rv[icur + 1]);
+                if (t > 0 && t < d) { d = t; i = icur + 1; j = jcur; k = kcur; }
+            }
+            if (jcur > 0)
+            {
+                double t = cone(g.s3c[jcur]);
+                if (t > 0 && t < d) { d = t; i = icur; j = jcur - 1; k = kcur; }
+            }
+            if (jcur < Nt - 1)
+            {
+                double t = cone(g.s3c[jcur + 1]);
+                if (t > 0 && t < d) { d = t; i = icur; j = jcur + 1; k = kcur; }
+            }
+            {
+                double t = plane(g.s3s[kcur], g.s3k[kcur]);
+                if (t > 0. && t < d) { d = t; i = icur; j = jcur; k = kcur > 0 ? kcur - 1 : Np - 1; }
+            }
+            {
+                double t = plane(g.s3s[kcur + 1], g.s3k[kcur + 1]);
+                if (t > 0. && t < d) { d = t; i = icur; j = jcur; k = (kcur + 1) % Np; }
+            }
+            if (d == DBL_MAX)
+            {
+                state = GS_OUTSIDE;
+                return false;
+            }
+            m = kcur + (jcur + icur * Nt) * Np;  // Sphere3DSpatialGrid::index
+            ds = d;
+            propagater(xadd(d, eps));
+            if (i >= Nr) state = GS_OUTSIDE;
+            return true;
+        }
+        double d = sphere(rv[0]);
+        if (d <= 0.)
+        {
+            state = GS_OUTSIDE;
+            return false;
+        }
+        m = -1;
+        ds = d;
+        propagater(xadd(d, eps));
+        if (!indices(g))
+        {
+            state = GS_OUTSIDE;
+            return false;
+        }
+        return true;
     }
 };
 

@@ -658,4 +658,10 @@ struct Sphere2DFast : Sphere2DExact
     using Acc = float;
 };
 
+// 3D spherical grid, production: the reference-order FP64 crossings with FP32 accumulators
+struct Sphere3DFast : Sphere3DExact
+{
+    using Acc = float;
+};
+
 }  // namespace skg

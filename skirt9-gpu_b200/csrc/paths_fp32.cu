@@ -23,6 +23,7 @@ cudaError_t launchTracePathsFP32(int precision, const GridDev& g, int n, const d
         case 4: tracePathsKernel<Sphere1DFast><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
         case 5: tracePathsKernel<Cylinder2DFast><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
         case 6: tracePathsKernel<Sphere2DFast><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
+        case 7: tracePathsKernel<Sphere3DFast><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
         default: return cudaErrorNotSupported;
     }
     return cudaGetLastError();
@@ -43,6 +44,7 @@ cudaError_t launchOpticalDepthsFP32(int precision, const GridDev& g, const doubl
         case 4: opticalDepthKernel<Sphere1DFast><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
         case 5: opticalDepthKernel<Cylinder2DFast><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
         case 6: opticalDepthKernel<Sphere2DFast><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
+        case 7: opticalDepthKernel<Sphere3DFast><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
         default: return cudaErrorNotSupported;
     }
     return cudaGetLastError();

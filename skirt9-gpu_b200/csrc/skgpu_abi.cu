@@ -679,6 +679,47 @@ int skgpu_upload_grid_sphere2d(skgpu_ctx* ctx, int32_t nrb, const double* rv, in
     return SKGPU_OK;
 }
 
+int skgpu_upload_grid_sphere3d(skgpu_ctx* ctx, int32_t nrb, const double* rv, int32_t ntb, const double* tv,
+                               const double* cv, int32_t npb, const double* pv, const double* sv, const double* kv,
+                               double eps)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (nrb < 2 || ntb < 2 || npb < 2 || !rv || !tv || !cv || !pv || !sv || !kv || !(rv[0] >= 0.) || !(eps > 0.))
+        return fail(ctx, SKGPU_ERR_ARG, "sphere3d: need >= 2 radial, polar and azimuthal borders, r >= 0 and eps > 0");
+    if (!finiteAll(rv, nrb) || !finiteAll(tv, ntb) || !finiteAll(cv, ntb) || !finiteAll(pv, npb) || !finiteAll(sv, npb)
+        || !finiteAll(kv, npb))
+        return fail(ctx, SKGPU_ERR_ARG, "sphere3d: non-finite border");
+    for (int i = 1; i < nrb; ++i)
+        if (!(rv[i] > rv[i - 1])) return fail(ctx, SKGPU_ERR_ARG, "sphere3d: radial borders must ascend");
+    for (int i = 1; i < ntb; ++i)
+        if (!(tv[i] > tv[i - 1])) return fail(ctx, SKGPU_ERR_ARG, "sphere3d: polar borders must ascend");
+    for (int i = 1; i < npb; ++i)
+        if (!(pv[i] > pv[i - 1])) return fail(ctx, SKGPU_ERR_ARG, "sphere3d: azimuthal borders must ascend");
+    if (static_cast<int64_t>(nrb - 1) * (ntb - 1) * (npb - 1) > 2147483647LL) return fail(ctx, SKGPU_ERR_ARG, "sphere3d: too many cells");
+    CK(cudaSetDevice(ctx->device));
+    freeGrid(ctx);
+    GridDev& g = ctx->g;
+    g.kind = SKGPU_GRID_SPHERE3D;
+    double r = rv[nrb - 1];
+    double e[6] = {-r, -r, -r, r, r, r};
+    for (int q = 0; q < 6; ++q) g.ext[q] = e[q];
+    g.eps = eps;
+    g.s3eps = eps;
+    g.s3Nr = nrb - 1;
+    g.s3Nt = ntb - 1;
+    g.s3Np = npb - 1;
+    g.numCells = g.s3Nr * g.s3Nt * g.s3Np;
+    int rc;
+    if ((rc = gridUpload(ctx, &g.s3r, rv, static_cast<size_t>(nrb)))) return rc;
+    if ((rc = gridUpload(ctx, &g.s3t, tv, static_cast<size_t>(ntb)))) return rc;
+    if ((rc = gridUpload(ctx, &g.s3c, cv, static_cast<size_t>(ntb)))) return rc;
+    if ((rc = gridUpload(ctx, &g.s3p, pv, static_cast<size_t>(npb)))) return rc;
+    if ((rc = gridUpload(ctx, &g.s3s, sv, static_cast<size_t>(npb)))) return rc;
+    if ((rc = gridUpload(ctx, &g.s3k, kv, static_cast<size_t>(npb)))) return rc;
+    ctx->hasGrid = true;
+    return SKGPU_OK;
+}
+
 int skgpu_upload_grid_tetra(skgpu_ctx* ctx, int32_t num_vertices, const double* vertices, int32_t num_tetra,
                             const int32_t* tetra_vertices, const double* face_normals, const int32_t* face_ntetra,
                             const int32_t* face_nface, const double* extent, double eps)

@@ -16,7 +16,7 @@ LIB_PATH = os.path.join(PKG_ROOT, "lib", "libskgpu.so")
 
 # status codes
 OK, ERR_ARG, ERR_CUDA, ERR_STATE, ERR_TIMEOUT, ERR_DEVICE, ERR_UNSUPPORTED = range(7)
-GRID_CARTESIAN, GRID_OCTREE, GRID_VORONOI, GRID_TETRA, GRID_SPHERE1D, GRID_CYLINDER2D, GRID_SPHERE2D = range(7)
+GRID_CARTESIAN, GRID_OCTREE, GRID_VORONOI, GRID_TETRA, GRID_SPHERE1D, GRID_CYLINDER2D, GRID_SPHERE2D, GRID_SPHERE3D = range(8)
 PREC_FP64_EXACT, PREC_FP32 = 0, 1
 SRC_POINT, SRC_EXPDISK, SRC_RADIAL = 0, 1, 2
 SPEC_DISCRETE, SPEC_TABLE = 0, 1
@@ -117,6 +117,7 @@ SIGNATURES = {
     "upload_grid_sphere1d": [_P, _I, _P],
     "upload_grid_cylinder2d": [_P, _I, _P, _I, _P],
     "upload_grid_sphere2d": [_P, _I, _P, _I, _P, _P],
+    "upload_grid_sphere3d": [_P, _I, _P, _I, _P, _P, _I, _P, _P, _P, _D],
     "upload_medium": [_P, _I, _P],
     "upload_dust_mix": [_P, _I, _P, _P, _P, _P],
     "upload_rf_grid": [_P, _I, _I, _P, _P],
@@ -199,6 +200,11 @@ class Backend:
         return rc
 
     # ---- typed helpers ----
+    def upload_grid_sphere3d(self, rv, thetav, cv, phiv, sinv, cosv, eps):
+        rv, tv, cv, pv, sv, kv = f64(rv), f64(thetav), f64(cv), f64(phiv), f64(sinv), f64(cosv)
+        self.call("upload_grid_sphere3d", len(rv), _ptr(rv), len(tv), _ptr(tv), _ptr(cv), len(pv), _ptr(pv), _ptr(sv),
+                  _ptr(kv), float(eps))
+
     def upload_grid_sphere2d(self, rv, thetav, cv):
         rv, tv, cv = f64(rv), f64(thetav), f64(cv)
         self.call("upload_grid_sphere2d", len(rv), _ptr(rv), len(tv), _ptr(tv), _ptr(cv))

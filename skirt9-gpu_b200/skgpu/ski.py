@@ -87,6 +87,25 @@ def sphere2d_grid(rmin_pc, rmax_pc, nr, ntheta):
             f'<meshPolar type="Mesh"><LinMesh numBins="{ntheta}"/></meshPolar></Sphere2DSpatialGrid>')
 
 
+def sphere3d_grid(rmin_pc, rmax_pc, nr, ntheta, nphi):
+    """Sphere3DSpatialGrid with linear radial, polar and azimuthal bins."""
+    return (f'<Sphere3DSpatialGrid minRadius="{rmin_pc} pc" maxRadius="{rmax_pc} pc">'
+            f'<meshRadial type="Mesh"><LinMesh numBins="{nr}"/></meshRadial>'
+            f'<meshPolar type="Mesh"><LinMesh numBins="{ntheta}"/></meshPolar>'
+            f'<meshAzimuthal type="Mesh"><LinMesh numBins="{nphi}"/></meshAzimuthal></Sphere3DSpatialGrid>')
+
+
+def disk_sphere3d(num_packets=1e5, npix=32, stats=True, rmin_pc=0.0):
+    """The disk scene of disk_cylinder2d on a Sphere3DSpatialGrid (r up to 4 pc in 12 bins, 9 polar and
+    8 azimuthal bins; with rmin 0 the grid adds its artificial inner hole), one frame at 60 degrees
+    with statistics plus one SED."""
+    mix = mean_list_mix([0.5, 0.6], [1, 1], [0.5, 0.5], [0.6, 0.6])
+    return simulation("OligoExtinctionOnly", num_packets, point_source(), expdisk_medium(1.0, 0.2, "pc", 1.0, mix),
+                      sphere3d_grid(rmin_pc, 4, 12, 9, 8),
+                      frame_instrument("i60", 60, 8, "pc", npix, stats) + sed_instrument("sed", 60, stats),
+                      num_density_samples=10)
+
+
 def disk_sphere2d(num_packets=1e5, npix=32, stats=True):
     """The disk scene of disk_cylinder2d on a Sphere2DSpatialGrid (r 0.05-4 pc in 20 bins, 15 polar
     bins; the grid adds the equatorial border), one frame at 60 degrees with statistics plus one SED."""
