@@ -44,6 +44,7 @@ extern "C" {
 #define SKGPU_GRID_CYLINDER2D 5
 #define SKGPU_GRID_SPHERE2D 6
 #define SKGPU_GRID_SPHERE3D 7
+#define SKGPU_GRID_CYLINDER3D 8
 
 /* traversal precision (path kernels and life cycle) */
 #define SKGPU_PREC_FP64_EXACT 0 /* FP64 with the reference generators' operation order, no FMA contraction */
@@ -176,6 +177,14 @@ int skgpu_upload_grid_sphere3d(skgpu_ctx* ctx, int32_t num_radial_borders, const
                                int32_t num_polar_borders, const double* polar_borders, const double* polar_cosines,
                                int32_t num_azimuth_borders, const double* azimuth_borders, const double* azimuth_sines,
                                const double* azimuth_cosines, double eps);
+/* Cylinder3DSpatialGrid: radial borders (with the artificial inner hole the grid adds when
+ * R_min = 0, has_hole = 0 then), azimuthal borders phi_0 = -pi .. pi with their sines and cosines,
+ * vertical borders and the grid's path step eps, as the grid holds them (its _Rv, _phiv, _sinv,
+ * _cosv, _zv, _eps, _hasHole: Cylinder3DSpatialGrid.cpp:20-60); cell index k + (j + i * Nphi) * Nz. */
+int skgpu_upload_grid_cylinder3d(skgpu_ctx* ctx, int32_t num_radial_borders, const double* radial_borders,
+                                 int32_t num_azimuth_borders, const double* azimuth_borders,
+                                 const double* azimuth_sines, const double* azimuth_cosines, int32_t num_z_borders,
+                                 const double* z_borders, double eps, int32_t has_hole);
 /* TetraMeshSpatialGrid: vertices, per tetrahedron its 4 vertex indices, and per face the outward
  * normal, the neighbouring tetrahedron (-1 on the hull) and its face index
  * (TetraMeshSpatialGrid.hpp:107-133). */
@@ -251,7 +260,7 @@ int skgpu_set_history_order(skgpu_ctx* ctx, int32_t mode);
  * and traversal precision, and guiding must be off. Each history draws from its own simulation's
  * random streams, so every simulation's tallies equal those of its own skgpu_run_primary; they land
  * in each context's device tallies. Counters and device time of the batch are those of the first
- * context (skgpu_get_counters, skgpu_last_run_ms). At most 64 contexts. */
+ * context (skgpu_get_counters, skgpu_last_run_ms). At most 48 contexts. */
 int skgpu_run_batch(skgpu_ctx* const* ctxs, int32_t n, const uint64_t* first, const uint64_t* count,
                     const uint64_t* total_packets);
 /* Adds the device tallies of one instrument into the caller's arrays and leaves the device

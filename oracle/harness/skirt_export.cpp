@@ -67,6 +67,7 @@
 #include "SpatialGridPath.hpp"
 #include "System.hpp"
 #include "Cylinder2DSpatialGrid.hpp"
+#include "Cylinder3DSpatialGrid.hpp"
 #include "Sphere1DSpatialGrid.hpp"
 #include "Sphere2DSpatialGrid.hpp"
 #include "Sphere3DSpatialGrid.hpp"
@@ -185,6 +186,19 @@ namespace
             std::vector<double> rv(begin(g->_Rv), end(g->_Rv)), zv(begin(g->_zv), end(g->_zv));
             writeVec(out + "/grid_rv.npy", rv);
             writeVec(out + "/grid_zv.npy", zv);
+            return;
+        }
+        if (auto g = dynamic_cast<Cylinder3DSpatialGrid*>(grid))
+        {
+            meta.kv("grid", "cylinder3d");
+            meta.kv("eps", g->_eps);
+            meta.kv("has_hole", g->_hasHole ? 1. : 0.);
+            auto vec = [](const Array& a) { return std::vector<double>(begin(a), end(a)); };
+            writeVec(out + "/grid_rv.npy", vec(g->_Rv));
+            writeVec(out + "/grid_phiv.npy", vec(g->_phiv));
+            writeVec(out + "/grid_sinv.npy", vec(g->_sinv));
+            writeVec(out + "/grid_cosv.npy", vec(g->_cosv));
+            writeVec(out + "/grid_zv.npy", vec(g->_zv));
             return;
         }
         if (auto g = dynamic_cast<Sphere3DSpatialGrid*>(grid))

@@ -126,6 +126,10 @@ typedef struct
     double *s3r, *s3t, *s3c, *s3p, *s3s, *s3k;
     int s3nr, s3nt, s3np;
     double s3eps;
+    /* cylinder3d */
+    double *c3r, *c3p, *c3s, *c3k, *c3z;
+    int c3nr, c3np, c3nz, c3hole;
+    double c3eps;
 } Grid;
 
 typedef struct
@@ -184,6 +188,7 @@ static void free_grid(Grid* g)
     free(g->crv); free(g->czv);
     free(g->s2r); free(g->s2t); free(g->s2c);
     free(g->s3r); free(g->s3t); free(g->s3c); free(g->s3p); free(g->s3s); free(g->s3k);
+    free(g->c3r); free(g->c3p); free(g->c3s); free(g->c3k); free(g->c3z);
     memset(g, 0, sizeof *g);
 }
 
@@ -381,6 +386,33 @@ int or_upload_grid_sphere3d(or_ctx* c, int32_t nrb, const double* rv, int32_t nt
     memcpy(g->ext, e, sizeof e);
     g->eps = eps;
     g->numCells = g->s3nr * g->s3nt * g->s3np;
+    c->hasGrid = 1;
+    return SKGPU_OK;
+}
+
+int or_upload_grid_cylinder3d(or_ctx* c, int32_t nrb, const double* rv, int32_t npb, const double* pv, const double* sv,
+                              const double* kv, int32_t nzb, const double* zv, double eps, int32_t hole)
+{
+    if (nrb < 2 || npb < 2 || nzb < 2 || !rv || !pv || !sv || !kv || !zv || !(rv[0] >= 0.) || !(eps > 0.))
+        return fail(c, SKGPU_ERR_ARG, "cylinder3d: bad borders");
+    free_grid(&c->g);
+    Grid* g = &c->g;
+    g->kind = SKGPU_GRID_CYLINDER3D;
+    g->c3nr = nrb - 1;
+    g->c3np = npb - 1;
+    g->c3nz = nzb - 1;
+    g->c3r = dup(rv, (size_t)nrb * sizeof(double));
+    g->c3p = dup(pv, (size_t)npb * sizeof(double));
+    g->c3s = dup(sv, (size_t)npb * sizeof(double));
+    g->c3k = dup(kv, (size_t)npb * sizeof(double));
+    g->c3z = dup(zv, (size_t)nzb * sizeof(double));
+    g->c3eps = eps;
+    g->c3hole = hole ? 1 : 0;
+    double r = rv[nrb - 1];
+    double e[6] = {-r, -r, zv[0], r, r, zv[nzb - 1]};
+    memcpy(g->ext, e, sizeof e);
+    g->eps = eps;
+    g->numCells = g->c3nr * g->c3np * g->c3nz;
     c->hasGrid = 1;
     return SKGPU_OK;
 }
@@ -1212,6 +1244,137 @@ static int sph3_next(const Grid* g, Gen* s)
     return 1;
 }
 
+/* NR::locateFail (SKIRT/utils/NR.hpp:186-191): -1 outside [xv[0], xv[n-1]] */
+static int nr_locate_fail(const double* xv, int n, double x)
+{
+    if (x > xv[n - 1]) return -1;
+    int jl = -1, ju = n - 1;
+    while (ju - jl > 1)
+    {
+        int jm = (ju + jl) >> 1;
+        if (x < xv[jm]) ju = jm; else jl = jm;
+    }
+    return jl;
+}
+
+/* Cylinder3DSpatialGrid::MySegmentGenerator (Cylinder3DSpatialGrid.cpp:180-440); EPS = 1e-12 (:19) */
+static double c3_cyl(const Grid* g, const Gen* s, double kq2, int i)
+{
+    if (fabs(kq2) < 1e-12) return 0.;
+    double b = s->rx * s->kx + s->ry * s->ky;
+    double c = s->rx * s->rx + s->ry * s->ry - g->c3r[i] * g->c3r[i];
+    return quad_sps(b / kq2, c / kq2);
+}
+static double c3_horiz(const Grid* g, const Gen* s, int k)
+{
+    if (fabs(s->kz) < 1e-12) return 0.;
+    return (g->c3z[k] - s->rz) / s->kz;
+}
+static int c3_indices(const Grid* g, Gen* s)
+{
+    double R = sqrt(s->rx * s->rx + s->ry * s->ry);
+    double phi = atan2(s->ry, s->rx);
+    s->i = nr_locate(g->c3r, g->c3nr + 1, R);
+    s->j = locate_clip(g->c3p, g->c3np + 1, phi);
+    s->k = nr_locate_fail(g->c3z, g->c3nz + 1, s->rz);
+    return s->i < g->c3nr && s->k >= 0;
+}
+static int cyl3_next(const Grid* g, Gen* s)
+{
+    int NR = g->c3nr, Np = g->c3np, Nz = g->c3nz;
+    double eps = g->c3eps;
+    if (s->state == OUTSIDE) return 0;
+    if (s->state == UNKNOWN)
+    {
+        s->cq = s->kx * s->kx + s->ky * s->ky;  /* kq2, kept for the rest of the path */
+        double cumds = 0.;
+        double R = sqrt(s->rx * s->rx + s->ry * s->ry);
+        if (R > g->c3r[NR])
+        {
+            double ds = c3_cyl(g, s, s->cq, NR);
+            if (ds <= 0.) { s->state = OUTSIDE; return 0; }
+            propagater(s, ds + eps);
+            cumds += ds;
+        }
+        if (s->rz < g->c3z[0])
+        {
+            double ds = c3_horiz(g, s, 0);
+            if (ds <= 0.) { s->state = OUTSIDE; return 0; }
+            propagater(s, ds + eps);
+            cumds += ds;
+        }
+        else if (s->rz > g->c3z[Nz])
+        {
+            double ds = c3_horiz(g, s, Nz);
+            if (ds <= 0.) { s->state = OUTSIDE; return 0; }
+            propagater(s, ds + eps);
+            cumds += ds;
+        }
+        if (!c3_indices(g, s)) { s->state = OUTSIDE; return 0; }
+        s->state = INSIDE;
+        if (cumds != 0.)
+        {
+            s->m = -1;
+            s->ds = cumds;
+            return 1;
+        }
+    }
+    double kq2 = s->cq;
+    if (s->i >= 0)
+    {
+        int icur = s->i, jcur = s->j, kcur = s->k;
+        double ds = DBL_MAX, t;
+        t = c3_cyl(g, s, kq2, icur);
+        if (t > 0. && t < ds) { ds = t; s->i = icur - 1; s->j = jcur; s->k = kcur; }
+        t = c3_cyl(g, s, kq2, icur + 1);
+        if (t > 0. && t < ds) { ds = t; s->i = icur + 1; s->j = jcur; s->k = kcur; }
+        t = s3_plane(s, g->c3s[jcur], g->c3k[jcur]);
+        if (t > 0. && t < ds) { ds = t; s->i = icur; s->j = jcur > 0 ? jcur - 1 : Np - 1; s->k = kcur; }
+        t = s3_plane(s, g->c3s[jcur + 1], g->c3k[jcur + 1]);
+        if (t > 0. && t < ds) { ds = t; s->i = icur; s->j = (jcur + 1) % Np; s->k = kcur; }
+        t = c3_horiz(g, s, kcur);
+        if (t > 0 && t < ds) { ds = t; s->i = icur; s->j = jcur; s->k = kcur - 1; }
+        t = c3_horiz(g, s, kcur + 1);
+        if (t > 0. && t < ds) { ds = t; s->i = icur; s->j = jcur; s->k = kcur + 1; }
+        if (ds == DBL_MAX) { s->state = OUTSIDE; return 0; }
+        s->m = kcur + (jcur + icur * Np) * Nz;  /* Cylinder3DSpatialGrid::index */
+        s->ds = ds;
+        propagater(s, ds + eps);
+        if (s->i >= NR || s->k < 0 || s->k >= Nz) s->state = OUTSIDE;
+    }
+    else if (!g->c3hole)
+    {
+        int kcur = s->k;
+        double ds = DBL_MAX, t;
+        t = c3_cyl(g, s, kq2, 0);
+        if (t > 0. && t < ds) ds = t;
+        t = c3_horiz(g, s, kcur);
+        if (t > 0 && t < ds) { ds = t; s->k = kcur - 1; }
+        t = c3_horiz(g, s, kcur + 1);
+        if (t > 0. && t < ds) { ds = t; s->k = kcur + 1; }
+        if (ds == DBL_MAX) { s->state = OUTSIDE; return 0; }
+        s->m = kcur + (s->j + 0 * Np) * Nz;  /* index(0, j, kcur) */
+        s->ds = ds;
+        propagater(s, ds + eps);
+        if (s->k == kcur)
+        {
+            if (!c3_indices(g, s)) { s->state = OUTSIDE; return 0; }
+        }
+        else if (s->k < 0 || s->k >= Nz)
+            s->state = OUTSIDE;
+    }
+    else
+    {
+        double ds = c3_cyl(g, s, kq2, 0);
+        if (ds <= 0.) { s->state = OUTSIDE; return 0; }
+        s->m = -1;
+        s->ds = ds;
+        propagater(s, ds + eps);
+        if (!c3_indices(g, s)) { s->state = OUTSIDE; return 0; }
+    }
+    return 1;
+}
+
 /* Cylinder2DSpatialGrid::MySegmentGenerator::moveInside (Cylinder2DSpatialGrid.cpp:124-198) */
 static int cyl_move_inside(const Grid* g, Gen* s)
 {
@@ -1363,6 +1526,7 @@ static int gen_next(const Grid* g, Gen* s)
         case SKGPU_GRID_CYLINDER2D: return cyl_next(g, s);
         case SKGPU_GRID_SPHERE2D: return sph2_next(g, s);
         case SKGPU_GRID_SPHERE3D: return sph3_next(g, s);
+        case SKGPU_GRID_CYLINDER3D: return cyl3_next(g, s);
     }
     return 0;
 }

@@ -43,6 +43,10 @@ int or_upload_grid_sphere3d(or_ctx* ctx, int32_t num_radial_borders, const doubl
                             int32_t num_polar_borders, const double* polar_borders, const double* polar_cosines,
                             int32_t num_azimuth_borders, const double* azimuth_borders, const double* azimuth_sines,
                             const double* azimuth_cosines, double eps);
+int or_upload_grid_cylinder3d(or_ctx* ctx, int32_t num_radial_borders, const double* radial_borders,
+                              int32_t num_azimuth_borders, const double* azimuth_borders, const double* azimuth_sines,
+                              const double* azimuth_cosines, int32_t num_z_borders, const double* z_borders, double eps,
+                              int32_t has_hole);
 int or_upload_grid_tetra(or_ctx* ctx, int32_t num_vertices, const double* vertices, int32_t num_tetra,
                          const int32_t* tetra_vertices, const double* face_normals, const int32_t* face_ntetra,
                          const int32_t* face_nface, const double* extent, double eps);

@@ -89,6 +89,14 @@ struct GridDev
     const double* s3k;
     int s3Nr, s3Nt, s3Np;
     double s3eps;
+    // 3D cylindrical: radial, azimuthal (+ sines, cosines) and vertical borders, path step, real hole
+    const double* c3r;
+    const double* c3p;
+    const double* c3s;
+    const double* c3k;
+    const double* c3z;
+    int c3Nr, c3Np, c3Nz, c3Hole;
+    double c3eps;
     const int* teBlkRep;         // teGridN^3: a tetrahedron overlapping each block (start of the walking locate)
 };
 
@@ -1270,6 +1278,202 @@ struct Sphere3DExact : GenBase
             return true;
         }
         double d = sphere(rv[0]);
+        if (d <= 0.)
+        {
+            state = GS_OUTSIDE;
+            return false;
+        }
+        m = -1;
+        ds = d;
+        propagater(xadd(d, eps));
+        if (!indices(g))
+        {
+            state = GS_OUTSIDE;
+            return false;
+        }
+        return true;
+    }
+};
+
+// ---------------------------------------------------------------------------------------------
+// 3D cylindrical grid (Cylinder3DSpatialGrid::MySegmentGenerator, Cylinder3DSpatialGrid.cpp:180-440):
+// the nearest positive intersection of the cell's two cylinders, two meridional planes and two
+// horizontal planes (EPS = 1e-12, :19); entry from outside by steps to the outer cylinder and the
+// bounding plane; in the artificial inner hole a segment of the hole's azimuth bin up to the hole
+// cylinder or a horizontal plane, in a real hole one empty step to the hole cylinder.
+// ---------------------------------------------------------------------------------------------
+// NR::locateFail (SKIRT/utils/NR.hpp:186-191): -1 outside [xv[0], xv[n - 1]]
+SKG_D int locateFailNR(const double* xv, int n, double x)
+{
+    if (x > xv[n - 1]) return -1;
+    int jl = -1, ju = n - 1;
+    while (ju - jl > 1)
+    {
+        int jm = (ju + jl) >> 1;
+        if (x < xv[jm])
+            ju = jm;
+        else
+            jl = jm;
+    }
+    return jl;
+}
+
+struct Cylinder3DExact : GenBase
+{
+    static constexpr int kMinBlocks = 3;
+    static constexpr int kRefillMin = 16;  // waiting lanes before a warp takes new tasks
+    double kq2;
+    int i, j, k;
+
+    SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz, int = -1)
+    {
+        startRay(x, y, z, ux, uy, uz);
+    }
+
+    SKG_D double cyl(const GridDev& g, int ii) const
+    {
+        if (fabs(kq2) < 1e-12) return 0.;
+        double b = xadd(xmul(rx, kx), xmul(ry, ky));
+        double c = xsub(xadd(xmul(rx, rx), xmul(ry, ry)), xmul(g.c3r[ii], g.c3r[ii]));
+        return quadSps(b / kq2, c / kq2);
+    }
+    SKG_D double meridional(const GridDev& g, int jj) const
+    {
+        double sn = g.c3s[jj], cs = g.c3k[jj];
+        double q = xsub(xmul(kx, sn), xmul(ky, cs));
+        if (fabs(q) < 1e-12) return 0.;
+        return -xsub(xmul(rx, sn), xmul(ry, cs)) / q;
+    }
+    SKG_D double horizontal(const GridDev& g, int kk) const
+    {
+        if (fabs(kz) < 1e-12) return 0.;
+        return xsub(g.c3z[kk], rz) / kz;
+    }
+    // setCellIndices with Position::cylindrical (Cylinder3DSpatialGrid.cpp:195-203)
+    SKG_D bool indices(const GridDev& g)
+    {
+        double R = sqrt(xadd(xmul(rx, rx), xmul(ry, ry)));
+        double phi = atan2(ry, rx);
+        i = locateNR(g.c3r, g.c3Nr + 1, R);
+        j = locateClip(g.c3p, g.c3Np + 1, phi);
+        k = locateFailNR(g.c3z, g.c3Nz + 1, rz);
+        return i < g.c3Nr && k >= 0;
+    }
+
+    SKG_D bool next(const GridDev& g)
+    {
+        if (state == GS_OUTSIDE) return false;
+        const int NR = g.c3Nr, Np = g.c3Np, Nz = g.c3Nz;
+        const double eps = g.c3eps;
+        if (state == GS_UNKNOWN)
+        {
+            kq2 = xadd(xmul(kx, kx), xmul(ky, ky));
+            double cumds = 0.;
+            double R = sqrt(xadd(xmul(rx, rx), xmul(ry, ry)));
+            if (R > g.c3r[NR])
+            {
+                double d = cyl(g, NR);
+                if (d <= 0.)
+                {
+                    state = GS_OUTSIDE;
+                    return false;
+                }
+                propagater(xadd(d, eps));
+                cumds = xadd(cumds, d);
+            }
+            if (rz < g.c3z[0])
+            {
+                double d = horizontal(g, 0);
+                if (d <= 0.)
+                {
+                    state = GS_OUTSIDE;
+                    return false;
+                }
+                propagater(xadd(d, eps));
+                cumds = xadd(cumds, d);
+            }
+            else if (rz > g.c3z[Nz])
+            {
+                double d = horizontal(g, Nz);
+                if (d <= 0.)
+                {
+                    state = GS_OUTSIDE;
+                    return false;
+                }
+                propagater(xadd(d, eps));
+                cumds = xadd(cumds, d);
+            }
+            if (!indices(g))
+            {
+                state = GS_OUTSIDE;
+                return false;
+            }
+            state = GS_INSIDE;
+            if (cumds != 0.)
+            {
+                m = -1;
+                ds = cumds;
+                return true;
+            }
+        }
+        if (i >= 0)
+        {
+            int icur = i, jcur = j, kcur = k;
+            double d = DBL_MAX, t;
+            t = cyl(g, icur);
+            if (t > 0. && t < d) { d = t; i = icur - 1; j = jcur; k = kcur; }
+            t = cyl(g, icur + 1);
+            if (t > 0. && t < d) { d = t; i = icur + 1; j = jcur; k = kcur; }
+            t = meridional(g, jcur);
+            if (t > 0. && t < d) { d = t; i = icur; j = jcur > 0 ? jcur - 1 : Np - 1; k = kcur; }
+            t = meridional(g, jcur + 1);
+            if (t > 0. && t < d) { d = t; i = icur; j = (jcur + 1) % Np; k = kcur; }
+            t = horizontal(g, kcur);
+            if (t > 0 && t < d) { d = t; i = icur; j = jcur; k = kcur - 1; }
+            t = horizontal(g, kcur + 1);
+            if (t > 0. && t < d) { d = t; i = icur; j = jcur; k = kcur + 1; }
+            if (d == DBL_MAX)
+            {
+                state = GS_OUTSIDE;
+                return false;
+            }
+            m = kcur + (jcur + icur * Np) * Nz;  // Cylinder3DSpatialGrid::index
+            ds = d;
+            propagater(xadd(d, eps));
+            if (i >= NR || k < 0 || k >= Nz) state = GS_OUTSIDE;
+            return true;
+        }
+        if (!g.c3Hole)
+        {
+            int kcur = k;
+            double d = DBL_MAX, t;
+            t = cyl(g, 0);
+            if (t > 0. && t < d) d = t;
+            t = horizontal(g, kcur);
+            if (t > 0 && t < d) { d = t; k = kcur - 1; }
+            t = horizontal(g, kcur + 1);
+            if (t > 0. && t < d) { d = t; k = kcur + 1; }
+            if (d == DBL_MAX)
+            {
+                state = GS_OUTSIDE;
+                return false;
+            }
+            m = kcur + j * Nz;  // index(0, j, kcur)
+            ds = d;
+            propagater(xadd(d, eps));
+            if (k == kcur)
+            {
+                if (!indices(g))
+                {
+                    state = GS_OUTSIDE;
+                    return false;
+                }
+            }
+            else if (k < 0 || k >= Nz)
+                state = GS_OUTSIDE;
+            return true;
+        }
+        double d = cyl(g, 0);
         if (d <= 0.)
         {
             state = GS_OUTSIDE;

@@ -664,4 +664,10 @@ struct Sphere3DFast : Sphere3DExact
     using Acc = float;
 };
 
+// 3D cylindrical grid, production: the reference-order FP64 crossings with FP32 accumulators
+struct Cylinder3DFast : Cylinder3DExact
+{
+    using Acc = float;
+};
+
 }  // namespace skg

@@ -23,6 +23,7 @@ cudaError_t launchTracePathsFP64(int precision, const GridDev& g, int n, const d
         case 5: tracePathsKernel<Cylinder2DExact><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
         case 6: tracePathsKernel<Sphere2DExact><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
         case 7: tracePathsKernel<Sphere3DExact><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
+        case 8: tracePathsKernel<Cylinder3DExact><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -44,6 +45,7 @@ cudaError_t launchOpticalDepthsFP64(int precision, const GridDev& g, const doubl
         case 5: opticalDepthKernel<Cylinder2DExact><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
         case 6: opticalDepthKernel<Sphere2DExact><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
         case 7: opticalDepthKernel<Sphere3DExact><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
+        case 8: opticalDepthKernel<Cylinder3DExact><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

@@ -720,6 +720,46 @@ int skgpu_upload_grid_sphere3d(skgpu_ctx* ctx, int32_t nrb, const double* rv, in
     return SKGPU_OK;
 }
 
+int skgpu_upload_grid_cylinder3d(skgpu_ctx* ctx, int32_t nrb, const double* rv, int32_t npb, const double* pv,
+                                 const double* sv, const double* kv, int32_t nzb, const double* zv, double eps,
+                                 int32_t has_hole)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (nrb < 2 || npb < 2 || nzb < 2 || !rv || !pv || !sv || !kv || !zv || !(rv[0] >= 0.) || !(eps > 0.))
+        return fail(ctx, SKGPU_ERR_ARG, "cylinder3d: need >= 2 radial, azimuthal and vertical borders, R >= 0 and eps > 0");
+    if (!finiteAll(rv, nrb) || !finiteAll(pv, npb) || !finiteAll(sv, npb) || !finiteAll(kv, npb) || !finiteAll(zv, nzb))
+        return fail(ctx, SKGPU_ERR_ARG, "cylinder3d: non-finite border");
+    for (int i = 1; i < nrb; ++i)
+        if (!(rv[i] > rv[i - 1])) return fail(ctx, SKGPU_ERR_ARG, "cylinder3d: radial borders must ascend");
+    for (int i = 1; i < npb; ++i)
+        if (!(pv[i] > pv[i - 1])) return fail(ctx, SKGPU_ERR_ARG, "cylinder3d: azimuthal borders must ascend");
+    for (int i = 1; i < nzb; ++i)
+        if (!(zv[i] > zv[i - 1])) return fail(ctx, SKGPU_ERR_ARG, "cylinder3d: vertical borders must ascend");
+    if (static_cast<int64_t>(nrb - 1) * (npb - 1) * (nzb - 1) > 2147483647LL) return fail(ctx, SKGPU_ERR_ARG, "cylinder3d: too many cells");
+    CK(cudaSetDevice(ctx->device));
+    freeGrid(ctx);
+    GridDev& g = ctx->g;
+    g.kind = SKGPU_GRID_CYLINDER3D;
+    double r = rv[nrb - 1];
+    double e[6] = {-r, -r, zv[0], r, r, zv[nzb - 1]};
+    for (int q = 0; q < 6; ++q) g.ext[q] = e[q];
+    g.eps = eps;
+    g.c3eps = eps;
+    g.c3Hole = has_hole ? 1 : 0;
+    g.c3Nr = nrb - 1;
+    g.c3Np = npb - 1;
+    g.c3Nz = nzb - 1;
+    g.numCells = g.c3Nr * g.c3Np * g.c3Nz;
+    int rc;
+    if ((rc = gridUpload(ctx, &g.c3r, rv, static_cast<size_t>(nrb)))) return rc;
+    if ((rc = gridUpload(ctx, &g.c3p, pv, static_cast<size_t>(npb)))) return rc;
+    if ((rc = gridUpload(ctx, &g.c3s, sv, static_cast<size_t>(npb)))) return rc;
+    if ((rc = gridUpload(ctx, &g.c3k, kv, static_cast<size_t>(npb)))) return rc;
+    if ((rc = gridUpload(ctx, &g.c3z, zv, static_cast<size_t>(nzb)))) return rc;
+    ctx->hasGrid = true;
+    return SKGPU_OK;
+}
+
 int skgpu_upload_grid_tetra(skgpu_ctx* ctx, int32_t num_vertices, const double* vertices, int32_t num_tetra,
                             const int32_t* tetra_vertices, const double* face_normals, const int32_t* face_ntetra,
                             const int32_t* face_nface, const double* extent, double eps)

@@ -77,7 +77,7 @@ struct Control
 // Batched runs trace the histories of several independent scenes (simulations) through one
 // wavefront: scene s owns the batch histories [prefix[s], prefix[s+1]), which are its segment
 // histories first[s], first[s] + 1, ... With one scene, sc is that scene and scenes is null.
-constexpr int MAX_BATCH = 64;
+constexpr int MAX_BATCH = 48;
 // buckets of the wavelength-ordered launch (top 14 bits of the FP32 wavelength)
 constexpr int ORDER_BUCKETS = 1 << 14;
 // a batch's scene table is staged in the traversal kernel's shared memory as int4 words, within the

@@ -20,6 +20,7 @@ cudaError_t runWaveFP32(int gridKind, const Wave& w, int numSMs, cudaStream_t s,
         case 5: return runWave<Cylinder2DFast>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer, cache);
         case 6: return runWave<Sphere2DFast>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer, cache);
         case 7: return runWave<Sphere3DFast>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer, cache);
+        case 8: return runWave<Cylinder3DFast>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer, cache);
     }
     return cudaErrorNotSupported;
 }
@@ -30,7 +31,7 @@ cudaError_t orderHistories(const Wave& w, unsigned short* keys, unsigned* counts
     cudaError_t e = cudaMemsetAsync(counts, 0, ORDER_BUCKETS * sizeof(unsigned), s);
     if (e != cudaSuccess) return e;
     int sceneBits = 0;
-    while ((1 << sceneBits) < w.nScenes) ++sceneBits;  // at most 6 (64 scenes)
+    while ((1 << sceneBits) < w.nScenes) ++sceneBits;  // at most 6 (48 scenes)
     orderKeyKernel<<<numSMs * 8, 256, 0, s>>>(w, sceneBits, keys, counts);
     orderScanKernel<<<1, 1024, 0, s>>>(counts, cursor);
     orderScatterKernel<<<numSMs * 8, 256, 0, s>>>(w.count, keys, cursor, order);

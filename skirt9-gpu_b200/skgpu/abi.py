@@ -16,7 +16,8 @@ LIB_PATH = os.path.join(PKG_ROOT, "lib", "libskgpu.so")
 
 # status codes
 OK, ERR_ARG, ERR_CUDA, ERR_STATE, ERR_TIMEOUT, ERR_DEVICE, ERR_UNSUPPORTED = range(7)
-GRID_CARTESIAN, GRID_OCTREE, GRID_VORONOI, GRID_TETRA, GRID_SPHERE1D, GRID_CYLINDER2D, GRID_SPHERE2D, GRID_SPHERE3D = range(8)
+(GRID_CARTESIAN, GRID_OCTREE, GRID_VORONOI, GRID_TETRA, GRID_SPHERE1D, GRID_CYLINDER2D, GRID_SPHERE2D, GRID_SPHERE3D,
+ GRID_CYLINDER3D) = range(9)
 PREC_FP64_EXACT, PREC_FP32 = 0, 1
 SRC_POINT, SRC_EXPDISK, SRC_RADIAL = 0, 1, 2
 SPEC_DISCRETE, SPEC_TABLE = 0, 1
@@ -118,6 +119,7 @@ SIGNATURES = {
     "upload_grid_cylinder2d": [_P, _I, _P, _I, _P],
     "upload_grid_sphere2d": [_P, _I, _P, _I, _P, _P],
     "upload_grid_sphere3d": [_P, _I, _P, _I, _P, _P, _I, _P, _P, _P, _D],
+    "upload_grid_cylinder3d": [_P, _I, _P, _I, _P, _P, _P, _I, _P, _D, _I],
     "upload_medium": [_P, _I, _P],
     "upload_dust_mix": [_P, _I, _P, _P, _P, _P],
     "upload_rf_grid": [_P, _I, _I, _P, _P],
@@ -200,6 +202,11 @@ class Backend:
         return rc
 
     # ---- typed helpers ----
+    def upload_grid_cylinder3d(self, rv, phiv, sinv, cosv, zv, eps, has_hole):
+        rv, pv, sv, kv, zv = f64(rv), f64(phiv), f64(sinv), f64(cosv), f64(zv)
+        self.call("upload_grid_cylinder3d", len(rv), _ptr(rv), len(pv), _ptr(pv), _ptr(sv), _ptr(kv), len(zv), _ptr(zv),
+                  float(eps), int(has_hole))
+
     def upload_grid_sphere3d(self, rv, thetav, cv, phiv, sinv, cosv, eps):
         rv, tv, cv, pv, sv, kv = f64(rv), f64(thetav), f64(cv), f64(phiv), f64(sinv), f64(cosv)
         self.call("upload_grid_sphere3d", len(rv), _ptr(rv), len(tv), _ptr(tv), _ptr(cv), len(pv), _ptr(pv), _ptr(sv),

@@ -62,6 +62,8 @@ class Scene:
             be.upload_grid_cylinder2d(g["rv"], g["zv"])
         elif k == abi.GRID_SPHERE2D:
             be.upload_grid_sphere2d(g["rv"], g["thetav"], g["cv"])
+        elif k == abi.GRID_CYLINDER3D:
+            be.upload_grid_cylinder3d(g["rv"], g["phiv"], g["sinv"], g["cosv"], g["zv"], g["eps"], g["has_hole"])
         elif k == abi.GRID_SPHERE3D:
             be.upload_grid_sphere3d(g["rv"], g["thetav"], g["cv"], g["phiv"], g["sinv"], g["cosv"], g["eps"])
         else:
@@ -239,6 +241,10 @@ class Scene:
             sc.grid = dict(kind=abi.GRID_SPHERE1D, rv=L("grid_rv"), extent=ext)
         elif kind == "cylinder2d":
             sc.grid = dict(kind=abi.GRID_CYLINDER2D, rv=L("grid_rv"), zv=L("grid_zv"), extent=ext)
+        elif kind == "cylinder3d":
+            sc.grid = dict(kind=abi.GRID_CYLINDER3D, rv=L("grid_rv"), phiv=L("grid_phiv"), sinv=L("grid_sinv"),
+                           cosv=L("grid_cosv"), zv=L("grid_zv"), eps=float(meta["eps"]),
+                           has_hole=int(float(meta["has_hole"])), extent=ext)
         elif kind == "sphere3d":
             sc.grid = dict(kind=abi.GRID_SPHERE3D, rv=L("grid_rv"), thetav=L("grid_thetav"), cv=L("grid_cv"),
                            phiv=L("grid_phiv"), sinv=L("grid_sinv"), cosv=L("grid_cosv"), eps=float(meta["eps"]),

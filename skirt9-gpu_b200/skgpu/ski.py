@@ -106,6 +106,25 @@ def disk_sphere3d(num_packets=1e5, npix=32, stats=True, rmin_pc=0.0):
                       num_density_samples=10)
 
 
+def cylinder3d_grid(rmin_pc, rmax_pc, zmin_pc, zmax_pc, nr, nphi, nz):
+    """Cylinder3DSpatialGrid with linear radial, azimuthal and vertical bins."""
+    return (f'<Cylinder3DSpatialGrid minRadius="{rmin_pc} pc" maxRadius="{rmax_pc} pc" minZ="{zmin_pc} pc" '
+            f'maxZ="{zmax_pc} pc"><meshRadial type="Mesh"><LinMesh numBins="{nr}"/></meshRadial>'
+            f'<meshAzimuthal type="Mesh"><LinMesh numBins="{nphi}"/></meshAzimuthal>'
+            f'<meshZ type="Mesh"><LinMesh numBins="{nz}"/></meshZ></Cylinder3DSpatialGrid>')
+
+
+def disk_cylinder3d(num_packets=1e5, npix=32, stats=True, rmin_pc=0.0):
+    """The disk scene of disk_cylinder2d on a Cylinder3DSpatialGrid (R up to 4 pc in 12 bins with the
+    grid's artificial inner hole, 8 azimuthal bins, z -1..1 pc in 10 bins), one frame at 60 degrees
+    with statistics plus one SED."""
+    mix = mean_list_mix([0.5, 0.6], [1, 1], [0.5, 0.5], [0.6, 0.6])
+    return simulation("OligoExtinctionOnly", num_packets, point_source(), expdisk_medium(1.0, 0.2, "pc", 1.0, mix),
+                      cylinder3d_grid(rmin_pc, 4, -1, 1, 12, 8, 10),
+                      frame_instrument("i60", 60, 8, "pc", npix, stats) + sed_instrument("sed", 60, stats),
+                      num_density_samples=10)
+
+
 def disk_sphere2d(num_packets=1e5, npix=32, stats=True):
     """The disk scene of disk_cylinder2d on a Sphere2DSpatialGrid (r 0.05-4 pc in 20 bins, 15 polar
     bins; the grid adds the equatorial border), one frame at 60 degrees with statistics plus one SED."""

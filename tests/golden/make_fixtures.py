@@ -16,9 +16,10 @@ Fixtures written:
   shell_c16_explicit.npz  reference frame/SED statistics of the same scene with explicit absorption
                      (forced and free propagation), 2e5 packets each; `python
                      tests/golden/make_fixtures.py explicit` writes only this one
-  paths_sphere1d.npz, paths_cylinder2d.npz, paths_sphere2d.npz, paths_sphere3d.npz  path fixtures
-                     that also hold reference frame/SED statistics of the same scene (arguments
-                     `sphere1d`, `cylinder2d`, `sphere2d`, `sphere3d` write only them)
+  paths_sphere1d.npz, paths_cylinder2d.npz, paths_sphere2d.npz, paths_sphere3d.npz,
+  paths_cylinder3d.npz  path fixtures that also hold reference frame/SED statistics of the same
+                     scene (arguments `sphere1d`, `cylinder2d`, `sphere2d`, `sphere3d`, `cylinder3d`
+                     write only them)
 """
 import os
 import shutil
@@ -121,6 +122,7 @@ def main():
     cylinder2d_fixture()
     sphere2d_fixture()
     sphere3d_fixture()
+    cylinder3d_fixture()
 
     # dust shell, 16^3 grid, 64^2 frame + SED: scene export + reference statistics (2e5 packets)
     npp = 200000
@@ -239,6 +241,23 @@ def sphere3d_fixture(rng=None):
     reference_stats("paths_sphere3d.npz", ski.disk_sphere3d(200000), "i60", 200000)
 
 
+def cylinder3d_fixture(rng=None):
+    """Cylinder3DSpatialGrid (the disk scene, R up to 4 pc in 12 bins with the grid's artificial inner
+    hole, 8 azimuthal bins, z -1..1 pc in 10 bins): scene export and path fixture (random rays plus
+    vertical rays through the hole, radial and tangent rays, starts outside), and reference
+    statistics of a single-threaded 2e5-packet run."""
+    rng = rng if rng is not None else np.random.default_rng(20260106)
+    rays = random_rays(rng, 300, 4.5 * PC)
+    extra = []
+    for k in ((0, 0, 1), (0, 0, -1), (1, 0, 0), (0.6, 0.8, 0.0), (0.3, 0.0, 0.95), (-0.5, 0.5, -0.7071067811865476)):
+        k = np.array(k, float) / np.linalg.norm(k)
+        for p in ((0.0, 0.0, 0.0), (1.0, 0.5, 0.3), (5.0, 0.0, 0.1), (0.0, 0.0, -2.0), (-0.02, 0.01, 0.0)):
+            extra.append(np.r_[np.array(p) * PC, k])
+    rays = np.vstack([rays, np.array(extra)])
+    path_fixture("cylinder3d", ski.disk_cylinder3d(1e4), rays)
+    reference_stats("paths_cylinder3d.npz", ski.disk_cylinder3d(200000), "i60", 200000)
+
+
 def reference_stats(fixture, ski_text, frame_name, npp):
     """Adds the frame and SED statistics of a single-threaded reference run of ski_text to a
     fixture; the run's stats scale c is recovered from its total image (MJy/sr per raw W from the
@@ -292,6 +311,8 @@ if __name__ == "__main__":
         sphere2d_fixture()
     elif sys.argv[1:] == ["sphere3d"]:
         sphere3d_fixture()
+    elif sys.argv[1:] == ["cylinder3d"]:
+        cylinder3d_fixture()
     elif sys.argv[1:] == ["explicit"]:
         z = np.load(os.path.join(OUT, "shell_c16.npz"))
         meta = __import__("skgpu").Scene.read_export(z)[0]

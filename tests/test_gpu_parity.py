@@ -65,7 +65,7 @@ def test_gpu_free_propagation_matches_oracle(golden, gpu_backend, oracle_backend
     assert_close_runs(rg, ro)
 
 
-@pytest.mark.parametrize("name", ["octree", "voronoi", "tetra", "cartesian_selftest", "sphere1d", "cylinder2d", "sphere2d", "sphere3d"])
+@pytest.mark.parametrize("name", ["octree", "voronoi", "tetra", "cartesian_selftest", "sphere1d", "cylinder2d", "sphere2d", "sphere3d", "cylinder3d"])
 def test_gpu_lifecycle_matches_oracle_grids(golden, gpu_backend, oracle_backend, name):
     sc = Scene.from_export(golden(f"paths_{name}.npz"))
     sc.instruments[0]["stats"] = 1
@@ -237,7 +237,7 @@ def test_gpu_fp32_octree_lifecycle_close_to_fp64(gpu_backend):
     assert np.median(np.abs(r32.rf[lit] / r64.rf[lit] - 1)) < 1e-3
 
 
-@pytest.mark.parametrize("name", ["sphere1d", "cylinder2d", "sphere2d", "sphere3d"])
+@pytest.mark.parametrize("name", ["sphere1d", "cylinder2d", "sphere2d", "sphere3d", "cylinder3d"])
 def test_gpu_curvilinear_lifecycle_matches_reference_statistics(golden, gpu_backend, name):
     """The dust shell on a Sphere1DSpatialGrid and the dust disk on a Cylinder2DSpatialGrid, both
     traversal precisions: frame and SED against the reference's own run of the same scene."""
