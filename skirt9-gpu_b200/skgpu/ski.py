@@ -106,6 +106,15 @@ def disk_sphere3d(num_packets=1e5, npix=32, stats=True, rmin_pc=0.0):
                       num_density_samples=10)
 
 
+def disk_scene(grid_xml, num_packets=1e5, npix=32, stats=True):
+    """The disk scene of disk_cylinder2d (exponential dust disk hR 1 pc, hz 0.2 pc, face-on tau 1,
+    central point source, one 60-degree frame of 8 pc with statistics plus one SED) on any grid."""
+    mix = mean_list_mix([0.5, 0.6], [1, 1], [0.5, 0.5], [0.6, 0.6])
+    return simulation("OligoExtinctionOnly", num_packets, point_source(), expdisk_medium(1.0, 0.2, "pc", 1.0, mix),
+                      grid_xml, frame_instrument("i60", 60, 8, "pc", npix, stats) + sed_instrument("sed", 60, stats),
+                      num_density_samples=10)
+
+
 def cylinder3d_grid(rmin_pc, rmax_pc, zmin_pc, zmax_pc, nr, nphi, nz):
     """Cylinder3DSpatialGrid with linear radial, azimuthal and vertical bins."""
     return (f'<Cylinder3DSpatialGrid minRadius="{rmin_pc} pc" maxRadius="{rmax_pc} pc" minZ="{zmin_pc} pc" '

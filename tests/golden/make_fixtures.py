@@ -20,6 +20,8 @@ Fixtures written:
   paths_cylinder3d.npz  path fixtures that also hold reference frame/SED statistics of the same
                      scene (arguments `sphere1d`, `cylinder2d`, `sphere2d`, `sphere3d`, `cylinder3d`
                      write only them)
+  stats_octree.npz, stats_voronoi.npz, stats_tetra.npz  the disk scene on these grids (scene export)
+                     with reference frame/SED statistics (argument `gridstats`)
 """
 import os
 import shutil
@@ -123,6 +125,7 @@ def main():
     sphere2d_fixture()
     sphere3d_fixture()
     cylinder3d_fixture()
+    grid_stats_fixtures()
 
     # dust shell, 16^3 grid, 64^2 frame + SED: scene export + reference statistics (2e5 packets)
     npp = 200000
@@ -258,6 +261,25 @@ def cylinder3d_fixture(rng=None):
     reference_stats("paths_cylinder3d.npz", ski.disk_cylinder3d(200000), "i60", 200000)
 
 
+def grid_stats_fixtures():
+    """The disk scene on the octree, Voronoi and tetrahedral grids of the path fixtures (4 pc box):
+    scene exports plus the statistics of single-threaded 2e5-packet reference runs
+    (stats_<grid>.npz), so that the life cycle on these grids is pinned against the reference's own
+    runs and not only through the oracle."""
+    grids = {
+        "octree": ski.octree_grid(4, "pc", 6, 1e-3),
+        "voronoi": ski.voronoi_grid(4, "pc", 2000),
+        "tetra": ski.tetra_grid(4, "pc", 2000),
+    }
+    for name, grid in grids.items():
+        with tempfile.TemporaryDirectory() as tmp:
+            data = export(ski.disk_scene(grid, 1e4), tmp)
+        path = os.path.join(OUT, f"stats_{name}.npz")
+        np.savez_compressed(path, **data)
+        reference_stats(f"stats_{name}.npz", ski.disk_scene(grid, 200000), "i60", 200000)
+        print(f"stats_{name} written")
+
+
 def reference_stats(fixture, ski_text, frame_name, npp):
     """Adds the frame and SED statistics of a single-threaded reference run of ski_text to a
     fixture; the run's stats scale c is recovered from its total image (MJy/sr per raw W from the
@@ -313,6 +335,8 @@ if __name__ == "__main__":
         sphere3d_fixture()
     elif sys.argv[1:] == ["cylinder3d"]:
         cylinder3d_fixture()
+    elif sys.argv[1:] == ["gridstats"]:
+        grid_stats_fixtures()
     elif sys.argv[1:] == ["explicit"]:
         z = np.load(os.path.join(OUT, "shell_c16.npz"))
         meta = __import__("skgpu").Scene.read_export(z)[0]

@@ -143,3 +143,25 @@ def test_oracle_curvilinear_lifecycle_matches_reference_statistics(golden, oracl
     sst = res[1]["stats"][:, 0]
     rs = z["ref_sedstats"]
     assert abs(zscores(sst[1:2], sst[2:3], n, rs[1:2], rs[2:3], n)[0]) < 4
+
+
+@pytest.mark.parametrize("name", ["octree", "voronoi", "tetra"])
+def test_oracle_grid_lifecycle_matches_reference_statistics(golden, oracle_backend, name):
+    """The dust disk on the reference's own octree, Voronoi and tetrahedral grids: the oracle's frame
+    and SED against the reference's run of the same scene (z-scores). With the GPU life cycle equal
+    to the oracle history by history on these grids, this pins the GPU too."""
+    z = golden(f"stats_{name}.npz")
+    sc = Scene.from_export(z)
+    sc.instruments[0]["stats"] = 1
+    sc.instruments[1]["stats"] = 1
+    sc.upload(oracle_backend)
+    n = int(z["ref_npp"])
+    res = sc.run(oracle_backend, n, seed=31)
+    st = res[0]["stats"][:, 0]
+    ref = z["ref_frame_w"]
+    zs = zscores(st[1], st[2], n, ref[1], ref[2], n)
+    assert len(zs) > 300
+    assert abs(zs.mean()) < 0.1 and 0.85 < zs.std() < 1.15
+    sst = res[1]["stats"][:, 0]
+    rs = z["ref_sedstats"]
+    assert abs(zscores(sst[1:2], sst[2:3], n, rs[1:2], rs[2:3], n)[0]) < 4
