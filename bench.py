@@ -179,7 +179,7 @@ def reference_batch(indices, fraction, cores):
     return tot_n / max(tot_s, 1e-3), tot_n, tot_s
 
 
-def cpu_baseline(name, budget_s=20.0):
+def cpu_baseline(name, sample_s=20.0):
     """The reference's own multithreaded CPU path on the host cores, on a bounded sample."""
     cores = os.cpu_count() or 1
     if name == "batch":
@@ -187,7 +187,7 @@ def cpu_baseline(name, budget_s=20.0):
             return {"value": None, "error": "reference build oracle/_ref missing"}
         idx = [0, 4, 8, 12]
         rate, _, _ = reference_batch(idx[:1], 0.0025, cores)
-        frac = min(1.0, rate * budget_s / 71e6 * 4)  # about budget_s of primary emission over 4 simulations
+        frac = min(1.0, rate * sample_s / 71e6 * 4)  # about sample_s of primary emission over 4 simulations
         rate, n, secs = reference_batch(idx, frac, cores)
         return {"value": rate, "unit": "packets/s", "cores": cores, "kind": "reference",
                 "sample": f"simulations {idx} of the batch, {frac:.4f} of their packets ({n} in all), one skirt -t "
@@ -195,7 +195,7 @@ def cpu_baseline(name, budget_s=20.0):
     if os.path.exists(REF_SKIRT):
         probe = 20000
         rate, secs = reference_run(reference_ski(name, probe), probe, cores)
-        npp = int(min(5e7, max(probe, rate * budget_s)))
+        npp = int(min(5e7, max(probe, rate * sample_s)))
         rate, secs = reference_run(reference_ski(name, npp), npp, cores)
         return {"value": rate, "unit": "packets/s", "cores": cores, "kind": "reference",
                 "sample": f"{npp} packets of the same workload, skirt -t {cores}, primary-emission segment "

@@ -113,7 +113,7 @@ struct CartesianFast : FastBase<Real>
 // neighbour-list base) and wall counts are held in registers; a crossing loads the ids of the exit
 // wall's neighbours and their records until one contains the exit point, and that record becomes
 // the current one (two dependent loads per crossing, all from a working set that stays in L2).
-// resident 256-thread blocks per SM requested for the FP32 octree trace kernel (register budget)
+// resident 256-thread blocks per SM requested for the FP32 octree trace kernel (register limit)
 #ifndef SKG_OCTREE32_MIN_BLOCKS
 #define SKG_OCTREE32_MIN_BLOCKS 4
 #endif
