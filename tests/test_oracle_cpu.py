@@ -165,3 +165,22 @@ def test_oracle_grid_lifecycle_matches_reference_statistics(golden, oracle_backe
     sst = res[1]["stats"][:, 0]
     rs = z["ref_sedstats"]
     assert abs(zscores(sst[1:2], sst[2:3], n, rs[1:2], rs[2:3], n)[0]) < 4
+
+
+def test_oracle_curvilinear_uploads_validate_their_borders(oracle_backend):
+    """The curvilinear grid uploads (mirrored by the CUDA library's checks) refuse descending borders
+    and negative inner radii with SKGPU_ERR_ARG."""
+    from skgpu import SkgpuError
+    be = oracle_backend
+    bad = [
+        lambda: be.upload_grid_sphere1d([0.0, 2.0, 1.0]),
+        lambda: be.upload_grid_sphere1d([-1.0, 1.0]),
+        lambda: be.upload_grid_cylinder2d([0.0, 1.0], [1.0, -1.0]),
+        lambda: be.upload_grid_sphere2d([0.0, 1.0], [0.0, 2.0, 1.0], [1.0, 0.0, -1.0]),
+    ]
+    for f in bad:
+        with pytest.raises(SkgpuError) as e:
+            f()
+        assert e.value.code == abi.ERR_ARG
+    be.upload_grid_sphere1d([0.0, 0.5, 1.0])
+    be.upload_grid_cylinder2d([0.0, 1.0, 2.0], [-1.0, 0.0, 1.0])
