@@ -486,9 +486,13 @@ def main():
 
     # end to end through the C ABI with host buffers, as the SKIRT bridge uses it: the medium state
     # goes in from pinned host memory, every tally (instrument totals and statistics, radiation
-    # field) is added into the caller's preallocated host arrays, every step
+    # field) is added into the caller's preallocated host arrays, every step. With several ranks the
+    # segment's tallies are first summed over the ranks on the device (one NCCL all-reduce per tally
+    # buffer over NVLink, the segment-end sum of the reference's ProcessManager) and rank 0 fetches
+    # the sum.
     e2e = None
     if not args.no_e2e:
+        from skgpu import sharding
         dens = torch.from_numpy(np.ascontiguousarray(sc.density)).pin_memory().numpy()
         sizes = [sc.instrument_size(i) for i in range(len(sc.instruments))]
         stats = [bool(sc.instruments[i].get("stats")) for i in range(len(sizes))]
@@ -498,6 +502,7 @@ def main():
         h2d = dens.nbytes
         d2h = sum(8 * n + (40 * n if st else 0) for n, st in zip(sizes, stats)) + 8 * rf_len
         e2e_times = []
+        reduced = 0
         # one untimed call first: the fetch's pinned staging buffers are allocated on first use
         for it in range(1 + max(1, min(args.steps, 3))):
             torch.cuda.synchronize()
@@ -505,15 +510,20 @@ def main():
             be.clear_tallies()
             be.upload_medium(dens)
             be.run_primary(first, per_gpu, npp_total)
-            for i, n in enumerate(sizes):
-                be.fetch_instrument(i, n, stats=stats[i], out=host[i][0], out_stats=host[i][1])
-            if rf_len:
-                be.fetch_radiation_field(rf_len, out=rf_host)
+            if world > 1:
+                reduced = sharding.allreduce_device_tallies(be, f"cuda:{local}")
+            if rank == 0:
+                for i, n in enumerate(sizes):
+                    be.fetch_instrument(i, n, stats=stats[i], out=host[i][0], out_stats=host[i][1])
+                if rf_len:
+                    be.fetch_radiation_field(rf_len, out=rf_host)
             torch.cuda.synchronize()
             if it > 0:
                 e2e_times.append(time.perf_counter() - t0)
         e2e_s = max_over_ranks(statistics.median(e2e_times), world, local)
         e2e = {"value": npp_total / e2e_s, "unit": "packets/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+        if world > 1:
+            e2e["allreduce_bytes_per_step_per_rank"] = reduced
 
     if rank == 0:
         line = result_line(args, name, world, value, total_ms, trace_ms, trace_launches, counters, sc.grid["kind"],

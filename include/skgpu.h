@@ -54,6 +54,11 @@ extern "C" {
 #define SKGPU_SRC_POINT 0   /* PointSource: fixed position */
 #define SKGPU_SRC_EXPDISK 1 /* GeometricSource + ExpDiskGeometry: params hR, hz, Rmin, Rmax, zmax */
 #define SKGPU_SRC_RADIAL 2  /* GeometricSource with a spherical geometry (Sersic, Shell, ...): tabulated radial CDF */
+/* GeometricSource with a spherical geometry whose radius is drawn by log-log interpolation in a
+ * cumulative-mass table, as SersicGeometry::randomRadius does with SersicFunction::inverseMass
+ * (SKIRT/core/SersicGeometry.cpp:41-45, SKIRT/utils/SersicFunction.cpp): radial_r holds the
+ * dimensionless radii s_i, radial_P the cumulative masses M_i, geometry[0] the scale (r = scale * s) */
+#define SKGPU_SRC_RADIAL_LOGLOG 3
 
 /* source spectral models */
 #define SKGPU_SPEC_DISCRETE 0 /* oligochromatic: pick one of n wavelengths uniformly, weight per wavelength */
@@ -222,6 +227,13 @@ int skgpu_set_options(skgpu_ctx* ctx, const skgpu_options* options);
  * storage, scattering peel-off, HG scattering) of histories [first, first+count) of a segment
  * of total_packets packets, adding into the device tallies. */
 int skgpu_run_primary(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t total_packets);
+/* Source launch only: histories [first, first+count) of a segment of total_packets packets go through
+ * the launch of skgpu_run_primary (the device form of SourceSystem::launch -> NormalizedSource::launch
+ * -> PointSource / GeometricSource::launchNormalized, SKIRT/core/SourceSystem.cpp,
+ * NormalizedSource.cpp:73-110) and are not traced. out receives 8 doubles per history: wavelength,
+ * luminosity times total_packets, position (3) and direction (3), the record the reference's launch
+ * writes into a PhotonPacket. Needs the sources and options; used to test the launch distributions. */
+int skgpu_probe_launch(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t total_packets, double* out);
 /* Same life cycle as skgpu_run_primary for callers that must not allocate device memory while it
  * runs: for example a host code that hands the GPU to this library between phases of its own
  * memory manager, or that cannot afford the implicit device synchronisation of cudaMalloc/cudaFree
@@ -235,8 +247,12 @@ int skgpu_run_primary(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t t
  * (scene, tallies, radiation-field tally) must have been set up by the upload calls, skgpu_set_options
  * and skgpu_clear_tallies beforehand. The first call on a device looks up the array's device
  * address (cudaGetSymbolAddress) with that device current; make that first call before any stream
- * capture. Calls share the one array and the call re-initialises what must start at zero; calls that
- * overlap on the GPU (other threads, other contexts on the same device) race on it. */
+ * capture. Every call looks the address up again with the caller's device current (a lookup
+ * allocates nothing once the module is loaded), so the address stays right after a device reset or
+ * under another context. The histories run in index order (the wavelength-ordered launch of
+ * skgpu_set_history_order needs device memory per history) with the context's launch shape. Calls
+ * share the one array and the call re-initialises what must start at zero; calls that overlap on the
+ * GPU (other threads, other contexts on the same device) race on it. */
 #define SKGPU_NOALLOC_MAX_SLOTS 32768
 #define SKGPU_NOALLOC_MAX_GROUPS 4
 #define SKGPU_NOALLOC_SCRATCH_BYTES (48u * 1024u * 1024u)
@@ -274,6 +290,14 @@ int skgpu_fetch_instrument_components(skgpu_ctx* ctx, int32_t instrument, double
 /* Adds the radiation-field tally (num_cells * num_rf_bins, index m*num_rf_bins + ell) into rf. */
 int skgpu_fetch_radiation_field(skgpu_ctx* ctx, double* rf);
 int skgpu_clear_tallies(skgpu_ctx* ctx);
+/* The device tally buffers of the context, for a collective across GPUs before one rank fetches
+ * (the segment-end sum of MonteCarloSimulation's ProcessManager::sumToAll / sumToRoot over the
+ * instruments and MediumSystem::communicateRadiationField, MediumSystem.cpp:2524-2547, done on the
+ * device, e.g. one NCCL all-reduce over NVLink): *num_buffers receives their number; when ptrs and
+ * lengths hold max_buffers >= that many entries they receive the device pointers (FP64 arrays,
+ * instrument buffers in upload order, then the radiation field) and their lengths in doubles. The
+ * pointers stay valid until the instruments, medium or radiation-field grid are uploaded again. */
+int skgpu_tally_buffers(skgpu_ctx* ctx, int32_t max_buffers, void** ptrs, uint64_t* lengths, int32_t* num_buffers);
 int skgpu_get_counters(skgpu_ctx* ctx, skgpu_counters* out);
 /* Milliseconds of device time of the last skgpu_run_primary (CUDA events on the launch stream). */
 int skgpu_last_run_ms(skgpu_ctx* ctx, double* ms);

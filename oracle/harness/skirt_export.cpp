@@ -10,7 +10,12 @@
 //   - the spatial grid (Cartesian borders, octree nodes + overlap-sorted neighbour lists,
 //     Voronoi sites + neighbour lists, tetrahedra + faces);
 //   - the medium state (number density per cell and medium) and dust-mix tables;
-//   - instrument and source parameters;
+//   - instrument and source parameters (for geometric sources the exponential-disk parameters or the
+//     Sersic cumulative-mass table, for black-body SEDs the launch table, and the wavelength bias);
+//   - a launch probe: SourceSystem::launch of SKGPU_PROBE_N packets (default 1000), src_probe.npy;
+//   - with SKGPU_EXPORT_RUN=1, the raw detector arrays of a single-threaded primary-emission segment
+//     (totals and per-history statistics sums, inst<i>_*.npy) and its primary radiation field
+//     MediumSystem::_rf1 (rf1.npy);
 //   - optionally, for each ray (x,y,z,kx,ky,kz) in rays.npy, the reference path segments
 //     (m, ds) produced by SpatialGrid::createPathSegmentGenerator() -> next(), i.e. by the
 //     reference's own CPU generators (CartesianSpatialGrid.cpp:77-155, TreeSpatialGrid.cpp:143-228,
@@ -23,6 +28,7 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <map>
@@ -44,6 +50,14 @@
 #define private public
 #define protected public
 #include "BuildInfo.hpp"
+#include "BlackBodySED.hpp"
+#include "DefaultWavelengthDistribution.hpp"
+#include "ExpDiskGeometry.hpp"
+#include "GeometricSource.hpp"
+#include "LogWavelengthDistribution.hpp"
+#include "NormalizedSource.hpp"
+#include "SersicFunction.hpp"
+#include "SersicGeometry.hpp"
 #include "CartesianSpatialGrid.hpp"
 #include "Configuration.hpp"
 #include "DisjointWavelengthGrid.hpp"
@@ -431,7 +445,13 @@ namespace
         writeNpy(out + "/src_probe.npy", v.data(), {num, 8});
     }
 
-    void exportSources(MonteCarloSimulation* sim, Meta& meta)
+    // Per source: type, luminosity fraction and launch weight; for normalised sources the wavelength
+    // bias (NormalizedSource::_xi) and the range of a log-uniform bias distribution; for black-body
+    // SEDs the launch table BlackBodySED holds (_lambdav, _pv, _Pv: PlanckFunction::cdf) as
+    // source<h>_sed_{lambda,p,P}.npy; for geometric sources the exponential-disk parameters
+    // (ExpDiskGeometry) or the Sersic index, effective radius and the cumulative-mass table of
+    // SersicFunction (_sv, _Mv: source<h>_sersic_{s,M}.npy).
+    void exportSources(MonteCarloSimulation* sim, const std::string& out, Meta& meta)
     {
         auto ss = sim->sourceSystem();
         meta.kv("source_total_luminosity", ss->_L);
@@ -442,7 +462,87 @@ namespace
             meta.kv(key + "_type", ss->_sources[h]->type());
             meta.kv(key + "_lfrac", ss->_Lv[h]);
             meta.kv(key + "_weight", ss->_Wv[h]);
+            auto ns = dynamic_cast<NormalizedSource*>(ss->_sources[h]);
+            if (!ns) continue;
+            meta.kv(key + "_xi", ns->_xi);
+            if (auto ld = dynamic_cast<LogWavelengthDistribution*>(ns->_biasDistribution))
+            {
+                meta.kv(key + "_bias_min", ld->range().min());
+                meta.kv(key + "_bias_max", ld->range().max());
+            }
+            else if (auto dd = dynamic_cast<DefaultWavelengthDistribution*>(ns->_biasDistribution))
+            {
+                // log-uniform over the source wavelength range (DefaultWavelengthDistribution.cpp:17-39)
+                meta.kv(key + "_bias_min", dd->_range.min());
+                meta.kv(key + "_bias_max", dd->_range.max());
+            }
+            if (auto bb = dynamic_cast<BlackBodySED*>(ns->_sed))
+            {
+                meta.kv(key + "_sed", "blackbody");
+                writeVec(out + "/" + key + "_sed_lambda.npy", std::vector<double>(begin(bb->_lambdav), end(bb->_lambdav)));
+                writeVec(out + "/" + key + "_sed_p.npy", std::vector<double>(begin(bb->_pv), end(bb->_pv)));
+                writeVec(out + "/" + key + "_sed_P.npy", std::vector<double>(begin(bb->_Pv), end(bb->_Pv)));
+            }
+            auto gs = dynamic_cast<GeometricSource*>(ss->_sources[h]);
+            if (!gs) continue;
+            if (auto ed = dynamic_cast<ExpDiskGeometry*>(gs->_geometry))
+            {
+                meta.kv(key + "_geometry", "expdisk");
+                meta.kv(key + "_hR", ed->_hR);
+                meta.kv(key + "_hz", ed->_hz);
+                meta.kv(key + "_Rmin", ed->_Rmin);
+                meta.kv(key + "_Rmax", ed->_Rmax);
+                meta.kv(key + "_zmax", ed->_zmax);
+            }
+            else if (auto sg = dynamic_cast<SersicGeometry*>(gs->_geometry))
+            {
+                meta.kv(key + "_geometry", "sersic");
+                meta.kv(key + "_reff", sg->_reff);
+                meta.kv(key + "_n", sg->_n);
+                auto sf = sg->_sersicfunction;
+                writeVec(out + "/" + key + "_sersic_s.npy", std::vector<double>(begin(sf->_sv), end(sf->_sv)));
+                writeVec(out + "/" + key + "_sersic_M.npy", std::vector<double>(begin(sf->_Mv), end(sf->_Mv)));
+            }
         }
+    }
+
+    // the raw detector arrays of every instrument after a primary-emission segment (before
+    // calibration): inst<i>_ifu.npy / inst<i>_sed.npy (total, raw W per pixel and bin, index
+    // l + ell * npix) and inst<i>_wifu.npy / inst<i>_wsed.npy (sum w^k, k = 0..4, per pixel and bin,
+    // FluxRecorder::recordContributions), in FP64 as FluxRecorder holds them
+    void exportDetectors(MonteCarloSimulation* sim, const std::string& out)
+    {
+        int i = 0;
+        for (Instrument* instr : sim->instrumentSystem()->instruments())
+        {
+            auto rec = instr->instrumentFluxRecorder();
+            std::string key = out + "/inst" + std::to_string(i);
+            auto dumpSet = [&](const vector<Array>& arrays, const std::string& name, bool stack) {
+                if (arrays.empty() || arrays[0].size() == 0) return;
+                if (!stack)
+                {
+                    writeVec(key + name, std::vector<double>(begin(arrays[0]), end(arrays[0])));
+                    return;
+                }
+                std::vector<double> all;
+                for (const Array& a : arrays) all.insert(all.end(), begin(a), end(a));
+                writeNpy(key + name, all.data(), {arrays.size(), arrays[0].size()});
+            };
+            if (rec->_ifu.size()) dumpSet(rec->_ifu, "_ifu.npy", false);
+            if (rec->_sed.size()) dumpSet(rec->_sed, "_sed.npy", false);
+            dumpSet(rec->_wifu, "_wifu.npy", true);
+            dumpSet(rec->_wsed, "_wsed.npy", true);
+            ++i;
+        }
+    }
+
+    // the primary radiation field MediumSystem::_rf1 (cells x radiation-field bins) after a run
+    void exportRadiationField(MonteCarloSimulation* sim, const std::string& out)
+    {
+        auto ms = sim->mediumSystem();
+        Table<2>& rf = ms->_rf1;
+        if (rf.size() == 0) return;
+        writeNpy(out + "/rf1.npy", &rf.data()[0], {rf.size(0), rf.size(1)});
     }
 
     void dumpRays(MonteCarloSimulation* sim, const std::string& raysPath, int maxSeg, double lambda,
@@ -511,6 +611,16 @@ int main(int argc, char** argv)
         sim->parallelFactory()->setup();
         sim->log()->setup();
         sim->setupSimulation();
+        // SKGPU_EXPORT_RUN=1: also run the primary-emission segment single-threaded
+        // (MonteCarloSimulation::runPrimaryEmission, which ends with the instrument flush) and dump the
+        // raw detector arrays and the primary radiation field; the run comes before the launch probe,
+        // so its random stream is that of `skirt -t 1`
+        const char* runEnv = std::getenv("SKGPU_EXPORT_RUN");
+        bool run = runEnv && std::atoi(runEnv) != 0;
+        if (run) sim->runPrimaryEmission();
+        // SKGPU_PROBE_N: number of packets launched by the launch probe (default 1000)
+        const char* probeEnv = std::getenv("SKGPU_PROBE_N");
+        size_t probeN = probeEnv ? static_cast<size_t>(std::atoll(probeEnv)) : 1000;
 
         Meta meta;
         meta.kv("oligochromatic", sim->config()->oligochromatic() ? 1 : 0);
@@ -526,8 +636,10 @@ int main(int argc, char** argv)
             exportWLG(sim->config()->radiationFieldWLG(), out + "/rf_wlg");
         }
         exportInstruments(sim, out, meta);
-        exportSources(sim, meta);
-        probeLaunch(sim, out, 1000, 1000);
+        exportSources(sim, out, meta);
+        if (run) exportDetectors(sim, out);
+        if (run && sim->config()->hasMedium()) exportRadiationField(sim, out);
+        probeLaunch(sim, out, probeN, probeN);
         if (argc >= 4)
         {
             int maxSeg = argc >= 5 ? std::atoi(argv[4]) : 4096;

@@ -547,6 +547,41 @@ static int move_inside(Gen* s, const double* b, double eps)
 }
 
 /* NR::locateClip */
+/* NR::locate (SKIRT/utils/NR.hpp:168-173): -1 below the first entry, n - 1 above the last, n - 2
+   exactly at the last */
+static int locate_nr(const double* xv, int n, double x)
+{
+    if (x == xv[n - 1]) return n - 2;
+    int jl = -1, ju = n;
+    while (ju - jl > 1)
+    {
+        int jm = (ju + jl) >> 1;
+        if (x < xv[jm])
+            ju = jm;
+        else
+            jl = jm;
+    }
+    return jl;
+}
+
+/* NR::clampedValue<NR::interpolateLogLog> (NR.hpp:349-358, 394-401); a first interval starting at
+   x = 0, where the power law is undefined, gives the interval's lower value */
+static double clamped_loglog(const double* xv, const double* yv, int n, double x)
+{
+    int i = locate_nr(xv, n, x);
+    if (i < 0) return yv[0];
+    if (i >= n - 1) return yv[n - 1];
+    double x1 = xv[i], x2 = xv[i + 1], f1 = yv[i], f2 = yv[i + 1];
+    if (f1 <= 0 || f2 <= 0)
+    {
+        if (x == x1) return f1;
+        if (x == x2) return f2;
+        return 0;
+    }
+    if (!(x1 > 0)) return f1;
+    return f1 * exp(log(x / x1) / log(x2 / x1) * (log(f2 / f1)));
+}
+
 static int locate_clip(const double* xv, int n, double x)
 {
     if (x < xv[0]) return 0;
@@ -2036,8 +2071,18 @@ static void launch(or_ctx* c, Rng* r, uint64_t hist, Packet* pk)
         double X = uniform(r);
         const double* rv = c->radR + S->radial_offset;
         const double* Pv = c->radP + S->radial_offset;
-        int i = locate_clip(Pv, S->radial_size, X);
-        double rr = rv[i] + (X - Pv[i]) / (Pv[i + 1] - Pv[i]) * (rv[i + 1] - rv[i]);
+        double rr;
+        if (S->position_model == SKGPU_SRC_RADIAL_LOGLOG)
+        {
+            /* SersicGeometry::randomRadius (SersicGeometry.cpp:41-45): reff * SersicFunction::inverseMass(X),
+               i.e. NR::clampedValue<NR::interpolateLogLog>(X, _Mv, _sv) (NR.hpp:349-358, 394-401) */
+            rr = S->geometry[0] * clamped_loglog(Pv, rv, S->radial_size, X);
+        }
+        else
+        {
+            int i = locate_clip(Pv, S->radial_size, X);
+            rr = rv[i] + (X - Pv[i]) / (Pv[i + 1] - Pv[i]) * (rv[i + 1] - rv[i]);
+        }
         double ux, uy, uz;
         iso_direction(r, &ux, &uy, &uz);
         pk->rx = S->position[0] + rr * ux;
@@ -2238,6 +2283,26 @@ static void life_cycle(or_ctx* c, uint64_t hist, Path* path, Packet* pk)
         }
     }
     if (pk->ncontrib) record_contributions(c, pk);
+}
+
+int or_probe_launch(or_ctx* c, uint64_t first, uint64_t count, uint64_t total_packets, double* out)
+{
+    if (!c->nsrc || !c->nmix) return fail(c, SKGPU_ERR_STATE, "probe_launch: no sources or dust mix uploaded");
+    if (total_packets == 0 || first + count > total_packets) return fail(c, SKGPU_ERR_ARG, "probe_launch: history range outside the segment");
+    Packet pk;
+    memset(&pk, 0, sizeof pk);
+    for (uint64_t t = 0; t < count; ++t)
+    {
+        Rng r;
+        launch(c, &r, first + t, &pk);
+        double* o = out + 8 * t;
+        o[0] = pk.lambda;
+        o[1] = pk.L * (double)total_packets;
+        o[2] = pk.rx; o[3] = pk.ry; o[4] = pk.rz;
+        o[5] = pk.kx; o[6] = pk.ky; o[7] = pk.kz;
+    }
+    free(pk.contrib);
+    return SKGPU_OK;
 }
 
 int or_run_primary(or_ctx* c, uint64_t first, uint64_t count, uint64_t total_packets)

@@ -61,6 +61,7 @@ int or_upload_instruments(or_ctx* ctx, int32_t num_instruments, const skgpu_inst
                           const double* wlg_borders, const int32_t* wlg_ellv);
 int or_set_options(or_ctx* ctx, const skgpu_options* options);
 int or_run_primary(or_ctx* ctx, uint64_t first, uint64_t count, uint64_t total_packets);
+int or_probe_launch(or_ctx* ctx, uint64_t first, uint64_t count, uint64_t total_packets, double* out);
 int or_fetch_instrument(or_ctx* ctx, int32_t instrument, double* ifu, double* sed, double* ifu_stats,
                         double* sed_stats);
 int or_fetch_instrument_components(or_ctx* ctx, int32_t instrument, double* ifu3, double* sed3);

@@ -241,6 +241,43 @@ SKG_HD int locateClip(const T* xv, int n, T x)
     return jl;
 }
 
+// NR::locate on an ascending array of n entries (SKIRT/utils/NR.hpp:168-173): -1 below the first
+// entry, n - 1 above the last, and n - 2 exactly at the last
+SKG_HD int locateNR(const double* xv, int n, double x)
+{
+    if (x == xv[n - 1]) return n - 2;
+    int jl = -1, ju = n;
+    while (ju - jl > 1)
+    {
+        int jm = (ju + jl) >> 1;
+        if (x < xv[jm])
+            ju = jm;
+        else
+            jl = jm;
+    }
+    return jl;
+}
+
+// NR::clampedValue<NR::interpolateLogLog>(x, xv, yv) (SKIRT/utils/NR.hpp:349-358, 394-401): the
+// table's end values outside it, power-law interpolation inside; a non-positive end value gives 0
+// between the points, and a first interval starting at x = 0 (where the power law is undefined)
+// gives the interval's lower value
+SKG_HD double clampedLogLog(const double* xv, const double* yv, int n, double x)
+{
+    int i = locateNR(xv, n, x);
+    if (i < 0) return yv[0];
+    if (i >= n - 1) return yv[n - 1];
+    double x1 = xv[i], x2 = xv[i + 1], f1 = yv[i], f2 = yv[i + 1];
+    if (f1 <= 0 || f2 <= 0)
+    {
+        if (x == x1) return f1;
+        if (x == x2) return f2;
+        return 0;
+    }
+    if (!(x1 > 0)) return f1;
+    return f1 * exp(log(x / x1) / log(x2 / x1) * (log(f2 / f1)));
+}
+
 // std::upper_bound index on an ascending array
 template<typename T>
 SKG_HD int upperBound(const T* xv, int n, T x)

@@ -51,6 +51,7 @@ struct skgpu_ctx
     std::vector<InstrDev> instrHost;
     InstrDev* instr = nullptr;
     std::vector<void*> instrBufs;
+    std::vector<size_t> instrBufLens;  // doubles per instrument buffer
     double* wlgB = nullptr;
     int* wlgEll = nullptr;
 

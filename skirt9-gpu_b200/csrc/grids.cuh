@@ -732,22 +732,6 @@ struct TetraExact : GenBase
 // outwards; each exit is at q_N = -/+ sqrt((r_N - p)(r_N + p)) along the ray, q measured from the
 // projection of the origin. The position is not advanced: the generator tracks q.
 // ---------------------------------------------------------------------------------------------
-// NR::locate (SKIRT/utils/NR.hpp:168-173): -1 below xv[0], n - 2 at xv[n - 1]
-SKG_D int locateNR(const double* xv, int n, double x)
-{
-    if (x == xv[n - 1]) return n - 2;
-    int jl = -1, ju = n;
-    while (ju - jl > 1)
-    {
-        int jm = (ju + jl) >> 1;
-        if (x < xv[jm])
-            ju = jm;
-        else
-            jl = jm;
-    }
-    return jl;
-}
-
 struct Sphere1DExact : GenBase
 {
     static constexpr int kMinBlocks = 4;

@@ -243,8 +243,17 @@ SKG_D Launched launchPacket(const Scene& p, unsigned long long hist, Rng& rng)
         double X = rng.uniform();
         const double* rv = p.radR + S.roff;
         const double* Pv = p.radP + S.roff;
-        int i = locateClip(Pv, S.rsize, X);
-        double r = rv[i] + (X - Pv[i]) / (Pv[i + 1] - Pv[i]) * (rv[i + 1] - rv[i]);
+        double r;
+        if (S.posModel == 3)
+        {
+            // SersicFunction::inverseMass: NR::clampedValue<NR::interpolateLogLog>(X, M, s), times the scale
+            r = S.geom[0] * clampedLogLog(Pv, rv, S.rsize, X);
+        }
+        else
+        {
+            int i = locateClip(Pv, S.rsize, X);
+            r = rv[i] + (X - Pv[i]) / (Pv[i + 1] - Pv[i]) * (rv[i + 1] - rv[i]);
+        }
         double ux, uy, uz;
         isotropicDirection(rng, ux, uy, uz);
         o.x = S.pos[0] + r * ux;

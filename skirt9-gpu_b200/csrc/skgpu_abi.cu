@@ -95,6 +95,7 @@ void freeInstruments(skgpu_ctx* ctx)
 {
     for (void* p : ctx->instrBufs) cudaFree(p);
     ctx->instrBufs.clear();
+    ctx->instrBufLens.clear();
     ctx->instrHost.clear();
     devFree(ctx->instr);
     devFree(ctx->wlgB);
@@ -951,13 +952,24 @@ int skgpu_upload_sources(skgpu_ctx* ctx, int32_t num_sources, const skgpu_source
     {
         const skgpu_source& s = sources[h];
         SourceDev& d = v[h];
-        if (s.position_model < 0 || s.position_model > 2) return fail(ctx, SKGPU_ERR_ARG, "sources: bad position model");
+        if (s.position_model < 0 || s.position_model > 3) return fail(ctx, SKGPU_ERR_ARG, "sources: bad position model");
         if (s.spectral_model < 0 || s.spectral_model > 1) return fail(ctx, SKGPU_ERR_ARG, "sources: bad spectral model");
         if (s.table_size < 1 || s.table_offset < 0 || s.table_offset + s.table_size > table_len)
             return fail(ctx, SKGPU_ERR_ARG, "sources: spectral table out of range");
         if (s.spectral_model == 1 && s.table_size < 2) return fail(ctx, SKGPU_ERR_ARG, "sources: SED table needs 2 points");
-        if (s.position_model == 2 && (s.radial_size < 2 || s.radial_offset < 0 || s.radial_offset + s.radial_size > radial_len))
+        if ((s.position_model == 2 || s.position_model == 3)
+            && (s.radial_size < 2 || s.radial_offset < 0 || s.radial_offset + s.radial_size > radial_len))
             return fail(ctx, SKGPU_ERR_ARG, "sources: radial table out of range");
+        if (s.position_model == 3)
+        {
+            for (int i = 0; i < s.radial_size; ++i)
+            {
+                double sv = radial_r[s.radial_offset + i], mv = radial_P[s.radial_offset + i];
+                if (!(sv > 0.) || !(mv >= 0.) || (i > 0 && !(mv >= radial_P[s.radial_offset + i - 1])))
+                    return fail(ctx, SKGPU_ERR_ARG, "sources: log-log radial table needs positive radii and ascending masses");
+            }
+            if (!(s.geometry[0] > 0.)) return fail(ctx, SKGPU_ERR_ARG, "sources: log-log radial table needs a positive scale");
+        }
         if (h > 0 && s.first_history < sources[h - 1].first_history)
             return fail(ctx, SKGPU_ERR_ARG, "sources: first_history must be ascending");
         d.posModel = s.position_model;
@@ -1032,6 +1044,7 @@ int skgpu_upload_instruments(skgpu_ctx* ctx, int32_t num_instruments, const skgp
             CK(devAlloc(p, cnt));
             CK(cudaMemset(*p, 0, cnt * sizeof(double)));
             ctx->instrBufs.push_back(*p);
+            ctx->instrBufLens.push_back(cnt);
             return SKGPU_OK;
         };
         int rc;
@@ -1243,6 +1256,48 @@ int skgpu_run_primary(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t t
 }
 
 // ------------------------------------------------------------------------------------------------
+// launch probe: the source launch of the life cycle without the traversal
+// ------------------------------------------------------------------------------------------------
+static __global__ void __launch_bounds__(256) probeLaunchKernel(const __grid_constant__ Scene sc, unsigned long long first,
+                                                                unsigned long long count, double total, double* out)
+{
+    for (unsigned long long t = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x; t < count;
+         t += static_cast<unsigned long long>(gridDim.x) * blockDim.x)
+    {
+        unsigned long long hist = first + t;
+        Rng rng;
+        rng.start(sc.seed, hist);
+        Launched o = launchPacket(sc, hist, rng);
+        double* r = out + 8 * t;
+        r[0] = o.lambda;
+        r[1] = o.L * total;
+        r[2] = o.x; r[3] = o.y; r[4] = o.z;
+        r[5] = o.kx; r[6] = o.ky; r[7] = o.kz;
+    }
+}
+
+int skgpu_probe_launch(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t total_packets, double* out)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (ctx->srcHost.empty()) return fail(ctx, SKGPU_ERR_STATE, "probe_launch: no sources uploaded");
+    if (total_packets == 0 || first + count > total_packets || (count && !out))
+        return fail(ctx, SKGPU_ERR_ARG, "probe_launch: history range outside the segment");
+    if (count == 0) return SKGPU_OK;
+    CK(cudaSetDevice(ctx->device));
+    double* dev = nullptr;
+    CK(devAlloc(&dev, 8 * count));
+    Scene sc = sceneOf(ctx);
+    unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((count + 255) / 256, 8ull * ctx->numSMs));
+    probeLaunchKernel<<<blocks, 256, 0, ctx->stream>>>(sc, first, count, static_cast<double>(total_packets), dev);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, dev, 8 * count * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(dev);
+    if (e != cudaSuccess) return fail(ctx, SKGPU_ERR_CUDA, std::string("probe_launch: ") + cudaGetErrorString(e));
+    return SKGPU_OK;
+}
+
+// ------------------------------------------------------------------------------------------------
 // run without allocations: the wavefront scratch comes from a file-scope device array
 // ------------------------------------------------------------------------------------------------
 
@@ -1316,24 +1371,18 @@ int skgpu_run_primary_noalloc(skgpu_ctx* ctx, uint64_t first, uint64_t count, ui
     if (carveWave(probe, nullptr, SKGPU_NOALLOC_MAX_SLOTS, groups, anyStats) > sizeof(g_noallocScratch))
         return fail(ctx, SKGPU_ERR_ARG, "run_noalloc: scene needs more scratch than the static array holds");
     CK(cudaSetDevice(ctx->device));
-    // the host-side name of the array is not a device address: ask the runtime once per device
-    static std::mutex mtx;
-    static void* addr[256] = {};
-    if (ctx->device < 0 || ctx->device >= 256) return fail(ctx, SKGPU_ERR_ARG, "run_noalloc: device index out of range");
-    {
-        std::lock_guard<std::mutex> lock(mtx);
-        if (!addr[ctx->device])
-        {
-            void* p = nullptr;
-            cudaError_t e = cudaGetSymbolAddress(&p, g_noallocScratch);
-            if (e != cudaSuccess || !p)
-                return fail(ctx, SKGPU_ERR_CUDA, std::string("run_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-            addr[ctx->device] = p;
-        }
-    }
+    // the host-side name of the array is not a device address: ask the runtime, with this device
+    // current, on every call (the lookup allocates nothing, and a cached address would go stale after
+    // a device reset or under another context on the same device)
+    void* addr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&addr, g_noallocScratch);
+    if (e != cudaSuccess || !addr)
+        return fail(ctx, SKGPU_ERR_CUDA, std::string("run_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
     Wave w{};
-    carveWave(w, static_cast<unsigned char*>(addr[ctx->device]), SKGPU_NOALLOC_MAX_SLOTS, groups, anyStats);
+    carveWave(w, static_cast<unsigned char*>(addr), SKGPU_NOALLOC_MAX_SLOTS, groups, anyStats);
     w.sc = sceneOf(ctx);
+    w.traceBlocksPerSM = ctx->shapeTraceBlocks;
+    w.shadeBlocksPerSM = ctx->shapeShadeBlocks;
     w.P = static_cast<int>(std::min<uint64_t>(std::max<uint64_t>(count, 1), SKGPU_NOALLOC_MAX_SLOTS));
     w.first = first;
     w.count = count;
@@ -1456,6 +1505,27 @@ int skgpu_fetch_radiation_field(skgpu_ctx* ctx, double* rf)
     rfTransposeKernel<<<grid, dim3(32, 8), 0, ctx->stream>>>(ctx->rf, ctx->rfT, cells, nbins);
     CK(cudaGetLastError());
     return addInto(ctx, ctx->rfT, ctx->rfLen, rf);
+}
+
+int skgpu_tally_buffers(skgpu_ctx* ctx, int32_t max_buffers, void** ptrs, uint64_t* lengths, int32_t* num_buffers)
+{
+    if (!ctx || !num_buffers) return SKGPU_ERR_ARG;
+    int n = static_cast<int>(ctx->instrBufs.size()) + (ctx->rf ? 1 : 0);
+    *num_buffers = n;
+    if (max_buffers < n) return ptrs ? fail(ctx, SKGPU_ERR_ARG, "tally_buffers: array too small") : SKGPU_OK;
+    if (!ptrs || !lengths) return fail(ctx, SKGPU_ERR_ARG, "tally_buffers: null output arrays");
+    size_t i = 0;
+    for (; i < ctx->instrBufs.size(); ++i)
+    {
+        ptrs[i] = ctx->instrBufs[i];
+        lengths[i] = ctx->instrBufLens[i];
+    }
+    if (ctx->rf)
+    {
+        ptrs[i] = ctx->rf;
+        lengths[i] = ctx->rfLen;
+    }
+    return SKGPU_OK;
 }
 
 int skgpu_clear_tallies(skgpu_ctx* ctx)

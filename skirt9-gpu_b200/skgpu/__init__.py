@@ -2,7 +2,8 @@
 
 The compute path is the CUDA library lib/libskgpu.so (C ABI in include/skgpu.h); this package
 binds it with ctypes (`abi`), describes scenes in the ABI layout (`scene`), builds the named
-workloads (`workloads`) and writes ski files for the reference (`ski`).
+workloads (`workloads`), writes ski files for the reference (`ski`) and sums a segment's tallies
+over ranks (`sharding`).
 """
 from .abi import Backend, SkgpuError, load_library  # noqa: F401
 from .scene import Scene, Results  # noqa: F401

@@ -19,7 +19,7 @@ OK, ERR_ARG, ERR_CUDA, ERR_STATE, ERR_TIMEOUT, ERR_DEVICE, ERR_UNSUPPORTED = ran
 (GRID_CARTESIAN, GRID_OCTREE, GRID_VORONOI, GRID_TETRA, GRID_SPHERE1D, GRID_CYLINDER2D, GRID_SPHERE2D, GRID_SPHERE3D,
  GRID_CYLINDER3D) = range(9)
 PREC_FP64_EXACT, PREC_FP32 = 0, 1
-SRC_POINT, SRC_EXPDISK, SRC_RADIAL = 0, 1, 2
+SRC_POINT, SRC_EXPDISK, SRC_RADIAL, SRC_RADIAL_LOGLOG = 0, 1, 2, 3
 SPEC_DISCRETE, SPEC_TABLE = 0, 1
 INSTR_FRAME, INSTR_SED = 0, 1
 
@@ -127,6 +127,7 @@ SIGNATURES = {
     "upload_instruments": [_P, _I, _P, _I, _P, _P],
     "set_options": [_P, _P],
     "run_primary": [_P, _U, _U, _U],
+    "probe_launch": [_P, _U, _U, _U, _P],
     "fetch_instrument": [_P, _I, _P, _P, _P, _P],
     "fetch_instrument_components": [_P, _I, _P, _P],
     "fetch_radiation_field": [_P, _P],
@@ -276,6 +277,13 @@ class Backend:
     def run_primary(self, first, count, total):
         self.call("run_primary", int(first), int(count), int(total))
 
+    def probe_launch(self, first, count, total):
+        """(count, 8) array: wavelength, luminosity x total, position, direction of the launched
+        histories [first, first+count) of a segment of `total` packets (no traversal)."""
+        out = np.zeros((int(count), 8))
+        self.call("probe_launch", int(first), int(count), int(total), _ptr(out))
+        return out
+
     @staticmethod
     def _into(out, n):
         """The caller's accumulation array (float64, contiguous, n entries) or a new zeroed one."""
@@ -405,6 +413,27 @@ def run_primary_noalloc(be, first, count, total):
     rc = f(be.ctx, int(first), int(count), int(total))
     if rc != OK:
         raise SkgpuError(rc, be.fn["last_error"](be.ctx).decode())
+
+
+EXPORTED += ["skgpu_tally_buffers"]
+
+
+def tally_buffers(be):
+    """[(device pointer, length in doubles)] of the context's device tally buffers (instrument
+    buffers in upload order, then the radiation field), for a collective across GPUs."""
+    f = be.lib.skgpu_tally_buffers
+    f.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]
+    f.restype = C.c_int
+    n = C.c_int32()
+    rc = f(be.ctx, 0, None, None, C.byref(n))
+    if rc != OK:
+        raise SkgpuError(rc, be.fn["last_error"](be.ctx).decode())
+    ptrs = (C.c_void_p * max(1, n.value))()
+    lens = (C.c_uint64 * max(1, n.value))()
+    rc = f(be.ctx, n.value, ptrs, lens, C.byref(n))
+    if rc != OK:
+        raise SkgpuError(rc, be.fn["last_error"](be.ctx).decode())
+    return [(int(ptrs[i] or 0), int(lens[i])) for i in range(n.value)]
 
 
 EXPORTED += ["skgpu_set_stage_timing", "skgpu_last_stage_times"]

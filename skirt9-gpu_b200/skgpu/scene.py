@@ -127,7 +127,7 @@ class Scene:
             tl.extend(src["table_lambda"])
             ta.extend(src["table_a"])
             tb.extend(src.get("table_b", np.zeros(len(src["table_lambda"]))))
-            if s.position_model == abi.SRC_RADIAL:
+            if s.position_model in (abi.SRC_RADIAL, abi.SRC_RADIAL_LOGLOG):
                 s.radial_offset = len(rr)
                 s.radial_size = len(src["radial_r"])
                 rr.extend(src["radial_r"])
@@ -164,6 +164,12 @@ class Scene:
         be.set_options(self.options(seed, precision))
         structs, tl, ta, tb, rr, rp = self.source_structs(npp)
         be.upload_sources(structs, tl, ta, tb, rr, rp)
+
+    def probe_launch(self, be, npp, count=None, seed=0, first=0):
+        """The launch record (wavelength, L x npp, position, direction) of histories [first,
+        first+count) of a segment of npp packets, without tracing them."""
+        self.prepare(be, npp, seed)
+        return be.probe_launch(first, npp if count is None else count, npp)
 
     def run(self, be, npp, seed=0, precision=abi.PREC_FP64_EXACT, first=0, count=None, clear=True):
         """One primary-emission segment of npp packets (histories [first, first+count))."""
@@ -216,6 +222,30 @@ class Scene:
                 meta[k] = v
         return meta, load, has
 
+    @staticmethod
+    def _panchromatic_source(meta, L, h):
+        """A geometric source with a black-body SED (panchromatic mode) from the reference's own launch
+        tables: the SED's (lambda, p, P) table for Random::cdfLogLog, the wavelength bias and its
+        log-uniform range, and the exponential-disk parameters or the Sersic cumulative-mass table."""
+        p = f"source{h}_"
+        if meta.get(p + "type") != "GeometricSource" or meta.get(p + "sed") != "blackbody":
+            raise ValueError("export loader supports geometric sources with black-body SEDs in panchromatic mode")
+        src = dict(spectral_model=abi.SPEC_TABLE, lfrac=float(meta[p + "lfrac"]), weight=float(meta[p + "weight"]),
+                   table_lambda=L(p + "sed_lambda"), table_a=L(p + "sed_p"), table_b=L(p + "sed_P"),
+                   wavelength_bias=float(meta.get(p + "xi", 0.0)))
+        if src["wavelength_bias"] > 0:
+            src["bias_range"] = (float(meta[p + "bias_min"]), float(meta[p + "bias_max"]))
+        geo = meta.get(p + "geometry")
+        if geo == "expdisk":
+            src.update(position_model=abi.SRC_EXPDISK,
+                       geometry=tuple(float(meta[p + k]) for k in ("hR", "hz", "Rmin", "Rmax", "zmax")))
+        elif geo == "sersic":
+            src.update(position_model=abi.SRC_RADIAL_LOGLOG, geometry=(float(meta[p + "reff"]),),
+                       radial_r=L(p + "sersic_s"), radial_P=L(p + "sersic_M"))
+        else:
+            raise ValueError(f"export loader: unsupported source geometry {geo}")
+        return src
+
     @classmethod
     def from_export(cls, d):
         """Scene from the arrays the reference export harness wrote (directory or mapping)."""
@@ -264,17 +294,21 @@ class Scene:
         if has("rf_wlg_borders"):
             ellv = L("rf_wlg_ellv")
             sc.rf = dict(num_bins=int(ellv.max()) + 1, borders=L("rf_wlg_borders"), ellv=ellv)
-        # sources: the launch probe gives lambda and L*npp of the reference's own launches
         sc.total_luminosity = float(meta["source_total_luminosity"])
         probe = L("src_probe")
         nsrc = int(meta["num_sources"])
-        if nsrc != 1 or meta["source0_type"] != "PointSource" or meta["oligochromatic"] != "1":
-            raise ValueError("export loader supports the oligochromatic single point source only")
-        lams = np.unique(probe[:, 0])
-        weights = np.array([probe[probe[:, 0] == l, 1][0] for l in lams]) / sc.total_luminosity
-        sc.sources = [dict(position_model=abi.SRC_POINT, spectral_model=abi.SPEC_DISCRETE,
-                           position=tuple(probe[0, 2:5]), lfrac=float(meta["source0_lfrac"]),
-                           weight=float(meta["source0_weight"]), table_lambda=lams, table_a=weights)]
+        if meta["oligochromatic"] == "1":
+            # oligochromatic point source: the launch probe gives lambda and L*npp of the reference's
+            # own launches (one weight per wavelength)
+            if nsrc != 1 or meta["source0_type"] != "PointSource":
+                raise ValueError("export loader supports a single point source in oligochromatic mode")
+            lams = np.unique(probe[:, 0])
+            weights = np.array([probe[probe[:, 0] == l, 1][0] for l in lams]) / sc.total_luminosity
+            sc.sources = [dict(position_model=abi.SRC_POINT, spectral_model=abi.SPEC_DISCRETE,
+                               position=tuple(probe[0, 2:5]), lfrac=float(meta["source0_lfrac"]),
+                               weight=float(meta["source0_weight"]), table_lambda=lams, table_a=weights)]
+        else:
+            sc.sources = [cls._panchromatic_source(meta, L, h) for h in range(nsrc)]
         for i in range(int(meta["num_instruments"])):
             p = f"instr{i}_"
             ellv = L(p + "wlg_ellv")

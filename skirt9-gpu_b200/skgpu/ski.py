@@ -259,11 +259,15 @@ def geometric_source(geometry_xml, temperature, luminosity_lsun):
 
 
 def galaxy_octree(num_packets=1e8, npix=512, nlambda=100, max_level=8, max_dust_fraction=1e-6, tau_v=1.0,
-                  half_size_kpc=25, store_rf=True):
+                  half_size_kpc=25, store_rf=True, stats=False, sed=False, grid=None, medium=None,
+                  num_density_samples=100):
     """Stellar exponential disk (hR 4 kpc, hz 0.35 kpc) + Sersic n=4 bulge (Re 1 kpc), B/T = 0.2,
     black bodies of 6000 K and 4000 K; dust exponential disk (hR 6 kpc, hz 0.2 kpc, face-on tau_V)
     with power-law MeanListDustMix on 100 log wavelengths 0.1-10 micron; octree by the dust-mass
-    fraction policy; three frames at 0, 60 and 90 degrees; radiation field on the same grid."""
+    fraction policy; three frames at 0, 60 and 90 degrees (with statistics when `stats`), plus an
+    SED instrument at 60 degrees when `sed`; radiation field on the same grid. `grid` and `medium`
+    replace the policy octree and the analytic dust disk (e.g. a FileTreeSpatialGrid and a
+    CellMedium holding the same tree and densities as a standalone scene)."""
     lam = [0.1 * (100.0 ** (i / (nlambda - 1))) for i in range(nlambda)]
     kappa = [(l / 0.55) ** -1.0 for l in lam]
     albedo = [min(0.9, max(0.05, 0.5 * (l / 0.55) ** -0.2)) for l in lam]
@@ -274,10 +278,17 @@ def galaxy_octree(num_packets=1e8, npix=512, nlambda=100, max_level=8, max_dust_
                + geometric_source('<SersicGeometry effectiveRadius="1 kpc" index="4"/>', 4000, 2e9))
     wlg = f'<LogWavelengthGrid minWavelength="0.1 micron" maxWavelength="10 micron" numWavelengths="{nlambda}"/>'
     fov = 2 * half_size_kpc
-    instruments = "".join(frame_instrument(f"i{inc}", inc, fov, "kpc", npix, stats=False) for inc in (0, 60, 90))
-    return simulation("ExtinctionOnly", num_packets, sources, expdisk_medium(6, 0.2, "kpc", tau_v, mix),
-                      octree_grid(half_size_kpc, "kpc", max_level, max_dust_fraction), instruments,
-                      instrument_wlg=wlg, store_rf=store_rf, rf_wlg=wlg)
+    instruments = "".join(frame_instrument(f"i{inc}", inc, fov, "kpc", npix, stats=stats) for inc in (0, 60, 90))
+    if sed:
+        instruments += sed_instrument("sed", 60, stats, comps=False)
+    if grid is None:
+        grid = octree_grid(half_size_kpc, "kpc", max_level, max_dust_fraction)
+    if medium is None:
+        medium = expdisk_medium(6, 0.2, "kpc", tau_v, mix)
+    else:
+        medium = medium(mix)
+    return simulation("ExtinctionOnly", num_packets, sources, medium, grid, instruments,
+                      instrument_wlg=wlg, store_rf=store_rf, rf_wlg=wlg, num_density_samples=num_density_samples)
 
 
 def galaxy_voronoi(num_packets=1e8, npix=512, nlambda=100, num_sites=1_000_000, tau_v=2.0, half_size_kpc=25,

@@ -22,6 +22,13 @@ Fixtures written:
                      write only them)
   stats_octree.npz, stats_voronoi.npz, stats_tetra.npz  the disk scene on these grids (scene export)
                      with reference frame/SED statistics (argument `gridstats`)
+  stats_galaxy.npz   the galaxy configuration reduced in size (stellar exponential disk + Sersic
+                     bulge with black-body SEDs and wavelength bias 0.5, dust disk on the reference's
+                     own octree of max level 6, 20 log wavelengths, three 32^2 frames and an SED with
+                     statistics, radiation field stored): scene export, the raw detector sums
+                     (w^0, w^1, w^2 per pixel and bin) and the primary radiation field of a
+                     single-threaded 5e5-packet reference run, and 2e4 reference launches
+                     (argument `galaxy`)
 """
 import os
 import shutil
@@ -126,6 +133,7 @@ def main():
     sphere3d_fixture()
     cylinder3d_fixture()
     grid_stats_fixtures()
+    galaxy_fixture()
 
     # dust shell, 16^3 grid, 64^2 frame + SED: scene export + reference statistics (2e5 packets)
     npp = 200000
@@ -280,6 +288,44 @@ def grid_stats_fixtures():
         print(f"stats_{name} written")
 
 
+def galaxy_fixture(npp=500000, probe=20000):
+    """The galaxy configuration at reduced size on the reference's own octree: the harness exports the
+    scene, runs the primary-emission segment single-threaded and dumps the raw FP64 detector arrays
+    and the radiation field MediumSystem::_rf1 (no FITS scaling to undo), and launches `probe`
+    packets through SourceSystem::launch."""
+    text = ski.galaxy_octree(npp, npix=32, nlambda=20, max_level=6, max_dust_fraction=1e-4, stats=True, sed=True)
+    with tempfile.TemporaryDirectory() as tmp:
+        env = dict(os.environ, SKGPU_EXPORT_RUN="1", SKGPU_PROBE_N=str(probe))
+        ski_path = os.path.join(tmp, "galaxy.ski")
+        with open(ski_path, "w") as f:
+            f.write(text)
+        exp = os.path.join(tmp, "export")
+        os.makedirs(exp)
+        subprocess.run([os.path.join(BIN, "skirt_export"), ski_path, exp], check=True, env=env,
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        data = {}
+        for fn in os.listdir(exp):
+            if fn.endswith(".npy"):
+                data[fn[:-4]] = np.load(os.path.join(exp, fn))
+        with open(os.path.join(exp, "meta.txt")) as f:
+            data["meta"] = np.array(f.read())
+    # keep w^0..w^2 of the statistics (the z-scores need no higher moments; w^1 is the total); the
+    # radiation field and the launch probe are rounded to FP32 for size (they are compared within
+    # Monte Carlo noise)
+    for k in list(data):
+        if k.startswith("inst") and (k.endswith("_wifu") or k.endswith("_wsed")):
+            data[k] = data[k][:3]
+        elif k.startswith("inst") and (k.endswith("_ifu") or k.endswith("_sed")):
+            del data[k]
+    rf = data.pop("rf1")
+    data["rf1_scale"] = rf.max()
+    data["rf1_scaled"] = (rf / rf.max()).astype(np.float32)  # rf1 = rf1_scaled * rf1_scale
+    data["src_probe"] = data["src_probe"].astype(np.float32)
+    data["ref_npp"] = npp
+    np.savez_compressed(os.path.join(OUT, "stats_galaxy.npz"), **data)
+    print(f"stats_galaxy: {len(data['medium_density'])} cells, {npp} packets")
+
+
 def reference_stats(fixture, ski_text, frame_name, npp):
     """Adds the frame and SED statistics of a single-threaded reference run of ski_text to a
     fixture; the run's stats scale c is recovered from its total image (MJy/sr per raw W from the
@@ -337,6 +383,8 @@ if __name__ == "__main__":
         cylinder3d_fixture()
     elif sys.argv[1:] == ["gridstats"]:
         grid_stats_fixtures()
+    elif sys.argv[1:] == ["galaxy"]:
+        galaxy_fixture()
     elif sys.argv[1:] == ["explicit"]:
         z = np.load(os.path.join(OUT, "shell_c16.npz"))
         meta = __import__("skgpu").Scene.read_export(z)[0]

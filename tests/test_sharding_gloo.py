@@ -1,11 +1,12 @@
 """Multi-process sharding of the life cycle, on CPU with the gloo backend (world size 2).
 
 Histories are independent and every tally is additive, so ranks split a segment into contiguous
-history ranges (as `bench.py` does under torchrun) and the segment's tallies are the sum over
-ranks. The ranks here trace their ranges with the CPU oracle (the same Philox streams and walkers
-as the CUDA library) and sum the frame, SED and radiation-field tallies with a gloo all-reduce;
-the result must equal one process tracing the whole segment. The max-over-ranks timing reduction
-is checked on the same group."""
+history ranges (skgpu.sharding.history_range, as `bench.py` does under torchrun) and the segment's
+tallies are the sum over ranks. The ranks here trace their ranges with the CPU oracle (the same
+Philox streams and walkers as the CUDA library) and sum every tally (frame and SED totals, their
+per-history statistics and components, the radiation field) with skgpu.sharding.allreduce_results
+over gloo; the result must equal one process tracing the whole segment. The max-over-ranks timing
+reduction is checked on the same group."""
 import os
 import socket
 
@@ -21,20 +22,16 @@ SEED = 5
 
 def _scene():
     from skgpu import workloads
-    sc = workloads.shell_cartesian(12, 16, stats=False)
+    sc = workloads.shell_cartesian(12, 16, stats=True)
+    sc.instruments[1]["comps"] = 1
+    sc.store_rf = True
+    sc.rf = dict(num_bins=1, borders=np.array([0.5e-6, 0.6e-6]), ellv=np.array([-1, 0, -1], np.int32))
     return sc
 
 
-def history_range(rank, world, n):
-    """Contiguous share of [0, n) for `rank` (the last rank takes the remainder)."""
-    per = n // world
-    first = rank * per
-    return first, (n - first if rank == world - 1 else per)
-
-
 def _flat(res):
-    parts = [np.asarray(i["total"], float).ravel() for i in res.instruments]
-    return np.concatenate(parts)
+    from skgpu.sharding import _result_arrays
+    return np.concatenate([np.asarray(a, float).ravel() for a in _result_arrays(res)])
 
 
 def _worker(rank, world, port, out):
@@ -42,6 +39,7 @@ def _worker(rank, world, port, out):
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     sys.path[:0] = [os.path.join(root, "skirt9-gpu_b200"), os.path.join(root, "oracle")]
     import oracle
+    from skgpu.sharding import allreduce_results, history_range
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
@@ -51,8 +49,8 @@ def _worker(rank, world, port, out):
         sc.upload(be)
         first, count = history_range(rank, world, N)
         res = sc.run(be, N, seed=SEED, first=first, count=count)
-        t = torch.from_numpy(_flat(res))
-        dist.all_reduce(t)
+        assert res.rf is not None and res.instruments[0]["stats"] is not None
+        t = torch.from_numpy(_flat(allreduce_results(res)))
         ms = torch.tensor([10.0 + rank])
         dist.all_reduce(ms, op=dist.ReduceOp.MAX)
         hist = torch.tensor([float(res.counters["histories"])])
@@ -72,6 +70,7 @@ def _free_port():
 
 
 def test_history_ranges_partition_the_segment():
+    from skgpu.sharding import history_range
     for world in (1, 2, 3, 8):
         spans = [history_range(r, world, 1001) for r in range(world)]
         assert spans[0][0] == 0 and sum(c for _, c in spans) == 1001

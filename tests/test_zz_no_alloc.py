@@ -34,6 +34,25 @@ def test_noalloc_equals_run_primary_on_two_calls(golden, gpu_backend):
                 np.testing.assert_allclose(b["components"], a["components"], rtol=1e-9, atol=0)
 
 
+def test_noalloc_allocates_no_device_memory(golden, gpu_backend):
+    """The property the entry point exists for: once the library is loaded and a first call has
+    run, a call leaves the device's free memory unchanged."""
+    import torch
+    sc = Scene.from_export(golden("shell_c16.npz"))
+    sc.upload(gpu_backend)
+    n = 40000
+    gpu_backend.clear_tallies()
+    sc.prepare(gpu_backend, n, seed=3)
+    abi.run_primary_noalloc(gpu_backend, 0, n, n)
+    torch.cuda.mem_get_info(0)  # the first query sets up torch's own CUDA state
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(0)
+    abi.run_primary_noalloc(gpu_backend, 0, n, n)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(0)
+    assert free1 == free0
+
+
 def test_noalloc_rejects_scenes_beyond_its_scratch(golden, gpu_backend):
     sc = Scene.from_export(golden("shell_c16.npz"))
     frame = sc.instruments[0]
