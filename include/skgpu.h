@@ -132,9 +132,10 @@ typedef struct skgpu_counters {
     uint64_t scatterings;      /* scattering events */
     uint64_t peel_detections;  /* instrument detections (per instrument) */
     uint64_t rf_stores;        /* radiation-field updates */
-    uint64_t stats_overflows;  /* histories whose statistics buffer overflowed (partial grouping) */
+    uint64_t stats_overflows;  /* statistics contributions lost because the spill log was full (the run then fails) */
     uint64_t kernel_launches;
-    uint64_t reserved;
+    uint64_t stats_spilled;    /* statistics contributions of histories with more distinct bins than the
+                                  per-slot buffer holds, grouped exactly through the spill log after the run */
 } skgpu_counters;
 
 /* ---- context ---- */

@@ -26,6 +26,19 @@ SKG_D double xdot3(double a, double b, double c, double d, double e, double f)
     return xadd(xadd(xmul(a, b), xmul(c, d)), xmul(e, f));
 }
 
+// The IEEE quotient a / b from y = 1 / b rounded to nearest (computed once per ray): q = a * y is
+// within one ulp of a / b, the FMA residual r = a - b * q is exact, and q + r * y rounded once is
+// the correctly rounded quotient (Markstein, IBM J. Res. Dev. 34 (1990) 111-119; the division
+// theorem of Muller et al., Handbook of Floating-Point Arithmetic, 2018, section 4.9) for finite
+// operands whose quotient neither overflows nor underflows: three FP64 operations instead of a
+// division per wall distance.
+SKG_D double qdiv(double a, double b, double y)
+{
+    double q = __dmul_rn(a, y);
+    double r = __fma_rn(-q, b, a);
+    return __fma_rn(r, y, q);
+}
+
 // ---------------------------------------------------------------------------------------------
 // Philox4x32-10 (Salmon, Moraes, Dror & Shaw 2011, "Parallel random numbers: as easy as 1, 2, 3").
 // Each history draws from its own counter stream: key = seed, counter = (draw, 0, hist_lo, hist_hi).

@@ -37,11 +37,17 @@ struct GridDev
     const int* tNbBegin;
     const int* tNb;
     int tNodes;
-    // leaf-indexed records of the FP32 walker: per cell two float4 (FP32 bounds, FP32 number
-    // density, neighbour-list base), per cell the cumulative offsets of its 6 walls in its neighbour list (9 bits each), and
-    // the neighbour cells (positive overlap only, overlap-sorted) of every leaf wall
-    const float4* tLeaf;   // 64-byte leaf records of the FP32 walker (4 float4 per cell)
-    const int* tLeafNb;    // their positive-overlap neighbour lists (cell indices)
+    // leaf-indexed 64-byte records of the production walker (four int4 per cell):
+    //   [0] wall indices x lo|hi<<16, y, z (16 bits each, into the lattice wall tables), FP32 density
+    //   [1] neighbour-list base, 9-bit cumulative wall offsets (64 bits), leaf node id
+    //   [2] [3] per wall the single positive-overlap neighbour (-1: domain wall, -2: scan the list)
+    // and the positive-overlap neighbour lists (overlap-sorted, cell indices) of every leaf wall
+    const int4* tRec;
+    const int* tLeafNb;
+    // the octree's lattice: every wall coordinate of a tree of depth L <= 15 built by halving is one
+    // of 2^L + 1 FP64 values per axis (a child's bounds are copies of its parent's bounds and centre)
+    const double* tWall;   // 3 x tWallN wall coordinates (x, y, z)
+    int tWallN;            // 2^L + 1, or 0 when the tree is not such a lattice (no production records)
 
     // Voronoi: sites, neighbour CSR (negative = wall), uniform site-search grid
     const double* vSites;

@@ -1,12 +1,11 @@
-// Production walkers: the reference generators' geometry with FP32 distance arithmetic.
-//
-// Each walker keeps the entry point of the current cell in FP64 and re-bases it at every crossing
-// (the coordinate of the crossed wall is set exactly, the others advance along the ray), so that all
-// per-cell geometry is computed in FP32 relative to that point: wall offsets (FP64 difference,
-// rounded once to FP32) times the precomputed FP32 inverse direction. There are no divisions per
-// crossing and the exit-axis selection is branch free. Exit-axis ties follow the reference's rule.
-// Errors against the FP64 walkers are a few FP32 ulps of the cell size per segment; cell sequences
-// differ only where a ray passes within that distance of a cell edge or corner.
+// Production walkers. The Cartesian and octree walkers follow the reference generators' FP64
+// operation order exactly (every wall distance, position update and containment test), so their
+// cell sequences and segment lengths equal the reference's bit for bit; what makes them fast is the
+// data layout and the division: a wall distance is the correctly rounded quotient from the ray's
+// precomputed reciprocal direction (qdiv, three FP64 operations), and the octree walker reads
+// 64-byte leaf records with exact FP64 walls from small per-axis lattice tables. Optical depth,
+// path length and radiation-field factors accumulate in FP32 (Acc); tallies stay FP64. The Voronoi
+// and tetrahedral walkers below keep FP32 face distances with FP64 re-decisions.
 #pragma once
 
 #include <type_traits>
@@ -15,238 +14,294 @@
 
 namespace skg {
 
-template<typename Real>
-struct RealLimits;
-template<>
-struct RealLimits<float>
+// 1 / k rounded to nearest for |k| > 1e-15 (the reference's threshold for a usable direction
+// component), 0 otherwise
+SKG_D double recipDir(double k) { return fabs(k) > 1e-15 ? 1.0 / k : 0.0; }
+
+// the reference's wall distance (wall - r) / k, or DBL_MAX for |k| <= 1e-15
+SKG_D double wallDist(double wall, double r, double k, double ik)
 {
-    SKG_D static float big() { return FLT_MAX; }
-};
-template<>
-struct RealLimits<double>
+    return fabs(k) > 1e-15 ? qdiv(xsub(wall, r), k, ik) : DBL_MAX;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Cartesian grid, production (CartesianSpatialGrid::MySegmentGenerator::next,
+// CartesianSpatialGrid.cpp:77-155): the reference's steps with the quotient from the reciprocal
+// direction; border arrays stay in L1.
+// ---------------------------------------------------------------------------------------------
+struct CartesianFast : GenBase
 {
-    SKG_D static double big() { return DBL_MAX; }
-};
-
-// common part: exact moveInside (once per ray, FP64, as the reference) and the inverse direction
-template<typename Real>
-struct FastBase : GenBase
-{
-    Real ikx, iky, ikz;
-
-    SKG_D void startFast(double x, double y, double z, double ux, double uy, double uz)
-    {
-        startRay(x, y, z, ux, uy, uz);
-        const Real big = RealLimits<Real>::big();
-        ikx = fabs(ux) > 1e-15 ? Real(1) / Real(ux) : big;
-        iky = fabs(uy) > 1e-15 ? Real(1) / Real(uy) : big;
-        ikz = fabs(uz) > 1e-15 ? Real(1) / Real(uz) : big;
-    }
-
-    // distance from the entry point to the wall at coordinate w along an axis (FP32 after one FP64 difference)
-    SKG_D static Real dist(double w, double r, Real ik, double k)
-    {
-        return fabs(k) > 1e-15 ? Real(w - r) * ik : RealLimits<Real>::big();
-    }
-
-    // selects the exit axis with the reference's tie rule (x if dx<=dy && dx<=dz, y if dy<dx && dy<=dz
-    // for the Cartesian grid; the octree uses dy<=dx) and rebases the entry point on the exit wall
-    SKG_D int pickAxis(Real dx, Real dy, Real dz, bool yStrict, Real& d) const
-    {
-        bool isx = dx <= dy && dx <= dz;
-        bool isy = !isx && (yStrict ? dy < dx : dy <= dx) && dy <= dz;
-        int a = isx ? 0 : (isy ? 1 : 2);
-        d = isx ? dx : (isy ? dy : dz);
-        return a;
-    }
-
-    SKG_D void rebase(int axis, double wall, double d)
-    {
-        double nx = rx + kx * d, ny = ry + ky * d, nz = rz + kz * d;
-        rx = axis == 0 ? wall : nx;
-        ry = axis == 1 ? wall : ny;
-        rz = axis == 2 ? wall : nz;
-    }
-};
-
-template<typename Real>
-struct CartesianFast : FastBase<Real>
-{
-    using Acc = Real;
+    using Acc = float;
     static constexpr int kMinBlocks = 4;
     static constexpr int kRefillMin = 16;  // waiting lanes before a warp takes new tasks
     int i, j, k;
+    double ikx, iky, ikz;
 
     SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz, int = -1)
     {
-        this->startFast(x, y, z, ux, uy, uz);
+        startRay(x, y, z, ux, uy, uz);
+        ikx = recipDir(ux);
+        iky = recipDir(uy);
+        ikz = recipDir(uz);
     }
 
     SKG_D bool next(const GridDev& g)
     {
-        if (this->state == GS_OUTSIDE) return false;
-        if (this->state == GS_UNKNOWN)
+        if (state == GS_OUTSIDE) return false;
+        if (state == GS_UNKNOWN)
         {
-            if (!this->moveInside(g.ext, xmul(1e-12, boxDiagonal(g.ext)))) return false;
-            i = locateClip(g.xb, g.nx + 1, this->rx);
-            j = locateClip(g.yb, g.ny + 1, this->ry);
-            k = locateClip(g.zb, g.nz + 1, this->rz);
-            if (this->ds > 0.) return true;
+            if (!moveInside(g.ext, xmul(1e-12, boxDiagonal(g.ext)))) return false;
+            i = locateClip(g.xb, g.nx + 1, rx);
+            j = locateClip(g.yb, g.ny + 1, ry);
+            k = locateClip(g.zb, g.nz + 1, rz);
+            if (ds > 0.) return true;
         }
-        int sx = this->kx < 0.0 ? 0 : 1, sy = this->ky < 0.0 ? 0 : 1, sz = this->kz < 0.0 ? 0 : 1;
-        double xE = g.xb[i + sx], yE = g.yb[j + sy], zE = g.zb[k + sz];
-        Real d;
-        int a = this->pickAxis(this->dist(xE, this->rx, this->ikx, this->kx), this->dist(yE, this->ry, this->iky, this->ky),
-                               this->dist(zE, this->rz, this->ikz, this->kz), true, d);
-        this->m = k + g.nz * j + g.nz * g.ny * i;
-        this->ds = d;
-        this->rebase(a, a == 0 ? xE : (a == 1 ? yE : zE), this->ds);
-        i += a == 0 ? 2 * sx - 1 : 0;
-        j += a == 1 ? 2 * sy - 1 : 0;
-        k += a == 2 ? 2 * sz - 1 : 0;
-        if (i < 0 || i >= g.nx || j < 0 || j >= g.ny || k < 0 || k >= g.nz) this->state = GS_OUTSIDE;
+        int mm = k + g.nz * j + g.nz * g.ny * i;
+        double xE = (kx < 0.0) ? __ldg(g.xb + i) : __ldg(g.xb + i + 1);
+        double yE = (ky < 0.0) ? __ldg(g.yb + j) : __ldg(g.yb + j + 1);
+        double zE = (kz < 0.0) ? __ldg(g.zb + k) : __ldg(g.zb + k + 1);
+        double dsx = wallDist(xE, rx, kx, ikx);
+        double dsy = wallDist(yE, ry, ky, iky);
+        double dsz = wallDist(zE, rz, kz, ikz);
+        m = mm;
+        if (dsx <= dsy && dsx <= dsz)
+        {
+            ds = dsx;
+            rx = xE;
+            ry = xadd(ry, xmul(ky, dsx));
+            rz = xadd(rz, xmul(kz, dsx));
+            i += (kx < 0.0) ? -1 : 1;
+            if (i >= g.nx || i < 0) state = GS_OUTSIDE;
+        }
+        else if (dsy < dsx && dsy <= dsz)
+        {
+            ds = dsy;
+            ry = yE;
+            rx = xadd(rx, xmul(kx, dsy));
+            rz = xadd(rz, xmul(kz, dsy));
+            j += (ky < 0.0) ? -1 : 1;
+            if (j >= g.ny || j < 0) state = GS_OUTSIDE;
+        }
+        else
+        {
+            ds = dsz;
+            rz = zE;
+            rx = xadd(rx, xmul(kx, dsz));
+            ry = xadd(ry, xmul(ky, dsz));
+            k += (kz < 0.0) ? -1 : 1;
+            if (k >= g.nz || k < 0) state = GS_OUTSIDE;
+        }
         return true;
     }
 };
 
-// Octree walker on the leaf-indexed FP32 records. The current cell's record (bounds, density,
-// neighbour-list base) and wall counts are held in registers; a crossing loads the ids of the exit
-// wall's neighbours and their records until one contains the exit point, and that record becomes
-// the current one (two dependent loads per crossing, all from a working set that stays in L2).
-// resident 256-thread blocks per SM requested for the FP32 octree trace kernel (register limit)
-#ifndef SKG_OCTREE32_MIN_BLOCKS
-#define SKG_OCTREE32_MIN_BLOCKS 4
+// ---------------------------------------------------------------------------------------------
+// Octree, production (TreeSpatialGrid::MySegmentGenerator::next, TreeSpatialGrid.cpp:143-228,
+// TreeNode::neighbor, TreeNode.cpp:103-112). A crossing reads the current leaf's record for the exit
+// wall's neighbours, then one candidate's record and its six FP64 walls from the lattice tables:
+// the candidate becomes the current cell when it contains the new position (Box::contains, closed),
+// as the reference's first-in-overlap-order rule decides. When no positive-overlap neighbour holds
+// the position the walker runs the reference's complete procedure on the FP64 node arrays: the
+// wall's full neighbour list, the top-down search, the nextafter escape. A start in a known cell (a
+// scattering event's interaction cell) skips the top-down search when the top-down search would
+// return that cell (half-open bounds).
+// ---------------------------------------------------------------------------------------------
+#ifndef SKG_OCTREE_MIN_BLOCKS
+#define SKG_OCTREE_MIN_BLOCKS 4
 #endif
 
-struct OctreeLeaf32 : FastBase<float>
+struct OctreeRec : GenBase
 {
     using Acc = float;
-    static constexpr int kMinBlocks = SKG_OCTREE32_MIN_BLOCKS;
+    static constexpr int kMinBlocks = SKG_OCTREE_MIN_BLOCKS;
     static constexpr int kRefillMin = 16;  // waiting lanes before a warp takes new tasks
+    double ikx, iky, ikz;                  // reciprocal direction
+    double xE, yE, zE;                     // exit walls of the current cell in the direction of travel
     int cell;
-    float4 ra, rb;                 // bounds, density and list base of the current cell (record words 0-1)
-    float segDens;                 // density of the cell of the segment just returned
-    int hint;                      // the start cell when the caller knows it (an interaction cell), else -1
+    float cellDens, segDens;               // density of the current cell / of the segment just returned
+    int hint;                              // the start cell when the caller knows it, else -1
 
     SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz, int h = -1)
     {
-        this->startFast(x, y, z, ux, uy, uz);
+        startRay(x, y, z, ux, uy, uz);
+        ikx = recipDir(ux);
+        iky = recipDir(uy);
+        ikz = recipDir(uz);
         cell = -1;
         hint = h;
     }
 
     SKG_D double density(const double*) const { return static_cast<double>(segDens); }
 
-    SKG_D void enter(const GridDev& g, int c)
+    SKG_D static double wall(const GridDev& g, int axis, unsigned idx)
     {
-        cell = c;
-        ra = __ldg(g.tLeaf + 4 * static_cast<size_t>(c));
-        rb = __ldg(g.tLeaf + 4 * static_cast<size_t>(c) + 1);
+        return __ldg(g.tWall + axis * g.tWallN + idx);
     }
 
-    // top-down location of the leaf containing a point (FP64 bounds), as a cell index
+    // the six FP64 walls of cell c (lo then hi per axis) and its density
+    SKG_D static void walls(const GridDev& g, int c, double& x0, double& x1, double& y0, double& y1, double& z0,
+                            double& z1, float& dens)
+    {
+        int4 w = __ldg(g.tRec + 4 * static_cast<size_t>(c));
+        x0 = wall(g, 0, static_cast<unsigned>(w.x) & 0xFFFFu);
+        x1 = wall(g, 0, static_cast<unsigned>(w.x) >> 16);
+        y0 = wall(g, 1, static_cast<unsigned>(w.y) & 0xFFFFu);
+        y1 = wall(g, 1, static_cast<unsigned>(w.y) >> 16);
+        z0 = wall(g, 2, static_cast<unsigned>(w.z) & 0xFFFFu);
+        z1 = wall(g, 2, static_cast<unsigned>(w.z) >> 16);
+        dens = __int_as_float(w.w);
+    }
+
+    SKG_D void become(int c, double x0, double x1, double y0, double y1, double z0, double z1, float dens)
+    {
+        cell = c;
+        xE = kx < 0.0 ? x0 : x1;
+        yE = ky < 0.0 ? y0 : y1;
+        zE = kz < 0.0 ? z0 : z1;
+        cellDens = dens;
+    }
+
+    SKG_D void enter(const GridDev& g, int c)
+    {
+        double x0, x1, y0, y1, z0, z1;
+        float d;
+        walls(g, c, x0, x1, y0, y1, z0, z1, d);
+        become(c, x0, x1, y0, y1, z0, z1, d);
+    }
+
+    // Box::contains (closed bounds) of cell c; on success c becomes the current cell
+    SKG_D bool tryEnter(const GridDev& g, int c)
+    {
+        double x0, x1, y0, y1, z0, z1;
+        float d;
+        walls(g, c, x0, x1, y0, y1, z0, z1, d);
+        bool in = rx >= x0 && rx <= x1 && ry >= y0 && ry <= y1 && rz >= z0 && rz <= z1;
+        if (in) become(c, x0, x1, y0, y1, z0, z1, d);
+        return in;
+    }
+
+    // the known start cell, if the top-down search (TreeNode::leafChild with OctTreeNode::child:
+    // lower half for coordinates below the centre) would return it: lo <= r < hi per axis, or r on
+    // the domain's upper wall
+    SKG_D bool tryHint(const GridDev& g, int c)
+    {
+        double x0, x1, y0, y1, z0, z1;
+        float d;
+        walls(g, c, x0, x1, y0, y1, z0, z1, d);
+        bool in = rx >= x0 && (rx < x1 || (rx == x1 && x1 == g.ext[3])) && ry >= y0 && (ry < y1 || (ry == y1 && y1 == g.ext[4]))
+                  && rz >= z0 && (rz < z1 || (rz == z1 && z1 == g.ext[5]));
+        if (in) become(c, x0, x1, y0, y1, z0, z1, d);
+        return in;
+    }
+
     SKG_D static int locate(const GridDev& g, double x, double y, double z)
     {
         int n = octreeLeafChild(g, x, y, z);
         return n < 0 ? -1 : g.tCell[n];
     }
 
-    // half-open interval test in the direction of travel: a point on the boundary belongs to the
-    // interval the ray moves into (closed on both ends for a zero direction component)
-    SKG_D static bool within(float p, float lo, float hi, double k)
-    {
-        return k > 0.0 ? (p >= lo && p < hi) : (k < 0.0 ? (p > lo && p <= hi) : (p >= lo && p <= hi));
-    }
-
     SKG_D bool next(const GridDev& g)
     {
-        if (this->state == GS_OUTSIDE) return false;
-        if (this->state == GS_UNKNOWN)
+        if (state == GS_OUTSIDE) return false;
+        if (state == GS_UNKNOWN)
         {
-            if (!this->moveInside(g.ext, g.eps)) return false;
-            // a start inside the domain in a known cell needs no top-down search
-            int c = (hint >= 0 && this->ds == 0.) ? hint : locate(g, this->rx, this->ry, this->rz);
-            if (c < 0)
+            if (!moveInside(g.ext, g.eps)) return false;
+            if (!(hint >= 0 && ds == 0. && tryHint(g, hint)))
             {
-                this->state = GS_OUTSIDE;
-                return false;
+                int c = locate(g, rx, ry, rz);
+                if (c < 0)
+                {
+                    state = GS_OUTSIDE;
+                    return false;
+                }
+                enter(g, c);
             }
-            enter(g, c);
-            if (this->ds > 0.) return true;
+            if (ds > 0.) return true;
         }
-        double xE = this->kx < 0.0 ? ra.x : ra.w;
-        double yE = this->ky < 0.0 ? ra.y : rb.x;
-        double zE = this->kz < 0.0 ? ra.z : rb.y;
-        float d;
-        int a = this->pickAxis(this->dist(xE, this->rx, this->ikx, this->kx), this->dist(yE, this->ry, this->iky, this->ky),
-                               this->dist(zE, this->rz, this->ikz, this->kz), false, d);
-        // the entry point may lie a rounding error beyond a wall of a cell entered through the
-        // fallback below: never step backwards, so that the walk advances monotonically
-        d = fmaxf(d, 0.f);
-        int wall = 2 * a + ((a == 0 ? this->kx : (a == 1 ? this->ky : this->kz)) < 0.0 ? 0 : 1);
-        this->m = cell;
-        this->ds = d;
-        segDens = rb.z;
-        this->rebase(a, a == 0 ? xE : (a == 1 ? yE : zE), this->ds);
-        // words 2-3 of the record (same cache line as words 0-1): the list offsets and, per wall,
-        // the single neighbour across it (-1: domain wall, -2: several neighbours)
-        const int* w23 = reinterpret_cast<const int*>(g.tLeaf + 4 * static_cast<size_t>(cell) + 2);
-        int one = __ldg(w23 + 2 + wall);
-        int old = cell, nb = -1;
+        double dsx = wallDist(xE, rx, kx, ikx);
+        double dsy = wallDist(yE, ry, ky, iky);
+        double dsz = wallDist(zE, rz, kz, ikz);
+        double d;
+        int wl;
+        if (dsx <= dsy && dsx <= dsz)
+        {
+            d = dsx;
+            wl = kx < 0.0 ? 0 : 1;
+        }
+        else if (dsy <= dsx && dsy <= dsz)
+        {
+            d = dsy;
+            wl = ky < 0.0 ? 2 : 3;
+        }
+        else
+        {
+            d = dsz;
+            wl = kz < 0.0 ? 4 : 5;
+        }
+        propagater(xadd(d, g.eps));
+        m = cell;
+        ds = d;
+        segDens = cellDens;
+        const int old = cell;
+        const int* R = reinterpret_cast<const int*>(g.tRec + 4 * static_cast<size_t>(old));
+        int one = __ldg(R + 8 + wl);
+        bool found = false;
         if (one >= 0)
         {
-            enter(g, one);
-            return true;
+            found = tryEnter(g, one);
         }
-        if (one == -1)
+        else if (one == -2)
         {
-            this->state = GS_OUTSIDE;
-            return true;
-        }
-        unsigned long long cnt = (static_cast<unsigned long long>(static_cast<unsigned>(__ldg(w23 + 1))) << 32)
-                                 | static_cast<unsigned>(__ldg(w23));
-        int base = __float_as_int(rb.w);
-        bool listed = cnt != ~0ULL;
-        int e0 = base + static_cast<int>((cnt >> (9 * wall)) & 511);
-        int n = listed ? base + static_cast<int>((cnt >> (9 * (wall + 1))) & 511) - e0 : 0;
-        float pu = static_cast<float>(a == 0 ? this->ry : this->rx);
-        float pv = static_cast<float>(a == 2 ? this->ry : this->rz);
-        double ku = a == 0 ? this->ky : this->kx;
-        double kv = a == 2 ? this->ky : this->kz;
-        for (int e = 0; e < n; ++e)
-        {
-            int c = __ldg(g.tLeafNb + e0 + e);
-            float4 qa = __ldg(g.tLeaf + 4 * static_cast<size_t>(c)), qb = __ldg(g.tLeaf + 4 * static_cast<size_t>(c) + 1);
-            float ulo = a == 0 ? qa.y : qa.x, uhi = a == 0 ? qb.x : qa.w;
-            float vlo = a == 2 ? qa.y : qa.z, vhi = a == 2 ? qb.x : qb.y;
-            if (within(pu, ulo, uhi, ku) && within(pv, vlo, vhi, kv))
+            unsigned long long cnt = (static_cast<unsigned long long>(static_cast<unsigned>(__ldg(R + 6))) << 32)
+                                     | static_cast<unsigned>(__ldg(R + 5));
+            if (cnt != ~0ULL)
             {
-                nb = c;
-                cell = c;
-                ra = qa;
-                rb = qb;
-                break;
+                int base = __ldg(R + 4);
+                int e0 = base + static_cast<int>((cnt >> (9 * wl)) & 511);
+                int e1 = base + static_cast<int>((cnt >> (9 * (wl + 1))) & 511);
+                for (int e = e0; e < e1 && !found; ++e) found = tryEnter(g, __ldg(g.tLeafNb + e));
             }
         }
-        if (nb < 0)
+        if (!found)
         {
-            // No listed neighbour holds the exit point (a wall without list, or an exit point on a
-            // cell edge). Move the point forward along every axis by a few FP32 roundings of the
-            // coordinates (so that it lies beyond any FP32-rounded wall it sits on) and locate it
-            // top-down in the FP64 tree; a point outside the domain ends the path.
-            double big = fmax(fabs(this->rx), fmax(fabs(this->ry), fabs(this->rz)));
-            double e = fmax(g.eps, 4.8e-7 * big);
-            this->rx += this->kx > 0.0 ? e : (this->kx < 0.0 ? -e : 0.0);
-            this->ry += this->ky > 0.0 ? e : (this->ky < 0.0 ? -e : 0.0);
-            this->rz += this->kz > 0.0 ? e : (this->kz < 0.0 ? -e : 0.0);
-            nb = locate(g, this->rx, this->ry, this->rz);
-            if (nb >= 0 && nb != old) enter(g, nb);
+            // the reference's complete procedure on the FP64 node arrays: the wall's full neighbour
+            // list in overlap order, the top-down search, the nextafter escape
+            int node = __ldg(R + 7);
+            int nb = -1;
+            int e1 = g.tNbBegin[6 * node + wl + 1];
+            for (int e = g.tNbBegin[6 * node + wl]; e < e1; ++e)
+            {
+                int cand = g.tNb[e];
+                if (boxContains(g.tBounds + 6 * static_cast<size_t>(cand), rx, ry, rz))
+                {
+                    nb = cand;
+                    break;
+                }
+            }
+            if (nb < 0) nb = octreeLeafChild(g, rx, ry, rz);
+            if (nb == node)
+            {
+                rx = nextafter(rx, (kx < 0.) ? -DBL_MAX : DBL_MAX);
+                ry = nextafter(ry, (ky < 0.) ? -DBL_MAX : DBL_MAX);
+                rz = nextafter(rz, (kz < 0.) ? -DBL_MAX : DBL_MAX);
+                nb = octreeLeafChild(g, rx, ry, rz);
+            }
+            if (nb < 0 || nb == node)
+                state = GS_OUTSIDE;
+            else
+                enter(g, g.tCell[nb]);
         }
-        if (nb < 0 || nb == old) this->state = GS_OUTSIDE;
         return true;
     }
 };
 
+
+// Octree, production precision for trees that are not a lattice of depth <= 15 (no leaf records):
+// the FP64 node walker with FP32 accumulators
+struct OctreeNodeFast : OctreeExact
+{
+    using Acc = float;
+};
 
 // Nearest site of a point by a greedy walk on the neighbour graph (the Delaunay graph of the sites,
 // on which the walk towards ever nearer sites ends at the nearest one), starting from the

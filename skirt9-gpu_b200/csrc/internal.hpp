@@ -32,6 +32,9 @@ cudaError_t runWaveFP64(int gridKind, const Wave& w, int numSMs, cudaStream_t s,
 cudaError_t runWaveFP32(int gridKind, const Wave& w, int numSMs, cudaStream_t s, unsigned long long* doneHost,
                         long long* passes, long long maxPasses, bool useGraph, StageTimer* timer, GraphCache* cache);
 
+// moments of the grouped per-history statistics of the spill log (n records)
+cudaError_t groupStats(const Wave& w, const StatSpill* groups, unsigned long long n, int numSMs, cudaStream_t s);
+
 // wavelength order of the histories of w's range into order[] (keys: count entries, counts and
 // cursor: ORDER_BUCKETS entries each, zeroed here)
 cudaError_t orderHistories(const Wave& w, unsigned short* keys, unsigned* counts, unsigned* cursor, unsigned* order,

@@ -1,6 +1,5 @@
-// Path-segment and optical-depth kernels with the FP32 walkers that keep the reference generators'
-// operation order. They back skgpu_trace_paths / skgpu_optical_depths, the replacements of the
-// reference's per-path GPU wrappers (GpuAcceleration::set*SpatialGridPath and the optical-depth
+// Path-segment and optical-depth kernels with the production walkers. They back skgpu_trace_paths /
+// skgpu_optical_depths, the replacements of the reference's per-path GPU wrappers (GpuAcceleration::set*SpatialGridPath and the optical-depth
 // sums, GpuAcceleration.hpp), and they are what the cell-sequence parity tests call.
 #include "internal.hpp"
 #include "paths.cuh"
@@ -16,8 +15,13 @@ cudaError_t launchTracePathsFP32(int precision, const GridDev& g, int n, const d
     (void)precision;
     switch (g.kind)
     {
-        case 0: tracePathsKernel<CartesianFast<float>><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
-        case 1: tracePathsKernel<OctreeLeaf32><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
+        case 0: tracePathsKernel<CartesianFast><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
+        case 1:
+            if (g.tWallN)
+                tracePathsKernel<OctreeRec><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err);
+            else
+                tracePathsKernel<OctreeNodeFast><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err);
+            break;
         case 2: tracePathsKernel<VoronoiRec32><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
         case 3: tracePathsKernel<TetraPlane32><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
         case 4: tracePathsKernel<Sphere1DFast><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
@@ -38,8 +42,13 @@ cudaError_t launchOpticalDepthsFP32(int precision, const GridDev& g, const doubl
     (void)precision;
     switch (g.kind)
     {
-        case 0: opticalDepthKernel<CartesianFast<float>><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
-        case 1: opticalDepthKernel<OctreeLeaf32><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
+        case 0: opticalDepthKernel<CartesianFast><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
+        case 1:
+            if (g.tWallN)
+                opticalDepthKernel<OctreeRec><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err);
+            else
+                opticalDepthKernel<OctreeNodeFast><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err);
+            break;
         case 2: opticalDepthKernel<VoronoiRec32><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
         case 3: opticalDepthKernel<TetraPlane32><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
         case 4: opticalDepthKernel<Sphere1DFast><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;

@@ -8,7 +8,10 @@
 namespace skg {
 
 constexpr int MAX_INSTR = 16;
-constexpr int STATS_CAP = 48;
+// distinct (instrument, wavelength bin, pixel) keys buffered per packet slot for the per-history
+// statistics: with the wavefront's own buffers, and within the static scratch of the no-allocation run
+constexpr int STATS_CAP = 128;
+constexpr int STATS_CAP_NOALLOC = 48;
 constexpr int MAX_SCATT_EVENTS = 1 << 20;
 
 struct SourceDev

@@ -11,6 +11,7 @@
 #include <type_traits>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <string>
 #include <thread>
 #include <vector>
@@ -110,18 +111,18 @@ bool finiteAll(const double* v, size_t n)
 }
 
 // copies the number densities into the FP32 leaf records of an octree grid (4 float4 per leaf)
-__global__ void fillLeafDensityKernel(float4* leaf, const double* dens, int n)
+__global__ void fillLeafDensityKernel(int4* rec, const double* dens, int n)
 {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c < n) leaf[4 * static_cast<size_t>(c) + 1].z = static_cast<float>(dens[c]);
+    if (c < n) rec[4 * static_cast<size_t>(c)].w = __float_as_int(static_cast<float>(dens[c]));
 }
 
 int syncLeafDensity(skgpu_ctx* ctx)
 {
-    if (!ctx->hasGrid || ctx->g.kind != SKGPU_GRID_OCTREE || !ctx->g.tLeaf || !ctx->dens) return SKGPU_OK;
+    if (!ctx->hasGrid || ctx->g.kind != SKGPU_GRID_OCTREE || !ctx->g.tRec || !ctx->dens) return SKGPU_OK;
     if (ctx->numCells != ctx->g.numCells) return SKGPU_OK;  // checked again at run time
     int n = ctx->numCells;
-    fillLeafDensityKernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(const_cast<float4*>(ctx->g.tLeaf), ctx->dens, n);
+    fillLeafDensityKernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(const_cast<int4*>(ctx->g.tRec), ctx->dens, n);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(ctx->stream));
     return SKGPU_OK;
@@ -168,6 +169,9 @@ int ensureWaveBuffers(skgpu_ctx* ctx, int P, int groups, int stats)
     size_t ns = stats ? static_cast<size_t>(P) * STATS_CAP : 1;
     if ((rc = waveAlloc(ctx, &k.skey, ns))) return rc;
     if ((rc = waveAlloc(ctx, &k.sw, ns))) return rc;
+    // spill log of the per-history statistics: histories with more than STATS_CAP distinct keys
+    k.spillCap = stats ? std::max<size_t>(size_t(1) << 20, 2 * static_cast<size_t>(P)) : 1;
+    if ((rc = waveAlloc(ctx, &k.spill, k.spillCap))) return rc;
     if ((rc = waveAlloc(ctx, &k.gD, P))) return rc;
     if ((rc = waveAlloc(ctx, &k.gLast, P))) return rc;
     if ((rc = waveAlloc(ctx, &k.gPend, P))) return rc;
@@ -372,27 +376,88 @@ int skgpu_upload_grid_octree(skgpu_ctx* ctx, int32_t num_nodes, const double* bo
     if ((rc = gridUpload<int>(ctx, &g.tChild, firstChild.data(), num_nodes))) return rc;
     if ((rc = gridUpload<int>(ctx, &g.tNbBegin, nb_begin, 6 * static_cast<size_t>(num_nodes) + 1))) return rc;
     if ((rc = gridUpload<int>(ctx, &g.tNb, nb_index, num_nb_index))) return rc;
-    // Leaf-indexed 64-byte records of the production walker (cell c <-> its leaf node), four float4:
-    //   [0] lo.x lo.y lo.z hi.x   [1] hi.y hi.z density base   [2] cnt.lo cnt.hi one[0] one[1]
-    //   [3] one[2] one[3] one[4] one[5]
-    // FP32 bounds, FP32 density (filled when the medium is uploaded), the base of the cell's neighbour
-    // list, the 9-bit cumulative offsets of its 6 walls in the list (all ones: no list), and per wall
-    // the one neighbour across it when there is exactly one (-1: no neighbour, the domain wall;
-    // -2: several, scan the list). The lists hold per wall the positive-overlap neighbours in the
-    // reference's overlap order (zero-overlap entries, which only touch an edge, come last in the
-    // reference's lists and are left out: exit points on an edge are resolved by the top-down fallback).
+    // The octree's lattice. OctTreeNode::createChildren (OctTreeNode.cpp:15-25) gives each child a
+    // copy of its parent's bounds and centre, so in a tree of depth L every wall coordinate is one of
+    // 2^L + 1 FP64 values per axis, indexed by its position at the finest level (root [0, 2^L]).
+    // The production walker's records hold these 16-bit indices (L <= 15) and the walker reads the
+    // exact FP64 walls from three small tables. A tree that is not such a lattice (or deeper) gets
+    // no production records; its FP32-precision runs use the FP64 node walker.
+    std::vector<int> depth(num_nodes, -1), ilo(3 * static_cast<size_t>(num_nodes)), ihi(3 * static_cast<size_t>(num_nodes));
+    std::vector<int> queue{0};
+    depth[0] = 0;
+    int L = 0;
+    for (size_t qi = 0; qi < queue.size(); ++qi)
+    {
+        int l = queue[qi];
+        L = std::max(L, depth[l]);
+        if (firstChild[l] < 0) continue;
+        for (int q = 0; q < 8; ++q)
+        {
+            int c = firstChild[l] + q;
+            if (depth[c] >= 0) return fail(ctx, SKGPU_ERR_ARG, "octree: a node is the child of two nodes");
+            depth[c] = depth[l] + 1;
+            queue.push_back(c);
+        }
+    }
+    if (static_cast<int>(queue.size()) != num_nodes) return fail(ctx, SKGPU_ERR_ARG, "octree: nodes unreachable from the root");
+    bool lattice = L <= 15;
+    const int N = lattice ? (1 << L) : 0;
+    std::vector<double> wall(lattice ? 3 * static_cast<size_t>(N + 1) : 0, std::numeric_limits<double>::quiet_NaN());
+    if (lattice)
+    {
+        for (int a = 0; a < 3; ++a)
+        {
+            ilo[a] = 0;
+            ihi[a] = N;
+        }
+        for (size_t qi = 0; qi < queue.size() && lattice; ++qi)
+        {
+            int l = queue[qi];
+            const double* b = bounds + 6 * static_cast<size_t>(l);
+            for (int a = 0; a < 3 && lattice; ++a)
+            {
+                int lo = ilo[3 * static_cast<size_t>(l) + a], hi = ihi[3 * static_cast<size_t>(l) + a];
+                double* wl = &wall[static_cast<size_t>(a) * (N + 1) + lo];
+                double* wh = &wall[static_cast<size_t>(a) * (N + 1) + hi];
+                if (std::isnan(*wl)) *wl = b[a];
+                if (std::isnan(*wh)) *wh = b[3 + a];
+                lattice = *wl == b[a] && *wh == b[3 + a] && hi > lo;
+            }
+            if (!lattice || firstChild[l] < 0) continue;
+            for (int q = 0; q < 8; ++q)
+            {
+                int c = firstChild[l] + q;
+                for (int a = 0; a < 3; ++a)
+                {
+                    int lo = ilo[3 * static_cast<size_t>(l) + a], hi = ihi[3 * static_cast<size_t>(l) + a], mid = (lo + hi) / 2;
+                    bool upper = (q >> a) & 1;
+                    ilo[3 * static_cast<size_t>(c) + a] = upper ? mid : lo;
+                    ihi[3 * static_cast<size_t>(c) + a] = upper ? hi : mid;
+                }
+            }
+        }
+    }
+    g.tWallN = 0;
+    if (!lattice)
+    {
+        ctx->hasGrid = true;
+        return syncLeafDensity(ctx);
+    }
+    // Leaf-indexed 64-byte records of the production walker (cell c <-> its leaf node), four int4:
+    //   [0] wall indices x lo | hi << 16, y, z; FP32 density (filled when the medium is uploaded)
+    //   [1] neighbour-list base, the 9-bit cumulative offsets of the 6 walls in the list (64 bits, all
+    //       ones: no list), the leaf's node id (for the full neighbour lists of the exact fallback)
+    //   [2] [3] per wall the one neighbour across it when there is exactly one (-1: no neighbour, the
+    //       domain wall; -2: several, scan the list), two spare words
+    // The lists hold per wall the positive-overlap neighbours in the reference's overlap order;
+    // zero-overlap entries, which only touch an edge, come last in the reference's lists (TreeNode
+    // sortNeighbors, TreeNode.cpp:200-207) and are left to the walker's exact fallback.
     std::vector<int> leafNode(numCells, -1);
     for (int l = 0; l < num_nodes; ++l)
         if (cell_index[l] >= 0) leafNode[cell_index[l]] = l;
-    std::vector<float4> leaf(4 * static_cast<size_t>(numCells));
+    std::vector<int4> rec(4 * static_cast<size_t>(numCells));
     std::vector<int> leafNb;
     leafNb.reserve(static_cast<size_t>(numCells) * 8);
-    auto bitsOf = [](auto v) {
-        float f;
-        static_assert(sizeof v == sizeof f, "32-bit field");
-        std::memcpy(&f, &v, sizeof f);
-        return f;
-    };
     for (int c = 0; c < numCells; ++c)
     {
         int l = leafNode[c];
@@ -400,7 +465,7 @@ int skgpu_upload_grid_octree(skgpu_ctx* ctx, int32_t num_nodes, const double* bo
         const double* b = bounds + 6 * static_cast<size_t>(l);
         int base = static_cast<int>(leafNb.size());
         // per wall the positive-overlap neighbours; 9-bit cumulative offsets of the 6 walls + end
-        // (a leaf with more than 511 such neighbours gets no list: its exits use the top-down search)
+        // (a leaf with more than 511 such neighbours gets no list: its exits use the exact fallback)
         std::vector<int> lists[6];
         size_t total = 0;
         for (int w = 0; w < 6; ++w)
@@ -436,18 +501,22 @@ int skgpu_upload_grid_octree(skgpu_ctx* ctx, int32_t num_nodes, const double* bo
         int one[6];
         for (int w = 0; w < 6; ++w)
             one[w] = lists[w].size() == 1 ? lists[w][0] : (lists[w].empty() && total <= 511 ? -1 : -2);
-        float4* r = &leaf[4 * static_cast<size_t>(c)];
-        r[0] = make_float4(static_cast<float>(b[0]), static_cast<float>(b[1]), static_cast<float>(b[2]),
-                           static_cast<float>(b[3]));
-        r[1] = make_float4(static_cast<float>(b[4]), static_cast<float>(b[5]), 0.f, bitsOf(base));
-        r[2] = make_float4(bitsOf(static_cast<unsigned>(cnt)), bitsOf(static_cast<unsigned>(cnt >> 32)),
-                           bitsOf(one[0]), bitsOf(one[1]));
-        r[3] = make_float4(bitsOf(one[2]), bitsOf(one[3]), bitsOf(one[4]), bitsOf(one[5]));
+        auto idx = [&](int a) {
+            return static_cast<int>(static_cast<unsigned>(ilo[3 * static_cast<size_t>(l) + a])
+                                    | (static_cast<unsigned>(ihi[3 * static_cast<size_t>(l) + a]) << 16));
+        };
+        int4* r = &rec[4 * static_cast<size_t>(c)];
+        r[0] = make_int4(idx(0), idx(1), idx(2), 0);
+        r[1] = make_int4(base, static_cast<int>(static_cast<unsigned>(cnt)), static_cast<int>(static_cast<unsigned>(cnt >> 32)), l);
+        r[2] = make_int4(one[0], one[1], one[2], one[3]);
+        r[3] = make_int4(one[4], one[5], 0, 0);
         if (leafNb.size() > 2147483647ULL) return fail(ctx, SKGPU_ERR_ARG, "octree: neighbour lists too long");
     }
     if (leafNb.empty()) leafNb.push_back(0);
-    if ((rc = gridUpload<float4>(ctx, &g.tLeaf, leaf.data(), leaf.size()))) return rc;
+    if ((rc = gridUpload<int4>(ctx, &g.tRec, rec.data(), rec.size()))) return rc;
     if ((rc = gridUpload<int>(ctx, &g.tLeafNb, leafNb.data(), leafNb.size()))) return rc;
+    if ((rc = gridUpload<double>(ctx, &g.tWall, wall.data(), wall.size()))) return rc;
+    g.tWallN = N + 1;
     ctx->hasGrid = true;
     return syncLeafDensity(ctx);
 }
@@ -1163,6 +1232,33 @@ static int prepareOrder(skgpu_ctx* ctx, Wave& w)
     return SKGPU_OK;
 }
 
+// FluxRecorder::recordContributions for the histories that spilled: their contributions (all in the
+// spill log once they ended) are summed per (history, key) on the host, written back over the log,
+// and a kernel adds w^0..w^4 of each sum into the statistics tallies. Allocates no device memory.
+static int groupSpilledStats(skgpu_ctx* ctx, const Wave& w, unsigned long long n)
+{
+    std::vector<StatSpill> log(n);
+    CK(cudaMemcpy(log.data(), w.pk.spill, n * sizeof(StatSpill), cudaMemcpyDeviceToHost));
+    std::stable_sort(log.begin(), log.end(), [](const StatSpill& a, const StatSpill& b) {
+        if (a.scene != b.scene) return a.scene < b.scene;
+        if (a.hist != b.hist) return a.hist < b.hist;
+        return a.key < b.key;
+    });
+    std::vector<StatSpill> groups;
+    for (size_t i = 0; i < log.size();)
+    {
+        StatSpill g = log[i];
+        size_t j = i + 1;
+        for (; j < log.size() && log[j].scene == g.scene && log[j].hist == g.hist && log[j].key == g.key; ++j) g.w += log[j].w;
+        groups.push_back(g);
+        i = j;
+    }
+    CK(cudaMemcpy(w.pk.spill, groups.data(), groups.size() * sizeof(StatSpill), cudaMemcpyHostToDevice));
+    CK(groupStats(w, w.pk.spill, groups.size(), ctx->numSMs, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return SKGPU_OK;
+}
+
 // runs the wavefront on prepared buffers and collects the counters and status of the run
 static int runAndCollect(skgpu_ctx* ctx, const Wave& w, bool useGraph, bool timed)
 {
@@ -1203,11 +1299,20 @@ static int runAndCollect(skgpu_ctx* ctx, const Wave& w, bool useGraph, bool time
     ctx->lastCounters.peel_detections = ctl.counters[3];
     ctx->lastCounters.rf_stores = ctl.counters[4];
     ctx->lastCounters.stats_overflows = ctl.counters[5];
+    ctx->lastCounters.stats_spilled = ctl.counters[6];
     ctx->lastCounters.kernel_launches = static_cast<uint64_t>(passes) * (w.sc.guideMode == 2 ? 8 : 7) + 1 + (w.order ? 3 : 0);
     ctx->lastPasses = passes;
     ctx->lastGuideWeightSum = ctl.guideWeightSum;
     ctx->lastGuideEvents = ctl.guideEvents;
     if (w.count > 0 && ctl.done != w.count) return fail(ctx, SKGPU_ERR_DEVICE, "run: not every history finished");
+    if (errFlag & 64)
+        return fail(ctx, SKGPU_ERR_DEVICE, "run: the per-history statistics spill log is full ("
+                                               + std::to_string(ctl.counters[5]) + " contributions lost)");
+    if (ctl.spillN > 0)
+    {
+        int rc = groupSpilledStats(ctx, w, ctl.spillN);
+        if (rc) return rc;
+    }
     if (errFlag & 4) return fail(ctx, SKGPU_ERR_TIMEOUT, "run: a traversal exceeded its segment guard");
     if (errFlag & 8) return fail(ctx, SKGPU_ERR_TIMEOUT, "run: a history exceeded the scattering-event guard");
     if (errFlag & 16) return fail(ctx, SKGPU_ERR_TIMEOUT, "run: a tensor-core wait of the guided-scattering stage gave up");
@@ -1251,6 +1356,7 @@ int skgpu_run_primary(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t t
     w.first = first;
     w.count = count;
     w.anyStats = anyStats;
+    w.statCap = STATS_CAP;
     if ((rc = prepareOrder(ctx, w))) return rc;
     return runAndCollect(ctx, w, true, true);
 }
@@ -1306,6 +1412,9 @@ int skgpu_probe_launch(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t 
 // GPU that loads this library holds it until the process exits.
 static __device__ __align__(256) unsigned char g_noallocScratch[SKGPU_NOALLOC_SCRATCH_BYTES];
 
+// entries of the statistics spill log within the static scratch
+constexpr size_t NOALLOC_SPILL = size_t(1) << 16;
+
 // lays the wavefront buffers for P slots out in a scratch area (base may be null: size only)
 static size_t carveWave(Wave& w, unsigned char* base, int P, int groups, int stats)
 {
@@ -1320,9 +1429,11 @@ static size_t carveWave(Wave& w, unsigned char* base, int P, int groups, int sta
     take(&k.rec, P);
     take(&k.nstat, P);
     take(&k.freeSlots, P);
-    size_t ns = stats ? static_cast<size_t>(P) * STATS_CAP : 1;
+    size_t ns = stats ? static_cast<size_t>(P) * STATS_CAP_NOALLOC : 1;
     take(&k.skey, ns);
     take(&k.sw, ns);
+    k.spillCap = stats ? NOALLOC_SPILL : 1;
+    take(&k.spill, k.spillCap);
     for (int b = 0; b < 2; ++b)
         for (int kind = 0; kind < NUM_KINDS; ++kind)
         {
@@ -1387,6 +1498,7 @@ int skgpu_run_primary_noalloc(skgpu_ctx* ctx, uint64_t first, uint64_t count, ui
     w.first = first;
     w.count = count;
     w.anyStats = anyStats;
+    w.statCap = STATS_CAP_NOALLOC;
     return runAndCollect(ctx, w, false, false);
 }
 
@@ -1957,6 +2069,7 @@ int skgpu_run_batch(skgpu_ctx* const* ctxs, int32_t n, const uint64_t* first, co
     w.first = 0;
     w.count = sum;
     w.anyStats = anyStats;
+    w.statCap = STATS_CAP;
     w.traceBlocksPerSM = ctx->shapeTraceBlocks;
     w.shadeBlocksPerSM = ctx->shapeShadeBlocks;
     if ((rc = prepareOrder(ctx, w))) return rc;

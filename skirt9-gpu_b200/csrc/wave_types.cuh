@@ -28,13 +28,28 @@ struct alignas(128) PacketRec
 };
 static_assert(sizeof(PacketRec) == 128, "one line per packet");
 
+// A per-history statistics contribution that did not fit its slot's buffer; the history's buffered
+// contributions join it when the history ends, and all are grouped per history after the run. The
+// same record carries the grouped sums to the kernel that adds their moments.
+struct StatSpill
+{
+    unsigned long long hist;
+    unsigned long long key;  // instrument << 48 | wavelength bin << 24 | pixel + 1
+    double w;
+    int scene;
+    int pad;
+};
+
 struct PacketPool
 {
     PacketRec* rec;  // P
-    // per-history statistics buffer (only when an instrument records statistics)
-    unsigned long long* skey;  // P * STATS_CAP
+    // per-history statistics buffer (only when an instrument records statistics): statCap distinct
+    // (instrument, bin, pixel) keys per slot with their summed contributions; unused keys are ~0
+    unsigned long long* skey;  // P * statCap
     double* sw;
-    int* nstat;
+    int* nstat;                // entries taken; above statCap the history has spilled
+    StatSpill* spill;          // spill log of the run
+    unsigned long long spillCap;
     int* freeSlots;            // P
     // pilot records of the guiding network: luminosity of the history detected by the target
     // instrument so far, last recorded event, event whose start value is still open
@@ -68,7 +83,10 @@ struct Control
     unsigned long long launched;
     unsigned long long done;
     unsigned long long launchHist0;
-    unsigned long long counters[8];  // histories, crossings, scatterings, detections, rfStores, overflows
+    // histories, crossings, scatterings, detections, rfStores, statistics contributions lost (spill
+    // log full), contributions spilled, traversal-guard reports
+    unsigned long long counters[8];
+    unsigned long long spillN;       // entries written to the statistics spill log
     double guideWeightSum;           // guided scattering: sum of the weight factors (mean 1 in expectation)
     unsigned long long guideEvents;  // guided scattering events
     int err;
@@ -101,6 +119,7 @@ struct Wave
     int P;
     unsigned long long first, count;
     int anyStats;
+    int statCap;  // per-slot statistics buffer entries
 };
 
 }  // namespace skg

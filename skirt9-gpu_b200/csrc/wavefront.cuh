@@ -91,29 +91,91 @@ SKG_D void statMoments(const Scene& sc, unsigned long long key, double wsum)
     }
 }
 
-// FluxRecorder::recordContributions (FluxRecorder.cpp:1355-1409): group the history's
-// contributions per (instrument, wavelength bin, pixel) and add w^0..w^4
+// appends one contribution of the slot's history to the spill log (grouped after the run)
+SKG_D void spillStat(const Wave& w, int slot, unsigned long long key, double v)
+{
+    unsigned long long i = atomicAdd(&w.ctl->spillN, 1ULL);
+    if (i < w.pk.spillCap)
+    {
+        StatSpill& e = w.pk.spill[i];
+        e.hist = w.pk.rec[slot].hist;
+        e.key = key;
+        e.w = v;
+        e.scene = w.nScenes > 1 ? w.pk.rec[slot].scene : 0;
+        atomicAdd(&w.ctl->counters[6], 1ULL);
+    }
+    else
+    {
+        atomicAdd(&w.ctl->counters[5], 1ULL);  // lost: the run fails
+        atomicOr(&w.ctl->err, 64);
+    }
+}
+
+// FluxRecorder::recordContributions (FluxRecorder.cpp:1355-1409) groups a history's contributions
+// per (instrument, wavelength bin, pixel). Here a contribution is added to its key's entry in the
+// slot's buffer, or takes a new entry. The threads that record one slot at the same time (one
+// shadePeelKernel thread per observer group of the slot's event) hold keys of different
+// instruments, so a key found in the buffer comes from an earlier pass and nobody else updates it;
+// an entry being written concurrently still holds the empty key ~0 or a key of another instrument.
+// A contribution that finds the buffer full goes to the spill log.
+SKG_D void recordStat(const Wave& w, int slot, unsigned long long key, double v)
+{
+    const int cap = w.statCap;
+    unsigned long long* keys = w.pk.skey + static_cast<size_t>(slot) * cap;
+    double* sw = w.pk.sw + static_cast<size_t>(slot) * cap;
+    int n = min(*static_cast<volatile int*>(w.pk.nstat + slot), cap);
+    for (int a = 0; a < n; ++a)
+    {
+        if (keys[a] == key)
+        {
+            sw[a] += v;
+            return;
+        }
+    }
+    int k = atomicAdd(&w.pk.nstat[slot], 1);
+    if (k < cap)
+    {
+        sw[k] = v;
+        keys[k] = key;
+    }
+    else
+    {
+        spillStat(w, slot, key, v);
+    }
+}
+
+// end of a history: w^0..w^4 of every grouped contribution, or, when the history spilled, its
+// buffered contributions join the spill log for the grouping after the run; the entries are reset
 SKG_D void flushStats(const Wave& w, int slot)
 {
-    int n = min(w.pk.nstat[slot], STATS_CAP);
-    unsigned long long* key = w.pk.skey + static_cast<size_t>(slot) * STATS_CAP;
-    double* sw = w.pk.sw + static_cast<size_t>(slot) * STATS_CAP;
+    const int cap = w.statCap;
+    int taken = w.pk.nstat[slot];
+    int n = min(taken, cap);
+    unsigned long long* key = w.pk.skey + static_cast<size_t>(slot) * cap;
+    double* sw = w.pk.sw + static_cast<size_t>(slot) * cap;
     for (int a = 0; a < n; ++a)
     {
         unsigned long long ka = key[a];
         if (ka == ~0ULL) continue;
-        double wsum = sw[a];
-        for (int b = a + 1; b < n; ++b)
-        {
-            if (key[b] == ka)
-            {
-                wsum += sw[b];
-                key[b] = ~0ULL;
-            }
-        }
-        statMoments(slotScene(w, slot), ka, wsum);
+        if (taken > cap)
+            spillStat(w, slot, ka, sw[a]);
+        else
+            statMoments(slotScene(w, slot), ka, sw[a]);
+        key[a] = ~0ULL;
     }
     w.pk.nstat[slot] = 0;
+}
+
+// moments of the grouped spill-log sums (one record per history and key, computed after the run)
+static __global__ void __launch_bounds__(256) statGroupKernel(const __grid_constant__ Wave w, const StatSpill* groups,
+                                                              unsigned long long n)
+{
+    for (unsigned long long t = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x; t < n;
+         t += static_cast<unsigned long long>(gridDim.x) * blockDim.x)
+    {
+        const StatSpill& g = groups[t];
+        statMoments(w.nScenes > 1 ? w.scenes[g.scene] : w.sc, g.key, g.w);
+    }
 }
 
 // end of a recorded pilot history: the downstream luminosity per unit packet luminosity of every
@@ -444,7 +506,7 @@ static __global__ void __launch_bounds__(256) shadePeelKernel(const __grid_const
 {
     unsigned n = w.ctl->qn[cur][K_PEEL];
     const TaskBuf& b = w.q[cur][K_PEEL];
-    unsigned long long det = 0, ovf = 0;
+    unsigned long long det = 0;
     for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
     {
         int slot = b.slot[t];
@@ -505,23 +567,11 @@ static __global__ void __launch_bounds__(256) shadePeelKernel(const __grid_const
                 unsigned long long key = (static_cast<unsigned long long>(i) << 48)
                                          | (static_cast<unsigned long long>(ell) << 24)
                                          | static_cast<unsigned long long>(l + 1);
-                int k = atomicAdd(&w.pk.nstat[slot], 1);
-                if (k < STATS_CAP)
-                {
-                    w.pk.skey[static_cast<size_t>(slot) * STATS_CAP + k] = key;
-                    w.pk.sw[static_cast<size_t>(slot) * STATS_CAP + k] = Lext;
-                }
-                else
-                {
-                    // buffer full: this contribution forms its own group
-                    statMoments(sc, key, Lext);
-                    ovf++;
-                }
+                recordStat(w, slot, key, Lext);
             }
         }
     }
     if (det) atomicAdd(&w.ctl->counters[3], det);
-    if (ovf) atomicAdd(&w.ctl->counters[5], ovf);
 }
 
 // forced scattering: sample the interaction optical depth (simulateForcedPropagation)
@@ -881,7 +931,11 @@ static __global__ void initPoolKernel(const __grid_constant__ Wave w)
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < w.P; t += gridDim.x * blockDim.x)
     {
         w.pk.freeSlots[t] = t;
-        if (w.anyStats) w.pk.nstat[t] = 0;
+        if (w.anyStats)
+        {
+            w.pk.nstat[t] = 0;
+            for (int a = 0; a < w.statCap; ++a) w.pk.skey[static_cast<size_t>(t) * w.statCap + a] = ~0ULL;
+        }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0)
     {
@@ -896,6 +950,7 @@ static __global__ void initPoolKernel(const __grid_constant__ Wave w)
         c->done = 0;
         c->launchHist0 = 0;
         for (int k = 0; k < 8; ++k) c->counters[k] = 0;
+        c->spillN = 0;
         c->guideWeightSum = 0.;
         c->guideEvents = 0;
         c->err = 0;

@@ -1,5 +1,6 @@
-// Wavefront life cycle with the FP32-distance walkers (production path). Grid kinds without such a
-// walker are reported as unsupported; there is no silent substitution of the FP64 walkers.
+// Wavefront life cycle with the production walkers (FP32 accumulators; the Cartesian and octree
+// walkers keep the reference's FP64 geometry, the Voronoi and tetrahedral ones FP32 face distances
+// with FP64 re-decisions).
 #include "internal.hpp"
 #include "grids_fast.cuh"
 #include "wavefront_driver.cuh"
@@ -12,8 +13,10 @@ cudaError_t runWaveFP32(int gridKind, const Wave& w, int numSMs, cudaStream_t s,
 {
     switch (gridKind)
     {
-        case 0: return runWave<CartesianFast<float>>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer, cache);
-        case 1: return runWave<OctreeLeaf32>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer, cache);
+        case 0: return runWave<CartesianFast>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer, cache);
+        case 1:
+            return w.sc.g.tWallN ? runWave<OctreeRec>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer, cache)
+                                 : runWave<OctreeNodeFast>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer, cache);
         case 2: return runWave<VoronoiRec32>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer, cache);
         case 3: return runWave<TetraPlane32>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer, cache);
         case 4: return runWave<Sphere1DFast>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer, cache);
@@ -23,6 +26,14 @@ cudaError_t runWaveFP32(int gridKind, const Wave& w, int numSMs, cudaStream_t s,
         case 8: return runWave<Cylinder3DFast>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer, cache);
     }
     return cudaErrorNotSupported;
+}
+
+cudaError_t groupStats(const Wave& w, const StatSpill* groups, unsigned long long n, int numSMs, cudaStream_t s)
+{
+    if (n == 0) return cudaSuccess;
+    unsigned blocks = static_cast<unsigned>(std::min<unsigned long long>((n + 255) / 256, 4ull * numSMs));
+    statGroupKernel<<<blocks, 256, 0, s>>>(w, groups, n);
+    return cudaGetLastError();
 }
 
 cudaError_t orderHistories(const Wave& w, unsigned short* keys, unsigned* counts, unsigned* cursor, unsigned* order,

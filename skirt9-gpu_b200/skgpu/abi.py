@@ -97,7 +97,7 @@ class Counters(C.Structure):
         ("rf_stores", C.c_uint64),
         ("stats_overflows", C.c_uint64),
         ("kernel_launches", C.c_uint64),
-        ("reserved", C.c_uint64),
+        ("stats_spilled", C.c_uint64),
     ]
 
 

@@ -12,7 +12,7 @@ import bench  # noqa: E402
 
 def _counters(**kw):
     c = dict(histories=100, crossings=1000, scatterings=50, peel_detections=200, rf_stores=300, stats_overflows=0,
-             kernel_launches=17, reserved=0)
+             kernel_launches=17, stats_spilled=0)
     c.update(kw)
     return c
 

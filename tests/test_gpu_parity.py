@@ -133,7 +133,23 @@ def test_gpu_edge_cases(golden, gpu_backend):
         gpu_backend.upload_grid_cartesian([0, 1], [1, 0], [0, 1])  # descending borders
 
 
-@pytest.mark.parametrize("name", ["cartesian_selftest", "cartesian_c16", "octree", "voronoi", "tetra"])
+@pytest.mark.parametrize("name", ["cartesian_selftest", "cartesian_c16", "octree"])
+def test_gpu_production_paths_equal_reference(golden, gpu_backend, name):
+    """Production Cartesian and octree walkers (the reference's FP64 geometry with the quotient from
+    the reciprocal direction, 64-byte octree leaf records with lattice wall tables): cell sequences
+    and segment lengths equal the reference generators' bit for bit on every golden ray, including
+    the rays through cell corners and along cell walls; optical depths (FP32 accumulation) within
+    1e-5 relative."""
+    z = golden(f"paths_{name}.npz")
+    sc = Scene.from_export(z)
+    sc.upload(gpu_backend)
+    count, m, ds = gpu_backend.trace_paths(z["rays"], 512, precision=abi.PREC_FP32)
+    assert compare_paths(z, count, m, ds) == []
+    tau = gpu_backend.optical_depths(z["rays"], 0.55e-6, precision=abi.PREC_FP32)
+    assert np.allclose(tau, z["ray_tau"], rtol=1e-5, atol=1e-9)
+
+
+@pytest.mark.parametrize("name", ["voronoi", "tetra"])
 def test_gpu_fp32_paths_close_to_reference(golden, gpu_backend, name):
     """FP32-distance walkers: cell sequences equal the reference's except for rays grazing a cell
     edge; segment lengths within 1e-5 of the path length; optical depths within 1e-5."""
@@ -155,6 +171,33 @@ def test_gpu_fp32_paths_close_to_reference(golden, gpu_backend, name):
     ref = z["ray_tau"]
     ok = np.isclose(tau, ref, rtol=1e-5, atol=1e-9)
     assert ok.mean() >= 0.98
+
+
+def test_gpu_statistics_exact_beyond_the_slot_buffer(golden, gpu_backend, oracle_backend):
+    """Per-history statistics (FluxRecorder::recordContributions) of histories with more distinct
+    (instrument, bin, pixel) keys than a packet slot buffers: 16 frames at different inclinations and
+    long histories (albedo 0.95, termination at 1e-8 of the launch weight) spill into the device log,
+    which is grouped exactly after the run. GPU statistics equal the oracle's unbounded grouping."""
+    sc = Scene.from_export(golden("shell_c16.npz"))
+    frame = dict(sc.instruments[0])
+    frame["stats"] = 1
+    sc.instruments = []
+    for inc in np.linspace(5, 175, 16):
+        f = dict(frame)
+        th = np.radians(inc)
+        f["kobs"] = (np.sin(th), 0.0, np.cos(th))
+        f["trig"] = (np.cos(th), np.sin(th), 1.0, 0.0, 1.0, 0.0)
+        f["same_observer"] = 0
+        sc.instruments.append(f)
+    sc.mix = dict(sc.mix, sigma_sca=0.95 * np.asarray(sc.mix["sigma_ext"]))
+    sc.min_weight_reduction = 1e8
+    rg, ro = run_both(sc, gpu_backend, oracle_backend, 1000, seed=23)
+    assert rg.counters["stats_spilled"] > 0 and rg.counters["stats_overflows"] == 0
+    for ig, io in zip(rg.instruments, ro.instruments):
+        for k in range(5):
+            a, b = ig["stats"][k], io["stats"][k]
+            assert np.mean(np.isclose(a, b, rtol=1e-9, atol=0)) > 0.995, k
+            assert a.sum() == pytest.approx(b.sum(), rel=1e-9)
 
 
 def test_gpu_fp32_lifecycle_close_to_fp64(golden, gpu_backend):
