@@ -97,12 +97,19 @@ struct CartesianFast : GenBase
 
 // ---------------------------------------------------------------------------------------------
 // Octree, production (TreeSpatialGrid::MySegmentGenerator::next, TreeSpatialGrid.cpp:143-228,
-// TreeNode::neighbor, TreeNode.cpp:103-112). A crossing reads the current leaf's record for the exit
-// wall's neighbours, then one candidate's record and its six FP64 walls from the lattice tables:
-// the candidate becomes the current cell when it contains the new position (Box::contains, closed),
-// as the reference's first-in-overlap-order rule decides. When no positive-overlap neighbour holds
-// the position the walker runs the reference's complete procedure on the FP64 node arrays: the
-// wall's full neighbour list, the top-down search, the nextafter escape. A start in a known cell (a
+// TreeNode::neighbor, TreeNode.cpp:103-112). The reference takes the first neighbour across the
+// exit wall, in overlap order, whose closed box contains the new position (Box::contains). Here:
+//  - a wall with a single positive-overlap neighbour: that neighbour's face covers the whole wall,
+//    and since entering the current cell (whose closed box held the position) the position has only
+//    moved towards the cell's exit walls; so the neighbour contains it exactly when it lies at or
+//    beyond the crossed wall and not beyond the other two exit walls: comparisons with the FP64
+//    exit walls held in registers (on the crossed axis the neighbour's far wall is at least one
+//    finest cell away, far beyond the eps step);
+//  - a wall with several neighbours, or a position past a corner: each candidate's six FP64 walls
+//    from the FP64 lattice tables, indexed by its record's 16-bit wall indices;
+//  - otherwise the reference's complete procedure on the FP64 node arrays: the wall's full neighbour
+//    list, the top-down search, the nextafter escape.
+// Entering a cell reads its exit walls from the lattice tables. A start in a known cell (a
 // scattering event's interaction cell) skips the top-down search when the top-down search would
 // return that cell (half-open bounds).
 // ---------------------------------------------------------------------------------------------
@@ -138,45 +145,49 @@ struct OctreeRec : GenBase
         return __ldg(g.tWall + axis * g.tWallN + idx);
     }
 
-    // the six FP64 walls of cell c (lo then hi per axis) and its density
-    SKG_D static void walls(const GridDev& g, int c, double& x0, double& x1, double& y0, double& y1, double& z0,
-                            double& z1, float& dens)
+    SKG_D static unsigned lo(int w) { return static_cast<unsigned>(w) & 0xFFFFu; }
+    SKG_D static unsigned hi(int w) { return static_cast<unsigned>(w) >> 16; }
+
+    // the six FP64 walls of the cell with record word w0
+    SKG_D static void walls(const GridDev& g, int4 w0, double& x0, double& x1, double& y0, double& y1, double& z0,
+                            double& z1)
     {
-        int4 w = __ldg(g.tRec + 4 * static_cast<size_t>(c));
-        x0 = wall(g, 0, static_cast<unsigned>(w.x) & 0xFFFFu);
-        x1 = wall(g, 0, static_cast<unsigned>(w.x) >> 16);
-        y0 = wall(g, 1, static_cast<unsigned>(w.y) & 0xFFFFu);
-        y1 = wall(g, 1, static_cast<unsigned>(w.y) >> 16);
-        z0 = wall(g, 2, static_cast<unsigned>(w.z) & 0xFFFFu);
-        z1 = wall(g, 2, static_cast<unsigned>(w.z) >> 16);
-        dens = __int_as_float(w.w);
+        x0 = wall(g, 0, lo(w0.x));
+        x1 = wall(g, 0, hi(w0.x));
+        y0 = wall(g, 1, lo(w0.y));
+        y1 = wall(g, 1, hi(w0.y));
+        z0 = wall(g, 2, lo(w0.z));
+        z1 = wall(g, 2, hi(w0.z));
     }
 
-    SKG_D void become(int c, double x0, double x1, double y0, double y1, double z0, double z1, float dens)
+    SKG_D void become(int c, float dens, double x0, double x1, double y0, double y1, double z0, double z1)
     {
         cell = c;
+        cellDens = dens;
         xE = kx < 0.0 ? x0 : x1;
         yE = ky < 0.0 ? y0 : y1;
         zE = kz < 0.0 ? z0 : z1;
-        cellDens = dens;
     }
 
+    // enters c, whose closed box is known to hold the position
     SKG_D void enter(const GridDev& g, int c)
     {
-        double x0, x1, y0, y1, z0, z1;
-        float d;
-        walls(g, c, x0, x1, y0, y1, z0, z1, d);
-        become(c, x0, x1, y0, y1, z0, z1, d);
+        int4 w0 = __ldg(g.tRec + 4 * static_cast<size_t>(c));
+        cell = c;
+        cellDens = __int_as_float(w0.w);
+        xE = wall(g, 0, kx < 0.0 ? lo(w0.x) : hi(w0.x));
+        yE = wall(g, 1, ky < 0.0 ? lo(w0.y) : hi(w0.y));
+        zE = wall(g, 2, kz < 0.0 ? lo(w0.z) : hi(w0.z));
     }
 
     // Box::contains (closed bounds) of cell c; on success c becomes the current cell
     SKG_D bool tryEnter(const GridDev& g, int c)
     {
+        int4 w0 = __ldg(g.tRec + 4 * static_cast<size_t>(c));
         double x0, x1, y0, y1, z0, z1;
-        float d;
-        walls(g, c, x0, x1, y0, y1, z0, z1, d);
+        walls(g, w0, x0, x1, y0, y1, z0, z1);
         bool in = rx >= x0 && rx <= x1 && ry >= y0 && ry <= y1 && rz >= z0 && rz <= z1;
-        if (in) become(c, x0, x1, y0, y1, z0, z1, d);
+        if (in) become(c, __int_as_float(w0.w), x0, x1, y0, y1, z0, z1);
         return in;
     }
 
@@ -185,12 +196,12 @@ struct OctreeRec : GenBase
     // the domain's upper wall
     SKG_D bool tryHint(const GridDev& g, int c)
     {
+        int4 w0 = __ldg(g.tRec + 4 * static_cast<size_t>(c));
         double x0, x1, y0, y1, z0, z1;
-        float d;
-        walls(g, c, x0, x1, y0, y1, z0, z1, d);
-        bool in = rx >= x0 && (rx < x1 || (rx == x1 && x1 == g.ext[3])) && ry >= y0 && (ry < y1 || (ry == y1 && y1 == g.ext[4]))
-                  && rz >= z0 && (rz < z1 || (rz == z1 && z1 == g.ext[5]));
-        if (in) become(c, x0, x1, y0, y1, z0, z1, d);
+        walls(g, w0, x0, x1, y0, y1, z0, z1);
+        bool in = rx >= x0 && (rx < x1 || (rx == x1 && x1 == g.ext[3])) && ry >= y0
+                  && (ry < y1 || (ry == y1 && y1 == g.ext[4])) && rz >= z0 && (rz < z1 || (rz == z1 && z1 == g.ext[5]));
+        if (in) become(c, __int_as_float(w0.w), x0, x1, y0, y1, z0, z1);
         return in;
     }
 
@@ -221,32 +232,31 @@ struct OctreeRec : GenBase
         double dsx = wallDist(xE, rx, kx, ikx);
         double dsy = wallDist(yE, ry, ky, iky);
         double dsz = wallDist(zE, rz, kz, ikz);
-        double d;
-        int wl;
-        if (dsx <= dsy && dsx <= dsz)
-        {
-            d = dsx;
-            wl = kx < 0.0 ? 0 : 1;
-        }
-        else if (dsy <= dsx && dsy <= dsz)
-        {
-            d = dsy;
-            wl = ky < 0.0 ? 2 : 3;
-        }
-        else
-        {
-            d = dsz;
-            wl = kz < 0.0 ? 4 : 5;
-        }
+        bool ax = dsx <= dsy && dsx <= dsz;
+        bool ay = !ax && dsy <= dsx && dsy <= dsz;
+        int axis = ax ? 0 : (ay ? 1 : 2);
+        double d = ax ? dsx : (ay ? dsy : dsz);
         propagater(xadd(d, g.eps));
         m = cell;
         ds = d;
         segDens = cellDens;
         const int old = cell;
+        // exit wall index: 2 * axis, +1 when the ray moves towards the upper wall
+        const int wl = 2 * axis + ((axis == 0 ? kx : (axis == 1 ? ky : kz)) < 0.0 ? 0 : 1);
         const int* R = reinterpret_cast<const int*>(g.tRec + 4 * static_cast<size_t>(old));
         int one = __ldg(R + 8 + wl);
+        // single neighbour: at or beyond the crossed exit wall, within the other two (branch free)
+        bool bxE = kx < 0.0 ? rx <= xE : rx >= xE, wxE = kx < 0.0 ? rx >= xE : rx <= xE;
+        bool byE = ky < 0.0 ? ry <= yE : ry >= yE, wyE = ky < 0.0 ? ry >= yE : ry <= yE;
+        bool bzE = kz < 0.0 ? rz <= zE : rz >= zE, wzE = kz < 0.0 ? rz >= zE : rz <= zE;
+        bool inOne = ax ? (bxE && wyE && wzE) : (ay ? (byE && wxE && wzE) : (bzE && wxE && wyE));
         bool found = false;
-        if (one >= 0)
+        if (one >= 0 && inOne)
+        {
+            enter(g, one);
+            found = true;
+        }
+        else if (one >= 0)
         {
             found = tryEnter(g, one);
         }
@@ -294,7 +304,6 @@ struct OctreeRec : GenBase
         return true;
     }
 };
-
 
 // Octree, production precision for trees that are not a lattice of depth <= 15 (no leaf records):
 // the FP64 node walker with FP32 accumulators
