@@ -122,20 +122,27 @@ struct OctreeRec : GenBase
     using Acc = float;
     static constexpr int kMinBlocks = SKG_OCTREE_MIN_BLOCKS;
     static constexpr int kRefillMin = 16;  // waiting lanes before a warp takes new tasks
-    double ikx, iky, ikz;                  // reciprocal direction
     double xE, yE, zE;                     // exit walls of the current cell in the direction of travel
-    int cell;
+
+    // the ray's reciprocal direction lives in a per-thread shared-memory slot (blocks of at most
+    // 256 threads), which keeps the walker's state within the registers of four resident blocks
+    SKG_D static double* recip()
+    {
+        __shared__ double slots[3][256];
+        return &slots[0][threadIdx.x];
+    }
+    int cell;                              // the current cell; before the first step the start cell when
+                                           // the caller knows it (an interaction cell), else -1
     float cellDens, segDens;               // density of the current cell / of the segment just returned
-    int hint;                              // the start cell when the caller knows it, else -1
 
     SKG_D void start(const GridDev&, double x, double y, double z, double ux, double uy, double uz, int h = -1)
     {
         startRay(x, y, z, ux, uy, uz);
-        ikx = recipDir(ux);
-        iky = recipDir(uy);
-        ikz = recipDir(uz);
-        cell = -1;
-        hint = h;
+        double* ik = recip();
+        ik[0] = recipDir(ux);
+        ik[256] = recipDir(uy);
+        ik[512] = recipDir(uz);
+        cell = h;
     }
 
     SKG_D double density(const double*) const { return static_cast<double>(segDens); }
@@ -217,7 +224,7 @@ struct OctreeRec : GenBase
         if (state == GS_UNKNOWN)
         {
             if (!moveInside(g.ext, g.eps)) return false;
-            if (!(hint >= 0 && ds == 0. && tryHint(g, hint)))
+            if (!(cell >= 0 && ds == 0. && tryHint(g, cell)))
             {
                 int c = locate(g, rx, ry, rz);
                 if (c < 0)
@@ -229,9 +236,10 @@ struct OctreeRec : GenBase
             }
             if (ds > 0.) return true;
         }
-        double dsx = wallDist(xE, rx, kx, ikx);
-        double dsy = wallDist(yE, ry, ky, iky);
-        double dsz = wallDist(zE, rz, kz, ikz);
+        const double* ik = recip();
+        double dsx = wallDist(xE, rx, kx, ik[0]);
+        double dsy = wallDist(yE, ry, ky, ik[256]);
+        double dsz = wallDist(zE, rz, kz, ik[512]);
         bool ax = dsx <= dsy && dsx <= dsz;
         bool ay = !ax && dsy <= dsx && dsy <= dsz;
         int axis = ax ? 0 : (ay ? 1 : 2);
