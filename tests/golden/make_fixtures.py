@@ -22,6 +22,9 @@ Fixtures written:
                      write only them)
   stats_octree.npz, stats_voronoi.npz, stats_tetra.npz  the disk scene on these grids (scene export)
                      with reference frame/SED statistics (argument `gridstats`)
+  shell_c16_free.npz the raw detector sums (w^0, w^1, w^2 of frame and SED) of a single-threaded
+                     2e5-packet reference run of the 16^3 shell with free (non-forced) propagation
+                     (argument `free`)
   stats_galaxy.npz   the galaxy configuration reduced in size (stellar exponential disk + Sersic
                      bulge with black-body SEDs and wavelength bias 0.5, dust disk on the reference's
                      own octree of max level 6, 20 log wavelengths, three 32^2 frames and an SED with
@@ -165,6 +168,7 @@ def main():
     np.savez_compressed(os.path.join(OUT, "shell_c16.npz"), **data)
     print("shell_c16: stats scale", c)
     explicit_fixture(mjysr_per_w, npp)
+    free_fixture()
 
 
 def sphere1d_fixture(rng=None):
@@ -288,6 +292,37 @@ def grid_stats_fixtures():
         print(f"stats_{name} written")
 
 
+def run_raw(ski_text, probe=1000):
+    """Exports a scene and runs its primary-emission segment in the harness (single-threaded); the
+    export arrays including the raw detector sums inst<i>_wifu / inst<i>_wsed and rf1."""
+    with tempfile.TemporaryDirectory() as tmp:
+        env = dict(os.environ, SKGPU_EXPORT_RUN="1", SKGPU_PROBE_N=str(probe))
+        ski_path = os.path.join(tmp, "scene.ski")
+        with open(ski_path, "w") as f:
+            f.write(ski_text)
+        exp = os.path.join(tmp, "export")
+        os.makedirs(exp)
+        subprocess.run([os.path.join(BIN, "skirt_export"), ski_path, exp], check=True, env=env,
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        data = {}
+        for fn in os.listdir(exp):
+            if fn.endswith(".npy"):
+                data[fn[:-4]] = np.load(os.path.join(exp, fn))
+        with open(os.path.join(exp, "meta.txt")) as f:
+            data["meta"] = np.array(f.read())
+    return data
+
+
+def free_fixture(npp=200000):
+    """The 16^3 shell with free (non-forced) propagation (MonteCarloSimulation::
+    simulateNonForcedPropagation): raw w^0..w^2 sums of the frame and the SED of a single-threaded
+    reference run."""
+    data = run_raw(ski.shell_cartesian(npp, nbins=16, npix=64, force_scattering=False))
+    out = dict(ref_npp=npp, ref_frame_w=data["inst0_wifu"][:3], ref_sed_w=data["inst1_wsed"][:3])
+    np.savez_compressed(os.path.join(OUT, "shell_c16_free.npz"), **out)
+    print("shell_c16_free written")
+
+
 def galaxy_fixture(npp=500000, probe=20000):
     """The galaxy configuration at reduced size on the reference's own octree: the harness exports the
     scene, runs the primary-emission segment single-threaded and dumps the raw FP64 detector arrays
@@ -385,6 +420,8 @@ if __name__ == "__main__":
         grid_stats_fixtures()
     elif sys.argv[1:] == ["galaxy"]:
         galaxy_fixture()
+    elif sys.argv[1:] == ["free"]:
+        free_fixture()
     elif sys.argv[1:] == ["explicit"]:
         z = np.load(os.path.join(OUT, "shell_c16.npz"))
         meta = __import__("skgpu").Scene.read_export(z)[0]

@@ -65,6 +65,26 @@ def test_gpu_free_propagation_matches_oracle(golden, gpu_backend, oracle_backend
     assert_close_runs(rg, ro)
 
 
+def test_gpu_free_propagation_matches_reference(golden, gpu_backend):
+    """Free (non-forced) propagation, both traversal precisions: frame and SED against the
+    reference's own run of the same scene (raw per-history statistics)."""
+    z = golden("shell_c16.npz")
+    f = golden("shell_c16_free.npz")
+    sc = Scene.from_export(z)
+    sc.force_scattering = False
+    sc.upload(gpu_backend)
+    n = int(f["ref_npp"])
+    for precision in (abi.PREC_FP64_EXACT, abi.PREC_FP32):
+        res = sc.run(gpu_backend, n, seed=37, precision=precision)
+        st = res[0]["stats"][:, 0].reshape(5, -1)
+        ref = f["ref_frame_w"]
+        zs = zscores(st[1], st[2], n, ref[1], ref[2], n)
+        assert abs(zs.mean()) < 0.1 and 0.9 < zs.std() < 1.1
+        sst = res[1]["stats"][:, 0]
+        rs = f["ref_sed_w"]
+        assert abs(zscores(sst[1:2], sst[2:3], n, rs[1:2, 0], rs[2:3, 0], n)[0]) < 4
+
+
 @pytest.mark.parametrize("name", ["octree", "voronoi", "tetra", "cartesian_selftest", "sphere1d", "cylinder2d", "sphere2d", "sphere3d", "cylinder3d"])
 def test_gpu_lifecycle_matches_oracle_grids(golden, gpu_backend, oracle_backend, name):
     sc = Scene.from_export(golden(f"paths_{name}.npz"))

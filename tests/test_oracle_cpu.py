@@ -65,14 +65,26 @@ def test_oracle_lifecycle_matches_reference_statistics(golden, oracle_backend):
     assert comp[1] * jy == pytest.approx(ref_jy[2], rel=1e-9)
 
 
-def test_oracle_free_propagation_runs(golden, oracle_backend):
+def test_oracle_free_propagation_matches_reference(golden, oracle_backend):
+    """Free (non-forced) propagation (MonteCarloSimulation::simulateNonForcedPropagation,
+    MediumSystem::setInteractionPointUsingExtinction): the oracle's frame and SED against the
+    reference's own single-threaded run of the same scene (raw per-history statistics)."""
     z = golden("shell_c16.npz")
+    f = golden("shell_c16_free.npz")
     sc = Scene.from_export(z)
     sc.force_scattering = False
     sc.upload(oracle_backend)
-    res = sc.run(oracle_backend, 20000, seed=3)
-    assert res.counters["histories"] == 20000
-    assert res[1]["total"].sum() > 0
+    n = int(f["ref_npp"])
+    res = sc.run(oracle_backend, n, seed=3)
+    assert res.counters["histories"] == n
+    st = res[0]["stats"][:, 0].reshape(5, -1)
+    ref = f["ref_frame_w"]
+    zs = zscores(st[1], st[2], n, ref[1], ref[2], n)
+    assert len(zs) > 2000
+    assert abs(zs.mean()) < 0.1 and 0.9 < zs.std() < 1.1
+    sst = res[1]["stats"][:, 0]
+    rs = f["ref_sed_w"]
+    assert abs(zscores(sst[1:2], sst[2:3], n, rs[1:2, 0], rs[2:3, 0], n)[0]) < 4
 
 
 def header_symbols():
