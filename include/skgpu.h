@@ -143,6 +143,9 @@ int skgpu_create(int device, skgpu_ctx** out);
 void skgpu_destroy(skgpu_ctx* ctx);
 const char* skgpu_last_error(const skgpu_ctx* ctx);
 int skgpu_abi_version(void);
+/* Number of CUDA devices visible to this process (the bridge maps process ranks onto them, as the
+ * reference's GPU layer does with SKIRTGPU_DEVICE / SKIRTGPU_USE_ALL_DEVICES, GpuAcceleration.cpp). */
+int skgpu_device_count(int32_t* count);
 
 /* ---- grids (one per context; a new upload replaces the previous grid) ---- */
 /* CartesianSpatialGrid: border arrays _xv,_yv,_zv (CartesianSpatialGrid.hpp:95-97). */
@@ -235,6 +238,68 @@ int skgpu_run_primary(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t t
  * luminosity times total_packets, position (3) and direction (3), the record the reference's launch
  * writes into a PhotonPacket. Needs the sources and options; used to test the launch distributions. */
 int skgpu_probe_launch(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t total_packets, double* out);
+/* ---- secondary (dust) emission ----
+ * Replaces the secondary-emission segment of MonteCarloSimulation::runSecondaryEmission
+ * (SKIRT/core/MonteCarloSimulation.cpp:211-245) for equilibrium dust emission from a single dust
+ * medium on a Cartesian or octree grid: DustSecondarySource (DustSecondarySource.cpp) with the
+ * AllCellsLibrary, SecondarySourceSystem (SecondarySourceSystem.cpp) with the dust source alone,
+ * EquilibriumDustEmissionCalculator (EquilibriumDustEmissionCalculator.cpp), and the reference's
+ * GPU layer calls on this path (GpuAcceleration::dustAbsorbedLuminosities, divideValues,
+ * compositeLaunchWeights, GpuAcceleration.hpp). */
+
+/* Tables of the equilibrium dust emission of the dust mix, as EquilibriumDustEmissionCalculator::
+ * precalculate builds them (EquilibriumDustEmissionCalculator.cpp:17-90), and the cell volumes:
+ *   num_rf radiation-field bins: rf_sigma_abs (_rfsigmaabsvv[0]), rf_width (_rfdlambdav, also the
+ *     widths of MediumSystem::meanIntensity), rf_cmb (_Bcmbv; zeros without CMB heating) and
+ *     rf_sigma_abs_lum, the mix's DustMix::sectionAbs at each bin's wavelength
+ *     (MediumSystem::dustLuminosity, MediumSystem.cpp:2752-2762);
+ *   num_T temperatures T (_Tv) with the Planck-integrated cross sections planck_abs (_planckabsvv[0]);
+ *   num_em dust-emission wavelengths em_lambda (DisjointWavelengthGrid::extlambdav of the dust-emission
+ *     grid) with em_sigma_abs (_emsigmaabsvv[0]) and the grid's range em_range[2] (wavelengthRange);
+ *   num_cells cell volumes (MediumState::volume). */
+int skgpu_upload_dust_emission(skgpu_ctx* ctx, int32_t num_rf, const double* rf_sigma_abs, const double* rf_width,
+                               const double* rf_cmb, const double* rf_sigma_abs_lum, int32_t num_T, const double* T,
+                               const double* planck_abs, int32_t num_em, const double* em_lambda,
+                               const double* em_sigma_abs, const double* em_range, int32_t num_cells,
+                               const double* cell_volume);
+/* Replaces the device radiation field (the tally of skgpu_run_primary) by rf, cells x bins in the
+ * layout of skgpu_fetch_radiation_field (MediumSystem::_rf1, e.g. after the segment-end sum over
+ * processes of MediumSystem::communicateRadiationField). */
+int skgpu_upload_radiation_field(skgpu_ctx* ctx, const double* rf);
+
+/* Options of the secondary launch (SecondaryEmissionOptions, DustEmissionOptions). */
+typedef struct skgpu_secondary_options {
+    double spatial_bias;     /* SecondaryEmissionOptions::spatialBias (uniform fraction over emitting cells) */
+    double source_bias;      /* SecondaryEmissionOptions::sourceBias */
+    double wavelength_bias;  /* DustEmissionOptions::wavelengthBias */
+    double bias_lambda_min;  /* its LogWavelengthDistribution range */
+    double bias_lambda_max;
+} skgpu_secondary_options;
+
+/* Philox key offset of the secondary segment: its histories draw from key seed ^ this value, streams
+ * independent of the primary segment's for the same history indices. */
+#define SKGPU_SECONDARY_KEY 0x5EC0DA4EB1A5C0DEULL
+
+/* Prepares the secondary-emission segment of total_packets packets from the device radiation field:
+ * on the device, per cell the absorbed dust luminosity (MediumSystem::dustLuminosity), the
+ * equilibrium temperature (EquilibriumDustEmissionCalculator::equilibriumTemperature) and the
+ * normalised emission spectrum (emissivity, NR::cdf<NR::interpolateLogLog>); on the host, the launch
+ * weights and history ranges per cell (DustSecondarySource::prepareLuminosities / preparePacketMap,
+ * SecondarySourceSystem::prepareForLaunch). *luminosity receives the total dust luminosity; when it
+ * is 0 there is nothing to launch and skgpu_run_secondary refuses to run. Grids: Cartesian, octree. */
+int skgpu_prepare_secondary(skgpu_ctx* ctx, const skgpu_secondary_options* options, uint64_t total_packets,
+                            double* luminosity);
+/* Results of the last preparation: per cell the dust luminosity and temperature; *num_points the
+ * points of the emission-spectrum axis, lambda that axis, pdf / cdf the normalised spectra (cells x
+ * num_points). Null outputs are skipped. */
+int skgpu_fetch_dust_emission(skgpu_ctx* ctx, double* luminosity, double* temperature, int32_t* num_points,
+                              double* lambda, double* pdf, double* cdf);
+/* Runs the life cycle of histories [first, first+count) of the prepared secondary segment
+ * (MonteCarloSimulation::performLifeCycle with primary = false: the dust source's launch, emission
+ * peel-off, forced or free propagation, scattering peel-off and scattering; no radiation-field
+ * storage), adding into the instrument tallies. */
+int skgpu_run_secondary(skgpu_ctx* ctx, uint64_t first, uint64_t count);
+
 /* Same life cycle as skgpu_run_primary for callers that must not allocate device memory while it
  * runs: for example a host code that hands the GPU to this library between phases of its own
  * memory manager, or that cannot afford the implicit device synchronisation of cudaMalloc/cudaFree

@@ -62,6 +62,8 @@
 #include "Configuration.hpp"
 #include "DisjointWavelengthGrid.hpp"
 #include "DustMix.hpp"
+#include "EquilibriumDustEmissionCalculator.hpp"
+#include "SecondarySourceSystem.hpp"
 #include "FatalError.hpp"
 #include "FilePaths.hpp"
 #include "FluxRecorder.hpp"
@@ -510,7 +512,7 @@ namespace
     // calibration): inst<i>_ifu.npy / inst<i>_sed.npy (total, raw W per pixel and bin, index
     // l + ell * npix) and inst<i>_wifu.npy / inst<i>_wsed.npy (sum w^k, k = 0..4, per pixel and bin,
     // FluxRecorder::recordContributions), in FP64 as FluxRecorder holds them
-    void exportDetectors(MonteCarloSimulation* sim, const std::string& out)
+    void exportDetectors(MonteCarloSimulation* sim, const std::string& out, const std::string& suffix = "")
     {
         int i = 0;
         for (Instrument* instr : sim->instrumentSystem()->instruments())
@@ -528,11 +530,22 @@ namespace
                 for (const Array& a : arrays) all.insert(all.end(), begin(a), end(a));
                 writeNpy(key + name, all.data(), {arrays.size(), arrays[0].size()});
             };
-            if (rec->_ifu.size()) dumpSet(rec->_ifu, "_ifu.npy", false);
-            if (rec->_sed.size()) dumpSet(rec->_sed, "_sed.npy", false);
-            dumpSet(rec->_wifu, "_wifu.npy", true);
-            dumpSet(rec->_wsed, "_wsed.npy", true);
+            if (rec->_ifu.size()) dumpSet(rec->_ifu, "_ifu" + suffix + ".npy", false);
+            if (rec->_sed.size()) dumpSet(rec->_sed, "_sed" + suffix + ".npy", false);
+            dumpSet(rec->_wifu, "_wifu" + suffix + ".npy", true);
+            dumpSet(rec->_wsed, "_wsed" + suffix + ".npy", true);
             ++i;
+        }
+    }
+
+    // zeroes every detector sum of every instrument (FluxRecorder totals, components and statistics)
+    void clearDetectors(MonteCarloSimulation* sim)
+    {
+        for (Instrument* instr : sim->instrumentSystem()->instruments())
+        {
+            auto rec = instr->instrumentFluxRecorder();
+            for (auto* set : {&rec->_sed, &rec->_ifu, &rec->_wsed, &rec->_wifu})
+                for (Array& a : *set) a = 0.;
         }
     }
 
@@ -543,6 +556,70 @@ namespace
         Table<2>& rf = ms->_rf1;
         if (rf.size() == 0) return;
         writeNpy(out + "/rf1.npy", &rf.data()[0], {rf.size(0), rf.size(1)});
+    }
+
+    // Equilibrium dust emission (DustEmission mode, after a primary segment): the tables that
+    // EquilibriumDustEmissionCalculator::precalculate (EquilibriumDustEmissionCalculator.cpp:17-90)
+    // built for the single dust mix, the mix's absorption cross section at each radiation-field
+    // wavelength (MediumSystem::dustLuminosity, MediumSystem.cpp:2752-2762), the cell volumes, the
+    // reference's own per-cell absorbed luminosity and equilibrium temperature
+    // (MediumSystem::indicativeDustTemperature) for the radiation field of the run, the emission
+    // spectrum MediumSystem::dustEmissionSpectrum of every 97th emitting cell, and the secondary
+    // launch configuration
+    void exportDustEmission(MonteCarloSimulation* sim, const std::string& out, Meta& meta)
+    {
+        auto ms = sim->mediumSystem();
+        auto config = sim->config();
+        auto mix = dynamic_cast<const DustMix*>(ms->mix(0, 0));
+        if (!mix || ms->_numMedia != 1) throw std::runtime_error("dust emission export: one dust medium expected");
+        const EquilibriumDustEmissionCalculator& c = mix->_calc;
+        writeVec(out + "/de_rf_lambda.npy", std::vector<double>(begin(c._rflambdav), end(c._rflambdav)));
+        writeVec(out + "/de_rf_width.npy", std::vector<double>(begin(c._rfdlambdav), end(c._rfdlambdav)));
+        writeVec(out + "/de_rf_cmb.npy", std::vector<double>(begin(c._Bcmbv), end(c._Bcmbv)));
+        writeVec(out + "/de_rf_sigma_abs.npy", std::vector<double>(begin(c._rfsigmaabsvv[0]), end(c._rfsigmaabsvv[0])));
+        writeVec(out + "/de_T.npy", std::vector<double>(begin(c._Tv), end(c._Tv)));
+        writeVec(out + "/de_planck_abs.npy", std::vector<double>(begin(c._planckabsvv[0]), end(c._planckabsvv[0])));
+        writeVec(out + "/de_em_lambda.npy", std::vector<double>(begin(c._emlambdav), end(c._emlambdav)));
+        writeVec(out + "/de_em_sigma_abs.npy", std::vector<double>(begin(c._emsigmaabsvv[0]), end(c._emsigmaabsvv[0])));
+        Range er = config->dustEmissionWLG()->wavelengthRange();
+        writeVec(out + "/de_em_range.npy", std::vector<double>{er.min(), er.max()});
+        auto rfw = config->radiationFieldWLG();
+        int nrf = rfw->numBins();
+        std::vector<double> sal(nrf);
+        for (int ell = 0; ell != nrf; ++ell) sal[ell] = mix->sectionAbs(rfw->wavelength(ell));
+        writeVec(out + "/de_rf_sigma_abs_lum.npy", sal);
+        int numCells = ms->_state._numCells;
+        std::vector<double> vol(numCells), L(numCells), T(numCells);
+        std::vector<int32_t> cells;
+        std::vector<double> spec;
+        for (int m = 0; m != numCells; ++m)
+        {
+            vol[m] = ms->_state.volume(m);
+            L[m] = ms->dustLuminosity(m);
+            T[m] = ms->indicativeDustTemperature(m);
+            if (L[m] > 0 && m % 97 == 0)
+            {
+                Array ev = ms->dustEmissionSpectrum(m);
+                cells.push_back(m);
+                spec.insert(spec.end(), begin(ev), end(ev));
+            }
+        }
+        writeVec(out + "/cell_volume.npy", vol);
+        writeVec(out + "/ref_dust_L.npy", L);
+        writeVec(out + "/ref_dust_T.npy", T);
+        writeVec(out + "/ref_dust_spec_cells.npy", cells);
+        if (!cells.empty())
+            writeNpy(out + "/ref_dust_spec.npy", spec.data(), {cells.size(), spec.size() / cells.size()});
+        meta.kv("secondary_spatial_bias", config->secondarySpatialBias());
+        meta.kv("secondary_source_bias", config->secondarySourceBias());
+        meta.kv("num_secondary_packets", static_cast<double>(config->numSecondaryPackets()));
+        meta.kv("dust_emission_wavelength_bias", config->dustEmissionWavelengthBias());
+        auto bd = dynamic_cast<const RangeWavelengthDistribution*>(config->dustEmissionWavelengthBiasDistribution());
+        if (bd)
+        {
+            meta.kv("dust_emission_bias_min", bd->range().min());
+            meta.kv("dust_emission_bias_max", bd->range().max());
+        }
     }
 
     void dumpRays(MonteCarloSimulation* sim, const std::string& raysPath, int maxSeg, double lambda,
@@ -639,6 +716,18 @@ int main(int argc, char** argv)
         exportSources(sim, out, meta);
         if (run) exportDetectors(sim, out);
         if (run && sim->config()->hasMedium()) exportRadiationField(sim, out);
+        // DustEmission mode: the dust emission tables and reference per-cell values for the primary
+        // radiation field of the run, then the secondary-emission segment
+        // (MonteCarloSimulation::runSecondaryEmission, single-threaded, continuing the random
+        // stream) into cleared detectors, whose sums are the secondary segment's alone
+        // (inst<i>_*_sec.npy)
+        if (run && sim->config()->hasDustEmission())
+        {
+            exportDustEmission(sim, out, meta);
+            clearDetectors(sim);
+            sim->runSecondaryEmission();
+            exportDetectors(sim, out, "_sec");
+        }
         probeLaunch(sim, out, probeN, probeN);
         if (argc >= 4)
         {

@@ -162,6 +162,17 @@ struct or_ctx
     skgpu_options opt;
     skgpu_counters cnt;
     int errFlag;
+    /* secondary (dust) emission: tables, per-cell results, launch tables */
+    int deNrf, deNT, deNem, deCells;
+    double *deRfSig, *deRfW, *deRfCmb, *deRfSigL, *deT, *dePlanck, *deEmL, *deEmSig, *deVol;
+    double deEmRange[2];
+    int secCells, secNpts;
+    double *secL, *secT, *secXv, *secPv, *secCv, *secLv, *secWv;
+    uint64_t* secIv;
+    int* secCellNode; /* octree: leaf node of each cell */
+    uint64_t secPackets;
+    double secLpk, secXi, secBmin, secBmax, secLogMin, secLogWidth;
+    int secRun; /* set while or_run_secondary runs */
 };
 
 static int fail(or_ctx* c, int code, const char* msg)
@@ -225,6 +236,10 @@ void or_destroy(or_ctx* c)
     free(c->dens); free(c->mixLb); free(c->mixExt); free(c->mixSca); free(c->mixG);
     free(c->rfB); free(c->rfEll); free(c->rf);
     free(c->src); free(c->tabL); free(c->tabA); free(c->tabB); free(c->radR); free(c->radP);
+    free(c->deRfSig); free(c->deRfW); free(c->deRfCmb); free(c->deRfSigL); free(c->deT); free(c->dePlanck);
+    free(c->deEmL); free(c->deEmSig); free(c->deVol);
+    free(c->secL); free(c->secT); free(c->secXv); free(c->secPv); free(c->secCv); free(c->secLv); free(c->secWv);
+    free(c->secIv); free(c->secCellNode);
     free(c);
 }
 
@@ -1986,8 +2001,15 @@ static void path_build(or_ctx* c, const Packet* pk, Path* path)
     }
 }
 
+static void launch_secondary(or_ctx* c, Rng* r, uint64_t hist, Packet* pk);
+
 static void launch(or_ctx* c, Rng* r, uint64_t hist, Packet* pk)
 {
+    if (c->secRun)
+    {
+        launch_secondary(c, r, hist, pk);
+        return;
+    }
     int h = 0;
     for (int q = 1; q < c->nsrc; ++q)
         if (c->src[q].first_history <= hist) h = q;
@@ -2157,7 +2179,7 @@ static void life_cycle(or_ctx* c, uint64_t hist, Path* path, Packet* pk)
         {
             path_build(c, pk, path);
             /* storeRadiationField */
-            if (c->opt.store_radiation_field && pk->ellRF >= 0)
+            if (c->opt.store_radiation_field && !c->secRun && pk->ellRF >= 0)
             {
                 double lnExtBeg = 0., extBeg = 1.;
                 for (int q = 0; q < path->n; ++q)
@@ -2283,6 +2305,374 @@ static void life_cycle(or_ctx* c, uint64_t hist, Path* path, Packet* pk)
         }
     }
     if (pk->ncontrib) record_contributions(c, pk);
+}
+
+/* ------------------------------------------------------------------------------------------------
+ * secondary (dust) emission
+ * ------------------------------------------------------------------------------------------------ */
+
+static double* dupd(const double* p, size_t n) { return (double*)dup(p, n * sizeof(double)); }
+
+int or_upload_dust_emission(or_ctx* c, int32_t num_rf, const double* rf_sigma_abs, const double* rf_width,
+                            const double* rf_cmb, const double* rf_sigma_abs_lum, int32_t num_T, const double* T,
+                            const double* planck_abs, int32_t num_em, const double* em_lambda,
+                            const double* em_sigma_abs, const double* em_range, int32_t num_cells,
+                            const double* cell_volume)
+{
+    if (num_rf < 1 || num_T < 2 || num_em < 2 || num_cells < 1) return fail(c, SKGPU_ERR_ARG, "dust emission: missing tables");
+    free(c->deRfSig); free(c->deRfW); free(c->deRfCmb); free(c->deRfSigL); free(c->deT); free(c->dePlanck);
+    free(c->deEmL); free(c->deEmSig); free(c->deVol);
+    c->deRfSig = dupd(rf_sigma_abs, num_rf);
+    c->deRfW = dupd(rf_width, num_rf);
+    c->deRfCmb = dupd(rf_cmb, num_rf);
+    c->deRfSigL = dupd(rf_sigma_abs_lum, num_rf);
+    c->deT = dupd(T, num_T);
+    c->dePlanck = dupd(planck_abs, num_T);
+    c->deEmL = dupd(em_lambda, num_em);
+    c->deEmSig = dupd(em_sigma_abs, num_em);
+    c->deVol = dupd(cell_volume, num_cells);
+    c->deEmRange[0] = em_range[0];
+    c->deEmRange[1] = em_range[1];
+    c->deNrf = num_rf; c->deNT = num_T; c->deNem = num_em; c->deCells = num_cells;
+    c->secPackets = 0;
+    return SKGPU_OK;
+}
+
+int or_upload_radiation_field(or_ctx* c, const double* rf)
+{
+    if (!c->nrf || !c->numCells) return fail(c, SKGPU_ERR_STATE, "radiation field: no medium or RF grid uploaded");
+    size_t len = (size_t)c->numCells * c->nrf;
+    if (c->rfLen != len)
+    {
+        free(c->rf);
+        c->rf = (double*)calloc(len, sizeof(double));
+        c->rfLen = len;
+    }
+    memcpy(c->rf, rf, len * sizeof(double));
+    return SKGPU_OK;
+}
+
+/* NR::interpolateLogLog (SKIRT/utils/NR.hpp:349-358) */
+static double interp_loglog(double x, double x1, double x2, double f1, double f2)
+{
+    if (f1 <= 0 || f2 <= 0)
+    {
+        if (x == x1) return f1;
+        if (x == x2) return f2;
+        return 0;
+    }
+    return f1 * exp(log(x / x1) / log(x2 / x1) * (log(f2 / f1)));
+}
+
+/* SpecialFunctions::gln (SKIRT/utils/SpecialFunctions.cpp:798-811) */
+static double gln(double p, double x)
+{
+    const double q = 1.0 - p;
+    if (q == 0.0) return log(x);
+    if (fabs(q) < 1e-3)
+    {
+        double lnx = log(x);
+        double s = q * lnx;
+        return lnx * (1.0 + 0.5 * s + 1.0 / 6.0 * s * s + 1.0 / 24.0 * s * s * s);
+    }
+    return (pow(x, q) - 1.0) / q;
+}
+
+/* PlanckFunction (SKIRT/utils/PlanckFunction.cpp:12-27) with the constants of SKIRT/utils/Constants.hpp */
+static double planck_value(double T, double lambda)
+{
+    const double h = 6.62606957e-34, cc = 2.99792458e8, k = 1.3806488e-23;
+    double f1 = h * cc / (k * T);
+    double f2 = 2.0 * h * cc * cc;
+    return f2 / pow(lambda, 5) / (exp(f1 / lambda) - 1.0);
+}
+
+/* std::upper_bound / std::lower_bound indices */
+static int ub_index(const double* v, int n, double x)
+{
+    int lo = 0, hi = n;
+    while (lo < hi)
+    {
+        int mid = (lo + hi) / 2;
+        if (x < v[mid]) hi = mid; else lo = mid + 1;
+    }
+    return lo;
+}
+static int lb_index(const double* v, int n, double x)
+{
+    int lo = 0, hi = n;
+    while (lo < hi)
+    {
+        int mid = (lo + hi) / 2;
+        if (v[mid] < x) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+int or_prepare_secondary(or_ctx* c, const skgpu_secondary_options* opt, uint64_t total_packets, double* luminosity)
+{
+    if (!opt || total_packets == 0) return fail(c, SKGPU_ERR_ARG, "secondary: missing options or packets");
+    if (!c->hasGrid || (c->g.kind != SKGPU_GRID_CARTESIAN && c->g.kind != SKGPU_GRID_OCTREE))
+        return fail(c, SKGPU_ERR_UNSUPPORTED, "secondary: dust emission needs a Cartesian or octree grid");
+    if (!c->deNrf || c->deCells != c->numCells || c->deNrf != c->nrf)
+        return fail(c, SKGPU_ERR_STATE, "secondary: dust emission tables do not match the medium and RF grid");
+    if (!c->rf || c->rfLen != (size_t)c->numCells * c->nrf) return fail(c, SKGPU_ERR_STATE, "secondary: no radiation field");
+    const int cells = c->numCells, nrf = c->nrf;
+    /* the spectrum axis of NR::cdf (NR.hpp:494-520) */
+    int minRight = ub_index(c->deEmL, c->deNem, c->deEmRange[0]);
+    int maxRight = lb_index(c->deEmL, c->deNem, c->deEmRange[1]);
+    int nb = 1 + maxRight - minRight, npts = nb + 1;
+    free(c->secL); free(c->secT); free(c->secXv); free(c->secPv); free(c->secCv); free(c->secLv); free(c->secWv);
+    free(c->secIv);
+    c->secL = (double*)calloc(cells, sizeof(double));
+    c->secT = (double*)calloc(cells, sizeof(double));
+    c->secXv = (double*)calloc(npts, sizeof(double));
+    c->secPv = (double*)calloc((size_t)cells * npts, sizeof(double));
+    c->secCv = (double*)calloc((size_t)cells * npts, sizeof(double));
+    c->secLv = (double*)calloc(cells, sizeof(double));
+    c->secWv = (double*)calloc(cells, sizeof(double));
+    c->secIv = (uint64_t*)calloc((size_t)cells + 1, sizeof(uint64_t));
+    c->secCells = cells;
+    c->secNpts = npts;
+    c->secPackets = 0;
+    free(c->secCellNode);
+    c->secCellNode = NULL;
+    if (c->g.kind == SKGPU_GRID_OCTREE)
+    {
+        c->secCellNode = (int*)calloc(cells, sizeof(int));
+        for (int q = 0; q < c->g.tnodes; ++q)
+            if (c->g.tcell[q] >= 0 && c->g.tcell[q] < cells) c->secCellNode[c->g.tcell[q]] = q;
+    }
+    double* xv = c->secXv;
+    xv[0] = c->deEmRange[0];
+    for (int j = minRight, i = 1; j < maxRight; ++j, ++i) xv[i] = c->deEmL[j];
+    xv[nb] = c->deEmRange[1];
+    double* ev = (double*)malloc(c->deNem * sizeof(double));
+    for (int m = 0; m < cells; ++m)
+    {
+        double n = c->dens[m];
+        /* MediumSystem::dustLuminosity (MediumSystem.cpp:2752-2762) with DustMix::opacityAbs */
+        double Labs = 0.;
+        for (int ell = 0; ell < nrf; ++ell)
+        {
+            double op = n > 0. ? n * c->deRfSigL[ell] : 0.;
+            Labs += op * c->rf[(size_t)m * nrf + ell];
+        }
+        c->secL[m] = Labs;
+        /* MediumSystem::meanIntensity (MediumSystem.cpp:2670-2680) and
+           EquilibriumDustEmissionCalculator::equilibriumTemperature (EquilibriumDustEmissionCalculator.cpp:
+           118-128): the valarray expression's sum() runs from the last element to the first */
+        double factor = 1. / (4. * M_PI * c->deVol[m]);
+        double inputabs = 0.;
+        for (int k = nrf - 1; k >= 0; --k)
+        {
+            double J = c->rf[(size_t)m * nrf + k] * factor / c->deRfW[k];
+            double term = c->deRfSig[k] * (J + c->deRfCmb[k]) * c->deRfW[k];
+            inputabs = (k == nrf - 1) ? term : inputabs + term;
+        }
+        double T = 0.;
+        if (inputabs > 0.)
+        {
+            int i = locate_nr(c->dePlanck, c->deNT, inputabs);
+            if (i < 0) T = c->deT[0];
+            else if (i >= c->deNT - 1) T = c->deT[c->deNT - 1];
+            else
+            {
+                double x1 = c->dePlanck[i], x2 = c->dePlanck[i + 1], f1 = c->deT[i], f2 = c->deT[i + 1];
+                T = f1 + ((inputabs - x1) / (x2 - x1)) * (f2 - f1);
+            }
+        }
+        /* the reported temperature is MediumSystem::indicativeDustTemperature's: 0 without dust */
+        c->secT[m] = n > 0. ? T : 0.;
+        /* emissivity (EquilibriumDustEmissionCalculator.cpp:132-148) times the number density
+           (DustMix::emissionSpectrum), then NR::cdf<NR::interpolateLogLog> and NR::cdf2 (NR.cpp:25-53) */
+        for (int j = 0; j < c->deNem; ++j) ev[j] = n * (c->deEmSig[j] * planck_value(T, c->deEmL[j]));
+        double* p = c->secPv + (size_t)m * npts;
+        double* P = c->secCv + (size_t)m * npts;
+        p[0] = minRight == 0 ? 0. : interp_loglog(xv[0], c->deEmL[minRight - 1], c->deEmL[minRight], ev[minRight - 1], ev[minRight]);
+        for (int i = 1; i < nb; ++i) p[i] = ev[minRight + i - 1];
+        p[nb] = maxRight == c->deNem ? 0. : interp_loglog(xv[nb], c->deEmL[maxRight - 1], c->deEmL[maxRight], ev[maxRight - 1], ev[maxRight]);
+        P[0] = 0.;
+        for (int i = 0; i < nb; ++i)
+        {
+            double area = 0.;
+            if (p[i] > 0 && p[i + 1] > 0)
+            {
+                double alpha = log(p[i + 1] / p[i]) / log(xv[i + 1] / xv[i]);
+                area = p[i] * xv[i] * gln(-alpha, xv[i + 1] / xv[i]);
+            }
+            P[i + 1] = P[i] + area;
+        }
+        double norm = P[nb];
+        if (norm > 0.)
+            for (int i = 0; i <= nb; ++i)
+            {
+                p[i] /= norm;
+                P[i] /= norm;
+            }
+    }
+    free(ev);
+    /* DustSecondarySource::prepareLuminosities / preparePacketMap (DustSecondarySource.cpp:27-152) with
+       the AllCellsLibrary, SecondarySourceSystem::prepareForLaunch (SecondarySourceSystem.cpp:62-104)
+       with the dust source alone */
+    double L = c->secL[0];
+    for (int m = 1; m < cells; ++m) L += c->secL[m];
+    if (luminosity) *luminosity = L;
+    if (!(L > 0.)) return SKGPU_OK;
+    for (int m = 0; m < cells; ++m) c->secLv[m] = c->secL[m] / L;
+    double xi = opt->spatial_bias;
+    double* wv = (double*)malloc(cells * sizeof(double));
+    for (int m = 0; m < cells; ++m) wv[m] = c->secLv[m] > 0 ? 1. : 0.;
+    double ws = wv[0];
+    for (int m = 1; m < cells; ++m) ws += wv[m];
+    for (int m = 0; m < cells; ++m) wv[m] /= ws;
+    for (int m = 0; m < cells; ++m) c->secWv[m] = (1 - xi) * c->secLv[m] + xi * wv[m];
+    free(wv);
+    uint64_t N = total_packets;
+    c->secIv[0] = 0;
+    double W = 0.;
+    for (int p = 1; p != cells; ++p)
+    {
+        W += c->secWv[p - 1];
+        uint64_t r = (uint64_t)round(W * (double)N);
+        c->secIv[p] = r < N ? r : N;
+    }
+    c->secIv[cells] = N;
+    double xs = opt->source_bias;
+    double Ws = (1 - xs) * 1. / 1. + xs * 1. / 1.;
+    c->secLpk = (L / (double)N) * (1. / Ws);
+    c->secXi = opt->wavelength_bias;
+    c->secBmin = opt->bias_lambda_min;
+    c->secBmax = opt->bias_lambda_max;
+    c->secLogMin = opt->wavelength_bias > 0. ? log(c->secBmin) : 0.;
+    c->secLogWidth = opt->wavelength_bias > 0. ? log(c->secBmax) - log(c->secBmin) : 0.;
+    c->secPackets = N;
+    return SKGPU_OK;
+}
+
+int or_fetch_dust_emission(or_ctx* c, double* luminosity, double* temperature, int32_t* num_points, double* lambda,
+                           double* pdf, double* cdf)
+{
+    if (!c->secCells || c->secCells != c->numCells) return fail(c, SKGPU_ERR_STATE, "fetch: no prepared dust emission");
+    size_t cells = c->secCells, rows = cells * c->secNpts;
+    if (num_points) *num_points = c->secNpts;
+    if (luminosity) memcpy(luminosity, c->secL, cells * sizeof(double));
+    if (temperature) memcpy(temperature, c->secT, cells * sizeof(double));
+    if (lambda) memcpy(lambda, c->secXv, c->secNpts * sizeof(double));
+    if (pdf) memcpy(pdf, c->secPv, rows * sizeof(double));
+    if (cdf) memcpy(cdf, c->secCv, rows * sizeof(double));
+    return SKGPU_OK;
+}
+
+/* SecondarySourceSystem::launch -> DustSecondarySource::launch / launchFromCell
+   (SecondarySourceSystem.cpp:118-133, DustSecondarySource.cpp:521-626; Random::cdfLogLog, Random.cpp:199-205;
+   Random::position, Random.cpp:168-176; Box::fracPos, Box.hpp:142-145) */
+static void launch_secondary(or_ctx* c, Rng* r, uint64_t hist, Packet* pk)
+{
+    rng_start(r, c->opt.seed ^ SKGPU_SECONDARY_KEY, hist);
+    pk->nscatt = 0;
+    int cells = c->secCells;
+    int m = 0;
+    {
+        int lo = 0, hi = cells + 1;
+        while (lo < hi)
+        {
+            int mid = (lo + hi) / 2;
+            if (hist < c->secIv[mid]) hi = mid; else lo = mid + 1;
+        }
+        m = lo - 1;
+        if (m < 0) m = 0;
+        if (m > cells - 1) m = cells - 1;
+    }
+    double ws = c->secLv[m] / c->secWv[m];
+    const int n = c->secNpts;
+    const double* xv = c->secXv;
+    const double* pv = c->secPv + (size_t)m * n;
+    const double* Pv = c->secCv + (size_t)m * n;
+    double lambda, w;
+    int fromSpectrum = 1;
+    if (c->secXi)
+        fromSpectrum = uniform(r) > c->secXi;
+    if (fromSpectrum)
+    {
+        double X = uniform(r);
+        int i = locate_clip(Pv, n, X);
+        double alpha = log(pv[i + 1] / pv[i]) / log(xv[i + 1] / xv[i]);
+        lambda = xv[i] * gexp(-alpha, (X - Pv[i]) / (pv[i] * xv[i]));
+    }
+    else
+        lambda = exp(c->secLogMin + c->secLogWidth * uniform(r));
+    if (!c->secXi)
+        w = 1.;
+    else
+    {
+        /* NR::value<NR::interpolateLogLog> (NR.hpp:371-377) with NR::locateFail */
+        double s = 0.;
+        if (!(lambda > xv[n - 1]))
+        {
+            int jl = -1, ju = n - 1;
+            while (ju - jl > 1)
+            {
+                int jm = (ju + jl) >> 1;
+                if (lambda < xv[jm]) ju = jm; else jl = jm;
+            }
+            if (jl >= 0) s = interp_loglog(lambda, xv[jl], xv[jl + 1], pv[jl], pv[jl + 1]);
+        }
+        if (!s)
+            w = 0.;
+        else
+        {
+            double b = (lambda >= c->secBmin * (1 - 1e-14) && lambda <= c->secBmax * (1 + 1e-14)) ? 1. / (c->secLogWidth * lambda) : 0.;
+            w = s / ((1 - c->secXi) * s + c->secXi * b);
+        }
+    }
+    double b0, b1, b2, b3, b4, b5;
+    if (c->g.kind == SKGPU_GRID_CARTESIAN)
+    {
+        int i = m / (c->g.nz * c->g.ny), j = (m / c->g.nz) % c->g.ny, k = m % c->g.nz;
+        b0 = c->g.xb[i]; b1 = c->g.yb[j]; b2 = c->g.zb[k];
+        b3 = c->g.xb[i + 1]; b4 = c->g.yb[j + 1]; b5 = c->g.zb[k + 1];
+    }
+    else
+    {
+        const double* bb = c->g.tb + 6 * (size_t)c->secCellNode[m];
+        b0 = bb[0]; b1 = bb[1]; b2 = bb[2]; b3 = bb[3]; b4 = bb[4]; b5 = bb[5];
+    }
+    double fx = uniform(r);
+    double fy = uniform(r);
+    double fz = uniform(r);
+    pk->rx = b0 + fx * (b3 - b0);
+    pk->ry = b1 + fy * (b4 - b1);
+    pk->rz = b2 + fz * (b5 - b2);
+    iso_direction(r, &pk->kx, &pk->ky, &pk->kz);
+    pk->lambda = lambda;
+    pk->L = c->secLpk * ws * w;
+    pk->ellMix = locate_clip(c->mixLb, c->nmix, lambda);
+    if (pk->ellMix < 0) pk->ellMix = 0;
+    pk->sext = c->mixExt[pk->ellMix];
+    pk->ssca = c->mixSca[pk->ellMix];
+    pk->g = c->mixG[pk->ellMix];
+    pk->ellRF = -1;
+}
+
+int or_run_secondary(or_ctx* c, uint64_t first, uint64_t count)
+{
+    if (!c->secPackets || c->secCells != c->numCells)
+        return fail(c, SKGPU_ERR_STATE, "secondary: no prepared segment (or_prepare_secondary)");
+    if (!c->nmix) return fail(c, SKGPU_ERR_STATE, "secondary: no dust mix uploaded");
+    if (first + count > c->secPackets) return fail(c, SKGPU_ERR_ARG, "secondary: history range outside the segment");
+    memset(&c->cnt, 0, sizeof c->cnt);
+    c->errFlag = 0;
+    c->secRun = 1;
+    Path path = {NULL, 0, 0};
+    Packet pk;
+    memset(&pk, 0, sizeof pk);
+    for (uint64_t h = first; h < first + count; ++h) life_cycle(c, h, &path, &pk);
+    free(path.v);
+    free(pk.contrib);
+    c->secRun = 0;
+    if (c->errFlag) return fail(c, SKGPU_ERR_DEVICE, "run: interaction point outside the grid");
+    return SKGPU_OK;
 }
 
 int or_probe_launch(or_ctx* c, uint64_t first, uint64_t count, uint64_t total_packets, double* out)

@@ -62,6 +62,17 @@ int or_upload_instruments(or_ctx* ctx, int32_t num_instruments, const skgpu_inst
 int or_set_options(or_ctx* ctx, const skgpu_options* options);
 int or_run_primary(or_ctx* ctx, uint64_t first, uint64_t count, uint64_t total_packets);
 int or_probe_launch(or_ctx* ctx, uint64_t first, uint64_t count, uint64_t total_packets, double* out);
+int or_upload_dust_emission(or_ctx* ctx, int32_t num_rf, const double* rf_sigma_abs, const double* rf_width,
+                            const double* rf_cmb, const double* rf_sigma_abs_lum, int32_t num_T, const double* T,
+                            const double* planck_abs, int32_t num_em, const double* em_lambda,
+                            const double* em_sigma_abs, const double* em_range, int32_t num_cells,
+                            const double* cell_volume);
+int or_upload_radiation_field(or_ctx* ctx, const double* rf);
+int or_prepare_secondary(or_ctx* ctx, const skgpu_secondary_options* options, uint64_t total_packets,
+                         double* luminosity);
+int or_fetch_dust_emission(or_ctx* ctx, double* luminosity, double* temperature, int32_t* num_points,
+                           double* lambda, double* pdf, double* cdf);
+int or_run_secondary(or_ctx* ctx, uint64_t first, uint64_t count);
 int or_fetch_instrument(or_ctx* ctx, int32_t instrument, double* ifu, double* sed, double* ifu_stats,
                         double* sed_stats);
 int or_fetch_instrument_components(or_ctx* ctx, int32_t instrument, double* ifu3, double* sed3);

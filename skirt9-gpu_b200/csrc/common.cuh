@@ -291,6 +291,44 @@ SKG_HD double clampedLogLog(const double* xv, const double* yv, int n, double x)
     return f1 * exp(log(x / x1) / log(x2 / x1) * (log(f2 / f1)));
 }
 
+// NR::interpolateLogLog (SKIRT/utils/NR.hpp:349-358): power-law interpolation between (x1, f1) and
+// (x2, f2); a non-positive end value gives that end's value at the end points and 0 between them
+SKG_HD double interpLogLog(double x, double x1, double x2, double f1, double f2)
+{
+    if (f1 <= 0 || f2 <= 0)
+    {
+        if (x == x1) return f1;
+        if (x == x2) return f2;
+        return 0;
+    }
+    return f1 * exp(log(x / x1) / log(x2 / x1) * (log(f2 / f1)));
+}
+
+// SpecialFunctions::gln(p, x) (SKIRT/utils/SpecialFunctions.cpp:798-811), the generalized
+// logarithm integrating a power law in NR::cdf2
+SKG_HD double gln(double p, double x)
+{
+    const double q = 1.0 - p;
+    if (q == 0.0) return log(x);
+    if (fabs(q) < 1e-3)
+    {
+        double lnx = log(x);
+        double s = q * lnx;
+        return lnx * (1.0 + 0.5 * s + 1.0 / 6.0 * s * s + 1.0 / 24.0 * s * s * s);
+    }
+    return (pow(x, q) - 1.0) / q;
+}
+
+// PlanckFunction(T)(lambda) (SKIRT/utils/PlanckFunction.cpp:12-27) with the constants of
+// SKIRT/utils/Constants.hpp (h, c, k): 2 h c^2 / lambda^5 / (exp(h c / (k T lambda)) - 1); 0 for T = 0
+SKG_HD double planckValue(double T, double lambda)
+{
+    const double h = 6.62606957e-34, c = 2.99792458e8, k = 1.3806488e-23;
+    double f1 = h * c / (k * T);
+    double f2 = 2.0 * h * c * c;
+    return f2 / pow(lambda, 5) / (exp(f1 / lambda) - 1.0);
+}
+
 // std::upper_bound index on an ascending array
 template<typename T>
 SKG_HD int upperBound(const T* xv, int n, T x)

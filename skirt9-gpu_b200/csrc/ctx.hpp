@@ -95,4 +95,21 @@ struct skgpu_ctx
 
     // learned path guiding (network, pilot records, optimizer state); null until first used
     skg::GuideState* guide = nullptr;
+
+    // secondary (dust) emission: the equilibrium-emission tables (skgpu_upload_dust_emission), the
+    // per-cell results and launch tables of the last skgpu_prepare_secondary, and the prepared source
+    skg::DustEmissionDev de{};
+    std::vector<void*> deBufs;        // the tables
+    std::vector<double> deEmLHost;    // the dust-emission grid wavelengths (host copy)
+    double deEmRange[2] = {0., 0.};
+    int deCells = 0;
+    std::vector<void*> secBufs;       // per-cell results and launch tables
+    int secCells = 0, secNpts = 0;
+    double *secL = nullptr, *secT = nullptr, *secPv = nullptr, *secCv = nullptr, *secXv = nullptr;
+    double *secLv = nullptr, *secWv = nullptr;
+    unsigned long long* secIv = nullptr;
+    int* secCellNode = nullptr;
+    skg::SecondaryDev* secDev = nullptr;
+    uint64_t secPackets = 0;          // packets of the prepared segment (0: not prepared)
+    double secLuminosity = 0.;
 };

@@ -40,6 +40,29 @@ cudaError_t groupStats(const Wave& w, const StatSpill* groups, unsigned long lon
 cudaError_t orderHistories(const Wave& w, unsigned short* keys, unsigned* counts, unsigned* cursor, unsigned* order,
                            int numSMs, cudaStream_t s);
 
+// tables of the equilibrium dust emission of the single dust mix (device pointers)
+struct DustEmissionDev
+{
+    const double* rfSig;   // nrf: sigma_abs on the radiation-field wavelengths (_rfsigmaabsvv[0])
+    const double* rfW;     // nrf: radiation-field bin widths (_rfdlambdav)
+    const double* rfCmb;   // nrf: CMB source term (_Bcmbv)
+    const double* rfSigL;  // nrf: the mix's sigma_abs at the bins' wavelengths (dust luminosity)
+    const double* T;       // nT: temperature grid (_Tv)
+    const double* planck;  // nT: Planck-integrated absorption cross sections (_planckabsvv[0])
+    const double* emL;     // nem: dust-emission grid wavelengths (extlambdav)
+    const double* emSig;   // nem: sigma_abs on the dust-emission grid (_emsigmaabsvv[0])
+    const double* vol;     // cells: cell volumes
+    int nrf, nT, nem;
+};
+
+// per-cell dust luminosity, equilibrium temperature and normalised emission pdf / cdf on the axis xv
+// (npts points; emission-grid entries [minRight, maxRight) between the range ends)
+cudaError_t launchDustCells(const DustEmissionDev& t, const double* dens, const double* rf, int numCells,
+                            const double* xv, int npts, int minRight, int maxRight, double* L, double* T, double* pv,
+                            double* Pv, cudaStream_t s);
+// the leaf node of every octree cell
+cudaError_t launchCellNodes(const int* tCell, int nodes, int* cellNode, cudaStream_t s);
+
 // path-segment and optical-depth kernels, FP64 (reference operation order) and FP32-distance walkers
 cudaError_t launchTracePathsFP64(int precision, const GridDev& g, int n, const double* rays, int maxSeg, int* count,
                                  int* m, double* ds, int* err, cudaStream_t s);

@@ -40,6 +40,23 @@ struct InstrDev
     double* sedStats;
 };
 
+// The prepared secondary (dust) emission source of a segment (DustSecondarySource with the
+// AllCellsLibrary: launch order = cell order). Histories [Iv[m], Iv[m+1]) launch from cell m.
+struct SecondaryDev
+{
+    const unsigned long long* Iv;  // numCells + 1 first history index per cell
+    const double* Lv;              // numCells normalised cell luminosities
+    const double* Wv;              // numCells composite-biased launch weights
+    const double* xv;              // npts wavelengths of the emission spectra (NR::cdf axis)
+    const double* pv;              // numCells * npts normalised emission pdf per cell
+    const double* Pv;              // numCells * npts normalised emission cdf per cell
+    const int* cellNode;           // octree: leaf node of each cell (its extent is the cell box)
+    int npts, numCells;
+    double Lpk;                    // _Lpp * Lv_s / Wv_s of SecondarySourceSystem (one source)
+    double xi;                     // DustEmissionOptions::wavelengthBias
+    double logMin, logWidth, bmin, bmax;  // its LogWavelengthDistribution
+};
+
 // read-only scene data of a run
 struct alignas(16) Scene  // 16-byte multiple: a batch stages its scene table as int4 words
 {
@@ -85,6 +102,8 @@ struct alignas(16) Scene  // 16-byte multiple: a batch stages its scene table as
     const float* guideImportance;    // per-pixel weight of the target frame's detections (null: 1)
     const unsigned char* guideBlob;  // packed BF16 network (mode 2)
     int* guideErr;
+    // secondary-emission segment: the prepared dust source (null for primary emission)
+    const SecondaryDev* sec;
 };
 
 // atomicAdd after summing the contributions of the warp's active lanes that target the same address
@@ -162,11 +181,90 @@ struct Launched
     double x, y, z, kx, ky, kz, L, lambda;
 };
 
+// SecondarySourceSystem::launch -> DustSecondarySource::launch / launchFromCell
+// (SecondarySourceSystem.cpp:118-133, DustSecondarySource.cpp:521-626): the cell from the history
+// index, the wavelength from the cell's emission spectrum (Random::cdfLogLog) or the log-uniform
+// bias distribution with its compensating weight (NR::value<NR::interpolateLogLog>), a uniform
+// position in the cell box (Random::position, Box::fracPos), an isotropic direction
+SKG_D Launched launchSecondary(const Scene& p, unsigned long long hist, Rng& rng)
+{
+    const SecondaryDev& S = *p.sec;
+    int m = upperBound(S.Iv, S.numCells + 1, hist) - 1;
+    m = min(max(m, 0), S.numCells - 1);
+    double ws = S.Lv[m] / S.Wv[m];
+    const double* xv = S.xv;
+    const double* pv = S.pv + static_cast<size_t>(m) * S.npts;
+    const double* Pv = S.Pv + static_cast<size_t>(m) * S.npts;
+    const int n = S.npts;
+    auto fromSpectrum = [&]() {
+        double X = rng.uniform();
+        int i = locateClip(Pv, n, X);
+        double alpha = log(pv[i + 1] / pv[i]) / log(xv[i + 1] / xv[i]);
+        return xv[i] * gexp(-alpha, (X - Pv[i]) / (pv[i] * xv[i]));
+    };
+    double lambda, w;
+    if (!S.xi)
+    {
+        lambda = fromSpectrum();
+        w = 1.;
+    }
+    else
+    {
+        if (rng.uniform() > S.xi)
+            lambda = fromSpectrum();
+        else
+            lambda = exp(S.logMin + S.logWidth * rng.uniform());
+        // NR::value<NR::interpolateLogLog>: 0 outside the spectrum's grid
+        double s = 0.;
+        if (!(lambda > xv[n - 1]))
+        {
+            int jl = -1, ju = n - 1;
+            while (ju - jl > 1)
+            {
+                int jm = (ju + jl) >> 1;
+                if (lambda < xv[jm]) ju = jm; else jl = jm;
+            }
+            if (jl >= 0) s = interpLogLog(lambda, xv[jl], xv[jl + 1], pv[jl], pv[jl + 1]);
+        }
+        if (!s)
+            w = 0.;
+        else
+        {
+            // LogWavelengthDistribution::probability, Range::containsFuzzy (relative 1e-14)
+            double b = (lambda >= S.bmin * (1 - 1e-14) && lambda <= S.bmax * (1 + 1e-14)) ? 1. / (S.logWidth * lambda) : 0.;
+            w = s / ((1 - S.xi) * s + S.xi * b);
+        }
+    }
+    // the cell box: Cartesian borders, or the extent of the octree leaf
+    double b0, b1, b2, b3, b4, b5;
+    if (p.g.kind == 0)
+    {
+        int i = m / (p.g.nz * p.g.ny), j = (m / p.g.nz) % p.g.ny, k = m % p.g.nz;
+        b0 = p.g.xb[i]; b1 = p.g.yb[j]; b2 = p.g.zb[k];
+        b3 = p.g.xb[i + 1]; b4 = p.g.yb[j + 1]; b5 = p.g.zb[k + 1];
+    }
+    else
+    {
+        const double* bb = p.g.tBounds + 6 * static_cast<size_t>(S.cellNode[m]);
+        b0 = bb[0]; b1 = bb[1]; b2 = bb[2]; b3 = bb[3]; b4 = bb[4]; b5 = bb[5];
+    }
+    Launched o;
+    double fx = rng.uniform(), fy = rng.uniform(), fz = rng.uniform();
+    o.x = xadd(b0, xmul(fx, xsub(b3, b0)));
+    o.y = xadd(b1, xmul(fy, xsub(b4, b1)));
+    o.z = xadd(b2, xmul(fz, xsub(b5, b2)));
+    isotropicDirection(rng, o.kx, o.ky, o.kz);
+    o.lambda = lambda;
+    o.L = xmul(xmul(S.Lpk, ws), w);
+    return o;
+}
+
 // SourceSystem::launch -> NormalizedSource::launch -> PointSource / GeometricSource
 // (SourceSystem.cpp, NormalizedSource.cpp:73-110, SepAxGeometry.cpp:11-19, SpheGeometry.cpp:25-32,
 // ExpDiskGeometry.cpp:46-69, LogWavelengthDistribution.cpp:31-34, Random.cpp:121-207)
 SKG_D Launched launchPacket(const Scene& p, unsigned long long hist, Rng& rng)
 {
+    if (p.sec) return launchSecondary(p, hist, rng);
     int h = 0;
     for (int q = 1; q < p.nsrc; ++q)
         if (p.src[q].first <= hist) h = q;

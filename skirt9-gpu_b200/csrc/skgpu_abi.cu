@@ -50,6 +50,12 @@ int fail(skgpu_ctx* c, int code, const std::string& msg)
             return fail(ctx, SKGPU_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
+void freeBufs(std::vector<void*>& v)
+{
+    for (void* p : v) cudaFree(p);
+    v.clear();
+}
+
 template<typename T>
 cudaError_t devAlloc(T** p, size_t n)
 {
@@ -134,6 +140,24 @@ constexpr uint64_t POOL_MAX = 1u << 22;
 // wavefront passes per run at most (each history needs about two passes per scattering event)
 constexpr long long MAX_PASSES = 2LL * MAX_SCATT_EVENTS + 64;
 
+template<typename T>
+int secAlloc(skgpu_ctx* ctx, std::vector<void*>& bufs, T** p, size_t n)
+{
+    CK(devAlloc(p, n));
+    bufs.push_back(*p);
+    return SKGPU_OK;
+}
+
+template<typename T>
+int secUpload(skgpu_ctx* ctx, std::vector<void*>& bufs, const T** p, const T* host, size_t n)
+{
+    T* d = nullptr;
+    CK(devUpload(&d, host, n));
+    bufs.push_back(d);
+    *p = d;
+    return SKGPU_OK;
+}
+
 void freeWave(skgpu_ctx* ctx)
 {
     ctx->graphCache.reset();  // its kernel nodes point into the buffers freed here
@@ -215,6 +239,15 @@ extern "C" {
 
 int skgpu_abi_version(void) { return SKGPU_ABI_VERSION; }
 
+int skgpu_device_count(int32_t* count)
+{
+    if (!count) return SKGPU_ERR_ARG;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) n = 0;
+    *count = n;
+    return SKGPU_OK;
+}
+
 int skgpu_create(int device, skgpu_ctx** out)
 {
     if (!out) return SKGPU_ERR_ARG;
@@ -271,6 +304,8 @@ void skgpu_destroy(skgpu_ctx* ctx)
     cudaFree(ctx->orderIdx);
     cudaFree(ctx->orderCounts);
     guideDestroy(ctx);
+    freeBufs(ctx->deBufs);
+    freeBufs(ctx->secBufs);
     devFree(ctx->errFlag);
     if (ctx->doneHost) cudaFreeHost(ctx->doneHost);
     for (int i = 0; i < 2; ++i)
@@ -1358,6 +1393,246 @@ int skgpu_run_primary(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t t
     w.anyStats = anyStats;
     w.statCap = STATS_CAP;
     if ((rc = prepareOrder(ctx, w))) return rc;
+    return runAndCollect(ctx, w, true, true);
+}
+
+// ------------------------------------------------------------------------------------------------
+// secondary (dust) emission
+// ------------------------------------------------------------------------------------------------
+
+int skgpu_upload_dust_emission(skgpu_ctx* ctx, int32_t num_rf, const double* rf_sigma_abs, const double* rf_width,
+                               const double* rf_cmb, const double* rf_sigma_abs_lum, int32_t num_T, const double* T,
+                               const double* planck_abs, int32_t num_em, const double* em_lambda,
+                               const double* em_sigma_abs, const double* em_range, int32_t num_cells,
+                               const double* cell_volume)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (num_rf < 1 || num_T < 2 || num_em < 2 || num_cells < 1 || !rf_sigma_abs || !rf_width || !rf_cmb
+        || !rf_sigma_abs_lum || !T || !planck_abs || !em_lambda || !em_sigma_abs || !em_range || !cell_volume)
+        return fail(ctx, SKGPU_ERR_ARG, "dust emission: missing tables");
+    if (!(em_range[0] > 0. && em_range[1] > em_range[0]))
+        return fail(ctx, SKGPU_ERR_ARG, "dust emission: empty wavelength range");
+    for (int i = 1; i < num_em; ++i)
+        if (!(em_lambda[i] > em_lambda[i - 1])) return fail(ctx, SKGPU_ERR_ARG, "dust emission: wavelengths not ascending");
+    if (!finiteAll(cell_volume, num_cells)) return fail(ctx, SKGPU_ERR_ARG, "dust emission: non-finite cell volume");
+    CK(cudaSetDevice(ctx->device));
+    freeBufs(ctx->deBufs);
+    ctx->de = DustEmissionDev{};
+    int rc = 0;
+    DustEmissionDev& d = ctx->de;
+    if ((rc = secUpload(ctx, ctx->deBufs, &d.rfSig, rf_sigma_abs, num_rf))) return rc;
+    if ((rc = secUpload(ctx, ctx->deBufs, &d.rfW, rf_width, num_rf))) return rc;
+    if ((rc = secUpload(ctx, ctx->deBufs, &d.rfCmb, rf_cmb, num_rf))) return rc;
+    if ((rc = secUpload(ctx, ctx->deBufs, &d.rfSigL, rf_sigma_abs_lum, num_rf))) return rc;
+    if ((rc = secUpload(ctx, ctx->deBufs, &d.T, T, num_T))) return rc;
+    if ((rc = secUpload(ctx, ctx->deBufs, &d.planck, planck_abs, num_T))) return rc;
+    if ((rc = secUpload(ctx, ctx->deBufs, &d.emL, em_lambda, num_em))) return rc;
+    if ((rc = secUpload(ctx, ctx->deBufs, &d.emSig, em_sigma_abs, num_em))) return rc;
+    if ((rc = secUpload(ctx, ctx->deBufs, &d.vol, cell_volume, num_cells))) return rc;
+    d.nrf = num_rf;
+    d.nT = num_T;
+    d.nem = num_em;
+    ctx->deEmLHost.assign(em_lambda, em_lambda + num_em);
+    ctx->deEmRange[0] = em_range[0];
+    ctx->deEmRange[1] = em_range[1];
+    ctx->deCells = num_cells;
+    ctx->secPackets = 0;
+    return SKGPU_OK;
+}
+
+int skgpu_upload_radiation_field(skgpu_ctx* ctx, const double* rf)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (!rf) return fail(ctx, SKGPU_ERR_ARG, "radiation field: missing array");
+    if (!ctx->nrf || !ctx->numCells) return fail(ctx, SKGPU_ERR_STATE, "radiation field: no medium or RF grid uploaded");
+    if (!finiteAll(rf, static_cast<size_t>(ctx->numCells) * ctx->nrf))
+        return fail(ctx, SKGPU_ERR_ARG, "radiation field: non-finite value");
+    CK(cudaSetDevice(ctx->device));
+    size_t len = static_cast<size_t>(ctx->numCells) * ctx->nrf;
+    if (ctx->rfLen != len)
+    {
+        devFree(ctx->rf);
+        devFree(ctx->rfT);
+        CK(devAlloc(&ctx->rf, len));
+        ctx->rfLen = len;
+    }
+    // the caller's layout is cell-major (m * nbins + ell), the device tally wavelength-major
+    std::vector<double> t(len);
+    const size_t cells = ctx->numCells, nb = ctx->nrf;
+    for (size_t m = 0; m < cells; ++m)
+        for (size_t e = 0; e < nb; ++e) t[e * cells + m] = rf[m * nb + e];
+    CK(cudaMemcpy(ctx->rf, t.data(), len * sizeof(double), cudaMemcpyHostToDevice));
+    return SKGPU_OK;
+}
+
+int skgpu_prepare_secondary(skgpu_ctx* ctx, const skgpu_secondary_options* opt, uint64_t total_packets,
+                            double* luminosity)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (!opt || total_packets == 0) return fail(ctx, SKGPU_ERR_ARG, "secondary: missing options or packets");
+    if (!ctx->hasGrid || (ctx->g.kind != SKGPU_GRID_CARTESIAN && ctx->g.kind != SKGPU_GRID_OCTREE))
+        return fail(ctx, SKGPU_ERR_UNSUPPORTED, "secondary: dust emission needs a Cartesian or octree grid");
+    if (!ctx->dens || ctx->numCells != ctx->g.numCells) return fail(ctx, SKGPU_ERR_STATE, "secondary: medium does not match the grid");
+    if (!ctx->de.nrf || ctx->deCells != ctx->numCells || ctx->de.nrf != ctx->nrf)
+        return fail(ctx, SKGPU_ERR_STATE, "secondary: dust emission tables do not match the medium and RF grid");
+    if (!ctx->rf || ctx->rfLen != static_cast<size_t>(ctx->numCells) * ctx->nrf)
+        return fail(ctx, SKGPU_ERR_STATE, "secondary: no radiation field on the device");
+    if (!(opt->spatial_bias >= 0. && opt->spatial_bias <= 1. && opt->source_bias >= 0. && opt->source_bias <= 1.
+          && opt->wavelength_bias >= 0. && opt->wavelength_bias <= 1.))
+        return fail(ctx, SKGPU_ERR_ARG, "secondary: bias fractions outside [0, 1]");
+    if (opt->wavelength_bias > 0. && !(opt->bias_lambda_min > 0. && opt->bias_lambda_max > opt->bias_lambda_min))
+        return fail(ctx, SKGPU_ERR_ARG, "secondary: empty wavelength-bias range");
+    CK(cudaSetDevice(ctx->device));
+    const int cells = ctx->numCells;
+
+    // the spectrum axis of NR::cdf: the range ends with the emission-grid wavelengths between them
+    const std::vector<double>& inx = ctx->deEmLHost;
+    const double rmin = ctx->deEmRange[0], rmax = ctx->deEmRange[1];
+    int minRight = static_cast<int>(std::upper_bound(inx.begin(), inx.end(), rmin) - inx.begin());
+    int maxRight = static_cast<int>(std::lower_bound(inx.begin(), inx.end(), rmax) - inx.begin());
+    int nb = 1 + maxRight - minRight;
+    if (nb < 1) return fail(ctx, SKGPU_ERR_ARG, "secondary: emission range outside the emission grid");
+    std::vector<double> xv(nb + 1);
+    xv[0] = rmin;
+    for (int j = minRight, i = 1; j < maxRight; ++j, ++i) xv[i] = inx[j];
+    xv[nb] = rmax;
+    const int npts = nb + 1;
+
+    if (ctx->secCells != cells || ctx->secNpts != npts)
+    {
+        freeBufs(ctx->secBufs);
+        ctx->secCells = ctx->secNpts = 0;
+        int rc = 0;
+        size_t rows = static_cast<size_t>(cells) * npts;
+        if ((rc = secAlloc(ctx, ctx->secBufs, &ctx->secL, cells))) return rc;
+        if ((rc = secAlloc(ctx, ctx->secBufs, &ctx->secT, cells))) return rc;
+        if ((rc = secAlloc(ctx, ctx->secBufs, &ctx->secPv, rows))) return rc;
+        if ((rc = secAlloc(ctx, ctx->secBufs, &ctx->secCv, rows))) return rc;
+        if ((rc = secAlloc(ctx, ctx->secBufs, &ctx->secXv, npts))) return rc;
+        if ((rc = secAlloc(ctx, ctx->secBufs, &ctx->secLv, cells))) return rc;
+        if ((rc = secAlloc(ctx, ctx->secBufs, &ctx->secWv, cells))) return rc;
+        if ((rc = secAlloc(ctx, ctx->secBufs, &ctx->secIv, static_cast<size_t>(cells) + 1))) return rc;
+        if ((rc = secAlloc(ctx, ctx->secBufs, &ctx->secCellNode, cells))) return rc;
+        if ((rc = secAlloc(ctx, ctx->secBufs, &ctx->secDev, 1))) return rc;
+        ctx->secCells = cells;
+        ctx->secNpts = npts;
+    }
+    ctx->secPackets = 0;
+    CK(cudaMemcpy(ctx->secXv, xv.data(), npts * sizeof(double), cudaMemcpyHostToDevice));
+    CK(launchDustCells(ctx->de, ctx->dens, ctx->rf, cells, ctx->secXv, npts, minRight, maxRight, ctx->secL, ctx->secT,
+                       ctx->secPv, ctx->secCv, ctx->stream));
+    if (ctx->g.kind == SKGPU_GRID_OCTREE) CK(launchCellNodes(ctx->g.tCell, ctx->g.tNodes, ctx->secCellNode, ctx->stream));
+    std::vector<double> Lv(cells);
+    CK(cudaMemcpyAsync(Lv.data(), ctx->secL, cells * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+
+    // DustSecondarySource::prepareLuminosities (DustSecondarySource.cpp:27-120) with the
+    // AllCellsLibrary (every cell its own entry, launch order = cell order): the cell luminosities
+    // normalised by their sum (valarray::sum, first to last)
+    double L = Lv[0];
+    for (int m = 1; m < cells; ++m) L += Lv[m];
+    if (luminosity) *luminosity = L;
+    ctx->secLuminosity = L;
+    if (!(L > 0.)) return SKGPU_OK;  // nothing to launch (SecondarySourceSystem::prepareForLaunch fails)
+    for (int m = 0; m < cells; ++m) Lv[m] /= L;
+    // DustSecondarySource::preparePacketMap (DustSecondarySource.cpp:124-152): composite-biased
+    // weights (1 - xi) Lv + xi / (number of emitting cells), and the first history index of every cell
+    // from the cumulative weight rounded to the nearest index
+    const double xi = opt->spatial_bias;
+    std::vector<double> wv(cells), Wv(cells);
+    for (int m = 0; m < cells; ++m) wv[m] = Lv[m] > 0 ? 1. : 0.;
+    double ws = wv[0];
+    for (int m = 1; m < cells; ++m) ws += wv[m];
+    for (int m = 0; m < cells; ++m) wv[m] /= ws;
+    for (int m = 0; m < cells; ++m) Wv[m] = (1 - xi) * Lv[m] + xi * wv[m];
+    const uint64_t N = total_packets;
+    std::vector<unsigned long long> Iv(static_cast<size_t>(cells) + 1);
+    Iv[0] = 0;
+    double W = 0.;
+    for (int p = 1; p != cells; ++p)
+    {
+        W += Wv[p - 1];
+        Iv[p] = std::min<uint64_t>(N, static_cast<uint64_t>(std::round(W * N)));
+    }
+    Iv[cells] = N;
+    CK(cudaMemcpy(ctx->secLv, Lv.data(), cells * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->secWv, Wv.data(), cells * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->secIv, Iv.data(), Iv.size() * sizeof(unsigned long long), cudaMemcpyHostToDevice));
+
+    // SecondarySourceSystem::prepareForLaunch / launch (SecondarySourceSystem.cpp:62-118) with the
+    // dust source alone (source weight 1): the source's launch weight Lv_s / Wv_s and the average
+    // packet luminosity L / N
+    const double xs = opt->source_bias;
+    const double Lpp = L / static_cast<double>(N);
+    const double Ws = (1 - xs) * 1. / 1. + xs * 1. / 1.;
+    SecondaryDev sd{};
+    sd.Iv = ctx->secIv;
+    sd.Lv = ctx->secLv;
+    sd.Wv = ctx->secWv;
+    sd.xv = ctx->secXv;
+    sd.pv = ctx->secPv;
+    sd.Pv = ctx->secCv;
+    sd.cellNode = ctx->secCellNode;
+    sd.npts = npts;
+    sd.numCells = cells;
+    sd.Lpk = Lpp * (1. / Ws);
+    sd.xi = opt->wavelength_bias;
+    sd.bmin = opt->bias_lambda_min;
+    sd.bmax = opt->bias_lambda_max;
+    sd.logMin = opt->wavelength_bias > 0. ? std::log(sd.bmin) : 0.;
+    sd.logWidth = opt->wavelength_bias > 0. ? std::log(sd.bmax) - std::log(sd.bmin) : 0.;
+    CK(cudaMemcpy(ctx->secDev, &sd, sizeof sd, cudaMemcpyHostToDevice));
+    ctx->secPackets = N;
+    return SKGPU_OK;
+}
+
+int skgpu_fetch_dust_emission(skgpu_ctx* ctx, double* luminosity, double* temperature, int32_t* num_points,
+                              double* lambda, double* pdf, double* cdf)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (!ctx->secCells || ctx->secCells != ctx->numCells) return fail(ctx, SKGPU_ERR_STATE, "fetch: no prepared dust emission");
+    CK(cudaSetDevice(ctx->device));
+    size_t cells = ctx->secCells, rows = cells * ctx->secNpts;
+    if (num_points) *num_points = ctx->secNpts;
+    if (luminosity) CK(cudaMemcpy(luminosity, ctx->secL, cells * sizeof(double), cudaMemcpyDeviceToHost));
+    if (temperature) CK(cudaMemcpy(temperature, ctx->secT, cells * sizeof(double), cudaMemcpyDeviceToHost));
+    if (lambda) CK(cudaMemcpy(lambda, ctx->secXv, ctx->secNpts * sizeof(double), cudaMemcpyDeviceToHost));
+    if (pdf) CK(cudaMemcpy(pdf, ctx->secPv, rows * sizeof(double), cudaMemcpyDeviceToHost));
+    if (cdf) CK(cudaMemcpy(cdf, ctx->secCv, rows * sizeof(double), cudaMemcpyDeviceToHost));
+    return SKGPU_OK;
+}
+
+int skgpu_run_secondary(skgpu_ctx* ctx, uint64_t first, uint64_t count)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (!ctx->secPackets || ctx->secCells != ctx->numCells)
+        return fail(ctx, SKGPU_ERR_STATE, "secondary: no prepared segment (skgpu_prepare_secondary)");
+    if (!ctx->hasOptions) return fail(ctx, SKGPU_ERR_STATE, "secondary: no options set");
+    if (!ctx->nmix) return fail(ctx, SKGPU_ERR_STATE, "secondary: no dust mix uploaded");
+    if (first + count > ctx->secPackets) return fail(ctx, SKGPU_ERR_ARG, "secondary: history range outside the segment");
+    CK(cudaSetDevice(ctx->device));
+    int groups, anyStats;
+    waveShape(ctx, groups, anyStats);
+    uint64_t poolMax = ctx->shapePool > 0 ? static_cast<uint64_t>(ctx->shapePool) : POOL_DEFAULT;
+    int P = static_cast<int>(std::min<uint64_t>(std::max<uint64_t>(count, 1), poolMax));
+    int rc = 0;
+    if ((rc = ensureWaveBuffers(ctx, P, groups, anyStats))) return rc;
+    Wave w = ctx->wave;
+    w.sc = sceneOf(ctx);
+    // the secondary source replaces the primary ones; the radiation field is not stored
+    // (SecondaryEmissionOptions::storeEmissionRadiationField off); the histories draw from streams
+    // of their own (a Philox key distinct from the primary segment's)
+    w.sc.sec = ctx->secDev;
+    w.sc.rfOn = 0;
+    w.sc.seed = ctx->opt.seed ^ SKGPU_SECONDARY_KEY;
+    w.traceBlocksPerSM = ctx->shapeTraceBlocks;
+    w.shadeBlocksPerSM = ctx->shapeShadeBlocks;
+    w.P = P;
+    w.first = first;
+    w.count = count;
+    w.anyStats = anyStats;
+    w.statCap = STATS_CAP;
+    w.order = nullptr;
     return runAndCollect(ctx, w, true, true);
 }
 

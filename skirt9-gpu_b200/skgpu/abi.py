@@ -101,6 +101,16 @@ class Counters(C.Structure):
     ]
 
 
+class SecondaryOptions(C.Structure):
+    _fields_ = [
+        ("spatial_bias", C.c_double),
+        ("source_bias", C.c_double),
+        ("wavelength_bias", C.c_double),
+        ("bias_lambda_min", C.c_double),
+        ("bias_lambda_max", C.c_double),
+    ]
+
+
 _P = C.c_void_p
 _I = C.c_int32
 _D = C.c_double
@@ -136,10 +146,15 @@ SIGNATURES = {
     "last_run_ms": [_P, _P],
     "trace_paths": [_P, _I, _P, _I, _I, _P, _P, _P],
     "optical_depths": [_P, _I, _P, _D, _I, _P],
+    "upload_dust_emission": [_P, _I, _P, _P, _P, _P, _I, _P, _P, _I, _P, _P, _P, _I, _P],
+    "upload_radiation_field": [_P, _P],
+    "prepare_secondary": [_P, _P, _U, _P],
+    "fetch_dust_emission": [_P, _P, _P, _P, _P, _P, _P],
+    "run_secondary": [_P, _U, _U],
 }
 
 # symbols of include/skgpu.h (the CUDA library must export every one)
-EXPORTED = ["skgpu_abi_version"] + ["skgpu_" + n for n in SIGNATURES]
+EXPORTED = ["skgpu_abi_version", "skgpu_device_count"] + ["skgpu_" + n for n in SIGNATURES]
 
 
 def _ptr(a):
@@ -322,6 +337,42 @@ class Backend:
         v = C.c_double()
         self.call("last_run_ms", C.cast(C.pointer(v), C.c_void_p))
         return v.value
+
+    # ---- secondary (dust) emission ----
+    def upload_dust_emission(self, rf_sigma_abs, rf_width, rf_cmb, rf_sigma_abs_lum, T, planck_abs, em_lambda,
+                             em_sigma_abs, em_range, cell_volume):
+        a = [f64(x) for x in (rf_sigma_abs, rf_width, rf_cmb, rf_sigma_abs_lum, T, planck_abs, em_lambda, em_sigma_abs,
+                              em_range, cell_volume)]
+        self.call("upload_dust_emission", len(a[0]), _ptr(a[0]), _ptr(a[1]), _ptr(a[2]), _ptr(a[3]), len(a[4]),
+                  _ptr(a[4]), _ptr(a[5]), len(a[6]), _ptr(a[6]), _ptr(a[7]), _ptr(a[8]), len(a[9]), _ptr(a[9]))
+
+    def upload_radiation_field(self, rf):
+        r = f64(rf).ravel()
+        self.call("upload_radiation_field", _ptr(r))
+
+    def prepare_secondary(self, total_packets, spatial_bias=0.5, source_bias=0.5, wavelength_bias=0.5,
+                          bias_range=(0.0, 0.0)):
+        """Prepares a secondary-emission segment of `total_packets` packets from the radiation field
+        of the context; returns the total dust luminosity."""
+        o = SecondaryOptions(float(spatial_bias), float(source_bias), float(wavelength_bias), float(bias_range[0]),
+                             float(bias_range[1]))
+        L = C.c_double()
+        self.call("prepare_secondary", C.cast(C.pointer(o), C.c_void_p), int(total_packets),
+                  C.cast(C.pointer(L), C.c_void_p))
+        return L.value
+
+    def fetch_dust_emission(self, num_cells):
+        """Per-cell dust luminosity and temperature, and the normalised emission spectra (axis, pdf, cdf)."""
+        n = C.c_int32()
+        L, T = np.zeros(num_cells), np.zeros(num_cells)
+        self.call("fetch_dust_emission", _ptr(L), _ptr(T), C.cast(C.pointer(n), C.c_void_p), None, None, None)
+        lam = np.zeros(n.value)
+        pdf, cdf = np.zeros((num_cells, n.value)), np.zeros((num_cells, n.value))
+        self.call("fetch_dust_emission", None, None, None, _ptr(lam), _ptr(pdf), _ptr(cdf))
+        return L, T, lam, pdf, cdf
+
+    def run_secondary(self, first, count):
+        self.call("run_secondary", int(first), int(count))
 
     def trace_paths(self, rays, max_segments, precision=PREC_FP64_EXACT):
         r = f64(rays).reshape(-1, 6)

@@ -42,6 +42,8 @@ class Scene:
         self.store_rf = False
         self.source_bias = 0.5
         self.explicit_absorption = False
+        self.dust_emission = None  # dict: equilibrium-emission tables (see Backend.upload_dust_emission)
+        self.secondary = None      # dict: spatial_bias, source_bias, wavelength_bias, bias_range
 
     # ------------------------------------------------------------------ uploads
     def upload(self, be):
@@ -77,6 +79,11 @@ class Scene:
             be.upload_rf_grid(self.rf["num_bins"], self.rf["borders"], self.rf["ellv"])
         if self.instruments:
             self._upload_instruments(be)
+        if self.dust_emission is not None:
+            d = self.dust_emission
+            be.upload_dust_emission(d["rf_sigma_abs"], d["rf_width"], d["rf_cmb"], d["rf_sigma_abs_lum"], d["T"],
+                                    d["planck_abs"], d["em_lambda"], d["em_sigma_abs"], d["em_range"],
+                                    d["cell_volume"])
 
     def _upload_instruments(self, be):
         structs, borders, ellv = [], [], []
@@ -179,7 +186,22 @@ class Scene:
         be.run_primary(first, npp if count is None else count, npp)
         return self.fetch(be)
 
-    def fetch(self, be):
+    def run_secondary(self, be, npp, seed=0, precision=abi.PREC_FP64_EXACT, first=0, count=None, clear=True,
+                      rf=None):
+        """One secondary (dust) emission segment of npp packets (histories [first, first+count)) from
+        the radiation field on the backend (the last primary segment's, or `rf`, cells x bins);
+        returns the tallies and the total dust luminosity."""
+        if clear:
+            be.clear_tallies()
+        be.set_options(self.options(seed, precision))
+        if rf is not None:
+            be.upload_radiation_field(rf)
+        s = self.secondary
+        L = be.prepare_secondary(npp, s["spatial_bias"], s["source_bias"], s["wavelength_bias"], s["bias_range"])
+        be.run_secondary(first, npp if count is None else count)
+        return self.fetch(be, rf=False), L
+
+    def fetch(self, be, rf=True):
         res = Results()
         for i, ins in enumerate(self.instruments):
             n = self.instrument_size(i)
@@ -195,7 +217,7 @@ class Scene:
                 if "components" in d:
                     d["components"] = d["components"].reshape((3,) + shape)
             res.instruments.append(d)
-        if self.store_rf:
+        if self.store_rf and rf:
             res.rf = be.fetch_radiation_field(len(self.density) * self.rf["num_bins"]).reshape(len(self.density), -1)
         res.counters = be.counters()
         res.ms = be.last_run_ms()
@@ -223,20 +245,24 @@ class Scene:
         return meta, load, has
 
     @staticmethod
-    def _panchromatic_source(meta, L, h):
-        """A geometric source with a black-body SED (panchromatic mode) from the reference's own launch
-        tables: the SED's (lambda, p, P) table for Random::cdfLogLog, the wavelength bias and its
-        log-uniform range, and the exponential-disk parameters or the Sersic cumulative-mass table."""
+    def _panchromatic_source(meta, L, h, position=None):
+        """A point or geometric source with a black-body SED (panchromatic mode) from the reference's own
+        launch tables: the SED's (lambda, p, P) table for Random::cdfLogLog, the wavelength bias and its
+        log-uniform range, and the point's position (from the launch probe), the exponential-disk
+        parameters or the Sersic cumulative-mass table."""
         p = f"source{h}_"
-        if meta.get(p + "type") != "GeometricSource" or meta.get(p + "sed") != "blackbody":
-            raise ValueError("export loader supports geometric sources with black-body SEDs in panchromatic mode")
+        if meta.get(p + "type") not in ("GeometricSource", "PointSource") or meta.get(p + "sed") != "blackbody":
+            raise ValueError("export loader supports point and geometric sources with black-body SEDs in "
+                             "panchromatic mode")
         src = dict(spectral_model=abi.SPEC_TABLE, lfrac=float(meta[p + "lfrac"]), weight=float(meta[p + "weight"]),
                    table_lambda=L(p + "sed_lambda"), table_a=L(p + "sed_p"), table_b=L(p + "sed_P"),
                    wavelength_bias=float(meta.get(p + "xi", 0.0)))
         if src["wavelength_bias"] > 0:
             src["bias_range"] = (float(meta[p + "bias_min"]), float(meta[p + "bias_max"]))
         geo = meta.get(p + "geometry")
-        if geo == "expdisk":
+        if meta.get(p + "type") == "PointSource":
+            src.update(position_model=abi.SRC_POINT, position=tuple(position))
+        elif geo == "expdisk":
             src.update(position_model=abi.SRC_EXPDISK,
                        geometry=tuple(float(meta[p + k]) for k in ("hR", "hz", "Rmin", "Rmax", "zmax")))
         elif geo == "sersic":
@@ -294,6 +320,18 @@ class Scene:
         if has("rf_wlg_borders"):
             ellv = L("rf_wlg_ellv")
             sc.rf = dict(num_bins=int(ellv.max()) + 1, borders=L("rf_wlg_borders"), ellv=ellv)
+        if has("de_T"):
+            # equilibrium dust emission (DustEmission mode): the reference's own tables and options
+            sc.dust_emission = {k: L("de_" + k) for k in ("rf_sigma_abs", "rf_width", "rf_cmb", "rf_sigma_abs_lum",
+                                                           "T", "planck_abs", "em_lambda", "em_sigma_abs",
+                                                           "em_range")}
+            sc.dust_emission["cell_volume"] = L("cell_volume")
+            sc.secondary = dict(spatial_bias=float(meta["secondary_spatial_bias"]),
+                                source_bias=float(meta["secondary_source_bias"]),
+                                wavelength_bias=float(meta["dust_emission_wavelength_bias"]),
+                                bias_range=(float(meta.get("dust_emission_bias_min", 0.0)),
+                                            float(meta.get("dust_emission_bias_max", 0.0))))
+            sc.store_rf = True
         sc.total_luminosity = float(meta["source_total_luminosity"])
         probe = L("src_probe")
         nsrc = int(meta["num_sources"])
@@ -308,7 +346,7 @@ class Scene:
                                position=tuple(probe[0, 2:5]), lfrac=float(meta["source0_lfrac"]),
                                weight=float(meta["source0_weight"]), table_lambda=lams, table_a=weights)]
         else:
-            sc.sources = [cls._panchromatic_source(meta, L, h) for h in range(nsrc)]
+            sc.sources = [cls._panchromatic_source(meta, L, h, probe[0, 2:5]) for h in range(nsrc)]
         for i in range(int(meta["num_instruments"])):
             p = f"instr{i}_"
             ellv = L(p + "wlg_ellv")

@@ -203,11 +203,30 @@ def sed_instrument(name, inclination_deg, stats=True, distance_mpc=10, comps=Tru
             f'numScatteringLevels="0" recordPolarization="false" recordStatistics="{"true" if stats else "false"}"/>')
 
 
+def dust_emission_options(em_min_um=1.0, em_max_um=1000.0, num_em=30, spatial_bias=0.5, source_bias=0.5,
+                          wavelength_bias=0.5, packets_multiplier=1.0):
+    """SecondaryEmissionOptions and DustEmissionOptions of a DustEmission simulation: equilibrium
+    emission, no CMB heating, AllCellsLibrary, a logarithmic dust-emission wavelength grid and a
+    log-uniform wavelength bias distribution over the same range."""
+    rng = f'minWavelength="{em_min_um:g} micron" maxWavelength="{em_max_um:g} micron"'
+    return (f'<secondaryEmissionOptions type="SecondaryEmissionOptions"><SecondaryEmissionOptions '
+            f'storeEmissionRadiationField="false" secondaryPacketsMultiplier="{packets_multiplier:g}" '
+            f'spatialBias="{spatial_bias:g}" sourceBias="{source_bias:g}"/></secondaryEmissionOptions>'
+            f'<dustEmissionOptions type="DustEmissionOptions"><DustEmissionOptions dustEmissionType="Equilibrium" '
+            f'includeHeatingByCMB="false" maxFractionOfPrimary="0.01" maxFractionOfPrevious="0.03" sourceWeight="1" '
+            f'wavelengthBias="{wavelength_bias:g}">'
+            f'<cellLibrary type="SpatialCellLibrary"><AllCellsLibrary/></cellLibrary>'
+            f'<dustEmissionWLG type="DisjointWavelengthGrid"><LogWavelengthGrid {rng} numWavelengths="{num_em}"/>'
+            f'</dustEmissionWLG><wavelengthBiasDistribution type="WavelengthDistribution">'
+            f'<LogWavelengthDistribution {rng}/></wavelengthBiasDistribution></DustEmissionOptions></dustEmissionOptions>')
+
+
 def simulation(mode, num_packets, sources, media, grid, instruments, source_wavelengths="0.55 micron",
                instrument_wlg='<ListWavelengthGrid wavelengths="0.55 micron" relativeHalfWidth="0" log="false"/>',
                force_scattering=True, store_rf=False, rf_wlg="", seed=0, num_density_samples=100,
-               min_weight_reduction=1e4, path_length_bias=0.5, explicit_absorption=False):
-    """A complete MonteCarloSimulation ski document."""
+               min_weight_reduction=1e4, path_length_bias=0.5, explicit_absorption=False, emission=""):
+    """A complete MonteCarloSimulation ski document (`emission`: the secondary and dust emission
+    options of a DustEmission simulation, see dust_emission_options)."""
     src_attr = f' wavelengths="{source_wavelengths}"' if mode.startswith("Oligo") else ' minWavelength="0.1 micron" maxWavelength="10 micron"'
     rf = ""
     if store_rf or rf_wlg:
@@ -215,6 +234,7 @@ def simulation(mode, num_packets, sources, media, grid, instruments, source_wave
               f'storeRadiationField="{"true" if store_rf else "false"}">'
               + (f'<radiationFieldWLG type="DisjointWavelengthGrid">{rf_wlg}</radiationFieldWLG>' if rf_wlg else "")
               + '</RadiationFieldOptions></radiationFieldOptions>')
+    rf += emission
     return f'''<?xml version="1.0" encoding="UTF-8"?>
 <skirt-simulation-hierarchy type="MonteCarloSimulation" format="9" producer="skgpu" time="2026-01-01T00:00:00">
 <MonteCarloSimulation userLevel="Expert" simulationMode="{mode}" iteratePrimaryEmission="false" iterateSecondaryEmission="false" numPackets="{num_packets:g}">
@@ -291,6 +311,30 @@ def galaxy_octree(num_packets=1e8, npix=512, nlambda=100, max_level=8, max_dust_
                       instrument_wlg=wlg, store_rf=store_rf, rf_wlg=wlg, num_density_samples=num_density_samples)
 
 
+def dust_galaxy(num_packets=1e5, npix=32, nlambda=20, num_em=30, max_level=6, max_dust_fraction=1e-4, tau_v=1.0,
+                half_size_kpc=25):
+    """The galaxy of galaxy_octree with dust emission (DustEmission mode) at reduced size: power-law
+    MeanListDustMix on 40 log wavelengths 0.1-1000 micron, radiation field on `nlambda` log bins 0.1-10
+    micron, equilibrium dust emission on `num_em` log bins 1-1000 micron, three frames at 0, 60 and 90
+    degrees and an SED instrument at 60 degrees on 30 log bins 0.1-1000 micron (statistics on)."""
+    lam = [0.1 * (1e4 ** (i / 39)) for i in range(40)]
+    kappa = [(l / 0.55) ** -1.0 for l in lam]
+    albedo = [min(0.9, max(0.01, 0.5 * (l / 0.55) ** -0.5)) for l in lam]
+    g = [min(0.9, max(0.0, 0.6 * (l / 0.55) ** -0.3)) for l in lam]
+    mix = mean_list_mix(lam, kappa, albedo, g)
+    sources = (geometric_source('<ExpDiskGeometry scaleLength="4 kpc" scaleHeight="0.35 kpc" minRadius="0 kpc" '
+                                'maxRadius="0 kpc" maxZ="0 kpc"/>', 6000, 8e9)
+               + geometric_source('<SersicGeometry effectiveRadius="1 kpc" index="4"/>', 4000, 2e9))
+    rf_wlg = f'<LogWavelengthGrid minWavelength="0.1 micron" maxWavelength="10 micron" numWavelengths="{nlambda}"/>'
+    iwlg = '<LogWavelengthGrid minWavelength="0.1 micron" maxWavelength="1000 micron" numWavelengths="30"/>'
+    fov = 2 * half_size_kpc
+    instruments = "".join(frame_instrument(f"i{inc}", inc, fov, "kpc", npix, stats=True) for inc in (0, 60, 90))
+    instruments += sed_instrument("sed", 60, True, comps=False)
+    return simulation("DustEmission", num_packets, sources, expdisk_medium(6, 0.2, "kpc", tau_v, mix),
+                      octree_grid(half_size_kpc, "kpc", max_level, max_dust_fraction), instruments,
+                      instrument_wlg=iwlg, store_rf=True, rf_wlg=rf_wlg, emission=dust_emission_options(num_em=num_em))
+
+
 def galaxy_voronoi(num_packets=1e8, npix=512, nlambda=100, num_sites=1_000_000, tau_v=2.0, half_size_kpc=25,
                    store_rf=True):
     """The galaxy of galaxy_octree on a VoronoiMeshSpatialGrid whose sites the reference draws from
@@ -321,6 +365,25 @@ def shell_cartesian(num_packets=1e6, nbins=64, npix=256, stats=True, points=None
                       shell_medium(0.1, 1, 2, 2, mix), cartesian_grid(1, nbins, points),
                       frame_instrument("i30", 30, 2, "pc", npix, stats) + sed_instrument("sed", 30, stats),
                       explicit_absorption=explicit_absorption, force_scattering=force_scattering)
+
+
+def dust_shell(num_packets=1e6, nbins=16, npix=32, stats=True, nlambda=20, num_em=30, grid=None):
+    """The dust shell of shell_cartesian with dust emission (DustEmission mode): a 5800 K black-body
+    point source of 1e5 Lsun (0.1-10 micron), power-law MeanListDustMix on 40 log wavelengths 0.1-1000
+    micron, radiation field on `nlambda` log bins 0.1-10 micron, equilibrium dust emission on `num_em`
+    log bins 1-1000 micron, a 32^2 frame at 30 degrees and an SED instrument at 30 degrees on 30 log
+    bins 0.1-1000 micron (statistics on). `grid` replaces the Cartesian grid."""
+    lam = [0.1 * (1e4 ** (i / 39)) for i in range(40)]
+    kappa = [(l / 0.55) ** -1.0 for l in lam]
+    albedo = [min(0.9, max(0.01, 0.5 * (l / 0.55) ** -0.5)) for l in lam]
+    g = [min(0.9, max(0.0, 0.6 * (l / 0.55) ** -0.3)) for l in lam]
+    mix = mean_list_mix(lam, kappa, albedo, g)
+    rf_wlg = f'<LogWavelengthGrid minWavelength="0.1 micron" maxWavelength="10 micron" numWavelengths="{nlambda}"/>'
+    iwlg = '<LogWavelengthGrid minWavelength="0.1 micron" maxWavelength="1000 micron" numWavelengths="30"/>'
+    return simulation("DustEmission", num_packets, point_source(luminosity_lsun=1e5), shell_medium(0.1, 1, 2, 2, mix),
+                      grid or cartesian_grid(1, nbins), frame_instrument("i30", 30, 2, "pc", npix, stats)
+                      + sed_instrument("sed", 30, stats, comps=False), instrument_wlg=iwlg, store_rf=True,
+                      rf_wlg=rf_wlg, emission=dust_emission_options(num_em=num_em))
 
 
 def galaxy_tetra(num_packets, vertex_filename, tau_v=1.0, npix=256, nlambda=32, half_size_kpc=25):

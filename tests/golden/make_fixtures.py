@@ -137,6 +137,7 @@ def main():
     cylinder3d_fixture()
     grid_stats_fixtures()
     galaxy_fixture()
+    dust_fixtures()
 
     # dust shell, 16^3 grid, 64^2 frame + SED: scene export + reference statistics (2e5 packets)
     npp = 200000
@@ -359,6 +360,26 @@ def galaxy_fixture(npp=500000, probe=20000):
     data["ref_npp"] = npp
     np.savez_compressed(os.path.join(OUT, "stats_galaxy.npz"), **data)
     print(f"stats_galaxy: {len(data['medium_density'])} cells, {npp} packets")
+
+
+def dust_fixtures():
+    """Equilibrium dust emission (DustEmission mode): the harness exports the scene, runs the primary
+    segment single-threaded, exports the dust-emission tables with the reference's own per-cell dust
+    luminosity, temperature and (every 97th emitting cell) emission spectrum for the radiation field of
+    that run, then runs the secondary segment into cleared detectors and dumps its raw sums. Two
+    scenes: the 16^3 Cartesian dust shell and the galaxy on the reference's octree at reduced size."""
+    for name, text, npp in (("dust_shell", ski.dust_shell(200000), 200000),
+                            ("dust_galaxy", ski.dust_galaxy(200000), 200000)):
+        data = run_raw(text, probe=2000)
+        for k in list(data):
+            if k.startswith("inst") and ("_wifu" in k or "_wsed" in k):
+                data[k] = data[k][:3]
+            elif k.startswith("inst") and (k.endswith("_ifu") or k.endswith("_sed") or k.endswith("_ifu_sec")
+                                           or k.endswith("_sed_sec")):
+                del data[k]
+        data["ref_npp"] = npp
+        np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **data)
+        print(f"{name}: {len(data['medium_density'])} cells, {npp} packets per segment")
 
 
 def reference_stats(fixture, ski_text, frame_name, npp):
