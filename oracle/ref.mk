@@ -69,7 +69,7 @@ LIBS := $(LIB)/libserialize.a $(LIB)/libschema.a $(LIB)/libfundamentals.a $(LIB)
         $(LIB)/libtetgen.a
 LINK_LIBS := -Wl,--start-group $(LIBS) -Wl,--end-group -pthread -ldl
 
-all: $(BIN)/skirt $(BIN)/skirt_export $(RES)/placeholder.txt
+all: $(BIN)/skirt $(BIN)/skirt_export $(RES)/placeholder.txt $(BIN)/skirt_gpu $(BIN)/skirt_oracle
 
 $(RES)/placeholder.txt:
 	@mkdir -p $(RES)
@@ -145,4 +145,54 @@ $(BIN)/skirt_export: $(OBJ)/harness/skirt_export.o $(O_MAINLIB) $(LIBS)
 	@mkdir -p $(BIN)
 	$(CXX) -o $@ $(OBJ)/harness/skirt_export.o $(O_MAINLIB) $(LINK_LIBS)
 
-.PHONY: all
+# The bridged program: the reference's skirt with the life-cycle hooks (patch_hooks.py, applied to
+# copies under $(OUT)/patched/) and the SKIRT-side bridge of the B200 library
+# (skirt9-gpu_b200/bridge/SkgpuLifeCycle.cpp), linked against lib/libskgpu.so. `skirt_gpu -g run.ski`
+# runs the ski file's life-cycle segments on the B200; without -g it is the reference program.
+PKG     := $(HERE)/../skirt9-gpu_b200
+BRIDGE  := $(PKG)/bridge
+PATCHED := $(OUT)/patched
+O_BRIDGE := $(OBJ)/bridge/MonteCarloSimulation.o $(OBJ)/bridge/SkirtCommandLineHandler.o $(OBJ)/bridge/SkgpuLifeCycle.o
+
+$(PATCHED)/MonteCarloSimulation.cpp $(PATCHED)/SkirtCommandLineHandler.cpp: $(HERE)/patch_hooks.py $(K_CORE)/MonteCarloSimulation.cpp $(K_MAIN)/SkirtCommandLineHandler.cpp
+	python3 $(HERE)/patch_hooks.py $(REF) $(PATCHED)
+
+$(OBJ)/bridge/MonteCarloSimulation.o: $(PATCHED)/MonteCarloSimulation.cpp $(BRIDGE)/SkgpuLifeCycle.hpp
+	@mkdir -p $(dir $@)
+	$(CXX) $(CXXFLAGS_REF) $(INC_CORE) -I$(K_CORE) -I$(BRIDGE) -c $< -o $@
+$(OBJ)/bridge/SkirtCommandLineHandler.o: $(PATCHED)/SkirtCommandLineHandler.cpp $(BRIDGE)/SkgpuLifeCycle.hpp $(GEN)/version.h
+	@mkdir -p $(dir $@)
+	$(CXX) $(CXXFLAGS_REF) $(INC_MAIN) -I$(K_MAIN) -I$(BRIDGE) -c $< -o $@
+$(OBJ)/bridge/SkgpuLifeCycle.o: $(BRIDGE)/SkgpuLifeCycle.cpp $(BRIDGE)/SkgpuLifeCycle.hpp $(HERE)/../include/skgpu.h
+	@mkdir -p $(dir $@)
+	$(CXX) $(CXXFLAGS_REF) $(INC_MAIN) $(INC_CORE) -I$(BRIDGE) -I$(HERE)/../include -c $< -o $@
+
+$(BIN)/skirt_gpu: $(O_BRIDGE) $(filter-out $(O_MAINLIB),$(O_MAIN)) $(LIBS) $(PKG)/lib/libskgpu.so
+	@mkdir -p $(BIN)
+	$(CXX) -o $@ $(O_BRIDGE) $(filter-out $(O_MAINLIB),$(O_MAIN)) $(LINK_LIBS) -L$(PKG)/lib -lskgpu \
+	    -Wl,-rpath,'$$ORIGIN/../../../../../skirt9-gpu_b200/lib'
+
+bridge: $(BIN)/skirt_gpu
+
+# Test infrastructure: the same bridged program with the bridge's skgpu_* calls renamed to the CPU
+# oracle's or_* entry points (same signatures, oracle/skoracle.h), linked against
+# oracle/_build/liboracle.so: runs the bridge's flattening and fetch logic end to end without a GPU
+# (tests/test_bridge_cpu.py).
+BRIDGE_FNS := create destroy last_error abi_version device_count upload_grid_cartesian upload_grid_sphere1d \
+    upload_grid_octree upload_medium upload_dust_mix upload_rf_grid upload_instruments upload_sources set_options \
+    clear_tallies run_primary fetch_instrument fetch_instrument_components fetch_radiation_field \
+    upload_dust_emission upload_radiation_field prepare_secondary run_secondary
+BRIDGE_ORACLE_DEFS := $(foreach f,$(BRIDGE_FNS),-Dskgpu_$(f)=or_$(f)) -Dskgpu_ctx=or_ctx -include $(HERE)/skoracle.h
+
+$(OBJ)/bridge/SkgpuLifeCycle_oracle.o: $(BRIDGE)/SkgpuLifeCycle.cpp $(BRIDGE)/SkgpuLifeCycle.hpp $(HERE)/skoracle.h
+	@mkdir -p $(dir $@)
+	$(CXX) $(CXXFLAGS_REF) $(INC_MAIN) $(INC_CORE) -I$(BRIDGE) -I$(HERE)/../include $(BRIDGE_ORACLE_DEFS) -c $< -o $@
+
+$(BIN)/skirt_oracle: $(OBJ)/bridge/MonteCarloSimulation.o $(OBJ)/bridge/SkirtCommandLineHandler.o \
+                     $(OBJ)/bridge/SkgpuLifeCycle_oracle.o $(filter-out $(O_MAINLIB),$(O_MAIN)) $(LIBS) $(HERE)/_build/liboracle.so
+	@mkdir -p $(BIN)
+	$(CXX) -o $@ $(OBJ)/bridge/MonteCarloSimulation.o $(OBJ)/bridge/SkirtCommandLineHandler.o \
+	    $(OBJ)/bridge/SkgpuLifeCycle_oracle.o $(filter-out $(O_MAINLIB),$(O_MAIN)) $(LINK_LIBS) \
+	    -L$(HERE)/_build -loracle -Wl,-rpath,'$$ORIGIN/../../../../_build'
+
+.PHONY: all bridge

@@ -245,6 +245,16 @@ void or_destroy(or_ctx* c)
 
 const char* or_last_error(const or_ctx* c) { return c ? c->err : "null context"; }
 
+int or_abi_version(void) { return SKGPU_ABI_VERSION; }
+
+/* the oracle has one (host) device */
+int or_device_count(int32_t* count)
+{
+    if (!count) return SKGPU_ERR_ARG;
+    *count = 1;
+    return SKGPU_OK;
+}
+
 /* ------------------------------------------------------------------------------------------- */
 /* grid uploads                                                                                */
 /* ------------------------------------------------------------------------------------------- */

@@ -25,6 +25,8 @@ typedef struct or_ctx or_ctx;
 int or_create(int device, or_ctx** out);
 void or_destroy(or_ctx* ctx);
 const char* or_last_error(const or_ctx* ctx);
+int or_abi_version(void);
+int or_device_count(int32_t* count);
 
 int or_upload_grid_cartesian(or_ctx* ctx, const double* xb, int32_t nxb, const double* yb, int32_t nyb,
                              const double* zb, int32_t nzb);

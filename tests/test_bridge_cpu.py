@@ -1,0 +1,76 @@
+"""The SKIRT-side bridge end to end without a GPU.
+
+oracle/_ref/exe/skirt/bin/skirt_oracle is the bridged reference program of tests/test_gpu_bridge.py
+with the bridge's C-ABI calls renamed to the CPU oracle's (oracle/ref.mk target skirt_oracle). It
+runs the bridge's own code (support checks, flattening of the SimulationItem tree into the upload
+calls, the fetch into FluxRecorder and MediumSystem arrays, the secondary-emission hand-over) with
+the oracle's life cycle; its outputs agree with the reference program's within Monte Carlo noise.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import test_gpu_bridge as tb
+from skgpu import ski
+
+SKIRT_ORACLE = os.path.join(tb.BIN, "skirt_oracle")
+
+needs_build = pytest.mark.skipif(not os.path.exists(SKIRT_ORACLE) or not os.path.exists(tb.SKIRT),
+                                 reason="reference build not present (oracle/ref.mk, run by __graft_entry__.build() "
+                                        "where the reference sources are)")
+
+
+def both(tmp_path, text, name):
+    log = tb.run(SKIRT_ORACLE, text, name, str(tmp_path / "bridge"), ["-g", "-t", "1"])
+    tb.run(tb.SKIRT, text, name, str(tmp_path / "cpu"), ["-t", "1"])
+    assert "primary histories on the B200" in log
+    return log, str(tmp_path / "bridge"), str(tmp_path / "cpu")
+
+
+@needs_build
+def test_bridge_shell_on_oracle(tmp_path):
+    log, g, c = both(tmp_path, ski.shell_cartesian(50000, nbins=16, npix=32), "shell")
+    z, (a, b) = tb.sed_z(g, c, "shell", "sed")
+    tb.check(z, 9.0, 4.0)
+    # the direct flux of the central point source is deterministic: equal to rounding
+    da, db = (np.loadtxt(os.path.join(d, "shell_sed_sed.dat"))[3] for d in (g, c))
+    assert da == pytest.approx(db, rel=1e-9)
+    z, _ = tb.frame_z(g, c, "shell", "i30")
+    tb.check(z, 1.3, 5.5)
+
+
+@needs_build
+def test_bridge_galaxy_octree_on_oracle(tmp_path):
+    text = ski.galaxy_octree(30000, npix=16, nlambda=10, max_level=5, max_dust_fraction=1e-3, stats=True, sed=True)
+    log, g, c = both(tmp_path, text, "galaxy")
+    z, _ = tb.sed_z(g, c, "galaxy", "sed")
+    tb.check(z, 1.8, 4.5)
+    for inc in (0, 60, 90):
+        z, _ = tb.frame_z(g, c, "galaxy", f"i{inc}")
+        tb.check(z, 1.4, 6.0)
+
+
+@needs_build
+def test_bridge_dust_emission_on_oracle(tmp_path):
+    log, g, c = both(tmp_path, ski.dust_shell(50000), "dust")
+    assert "secondary histories on the B200" in log
+    z, (a, b) = tb.sed_z(g, c, "dust", "sed")
+    fa, ra = a
+    fb, rb = b
+    m = (fa > 0) & (fb > 0) & (ra < 0.05) & (rb < 0.05)
+    assert m.sum() > 12
+    assert np.all(np.abs(fa[m] / fb[m] - 1) < np.maximum(5 * np.hypot(ra[m], rb[m]), 0.12))
+    ir = np.loadtxt(os.path.join(g, "dust_sed_sed.dat"))[:, 0] > 20
+    assert fa[ir].sum() == pytest.approx(fb[ir].sum(), rel=0.04)
+
+
+@needs_build
+def test_bridge_off_is_the_reference(tmp_path):
+    """Without -g the bridged program is the reference program: identical outputs."""
+    text = ski.shell_cartesian(5000, nbins=8, npix=8)
+    la = tb.run(SKIRT_ORACLE, text, "s", str(tmp_path / "a"), ["-t", "1"])
+    tb.run(tb.SKIRT, text, "s", str(tmp_path / "b"), ["-t", "1"])
+    assert "on the B200" not in la
+    sa, sb = (np.loadtxt(os.path.join(tmp_path / d, "s_sed_sed.dat")) for d in ("a", "b"))
+    assert np.array_equal(sa, sb)
