@@ -403,6 +403,56 @@ def result_line(args, name, world, value, total_ms, trace_ms, trace_launches, co
     }
 
 
+def fp32_error_report(args):
+    """The error of the production precision (FP32 walkers and accumulators) against the FP64
+    reference-order life cycle, on one segment of the workload with the same histories (same Philox
+    streams): per frame, per wavelength of the frames' integrated SED, per radiation-field entry and
+    per cell's absorbed luminosity, the relative difference of the total and the median / 99th
+    percentile over the entries above 1e-3 of the largest. Histories whose FP32 decisions differ
+    (a different interaction cell or scattering count) diverge afterwards, so the per-entry figures
+    include some Monte Carlo noise of those histories."""
+    from skgpu import Backend, abi
+    name = args.workload
+    sc = build_scene(name)
+    npp = args.packets or WORKLOADS[name][1]
+    be = Backend(device=0)
+    sc.upload(be)
+    res = {}
+    for prec in (abi.PREC_FP64_EXACT, abi.PREC_FP32):
+        t0 = time.perf_counter()
+        r = sc.run(be, npp, seed=12345, precision=prec)
+        res[prec] = (r, time.perf_counter() - t0)
+    r64, t64 = res[abi.PREC_FP64_EXACT]
+    r32, t32 = res[abi.PREC_FP32]
+
+    def stats(a, b):
+        a, b = np.asarray(a, float).ravel(), np.asarray(b, float).ravel()
+        m = np.abs(b) >= 1e-3 * np.abs(b).max()
+        rel = np.abs(a[m] - b[m]) / np.abs(b[m])
+        return {"total_rel": float(abs(a.sum() - b.sum()) / abs(b.sum())), "entries": int(m.sum()),
+                "median_rel": float(np.median(rel)), "p99_rel": float(np.quantile(rel, 0.99))}
+
+    out = {"mode": "fp32-vs-fp64", "workload": name, "packets": npp, "fp64_s": t64, "fp32_s": t32, "outputs": {}}
+    for i, ins in enumerate(sc.instruments):
+        a, b = r32[i]["total"], r64[i]["total"]
+        key = f"instrument{i}" + ("_frame" if ins["kind"] == abi.INSTR_FRAME else "_sed")
+        out["outputs"][key] = stats(a, b)
+        if ins["kind"] == abi.INSTR_FRAME:
+            out["outputs"][key + "_integrated_sed"] = stats(a.reshape(a.shape[0], -1).sum(axis=1),
+                                                            b.reshape(b.shape[0], -1).sum(axis=1))
+    if r64.rf is not None:
+        out["outputs"]["radiation_field"] = stats(r32.rf, r64.rf)
+        sig_abs = np.asarray(sc.mix["sigma_ext"]) - np.asarray(sc.mix["sigma_sca"])
+        nb = r64.rf.shape[1]
+        sab = sig_abs[:nb] if len(sig_abs) >= nb else np.resize(sig_abs, nb)
+        labs = lambda rf: (np.asarray(sc.density)[:, None] * sab[None, :] * rf).sum(axis=1)
+        out["outputs"]["absorbed_luminosity"] = stats(labs(r32.rf), labs(r64.rf))
+    out["counters_fp64"] = r64.counters
+    out["counters_fp32"] = r32.counters
+    print(json.dumps(out))
+    be.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -418,7 +468,13 @@ def main():
     ap.add_argument("--sims", type=int, default=16, help="batch workload: the first K simulations (profiling cases)")
     ap.add_argument("--packet-scale", type=float, default=1.0,
                     help="batch workload: fraction of every simulation's packets (profiling cases)")
+    ap.add_argument("--fp32-error", action="store_true",
+                    help="instead of timing: one segment of the workload in FP64 (reference operation order) and "
+                         "one in FP32 (production) on the same histories; prints the FP32 error of every output")
     args = ap.parse_args()
+    if args.fp32_error:
+        fp32_error_report(args)
+        return
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

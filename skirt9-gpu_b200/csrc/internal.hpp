@@ -17,11 +17,34 @@ struct GraphCache
 {
     cudaGraphExec_t exec = nullptr;
     std::vector<unsigned char> key;
+    // the second stream and the events of the split traversal (peel-off rays and propagation rays
+    // walked by two kernels side by side), created with the first captured graph
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, peelDone = nullptr, join = nullptr;
     void reset()
     {
         if (exec) cudaGraphExecDestroy(exec);
         exec = nullptr;
         key.clear();
+    }
+    cudaError_t ensureSplit()
+    {
+        cudaError_t e = cudaSuccess;
+        if (!side) e = cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking);
+        if (e == cudaSuccess && !fork) e = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
+        if (e == cudaSuccess && !peelDone) e = cudaEventCreateWithFlags(&peelDone, cudaEventDisableTiming);
+        if (e == cudaSuccess && !join) e = cudaEventCreateWithFlags(&join, cudaEventDisableTiming);
+        return e;
+    }
+    void release()
+    {
+        reset();
+        if (fork) cudaEventDestroy(fork);
+        if (peelDone) cudaEventDestroy(peelDone);
+        if (join) cudaEventDestroy(join);
+        if (side) cudaStreamDestroy(side);
+        fork = peelDone = join = nullptr;
+        side = nullptr;
     }
 };
 

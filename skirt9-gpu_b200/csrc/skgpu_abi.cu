@@ -297,7 +297,7 @@ void skgpu_destroy(skgpu_ctx* ctx)
     devFree(ctx->radR);
     devFree(ctx->radP);
     freeWave(ctx);
-    ctx->graphCache.reset();
+    ctx->graphCache.release();
     for (void* p : ctx->batchBufs) cudaFree(p);
     cudaFree(ctx->rfT);
     cudaFree(ctx->orderKeys);

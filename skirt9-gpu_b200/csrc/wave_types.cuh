@@ -76,7 +76,8 @@ struct TaskBuf
 struct Control
 {
     unsigned qn[2][NUM_KINDS];  // task counts per buffer and kind
-    unsigned traceCursor;
+    unsigned traceCursor;   // next task of the pass (all kinds, or the peel-off kernel's)
+    unsigned traceCursor2;  // next propagation task of the pass (propagation kernel)
     int freeTop;
     int nLaunch;
     int launchBase;

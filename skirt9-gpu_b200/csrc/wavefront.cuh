@@ -261,7 +261,13 @@ SKG_D float aadd(float a, float b) { return a + b; }
 SKG_D float amul(float a, float b) { return a * b; }
 SKG_D float aexp(float x) { return __expf(x); }
 
-template<class Walker, bool Multi = false>
+// Mode selects the task kinds a launch walks: TRACE_ALL every kind; TRACE_PEEL the peel-off rays
+// and TRACE_PROP the propagation rays (PROP1, PROP2, FREE), two kernels that the captured pass graph
+// runs side by side on two streams, each with its own task cursor. The peel-off kernel, which walks
+// two thirds of the crossings of the galaxy, then carries none of the propagation tasks' state.
+enum TraceMode { TRACE_ALL = 0, TRACE_PEEL = 1, TRACE_PROP = 2 };
+
+template<class Walker, bool Multi = false, int Mode = TRACE_ALL>
 __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __grid_constant__ Wave w, int cur)
 {
     // the scene of the lane's task: the kernel parameter's for one scene; for a batch, the scene
@@ -286,12 +292,16 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __g
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     unsigned n0 = w.ctl->qn[cur][0], n1 = w.ctl->qn[cur][1], n2 = w.ctl->qn[cur][2], n3 = w.ctl->qn[cur][3];
-    unsigned total = n0 + n1 + n2 + n3;
+    const unsigned total = Mode == TRACE_PEEL ? n0 : (Mode == TRACE_PROP ? n1 + n2 + n3 : n0 + n1 + n2 + n3);
     if (total == 0) return;
+    unsigned* const cursor = Mode == TRACE_PROP ? &w.ctl->traceCursor2 : &w.ctl->traceCursor;
 
     using Acc = typename Walker::Acc;  // FP64 (reference rounding) or FP32 optical depth and path length
     Walker wk;
     int kind = -1;  // -1: needs a task, -2: finished
+    // the task kind of a lane's current task, known at compile time where the mode fixes it
+    auto isPeel = [&]() { return Mode == TRACE_PEEL || (Mode == TRACE_ALL && kind == K_PEEL); };
+    auto isProp1 = [&]() { return Mode != TRACE_PEEL && kind == K_PROP1; };
     unsigned idx = 0;
     int slot = 0;
     // Per-task accumulators. The task kinds never share a lane at the same time, so their
@@ -316,7 +326,7 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __g
         {
             int leader = __ffs(need) - 1;
             unsigned base = 0;
-            if (lane == leader) base = atomicAdd(&w.ctl->traceCursor, static_cast<unsigned>(__popc(need)));
+            if (lane == leader) base = atomicAdd(cursor, static_cast<unsigned>(__popc(need)));
             base = __shfl_sync(FULL, base, leader);
             if (kind == -1)
             {
@@ -327,7 +337,8 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __g
                 }
                 else
                 {
-                    if (t < n0) { kind = K_PEEL; idx = t; }
+                    if (Mode == TRACE_PROP) t += n0;
+                    if (Mode == TRACE_PEEL || t < n0) { kind = K_PEEL; idx = t; }
                     else if (t < n0 + n1) { kind = K_PROP1; idx = t - n0; }
                     else if (t < n0 + n1 + n2) { kind = K_PROP2; idx = t - n0 - n1; }
                     else { kind = K_FREE; idx = t - n0 - n1 - n2; }
@@ -339,12 +350,13 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __g
                     // walk on the scattering optical depth (setScatteringAndAbsorptionOpticalDepths)
                     {
                         int ell = w.pk.rec[slot].ellMix;
-                        sext = static_cast<Acc>(scn().explicitAbs && kind >= K_PROP2 ? scn().mixSca[ell] : scn().mixExt[ell]);
+                        sext = static_cast<Acc>(scn().explicitAbs && !isPeel() && kind >= K_PROP2 ? scn().mixSca[ell]
+                                                                                                   : scn().mixExt[ell]);
                     }
                     tau = 0.;
                     nseg = 0;
                     guard = 0;
-                    if (kind == K_PEEL)
+                    if (isPeel())
                     {
                         const InstrDev& in = scn().instr[b.info[idx] & 0xFF];
                         fA = static_cast<Acc>(log(b.par[idx]) + 745.);  // taumax = log(L) + 745
@@ -355,7 +367,7 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __g
                     {
                         wk.start(scn().g, w.pk.rec[slot].x, w.pk.rec[slot].y, w.pk.rec[slot].z, w.pk.rec[slot].kx, w.pk.rec[slot].ky,
                                  w.pk.rec[slot].kz, w.pk.rec[slot].cell);
-                        if (kind == K_PROP1)
+                        if (isProp1())
                         {
                             fA = static_cast<Acc>(w.pk.rec[slot].L);
                             iA = scn().rfOn ? w.pk.rec[slot].ellRF : -1;
@@ -383,7 +395,7 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __g
             cross++;
             int m = wk.m;
             Acc ds = static_cast<Acc>(wk.ds);
-            if (kind == K_PEEL)
+            if (isPeel())
             {
                 if (m >= 0)
                 {
@@ -395,7 +407,7 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __g
                     }
                 }
             }
-            else if (kind == K_PROP1)
+            else if (isProp1())
             {
                 if (ds > 0.)
                 {
@@ -449,7 +461,7 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __g
                 if (atomicAdd(&w.ctl->counters[7], 1ULL) < 4ULL)
                 {
                     const TaskBuf& b = w.q[cur][kind];
-                    bool peel = kind == K_PEEL;
+                    bool peel = isPeel();
                     const double* ko = peel ? scn().instr[b.info[idx] & 0xFF].kobs : nullptr;
                     printf("skgpu: traversal guard: kind %d hist %llu start (%.17g %.17g %.17g) dir (%.17g %.17g %.17g) cell %d\n",
                            kind, static_cast<unsigned long long>(w.pk.rec[slot].hist), peel ? b.x[idx] : w.pk.rec[slot].x,
@@ -463,9 +475,9 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __g
         if (done)
         {
             const TaskBuf& b = w.q[cur][kind];
-            if (kind == K_PEEL)
+            if (isPeel())
                 b.tau[idx] = static_cast<double>(tau);
-            else if (kind == K_PROP1)
+            else if (isProp1())
                 b.tau[idx] = nseg ? static_cast<double>(tau) : 0.;
             else
             {
@@ -871,6 +883,7 @@ static __global__ void launchPrepKernel(const __grid_constant__ Wave w, int nxt)
     c->launchHist0 = w.first + c->launched;
     c->launched += n;
     c->traceCursor = 0;
+    c->traceCursor2 = 0;
     for (int k = 0; k < NUM_KINDS; ++k) c->qn[1 - nxt][k] = 0;  // the buffer consumed by this pass
 }
 
@@ -943,6 +956,7 @@ static __global__ void initPoolKernel(const __grid_constant__ Wave w)
         for (int b = 0; b < 2; ++b)
             for (int k = 0; k < NUM_KINDS; ++k) c->qn[b][k] = 0;
         c->traceCursor = 0;
+        c->traceCursor2 = 0;
         c->freeTop = w.P;
         c->nLaunch = 0;
         c->launchBase = 0;

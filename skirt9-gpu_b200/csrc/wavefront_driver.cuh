@@ -3,6 +3,7 @@
 #pragma once
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 #include <cuda_runtime.h>
@@ -16,19 +17,33 @@ struct WaveLaunch
 {
     int traceBlocks, shadeBlocks, guideBlocks, threads;
     bool guided, multi;
+    // split traversal: the peel-off kernel on the side stream, the propagation kernel on the main one
+    bool split;
+    int peelBlocks, propBlocks;
+    cudaStream_t side;
+    cudaEvent_t fork, peelDone, join;
 };
 
 // shared memory of the traversal kernel: the scene table of a batch
 inline size_t traceSmemBytes(const Wave& w) { return w.nScenes > 1 ? w.nScenes * sizeof(Scene) : 0; }
 
-template<class Walker>
+template<class Walker, int Mode = TRACE_ALL>
 int traceBlocksPerSM(bool multi, size_t smem)
 {
     int n = 0;
-    cudaError_t e = multi ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, traceKernel<Walker, true>, 256, smem)
-                          : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, traceKernel<Walker, false>, 256, 0);
+    cudaError_t e = multi ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, traceKernel<Walker, true, Mode>, 256, smem)
+                          : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, traceKernel<Walker, false, Mode>, 256, 0);
     if (e != cudaSuccess) return 1;
     return n > 0 ? n : 1;
+}
+
+template<class Walker, int Mode>
+void launchTrace(const Wave& w, int cur, int blocks, const WaveLaunch& L, cudaStream_t s)
+{
+    if (L.multi)
+        traceKernel<Walker, true, Mode><<<blocks, L.threads, traceSmemBytes(w), s>>>(w, cur);
+    else
+        traceKernel<Walker, false, Mode><<<blocks, L.threads, 0, s>>>(w, cur);
 }
 
 // `pass` is the index of the pass within its batch (selects the timer's events)
@@ -38,12 +53,27 @@ cudaError_t enqueuePass(const Wave& w, int pass, const WaveLaunch& L, cudaStream
     int cur = pass & 1, nxt = 1 - cur;
     cudaError_t e;
     if ((e = stageMark(t, pass, 0, s, capturing)) != cudaSuccess) return e;
-    if (L.multi)
-        traceKernel<Walker, true><<<L.traceBlocks, L.threads, traceSmemBytes(w), s>>>(w, cur);
+    if (L.split)
+    {
+        // peel-off rays and their detection on the side stream, propagation rays on this one; the
+        // stage kernels that end histories (and flush their statistics) wait for the detection
+        if ((e = cudaEventRecord(L.fork, s)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(L.side, L.fork, 0)) != cudaSuccess) return e;
+        launchTrace<Walker, TRACE_PEEL>(w, cur, L.peelBlocks, L, L.side);
+        if ((e = cudaEventRecord(L.peelDone, L.side)) != cudaSuccess) return e;
+        shadePeelKernel<<<L.shadeBlocks, L.threads, 0, L.side>>>(w, cur);
+        if ((e = cudaEventRecord(L.join, L.side)) != cudaSuccess) return e;
+        launchTrace<Walker, TRACE_PROP>(w, cur, L.propBlocks, L, s);
+        if ((e = cudaStreamWaitEvent(s, L.peelDone, 0)) != cudaSuccess) return e;
+        if ((e = stageMark(t, pass, 1, s, capturing)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(s, L.join, 0)) != cudaSuccess) return e;
+    }
     else
-        traceKernel<Walker, false><<<L.traceBlocks, L.threads, 0, s>>>(w, cur);
-    if ((e = stageMark(t, pass, 1, s, capturing)) != cudaSuccess) return e;
-    shadePeelKernel<<<L.shadeBlocks, L.threads, 0, s>>>(w, cur);
+    {
+        launchTrace<Walker, TRACE_ALL>(w, cur, L.traceBlocks, L, s);
+        if ((e = stageMark(t, pass, 1, s, capturing)) != cudaSuccess) return e;
+        shadePeelKernel<<<L.shadeBlocks, L.threads, 0, s>>>(w, cur);
+    }
     if ((e = stageMark(t, pass, 2, s, capturing)) != cudaSuccess) return e;
     shadeProp1Kernel<<<L.shadeBlocks, L.threads, 0, s>>>(w, cur, nxt);
     if ((e = stageMark(t, pass, 3, s, capturing)) != cudaSuccess) return e;
@@ -66,6 +96,16 @@ cudaError_t enqueuePass(const Wave& w, int pass, const WaveLaunch& L, cudaStream
 // pass limit is reached without finishing. `passes` receives the number of passes run.
 // the inputs a captured pass graph depends on: the wave parameters (by value in every kernel
 // node), the launch shape, the walker and the timing events recorded into it
+// the split traversal is on unless SKGPU_SPLIT_TRAVERSAL=0 (a switch for comparing the two forms)
+inline bool splitTraversal()
+{
+    static const bool on = [] {
+        const char* v = std::getenv("SKGPU_SPLIT_TRAVERSAL");
+        return !(v && v[0] == '0');
+    }();
+    return on;
+}
+
 template<class Walker>
 std::vector<unsigned char> graphKey(const Wave& w, const WaveLaunch& L, const StageTimer* timer)
 {
@@ -88,7 +128,7 @@ template<class Walker>
 cudaError_t runWave(const Wave& w, int numSMs, cudaStream_t s, unsigned long long* doneHost, long long* passes,
                     long long maxPasses, bool useGraph, StageTimer* timer, GraphCache* cache = nullptr)
 {
-    WaveLaunch L;
+    WaveLaunch L{};
     L.threads = 256;
     L.multi = w.nScenes > 1;
     int resident = traceBlocksPerSM<Walker>(L.multi, traceSmemBytes(w));
@@ -97,6 +137,22 @@ cudaError_t runWave(const Wave& w, int numSMs, cudaStream_t s, unsigned long lon
     L.shadeBlocks = numSMs * (w.shadeBlocksPerSM > 0 ? w.shadeBlocksPerSM : 4);
     L.guideBlocks = numSMs * 2;
     L.guided = w.sc.guideMode == 2;
+    // the split traversal runs in captured graphs without per-stage timing
+    L.split = false;
+    if (useGraph && cache && (!timer || timer->level <= 1) && splitTraversal())
+    {
+        if (cache->ensureSplit() == cudaSuccess)
+        {
+            L.split = true;
+            int cap = w.traceBlocksPerSM > 0 ? w.traceBlocksPerSM : 1 << 30;
+            L.peelBlocks = numSMs * std::min(cap, traceBlocksPerSM<Walker, TRACE_PEEL>(L.multi, traceSmemBytes(w)));
+            L.propBlocks = numSMs * std::min(cap, traceBlocksPerSM<Walker, TRACE_PROP>(L.multi, traceSmemBytes(w)));
+            L.side = cache->side;
+            L.fork = cache->fork;
+            L.peelDone = cache->peelDone;
+            L.join = cache->join;
+        }
+    }
     *passes = 0;
     if (timer)
         for (int i = 0; i < StageTimer::kStages; ++i) timer->active[i] = i != 5 || L.guided;
