@@ -42,6 +42,10 @@ WORKLOADS = {
     "voronoi": ("the galaxy's sources and 100 wavelengths on a Voronoi mesh of 1e6 sites drawn (seed 1234) from the "
                 "dust exp. disk, analytic density per cell, face-on tau_V=2, two 512^2 frames at 0/90 deg, radiation "
                 "field on 100 bins; one step = a 1e7-packet segment (a tenth of the 1e8-packet run)", 10_000_000),
+    "guided": ("learned path guiding on the edge-on dust disk (stellar disk + bulge in a dust disk of face-on "
+               "tau_V=50, 0.55 um, albedo 0.6, g=0.6) on a ~1e6-leaf octree, 512^2 edge-on frame with statistics: "
+               "1e7-packet plain pilot with recorded scattering events, training on the GPU, then 1e8-packet plain "
+               "and guided runs; value = figure-of-merit ratio guided / plain (FOM = 1 / (R_med^2 t))", 100_000_000),
     "batch": ("16 independent galaxies on Delaunay tetrahedral meshes (TetraMeshSpatialGrid), parameters from "
               "default_rng(2024): vertex counts log-uniform 1e4-4e5 (half uniform in the box, half from the dust "
               "disk), face-on tau_V log-uniform 0.1-10, packets log-uniform 1e6-1e7 (7.1e7 in all), 32 log "
@@ -150,14 +154,19 @@ def reference_run(scene_ski, npp, threads, files=None):
         return npp / max(secs, 1e-3), secs
 
 
-def reference_ski(name, npp):
-    from skgpu import ski
+def reference_inputs(name, npp):
+    """The ski file of the workload for the reference's own run and the input files beside it: the
+    Voronoi workload's reference reads the GPU arm's seeded sites (VoronoiMeshSpatialGrid policy
+    File) instead of drawing its own."""
+    from skgpu import ski, workloads
     if name == "shell":
-        return ski.shell_cartesian(npp, nbins=64, npix=256)
+        return ski.shell_cartesian(npp, nbins=64, npix=256), None
     if name == "galaxy":
-        return ski.galaxy_octree(npp)
+        return ski.galaxy_octree(npp), None
     if name == "voronoi":
-        return ski.galaxy_voronoi(npp)
+        h = 25.0 * workloads.KPC
+        sites = workloads.disk_sites(1_000_000, 6 * workloads.KPC, 0.2 * workloads.KPC, h)
+        return ski.galaxy_voronoi(npp, sites_file="sites.txt"), {"sites.txt": ski.vertex_file_text(sites)}
     raise SystemExit(name)
 
 
@@ -194,9 +203,11 @@ def cpu_baseline(name, sample_s=20.0):
                           f"{cores} run each, primary-emission segments {secs:.2f} s (setup excluded)"}
     if os.path.exists(REF_SKIRT):
         probe = 20000
-        rate, secs = reference_run(reference_ski(name, probe), probe, cores)
+        text, files = reference_inputs(name, probe)
+        rate, secs = reference_run(text, probe, cores, files)
         npp = int(min(5e7, max(probe, rate * sample_s)))
-        rate, secs = reference_run(reference_ski(name, npp), npp, cores)
+        text, files = reference_inputs(name, npp)
+        rate, secs = reference_run(text, npp, cores, files)
         return {"value": rate, "unit": "packets/s", "cores": cores, "kind": "reference",
                 "sample": f"{npp} packets of the same workload, skirt -t {cores}, primary-emission segment "
                           f"{secs:.2f} s (setup excluded)"}
@@ -224,13 +235,16 @@ def run_reference_arm(args, rank, world):
     if name == "batch":
         return run_reference_batch_arm(args, cores)
     probe = 20000
-    rate, _ = reference_run(reference_ski(name, probe), probe, cores)
+    text, files = reference_inputs(name, probe)
+    rate, _ = reference_run(text, probe, cores, files)
     npp = int(min(5e7, max(probe, rate * 8.0)))
     vals = []
     for _ in range(args.warmup):
-        reference_run(reference_ski(name, min(npp, probe)), min(npp, probe), cores)
+        text, files = reference_inputs(name, min(npp, probe))
+        reference_run(text, min(npp, probe), cores, files)
+    text, files = reference_inputs(name, npp)
     for _ in range(args.steps):
-        r, _ = reference_run(reference_ski(name, npp), npp, cores)
+        r, _ = reference_run(text, npp, cores, files)
         vals.append(r)
     value = statistics.median(vals)
     line = {"metric": "packets/s on 1 B200", "value": value, "unit": "packets/s", "n_gpus": args.gpus,
@@ -294,6 +308,13 @@ def run_batch_arm(args, rank, world, local):
         abi.run_batch(bes, zeros, packets, packets)
         return be0.last_run_ms()
 
+    # launch shape by the project autotuner (coordinate descent on a tenth of every simulation's
+    # histories), kept per grid kind; the timed steps run with it
+    shape = None
+    if not args.no_tune:
+        from skgpu import batch
+        part = [max(1, p // 10) for p in packets]
+        shape, _ = batch.tuned_shape(be0, abi.GRID_TETRA, lambda: abi.run_batch(bes, zeros, part, packets))
     for _ in range(args.warmup):
         step()
     abi.set_stage_timing(be0, 1)
@@ -346,7 +367,9 @@ def run_batch_arm(args, rank, world, local):
         line["config"]["simulations"] = n
         if n != 16 or args.packet_scale != 1.0:
             line["config"]["subset"] = f"first {n} simulations, {args.packet_scale:g} of their packets (profiling case)"
-        line["config"]["launch_shape"] = "default (pool 2^22 slots, resident traversal blocks, 4 stage blocks/SM)"
+        line["config"]["launch_shape"] = ({"tuned": shape, "note": "autotuner (skgpu.batch.autotune) on a tenth of the "
+                                           "histories; 0 = default"} if shape is not None else
+                                          "default (pool 2^22 slots, resident traversal blocks, 4 stage blocks/SM)")
         if not args.no_cpu_baseline:
             try:
                 line["cpu_baseline"] = cpu_baseline("batch")
@@ -376,11 +399,12 @@ def result_line(args, name, world, value, total_ms, trace_ms, trace_launches, co
     trace_bytes_per_launch = trace_algorithmic_bytes(counters, kind) / max(1, trace_launches / args.steps)
     trace_avg_ms = trace_ms / max(1, trace_launches)
     achieved = trace_bytes_per_launch / (trace_avg_ms / 1e3) / 1e9
-    traffic = None
+    traffic, profile = None, {}
     prof = os.path.join(ROOT, "profiles", f"trace_kernel_{name}_{args.precision}.json")
     if os.path.exists(prof):
         with open(prof) as f:
-            ratio = json.load(f).get("dram_bytes_per_algorithmic_byte")
+            profile = json.load(f)
+        ratio = profile.get("dram_bytes_per_algorithmic_byte")
         if ratio:
             traffic = ratio * trace_bytes_per_launch
     return {
@@ -392,15 +416,125 @@ def result_line(args, name, world, value, total_ms, trace_ms, trace_launches, co
                    "traversal": args.precision, "l2": "flushed between steps (256 MB write)",
                    "parallelism": f"history ranges x{world}" if name != "batch" else f"independent batches x{world}"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "peak_kind": peak_kind, "kernel": "skg::traceKernel",
+                     "traffic": traffic, "peak_kind": peak_kind,
+                     "kernel": profile.get("kernel", "skg::traceKernel"),
                      "launches_per_step": trace_launches / args.steps, "avg_launch_ms": trace_avg_ms,
                      "algorithmic_bytes_per_launch": trace_bytes_per_launch,
-                     "share_of_step": trace_ms / max(total_ms, 1e-9)},
+                     "share_of_step": trace_ms / max(total_ms, 1e-9),
+                     # what ncu shows limits it (profiles/): the algorithmic bytes come mostly from L2
+                     "limiter": profile.get("limiter"), "l2_throughput_frac": profile.get("l2_throughput_frac"),
+                     "dram_throughput_frac": profile.get("dram_throughput_frac")},
         "clocks": clk.summary(),
         "e2e": e2e,
         "gpu_launches": int(counters["kernel_launches"]) * args.steps,
         "counters_per_step": counters,
     }
+
+
+def run_guided_arm(args, rank, world, local):
+    """C5, the learned path guiding protocol on one GPU: a plain pilot of 1e7 packets records a
+    quarter of its scattering events with the downstream luminosity the edge-on frame detects,
+    the network trains on the GPU, then plain and guided runs of the same packet count are timed on
+    the device. FOM = 1 / (R_med^2 t) with R the per-pixel relative error from the frame's
+    per-history statistics, over all lit pixels and over the pixels whose flux is mostly scattered
+    light (more than half of it in the scattered component). Two trainings: the plain one
+    (importance = the target's detected luminosity) and one restricted to scattered light (a plain
+    pre-pilot's scattered-component image gives every scattered-light-dominated pixel the weight
+    1 / F_scattered and every other pixel 0). With --truth-packets N a plain run of N packets (in
+    segments) is the reference for the median per-pixel error of both runs."""
+    import torch
+    from skgpu import Backend, abi, guiding, workloads
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    sc = workloads.guided_disk()
+    sc.instruments[0]["comps"] = 1
+    n = args.packets or WORKLOADS["guided"][1]
+    pilot = max(1, n // 10)
+    be = Backend(device=local)
+    sc.upload(be)
+
+    def frame_stats(res):
+        ins = res.instruments[0]
+        st = np.asarray(ins["stats"]).reshape(5, -1)
+        comp = np.asarray(ins["components"]).reshape(3, -1)  # transparent, direct, scattered
+        return st, comp
+
+    def scored(res, seconds, n_hist, mask):
+        st, _ = frame_stats(res)
+        r = guiding.relative_error(st, n_hist)
+        lit = (st[1] > 0) & np.isfinite(r)
+        out = {"seconds": seconds}
+        for key, sel in (("all", lit), ("scattered", lit & mask)):
+            rm = float(np.median(r[sel])) if sel.any() else float("nan")
+            out[key] = {"pixels": int(sel.sum()), "R_med": rm, "FOM": 1.0 / (rm * rm * seconds) if rm > 0 else None}
+        return out
+
+    # plain run (also the classification of the pixels by their scattered fraction)
+    for _ in range(max(1, args.warmup)):
+        guiding.run(sc, be, pilot, seed=99)
+    plain, t_plain = guiding.run(sc, be, n, seed=1)
+    _, comp = frame_stats(plain)
+    tot = comp[1] + comp[2]
+    scat_mask = (tot > 0) & (comp[2] > 0.5 * tot)
+    line = {"metric": "figure-of-merit gain of guided over plain runs (edge-on frame)", "unit": "ratio",
+            "n_gpus": 1, "higher_is_better": True, "data": "synthetic", "dtype": "f32+f64 (BF16 network)",
+            "config": {"workload": "guided", "description": WORKLOADS["guided"][0], "packets": n,
+                       "pilot_packets": pilot}}
+    line["plain"] = scored(plain, t_plain, n, scat_mask)
+    variants = {}
+    images = {"plain": np.asarray(plain.instruments[0]["total"]).ravel()}
+    for name, restrict in (("plain-importance", False), ("scattered-importance", True)):
+        info = {}
+        if not restrict:
+            info = guiding.train(sc, be, pilot, target=0, seed=7, record_fraction=0.25, steps=2000,
+                                 prepilot_packets=0)
+        else:
+            pre, _ = guiding.run(sc, be, pilot, seed=5)
+            _, c = frame_stats(pre)
+            t = c[1] + c[2]
+            w = guiding.importance_from_image(c[2])
+            w = np.where((t > 0) & (c[2] > 0.5 * t), w, 0.0).astype(np.float32)
+            abi.guide_init(be, None, 11)
+            abi.guide_set_mode(be, abi.GUIDE_RECORD, 0, 0.0, 0.25, 1 << 22)
+            abi.guide_set_importance(be, w)
+            try:
+                guiding.run(sc, be, pilot, seed=7)
+            finally:
+                abi.guide_set_mode(be, abi.GUIDE_OFF)
+            abi.guide_set_training(be, 0)
+            info["loss_final"] = abi.guide_train(be, 2000, 16384, 1e-3, 9)
+        guided, t_guided = guiding.run_guided(sc, be, n, seed=1, alpha=0.5)
+        images[name] = np.asarray(guided.instruments[0]["total"]).ravel()
+        events, mean_w = abi.guide_last_weights(be)
+        v = scored(guided, t_guided, n, scat_mask)
+        v["training_loss"] = info.get("loss_final")
+        v["mean_weight_factor"] = mean_w
+        v["total_ratio"] = float(np.asarray(guided.instruments[0]["total"]).sum()
+                                 / np.asarray(plain.instruments[0]["total"]).sum())
+        for key in ("all", "scattered"):
+            fp, fg = line["plain"][key]["FOM"], v[key]["FOM"]
+            v[key]["FOM_gain"] = fg / fp if fp and fg else None
+        variants[name] = v
+    line["guided"] = variants
+    if args.truth_packets:
+        # the plain reference, in segments of 10x the run's packets (one random stream per history)
+        done, seg = 0, 10 * n
+        be.clear_tallies()
+        sc.prepare(be, args.truth_packets, seed=1000)
+        while done < args.truth_packets:
+            cnt = min(seg, args.truth_packets - done)
+            be.run_primary(done, cnt, args.truth_packets)
+            done += cnt
+        truth = np.asarray(sc.fetch(be).instruments[0]["total"]).ravel()
+        line["truth_packets"] = args.truth_packets
+        for key, sel in (("all", truth > 0), ("scattered", (truth > 0) & scat_mask)):
+            for name, img in images.items():
+                e = float(np.median(np.abs(img[sel] - truth[sel]) / truth[sel])) if sel.any() else None
+                (line["plain"] if name == "plain" else variants[name])[key]["median_error_vs_truth"] = e
+    line["value"] = variants["plain-importance"]["all"]["FOM_gain"]
+    print(json.dumps(line))
+    be.close()
 
 
 def fp32_error_report(args):
@@ -468,6 +602,10 @@ def main():
     ap.add_argument("--sims", type=int, default=16, help="batch workload: the first K simulations (profiling cases)")
     ap.add_argument("--packet-scale", type=float, default=1.0,
                     help="batch workload: fraction of every simulation's packets (profiling cases)")
+    ap.add_argument("--no-tune", action="store_true", help="batch workload: default launch shape instead of the "
+                                                            "autotuner's")
+    ap.add_argument("--truth-packets", type=int, default=0,
+                    help="guided workload: packets of a plain reference run for the per-pixel error (0: none)")
     ap.add_argument("--fp32-error", action="store_true",
                     help="instead of timing: one segment of the workload in FP64 (reference operation order) and "
                          "one in FP32 (production) on the same histories; prints the FP32 error of every output")
@@ -487,6 +625,12 @@ def main():
 
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    if args.workload == "guided":
+        run_guided_arm(args, rank, world, local)
         if dist:
             dist.destroy_process_group()
         return

@@ -324,9 +324,13 @@ int skgpu_run_secondary(skgpu_ctx* ctx, uint64_t first, uint64_t count);
 #define SKGPU_NOALLOC_SCRATCH_BYTES (48u * 1024u * 1024u)
 int skgpu_run_primary_noalloc(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t total_packets);
 /* Launch shape of later runs (0 keeps a default): packet slots in flight (default and maximum 2^22), resident
- * traversal blocks per SM (capped by what fits) and stage-kernel blocks per SM. Set by an
- * autotuner (skgpu/autotune.py); no reference counterpart. */
+ * traversal blocks per SM (capped by what fits) and stage-kernel blocks per SM. Set by the
+ * autotuner (skgpu/batch.py autotune); no reference counterpart. */
 int skgpu_set_launch_shape(skgpu_ctx* ctx, int32_t pool_slots, int32_t trace_blocks_per_sm, int32_t shade_blocks_per_sm);
+/* Number of waiting lanes (1-32) at which a warp of the traversal kernel takes new tasks in later
+ * runs; 0 keeps the walker's default (16 for Cartesian grids and octrees, 8 for Voronoi and
+ * tetrahedral meshes). Part of the launch shape the autotuner sets; no reference counterpart. */
+int skgpu_set_trace_refill(skgpu_ctx* ctx, int32_t lanes);
 /* Launch order of the histories of later runs. SKGPU_ORDER_WAVELENGTH (default): histories are
  * taken up in order of their launch wavelength (a counting sort at the start of every run whose
  * range exceeds the pool; 6 bytes of device memory per history), so that the packets in flight

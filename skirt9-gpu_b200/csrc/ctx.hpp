@@ -79,7 +79,7 @@ struct skgpu_ctx
     cudaEvent_t pinEv[2] = {nullptr, nullptr};
 
     // launch shape set by skgpu_set_launch_shape (0: defaults)
-    int shapePool = 0, shapeTraceBlocks = 0, shapeShadeBlocks = 0;
+    int shapePool = 0, shapeTraceBlocks = 0, shapeShadeBlocks = 0, shapeRefill = 0;
     // device tables of the last batched run (scene table, history prefix, first histories)
     std::vector<void*> batchBufs;
     // pass graph of the last run, replayed by the next run with the same parameters

@@ -126,6 +126,8 @@ static_assert(sizeof(TetRec) == 128, "one cache line per tetrahedron");
 struct GenBase
 {
     using Acc = double;  // accumulator type of optical depth and path length along the walk
+    // the wavefront runs peel-off and propagation rays as two concurrent traversal kernels
+    static constexpr bool kSplit = true;
     double rx, ry, rz, kx, ky, kz;
     double ds;
     int m;
@@ -598,6 +600,87 @@ SKG_D void xcross(double ax, double ay, double az, double bx, double by, double 
     cz = xsub(xmul(ax, by), xmul(ay, bx));
 }
 
+// Tetra::findEnteringFace (TetraMeshSpatialGrid.cpp:87-112): the face of tetrahedron t the ray at
+// (rx, ry, rz) with direction (kx, ky, kz) entered through, from Plucker products with its edges
+SKG_D int teFindEnteringFace(const GridDev& g, int t, double rx, double ry, double rz, double kx, double ky, double kz)
+{
+    const int etable[6][2] = {{3, 2}, {1, 3}, {2, 1}, {3, 0}, {0, 2}, {1, 0}};
+    int e = 0;
+    for (int t1 = 0; t1 < 3; t1++)
+    {
+        double v1x, v1y, v1z;
+        teVertex(g, t, t1, v1x, v1y, v1z);
+        for (int t2 = t1 + 1; t2 < 4; t2++)
+        {
+            double v2x, v2y, v2z;
+            teVertex(g, t, t2, v2x, v2y, v2z);
+            double mx, my, mz;
+            xcross(kx, ky, kz, xsub(rx, v1x), xsub(ry, v1y), xsub(rz, v1z), mx, my, mz);
+            double prod = xdot3(mx, xsub(v2x, v1x), my, xsub(v2y, v1y), mz, xsub(v2z, v1z));
+            if (prod != 0.) return prod < 0 ? etable[e][0] : etable[e][1];
+            e++;
+        }
+    }
+    return -1;
+}
+
+// The leaving face of tetrahedron t and the distance d to it, as one iteration of
+// TetraMeshSpatialGrid::MySegmentGenerator::next decides them (TetraMeshSpatialGrid.cpp:720-785):
+// the Plucker products of the ray with the edges of the entering face pick the leaving face; where a
+// product is zero the smallest positive plane distance over the three other faces does. enteringFace
+// is found first when it is -1. Returns -1 when no face lies ahead.
+SKG_D int teLeavingFace(const GridDev& g, int t, int& enteringFace, double rx, double ry, double rz, double kx, double ky,
+                        double kz, double& d)
+{
+    d = DBL_MAX;
+    if (enteringFace == -1) enteringFace = teFindEnteringFace(g, t, rx, ry, rz, kx, ky, kz);
+    if (enteringFace < 0) enteringFace = 0;  // degenerate direction: the plane fallback below decides
+    double vex, vey, vez;
+    teVertex(g, t, enteringFace, vex, vey, vez);
+    double mx, my, mz;
+    xcross(kx, ky, kz, xsub(rx, vex), xsub(ry, vey), xsub(rz, vez), mx, my, mz);
+    int cv[3];
+    clockwiseVertices(enteringFace, cv);
+    double c0x, c0y, c0z;
+    teVertex(g, t, cv[0], c0x, c0y, c0z);
+    double prod0 = xdot3(mx, xsub(vex, c0x), my, xsub(vey, c0y), mz, xsub(vez, c0z));
+    int clock0 = prod0 < 0;
+    int i = clock0 ? 1 : 2;
+    double cix, ciy, ciz;
+    teVertex(g, t, cv[i], cix, ciy, ciz);
+    double prodi = xdot3(mx, xsub(vex, cix), my, xsub(vey, ciy), mz, xsub(vez, ciz));
+    int cclocki = prodi >= 0;
+    const double* nrm = g.teNormals + 12 * static_cast<size_t>(t);
+    int leavingFace = -1;
+    if (prod0 == 0. || prodi == 0.)
+    {
+        for (int q = 0; q < 3; ++q)
+        {
+            int face = cv[q];
+            const double* n = nrm + 3 * face;
+            double ndotk = xdot3(n[0], kx, n[1], ky, n[2], kz);
+            if (ndotk > 0)
+            {
+                double dq = xdot3(n[0], xsub(vex, rx), n[1], xsub(vey, ry), n[2], xsub(vez, rz)) / ndotk;
+                if (dq < d)
+                {
+                    d = dq;
+                    leavingFace = face;
+                }
+            }
+        }
+    }
+    else
+    {
+        const int dtable[2][2] = {{1, 0}, {0, 2}};
+        leavingFace = cv[dtable[clock0][cclocki]];
+        const double* n = nrm + 3 * leavingFace;
+        double ndotk = xdot3(n[0], kx, n[1], ky, n[2], kz);
+        d = xdot3(n[0], xsub(vex, rx), n[1], xsub(vey, ry), n[2], xsub(vez, rz)) / ndotk;
+    }
+    return leavingFace;
+}
+
 struct TetraExact : GenBase
 {
     static constexpr int kMinBlocks = 3;
@@ -610,29 +693,6 @@ struct TetraExact : GenBase
         startRay(x, y, z, ux, uy, uz);
         mr = -1;
         enteringFace = -1;
-    }
-
-    // Tetra::findEnteringFace (TetraMeshSpatialGrid.cpp:87-112)
-    SKG_D int findEnteringFace(const GridDev& g, int t) const
-    {
-        const int etable[6][2] = {{3, 2}, {1, 3}, {2, 1}, {3, 0}, {0, 2}, {1, 0}};
-        int e = 0;
-        for (int t1 = 0; t1 < 3; t1++)
-        {
-            double v1x, v1y, v1z;
-            teVertex(g, t, t1, v1x, v1y, v1z);
-            for (int t2 = t1 + 1; t2 < 4; t2++)
-            {
-                double v2x, v2y, v2z;
-                teVertex(g, t, t2, v2x, v2y, v2z);
-                double mx, my, mz;
-                xcross(kx, ky, kz, xsub(rx, v1x), xsub(ry, v1y), xsub(rz, v1z), mx, my, mz);
-                double prod = xdot3(mx, xsub(v2x, v1x), my, xsub(v2y, v1y), mz, xsub(v2z, v1z));
-                if (prod != 0.) return prod < 0 ? etable[e][0] : etable[e][1];
-                e++;
-            }
-        }
-        return -1;
     }
 
     SKG_D bool next(const GridDev& g)
@@ -652,52 +712,8 @@ struct TetraExact : GenBase
         }
         for (int guard = 0; guard < 1000; ++guard)
         {
-            int leavingFace = -1;
-            double d = DBL_MAX;
-            if (enteringFace == -1) enteringFace = findEnteringFace(g, mr);
-            if (enteringFace < 0) enteringFace = 0;  // degenerate direction: the plane fallback below decides
-            double vex, vey, vez;
-            teVertex(g, mr, enteringFace, vex, vey, vez);
-            double mx, my, mz;
-            xcross(kx, ky, kz, xsub(rx, vex), xsub(ry, vey), xsub(rz, vez), mx, my, mz);
-            int cv[3];
-            clockwiseVertices(enteringFace, cv);
-            double c0x, c0y, c0z;
-            teVertex(g, mr, cv[0], c0x, c0y, c0z);
-            double prod0 = xdot3(mx, xsub(vex, c0x), my, xsub(vey, c0y), mz, xsub(vez, c0z));
-            int clock0 = prod0 < 0;
-            int i = clock0 ? 1 : 2;
-            double cix, ciy, ciz;
-            teVertex(g, mr, cv[i], cix, ciy, ciz);
-            double prodi = xdot3(mx, xsub(vex, cix), my, xsub(vey, ciy), mz, xsub(vez, ciz));
-            int cclocki = prodi >= 0;
-            const double* nrm = g.teNormals + 12 * static_cast<size_t>(mr);
-            if (prod0 == 0. || prodi == 0.)
-            {
-                for (int q = 0; q < 3; ++q)
-                {
-                    int face = cv[q];
-                    const double* n = nrm + 3 * face;
-                    double ndotk = xdot3(n[0], kx, n[1], ky, n[2], kz);
-                    if (ndotk > 0)
-                    {
-                        double dq = xdot3(n[0], xsub(vex, rx), n[1], xsub(vey, ry), n[2], xsub(vez, rz)) / ndotk;
-                        if (dq < d)
-                        {
-                            d = dq;
-                            leavingFace = face;
-                        }
-                    }
-                }
-            }
-            else
-            {
-                const int dtable[2][2] = {{1, 0}, {0, 2}};
-                leavingFace = cv[dtable[clock0][cclocki]];
-                const double* n = nrm + 3 * leavingFace;
-                double ndotk = xdot3(n[0], kx, n[1], ky, n[2], kz);
-                d = xdot3(n[0], xsub(vex, rx), n[1], xsub(vey, ry), n[2], xsub(vez, rz)) / ndotk;
-            }
+            double d;
+            int leavingFace = teLeavingFace(g, mr, enteringFace, rx, ry, rz, kx, ky, kz, d);
             if (leavingFace == -1 || d < g.eps)
             {
                 propagater(g.eps);

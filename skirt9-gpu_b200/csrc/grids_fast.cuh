@@ -383,6 +383,9 @@ struct VoronoiRec32 : GenBase
     using Acc = float;
     static constexpr int kMinBlocks = SKG_VORONOI32_MIN_BLOCKS;
     static constexpr int kRefillMin = SKG_VORONOI32_REFILL;  // waiting lanes before a warp takes new tasks
+    // one traversal kernel: the Voronoi walk's register footprint leaves no room for two resident
+    // kernels (4.62e6 packets/s unsplit against 4.41e6 split on the Voronoi galaxy)
+    static constexpr bool kSplit = false;
     static constexpr int kNone = -99;     // no previous cell (the wall ids -1..-6 are taken)
     static constexpr int kPad = -100;     // padding face
     int rec, prev;                        // record offsets of the current and the previous cell
@@ -545,8 +548,10 @@ struct VoronoiRec32 : GenBase
 // tetrahedron: the exit is the nearest face plane ahead, s_f = (c_f - n_f . r) / (n_f . k) over the
 // faces with n_f . k > 0 other than the face just entered (a ray cannot re-enter a convex cell),
 // with the plane offset difference in FP64 and the division in FP32. Shared faces are one plane
-// seen from both sides, so the walk stays watertight: a point that rounding puts just past the exit
-// plane gives a zero-length step into the neighbour, which is taken without reporting a segment.
+// seen from both sides, so the walk stays watertight. The float planes are tilted from the exact
+// ones by up to ~1e-7 of a tetrahedron's size; a decision within that bound of an edge, a vertex or
+// a tie between two faces is re-taken in FP64 by the reference's Plucker decision (teLeavingFace),
+// so that the cell sequence is the reference's.
 // As the reference, the last in-mesh segment is dropped when the path leaves the hull. A start at a
 // known cell (a scattering event's interaction cell) needs no point location; otherwise a walk over
 // the face planes from the search block's representative finds the containing tetrahedron.
@@ -621,6 +626,10 @@ struct TetraPlane32 : GenBase
     using Acc = float;
     static constexpr int kMinBlocks = SKG_TETRA32_MIN_BLOCKS;
     static constexpr int kRefillMin = 8;  // waiting lanes before a warp takes new tasks
+    // bound on the displacement of a float plane from its exact one, in units of eps (1e-12 of the
+    // domain diagonal): 2^-24 per normal component over at most the diagonal, with margin
+    static constexpr double kTilt = 1.6e5;
+    static constexpr float kNk = 1e-6f;  // |n.k| below this may have either sign in exact arithmetic
     int mr, ef;  // current tetrahedron, face it was entered through (-1: none)
     int hint;
     float kxf, kyf, kzf;
@@ -651,47 +660,79 @@ struct TetraPlane32 : GenBase
             }
             if (ds > 0.) return true;
         }
+        // the float planes (normals rounded to FP32, offsets through a shared vertex, so neighbours
+        // agree) lie within kTilt * eps = 1.6e-7 of the domain diagonal of the exact ones; a decision
+        // closer than that to an edge, a vertex or a tie is re-taken in FP64 the reference's way
+        const double tol = kTilt * g.eps;
         for (int guard = 0; guard < 256; ++guard)
         {
             TetRegs r = TetRegs::load(g.teRec + mr);
-            float best = FLT_MAX;
+            float best = FLT_MAX, second = FLT_MAX, nkBest = 1.f, nkSecond = 1.f;
+            double inside = DBL_MAX, graze = DBL_MAX;
             int lf = -1;
             auto face = [&](auto F) {
                 constexpr int f = decltype(F)::value;
+                if (f == ef) return;
                 float nk = r.n[3 * f] * kxf + r.n[3 * f + 1] * kyf + r.n[3 * f + 2] * kzf;
-                if (f == ef || !(nk > 0.f)) return;
-                float s = static_cast<float>(-r.template excess<f>(rx, ry, rz)) / nk;
+                double e = r.template excess<f>(rx, ry, rz);
+                if (!(nk > 0.f))
+                {
+                    if (nk > -kNk) graze = fmin(graze, -e);  // may be a face ahead in exact arithmetic
+                    return;
+                }
+                float s = static_cast<float>(-e) / nk;
                 if (s < best)
                 {
+                    second = best;
+                    nkSecond = nkBest;
                     best = s;
+                    nkBest = nk;
+                    inside = -e;
                     lf = f;
+                }
+                else if (s < second)
+                {
+                    second = s;
+                    nkSecond = nk;
                 }
             };
             face(std::integral_constant<int, 0>());
             face(std::integral_constant<int, 1>());
             face(std::integral_constant<int, 2>());
             face(std::integral_constant<int, 3>());
-            if (lf < 0)
+            bool exact = lf < 0 || inside < tol || graze < tol + 1e-6 * best ||
+                         (second < FLT_MAX && second - best < tol * (1. / nkBest + 1. / nkSecond) + 1e-6 * second);
+            int nt, nf;
+            if (!exact)
             {
-                // no face ahead (degenerate direction or position): the reference's eps step and a
-                // fresh point location
-                propagater(g.eps);
-                mr = tetraLocate(g, rx, ry, rz);
-                ef = -1;
-                if (mr < 0)
-                {
-                    state = GS_OUTSIDE;
-                    return false;
-                }
-                continue;
-            }
-            int nt = r.neighbour(lf);
-            int nf = (r.nface >> (8 * lf)) & 0xff;
-            if (best > 0.f)
-            {
+                nt = r.neighbour(lf);
+                nf = (r.nface >> (8 * lf)) & 0xff;
                 m = mr;
                 ds = best;
                 propagater(ds);
+            }
+            else
+            {
+                double d;
+                int xf = teLeavingFace(g, mr, ef, rx, ry, rz, kx, ky, kz, d);
+                if (xf == -1 || d < g.eps)
+                {
+                    // no exit point: the reference's eps step and its own point location
+                    propagater(g.eps);
+                    mr = tetraCellIndex(g, rx, ry, rz);
+                    ef = -1;
+                    if (mr < 0)
+                    {
+                        state = GS_OUTSIDE;
+                        return false;
+                    }
+                    continue;
+                }
+                nt = g.teNTet[4 * static_cast<size_t>(mr) + xf];
+                nf = g.teNFace[4 * static_cast<size_t>(mr) + xf];
+                m = mr;
+                ds = d;
+                propagater(d);
             }
             mr = nt;
             ef = nf;
@@ -701,7 +742,7 @@ struct TetraPlane32 : GenBase
                 state = GS_OUTSIDE;
                 return false;
             }
-            if (best > 0.f) return true;
+            return true;
         }
         state = GS_OUTSIDE;
         return false;

@@ -21,6 +21,7 @@ struct GraphCache
     // walked by two kernels side by side), created with the first captured graph
     cudaStream_t side = nullptr;
     cudaEvent_t fork = nullptr, peelDone = nullptr, join = nullptr;
+    bool lastSplit = false;  // the last run split its traversal (one more kernel per pass)
     void reset()
     {
         if (exec) cudaGraphExecDestroy(exec);

@@ -1335,7 +1335,8 @@ static int runAndCollect(skgpu_ctx* ctx, const Wave& w, bool useGraph, bool time
     ctx->lastCounters.rf_stores = ctl.counters[4];
     ctx->lastCounters.stats_overflows = ctl.counters[5];
     ctx->lastCounters.stats_spilled = ctl.counters[6];
-    ctx->lastCounters.kernel_launches = static_cast<uint64_t>(passes) * (w.sc.guideMode == 2 ? 8 : 7) + 1 + (w.order ? 3 : 0);
+    const int perPass = (w.sc.guideMode == 2 ? 8 : 7) + (useGraph && ctx->graphCache.lastSplit ? 1 : 0);
+    ctx->lastCounters.kernel_launches = static_cast<uint64_t>(passes) * perPass + 1 + (w.order ? 3 : 0);
     ctx->lastPasses = passes;
     ctx->lastGuideWeightSum = ctl.guideWeightSum;
     ctx->lastGuideEvents = ctl.guideEvents;
@@ -1386,6 +1387,7 @@ int skgpu_run_primary(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t t
     Wave w = ctx->wave;
     w.sc = sceneOf(ctx);
     w.traceBlocksPerSM = ctx->shapeTraceBlocks;
+    w.refillMin = ctx->shapeRefill;
     w.shadeBlocksPerSM = ctx->shapeShadeBlocks;
     w.P = P;
     w.first = first;
@@ -1626,6 +1628,7 @@ int skgpu_run_secondary(skgpu_ctx* ctx, uint64_t first, uint64_t count)
     w.sc.rfOn = 0;
     w.sc.seed = ctx->opt.seed ^ SKGPU_SECONDARY_KEY;
     w.traceBlocksPerSM = ctx->shapeTraceBlocks;
+    w.refillMin = ctx->shapeRefill;
     w.shadeBlocksPerSM = ctx->shapeShadeBlocks;
     w.P = P;
     w.first = first;
@@ -1768,6 +1771,7 @@ int skgpu_run_primary_noalloc(skgpu_ctx* ctx, uint64_t first, uint64_t count, ui
     carveWave(w, static_cast<unsigned char*>(addr), SKGPU_NOALLOC_MAX_SLOTS, groups, anyStats);
     w.sc = sceneOf(ctx);
     w.traceBlocksPerSM = ctx->shapeTraceBlocks;
+    w.refillMin = ctx->shapeRefill;
     w.shadeBlocksPerSM = ctx->shapeShadeBlocks;
     w.P = static_cast<int>(std::min<uint64_t>(std::max<uint64_t>(count, 1), SKGPU_NOALLOC_MAX_SLOTS));
     w.first = first;
@@ -2281,6 +2285,14 @@ int skgpu_set_launch_shape(skgpu_ctx* ctx, int32_t pool_slots, int32_t trace_blo
     return SKGPU_OK;
 }
 
+int skgpu_set_trace_refill(skgpu_ctx* ctx, int32_t lanes)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (lanes < 0 || lanes > 32) return fail(ctx, SKGPU_ERR_ARG, "trace refill: lanes in [0, 32]");
+    ctx->shapeRefill = lanes;
+    return SKGPU_OK;
+}
+
 int skgpu_run_batch(skgpu_ctx* const* ctxs, int32_t n, const uint64_t* first, const uint64_t* count,
                     const uint64_t* total_packets)
 {
@@ -2346,6 +2358,7 @@ int skgpu_run_batch(skgpu_ctx* const* ctxs, int32_t n, const uint64_t* first, co
     w.anyStats = anyStats;
     w.statCap = STATS_CAP;
     w.traceBlocksPerSM = ctx->shapeTraceBlocks;
+    w.refillMin = ctx->shapeRefill;
     w.shadeBlocksPerSM = ctx->shapeShadeBlocks;
     if ((rc = prepareOrder(ctx, w))) return rc;
     return runAndCollect(ctx, w, true, true);

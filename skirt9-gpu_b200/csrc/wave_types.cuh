@@ -110,8 +110,9 @@ struct Wave
     int nScenes;
     const unsigned long long* prefix;  // nScenes + 1
     const unsigned long long* sfirst;  // nScenes: first segment history of each scene
-    // launch shape (0: defaults): resident trace blocks per SM, shade blocks per SM
-    int traceBlocksPerSM, shadeBlocksPerSM;
+    // launch shape (0: defaults): resident trace blocks per SM, shade blocks per SM, and the number
+    // of waiting lanes at which a warp of the traversal kernel takes new tasks
+    int traceBlocksPerSM, shadeBlocksPerSM, refillMin;
     // launch order: histories first + order[i] for i = 0, 1, ... (null: index order)
     const unsigned* order;
     PacketPool pk;

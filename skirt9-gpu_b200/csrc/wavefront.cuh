@@ -291,6 +291,7 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __g
     };
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
+    const int refillMin = w.refillMin > 0 ? w.refillMin : Walker::kRefillMin;
     unsigned n0 = w.ctl->qn[cur][0], n1 = w.ctl->qn[cur][1], n2 = w.ctl->qn[cur][2], n3 = w.ctl->qn[cur][3];
     const unsigned total = Mode == TRACE_PEEL ? n0 : (Mode == TRACE_PROP ? n1 + n2 + n3 : n0 + n1 + n2 + n3);
     if (total == 0) return;
@@ -317,12 +318,13 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __g
     while (true)
     {
         unsigned need = __ballot_sync(FULL, kind == -1);
-        // A warp takes new tasks once Walker::kRefillMin lanes wait (or none is busy), not for every
+        // A warp takes new tasks once refillMin lanes wait (or none is busy), not for every
         // lane that finishes: the refill (task-buffer and packet-state loads, walker start) then runs
         // once for several lanes instead of stalling the busy lanes at almost every crossing. The
         // best count depends on the cost of a crossing (measured: 16 for the Cartesian grid and the
-        // octree, 8 for tetrahedra and Voronoi cells).
-        if (need && (__popc(need) >= Walker::kRefillMin || __ballot_sync(FULL, kind >= 0) == 0))
+        // octree, 8 for tetrahedra and Voronoi cells): Walker::kRefillMin, unless the launch shape
+        // sets it (skgpu_set_trace_refill).
+        if (need && (__popc(need) >= refillMin || __ballot_sync(FULL, kind >= 0) == 0))
         {
             int leader = __ffs(need) - 1;
             unsigned base = 0;

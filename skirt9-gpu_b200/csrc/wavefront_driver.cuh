@@ -137,9 +137,10 @@ cudaError_t runWave(const Wave& w, int numSMs, cudaStream_t s, unsigned long lon
     L.shadeBlocks = numSMs * (w.shadeBlocksPerSM > 0 ? w.shadeBlocksPerSM : 4);
     L.guideBlocks = numSMs * 2;
     L.guided = w.sc.guideMode == 2;
-    // the split traversal runs in captured graphs without per-stage timing
+    // the split traversal runs in captured graphs without per-stage timing, for walkers that gain
+    // from it
     L.split = false;
-    if (useGraph && cache && (!timer || timer->level <= 1) && splitTraversal())
+    if (Walker::kSplit && useGraph && cache && (!timer || timer->level <= 1) && splitTraversal())
     {
         if (cache->ensureSplit() == cudaSuccess)
         {
@@ -161,6 +162,7 @@ cudaError_t runWave(const Wave& w, int numSMs, cudaStream_t s, unsigned long lon
         cudaError_t ea = cudaFuncSetAttribute(guideScatterKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, GM_SMEM_BYTES);
         if (ea != cudaSuccess) return ea;
     }
+    if (cache) cache->lastSplit = L.split;
     initPoolKernel<<<L.shadeBlocks, L.threads, 0, s>>>(w);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;

@@ -671,12 +671,16 @@ def build_tetra(points, extent, threads=0, lib=None):
     return out
 
 
-EXPORTED += ["skgpu_set_launch_shape", "skgpu_run_batch"]
+EXPORTED += ["skgpu_set_launch_shape", "skgpu_set_trace_refill", "skgpu_run_batch"]
 
 
 def set_launch_shape(be, pool_slots=0, trace_blocks_per_sm=0, shade_blocks_per_sm=0):
     _guide_call(be, "set_launch_shape", [C.c_int32, C.c_int32, C.c_int32], int(pool_slots), int(trace_blocks_per_sm),
                 int(shade_blocks_per_sm))
+
+
+def set_trace_refill(be, lanes=0):
+    _guide_call(be, "set_trace_refill", [C.c_int32], int(lanes))
 
 
 def run_batch(backends, first, count, total):

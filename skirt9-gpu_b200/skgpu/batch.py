@@ -10,8 +10,10 @@ of its own skgpu_run_primary. There is no reference counterpart; the reference r
 simulations one after another (`skirt` per ski file).
 
 `autotune` picks the launch shape (packet slots in flight, resident traversal blocks per SM, stage
-blocks per SM) that gives the shortest device time for a given run, by coordinate descent over
-the candidates.
+blocks per SM, and the number of waiting lanes at which a traversal warp takes new tasks) that gives
+the shortest device time for a given run, by coordinate descent over the candidates.
+`tuned_shape` runs it once per grid kind and keeps the result: later calls for a scene of the same
+grid kind set the stored shape on the backend without tuning again.
 """
 from . import abi
 
@@ -37,7 +39,18 @@ DEFAULT_CANDIDATES = {
     "pool_slots": [1 << 20, 1 << 21, 1 << 22],
     "trace_blocks_per_sm": [1, 2, 3, 4, 6, 8],
     "shade_blocks_per_sm": [2, 4, 8, 16],
+    "trace_refill": [4, 8, 12, 16, 24],
 }
+
+KNOBS = ("pool_slots", "trace_blocks_per_sm", "shade_blocks_per_sm", "trace_refill")
+
+
+def apply_shape(be, shape):
+    """Sets a launch shape (dict of KNOBS; missing or 0 entries keep the defaults) on a backend."""
+    abi.set_launch_shape(be, shape.get("pool_slots", 0), shape.get("trace_blocks_per_sm", 0),
+                         shape.get("shade_blocks_per_sm", 0))
+    abi.set_trace_refill(be, shape.get("trace_refill", 0))
+    be.launch_shape = dict(shape)
 
 
 def autotune(be, run, candidates=None, repeats=1, rounds=2):
@@ -46,11 +59,11 @@ def autotune(be, run, candidates=None, repeats=1, rounds=2):
     (skgpu_last_run_ms after `run()`) kept; `rounds` sweeps. Leaves the best shape set and returns
     (shape dict, best ms, trials list)."""
     cand = dict(DEFAULT_CANDIDATES if candidates is None else candidates)
-    shape = {"pool_slots": 0, "trace_blocks_per_sm": 0, "shade_blocks_per_sm": 0}
+    shape = {k: 0 for k in KNOBS}
     trials = []
 
     def measure(s):
-        abi.set_launch_shape(be, s["pool_slots"], s["trace_blocks_per_sm"], s["shade_blocks_per_sm"])
+        apply_shape(be, s)
         ms = min(_timed(be, run) for _ in range(max(1, repeats)))
         trials.append((dict(s), ms))
         return ms
@@ -69,8 +82,23 @@ def autotune(be, run, candidates=None, repeats=1, rounds=2):
                     best, shape, changed = ms, trial, True
         if not changed:
             break
-    abi.set_launch_shape(be, shape["pool_slots"], shape["trace_blocks_per_sm"], shape["shade_blocks_per_sm"])
+    apply_shape(be, shape)
     return shape, best, trials
+
+
+_TUNED = {}  # grid kind -> launch shape found by autotune
+
+
+def tuned_shape(be, grid_kind, run, candidates=None, repeats=1, rounds=2):
+    """The launch shape for scenes of `grid_kind`: tuned by `autotune` with `run` the first time a
+    grid kind is seen in this process, then reused. Sets it on the backend and returns
+    (shape, tuned now)."""
+    if grid_kind in _TUNED:
+        apply_shape(be, _TUNED[grid_kind])
+        return _TUNED[grid_kind], False
+    shape, _, _ = autotune(be, run, candidates, repeats, rounds)
+    _TUNED[grid_kind] = shape
+    return shape, True
 
 
 def _timed(be, run):

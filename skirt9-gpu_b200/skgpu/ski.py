@@ -37,10 +37,11 @@ def octree_grid(half_size, unit, max_level, max_dust_fraction, min_level=2):
             f'</PolicyTreeSpatialGrid>')
 
 
-def voronoi_grid(half_size, unit, num_sites, policy="DustDensity"):
+def voronoi_grid(half_size, unit, num_sites, policy="DustDensity", filename=None):
     h = half_size
+    f = f' filename="{filename}"' if filename else ""
     return (f'<VoronoiMeshSpatialGrid minX="{-h} {unit}" maxX="{h} {unit}" minY="{-h} {unit}" maxY="{h} {unit}" '
-            f'minZ="{-h} {unit}" maxZ="{h} {unit}" policy="{policy}" numSites="{num_sites}" relaxSites="false"/>')
+            f'minZ="{-h} {unit}" maxZ="{h} {unit}" policy="{policy}" numSites="{num_sites}"{f} relaxSites="false"/>')
 
 
 def tetra_grid(half_size, unit, num_samples, policy="DustDensity", filename=None):
@@ -336,9 +337,11 @@ def dust_galaxy(num_packets=1e5, npix=32, nlambda=20, num_em=30, max_level=6, ma
 
 
 def galaxy_voronoi(num_packets=1e8, npix=512, nlambda=100, num_sites=1_000_000, tau_v=2.0, half_size_kpc=25,
-                   store_rf=True):
-    """The galaxy of galaxy_octree on a VoronoiMeshSpatialGrid whose sites the reference draws from
-    the dust density (1e6 sites), face-on tau_V = 2, two frames at 0 and 90 degrees."""
+                   store_rf=True, sites_file=None):
+    """The galaxy of galaxy_octree on a VoronoiMeshSpatialGrid with 1e6 sites, face-on tau_V = 2, two
+    frames at 0 and 90 degrees. With `sites_file` the reference reads the site positions from that
+    text column file (policy File, e.g. the seeded sites of skgpu.workloads.disk_sites written by
+    vertex_file_text); otherwise it draws them from the dust density itself."""
     lam = [0.1 * (100.0 ** (i / (nlambda - 1))) for i in range(nlambda)]
     kappa = [(l / 0.55) ** -1.0 for l in lam]
     albedo = [min(0.9, max(0.05, 0.5 * (l / 0.55) ** -0.2)) for l in lam]
@@ -351,7 +354,7 @@ def galaxy_voronoi(num_packets=1e8, npix=512, nlambda=100, num_sites=1_000_000, 
     fov = 2 * half_size_kpc
     instruments = "".join(frame_instrument(f"i{inc}", inc, fov, "kpc", npix, stats=False) for inc in (0, 90))
     return simulation("ExtinctionOnly", num_packets, sources, expdisk_medium(6, 0.2, "kpc", tau_v, mix),
-                      voronoi_grid(half_size_kpc, "kpc", num_sites), instruments,
+                      voronoi_grid(half_size_kpc, "kpc", num_sites, "File" if sites_file else "DustDensity", sites_file), instruments,
                       instrument_wlg=wlg, store_rf=store_rf, rf_wlg=wlg)
 
 

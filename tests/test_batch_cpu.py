@@ -39,8 +39,9 @@ def test_batch_symbols_exported():
 def test_autotune_descends_to_the_fastest_shape(monkeypatch):
     """The coordinate descent of skgpu.batch.autotune on a fake timing model: it visits every
     candidate of each knob with the others fixed, keeps the fastest, and leaves that shape set."""
-    state = {"shape": (0, 0, 0)}
+    state = {"shape": (0, 0, 0), "refill": 0}
     monkeypatch.setattr(abi, "set_launch_shape", lambda be, p, t, s: state.update(shape=(p, t, s)))
+    monkeypatch.setattr(abi, "set_trace_refill", lambda be, r: state.update(refill=r))
 
     class Fake:
         def last_run_ms(self):
@@ -49,12 +50,24 @@ def test_autotune_descends_to_the_fastest_shape(monkeypatch):
             cost -= {0: 0, 1 << 20: 5, 1 << 21: 8, 1 << 22: 10}[p]
             cost -= {0: 0, 1: -20, 2: 3, 3: 1}[t]
             cost -= {0: 0, 2: 1, 4: 2, 8: -1}[s]
+            cost -= {0: 0, 8: 4, 16: 1}[state["refill"]]
             return cost
 
     be = Fake()
-    cand = {"pool_slots": [1 << 20, 1 << 21, 1 << 22], "trace_blocks_per_sm": [1, 2, 3], "shade_blocks_per_sm": [2, 4, 8]}
+    cand = {"pool_slots": [1 << 20, 1 << 21, 1 << 22], "trace_blocks_per_sm": [1, 2, 3], "shade_blocks_per_sm": [2, 4, 8],
+            "trace_refill": [8, 16]}
     shape, ms, trials = batch.autotune(be, lambda: None, cand, rounds=2)
-    assert shape == {"pool_slots": 1 << 22, "trace_blocks_per_sm": 2, "shade_blocks_per_sm": 4}
-    assert ms == 100.0 - 10 - 3 - 2
-    assert state["shape"] == (1 << 22, 2, 4)
-    assert len(trials) >= 1 + 3 + 3 + 3
+    assert shape == {"pool_slots": 1 << 22, "trace_blocks_per_sm": 2, "shade_blocks_per_sm": 4, "trace_refill": 8}
+    assert ms == 100.0 - 10 - 3 - 2 - 4
+    assert state["shape"] == (1 << 22, 2, 4) and state["refill"] == 8
+    assert be.launch_shape == shape
+    assert len(trials) >= 1 + 3 + 3 + 3 + 2
+
+    # tuned once per grid kind, then reused without new trials
+    batch._TUNED.clear()
+    calls = []
+    first, tuned = batch.tuned_shape(be, 3, lambda: calls.append(1), cand)
+    n = len(calls)
+    again, tuned2 = batch.tuned_shape(be, 3, lambda: calls.append(1), cand)
+    assert tuned and not tuned2 and again == first and len(calls) == n
+    batch._TUNED.clear()

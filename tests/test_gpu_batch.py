@@ -93,8 +93,8 @@ def test_autotune_keeps_results_and_returns_a_shape():
         ref = sc.run(be, 40000, seed=3, precision=abi.PREC_FP32)
         run = lambda: sc.run(be, 40000, seed=3, precision=abi.PREC_FP32)
         shape, ms, trials = batch.autotune(be, run, {"pool_slots": [1 << 14, 1 << 16], "trace_blocks_per_sm": [1, 2],
-                                                     "shade_blocks_per_sm": [2, 8]}, rounds=1)
-        assert ms > 0 and len(trials) >= 4 and set(shape) == {"pool_slots", "trace_blocks_per_sm", "shade_blocks_per_sm"}
+                                                     "shade_blocks_per_sm": [2, 8], "trace_refill": [4, 24]}, rounds=1)
+        assert ms > 0 and len(trials) >= 5 and set(shape) == set(batch.KNOBS)
         _assert_same(ref, sc.run(be, 40000, seed=3, precision=abi.PREC_FP32))
     finally:
         be.close()

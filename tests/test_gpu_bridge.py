@@ -70,8 +70,9 @@ def frame_z(da, db, name, instr):
 
 
 def both(tmp_path, text, name):
-    # the reference runs single-threaded: its multi-threaded runs scatter the direct (unscattered)
-    # flux of a point source between runs by several per cent, beyond their own statistics
+    # the reference runs single-threaded: its multi-threaded runs sample the cell densities from
+    # randomly seeded threads, so their medium differs from run to run (and from the bridge's, which
+    # takes the densities of its own single-threaded setup)
     log = run(SKIRT_GPU, text, name, str(tmp_path / "gpu"), ["-g", "-t", "1"])
     run(SKIRT, text, name, str(tmp_path / "cpu"), ["-t", "1"])
     assert "B200 photon-packet life cycle" in log
@@ -81,8 +82,7 @@ def both(tmp_path, text, name):
 
 def check(z, chi2_max, zmax):
     """Mean square z below chi2_max; the 99.9th percentile of |z| below zmax (frame pixels see rare
-    high-weight contributions: two reference runs with different seeds reach |z| ~ 10 in a few of
-    ~2e4 pixels)."""
+    high-weight contributions, so the largest |z| of ~2e4 pixels is not a good test)."""
     assert len(z) > 0
     assert (z ** 2).mean() < chi2_max, (z ** 2).mean()
     assert np.quantile(np.abs(z), 0.999) < zmax, np.quantile(np.abs(z), 0.999)
@@ -120,17 +120,12 @@ def test_bridge_dust_emission(tmp_path):
     text = ski.dust_shell(200000)
     log, g, c = both(tmp_path, text, "dust")
     assert "secondary histories on the B200" in log
-    # This SED varies between reference runs more than its per-history statistics say (four runs of
-    # the reference with different seeds spread by 2-4 % rms in the 0.2-5 micron bins against 0.7-1.2 %
-    # relative errors, by ~1 % in the dust-emission bins; the secondary segment also inherits the noise
-    # of the primary radiation field): per-bin agreement within that spread, and the integrated dust
-    # emission
+    # the secondary emission also inherits the noise of the primary segment's radiation field, which
+    # the per-history statistics do not include: a little more room for the mean square z
     z, (a, b) = sed_z(g, c, "dust", "sed")
-    fa, ra = a
-    fb, rb = b
-    m = (fa > 0) & (fb > 0) & (ra < 0.05) & (rb < 0.05)
-    assert m.sum() > 15
-    assert np.all(np.abs(fa[m] / fb[m] - 1) < np.maximum(5 * np.hypot(ra[m], rb[m]), 0.12))
+    assert len(z) > 25
+    check(z, 2.0, 5.0)
+    fa, fb = a[0], b[0]
     ir = np.loadtxt(os.path.join(g, "dust_sed_sed.dat"))[:, 0] > 20
     assert fa[ir].sum() == pytest.approx(fb[ir].sum(), rel=0.03)  # the dust emission itself
     z, _ = frame_z(g, c, "dust", "i30")

@@ -171,26 +171,22 @@ def test_gpu_production_paths_equal_reference(golden, gpu_backend, name):
 
 @pytest.mark.parametrize("name", ["voronoi", "tetra"])
 def test_gpu_fp32_paths_close_to_reference(golden, gpu_backend, name):
-    """FP32-distance walkers: cell sequences equal the reference's except for rays grazing a cell
-    edge; segment lengths within 1e-5 of the path length; optical depths within 1e-5."""
+    """Voronoi and tetrahedral production walkers (FP32 face distances with FP64 re-decisions of near
+    ties): cell sequences equal the reference's on every golden ray; segment lengths within 1e-5 of
+    the path length; optical depths within 1e-5."""
     z = golden(f"paths_{name}.npz")
     sc = Scene.from_export(z)
     sc.upload(gpu_backend)
     count, m, ds = gpu_backend.trace_paths(z["rays"], 512, precision=abi.PREC_FP32)
     off = z["ray_offset"]
-    same = 0
     for r in range(len(count)):
         rm, rds = z["ray_m"][off[r]:off[r + 1]], z["ray_ds"][off[r]:off[r + 1]]
-        if count[r] == len(rm) and np.array_equal(m[r, :count[r]], rm):
-            same += 1
-            if count[r] > 0:
-                scale = max(np.abs(rds).sum(), 1e-300)
-                assert np.abs(ds[r, :count[r]] - rds).max() <= 1e-5 * scale
-    assert same >= 0.98 * len(count)
+        assert count[r] == len(rm) and np.array_equal(m[r, :count[r]], rm), r
+        if count[r] > 0:
+            scale = max(np.abs(rds).sum(), 1e-300)
+            assert np.abs(ds[r, :count[r]] - rds).max() <= 1e-5 * scale, r
     tau = gpu_backend.optical_depths(z["rays"], 0.55e-6, precision=abi.PREC_FP32)
-    ref = z["ray_tau"]
-    ok = np.isclose(tau, ref, rtol=1e-5, atol=1e-9)
-    assert ok.mean() >= 0.98
+    assert np.allclose(tau, z["ray_tau"], rtol=1e-5, atol=1e-9)
 
 
 def test_gpu_statistics_exact_beyond_the_slot_buffer(golden, gpu_backend, oracle_backend):

@@ -47,7 +47,9 @@ def test_stage_timing_level_one_times_trace_only(golden, gpu_backend):
     finally:
         abi.set_stage_timing(gpu_backend, 0)
     assert list(stages) == ["trace"]
-    assert stages["trace"][1] == (res.counters["kernel_launches"] - 1) // 7
+    # one traversal stage per pass; a pass is 8 kernels with the split traversal of the captured graph
+    passes = stages["trace"][1]
+    assert res.counters["kernel_launches"] - 1 in (7 * passes, 8 * passes)
     with pytest.raises(abi.SkgpuError):
         abi.set_stage_timing(gpu_backend, 3)
 
