@@ -224,6 +224,23 @@ int skgpu_upload_sources(skgpu_ctx* ctx, int32_t num_sources, const skgpu_source
 /* ---- instruments ---- */
 int skgpu_upload_instruments(skgpu_ctx* ctx, int32_t num_instruments, const skgpu_instrument* instruments,
                              int32_t wlg_len, const double* wlg_borders, const int32_t* wlg_ellv);
+/* Scattering levels of an instrument that records components (Instrument::numScatteringLevels,
+ * FluxRecorder::setUserFlags, FluxRecorder.cpp:162-170): the flux of primary packets scattered
+ * n = 1..levels times also goes to level plane n-1 (the PrimaryScatteredLevel arrays,
+ * FluxRecorder.cpp:430-433); secondary packets record no levels. Call after skgpu_upload_instruments;
+ * clears the instrument's component planes. levels 0 removes them. */
+int skgpu_set_instrument_scattering_levels(skgpu_ctx* ctx, int32_t instrument, int32_t levels);
+/* Band wavelength grid of an instrument (BandWavelengthGrid, BandWavelengthGrid.cpp): bin ell is band
+ * ell in pivot-wavelength order; a packet of wavelength lambda is recorded in every band whose table
+ * range [lambda_0, lambda_last] holds lambda, with luminosity times Band::transmission(lambda)
+ * (Band.cpp: linear interpolation of the normalised transmission table times the effective width),
+ * as FluxRecorder::detect loops over WavelengthGrid::bins (FluxRecorder.cpp:380-384). band_sizes[b]
+ * table points of band b follow one another in lambda and transmission (the normalised
+ * TabulatedBand values, increasing wavelengths); width[b] = Band::effectiveWidth().
+ * num_bands must equal the instrument's num_wavelength_bins; replaces its disjoint grid. Call after
+ * skgpu_upload_instruments. */
+int skgpu_set_instrument_bands(skgpu_ctx* ctx, int32_t instrument, int32_t num_bands, const int32_t* band_sizes,
+                               const double* lambda, const double* transmission, const double* width);
 
 /* ---- run ---- */
 int skgpu_set_options(skgpu_ctx* ctx, const skgpu_options* options);
@@ -357,6 +374,9 @@ int skgpu_fetch_instrument(skgpu_ctx* ctx, int32_t instrument, double* ifu, doub
 /* Adds the component planes (transparent, direct, scattered) of an instrument with
  * record_components set: ifu3 holds 3 planes of ifu size, sed3 3 planes of sed size (either may be NULL). */
 int skgpu_fetch_instrument_components(skgpu_ctx* ctx, int32_t instrument, double* ifu3, double* sed3);
+/* Adds the scattering-level planes of an instrument (skgpu_set_instrument_scattering_levels): levels
+ * planes of ifu size or of sed size, plane n-1 for n scatterings. */
+int skgpu_fetch_instrument_levels(skgpu_ctx* ctx, int32_t instrument, double* ifu_levels, double* sed_levels);
 /* Adds the radiation-field tally (num_cells * num_rf_bins, index m*num_rf_bins + ell) into rf. */
 int skgpu_fetch_radiation_field(skgpu_ctx* ctx, double* rf);
 int skgpu_clear_tallies(skgpu_ctx* ctx);

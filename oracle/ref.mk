@@ -181,7 +181,8 @@ bridge: $(BIN)/skirt_gpu
 BRIDGE_FNS := create destroy last_error abi_version device_count upload_grid_cartesian upload_grid_sphere1d \
     upload_grid_octree upload_medium upload_dust_mix upload_rf_grid upload_instruments upload_sources set_options \
     clear_tallies run_primary fetch_instrument fetch_instrument_components fetch_radiation_field \
-    upload_dust_emission upload_radiation_field prepare_secondary run_secondary
+    upload_dust_emission upload_radiation_field prepare_secondary run_secondary \
+    set_instrument_scattering_levels set_instrument_bands fetch_instrument_levels
 BRIDGE_ORACLE_DEFS := $(foreach f,$(BRIDGE_FNS),-Dskgpu_$(f)=or_$(f)) -Dskgpu_ctx=or_ctx -include $(HERE)/skoracle.h
 
 $(OBJ)/bridge/SkgpuLifeCycle_oracle.o: $(BRIDGE)/SkgpuLifeCycle.cpp $(BRIDGE)/SkgpuLifeCycle.hpp $(HERE)/skoracle.h

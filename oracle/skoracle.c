@@ -137,6 +137,10 @@ typedef struct
     skgpu_instrument d;
     double *ifu, *sed, *comp, *stats;
     size_t n;
+    int levels;                     /* scattering-level planes after the 3 component planes */
+    int nband;                      /* > 0: band wavelength grid */
+    int* bandBeg;                   /* nband + 1 table offsets */
+    double *bandLam, *bandTr, *bandW;
 } Instr;
 
 struct or_ctx
@@ -208,6 +212,7 @@ static void free_instruments(or_ctx* c)
     for (int i = 0; i < c->ninstr; ++i)
     {
         free(c->instr[i].ifu); free(c->instr[i].sed); free(c->instr[i].comp); free(c->instr[i].stats);
+        free(c->instr[i].bandBeg); free(c->instr[i].bandLam); free(c->instr[i].bandTr); free(c->instr[i].bandW);
     }
     free(c->instr);
     c->instr = NULL;
@@ -1690,6 +1695,46 @@ int or_upload_instruments(or_ctx* c, int32_t num_instruments, const skgpu_instru
     return SKGPU_OK;
 }
 
+/* Instrument::numScatteringLevels with recordComponents (FluxRecorder.cpp:270-292) */
+int or_set_instrument_scattering_levels(or_ctx* c, int32_t i, int32_t levels)
+{
+    if (i < 0 || i >= c->ninstr) return fail(c, SKGPU_ERR_ARG, "levels: bad instrument index");
+    Instr* in = &c->instr[i];
+    if (!in->comp) return fail(c, SKGPU_ERR_STATE, "levels: instrument does not record components");
+    if (levels < 0 || levels > 1000) return fail(c, SKGPU_ERR_ARG, "levels: out of range [0, 1000]");
+    free(in->comp);
+    in->comp = (double*)calloc((size_t)(3 + levels) * in->n, sizeof(double));
+    in->levels = levels;
+    return SKGPU_OK;
+}
+
+/* BandWavelengthGrid with the bands' TabulatedBand tables (BandWavelengthGrid.cpp, Band.cpp) */
+int or_set_instrument_bands(or_ctx* c, int32_t i, int32_t num_bands, const int32_t* sizes, const double* lambda,
+                            const double* transmission, const double* width)
+{
+    if (i < 0 || i >= c->ninstr) return fail(c, SKGPU_ERR_ARG, "bands: bad instrument index");
+    Instr* in = &c->instr[i];
+    if (num_bands != in->d.num_wavelength_bins) return fail(c, SKGPU_ERR_ARG, "bands: count differs from the instrument's wavelength bins");
+    if (!sizes || !lambda || !transmission || !width) return fail(c, SKGPU_ERR_ARG, "bands: missing tables");
+    int* beg = (int*)calloc((size_t)num_bands + 1, sizeof(int));
+    for (int b = 0; b < num_bands; ++b)
+    {
+        if (sizes[b] < 2 || !(width[b] > 0))
+        {
+            free(beg);
+            return fail(c, SKGPU_ERR_ARG, "bands: bad table");
+        }
+        beg[b + 1] = beg[b] + sizes[b];
+    }
+    free(in->bandBeg); free(in->bandLam); free(in->bandTr); free(in->bandW);
+    in->bandBeg = beg;
+    in->bandLam = (double*)dup(lambda, (size_t)beg[num_bands] * sizeof(double));
+    in->bandTr = (double*)dup(transmission, (size_t)beg[num_bands] * sizeof(double));
+    in->bandW = (double*)dup(width, (size_t)num_bands * sizeof(double));
+    in->nband = num_bands;
+    return SKGPU_OK;
+}
+
 int or_set_options(or_ctx* c, const skgpu_options* o)
 {
     c->opt = *o;
@@ -1740,6 +1785,16 @@ static int upper_bound(const double* xv, int n, double x)
 }
 
 static int wlg_bin(const double* b, int nb, const int* ellv, double lambda) { return ellv[upper_bound(b, nb, lambda)]; }
+
+/* Band::transmission (Band.cpp): NR::interpolateLinLin (NR.hpp:328-331) in the normalised table,
+   zero outside it, times the effective width */
+static double band_transmission(const double* lv, const double* tv, int size, double width, double lambda)
+{
+    int index = upper_bound(lv, size, lambda);
+    if (index == 0 || index >= size) return 0.;
+    double T = tv[index - 1] + ((lambda - lv[index - 1]) / (lv[index] - lv[index - 1])) * (tv[index] - tv[index - 1]);
+    return T * width;
+}
 
 /* SpecialFunctions::gexp */
 static double gexp(double p, double x)
@@ -1947,30 +2002,53 @@ static void peel_off(or_ctx* c, Packet* pk, int scattering)
         }
         int l = in->d.kind == SKGPU_INSTR_FRAME ? frame_pixel(&in->d, pk) : -1;
         if (in->d.kind == SKGPU_INSTR_FRAME && l < 0) continue;
-        int ell = wlg_bin(c->wlgB + in->d.wlg_offset, in->d.wlg_num_borders, c->wlgEll + in->d.wlg_offset, pk->lambda);
-        if (ell < 0) continue;
-        if (!tauKnown)
+        /* WavelengthGrid::bins and ::transmission: one disjoint bin with transmission 1, or every band
+           whose table range holds the wavelength (FluxRecorder.cpp:380-384) */
+        int nb = in->nband ? in->nband : 1;
+        for (int b = 0; b < nb; ++b)
         {
-            tau = observed_tau(c, pk, kobs, Lp);
-            tauKnown = 1;
-        }
-        double Lext = Lp * exp(-tau);
-        c->cnt.peel_detections++;
-        size_t idx = in->d.kind == SKGPU_INSTR_FRAME ? (size_t)l + (size_t)ell * in->d.num_pixels_x * in->d.num_pixels_y
-                                                     : (size_t)ell;
-        double* total = in->d.kind == SKGPU_INSTR_FRAME ? in->ifu : in->sed;
-        total[idx] += Lext;
-        if (in->d.record_components)
-        {
-            if (numScatt == 0)
+            int ell;
+            double L = Lp;
+            if (!in->nband)
             {
-                in->comp[idx] += Lp;
-                in->comp[in->n + idx] += Lext;
+                ell = wlg_bin(c->wlgB + in->d.wlg_offset, in->d.wlg_num_borders, c->wlgEll + in->d.wlg_offset, pk->lambda);
+                if (ell < 0) continue;
             }
             else
-                in->comp[2 * in->n + idx] += Lext;
+            {
+                ell = b;
+                const double* lv = in->bandLam + in->bandBeg[b];
+                int size = in->bandBeg[b + 1] - in->bandBeg[b];
+                if (!(pk->lambda >= lv[0] && pk->lambda <= lv[size - 1])) continue;
+                L = Lp * band_transmission(lv, in->bandTr + in->bandBeg[b], size, in->bandW[b], pk->lambda);
+            }
+            if (!tauKnown)
+            {
+                tau = observed_tau(c, pk, kobs, Lp);
+                tauKnown = 1;
+            }
+            double Lext = L * exp(-tau);
+            c->cnt.peel_detections++;
+            size_t idx = in->d.kind == SKGPU_INSTR_FRAME ? (size_t)l + (size_t)ell * in->d.num_pixels_x * in->d.num_pixels_y
+                                                         : (size_t)ell;
+            double* total = in->d.kind == SKGPU_INSTR_FRAME ? in->ifu : in->sed;
+            total[idx] += Lext;
+            if (in->d.record_components)
+            {
+                if (numScatt == 0)
+                {
+                    in->comp[idx] += L;
+                    in->comp[in->n + idx] += Lext;
+                }
+                else
+                {
+                    in->comp[2 * in->n + idx] += Lext;
+                    /* PrimaryScatteredLevel + numScatt - 1, primary packets only (FluxRecorder.cpp:430-433) */
+                    if (numScatt <= in->levels && !c->secRun) in->comp[(size_t)(2 + numScatt) * in->n + idx] += Lext;
+                }
+            }
+            if (in->d.record_statistics) add_contrib(pk, i, ell, l, Lext);
         }
-        if (in->d.record_statistics) add_contrib(pk, i, ell, l, Lext);
     }
 }
 
@@ -2764,6 +2842,15 @@ int or_fetch_instrument_components(or_ctx* c, int32_t i, double* ifu3, double* s
     return SKGPU_OK;
 }
 
+int or_fetch_instrument_levels(or_ctx* c, int32_t i, double* ifu_levels, double* sed_levels)
+{
+    if (i < 0 || i >= c->ninstr) return fail(c, SKGPU_ERR_ARG, "fetch: bad instrument index");
+    Instr* in = &c->instr[i];
+    if (!in->comp || in->levels < 1) return fail(c, SKGPU_ERR_STATE, "fetch: instrument records no scattering levels");
+    add_into(in->comp + 3 * in->n, (size_t)in->levels * in->n, in->d.kind == SKGPU_INSTR_FRAME ? ifu_levels : sed_levels);
+    return SKGPU_OK;
+}
+
 int or_fetch_radiation_field(or_ctx* c, double* rf)
 {
     if (!c->rf) return fail(c, SKGPU_ERR_STATE, "fetch: no radiation field recorded");
@@ -2778,7 +2865,7 @@ int or_clear_tallies(or_ctx* c)
         Instr* in = &c->instr[i];
         if (in->ifu) memset(in->ifu, 0, in->n * sizeof(double));
         if (in->sed) memset(in->sed, 0, in->n * sizeof(double));
-        if (in->comp) memset(in->comp, 0, 3 * in->n * sizeof(double));
+        if (in->comp) memset(in->comp, 0, (size_t)(3 + in->levels) * in->n * sizeof(double));
         if (in->stats) memset(in->stats, 0, 5 * in->n * sizeof(double));
     }
     if (c->rf) memset(c->rf, 0, c->rfLen * sizeof(double));

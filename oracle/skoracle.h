@@ -61,6 +61,9 @@ int or_upload_sources(or_ctx* ctx, int32_t num_sources, const skgpu_source* sour
                       const double* radial_r, const double* radial_P);
 int or_upload_instruments(or_ctx* ctx, int32_t num_instruments, const skgpu_instrument* instruments, int32_t wlg_len,
                           const double* wlg_borders, const int32_t* wlg_ellv);
+int or_set_instrument_scattering_levels(or_ctx* ctx, int32_t instrument, int32_t levels);
+int or_set_instrument_bands(or_ctx* ctx, int32_t instrument, int32_t num_bands, const int32_t* band_sizes,
+                            const double* lambda, const double* transmission, const double* width);
 int or_set_options(or_ctx* ctx, const skgpu_options* options);
 int or_run_primary(or_ctx* ctx, uint64_t first, uint64_t count, uint64_t total_packets);
 int or_probe_launch(or_ctx* ctx, uint64_t first, uint64_t count, uint64_t total_packets, double* out);
@@ -78,6 +81,7 @@ int or_run_secondary(or_ctx* ctx, uint64_t first, uint64_t count);
 int or_fetch_instrument(or_ctx* ctx, int32_t instrument, double* ifu, double* sed, double* ifu_stats,
                         double* sed_stats);
 int or_fetch_instrument_components(or_ctx* ctx, int32_t instrument, double* ifu3, double* sed3);
+int or_fetch_instrument_levels(or_ctx* ctx, int32_t instrument, double* ifu_levels, double* sed_levels);
 int or_fetch_radiation_field(or_ctx* ctx, double* rf);
 int or_clear_tallies(or_ctx* ctx);
 int or_get_counters(or_ctx* ctx, skgpu_counters* out);

@@ -32,6 +32,7 @@
 #include "Configuration.hpp"
 #include "ContSED.hpp"
 #include "DefaultWavelengthDistribution.hpp"
+#include "BandWavelengthGrid.hpp"
 #include "DisjointWavelengthGrid.hpp"
 #include "DustMix.hpp"
 #include "EquilibriumDustEmissionCalculator.hpp"
@@ -119,11 +120,13 @@ namespace
         for (Instrument* instr : sim->instrumentSystem()->instruments())
         {
             auto rec = instr->instrumentFluxRecorder();
-            if (rec->_numScatteringLevels > 0 || rec->_recordPolarization) return (why = "instrument options"), false;
+            if (rec->_recordPolarization || rec->_redshift != 0. || rec->_local) return (why = "instrument options"), false;
             auto sed = dynamic_cast<SEDInstrument*>(instr);
             if (!dynamic_cast<FrameInstrument*>(instr) && !sed) return (why = "instrument type"), false;
             if (sed && sed->radius() > 0) return (why = "SED aperture"), false;
-            if (!dynamic_cast<const DisjointWavelengthGrid*>(rec->_lambdagrid)) return (why = "instrument grid"), false;
+            if (!dynamic_cast<const DisjointWavelengthGrid*>(rec->_lambdagrid)
+                && !dynamic_cast<const BandWavelengthGrid*>(rec->_lambdagrid))
+                return (why = "instrument grid"), false;
         }
         if (!secondary)
         {
@@ -248,9 +251,9 @@ namespace
             d.record_statistics = rec->_recordStatistics ? 1 : 0;
             d.record_components = rec->_recordTotalOnly ? 0 : 1;
             d.num_wavelength_bins = rec->_lambdagrid->numBins();
-            std::vector<double> b;
-            std::vector<int32_t> e;
-            uploadWLG(rec->_lambdagrid, b, e);
+            std::vector<double> b{0.};
+            std::vector<int32_t> e{-1, -1};  // band grids: no disjoint bin (skgpu_set_instrument_bands below)
+            if (!dynamic_cast<const BandWavelengthGrid*>(rec->_lambdagrid)) uploadWLG(rec->_lambdagrid, b, e);
             d.wlg_offset = ellv.size();
             d.wlg_num_borders = b.size();
             borders.insert(borders.end(), b.begin(), b.end());
@@ -274,6 +277,32 @@ namespace
         }
         check(skgpu_upload_instruments(g_ctx, v.size(), v.data(), ellv.size(), borders.data(), ellv.data()),
               "instruments");
+        int i = 0;
+        for (Instrument* instr : sim->instrumentSystem()->instruments())
+        {
+            auto rec = instr->instrumentFluxRecorder();
+            if (!rec->_recordTotalOnly && rec->_numScatteringLevels > 0)
+                check(skgpu_set_instrument_scattering_levels(g_ctx, i, rec->_numScatteringLevels), "scattering levels");
+            if (auto bg = dynamic_cast<const BandWavelengthGrid*>(rec->_lambdagrid))
+            {
+                // the bands in the grid's (pivot wavelength) order with their normalised tables
+                std::vector<int32_t> sizes;
+                std::vector<double> lambda, trans, width;
+                for (int ell = 0; ell != bg->numBins(); ++ell)
+                {
+                    const Band* band = bg->band(ell);
+                    size_t size = band->transmissionDataSize();
+                    sizes.push_back(static_cast<int32_t>(size));
+                    lambda.insert(lambda.end(), band->transmissionWavelengthData(), band->transmissionWavelengthData() + size);
+                    trans.insert(trans.end(), band->transmissionValueData(), band->transmissionValueData() + size);
+                    width.push_back(band->effectiveWidth());
+                }
+                check(skgpu_set_instrument_bands(g_ctx, i, sizes.size(), sizes.data(), lambda.data(), trans.data(),
+                                                 width.data()),
+                      "instrument bands");
+            }
+            ++i;
+        }
     }
 
     // the sources of SourceSystem after prepareForLaunch(Npp): history ranges, packet luminosities,
@@ -453,6 +482,23 @@ namespace
                     if (arrays[planes[c]].size() != n)
                         throw FATALERROR("B200 life cycle: component arrays missing (secondary emission without medium emission?)");
                     for (size_t q = 0; q != n; ++q) arrays[planes[c]][q] += comp[c * n + q];
+                }
+                // PrimaryScatteredLevel + n - 1 for n = 1..levels, the planes after Total, the six
+                // components and the 21 polarisation planes (FluxRecorder.cpp:31-61); the secondary
+                // segment records none
+                int levels = rec->_numScatteringLevels;
+                if (primary && levels > 0)
+                {
+                    const int PrimaryScatteredLevel = 28;
+                    std::vector<double> lv(static_cast<size_t>(levels) * n, 0.);
+                    check(skgpu_fetch_instrument_levels(g_ctx, i, frame ? lv.data() : nullptr, frame ? nullptr : lv.data()),
+                          "scattering levels");
+                    for (int c = 0; c != levels; ++c)
+                    {
+                        if (arrays[PrimaryScatteredLevel + c].size() != n)
+                            throw FATALERROR("B200 life cycle: scattering-level arrays missing");
+                        for (size_t q = 0; q != n; ++q) arrays[PrimaryScatteredLevel + c][q] += lv[c * n + q];
+                    }
                 }
             }
             ++i;

@@ -52,6 +52,7 @@ struct skgpu_ctx
     InstrDev* instr = nullptr;
     std::vector<void*> instrBufs;
     std::vector<size_t> instrBufLens;  // doubles per instrument buffer
+    std::vector<void*> instrAux;       // band tables of the instruments
     double* wlgB = nullptr;
     int* wlgEll = nullptr;
 

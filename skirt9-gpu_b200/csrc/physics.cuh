@@ -38,6 +38,12 @@ struct InstrDev
     double* sedComp;
     double* ifuStats;   // 5 planes: sum w^k, k = 0..4
     double* sedStats;
+    int levels;             // scattering-level planes after the 3 component planes (primary packets)
+    int nband;              // > 0: band wavelength grid of nband bands in place of the disjoint grid
+    const int* bandBeg;     // nband + 1 offsets into the band tables
+    const double* bandLam;  // band tables: increasing wavelengths
+    const double* bandTr;   // normalised transmissions
+    const double* bandW;    // nband effective widths
 };
 
 // The prepared secondary (dust) emission source of a segment (DustSecondarySource with the
@@ -127,6 +133,16 @@ SKG_D void atomicAddAgg(double* addr, double v)
 SKG_D int wlgBin(const double* borders, int nb, const int* ellv, double lambda)
 {
     return ellv[upperBound(borders, nb, lambda)];
+}
+
+// Band::transmission (SKIRT/core/Band.cpp): NR::interpolateLinLin in the normalised transmission
+// table (zero outside it), scaled to relative transmission by the effective width
+SKG_D double bandTransmission(const double* lv, const double* tv, int size, double width, double lambda)
+{
+    int index = upperBound(lv, size, lambda);
+    if (index == 0 || index >= size) return 0.;
+    double T = tv[index - 1] + ((lambda - lv[index - 1]) / (lv[index] - lv[index - 1])) * (tv[index] - tv[index - 1]);
+    return T * width;
 }
 
 // SpecialFunctions::gexp(p, x) (SKIRT/utils/SpecialFunctions.cpp:822-836), the inverse of the

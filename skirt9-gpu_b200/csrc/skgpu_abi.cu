@@ -101,6 +101,8 @@ int gridUpload(skgpu_ctx* ctx, const T** dst, const T* host, size_t n)
 void freeInstruments(skgpu_ctx* ctx)
 {
     for (void* p : ctx->instrBufs) cudaFree(p);
+    for (void* p : ctx->instrAux) cudaFree(p);
+    ctx->instrAux.clear();
     ctx->instrBufs.clear();
     ctx->instrBufLens.clear();
     ctx->instrHost.clear();
@@ -1143,6 +1145,10 @@ int skgpu_upload_instruments(skgpu_ctx* ctx, int32_t num_instruments, const skgp
         d.ct = s.cos_theta; d.st = s.sin_theta; d.cp = s.cos_phi; d.sp = s.sin_phi; d.co = s.cos_omega; d.so = s.sin_omega;
         d.xpmin = s.xp_min; d.xpsiz = s.xp_size; d.ypmin = s.yp_min; d.ypsiz = s.yp_size;
         d.ifu = d.sed = d.ifuComp = d.sedComp = d.ifuStats = d.sedStats = nullptr;
+        d.levels = 0;
+        d.nband = 0;
+        d.bandBeg = nullptr;
+        d.bandLam = d.bandTr = d.bandW = nullptr;
         size_t n = static_cast<size_t>(d.nbins) * (d.kind == SKGPU_INSTR_FRAME ? static_cast<size_t>(d.npx) * d.npy : 1);
         auto alloc = [&](double** p, size_t cnt) -> int {
             CK(devAlloc(p, cnt));
@@ -1163,6 +1169,77 @@ int skgpu_upload_instruments(skgpu_ctx* ctx, int32_t num_instruments, const skgp
     CK(devUpload(&ctx->wlgB, wlg_borders, wlg_len));
     CK(devUpload<int>(&ctx->wlgEll, wlg_ellv, wlg_len));
     ctx->instrHost = v;
+    return SKGPU_OK;
+}
+
+int skgpu_set_instrument_scattering_levels(skgpu_ctx* ctx, int32_t instrument, int32_t levels)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (instrument < 0 || instrument >= static_cast<int>(ctx->instrHost.size())) return fail(ctx, SKGPU_ERR_ARG, "levels: bad instrument index");
+    InstrDev& d = ctx->instrHost[instrument];
+    if (!d.comps) return fail(ctx, SKGPU_ERR_STATE, "levels: instrument does not record components");
+    if (levels < 0 || levels > 1000) return fail(ctx, SKGPU_ERR_ARG, "levels: out of range [0, 1000]");
+    CK(cudaSetDevice(ctx->device));
+    double*& comp = d.kind == SKGPU_INSTR_FRAME ? d.ifuComp : d.sedComp;
+    size_t n = static_cast<size_t>(d.nbins) * d.npx * d.npy;
+    size_t cnt = static_cast<size_t>(3 + levels) * n;
+    double* p = nullptr;
+    CK(devAlloc(&p, cnt));
+    CK(cudaMemset(p, 0, cnt * sizeof(double)));
+    for (size_t b = 0; b < ctx->instrBufs.size(); ++b)
+        if (ctx->instrBufs[b] == comp)
+        {
+            cudaFree(comp);
+            ctx->instrBufs[b] = p;
+            ctx->instrBufLens[b] = cnt;
+        }
+    comp = p;
+    d.levels = levels;
+    CK(cudaMemcpy(ctx->instr + instrument, &d, sizeof(InstrDev), cudaMemcpyHostToDevice));
+    return SKGPU_OK;
+}
+
+int skgpu_set_instrument_bands(skgpu_ctx* ctx, int32_t instrument, int32_t num_bands, const int32_t* band_sizes,
+                               const double* lambda, const double* transmission, const double* width)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (instrument < 0 || instrument >= static_cast<int>(ctx->instrHost.size())) return fail(ctx, SKGPU_ERR_ARG, "bands: bad instrument index");
+    InstrDev& d = ctx->instrHost[instrument];
+    if (num_bands != d.nbins) return fail(ctx, SKGPU_ERR_ARG, "bands: count differs from the instrument's wavelength bins");
+    if (!band_sizes || !lambda || !transmission || !width) return fail(ctx, SKGPU_ERR_ARG, "bands: missing tables");
+    std::vector<int> beg(static_cast<size_t>(num_bands) + 1, 0);
+    for (int b = 0; b < num_bands; ++b)
+    {
+        if (band_sizes[b] < 2) return fail(ctx, SKGPU_ERR_ARG, "bands: fewer than 2 table points");
+        if (!(std::isfinite(width[b]) && width[b] > 0)) return fail(ctx, SKGPU_ERR_ARG, "bands: bad effective width");
+        beg[b + 1] = beg[b] + band_sizes[b];
+        const double* lv = lambda + beg[b];
+        for (int k = 0; k < band_sizes[b]; ++k)
+        {
+            if (!std::isfinite(lv[k]) || !std::isfinite(transmission[beg[b] + k]))
+                return fail(ctx, SKGPU_ERR_ARG, "bands: non-finite table value");
+            if (k > 0 && lv[k] < lv[k - 1]) return fail(ctx, SKGPU_ERR_ARG, "bands: wavelengths not increasing");
+        }
+        if (!(lv[0] < lv[band_sizes[b] - 1])) return fail(ctx, SKGPU_ERR_ARG, "bands: empty wavelength range");
+    }
+    CK(cudaSetDevice(ctx->device));
+    size_t tot = static_cast<size_t>(beg[num_bands]);
+    int* dBeg = nullptr;
+    double *dLam = nullptr, *dTr = nullptr, *dW = nullptr;
+    CK(devUpload<int>(&dBeg, beg.data(), beg.size()));
+    ctx->instrAux.push_back(dBeg);
+    CK(devUpload(&dLam, lambda, tot));
+    ctx->instrAux.push_back(dLam);
+    CK(devUpload(&dTr, transmission, tot));
+    ctx->instrAux.push_back(dTr);
+    CK(devUpload(&dW, width, static_cast<size_t>(num_bands)));
+    ctx->instrAux.push_back(dW);
+    d.nband = num_bands;
+    d.bandBeg = dBeg;
+    d.bandLam = dLam;
+    d.bandTr = dTr;
+    d.bandW = dW;
+    CK(cudaMemcpy(ctx->instr + instrument, &d, sizeof(InstrDev), cudaMemcpyHostToDevice));
     return SKGPU_OK;
 }
 
@@ -1865,6 +1942,19 @@ int skgpu_fetch_instrument_components(skgpu_ctx* ctx, int32_t instrument, double
     return d.kind == SKGPU_INSTR_FRAME ? addInto(ctx, d.ifuComp, 3 * n, ifu3) : addInto(ctx, d.sedComp, 3 * n, sed3);
 }
 
+int skgpu_fetch_instrument_levels(skgpu_ctx* ctx, int32_t instrument, double* ifu_levels, double* sed_levels)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (instrument < 0 || instrument >= static_cast<int>(ctx->instrHost.size())) return fail(ctx, SKGPU_ERR_ARG, "fetch: bad instrument index");
+    const InstrDev& d = ctx->instrHost[instrument];
+    if (!d.comps || d.levels < 1) return fail(ctx, SKGPU_ERR_STATE, "fetch: instrument records no scattering levels");
+    CK(cudaSetDevice(ctx->device));
+    size_t n = static_cast<size_t>(d.nbins) * d.npx * d.npy;
+    size_t lv = static_cast<size_t>(d.levels) * n;
+    return d.kind == SKGPU_INSTR_FRAME ? addInto(ctx, d.ifuComp + 3 * n, lv, ifu_levels)
+                                       : addInto(ctx, d.sedComp + 3 * n, lv, sed_levels);
+}
+
 // out[m * nbins + ell] = in[ell * cells + m], through 32 x 32 shared-memory tiles (both sides coalesced)
 static __global__ void rfTransposeKernel(const double* __restrict__ in, double* __restrict__ out, int cells, int nbins)
 {
@@ -1932,7 +2022,7 @@ int skgpu_clear_tallies(skgpu_ctx* ctx)
         double* c = d.kind == SKGPU_INSTR_FRAME ? d.ifuComp : d.sedComp;
         double* s = d.kind == SKGPU_INSTR_FRAME ? d.ifuStats : d.sedStats;
         CK(cudaMemsetAsync(t, 0, n * sizeof(double), ctx->stream));
-        if (c) CK(cudaMemsetAsync(c, 0, 3 * n * sizeof(double), ctx->stream));
+        if (c) CK(cudaMemsetAsync(c, 0, (3 + d.levels) * n * sizeof(double), ctx->stream));
         if (s) CK(cudaMemsetAsync(s, 0, 5 * n * sizeof(double), ctx->stream));
     }
     if (ctx->rf) CK(cudaMemsetAsync(ctx->rf, 0, ctx->rfLen * sizeof(double), ctx->stream));

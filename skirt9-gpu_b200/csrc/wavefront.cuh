@@ -515,6 +515,44 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __g
 // shade kernels (one thread per completed task of one kind)
 // ---------------------------------------------------------------------------------------------
 
+// The record lambda of FluxRecorder::detect for one wavelength bin ell of instrument i
+// (FluxRecorder.cpp:412-440 and the statistics at :522-536): total, components, scattering levels
+// of primary packets, per-history statistics, and the guiding pilot's record.
+SKG_D void detectBin(const Wave& w, const Scene& sc, const InstrDev& in, int i, int slot, int l, int ell, int numScatt,
+                     double L, double Lext)
+{
+    if (sc.guideMode == 1 && i == sc.guideTarget)
+    {
+        // pilot records: the history's detected luminosity in the target instrument
+        double wp = (sc.guideImportance && l >= 0) ? static_cast<double>(sc.guideImportance[l]) : 1.0;
+        atomicAdd(w.pk.gD + slot, Lext * wp);
+    }
+    size_t plane = static_cast<size_t>(in.npx) * in.npy * in.nbins;
+    size_t at = in.kind == 0 ? static_cast<size_t>(l) + static_cast<size_t>(ell) * in.npx * in.npy
+                             : static_cast<size_t>(ell);
+    atomicAddAgg((in.kind == 0 ? in.ifu : in.sed) + at, Lext);
+    if (in.comps)
+    {
+        double* c = in.kind == 0 ? in.ifuComp : in.sedComp;
+        if (numScatt == 0)
+        {
+            atomicAddAgg(c + at, L);
+            atomicAddAgg(c + plane + at, Lext);
+        }
+        else
+        {
+            atomicAddAgg(c + 2 * plane + at, Lext);
+            if (numScatt <= in.levels && !sc.sec) atomicAddAgg(c + (2 + numScatt) * plane + at, Lext);
+        }
+    }
+    if (in.stats)
+    {
+        unsigned long long key = (static_cast<unsigned long long>(i) << 48) | (static_cast<unsigned long long>(ell) << 24)
+                                 | static_cast<unsigned long long>(l + 1);
+        recordStat(w, slot, key, Lext);
+    }
+}
+
 // FluxRecorder::detect for the instruments of one observer group (FluxRecorder.cpp:372-538)
 static __global__ void __launch_bounds__(256) shadePeelKernel(const __grid_constant__ Wave w, int cur)
 {
@@ -528,7 +566,7 @@ static __global__ void __launch_bounds__(256) shadePeelKernel(const __grid_const
         int group = b.info[t] & 0xFF;
         int numScatt = b.info[t] >> 8;
         double Lp = b.par[t];
-        double Lext = Lp * exp(-b.tau[t]);
+        double ext = exp(-b.tau[t]);
         double x = b.x[t], y = b.y[t], z = b.z[t];
         double lambda = w.pk.rec[slot].lam;
         for (int i = group; i < sc.ninstr && (i == group || sc.instr[i].same); ++i)
@@ -536,52 +574,26 @@ static __global__ void __launch_bounds__(256) shadePeelKernel(const __grid_const
             const InstrDev& in = sc.instr[i];
             int l = in.kind == 0 ? framePixel(in, x, y, z) : -1;
             if (in.kind == 0 && l < 0) continue;
-            int ell = wlgBin(sc.wlgB + in.woff, in.wnb, sc.wlgEll + in.woff, lambda);
-            if (ell < 0) continue;
-            det++;
-            if (sc.guideMode == 1 && i == sc.guideTarget)
+            if (in.nband == 0)
             {
-                // pilot records: the history's detected luminosity in the target instrument
-                double wp = (sc.guideImportance && l >= 0) ? static_cast<double>(sc.guideImportance[l]) : 1.0;
-                atomicAdd(w.pk.gD + slot, Lext * wp);
-            }
-            if (in.kind == 0)
-            {
-                size_t npix = static_cast<size_t>(in.npx) * in.npy;
-                size_t at = static_cast<size_t>(l) + static_cast<size_t>(ell) * npix;
-                atomicAddAgg(in.ifu + at, Lext);
-                if (in.comps)
-                {
-                    size_t plane = npix * in.nbins;
-                    if (numScatt == 0)
-                    {
-                        atomicAddAgg(in.ifuComp + at, Lp);
-                        atomicAddAgg(in.ifuComp + plane + at, Lext);
-                    }
-                    else
-                        atomicAddAgg(in.ifuComp + 2 * plane + at, Lext);
-                }
+                // DisjointWavelengthGrid::bins: at most one bin, transmission 1
+                int ell = wlgBin(sc.wlgB + in.woff, in.wnb, sc.wlgEll + in.woff, lambda);
+                if (ell < 0) continue;
+                det++;
+                detectBin(w, sc, in, i, slot, l, ell, numScatt, Lp, Lp * ext);
             }
             else
             {
-                atomicAddAgg(in.sed + ell, Lext);
-                if (in.comps)
+                // BandWavelengthGrid::bins: every band whose range holds the wavelength
+                for (int ell = 0; ell < in.nband; ++ell)
                 {
-                    if (numScatt == 0)
-                    {
-                        atomicAddAgg(in.sedComp + ell, Lp);
-                        atomicAddAgg(in.sedComp + in.nbins + ell, Lext);
-                    }
-                    else
-                        atomicAddAgg(in.sedComp + 2 * in.nbins + ell, Lext);
+                    int b0 = in.bandBeg[ell], size = in.bandBeg[ell + 1] - b0;
+                    const double* lv = in.bandLam + b0;
+                    if (!(lambda >= lv[0] && lambda <= lv[size - 1])) continue;
+                    double L = Lp * bandTransmission(lv, in.bandTr + b0, size, in.bandW[ell], lambda);
+                    det++;
+                    detectBin(w, sc, in, i, slot, l, ell, numScatt, L, L * ext);
                 }
-            }
-            if (in.stats)
-            {
-                unsigned long long key = (static_cast<unsigned long long>(i) << 48)
-                                         | (static_cast<unsigned long long>(ell) << 24)
-                                         | static_cast<unsigned long long>(l + 1);
-                recordStat(w, slot, key, Lext);
             }
         }
     }

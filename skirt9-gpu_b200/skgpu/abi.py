@@ -135,11 +135,14 @@ SIGNATURES = {
     "upload_rf_grid": [_P, _I, _I, _P, _P],
     "upload_sources": [_P, _I, _P, _I, _P, _P, _P, _I, _P, _P],
     "upload_instruments": [_P, _I, _P, _I, _P, _P],
+    "set_instrument_scattering_levels": [_P, _I, _I],
+    "set_instrument_bands": [_P, _I, _I, _P, _P, _P, _P],
     "set_options": [_P, _P],
     "run_primary": [_P, _U, _U, _U],
     "probe_launch": [_P, _U, _U, _U, _P],
     "fetch_instrument": [_P, _I, _P, _P, _P, _P],
     "fetch_instrument_components": [_P, _I, _P, _P],
+    "fetch_instrument_levels": [_P, _I, _P, _P],
     "fetch_radiation_field": [_P, _P],
     "clear_tallies": [_P],
     "get_counters": [_P, _P],
@@ -286,6 +289,17 @@ class Backend:
         b, e = f64(wlg_borders), i32(wlg_ellv)
         self.call("upload_instruments", len(instruments), C.cast(arr, C.c_void_p), len(e), _ptr(b), _ptr(e))
 
+    def set_instrument_scattering_levels(self, i, levels):
+        self.call("set_instrument_scattering_levels", int(i), int(levels))
+
+    def set_instrument_bands(self, i, bands):
+        """bands: list of (wavelengths, normalised transmissions, effective width), in bin order."""
+        sizes = i32([len(b[0]) for b in bands])
+        lam = f64(np.concatenate([np.asarray(b[0], dtype=np.float64) for b in bands]))
+        tr = f64(np.concatenate([np.asarray(b[1], dtype=np.float64) for b in bands]))
+        wd = f64([b[2] for b in bands])
+        self.call("set_instrument_bands", int(i), len(bands), _ptr(sizes), _ptr(lam), _ptr(tr), _ptr(wd))
+
     def set_options(self, opt):
         self.call("set_options", C.cast(C.pointer(opt), C.c_void_p))
 
@@ -319,6 +333,11 @@ class Backend:
         comp = self._into(out, 3 * n)
         self.call("fetch_instrument_components", i, _ptr(comp), _ptr(comp))
         return comp.reshape(3, n)
+
+    def fetch_instrument_levels(self, i, n, levels, out=None):
+        lv = self._into(out, levels * n)
+        self.call("fetch_instrument_levels", i, _ptr(lv), _ptr(lv))
+        return lv.reshape(levels, n)
 
     def fetch_radiation_field(self, n, out=None):
         rf = self._into(out, n)

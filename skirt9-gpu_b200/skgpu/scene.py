@@ -13,6 +13,43 @@ import numpy as np
 from . import abi
 
 
+def list_bands(bands, unit=1e-6):
+    """Band tables of a BandWavelengthGrid built from ListBand definitions, in the form
+    Backend.set_instrument_bands takes: (wavelengths in m, normalised transmissions, effective
+    width) per band, sorted by pivot wavelength. bands: (wavelengths, transmissions) pairs with
+    wavelengths in units of `unit` (micron by default). Follows TabulatedBand::setupSelfBefore
+    (increasing order, normalisation to unit integral, SKIRT/core/TabulatedBand.cpp) and
+    Band::setupSelfAfter (pivot wavelength and effective width 1/max T, Band.cpp); the bands are
+    ordered as BandWavelengthGrid::setupSelfAfter orders them."""
+    out = []
+    for lam, tr in bands:
+        lv = np.asarray(lam, dtype=np.float64) * unit
+        tv = np.asarray(tr, dtype=np.float64).copy()
+        if lv[0] > lv[-1]:
+            lv, tv = lv[::-1].copy(), tv[::-1].copy()
+        norm = 0.0
+        for i in range(1, len(lv)):
+            norm += 0.5 * (tv[i - 1] + tv[i]) * (lv[i] - lv[i - 1])
+        tv /= norm
+        integral = 0.0
+        for i in range(1, len(lv)):
+            lm = 0.5 * (lv[i - 1] + lv[i])
+            integral += 0.5 * (tv[i - 1] + tv[i]) * (lv[i] - lv[i - 1]) / lm / lm
+        out.append((1.0 / np.sqrt(integral), lv, tv, 1.0 / tv.max()))
+    out.sort(key=lambda b: b[0])
+    return [(lv, tv, w) for _, lv, tv, w in out]
+
+
+def band_transmission(band, lam):
+    """Band::transmission(lambda) (SKIRT/core/Band.cpp) of a list_bands entry."""
+    lv, tv, width = band
+    index = int(np.searchsorted(lv, lam, side="right"))
+    if index == 0 or index >= len(lv):
+        return 0.0
+    t = tv[index - 1] + ((lam - lv[index - 1]) / (lv[index] - lv[index - 1])) * (tv[index] - tv[index - 1])
+    return t * width
+
+
 class Results:
     """Tallies of one segment, per instrument in instrument order, plus the radiation field."""
 
@@ -93,11 +130,17 @@ class Scene:
             s.same_observer = int(ins.get("same_observer", 0))
             s.record_statistics = int(ins.get("stats", 0))
             s.record_components = int(ins.get("comps", 0))
+            if ins.get("bands") is not None:
+                # band grid (set after the upload): no disjoint bin
+                ins["num_bins"] = len(ins["bands"])
+                wb, we = [0.0], [-1, -1]
+            else:
+                wb, we = list(ins["wlg_borders"]), list(ins["wlg_ellv"])
             s.num_wavelength_bins = int(ins["num_bins"])
             s.wlg_offset = len(ellv)
-            s.wlg_num_borders = len(ins["wlg_borders"])
-            borders.extend(list(ins["wlg_borders"]) + [0.0])
-            ellv.extend(list(ins["wlg_ellv"]))
+            s.wlg_num_borders = len(wb)
+            borders.extend(wb + [0.0])
+            ellv.extend(we)
             s.kobs[:] = list(ins["kobs"])
             if s.kind == abi.INSTR_FRAME:
                 s.num_pixels_x, s.num_pixels_y = int(ins["nx"]), int(ins["ny"])
@@ -105,6 +148,11 @@ class Scene:
                 s.xp_min, s.xp_size, s.yp_min, s.yp_size = ins["xp_min"], ins["xp_size"], ins["yp_min"], ins["yp_size"]
             structs.append(s)
         be.upload_instruments(structs, np.array(borders), np.array(ellv, np.int32))
+        for i, ins in enumerate(self.instruments):
+            if ins.get("levels"):
+                be.set_instrument_scattering_levels(i, ins["levels"])
+            if ins.get("bands") is not None:
+                be.set_instrument_bands(i, ins["bands"])
 
     def source_structs(self, npp):
         """ABI source records for a segment of npp packets (SourceSystem::prepareForLaunch)."""
@@ -209,6 +257,8 @@ class Scene:
             d = {"total": total, "stats": stats}
             if ins.get("comps"):
                 d["components"] = be.fetch_instrument_components(i, n)
+                if ins.get("levels"):
+                    d["levels"] = be.fetch_instrument_levels(i, n, ins["levels"])
             if ins["kind"] == abi.INSTR_FRAME:
                 shape = (ins["num_bins"], ins["ny"], ins["nx"])
                 d["total"] = total.reshape(shape)
@@ -216,6 +266,8 @@ class Scene:
                     d["stats"] = stats.reshape((5,) + shape)
                 if "components" in d:
                     d["components"] = d["components"].reshape((3,) + shape)
+                if "levels" in d:
+                    d["levels"] = d["levels"].reshape((ins["levels"],) + shape)
             res.instruments.append(d)
         if self.store_rf and rf:
             res.rf = be.fetch_radiation_field(len(self.density) * self.rf["num_bins"]).reshape(len(self.density), -1)

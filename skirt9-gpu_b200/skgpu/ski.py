@@ -190,18 +190,41 @@ def point_source(temperature=5800, luminosity_lsun=1.0):
             f'integratedLuminosity="{luminosity_lsun} Lsun"/></normalization></PointSource>')
 
 
-def frame_instrument(name, inclination_deg, fov, unit, npix, stats=True, distance_mpc=10, comps=False):
+def _instrument_tail(tag, wlg):
+    """Closing of an instrument element, with its own wavelength grid (an XML wavelength-grid item)
+    when one is given."""
+    return f'><wavelengthGrid type="WavelengthGrid">{wlg}</wavelengthGrid></{tag}>' if wlg else "/>"
+
+
+def frame_instrument(name, inclination_deg, fov, unit, npix, stats=True, distance_mpc=10, comps=False, levels=0,
+                     wlg=None):
     return (f'<FrameInstrument instrumentName="{name}" distance="{distance_mpc} Mpc" inclination="{inclination_deg} deg" '
             f'azimuth="0 deg" roll="0 deg" fieldOfViewX="{fov} {unit}" numPixelsX="{npix}" centerX="0 {unit}" '
             f'fieldOfViewY="{fov} {unit}" numPixelsY="{npix}" centerY="0 {unit}" '
-            f'recordComponents="{"true" if comps else "false"}" numScatteringLevels="0" recordPolarization="false" '
-            f'recordStatistics="{"true" if stats else "false"}"/>')
+            f'recordComponents="{"true" if comps else "false"}" numScatteringLevels="{levels}" recordPolarization="false" '
+            f'recordStatistics="{"true" if stats else "false"}"' + _instrument_tail("FrameInstrument", wlg))
 
 
-def sed_instrument(name, inclination_deg, stats=True, distance_mpc=10, comps=True):
+def sed_instrument(name, inclination_deg, stats=True, distance_mpc=10, comps=True, levels=0, wlg=None):
     return (f'<SEDInstrument instrumentName="{name}" distance="{distance_mpc} Mpc" inclination="{inclination_deg} deg" '
             f'azimuth="0 deg" roll="0 deg" radius="0 pc" recordComponents="{"true" if comps else "false"}" '
-            f'numScatteringLevels="0" recordPolarization="false" recordStatistics="{"true" if stats else "false"}"/>')
+            f'numScatteringLevels="{levels}" recordPolarization="false" recordStatistics="{"true" if stats else "false"}"'
+            + _instrument_tail("SEDInstrument", wlg))
+
+
+def band_grid(bands):
+    """ConfigurableBandWavelengthGrid of ListBands; bands: list of (wavelengths in micron,
+    transmission values)."""
+    items = "".join(f'<ListBand wavelengths="{", ".join(f"{l:g} micron" for l in lam)}" '
+                    f'transmissionValues="{", ".join(f"{t:g}" for t in tr)}"/>' for lam, tr in bands)
+    return f'<ConfigurableBandWavelengthGrid><bands type="Band">{items}</bands></ConfigurableBandWavelengthGrid>'
+
+
+# four overlapping bands over 0.2-3 micron (triangles and a flat top), for tests of band grids
+TEST_BANDS = [([0.2, 0.35, 0.5], [0.1, 1.0, 0.1]),
+              ([0.4, 0.45, 0.7, 0.75], [0.2, 1.0, 1.0, 0.2]),
+              ([0.5, 1.0, 1.6], [0.3, 0.9, 0.3]),
+              ([1.2, 2.0, 3.0], [1.0, 0.5, 0.2])]
 
 
 def dust_emission_options(em_min_um=1.0, em_max_um=1000.0, num_em=30, spatial_bias=0.5, source_bias=0.5,
@@ -405,3 +428,24 @@ def galaxy_tetra(num_packets, vertex_filename, tau_v=1.0, npix=256, nlambda=32, 
     return simulation("ExtinctionOnly", num_packets, sources, expdisk_medium(6, 0.2, "kpc", tau_v, mix),
                       tetra_grid(half_size_kpc, "kpc", 100, policy="File", filename=vertex_filename), instruments,
                       instrument_wlg=wlg, store_rf=False)
+
+
+def galaxy_levels_bands(num_packets=30000, npix=16, nlambda=10, max_level=5, max_dust_fraction=1e-3, levels=3,
+                        bands=None):
+    """The galaxy on a small octree with two instruments at 60 degrees that record components: a
+    frame on the log wavelength grid with `levels` scattering levels, and an SED on a band
+    wavelength grid (TEST_BANDS) with statistics and two scattering levels."""
+    lam = [0.1 * (100.0 ** (i / (nlambda - 1))) for i in range(nlambda)]
+    kappa = [(l / 0.55) ** -1.0 for l in lam]
+    albedo = [min(0.9, max(0.05, 0.5 * (l / 0.55) ** -0.2)) for l in lam]
+    g = [min(0.9, max(0.0, 0.6 * (l / 0.55) ** -0.3)) for l in lam]
+    mix = mean_list_mix(lam, kappa, albedo, g)
+    sources = (geometric_source('<ExpDiskGeometry scaleLength="4 kpc" scaleHeight="0.35 kpc" minRadius="0 kpc" '
+                                'maxRadius="0 kpc" maxZ="0 kpc"/>', 6000, 8e9)
+               + geometric_source('<SersicGeometry effectiveRadius="1 kpc" index="4"/>', 4000, 2e9))
+    wlg = f'<LogWavelengthGrid minWavelength="0.1 micron" maxWavelength="10 micron" numWavelengths="{nlambda}"/>'
+    instruments = (frame_instrument("i60", 60, 50, "kpc", npix, stats=True, comps=True, levels=levels)
+                   + sed_instrument("bands", 60, stats=True, comps=True, levels=2,
+                                    wlg=band_grid(bands or TEST_BANDS)))
+    return simulation("ExtinctionOnly", num_packets, sources, expdisk_medium(6, 0.2, "kpc", 1.0, mix),
+                      octree_grid(25, "kpc", max_level, max_dust_fraction), instruments, instrument_wlg=wlg)

@@ -32,3 +32,42 @@ def median_relative_error(stats, n):
     w1, w2 = stats[1], stats[2]
     m = w1 > 0
     return float(np.median(np.sqrt(np.maximum(w2[m] / w1[m] ** 2 - 1.0 / n, 0))))
+
+
+def tetra_hull_edge_exits(z, rel=1e-9):
+    """Rays of a tetrahedral path fixture that leave the mesh's convex hull through an edge or a
+    vertex of its boundary triangulation: two or more boundary faces hold the exit point. There the
+    reference's own exit decision (TetraMeshSpatialGrid.cpp:750-766, the plane fallback when a
+    Plucker product is exactly zero) compares two equal distances, and the rounding of its FP64
+    position picks the face."""
+    V, T, N, NT = z["tet_vertices"], z["tet_tetra"], z["tet_normals"], z["tet_ntetra"]
+    ext = z["grid_extent"]
+    tol = rel * np.sqrt(((ext[3:] - ext[:3]) ** 2).sum())
+    faces = [(t, f) for t, f in zip(*np.nonzero(NT < 0))]
+    tri = np.array([[V[T[t, v]] for v in range(4) if v != f] for t, f in faces])
+    nrm = np.array([N[t, f] for t, f in faces])
+    out = set()
+    for r, ray in enumerate(z["rays"]):
+        p0, k = ray[:3], ray[3:]
+        nk = nrm @ k
+        ahead = nk > 0
+        dist = np.full(len(faces), np.inf)
+        dist[ahead] = np.einsum("ij,ij->i", nrm[ahead], tri[ahead, 0] - p0) / nk[ahead]
+        t_exit = dist.min()
+        if not np.isfinite(t_exit):
+            continue
+        p = p0 + k * t_exit
+        held = 0
+        for q in np.nonzero(np.abs(dist - t_exit) <= tol)[0]:
+            a, b, c = tri[q]
+            # barycentric containment with a tolerance of rel
+            n = np.cross(b - a, c - a)
+            area = n @ n
+            wa = np.cross(c - b, p - b) @ n / area
+            wb = np.cross(a - c, p - c) @ n / area
+            wc = 1.0 - wa - wb
+            if min(wa, wb, wc) >= -rel:
+                held += 1
+        if held >= 2:
+            out.add(r)
+    return out

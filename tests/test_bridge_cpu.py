@@ -63,6 +63,15 @@ def test_bridge_dust_emission_on_oracle(tmp_path):
 
 
 @needs_build
+def test_bridge_levels_and_bands_on_oracle(tmp_path):
+    """Scattering levels (frame, 3 levels; SED, 2 levels) and a band wavelength grid (four
+    overlapping ListBands) through the bridge: SKIRT's own level FITS files and band SED agree with
+    the reference program's."""
+    log, g, c = both(tmp_path, ski.galaxy_levels_bands(200000), "lb")
+    tb.check_levels_and_bands(g, c, "lb")
+
+
+@needs_build
 def test_bridge_off_is_the_reference(tmp_path):
     """Without -g the bridged program is the reference program: identical outputs."""
     text = ski.shell_cartesian(5000, nbins=8, npix=8)

@@ -80,6 +80,24 @@ def both(tmp_path, text, name):
     return log, str(tmp_path / "gpu"), str(tmp_path / "cpu")
 
 
+def check_levels_and_bands(g, c, name):
+    """Band SED (z-scores from the per-band statistics), frame, and the scattering-level outputs of
+    ski.galaxy_levels_bands: summed level planes and the SED's level columns within a few per cent
+    (no per-plane statistics exist; at 2e5 packets the spread is ~1 % for levels 1-2)."""
+    z, _ = sed_z(g, c, name, "bands")
+    assert len(z) == 4
+    check(z, 4.0, 4.0)
+    z, _ = frame_z(g, c, name, "i60")
+    check(z, 1.4, 6.0)
+    for n, tol in ((1, 0.04), (2, 0.04), (3, 0.08)):
+        a, b = (fits.read(os.path.join(d, f"{name}_i60_primaryscattered{n}.fits"))[0].astype(np.float64).sum()
+                for d in (g, c))
+        assert a > 0 and a == pytest.approx(b, rel=tol), n
+    sa, sb = (np.loadtxt(os.path.join(d, f"{name}_bands_sed.dat")) for d in (g, c))
+    assert sa.shape == sb.shape == (4, 10)
+    assert np.allclose(sa[:, 8:10].sum(axis=0), sb[:, 8:10].sum(axis=0), rtol=0.04)
+
+
 def check(z, chi2_max, zmax):
     """Mean square z below chi2_max; the 99.9th percentile of |z| below zmax (frame pixels see rare
     high-weight contributions, so the largest |z| of ~2e4 pixels is not a good test)."""
@@ -111,6 +129,13 @@ def test_bridge_galaxy_octree(tmp_path):
     for inc in (0, 60, 90):
         z, _ = frame_z(g, c, "galaxy", f"i{inc}")
         check(z, 1.3, 6.0)
+
+
+@needs_build
+def test_bridge_levels_and_bands(tmp_path):
+    """Scattering levels and a band wavelength grid on the B200 through SKIRT's own program."""
+    log, g, c = both(tmp_path, ski.galaxy_levels_bands(200000), "lb")
+    check_levels_and_bands(g, c, "lb")
 
 
 @needs_build
