@@ -45,6 +45,7 @@ extern "C" {
 #define SKGPU_GRID_SPHERE2D 6
 #define SKGPU_GRID_SPHERE3D 7
 #define SKGPU_GRID_CYLINDER3D 8
+#define SKGPU_GRID_ADAPTIVE_MESH 9
 
 /* traversal precision (path kernels and life cycle) */
 #define SKGPU_PREC_FP64_EXACT 0 /* FP64 with the reference generators' operation order, no FMA contraction */
@@ -159,6 +160,17 @@ int skgpu_upload_grid_octree(skgpu_ctx* ctx, int32_t num_nodes, const double* bo
                              const int32_t* child_begin, const int32_t* child_count, const int32_t* child_index,
                              int32_t num_child_index, const int32_t* nb_begin, const int32_t* nb_index,
                              int32_t num_nb_index, double eps);
+/* AdaptiveMeshSpatialGrid: the snapshot's traversal arrays (AdaptiveMeshSpatialGrid::traversalNodeBounds,
+ * traversalChildBegin, traversalChildCount, traversalChildIndex, traversalCellIndex,
+ * AdaptiveMeshSnapshot.cpp:172-199; the data GpuAcceleration::setAdaptiveMeshSpatialGridPath hands to
+ * its tree kernel), nodes in depth-first order from the root, children in local Morton order, and
+ * the snapshot's eps (1e-12 of the domain diagonal). The library derives each node's subdivision
+ * from its children's bounds and each leaf wall's neighbour by Node::addNeighbors
+ * (AdaptiveMeshSnapshot.cpp:67-83); paths follow AdaptiveMeshSnapshot::MySegmentGenerator::next
+ * (AdaptiveMeshSnapshot.cpp:378-449). */
+int skgpu_upload_grid_adaptive_mesh(skgpu_ctx* ctx, int32_t num_nodes, const double* bounds, const int32_t* cell_index,
+                                    const int32_t* child_begin, const int32_t* child_count, const int32_t* child_index,
+                                    int32_t num_child_index, double eps);
 /* VoronoiMeshSnapshot: sites (x,y,z) and neighbour CSR with wall ids -1..-6
  * (VoronoiMeshSnapshot.cpp:725-740); extent xmin..zmax; eps = 1e-12 * diagonal. */
 int skgpu_upload_grid_voronoi(skgpu_ctx* ctx, int32_t num_sites, const double* sites, const int32_t* nb_begin,

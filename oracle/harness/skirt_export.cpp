@@ -58,6 +58,8 @@
 #include "NormalizedSource.hpp"
 #include "SersicFunction.hpp"
 #include "SersicGeometry.hpp"
+#include "AdaptiveMeshSnapshot.hpp"
+#include "AdaptiveMeshSpatialGrid.hpp"
 #include "CartesianSpatialGrid.hpp"
 #include "Configuration.hpp"
 #include "DisjointWavelengthGrid.hpp"
@@ -283,6 +285,24 @@ namespace
             writeVec(out + "/tree_child_index.npy", childIndex);
             writeVec(out + "/tree_nb_begin.npy", nbBegin);
             writeVec(out + "/tree_nb_index.npy", nbIndex);
+            return;
+        }
+        if (auto g = dynamic_cast<AdaptiveMeshSpatialGrid*>(grid))
+        {
+            // the snapshot's traversal arrays (AdaptiveMeshSnapshot.cpp:172-199), depth-first from the root
+            meta.kv("grid", "adaptive");
+            meta.kv("eps", g->_mesh->_eps);
+            Box bb = g->boundingBox();
+            std::vector<double> e = {bb.xmin(), bb.ymin(), bb.zmin(), bb.xmax(), bb.ymax(), bb.zmax()};
+            writeVec(out + "/grid_extent.npy", e);
+            const std::vector<double>& b = g->traversalNodeBounds();
+            size_t n = b.size() / 6;
+            writeNpy(out + "/am_bounds.npy", b.data(), {n, 6});
+            auto i32 = [](const std::vector<int>& v) { return std::vector<int32_t>(v.begin(), v.end()); };
+            writeVec(out + "/am_cell_index.npy", i32(g->traversalCellIndex()));
+            writeVec(out + "/am_child_begin.npy", i32(g->traversalChildBegin()));
+            writeVec(out + "/am_child_count.npy", i32(g->traversalChildCount()));
+            writeVec(out + "/am_child_index.npy", i32(g->traversalChildIndex()));
             return;
         }
         if (auto vg = dynamic_cast<VoronoiMeshSpatialGrid*>(grid))

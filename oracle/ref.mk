@@ -98,6 +98,14 @@ $(OBJ)/build/%.o: $(S_BLD)/% $(GEN)/version.h $(GEN)/timestamp.h
 $(OBJ)/skirtcore/%.o: $(K_CORE)/%
 	@mkdir -p $(dir $@)
 	$(CXX) $(CXXFLAGS_REF) $(INC_CORE) -c $< -o $@
+# AdaptiveMeshSnapshot::Node::appendTraversalData (AdaptiveMeshSnapshot.cpp:193-198) assigns
+# `childIndex[begin + l] = <recursive call that grows childIndex>`; C++14 leaves the two operands
+# unsequenced and GCC takes the element address first, so the write can land in the freed buffer
+# (heap corruption, or traversal arrays with -1 entries). C++17 evaluates the right operand first:
+# this one file is compiled as C++17, which changes nothing else.
+$(OBJ)/skirtcore/AdaptiveMeshSnapshot.cpp.o: $(K_CORE)/AdaptiveMeshSnapshot.cpp
+	@mkdir -p $(dir $@)
+	$(CXX) $(CXXFLAGS_REF) -std=c++17 $(INC_CORE) -c $< -o $@
 $(OBJ)/utils/%.o: $(K_UTIL)/%
 	@mkdir -p $(dir $@)
 	$(CXX) $(CXXFLAGS_REF) -I$(S_FUND) -c $< -o $@
@@ -182,7 +190,9 @@ BRIDGE_FNS := create destroy last_error abi_version device_count upload_grid_car
     upload_grid_octree upload_medium upload_dust_mix upload_rf_grid upload_instruments upload_sources set_options \
     clear_tallies run_primary fetch_instrument fetch_instrument_components fetch_radiation_field \
     upload_dust_emission upload_radiation_field prepare_secondary run_secondary \
-    set_instrument_scattering_levels set_instrument_bands fetch_instrument_levels
+    set_instrument_scattering_levels set_instrument_bands fetch_instrument_levels \
+    upload_grid_sphere2d upload_grid_sphere3d upload_grid_cylinder2d upload_grid_cylinder3d \
+    upload_grid_adaptive_mesh upload_grid_voronoi upload_grid_tetra
 BRIDGE_ORACLE_DEFS := $(foreach f,$(BRIDGE_FNS),-Dskgpu_$(f)=or_$(f)) -Dskgpu_ctx=or_ctx -include $(HERE)/skoracle.h
 
 $(OBJ)/bridge/SkgpuLifeCycle_oracle.o: $(BRIDGE)/SkgpuLifeCycle.cpp $(BRIDGE)/SkgpuLifeCycle.hpp $(HERE)/skoracle.h

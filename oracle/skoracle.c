@@ -101,10 +101,12 @@ typedef struct
     /* cartesian */
     double *xb, *yb, *zb;
     int nx, ny, nz;
-    /* octree */
+    /* octree (and the adaptive mesh: one neighbour per leaf wall) */
     double* tb;
     int *tcell, *tchild, *tnbb, *tnb;
     int tnodes;
+    /* adaptive mesh: subdivision nx, ny, nz per node (0 for leaves), children CSR */
+    int *adiv, *acb, *ach;
     /* voronoi */
     double* vs;
     int *vnbb, *vnb;
@@ -197,6 +199,7 @@ static void free_grid(Grid* g)
 {
     free(g->xb); free(g->yb); free(g->zb);
     free(g->tb); free(g->tcell); free(g->tchild); free(g->tnbb); free(g->tnb);
+    free(g->adiv); free(g->acb); free(g->ach);
     free(g->vs); free(g->vnbb); free(g->vnb);
     free(g->tev); free(g->ten); free(g->tebox); free(g->tet); free(g->tent); free(g->tenf);
     free(g->srv);
@@ -303,6 +306,104 @@ int or_upload_grid_octree(or_ctx* c, int32_t num_nodes, const double* bounds, co
     }
     g->tnbb = dup(nb_begin, (6 * (size_t)num_nodes + 1) * sizeof(int));
     g->tnb = dup(nb_index, (size_t)num_nb_index * sizeof(int));
+    memcpy(g->ext, bounds, 6 * sizeof(double));
+    g->eps = eps;
+    g->numCells = numCells;
+    c->hasGrid = 1;
+    return SKGPU_OK;
+}
+
+/* AdaptiveMeshSnapshot::Node::leaf and Node::child (AdaptiveMeshSnapshot.cpp:103-145): Box::cellIndices
+   estimate (Box.hpp:162-167), one-index correction per axis; -1 outside the root, -2 where the
+   reference stops with a FatalError */
+static int box_contains(const double* b, double x, double y, double z);
+static int am_leaf(const Grid* g, double x, double y, double z)
+{
+    if (!box_contains(g->tb, x, y, z)) return -1;
+    int node = 0;
+    for (int guard = 0; guard < 256; ++guard)
+    {
+        int nx = g->adiv[3 * node], ny = g->adiv[3 * node + 1], nz = g->adiv[3 * node + 2];
+        if (nx == 0) return node;
+        const double* b = g->tb + 6 * (size_t)node;
+        int i = (int)(nx * (x - b[0]) / (b[3] - b[0]));
+        int j = (int)(ny * (y - b[1]) / (b[4] - b[1]));
+        int k = (int)(nz * (z - b[2]) / (b[5] - b[2]));
+        i = i < 0 ? 0 : (i > nx - 1 ? nx - 1 : i);
+        j = j < 0 ? 0 : (j > ny - 1 ? ny - 1 : j);
+        k = k < 0 ? 0 : (k > nz - 1 ? nz - 1 : k);
+        const int* kids = g->ach + g->acb[node];
+        int c = kids[(k * ny + j) * nx + i];
+        const double* cb = g->tb + 6 * (size_t)c;
+        if (!box_contains(cb, x, y, z))
+        {
+            if (x < cb[0]) i--;
+            else if (x > cb[3]) i++;
+            if (y < cb[1]) j--;
+            else if (y > cb[4]) j++;
+            if (z < cb[2]) k--;
+            else if (z > cb[5]) k++;
+            if (i < 0 || i >= nx || j < 0 || j >= ny || k < 0 || k >= nz) return -2;
+            c = kids[(k * ny + j) * nx + i];
+            if (!box_contains(g->tb + 6 * (size_t)c, x, y, z)) return -2;
+        }
+        node = c;
+    }
+    return -2;
+}
+
+int or_upload_grid_adaptive_mesh(or_ctx* c, int32_t num_nodes, const double* bounds, const int32_t* cell_index,
+                                 const int32_t* child_begin, const int32_t* child_count, const int32_t* child_index,
+                                 int32_t num_child_index, double eps)
+{
+    if (num_nodes < 1 || !bounds || !cell_index || !child_begin || !child_count) return fail(c, SKGPU_ERR_ARG, "adaptive mesh: missing arrays");
+    free_grid(&c->g);
+    Grid* g = &c->g;
+    g->kind = SKGPU_GRID_ADAPTIVE_MESH;
+    g->tnodes = num_nodes;
+    g->tb = dup(bounds, 6 * (size_t)num_nodes * sizeof(double));
+    g->tcell = dup(cell_index, num_nodes * sizeof(int));
+    g->acb = dup(child_begin, num_nodes * sizeof(int));
+    g->ach = dup(child_index, (size_t)(num_child_index > 0 ? num_child_index : 1) * sizeof(int));
+    g->adiv = (int*)calloc(3 * (size_t)num_nodes, sizeof(int));
+    int numCells = 0;
+    /* subdivision: children sharing child 0's (y, z), (x, z) and (x, y) lower corners count nx, ny, nz */
+    for (int l = 0; l < num_nodes; ++l)
+    {
+        if (cell_index[l] + 1 > numCells) numCells = cell_index[l] + 1;
+        int cnt = child_count[l];
+        if (cnt == 0) continue;
+        const int* kids = child_index + child_begin[l];
+        const double* c0 = bounds + 6 * (size_t)kids[0];
+        int nx = 0, ny = 0, nz = 0;
+        for (int q = 0; q < cnt; ++q)
+        {
+            const double* b = bounds + 6 * (size_t)kids[q];
+            nx += b[1] == c0[1] && b[2] == c0[2];
+            ny += b[0] == c0[0] && b[2] == c0[2];
+            nz += b[0] == c0[0] && b[1] == c0[1];
+        }
+        if (nx * ny * nz != cnt) return fail(c, SKGPU_ERR_ARG, "adaptive mesh: children are not a lattice");
+        g->adiv[3 * l] = nx; g->adiv[3 * l + 1] = ny; g->adiv[3 * l + 2] = nz;
+    }
+    /* Node::addNeighbors (AdaptiveMeshSnapshot.cpp:67-83): the leaf eps beyond each wall centre */
+    g->tnbb = (int*)calloc(6 * (size_t)num_nodes + 1, sizeof(int));
+    g->tnb = (int*)malloc(6 * (size_t)num_nodes * sizeof(int));
+    int n = 0;
+    for (int l = 0; l < num_nodes; ++l)
+        for (int w = 0; w < 6; ++w)
+        {
+            g->tnbb[6 * l + w] = n;
+            if (child_count[l]) continue;
+            const double* b = bounds + 6 * (size_t)l;
+            double ctr[3] = {0.5 * (b[0] + b[3]), 0.5 * (b[1] + b[4]), 0.5 * (b[2] + b[5])};
+            double d[3] = {0., 0., 0.};
+            d[w / 2] = (w % 2) ? eps : -eps;
+            int nb = am_leaf(g, ctr[0] + d[0], ctr[1] + d[1], ctr[2] + d[2]);
+            if (nb == -2) return fail(c, SKGPU_ERR_ARG, "adaptive mesh: cannot locate a child node");
+            if (nb >= 0) g->tnb[n++] = nb;
+        }
+    g->tnbb[6 * (size_t)num_nodes] = n;
     memcpy(g->ext, bounds, 6 * sizeof(double));
     g->eps = eps;
     g->numCells = numCells;
@@ -681,13 +782,26 @@ static int leaf_child(const Grid* g, double x, double y, double z)
     return node;
 }
 
+/* the leaf search of a tree grid: the octree's, or the adaptive mesh's (-2 counts as outside) */
+static int tree_leaf(const Grid* g, double x, double y, double z)
+{
+    if (g->kind == SKGPU_GRID_ADAPTIVE_MESH)
+    {
+        int l = am_leaf(g, x, y, z);
+        return l < 0 ? -1 : l;
+    }
+    return leaf_child(g, x, y, z);
+}
+
+/* TreeSpatialGrid::MySegmentGenerator::next (TreeSpatialGrid.cpp:143-228) and
+   AdaptiveMeshSnapshot::MySegmentGenerator::next (AdaptiveMeshSnapshot.cpp:378-449) */
 static int tree_next(const Grid* g, Gen* s)
 {
     if (s->state == OUTSIDE) return 0;
     if (s->state == UNKNOWN)
     {
         if (!move_inside(s, g->ext, g->eps)) return 0;
-        s->node = leaf_child(g, s->rx, s->ry, s->rz);
+        s->node = tree_leaf(g, s->rx, s->ry, s->rz);
         if (s->node < 0)
         {
             s->state = OUTSIDE;
@@ -720,13 +834,13 @@ static int tree_next(const Grid* g, Gen* s)
             break;
         }
     }
-    if (nb < 0) nb = leaf_child(g, s->rx, s->ry, s->rz);
+    if (nb < 0) nb = tree_leaf(g, s->rx, s->ry, s->rz);
     if (nb == old)
     {
         s->rx = nextafter(s->rx, (s->kx < 0.) ? -DBL_MAX : DBL_MAX);
         s->ry = nextafter(s->ry, (s->ky < 0.) ? -DBL_MAX : DBL_MAX);
         s->rz = nextafter(s->rz, (s->kz < 0.) ? -DBL_MAX : DBL_MAX);
-        nb = leaf_child(g, s->rx, s->ry, s->rz);
+        nb = tree_leaf(g, s->rx, s->ry, s->rz);
     }
     s->node = nb;
     if (nb < 0 || nb == old) s->state = OUTSIDE;
@@ -1585,6 +1699,7 @@ static int gen_next(const Grid* g, Gen* s)
     {
         case SKGPU_GRID_CARTESIAN: return cart_next(g, s);
         case SKGPU_GRID_OCTREE: return tree_next(g, s);
+        case SKGPU_GRID_ADAPTIVE_MESH: return tree_next(g, s);
         case SKGPU_GRID_VORONOI: return vor_next(g, s);
         case SKGPU_GRID_TETRA: return tet_next(g, s);
         case SKGPU_GRID_SPHERE1D: return sph_next(g, s);
@@ -2500,8 +2615,9 @@ static int lb_index(const double* v, int n, double x)
 int or_prepare_secondary(or_ctx* c, const skgpu_secondary_options* opt, uint64_t total_packets, double* luminosity)
 {
     if (!opt || total_packets == 0) return fail(c, SKGPU_ERR_ARG, "secondary: missing options or packets");
-    if (!c->hasGrid || (c->g.kind != SKGPU_GRID_CARTESIAN && c->g.kind != SKGPU_GRID_OCTREE))
-        return fail(c, SKGPU_ERR_UNSUPPORTED, "secondary: dust emission needs a Cartesian or octree grid");
+    if (!c->hasGrid || (c->g.kind != SKGPU_GRID_CARTESIAN && c->g.kind != SKGPU_GRID_OCTREE
+                        && c->g.kind != SKGPU_GRID_ADAPTIVE_MESH))
+        return fail(c, SKGPU_ERR_UNSUPPORTED, "secondary: dust emission needs a Cartesian, octree or adaptive-mesh grid");
     if (!c->deNrf || c->deCells != c->numCells || c->deNrf != c->nrf)
         return fail(c, SKGPU_ERR_STATE, "secondary: dust emission tables do not match the medium and RF grid");
     if (!c->rf || c->rfLen != (size_t)c->numCells * c->nrf) return fail(c, SKGPU_ERR_STATE, "secondary: no radiation field");
@@ -2525,7 +2641,7 @@ int or_prepare_secondary(or_ctx* c, const skgpu_secondary_options* opt, uint64_t
     c->secPackets = 0;
     free(c->secCellNode);
     c->secCellNode = NULL;
-    if (c->g.kind == SKGPU_GRID_OCTREE)
+    if (c->g.kind == SKGPU_GRID_OCTREE || c->g.kind == SKGPU_GRID_ADAPTIVE_MESH)
     {
         c->secCellNode = (int*)calloc(cells, sizeof(int));
         for (int q = 0; q < c->g.tnodes; ++q)

@@ -27,8 +27,12 @@
 
 #define private public
 #define protected public
+#include "AdaptiveMeshSnapshot.hpp"
+#include "AdaptiveMeshSpatialGrid.hpp"
 #include "BlackBodySED.hpp"
 #include "CartesianSpatialGrid.hpp"
+#include "Cylinder2DSpatialGrid.hpp"
+#include "Cylinder3DSpatialGrid.hpp"
 #include "Configuration.hpp"
 #include "ContSED.hpp"
 #include "DefaultWavelengthDistribution.hpp"
@@ -57,8 +61,13 @@
 #include "SersicGeometry.hpp"
 #include "SourceSystem.hpp"
 #include "Sphere1DSpatialGrid.hpp"
+#include "Sphere2DSpatialGrid.hpp"
+#include "Sphere3DSpatialGrid.hpp"
+#include "TetraMeshSpatialGrid.hpp"
 #include "TreeNode.hpp"
 #include "TreeSpatialGrid.hpp"
+#include "VoronoiMeshSnapshot.hpp"
+#include "VoronoiMeshSpatialGrid.hpp"
 #include "WavelengthDistribution.hpp"
 #undef private
 #undef protected
@@ -115,8 +124,14 @@ namespace
             || config->_hasLymanAlpha || config->hasDynamicState() || config->hasVariableMedia())
             return (why = "polarisation, kinematics, Lyman-alpha or a dynamic medium"), false;
         auto grid = sim->mediumSystem()->grid();
-        bool box = dynamic_cast<CartesianSpatialGrid*>(grid) || dynamic_cast<TreeSpatialGrid*>(grid);
-        if (!box && !dynamic_cast<Sphere1DSpatialGrid*>(grid)) return (why = "grid type"), false;
+        // grids whose cells are boxes (the secondary launch draws positions in them)
+        bool box = dynamic_cast<CartesianSpatialGrid*>(grid) || dynamic_cast<TreeSpatialGrid*>(grid)
+                   || dynamic_cast<AdaptiveMeshSpatialGrid*>(grid);
+        bool other = dynamic_cast<Sphere1DSpatialGrid*>(grid) || dynamic_cast<Sphere2DSpatialGrid*>(grid)
+                     || dynamic_cast<Sphere3DSpatialGrid*>(grid) || dynamic_cast<Cylinder2DSpatialGrid*>(grid)
+                     || dynamic_cast<Cylinder3DSpatialGrid*>(grid) || dynamic_cast<VoronoiMeshSpatialGrid*>(grid)
+                     || dynamic_cast<TetraMeshSpatialGrid*>(grid);
+        if (!box && !other) return (why = "grid type"), false;
         for (Instrument* instr : sim->instrumentSystem()->instruments())
         {
             auto rec = instr->instrumentFluxRecorder();
@@ -147,7 +162,7 @@ namespace
         }
         else
         {
-            if (!box) return (why = "secondary emission needs a Cartesian or octree grid"), false;
+            if (!box) return (why = "secondary emission needs a Cartesian, octree or adaptive-mesh grid"), false;
             if (!config->hasDustEmission() || config->hasGasEmission() || config->hasStochasticDustEmission()
                 || config->storeEmissionRadiationField() || !config->hasPanRadiationField())
                 return (why = "secondary emission other than equilibrium dust emission"), false;
@@ -176,6 +191,98 @@ namespace
         {
             const Array& rv = g->radialBorderPositions();
             check(skgpu_upload_grid_sphere1d(g_ctx, rv.size(), &rv[0]), "1D spherical grid");
+            return;
+        }
+        if (auto g = dynamic_cast<Sphere2DSpatialGrid*>(grid))
+        {
+            check(skgpu_upload_grid_sphere2d(g_ctx, g->_rv.size(), &g->_rv[0], g->_thetav.size(), &g->_thetav[0],
+                                             &g->_cv[0]),
+                  "2D spherical grid");
+            return;
+        }
+        if (auto g = dynamic_cast<Sphere3DSpatialGrid*>(grid))
+        {
+            check(skgpu_upload_grid_sphere3d(g_ctx, g->_rv.size(), &g->_rv[0], g->_thetav.size(), &g->_thetav[0],
+                                             &g->_cv[0], g->_phiv.size(), &g->_phiv[0], &g->_sinv[0], &g->_cosv[0],
+                                             g->_eps),
+                  "3D spherical grid");
+            return;
+        }
+        if (auto g = dynamic_cast<Cylinder2DSpatialGrid*>(grid))
+        {
+            check(skgpu_upload_grid_cylinder2d(g_ctx, g->_Rv.size(), &g->_Rv[0], g->_zv.size(), &g->_zv[0]),
+                  "2D cylindrical grid");
+            return;
+        }
+        if (auto g = dynamic_cast<Cylinder3DSpatialGrid*>(grid))
+        {
+            check(skgpu_upload_grid_cylinder3d(g_ctx, g->_Rv.size(), &g->_Rv[0], g->_phiv.size(), &g->_phiv[0],
+                                               &g->_sinv[0], &g->_cosv[0], g->_zv.size(), &g->_zv[0], g->_eps,
+                                               g->_hasHole ? 1 : 0),
+                  "3D cylindrical grid");
+            return;
+        }
+        if (auto g = dynamic_cast<AdaptiveMeshSpatialGrid*>(grid))
+        {
+            // the snapshot's own traversal arrays (AdaptiveMeshSnapshot.cpp:172-199)
+            const std::vector<double>& b = g->traversalNodeBounds();
+            std::vector<int32_t> cell(g->traversalCellIndex().begin(), g->traversalCellIndex().end()),
+                begin(g->traversalChildBegin().begin(), g->traversalChildBegin().end()),
+                count(g->traversalChildCount().begin(), g->traversalChildCount().end()),
+                child(g->traversalChildIndex().begin(), g->traversalChildIndex().end());
+            check(skgpu_upload_grid_adaptive_mesh(g_ctx, cell.size(), b.data(), cell.data(), begin.data(), count.data(),
+                                                  child.data(), child.size(), g->_mesh->_eps),
+                  "adaptive mesh");
+            return;
+        }
+        if (auto vg = dynamic_cast<VoronoiMeshSpatialGrid*>(grid))
+        {
+            // the snapshot's traversal arrays: sites and the neighbour CSR with wall ids -1..-6
+            // (VoronoiMeshSnapshot.cpp:725-740)
+            auto m = vg->_mesh;
+            int n = m->_traversalNeighborBegin.size();
+            std::vector<int32_t> begin(n + 1), index(m->_traversalNeighborIndex.begin(), m->_traversalNeighborIndex.end());
+            for (int c = 0; c != n; ++c) begin[c] = m->_traversalNeighborBegin[c];
+            begin[n] = index.size();
+            Box e = vg->extent();
+            double ext[6] = {e.xmin(), e.ymin(), e.zmin(), e.xmax(), e.ymax(), e.zmax()};
+            check(skgpu_upload_grid_voronoi(g_ctx, n, m->_traversalSiteCoordinates.data(), begin.data(), index.data(),
+                                            index.size(), ext, m->_eps),
+                  "Voronoi mesh");
+            return;
+        }
+        if (auto g = dynamic_cast<TetraMeshSpatialGrid*>(grid))
+        {
+            // vertices, per tetrahedron its vertex indices and per face the outward normal and the
+            // neighbour across it (TetraMeshSpatialGrid.hpp, Tetra / Face)
+            int nv = g->_vertices.size(), nt = g->_tetrahedra.size();
+            std::vector<double> verts(3 * static_cast<size_t>(nv)), normals(12 * static_cast<size_t>(nt));
+            std::vector<int32_t> tv(4 * static_cast<size_t>(nt)), ntet(4 * static_cast<size_t>(nt)),
+                nface(4 * static_cast<size_t>(nt));
+            for (int i = 0; i != nv; ++i)
+            {
+                verts[3 * i] = g->_vertices[i].x();
+                verts[3 * i + 1] = g->_vertices[i].y();
+                verts[3 * i + 2] = g->_vertices[i].z();
+            }
+            for (int t = 0; t != nt; ++t)
+            {
+                const auto& tet = g->_tetrahedra[t];
+                for (int f = 0; f != 4; ++f)
+                {
+                    tv[4 * t + f] = tet._vertexIndices[f];
+                    ntet[4 * t + f] = tet._faces[f]._ntetra;
+                    nface[4 * t + f] = tet._faces[f]._nface;
+                    normals[12 * t + 3 * f] = tet._faces[f]._normal.x();
+                    normals[12 * t + 3 * f + 1] = tet._faces[f]._normal.y();
+                    normals[12 * t + 3 * f + 2] = tet._faces[f]._normal.z();
+                }
+            }
+            Box e = g->extent();
+            double ext[6] = {e.xmin(), e.ymin(), e.zmin(), e.xmax(), e.ymax(), e.zmax()};
+            check(skgpu_upload_grid_tetra(g_ctx, nv, verts.data(), nt, tv.data(), normals.data(), ntet.data(),
+                                          nface.data(), ext, g->_eps),
+                  "tetrahedral mesh");
             return;
         }
         auto g = dynamic_cast<TreeSpatialGrid*>(grid);

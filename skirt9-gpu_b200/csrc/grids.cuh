@@ -4,6 +4,7 @@
 // rays they return the same cell sequences and segment lengths as the CPU code:
 //   CartesianExact  <- CartesianSpatialGrid::MySegmentGenerator::next   (CartesianSpatialGrid.cpp:77-155)
 //   OctreeExact     <- TreeSpatialGrid::MySegmentGenerator::next        (TreeSpatialGrid.cpp:143-228)
+//   AdaptiveMeshExact <- AdaptiveMeshSnapshot::MySegmentGenerator::next (AdaptiveMeshSnapshot.cpp:378-449)
 //   VoronoiExact    <- VoronoiMeshSnapshot::MySegmentGenerator::next    (VoronoiMeshSnapshot.cpp:1089-1222)
 //   TetraExact      <- TetraMeshSpatialGrid::MySegmentGenerator::next   (TetraMeshSpatialGrid.cpp:688-831)
 // and PathSegmentGenerator::moveInside (SKIRT/utils/PathSegmentGenerator.cpp:11-112).
@@ -37,6 +38,12 @@ struct GridDev
     const int* tNbBegin;
     const int* tNb;
     int tNodes;
+    // adaptive mesh (shares tBounds, tCell, tNbBegin, tNb with the octree, one neighbour per leaf
+    // wall): per node the subdivision nx, ny, nz (0 for leaves) and the first entry of its
+    // children in amChild (local Morton order, x fastest)
+    const int* amDiv;
+    const int* amChildBegin;
+    const int* amChild;
     // leaf-indexed 64-byte records of the production walker (four int4 per cell):
     //   [0] wall indices x lo|hi<<16, y, z (16 bits each, into the lattice wall tables), FP32 density
     //   [1] neighbour-list base, 9-bit cumulative wall offsets (64 bits), leaf node id
@@ -314,7 +321,61 @@ SKG_D int octreeLeafChild(const GridDev& g, double x, double y, double z)
     return -1;
 }
 
-struct OctreeExact : GenBase
+// AdaptiveMeshSnapshot::Node::leaf with Node::child (AdaptiveMeshSnapshot.cpp:103-145): the child
+// holding the point is estimated by Box::cellIndices over the node's nx x ny x nz subdivision and
+// corrected by one index per axis when the estimate does not contain the point. Returns -1 outside
+// the root; -2 where the reference stops with "Can't locate the appropriate child node".
+SKG_D int adaptiveLeaf(const GridDev& g, double x, double y, double z)
+{
+    if (!GenBase::boxContains(g.tBounds, x, y, z)) return -1;
+    int node = 0;
+    for (int guard = 0; guard < 256; ++guard)
+    {
+        const int* d = g.amDiv + 3 * static_cast<size_t>(node);
+        int nx = d[0], ny = d[1], nz = d[2];
+        if (nx == 0) return node;
+        const double* b = g.tBounds + 6 * static_cast<size_t>(node);
+        // Box::cellIndices (SKIRT/utils/Box.hpp:162-167)
+        int i = max(0, min(nx - 1, static_cast<int>(xmul(static_cast<double>(nx), xsub(x, b[0])) / xsub(b[3], b[0]))));
+        int j = max(0, min(ny - 1, static_cast<int>(xmul(static_cast<double>(ny), xsub(y, b[1])) / xsub(b[4], b[1]))));
+        int k = max(0, min(nz - 1, static_cast<int>(xmul(static_cast<double>(nz), xsub(z, b[2])) / xsub(b[5], b[2]))));
+        const int* kids = g.amChild + g.amChildBegin[node];
+        int c = kids[(k * ny + j) * nx + i];
+        const double* cb = g.tBounds + 6 * static_cast<size_t>(c);
+        if (!GenBase::boxContains(cb, x, y, z))
+        {
+            if (x < cb[0]) i--;
+            else if (x > cb[3]) i++;
+            if (y < cb[1]) j--;
+            else if (y > cb[4]) j++;
+            if (z < cb[2]) k--;
+            else if (z > cb[5]) k++;
+            if (i < 0 || i >= nx || j < 0 || j >= ny || k < 0 || k >= nz) return -2;
+            c = kids[(k * ny + j) * nx + i];
+            if (!GenBase::boxContains(g.tBounds + 6 * static_cast<size_t>(c), x, y, z)) return -2;
+        }
+        node = c;
+    }
+    return -2;
+}
+
+// the leaf search of a tree walker: the octree's (TreeNode::leafChild) or the adaptive mesh's
+template<bool Adaptive>
+SKG_D int treeLeaf(const GridDev& g, double x, double y, double z)
+{
+    if (Adaptive)
+    {
+        int l = adaptiveLeaf(g, x, y, z);
+        return l < 0 ? -1 : l;
+    }
+    return octreeLeafChild(g, x, y, z);
+}
+
+// TreeSpatialGrid::MySegmentGenerator::next (TreeSpatialGrid.cpp:143-228) and, with the adaptive
+// leaf search, AdaptiveMeshSnapshot::MySegmentGenerator::next (AdaptiveMeshSnapshot.cpp:378-449):
+// the same wall ties, step ds + eps, neighbour (list) then top-down search, nextafter escape.
+template<bool Adaptive>
+struct TreeExactT : GenBase
 {
     static constexpr int kMinBlocks = 3;
     static constexpr int kRefillMin = 16;  // waiting lanes before a warp takes new tasks
@@ -332,7 +393,7 @@ struct OctreeExact : GenBase
         if (state == GS_UNKNOWN)
         {
             if (!moveInside(g.ext, g.eps)) return false;
-            node = octreeLeafChild(g, rx, ry, rz);
+            node = treeLeaf<Adaptive>(g, rx, ry, rz);
             if (node < 0)
             {
                 state = GS_OUTSIDE;
@@ -368,7 +429,8 @@ struct OctreeExact : GenBase
         m = g.tCell[node];
         ds = d;
         int old = node;
-        // TreeNode::neighbor: first neighbour across the wall (overlap-sorted) containing r
+        // TreeNode::neighbor / Node::neighbor: the first neighbour across the wall (overlap-sorted
+        // for the octree, the single most likely one for the adaptive mesh) containing r
         int nb = -1;
         int e0 = g.tNbBegin[6 * node + wall], e1 = g.tNbBegin[6 * node + wall + 1];
         for (int e = e0; e < e1; ++e)
@@ -380,19 +442,22 @@ struct OctreeExact : GenBase
                 break;
             }
         }
-        if (nb < 0) nb = octreeLeafChild(g, rx, ry, rz);
+        if (nb < 0) nb = treeLeaf<Adaptive>(g, rx, ry, rz);
         if (nb == old)
         {
             rx = nextafter(rx, (kx < 0.) ? -DBL_MAX : DBL_MAX);
             ry = nextafter(ry, (ky < 0.) ? -DBL_MAX : DBL_MAX);
             rz = nextafter(rz, (kz < 0.) ? -DBL_MAX : DBL_MAX);
-            nb = octreeLeafChild(g, rx, ry, rz);
+            nb = treeLeaf<Adaptive>(g, rx, ry, rz);
         }
         node = nb;
         if (nb < 0 || nb == old) state = GS_OUTSIDE;
         return true;
     }
 };
+
+using OctreeExact = TreeExactT<false>;
+using AdaptiveMeshExact = TreeExactT<true>;
 
 // ---------------------------------------------------------------------------------------------
 // Voronoi

@@ -320,6 +320,13 @@ struct OctreeNodeFast : OctreeExact
     using Acc = float;
 };
 
+// Adaptive mesh, production: the reference-order FP64 walk (single neighbour per wall, top-down
+// fallback) with FP32 accumulators
+struct AdaptiveMeshFast : AdaptiveMeshExact
+{
+    using Acc = float;
+};
+
 // Nearest site of a point by a greedy walk on the neighbour graph (the Delaunay graph of the sites,
 // on which the walk towards ever nearer sites ends at the nearest one), starting from the
 // representative site of the point's block in the site-search grid. -1 outside the domain.

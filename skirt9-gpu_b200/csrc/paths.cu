@@ -24,6 +24,7 @@ cudaError_t launchTracePathsFP64(int precision, const GridDev& g, int n, const d
         case 6: tracePathsKernel<Sphere2DExact><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
         case 7: tracePathsKernel<Sphere3DExact><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
         case 8: tracePathsKernel<Cylinder3DExact><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
+        case 9: tracePathsKernel<AdaptiveMeshExact><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -46,6 +47,7 @@ cudaError_t launchOpticalDepthsFP64(int precision, const GridDev& g, const doubl
         case 6: opticalDepthKernel<Sphere2DExact><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
         case 7: opticalDepthKernel<Sphere3DExact><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
         case 8: opticalDepthKernel<Cylinder3DExact><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
+        case 9: opticalDepthKernel<AdaptiveMeshExact><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

@@ -29,6 +29,7 @@ cudaError_t launchTracePathsFP32(int precision, const GridDev& g, int n, const d
         case 6: tracePathsKernel<Sphere2DFast><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
         case 7: tracePathsKernel<Sphere3DFast><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
         case 8: tracePathsKernel<Cylinder3DFast><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
+        case 9: tracePathsKernel<AdaptiveMeshFast><<<blocks, threads, 0, s>>>(g, n, rays, maxSeg, count, m, ds, err); break;
         default: return cudaErrorNotSupported;
     }
     return cudaGetLastError();
@@ -56,6 +57,7 @@ cudaError_t launchOpticalDepthsFP32(int precision, const GridDev& g, const doubl
         case 6: opticalDepthKernel<Sphere2DFast><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
         case 7: opticalDepthKernel<Sphere3DFast><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
         case 8: opticalDepthKernel<Cylinder3DFast><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
+        case 9: opticalDepthKernel<AdaptiveMeshFast><<<blocks, threads, 0, s>>>(g, dens, section, n, rays, tau, err); break;
         default: return cudaErrorNotSupported;
     }
     return cudaGetLastError();

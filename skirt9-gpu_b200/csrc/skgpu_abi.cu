@@ -364,6 +364,151 @@ int skgpu_upload_grid_cartesian(skgpu_ctx* ctx, const double* xb, int32_t nxb, c
     return SKGPU_OK;
 }
 
+namespace {
+// AdaptiveMeshSnapshot::Node::leaf / child on the host (AdaptiveMeshSnapshot.cpp:103-145), over the
+// traversal arrays and the derived subdivisions: -1 outside the root, -2 where the reference stops
+// with "Can't locate the appropriate child node"
+int adaptiveLeafHost(const double* bounds, const int* div, const int* childBegin, const int* child, double x, double y,
+                     double z)
+{
+    auto contains = [&](int l) {
+        const double* b = bounds + 6 * static_cast<size_t>(l);
+        return x >= b[0] && x <= b[3] && y >= b[1] && y <= b[4] && z >= b[2] && z <= b[5];
+    };
+    if (!contains(0)) return -1;
+    int node = 0;
+    for (int guard = 0; guard < 256; ++guard)
+    {
+        int nx = div[3 * node], ny = div[3 * node + 1], nz = div[3 * node + 2];
+        if (nx == 0) return node;
+        const double* b = bounds + 6 * static_cast<size_t>(node);
+        int i = std::max(0, std::min(nx - 1, static_cast<int>(nx * (x - b[0]) / (b[3] - b[0]))));
+        int j = std::max(0, std::min(ny - 1, static_cast<int>(ny * (y - b[1]) / (b[4] - b[1]))));
+        int k = std::max(0, std::min(nz - 1, static_cast<int>(nz * (z - b[2]) / (b[5] - b[2]))));
+        const int* kids = child + childBegin[node];
+        int c = kids[(k * ny + j) * nx + i];
+        if (!contains(c))
+        {
+            const double* cb = bounds + 6 * static_cast<size_t>(c);
+            if (x < cb[0]) i--;
+            else if (x > cb[3]) i++;
+            if (y < cb[1]) j--;
+            else if (y > cb[4]) j++;
+            if (z < cb[2]) k--;
+            else if (z > cb[5]) k++;
+            if (i < 0 || i >= nx || j < 0 || j >= ny || k < 0 || k >= nz) return -2;
+            c = kids[(k * ny + j) * nx + i];
+            if (!contains(c)) return -2;
+        }
+        node = c;
+    }
+    return -2;
+}
+}  // namespace
+
+int skgpu_upload_grid_adaptive_mesh(skgpu_ctx* ctx, int32_t num_nodes, const double* bounds, const int32_t* cell_index,
+                                    const int32_t* child_begin, const int32_t* child_count, const int32_t* child_index,
+                                    int32_t num_child_index, double eps)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (num_nodes < 1 || !bounds || !cell_index || !child_begin || !child_count || (num_child_index > 0 && !child_index))
+        return fail(ctx, SKGPU_ERR_ARG, "adaptive mesh: missing arrays");
+    if (num_child_index < 0) return fail(ctx, SKGPU_ERR_ARG, "adaptive mesh: negative sizes");
+    if (!finiteAll(bounds, 6 * static_cast<size_t>(num_nodes))) return fail(ctx, SKGPU_ERR_ARG, "adaptive mesh: non-finite bounds");
+    if (!(eps > 0) || !std::isfinite(eps)) return fail(ctx, SKGPU_ERR_ARG, "adaptive mesh: bad eps");
+    // the subdivision of every nonleaf node from its children's bounds: the children form an
+    // nx x ny x nz lattice in local Morton order (x fastest), each the parent's Box::fracPos cell
+    std::vector<int> div(3 * static_cast<size_t>(num_nodes), 0);
+    std::vector<int> parents(num_nodes, 0);
+    int numCells = 0, numLeaves = 0;
+    for (int l = 0; l < num_nodes; ++l)
+    {
+        int cnt = child_count[l];
+        const double* b = bounds + 6 * static_cast<size_t>(l);
+        if (cnt == 0)
+        {
+            if (cell_index[l] < 0 || cell_index[l] >= num_nodes) return fail(ctx, SKGPU_ERR_ARG, "adaptive mesh: leaf without cell index");
+            numCells = std::max(numCells, cell_index[l] + 1);
+            numLeaves++;
+            continue;
+        }
+        int cb = child_begin[l];
+        if (cnt < 0 || cb < 0 || cb + cnt > num_child_index) return fail(ctx, SKGPU_ERR_ARG, "adaptive mesh: child index out of range");
+        const int* kids = child_index + cb;
+        for (int q = 0; q < cnt; ++q)
+        {
+            if (kids[q] <= 0 || kids[q] >= num_nodes) return fail(ctx, SKGPU_ERR_ARG, "adaptive mesh: child id out of range");
+            if (++parents[kids[q]] > 1) return fail(ctx, SKGPU_ERR_ARG, "adaptive mesh: a node is the child of two nodes");
+        }
+        const double* c0 = bounds + 6 * static_cast<size_t>(kids[0]);
+        int nx = 0, ny = 0, nz = 0;
+        for (int q = 0; q < cnt; ++q)
+        {
+            const double* c = bounds + 6 * static_cast<size_t>(kids[q]);
+            if (c[1] == c0[1] && c[2] == c0[2]) nx++;
+            if (c[0] == c0[0] && c[2] == c0[2]) ny++;
+            if (c[0] == c0[0] && c[1] == c0[1]) nz++;
+        }
+        if (nx * ny * nz != cnt) return fail(ctx, SKGPU_ERR_ARG, "adaptive mesh: children are not a lattice");
+        for (int k = 0; k < nz; ++k)
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i)
+                {
+                    // Box::fracPos(i, j, k, nx, ny, nz) and (i+1, j+1, k+1) (SKIRT/utils/Box.hpp:154-158)
+                    const double* c = bounds + 6 * static_cast<size_t>(kids[(k * ny + j) * nx + i]);
+                    double e[6] = {b[0] + i * (b[3] - b[0]) / nx, b[1] + j * (b[4] - b[1]) / ny, b[2] + k * (b[5] - b[2]) / nz,
+                                   b[0] + (i + 1) * (b[3] - b[0]) / nx, b[1] + (j + 1) * (b[4] - b[1]) / ny,
+                                   b[2] + (k + 1) * (b[5] - b[2]) / nz};
+                    for (int a = 0; a < 6; ++a)
+                        if (c[a] != e[a]) return fail(ctx, SKGPU_ERR_ARG, "adaptive mesh: children not in local Morton order");
+                }
+        div[3 * static_cast<size_t>(l)] = nx;
+        div[3 * static_cast<size_t>(l) + 1] = ny;
+        div[3 * static_cast<size_t>(l) + 2] = nz;
+    }
+    if (numCells != numLeaves) return fail(ctx, SKGPU_ERR_ARG, "adaptive mesh: cell indices are not 0..leaves-1");
+    for (int l = 1; l < num_nodes; ++l)
+        if (parents[l] != 1) return fail(ctx, SKGPU_ERR_ARG, "adaptive mesh: node unreachable from the root");
+    // Node::addNeighbors (AdaptiveMeshSnapshot.cpp:67-83): per leaf wall the leaf holding the point
+    // eps beyond the centre of the wall, in CSR form (no entry at domain walls)
+    std::vector<int32_t> nbBegin(6 * static_cast<size_t>(num_nodes) + 1, 0), nb;
+    for (int l = 0; l < num_nodes; ++l)
+    {
+        for (int w = 0; w < 6; ++w)
+        {
+            nbBegin[6 * static_cast<size_t>(l) + w] = static_cast<int32_t>(nb.size());
+            if (child_count[l] != 0) continue;
+            const double* b = bounds + 6 * static_cast<size_t>(l);
+            double cx = 0.5 * (b[0] + b[3]), cy = 0.5 * (b[1] + b[4]), cz = 0.5 * (b[2] + b[5]);
+            double x = cx + (w == 0 ? -eps : w == 1 ? eps : 0.);
+            double y = cy + (w == 2 ? -eps : w == 3 ? eps : 0.);
+            double z = cz + (w == 4 ? -eps : w == 5 ? eps : 0.);
+            int n = adaptiveLeafHost(bounds, div.data(), child_begin, child_index, x, y, z);
+            if (n == -2) return fail(ctx, SKGPU_ERR_ARG, "adaptive mesh: cannot locate a child node");
+            if (n >= 0) nb.push_back(n);
+        }
+    }
+    nbBegin[6 * static_cast<size_t>(num_nodes)] = static_cast<int32_t>(nb.size());
+    CK(cudaSetDevice(ctx->device));
+    freeGrid(ctx);
+    GridDev& g = ctx->g;
+    g.kind = SKGPU_GRID_ADAPTIVE_MESH;
+    for (int q = 0; q < 6; ++q) g.ext[q] = bounds[q];
+    g.eps = eps;
+    g.tNodes = num_nodes;
+    g.numCells = numCells;
+    int rc;
+    if ((rc = gridUpload(ctx, &g.tBounds, bounds, 6 * static_cast<size_t>(num_nodes)))) return rc;
+    if ((rc = gridUpload<int>(ctx, &g.tCell, cell_index, num_nodes))) return rc;
+    if ((rc = gridUpload<int>(ctx, &g.tNbBegin, nbBegin.data(), nbBegin.size()))) return rc;
+    if ((rc = gridUpload<int>(ctx, &g.tNb, nb.data(), nb.size()))) return rc;
+    if ((rc = gridUpload<int>(ctx, &g.amDiv, div.data(), div.size()))) return rc;
+    if ((rc = gridUpload<int>(ctx, &g.amChildBegin, child_begin, num_nodes))) return rc;
+    if ((rc = gridUpload<int>(ctx, &g.amChild, child_index, static_cast<size_t>(num_child_index)))) return rc;
+    ctx->hasGrid = true;
+    return SKGPU_OK;
+}
+
 int skgpu_upload_grid_octree(skgpu_ctx* ctx, int32_t num_nodes, const double* bounds, const int32_t* cell_index,
                              const int32_t* child_begin, const int32_t* child_count, const int32_t* child_index,
                              int32_t num_child_index, const int32_t* nb_begin, const int32_t* nb_index,
@@ -1549,8 +1694,9 @@ int skgpu_prepare_secondary(skgpu_ctx* ctx, const skgpu_secondary_options* opt, 
 {
     if (!ctx) return SKGPU_ERR_ARG;
     if (!opt || total_packets == 0) return fail(ctx, SKGPU_ERR_ARG, "secondary: missing options or packets");
-    if (!ctx->hasGrid || (ctx->g.kind != SKGPU_GRID_CARTESIAN && ctx->g.kind != SKGPU_GRID_OCTREE))
-        return fail(ctx, SKGPU_ERR_UNSUPPORTED, "secondary: dust emission needs a Cartesian or octree grid");
+    if (!ctx->hasGrid || (ctx->g.kind != SKGPU_GRID_CARTESIAN && ctx->g.kind != SKGPU_GRID_OCTREE
+                          && ctx->g.kind != SKGPU_GRID_ADAPTIVE_MESH))
+        return fail(ctx, SKGPU_ERR_UNSUPPORTED, "secondary: dust emission needs a Cartesian, octree or adaptive-mesh grid");
     if (!ctx->dens || ctx->numCells != ctx->g.numCells) return fail(ctx, SKGPU_ERR_STATE, "secondary: medium does not match the grid");
     if (!ctx->de.nrf || ctx->deCells != ctx->numCells || ctx->de.nrf != ctx->nrf)
         return fail(ctx, SKGPU_ERR_STATE, "secondary: dust emission tables do not match the medium and RF grid");
@@ -1600,7 +1746,8 @@ int skgpu_prepare_secondary(skgpu_ctx* ctx, const skgpu_secondary_options* opt, 
     CK(cudaMemcpy(ctx->secXv, xv.data(), npts * sizeof(double), cudaMemcpyHostToDevice));
     CK(launchDustCells(ctx->de, ctx->dens, ctx->rf, cells, ctx->secXv, npts, minRight, maxRight, ctx->secL, ctx->secT,
                        ctx->secPv, ctx->secCv, ctx->stream));
-    if (ctx->g.kind == SKGPU_GRID_OCTREE) CK(launchCellNodes(ctx->g.tCell, ctx->g.tNodes, ctx->secCellNode, ctx->stream));
+    if (ctx->g.kind == SKGPU_GRID_OCTREE || ctx->g.kind == SKGPU_GRID_ADAPTIVE_MESH)
+        CK(launchCellNodes(ctx->g.tCell, ctx->g.tNodes, ctx->secCellNode, ctx->stream));
     std::vector<double> Lv(cells);
     CK(cudaMemcpyAsync(Lv.data(), ctx->secL, cells * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));

@@ -24,6 +24,7 @@ cudaError_t runWaveFP32(int gridKind, const Wave& w, int numSMs, cudaStream_t s,
         case 6: return runWave<Sphere2DFast>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer, cache);
         case 7: return runWave<Sphere3DFast>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer, cache);
         case 8: return runWave<Cylinder3DFast>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer, cache);
+        case 9: return runWave<AdaptiveMeshFast>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer, cache);
     }
     return cudaErrorNotSupported;
 }

@@ -21,6 +21,7 @@ cudaError_t runWaveFP64(int gridKind, const Wave& w, int numSMs, cudaStream_t s,
         case 6: return runWave<Sphere2DExact>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer, cache);
         case 7: return runWave<Sphere3DExact>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer, cache);
         case 8: return runWave<Cylinder3DExact>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer, cache);
+        case 9: return runWave<AdaptiveMeshExact>(w, numSMs, s, doneHost, passes, maxPasses, useGraph, timer, cache);
     }
     return cudaErrorInvalidValue;
 }

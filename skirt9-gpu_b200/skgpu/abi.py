@@ -17,7 +17,7 @@ LIB_PATH = os.path.join(PKG_ROOT, "lib", "libskgpu.so")
 # status codes
 OK, ERR_ARG, ERR_CUDA, ERR_STATE, ERR_TIMEOUT, ERR_DEVICE, ERR_UNSUPPORTED = range(7)
 (GRID_CARTESIAN, GRID_OCTREE, GRID_VORONOI, GRID_TETRA, GRID_SPHERE1D, GRID_CYLINDER2D, GRID_SPHERE2D, GRID_SPHERE3D,
- GRID_CYLINDER3D) = range(9)
+ GRID_CYLINDER3D, GRID_ADAPTIVE_MESH) = range(10)
 PREC_FP64_EXACT, PREC_FP32 = 0, 1
 SRC_POINT, SRC_EXPDISK, SRC_RADIAL, SRC_RADIAL_LOGLOG = 0, 1, 2, 3
 SPEC_DISCRETE, SPEC_TABLE = 0, 1
@@ -123,6 +123,7 @@ SIGNATURES = {
     "last_error": [_P],
     "upload_grid_cartesian": [_P, _P, _I, _P, _I, _P, _I],
     "upload_grid_octree": [_P, _I, _P, _P, _P, _P, _P, _I, _P, _P, _I, _D],
+    "upload_grid_adaptive_mesh": [_P, _I, _P, _P, _P, _P, _P, _I, _D],
     "upload_grid_voronoi": [_P, _I, _P, _P, _P, _I, _P, _D],
     "upload_grid_tetra": [_P, _I, _P, _I, _P, _P, _P, _P, _P, _D],
     "upload_grid_sphere1d": [_P, _I, _P],
@@ -252,6 +253,11 @@ class Backend:
                                        i32(child_index), i32(nb_begin), i32(nb_index))
         self.call("upload_grid_octree", len(ci), _ptr(b), _ptr(ci), _ptr(cb), _ptr(cc), _ptr(cx), len(cx),
                   _ptr(nbb), _ptr(nbi), len(nbi), float(eps))
+
+    def upload_grid_adaptive_mesh(self, bounds, cell_index, child_begin, child_count, child_index, eps):
+        b, ci, cb, cc, cx = f64(bounds), i32(cell_index), i32(child_begin), i32(child_count), i32(child_index)
+        self.call("upload_grid_adaptive_mesh", len(ci), _ptr(b), _ptr(ci), _ptr(cb), _ptr(cc), _ptr(cx), len(cx),
+                  float(eps))
 
     def upload_grid_voronoi(self, sites, nb_begin, nb_index, extent, eps):
         s, nbb, nbi, ext = f64(sites), i32(nb_begin), i32(nb_index), f64(extent)

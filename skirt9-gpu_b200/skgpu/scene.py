@@ -91,6 +91,9 @@ class Scene:
         elif k == abi.GRID_OCTREE:
             be.upload_grid_octree(g["bounds"], g["cell_index"], g["child_begin"], g["child_count"], g["child_index"],
                                   g["nb_begin"], g["nb_index"], g["eps"])
+        elif k == abi.GRID_ADAPTIVE_MESH:
+            be.upload_grid_adaptive_mesh(g["bounds"], g["cell_index"], g["child_begin"], g["child_count"],
+                                         g["child_index"], g["eps"])
         elif k == abi.GRID_VORONOI:
             be.upload_grid_voronoi(g["sites"], g["nb_begin"], g["nb_index"], g["extent"], g["eps"])
         elif k == abi.GRID_TETRA:
@@ -338,6 +341,10 @@ class Scene:
                            child_begin=L("tree_child_begin"), child_count=L("tree_child_count"),
                            child_index=L("tree_child_index"), nb_begin=L("tree_nb_begin"),
                            nb_index=L("tree_nb_index"), eps=float(meta["eps"]), extent=ext)
+        elif kind == "adaptive":
+            sc.grid = dict(kind=abi.GRID_ADAPTIVE_MESH, bounds=L("am_bounds"), cell_index=L("am_cell_index"),
+                           child_begin=L("am_child_begin"), child_count=L("am_child_count"),
+                           child_index=L("am_child_index"), eps=float(meta["eps"]), extent=ext)
         elif kind == "voronoi":
             sc.grid = dict(kind=abi.GRID_VORONOI, sites=L("vor_sites"), nb_begin=L("vor_nb_begin"),
                            nb_index=L("vor_nb_index"), extent=ext, eps=float(meta["eps"]))

@@ -5,6 +5,7 @@ disk galaxy on an octree, Voronoi and tetrahedral meshes, the edge-on thick disk
 reference CPU code and this tracer run the same configuration. Element and attribute names are
 those of the reference's schema (`skirt -x`, registered in SKIRT/core/SimulationItemRegistry.cpp).
 """
+import math
 
 PC = 3.0856775814913673e16  # m, SKIRT Constants::pc()
 
@@ -449,3 +450,56 @@ def galaxy_levels_bands(num_packets=30000, npix=16, nlambda=10, max_level=5, max
                                     wlg=band_grid(bands or TEST_BANDS)))
     return simulation("ExtinctionOnly", num_packets, sources, expdisk_medium(6, 0.2, "kpc", 1.0, mix),
                       octree_grid(25, "kpc", max_level, max_dust_fraction), instruments, instrument_wlg=wlg)
+
+
+def adaptive_mesh_text(half_pc=4.0, root=(4, 4, 2), max_level=3, rho0=2000.0, hR=1.0, hz=0.2):
+    """An adaptive-mesh data file (the text format AdaptiveMeshSnapshot reads: "! nx ny nz" lines for
+    subdivided nodes, one density row per leaf, children in local Morton order with x fastest) of an
+    exponential disk of mass density rho0 * exp(-R/hR - |z|/hz) Msun/pc3 on the cube of half size
+    half_pc. The root is split root = (nx, ny, nz); nodes near the disk are refined up to max_level
+    with subdivisions that vary by level (2x2x2, 3x3x1, 1x2x3), so that the mesh exercises
+    non-cubic splits."""
+    splits = {1: (2, 2, 2), 2: (3, 3, 1), 3: (1, 2, 3)}
+    lines = ["# adaptive mesh: exponential disk", "# column 1: mass density (Msun/pc3)"]
+
+    def node(b, level):
+        (x0, y0, z0), (x1, y1, z1) = b
+        cx, cy, cz = 0.5 * (x0 + x1), 0.5 * (y0 + y1), 0.5 * (z0 + z1)
+        size = max(x1 - x0, y1 - y0, z1 - z0)
+        near = (cx * cx + cy * cy) ** 0.5 < 2.0 * hR + size and abs(cz) < 3.0 * hz + size
+        div = root if level == 0 else (splits.get(level) if near and level <= max_level else None)
+        if div is None:
+            lines.append(f"{rho0 * math.exp(-((cx * cx + cy * cy) ** 0.5) / hR - abs(cz) / hz):.9e}")
+            return
+        nx, ny, nz = div
+        lines.append(f"! {nx} {ny} {nz}")
+        for k in range(nz):
+            for j in range(ny):
+                for i in range(nx):
+                    lo = (x0 + i * (x1 - x0) / nx, y0 + j * (y1 - y0) / ny, z0 + k * (z1 - z0) / nz)
+                    hi = (x0 + (i + 1) * (x1 - x0) / nx, y0 + (j + 1) * (y1 - y0) / ny, z0 + (k + 1) * (z1 - z0) / nz)
+                    node((lo, hi), level + 1)
+
+    h = half_pc
+    node(((-h, -h, -h), (h, h, h)), 0)
+    return "\n".join(lines) + "\n"
+
+
+def adaptive_mesh_medium(filename, half_pc, mix):
+    h = half_pc
+    return (f'<AdaptiveMeshMedium filename="{filename}" minX="{-h} pc" maxX="{h} pc" minY="{-h} pc" maxY="{h} pc" '
+            f'minZ="{-h} pc" maxZ="{h} pc" massType="MassDensity" massFraction="1" importMetallicity="false" '
+            f'importTemperature="false" maxTemperature="0 K" importVelocity="false" importMagneticField="false" '
+            f'importVariableMixParams="false" useColumns=""><materialMix type="MaterialMix">{mix}</materialMix>'
+            f'</AdaptiveMeshMedium>')
+
+
+def disk_adaptive(num_packets=1e5, filename="mesh.txt", npix=32, stats=True, half_pc=4.0):
+    """The disk scene (central point source, one 60-degree frame of 8 pc with statistics plus one SED)
+    on an AdaptiveMeshSpatialGrid of an imported AdaptiveMeshMedium (adaptive_mesh_text in
+    `filename`, next to the ski file)."""
+    mix = mean_list_mix([0.5, 0.6], [1, 1], [0.5, 0.5], [0.6, 0.6])
+    return simulation("OligoExtinctionOnly", num_packets, point_source(), adaptive_mesh_medium(filename, half_pc, mix),
+                      "<AdaptiveMeshSpatialGrid/>",
+                      frame_instrument("i60", 60, 2 * half_pc, "pc", npix, stats) + sed_instrument("sed", 60, stats),
+                      num_density_samples=10)

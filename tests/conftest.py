@@ -37,7 +37,7 @@ def gpu_backend():
     be.close()
 
 
-PATH_FIXTURES = ["cartesian_selftest", "cartesian_c16", "octree", "voronoi", "tetra", "sphere1d", "cylinder2d", "sphere2d", "sphere3d", "cylinder3d"]
+PATH_FIXTURES = ["cartesian_selftest", "cartesian_c16", "octree", "voronoi", "tetra", "sphere1d", "cylinder2d", "sphere2d", "sphere3d", "cylinder3d", "adaptive"]
 
 
 def segments_of(z, r):

@@ -17,8 +17,8 @@ Fixtures written:
                      (forced and free propagation), 2e5 packets each; `python
                      tests/golden/make_fixtures.py explicit` writes only this one
   paths_sphere1d.npz, paths_cylinder2d.npz, paths_sphere2d.npz, paths_sphere3d.npz,
-  paths_cylinder3d.npz  path fixtures that also hold reference frame/SED statistics of the same
-                     scene (arguments `sphere1d`, `cylinder2d`, `sphere2d`, `sphere3d`, `cylinder3d`
+  paths_cylinder3d.npz, paths_adaptive.npz  path fixtures that also hold reference frame/SED statistics of the same
+                     scene (arguments `sphere1d`, `cylinder2d`, `sphere2d`, `sphere3d`, `cylinder3d`, `adaptive`
                      write only them)
   stats_octree.npz, stats_voronoi.npz, stats_tetra.npz  the disk scene on these grids (scene export)
                      with reference frame/SED statistics (argument `gridstats`)
@@ -50,17 +50,20 @@ OUT = os.path.dirname(os.path.abspath(__file__))
 PC = 3.08567758e16  # SKIRT's parsec in m
 
 
-def export(ski_text, tmp, rays=None, max_seg=512, lam=0.55e-6):
+def export(ski_text, tmp, rays=None, max_seg=512, lam=0.55e-6, files=None):
     ski_path = os.path.join(tmp, "scene.ski")
     with open(ski_path, "w") as f:
         f.write(ski_text)
+    for name, text in (files or {}).items():
+        with open(os.path.join(tmp, name), "w") as f:
+            f.write(text)
     exp = os.path.join(tmp, "export")
     os.makedirs(exp, exist_ok=True)
     args = [os.path.join(BIN, "skirt_export"), ski_path, exp]
     if rays is not None:
         np.save(os.path.join(tmp, "rays.npy"), rays)
         args += [os.path.join(tmp, "rays.npy"), str(max_seg), repr(lam)]
-    subprocess.run(args, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+    subprocess.run(args, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL, cwd=tmp)
     data = {}
     for fn in os.listdir(exp):
         if fn.endswith(".npy"):
@@ -86,9 +89,9 @@ def random_rays(rng, n, half, out_frac=0.3):
     return np.vstack([np.hstack([pos, d]), np.array(special)])
 
 
-def path_fixture(name, ski_text, rays, max_seg=512):
+def path_fixture(name, ski_text, rays, max_seg=512, files=None):
     with tempfile.TemporaryDirectory() as tmp:
-        data = export(ski_text, tmp, rays, max_seg)
+        data = export(ski_text, tmp, rays, max_seg, files=files)
     data["rays"] = rays
     # keep the segments ragged: ray r owns ray_m[off[r]:off[r+1]] (no truncated paths allowed)
     cnt = data["ray_count"]
@@ -274,6 +277,24 @@ def cylinder3d_fixture(rng=None):
     reference_stats("paths_cylinder3d.npz", ski.disk_cylinder3d(200000), "i60", 200000)
 
 
+def adaptive_fixture(rng=None):
+    """AdaptiveMeshSpatialGrid of an imported AdaptiveMeshMedium (ski.adaptive_mesh_text: a 4x4x2
+    root, then 2x2x2, 3x3x1 and 1x2x3 subdivisions near the disk, 5488 leaves, 8 pc box): scene export
+    and path fixture (random rays, starts outside, rays along the axes and node walls through the
+    centre), and reference statistics of a single-threaded 2e5-packet run."""
+    rng = rng if rng is not None else np.random.default_rng(20260107)
+    files = {"mesh.txt": ski.adaptive_mesh_text()}
+    rays = random_rays(rng, 300, 4.0 * PC)
+    extra = []
+    for k in ((1, 0, 0), (0, 1, 0), (0, 0, -1), (1, 1, 0), (0.3, 0.0, 0.95), (-0.5, 0.5, -0.7071067811865476)):
+        k = np.array(k, float) / np.linalg.norm(k)
+        for p in ((0.0, 0.0, 0.0), (1.0, 0.5, 0.0), (0.0, 2.0, 0.5), (-3.0, -1.0, 0.25), (5.0, 0.0, 0.1)):
+            extra.append(np.r_[np.array(p) * PC, k])
+    rays = np.vstack([rays, np.array(extra)])
+    path_fixture("adaptive", ski.disk_adaptive(1e4), rays, files=files)
+    reference_stats("paths_adaptive.npz", ski.disk_adaptive(200000), "i60", 200000, files=files)
+
+
 def grid_stats_fixtures():
     """The disk scene on the octree, Voronoi and tetrahedral grids of the path fixtures (4 pc box):
     scene exports plus the statistics of single-threaded 2e5-packet reference runs
@@ -382,7 +403,7 @@ def dust_fixtures():
         print(f"{name}: {len(data['medium_density'])} cells, {npp} packets per segment")
 
 
-def reference_stats(fixture, ski_text, frame_name, npp):
+def reference_stats(fixture, ski_text, frame_name, npp, files=None):
     """Adds the frame and SED statistics of a single-threaded reference run of ski_text to a
     fixture; the run's stats scale c is recovered from its total image (MJy/sr per raw W from the
     SED's Jy per raw W of the shell_c16 run, same distance, and this frame's pixel)."""
@@ -394,6 +415,9 @@ def reference_stats(fixture, ski_text, frame_name, npp):
     with tempfile.TemporaryDirectory() as tmp:
         with open(os.path.join(tmp, "r.ski"), "w") as f:
             f.write(ski_text)
+        for name, text in (files or {}).items():
+            with open(os.path.join(tmp, name), "w") as f:
+                f.write(text)
         subprocess.run([os.path.join(BIN, "skirt"), "-t", "1", "r.ski"], cwd=tmp, check=True,
                        stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
         st = np.array([fits.read(os.path.join(tmp, f"r_{frame_name}_stats{k}.fits"))[0][0] for k in range(5)])
@@ -437,6 +461,8 @@ if __name__ == "__main__":
         sphere3d_fixture()
     elif sys.argv[1:] == ["cylinder3d"]:
         cylinder3d_fixture()
+    elif sys.argv[1:] == ["adaptive"]:
+        adaptive_fixture()
     elif sys.argv[1:] == ["gridstats"]:
         grid_stats_fixtures()
     elif sys.argv[1:] == ["galaxy"]:

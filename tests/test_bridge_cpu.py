@@ -21,9 +21,9 @@ needs_build = pytest.mark.skipif(not os.path.exists(SKIRT_ORACLE) or not os.path
                                         "where the reference sources are)")
 
 
-def both(tmp_path, text, name):
-    log = tb.run(SKIRT_ORACLE, text, name, str(tmp_path / "bridge"), ["-g", "-t", "1"])
-    tb.run(tb.SKIRT, text, name, str(tmp_path / "cpu"), ["-t", "1"])
+def both(tmp_path, text, name, files=None):
+    log = tb.run(SKIRT_ORACLE, text, name, str(tmp_path / "bridge"), ["-g", "-t", "1"], files)
+    tb.run(tb.SKIRT, text, name, str(tmp_path / "cpu"), ["-t", "1"], files)
     assert "primary histories on the B200" in log
     return log, str(tmp_path / "bridge"), str(tmp_path / "cpu")
 
@@ -69,6 +69,16 @@ def test_bridge_levels_and_bands_on_oracle(tmp_path):
     the reference program's."""
     log, g, c = both(tmp_path, ski.galaxy_levels_bands(200000), "lb")
     tb.check_levels_and_bands(g, c, "lb")
+
+
+@needs_build
+@pytest.mark.parametrize("grid", sorted(tb.GRID_SCENES))
+def test_bridge_grids_on_oracle(tmp_path, grid):
+    """The disk scene on the adaptive-mesh, Voronoi, tetrahedral, spherical and cylindrical grids:
+    the bridge's flattening of each grid through the oracle against the reference program."""
+    text, files = tb.GRID_SCENES[grid](50000)
+    log, g, c = both(tmp_path, text, "disk", files)
+    tb.check_disk(g, c, "disk")
 
 
 @needs_build

@@ -29,10 +29,13 @@ needs_build = pytest.mark.skipif(not os.path.exists(SKIRT_GPU) or not os.path.ex
                                         "run by __graft_entry__.build() where the reference sources are)")
 
 
-def run(exe, text, name, cwd, args):
+def run(exe, text, name, cwd, args, files=None):
     os.makedirs(cwd, exist_ok=True)
     with open(os.path.join(cwd, name + ".ski"), "w") as f:
         f.write(text)
+    for fn, content in (files or {}).items():
+        with open(os.path.join(cwd, fn), "w") as f:
+            f.write(content)
     p = subprocess.run([exe] + args + [name + ".ski"], cwd=cwd, capture_output=True, text=True, timeout=900)
     assert p.returncode == 0, p.stdout[-3000:] + p.stderr[-3000:]
     with open(os.path.join(cwd, name + "_log.txt")) as f:
@@ -69,12 +72,12 @@ def frame_z(da, db, name, instr):
     return z_of(out[0][0], out[0][1], out[1][0], out[1][1]), out
 
 
-def both(tmp_path, text, name):
+def both(tmp_path, text, name, files=None):
     # the reference runs single-threaded: its multi-threaded runs sample the cell densities from
     # randomly seeded threads, so their medium differs from run to run (and from the bridge's, which
     # takes the densities of its own single-threaded setup)
-    log = run(SKIRT_GPU, text, name, str(tmp_path / "gpu"), ["-g", "-t", "1"])
-    run(SKIRT, text, name, str(tmp_path / "cpu"), ["-t", "1"])
+    log = run(SKIRT_GPU, text, name, str(tmp_path / "gpu"), ["-g", "-t", "1"], files)
+    run(SKIRT, text, name, str(tmp_path / "cpu"), ["-t", "1"], files)
     assert "B200 photon-packet life cycle" in log
     assert "primary histories on the B200" in log
     return log, str(tmp_path / "gpu"), str(tmp_path / "cpu")
@@ -136,6 +139,35 @@ def test_bridge_levels_and_bands(tmp_path):
     """Scattering levels and a band wavelength grid on the B200 through SKIRT's own program."""
     log, g, c = both(tmp_path, ski.galaxy_levels_bands(200000), "lb")
     check_levels_and_bands(g, c, "lb")
+
+
+# the disk scene on every other grid kind the bridge hands over (name, ski text, input files)
+GRID_SCENES = {
+    "adaptive": lambda n: (ski.disk_adaptive(n), {"mesh.txt": ski.adaptive_mesh_text()}),
+    "voronoi": lambda n: (ski.disk_scene(ski.voronoi_grid(4, "pc", 2000), n), None),
+    "tetra": lambda n: (ski.disk_scene(ski.tetra_grid(4, "pc", 2000), n), None),
+    "sphere2d": lambda n: (ski.disk_sphere2d(n), None),
+    "sphere3d": lambda n: (ski.disk_sphere3d(n), None),
+    "cylinder2d": lambda n: (ski.disk_cylinder2d(n), None),
+    "cylinder3d": lambda n: (ski.disk_cylinder3d(n), None),
+}
+
+
+def check_disk(g, c, name):
+    z, _ = frame_z(g, c, name, "i60")
+    check(z, 1.4, 6.0)
+    z, _ = sed_z(g, c, name, "sed")
+    assert len(z) == 1 and abs(z[0]) < 4.5
+
+
+@needs_build
+@pytest.mark.parametrize("grid", sorted(GRID_SCENES))
+def test_bridge_grids(tmp_path, grid):
+    """The disk scene on the adaptive-mesh, Voronoi, tetrahedral, spherical and cylindrical grids
+    through skirt_gpu -g: frame and SED against the reference program's run."""
+    text, files = GRID_SCENES[grid](200000)
+    log, g, c = both(tmp_path, text, "disk", files)
+    check_disk(g, c, "disk")
 
 
 @needs_build

@@ -101,7 +101,7 @@ def test_gpu_free_propagation_matches_reference(golden, gpu_backend):
         assert abs(zscores(sst[1:2], sst[2:3], n, rs[1:2, 0], rs[2:3, 0], n)[0]) < 4
 
 
-@pytest.mark.parametrize("name", ["octree", "voronoi", "tetra", "cartesian_selftest", "sphere1d", "cylinder2d", "sphere2d", "sphere3d", "cylinder3d"])
+@pytest.mark.parametrize("name", ["octree", "voronoi", "tetra", "cartesian_selftest", "sphere1d", "cylinder2d", "sphere2d", "sphere3d", "cylinder3d", "adaptive"])
 def test_gpu_lifecycle_matches_oracle_grids(golden, gpu_backend, oracle_backend, name):
     sc = Scene.from_export(golden(f"paths_{name}.npz"))
     sc.instruments[0]["stats"] = 1
@@ -169,7 +169,7 @@ def test_gpu_edge_cases(golden, gpu_backend):
         gpu_backend.upload_grid_cartesian([0, 1], [1, 0], [0, 1])  # descending borders
 
 
-@pytest.mark.parametrize("name", ["cartesian_selftest", "cartesian_c16", "octree"])
+@pytest.mark.parametrize("name", ["cartesian_selftest", "cartesian_c16", "octree", "adaptive"])
 def test_gpu_production_paths_equal_reference(golden, gpu_backend, name):
     """Production Cartesian and octree walkers (the reference's FP64 geometry with the quotient from
     the reciprocal direction, 64-byte octree leaf records with lattice wall tables): cell sequences
@@ -323,10 +323,11 @@ def test_gpu_fp32_octree_lifecycle_close_to_fp64(gpu_backend):
     assert np.median(np.abs(r32.rf[lit] / r64.rf[lit] - 1)) < 1e-3
 
 
-@pytest.mark.parametrize("name", ["sphere1d", "cylinder2d", "sphere2d", "sphere3d", "cylinder3d"])
+@pytest.mark.parametrize("name", ["sphere1d", "cylinder2d", "sphere2d", "sphere3d", "cylinder3d", "adaptive"])
 def test_gpu_curvilinear_lifecycle_matches_reference_statistics(golden, gpu_backend, name):
-    """The dust shell on a Sphere1DSpatialGrid and the dust disk on a Cylinder2DSpatialGrid, both
-    traversal precisions: frame and SED against the reference's own run of the same scene."""
+    """The dust shell on a Sphere1DSpatialGrid, the dust disk on the cylindrical, spherical and
+    adaptive-mesh grids, both traversal precisions: frame and SED against the reference's own run
+    of the same scene."""
     z = golden(f"paths_{name}.npz")
     sc = Scene.from_export(z)
     sc.instruments[0]["stats"] = 1

@@ -136,7 +136,7 @@ def test_oracle_explicit_absorption_matches_reference_statistics(golden, oracle_
     assert abs(zsed[0]) < 4
 
 
-@pytest.mark.parametrize("name", ["sphere1d", "cylinder2d", "sphere2d", "sphere3d", "cylinder3d"])
+@pytest.mark.parametrize("name", ["sphere1d", "cylinder2d", "sphere2d", "sphere3d", "cylinder3d", "adaptive"])
 def test_oracle_curvilinear_lifecycle_matches_reference_statistics(golden, oracle_backend, name):
     """The dust shell on a Sphere1DSpatialGrid and the dust disk on a Cylinder2DSpatialGrid: the
     oracle's frame and SED against the reference's own run of the same scene (z-scores)."""
