@@ -394,12 +394,13 @@ def shell_cartesian(num_packets=1e6, nbins=64, npix=256, stats=True, points=None
                       explicit_absorption=explicit_absorption, force_scattering=force_scattering)
 
 
-def dust_shell(num_packets=1e6, nbins=16, npix=32, stats=True, nlambda=20, num_em=30, grid=None):
+def dust_shell(num_packets=1e6, nbins=16, npix=32, stats=True, nlambda=20, num_em=30, grid=None, medium=None):
     """The dust shell of shell_cartesian with dust emission (DustEmission mode): a 5800 K black-body
     point source of 1e5 Lsun (0.1-10 micron), power-law MeanListDustMix on 40 log wavelengths 0.1-1000
     micron, radiation field on `nlambda` log bins 0.1-10 micron, equilibrium dust emission on `num_em`
     log bins 1-1000 micron, a 32^2 frame at 30 degrees and an SED instrument at 30 degrees on 30 log
-    bins 0.1-1000 micron (statistics on). `grid` replaces the Cartesian grid."""
+    bins 0.1-1000 micron (statistics on). `grid` replaces the Cartesian grid, `medium` (a function of
+    the mix XML) the shell medium."""
     lam = [0.1 * (1e4 ** (i / 39)) for i in range(40)]
     kappa = [(l / 0.55) ** -1.0 for l in lam]
     albedo = [min(0.9, max(0.01, 0.5 * (l / 0.55) ** -0.5)) for l in lam]
@@ -407,7 +408,8 @@ def dust_shell(num_packets=1e6, nbins=16, npix=32, stats=True, nlambda=20, num_e
     mix = mean_list_mix(lam, kappa, albedo, g)
     rf_wlg = f'<LogWavelengthGrid minWavelength="0.1 micron" maxWavelength="10 micron" numWavelengths="{nlambda}"/>'
     iwlg = '<LogWavelengthGrid minWavelength="0.1 micron" maxWavelength="1000 micron" numWavelengths="30"/>'
-    return simulation("DustEmission", num_packets, point_source(luminosity_lsun=1e5), shell_medium(0.1, 1, 2, 2, mix),
+    med = medium(mix) if medium else shell_medium(0.1, 1, 2, 2, mix)
+    return simulation("DustEmission", num_packets, point_source(luminosity_lsun=1e5), med,
                       grid or cartesian_grid(1, nbins), frame_instrument("i30", 30, 2, "pc", npix, stats)
                       + sed_instrument("sed", 30, stats, comps=False), instrument_wlg=iwlg, store_rf=True,
                       rf_wlg=rf_wlg, emission=dust_emission_options(num_em=num_em))
@@ -503,3 +505,12 @@ def disk_adaptive(num_packets=1e5, filename="mesh.txt", npix=32, stats=True, hal
                       "<AdaptiveMeshSpatialGrid/>",
                       frame_instrument("i60", 60, 2 * half_pc, "pc", npix, stats) + sed_instrument("sed", 60, stats),
                       num_density_samples=10)
+
+
+def dust_adaptive(num_packets=1e5):
+    """DustEmission (the dust_shell configuration) on an AdaptiveMeshSpatialGrid: an imported
+    adaptive-mesh disk (hR 0.25 pc, hz 0.05 pc) in the +-1 pc box around the 1e5 Lsun point source.
+    Returns the ski text and its input files."""
+    text = dust_shell(num_packets, grid="<AdaptiveMeshSpatialGrid/>",
+                      medium=lambda mix: adaptive_mesh_medium("mesh.txt", 1.0, mix))
+    return text, {"mesh.txt": adaptive_mesh_text(half_pc=1.0, hR=0.25, hz=0.05, rho0=500.0)}

@@ -72,6 +72,17 @@ def test_bridge_levels_and_bands_on_oracle(tmp_path):
 
 
 @needs_build
+def test_bridge_dust_emission_adaptive_on_oracle(tmp_path):
+    """Primary and secondary segments on an adaptive mesh (the secondary launch in its leaf boxes)."""
+    text, files = ski.dust_adaptive(50000)
+    log, g, c = both(tmp_path, text, "dust", files)
+    assert "secondary histories on the B200" in log
+    z, (a, b) = tb.sed_z(g, c, "dust", "sed")
+    assert len(z) > 25
+    tb.check(z, 2.0, 5.0)
+
+
+@needs_build
 @pytest.mark.parametrize("grid", sorted(tb.GRID_SCENES))
 def test_bridge_grids_on_oracle(tmp_path, grid):
     """The disk scene on the adaptive-mesh, Voronoi, tetrahedral, spherical and cylindrical grids:

@@ -161,6 +161,19 @@ def check_disk(g, c, name):
 
 
 @needs_build
+def test_bridge_dust_emission_adaptive(tmp_path):
+    """DustEmission on an adaptive mesh: both segments on the B200, secondary launches in leaf boxes."""
+    text, files = ski.dust_adaptive(200000)
+    log, g, c = both(tmp_path, text, "dust", files)
+    assert "secondary histories on the B200" in log
+    z, (a, b) = sed_z(g, c, "dust", "sed")
+    assert len(z) > 25
+    check(z, 2.0, 5.0)
+    z, _ = frame_z(g, c, "dust", "i30")
+    check(z, 1.3, 6.0)
+
+
+@needs_build
 @pytest.mark.parametrize("grid", sorted(GRID_SCENES))
 def test_bridge_grids(tmp_path, grid):
     """The disk scene on the adaptive-mesh, Voronoi, tetrahedral, spherical and cylindrical grids
