@@ -1,6 +1,6 @@
 """Throughput benchmark of the photon-packet life cycle: packets/s on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference|reference-gpu] [--workload NAME]
 
 One step = one primary-emission segment of the workload's packets through the C ABI
 (skgpu_run_primary): launch, emission peel-off, forced-scattering propagation, radiation-field
@@ -30,6 +30,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path[:0] = [os.path.join(ROOT, "skirt9-gpu_b200"), os.path.join(ROOT, "oracle")]
 
 REF_SKIRT = os.path.join(ROOT, "oracle", "_ref", "exe", "skirt", "bin", "skirt")
+# the reference's own GPU layer (GpuAcceleration, run with -g): the reference program built with its
+# driver-symbol loader preferring the versioned CUDA entry points (oracle/patch_refgpu.py)
+REF_SKIRT_GPU = os.path.join(ROOT, "oracle", "_ref", "exe", "skirt", "bin", "skirt_refgpu")
 
 WORKLOADS = {
     # name: (description, packets per step per GPU)
@@ -130,9 +133,10 @@ def trace_algorithmic_bytes(counters, grid_kind):
     return BYTES_PER_CROSSING[grid_kind] * counters["crossings"] + 16 * counters["rf_stores"]
 
 
-def reference_run(scene_ski, npp, threads, files=None):
-    """Runs the reference CPU code on a ski file (plus input files {name: text} beside it); returns
-    (packets/s of the primary segment, secs)."""
+def reference_run(scene_ski, npp, threads, files=None, gpu=False):
+    """Runs the reference CPU code on a ski file (plus input files {name: text} beside it), or with
+    `gpu` the reference's own GPU layer (`skirt_refgpu -g`); returns (packets/s of the primary
+    segment, secs)."""
     with tempfile.TemporaryDirectory() as tmp:
         path = os.path.join(tmp, "bench.ski")
         with open(path, "w") as f:
@@ -140,9 +144,22 @@ def reference_run(scene_ski, npp, threads, files=None):
         for fname, text in (files or {}).items():
             with open(os.path.join(tmp, fname), "w") as f:
                 f.write(text)
-        out = subprocess.run([REF_SKIRT, "-t", str(threads), "bench.ski"], cwd=tmp, capture_output=True, text=True)
+        env = dict(os.environ)
+        cmd = [REF_SKIRT, "-t", str(threads), "bench.ski"]
+        if gpu:
+            cmd = [REF_SKIRT_GPU, "-g", "-t", str(threads), "bench.ski"]
+            nvrtc = "/usr/local/cuda/lib64/libnvrtc.so"
+            if "SKIRTGPU_NVRTC_LIBRARY" not in env and os.path.exists(nvrtc):
+                env["SKIRTGPU_NVRTC_LIBRARY"] = nvrtc
+        out = subprocess.run(cmd, cwd=tmp, capture_output=True, text=True, env=env)
         if out.returncode != 0:
             raise RuntimeError("reference run failed: " + out.stdout[-500:] + out.stderr[-500:])
+        if gpu:
+            with open(os.path.join(tmp, "bench_log.txt")) as f:
+                m = re.search(r"GPU acceleration is ([^\n]*)", f.read())
+            status = m.group(1).strip() if m else "no status line"
+            if not status.startswith("enabled"):
+                raise RuntimeError("reference GPU layer not running: " + status)
         # primary-emission segment from the log time stamps (millisecond resolution): from
         # "Launching ... primary emission photon packets" to "Finished primary emission"
         def stamp(pattern):
@@ -221,6 +238,40 @@ def cpu_baseline(name, sample_s=20.0):
     secs = time.perf_counter() - t
     return {"value": n / secs, "unit": "packets/s", "cores": 1, "kind": "port",
             "sample": f"{n} packets of the same workload through the single-threaded C oracle"}
+
+
+def run_reference_gpu_arm(args, rank, world):
+    """The reference's own GPU route on this box (`skirt_refgpu -g -t <cores>`, its default promoted
+    configuration) on the workload's ski file: packets/s of the primary segment from its log, each
+    step a sample of about 30 s. A second baseline beside the CPU reference arm."""
+    if rank != 0:
+        return
+    name = args.workload
+    if not os.path.exists(REF_SKIRT_GPU) or name == "batch" or name not in ("shell", "galaxy", "voronoi"):
+        print(json.dumps({"impl": "reference-gpu", "unavailable": "skirt_refgpu missing or workload not a single ski "
+                          "file (oracle/ref.mk target refgpu)"}))
+        return
+    cores = os.cpu_count() or 1
+    try:
+        # the route has seconds of fixed cost per primary segment (chunk set-up, resident tables):
+        # a probe of 1e5 packets, then samples of about 30 s
+        probe = 100000
+        text, files = reference_inputs(name, probe)
+        rate, _ = reference_run(text, probe, cores, files, gpu=True)
+        npp = int(min(5e6, max(probe, rate * 30.0)))
+        text, files = reference_inputs(name, npp)
+        vals = [reference_run(text, npp, cores, files, gpu=True)[0] for _ in range(args.steps)]
+    except RuntimeError as e:
+        print(json.dumps({"impl": "reference-gpu", "unavailable": str(e)[:300]}))
+        return
+    value = statistics.median(vals)
+    print(json.dumps({"metric": "packets/s on 1 B200", "value": value, "unit": "packets/s", "n_gpus": 1,
+                      "steps": args.steps, "warmup": 0, "ms_per_step": 1e3 * npp / value, "higher_is_better": True,
+                      "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                      "impl": "reference-gpu",
+                      "config": {"workload": name, "description": WORKLOADS[name][0], "packets_per_step": npp,
+                                 "route": f"reference GpuAcceleration, skirt -g -t {cores}, default (promoted) route"},
+                      "samples": vals}))
 
 
 def run_reference_arm(args, rank, world):
@@ -592,7 +643,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-gpu"])
     ap.add_argument("--workload", default="galaxy", choices=sorted(WORKLOADS))
     ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32"],
                     help="traversal precision: fp32 (production) or fp64 (reference operation order)")
@@ -623,8 +674,8 @@ def main():
         import datetime
         dist.init_process_group("nccl" if args.impl == "ours" else "gloo", timeout=datetime.timedelta(seconds=300))
 
-    if args.impl == "reference":
-        run_reference_arm(args, rank, world)
+    if args.impl in ("reference", "reference-gpu"):
+        (run_reference_arm if args.impl == "reference" else run_reference_gpu_arm)(args, rank, world)
         if dist:
             dist.destroy_process_group()
         return

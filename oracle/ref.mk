@@ -69,7 +69,7 @@ LIBS := $(LIB)/libserialize.a $(LIB)/libschema.a $(LIB)/libfundamentals.a $(LIB)
         $(LIB)/libtetgen.a
 LINK_LIBS := -Wl,--start-group $(LIBS) -Wl,--end-group -pthread -ldl
 
-all: $(BIN)/skirt $(BIN)/skirt_export $(RES)/placeholder.txt $(BIN)/skirt_gpu $(BIN)/skirt_oracle
+all: $(BIN)/skirt $(BIN)/skirt_export $(RES)/placeholder.txt $(BIN)/skirt_gpu $(BIN)/skirt_oracle $(BIN)/skirt_refgpu
 
 $(RES)/placeholder.txt:
 	@mkdir -p $(RES)
@@ -182,6 +182,21 @@ $(BIN)/skirt_gpu: $(O_BRIDGE) $(filter-out $(O_MAINLIB),$(O_MAIN)) $(LIBS) $(PKG
 
 bridge: $(BIN)/skirt_gpu
 
+# The reference's own GPU route for a second baseline: the unmodified reference program except for
+# a copy of GpuAcceleration.cpp whose driver-symbol loader prefers the versioned entry points
+# (patch_refgpu.py; on this pool's driver the original resolves the legacy cuCtxCreate and its GPU
+# runtime does not start). `skirt_refgpu -g run.ski` runs the reference's GPU layer.
+$(PATCHED)/GpuAcceleration.cpp: $(HERE)/patch_refgpu.py $(K_CORE)/GpuAcceleration.cpp
+	python3 $(HERE)/patch_refgpu.py $(REF) $(PATCHED)
+$(OBJ)/refgpu/GpuAcceleration.o: $(PATCHED)/GpuAcceleration.cpp
+	@mkdir -p $(dir $@)
+	$(CXX) $(CXXFLAGS_REF) $(INC_CORE) -I$(K_CORE) -c $< -o $@
+$(BIN)/skirt_refgpu: $(OBJ)/refgpu/GpuAcceleration.o $(O_MAIN) $(LIBS)
+	@mkdir -p $(BIN)
+	$(CXX) -o $@ $(OBJ)/refgpu/GpuAcceleration.o $(O_MAIN) $(LINK_LIBS)
+
+refgpu: $(BIN)/skirt_refgpu
+
 # Test infrastructure: the same bridged program with the bridge's skgpu_* calls renamed to the CPU
 # oracle's or_* entry points (same signatures, oracle/skoracle.h), linked against
 # oracle/_build/liboracle.so: runs the bridge's flattening and fetch logic end to end without a GPU
@@ -206,4 +221,4 @@ $(BIN)/skirt_oracle: $(OBJ)/bridge/MonteCarloSimulation.o $(OBJ)/bridge/SkirtCom
 	    $(OBJ)/bridge/SkgpuLifeCycle_oracle.o $(filter-out $(O_MAINLIB),$(O_MAIN)) $(LINK_LIBS) \
 	    -L$(HERE)/_build -loracle -Wl,-rpath,'$$ORIGIN/../../../../_build'
 
-.PHONY: all bridge
+.PHONY: all bridge refgpu
