@@ -80,6 +80,17 @@ void devFree(T*& p)
     p = nullptr;
 }
 
+// warp aggregation of the radiation-field atomics (off unless SKGPU_RF_WARP_AGG=1; a switch for
+// comparing the two forms)
+int rfWarpAggregation()
+{
+    static const int on = [] {
+        const char* v = std::getenv("SKGPU_RF_WARP_AGG");
+        return v && v[0] == '1' ? 1 : 0;
+    }();
+    return on;
+}
+
 void freeGrid(skgpu_ctx* ctx)
 {
     for (void* p : ctx->gridBufs) cudaFree(p);
@@ -1610,6 +1621,7 @@ int skgpu_run_primary(skgpu_ctx* ctx, uint64_t first, uint64_t count, uint64_t t
     w.sc = sceneOf(ctx);
     w.traceBlocksPerSM = ctx->shapeTraceBlocks;
     w.refillMin = ctx->shapeRefill;
+    w.rfAgg = rfWarpAggregation();
     w.shadeBlocksPerSM = ctx->shapeShadeBlocks;
     w.P = P;
     w.first = first;
@@ -1853,6 +1865,7 @@ int skgpu_run_secondary(skgpu_ctx* ctx, uint64_t first, uint64_t count)
     w.sc.seed = ctx->opt.seed ^ SKGPU_SECONDARY_KEY;
     w.traceBlocksPerSM = ctx->shapeTraceBlocks;
     w.refillMin = ctx->shapeRefill;
+    w.rfAgg = rfWarpAggregation();
     w.shadeBlocksPerSM = ctx->shapeShadeBlocks;
     w.P = P;
     w.first = first;
@@ -1996,6 +2009,7 @@ int skgpu_run_primary_noalloc(skgpu_ctx* ctx, uint64_t first, uint64_t count, ui
     w.sc = sceneOf(ctx);
     w.traceBlocksPerSM = ctx->shapeTraceBlocks;
     w.refillMin = ctx->shapeRefill;
+    w.rfAgg = rfWarpAggregation();
     w.shadeBlocksPerSM = ctx->shapeShadeBlocks;
     w.P = static_cast<int>(std::min<uint64_t>(std::max<uint64_t>(count, 1), SKGPU_NOALLOC_MAX_SLOTS));
     w.first = first;
@@ -2596,6 +2610,7 @@ int skgpu_run_batch(skgpu_ctx* const* ctxs, int32_t n, const uint64_t* first, co
     w.statCap = STATS_CAP;
     w.traceBlocksPerSM = ctx->shapeTraceBlocks;
     w.refillMin = ctx->shapeRefill;
+    w.rfAgg = rfWarpAggregation();
     w.shadeBlocksPerSM = ctx->shapeShadeBlocks;
     if ((rc = prepareOrder(ctx, w))) return rc;
     return runAndCollect(ctx, w, true, true);

@@ -113,6 +113,8 @@ struct Wave
     // launch shape (0: defaults): resident trace blocks per SM, shade blocks per SM, and the number
     // of waiting lanes at which a warp of the traversal kernel takes new tasks
     int traceBlocksPerSM, shadeBlocksPerSM, refillMin;
+    // radiation-field updates of a warp summed per address before the atomic (SKGPU_RF_WARP_AGG=1)
+    int rfAgg;
     // launch order: histories first + order[i] for i = 0, 1, ... (null: index order)
     const unsigned* order;
     PacketPool pk;

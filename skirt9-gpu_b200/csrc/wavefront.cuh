@@ -426,7 +426,11 @@ __global__ void __launch_bounds__(256, Walker::kMinBlocks) traceKernel(const __g
                                          * static_cast<double>(ds);
                             // device layout ell * cells + m: the packets in flight (taken up in
                             // wavelength order) update one contiguous slice; the fetch transposes
-                            atomicAdd(scn().rf + static_cast<size_t>(iA) * scn().g.numCells + m, Lds);
+                            double* at = scn().rf + static_cast<size_t>(iA) * scn().g.numCells + m;
+                            if (w.rfAgg)
+                                atomicAddAgg(at, Lds);
+                            else
+                                atomicAdd(at, Lds);
                             rfStores++;
                         }
                         fB = lnExtEnd;

@@ -106,6 +106,34 @@ inline bool splitTraversal()
     return on;
 }
 
+// the shared-memory carveout of the traversal kernels in percent (SKGPU_TRACE_CARVEOUT, unset: the
+// driver's choice): the split of each SM's on-chip memory between L1 (which caches the grid records)
+// and shared memory, for measuring what on-chip capacity for grid records is worth
+inline int traceCarveout()
+{
+    static const int pct = [] {
+        const char* v = std::getenv("SKGPU_TRACE_CARVEOUT");
+        if (!v || !v[0]) return -1;
+        int p = std::atoi(v);
+        return p < 0 ? 0 : (p > 100 ? 100 : p);
+    }();
+    return pct;
+}
+
+template<class Walker>
+void applyTraceCarveout()
+{
+    int pct = traceCarveout();
+    if (pct < 0) return;
+    auto set = [pct](const void* f) { cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, pct); };
+    set(reinterpret_cast<const void*>(&traceKernel<Walker, false, TRACE_ALL>));
+    set(reinterpret_cast<const void*>(&traceKernel<Walker, false, TRACE_PEEL>));
+    set(reinterpret_cast<const void*>(&traceKernel<Walker, false, TRACE_PROP>));
+    set(reinterpret_cast<const void*>(&traceKernel<Walker, true, TRACE_ALL>));
+    set(reinterpret_cast<const void*>(&traceKernel<Walker, true, TRACE_PEEL>));
+    set(reinterpret_cast<const void*>(&traceKernel<Walker, true, TRACE_PROP>));
+}
+
 template<class Walker>
 std::vector<unsigned char> graphKey(const Wave& w, const WaveLaunch& L, const StageTimer* timer)
 {
@@ -130,6 +158,7 @@ cudaError_t runWave(const Wave& w, int numSMs, cudaStream_t s, unsigned long lon
 {
     WaveLaunch L{};
     L.threads = 256;
+    applyTraceCarveout<Walker>();
     L.multi = w.nScenes > 1;
     int resident = traceBlocksPerSM<Walker>(L.multi, traceSmemBytes(w));
     // a tuned shape may ask for fewer resident trace blocks, never for more than fit
