@@ -389,6 +389,14 @@ int skgpu_fetch_instrument_components(skgpu_ctx* ctx, int32_t instrument, double
 /* Adds the scattering-level planes of an instrument (skgpu_set_instrument_scattering_levels): levels
  * planes of ifu size or of sed size, plane n-1 for n scatterings. */
 int skgpu_fetch_instrument_levels(skgpu_ctx* ctx, int32_t instrument, double* ifu_levels, double* sed_levels);
+/* Calibration on the device (FluxRecorder::calibrateAndWrite, FluxRecorder.cpp:876-921, with
+ * scaleWavelengthArray / scaleFrameWavelengthArray :97-115; replaces GpuAcceleration::
+ * scaleWavelengthValues / scaleFrameWavelengthValues, GpuAcceleration.hpp:488-494): multiplies the
+ * instrument's device tallies -- total, component and scattering-level planes, not the statistics --
+ * by factors[ell] per wavelength bin, in place (frame entries l + ell*npix). The caller computes the
+ * factors as FluxRecorder does: 1 / (4 pi d^2) / effectiveWidth(ell) * Units::ofluxdensity(lambda_ell, 1)
+ * for an SED, additionally / omega with Units::osurfacebrightness for a frame. */
+int skgpu_calibrate_instrument(skgpu_ctx* ctx, int32_t instrument, const double* factors);
 /* Adds the radiation-field tally (num_cells * num_rf_bins, index m*num_rf_bins + ell) into rf. */
 int skgpu_fetch_radiation_field(skgpu_ctx* ctx, double* rf);
 int skgpu_clear_tallies(skgpu_ctx* ctx);

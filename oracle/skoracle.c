@@ -2958,6 +2958,21 @@ int or_fetch_instrument_components(or_ctx* c, int32_t i, double* ifu3, double* s
     return SKGPU_OK;
 }
 
+/* FluxRecorder::calibrateAndWrite's scaling (FluxRecorder.cpp:97-115, 891-921) */
+int or_calibrate_instrument(or_ctx* c, int32_t i, const double* factors)
+{
+    if (i < 0 || i >= c->ninstr) return fail(c, SKGPU_ERR_ARG, "calibrate: bad instrument index");
+    if (!factors) return fail(c, SKGPU_ERR_ARG, "calibrate: missing factors");
+    Instr* in = &c->instr[i];
+    size_t npix = in->d.kind == SKGPU_INSTR_FRAME ? (size_t)in->d.num_pixels_x * in->d.num_pixels_y : 1;
+    size_t n = in->n;
+    double* total = in->d.kind == SKGPU_INSTR_FRAME ? in->ifu : in->sed;
+    for (size_t q = 0; q < n; ++q) total[q] *= factors[q / npix];
+    if (in->comp)
+        for (size_t q = 0; q < (size_t)(3 + in->levels) * n; ++q) in->comp[q] *= factors[(q % n) / npix];
+    return SKGPU_OK;
+}
+
 int or_fetch_instrument_levels(or_ctx* c, int32_t i, double* ifu_levels, double* sed_levels)
 {
     if (i < 0 || i >= c->ninstr) return fail(c, SKGPU_ERR_ARG, "fetch: bad instrument index");

@@ -84,6 +84,7 @@ int or_run_secondary(or_ctx* ctx, uint64_t first, uint64_t count);
 int or_fetch_instrument(or_ctx* ctx, int32_t instrument, double* ifu, double* sed, double* ifu_stats,
                         double* sed_stats);
 int or_fetch_instrument_components(or_ctx* ctx, int32_t instrument, double* ifu3, double* sed3);
+int or_calibrate_instrument(or_ctx* ctx, int32_t instrument, const double* factors);
 int or_fetch_instrument_levels(or_ctx* ctx, int32_t instrument, double* ifu_levels, double* sed_levels);
 int or_fetch_radiation_field(or_ctx* ctx, double* rf);
 int or_clear_tallies(or_ctx* ctx);

@@ -2103,6 +2103,43 @@ int skgpu_fetch_instrument_components(skgpu_ctx* ctx, int32_t instrument, double
     return d.kind == SKGPU_INSTR_FRAME ? addInto(ctx, d.ifuComp, 3 * n, ifu3) : addInto(ctx, d.sedComp, 3 * n, sed3);
 }
 
+// values[i] *= factors[(i % n) / npix] over `planes` planes of n = nbins * npix entries
+static __global__ void calibrateKernel(double* __restrict__ values, size_t total, size_t n, size_t npix,
+                                       const double* __restrict__ factors)
+{
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x)
+        values[i] *= factors[(i % n) / npix];
+}
+
+int skgpu_calibrate_instrument(skgpu_ctx* ctx, int32_t instrument, const double* factors)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (instrument < 0 || instrument >= static_cast<int>(ctx->instrHost.size())) return fail(ctx, SKGPU_ERR_ARG, "calibrate: bad instrument index");
+    if (!factors) return fail(ctx, SKGPU_ERR_ARG, "calibrate: missing factors");
+    const InstrDev& d = ctx->instrHost[instrument];
+    if (!finiteAll(factors, static_cast<size_t>(d.nbins))) return fail(ctx, SKGPU_ERR_ARG, "calibrate: non-finite factor");
+    CK(cudaSetDevice(ctx->device));
+    size_t npix = static_cast<size_t>(d.npx) * d.npy, n = npix * d.nbins;
+    double* f = nullptr;
+    CK(devUpload(&f, factors, static_cast<size_t>(d.nbins)));
+    int blocks = 0;
+    cudaError_t e = cudaDeviceGetAttribute(&blocks, cudaDevAttrMultiProcessorCount, ctx->device);
+    if (e == cudaSuccess)
+    {
+        blocks *= 4;
+        double* total = d.kind == SKGPU_INSTR_FRAME ? d.ifu : d.sed;
+        double* comp = d.kind == SKGPU_INSTR_FRAME ? d.ifuComp : d.sedComp;
+        calibrateKernel<<<blocks, 256, 0, ctx->stream>>>(total, n, n, npix, f);
+        if (comp) calibrateKernel<<<blocks, 256, 0, ctx->stream>>>(comp, (3 + d.levels) * n, n, npix, f);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    }
+    cudaFree(f);
+    CK(e);
+    return SKGPU_OK;
+}
+
 int skgpu_fetch_instrument_levels(skgpu_ctx* ctx, int32_t instrument, double* ifu_levels, double* sed_levels)
 {
     if (!ctx) return SKGPU_ERR_ARG;

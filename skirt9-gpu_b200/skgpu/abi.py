@@ -144,6 +144,7 @@ SIGNATURES = {
     "fetch_instrument": [_P, _I, _P, _P, _P, _P],
     "fetch_instrument_components": [_P, _I, _P, _P],
     "fetch_instrument_levels": [_P, _I, _P, _P],
+    "calibrate_instrument": [_P, _I, _P],
     "fetch_radiation_field": [_P, _P],
     "clear_tallies": [_P],
     "get_counters": [_P, _P],
@@ -339,6 +340,11 @@ class Backend:
         comp = self._into(out, 3 * n)
         self.call("fetch_instrument_components", i, _ptr(comp), _ptr(comp))
         return comp.reshape(3, n)
+
+    def calibrate_instrument(self, i, factors):
+        """Scales instrument i's device tallies by factors[ell] per wavelength bin (in place)."""
+        f = f64(factors)
+        self.call("calibrate_instrument", int(i), _ptr(f))
 
     def fetch_instrument_levels(self, i, n, levels, out=None):
         lv = self._into(out, levels * n)

@@ -6,6 +6,7 @@ instruments, options). It is filled either from the export of a reference simula
 workload builders in `skgpu.workloads`. `Scene.upload` sends it through a `Backend`;
 `Scene.run` performs one primary-emission segment and returns the tallies.
 """
+import math
 import os
 
 import numpy as np
@@ -38,6 +39,27 @@ def list_bands(bands, unit=1e-6):
         out.append((1.0 / np.sqrt(integral), lv, tv, 1.0 / tv.max()))
     out.sort(key=lambda b: b[0])
     return [(lv, tv, w) for _, lv, tv, w in out]
+
+
+def calibration_factors(distance, wavelengths, widths, pixel_size=None):
+    """FluxRecorder::calibrateAndWrite's factors per wavelength bin (SKIRT/core/FluxRecorder.cpp:891-921)
+    for a distant instrument at redshift 0 (luminosity and angular-diameter distance both `distance`)
+    with SKIRT's frequency output style: SED flux densities in Jy (Units::ofluxdensity, unit
+    `frequencyfluxdensity` Jy = 1e-26), frames in MJy/sr (Units::osurfacebrightness, MJy/sr = 1e-20)
+    over the pixel solid angle 4 atan(px / 2d) atan(py / 2d); pixel_size = (px, py) selects the frame
+    form. wavelengths and widths are the grid's characteristic wavelengths and effective widths."""
+    c = 2.99792458e8  # Constants::c()
+    fourpid2 = 4.0 * math.pi * (distance * distance)
+    out = []
+    for lam, w in zip(wavelengths, widths):
+        conv = lam * lam * 1.0 / c
+        if pixel_size is None:
+            out.append(1.0 / fourpid2 / w * ((conv - 0.0) / 1e-26))
+        else:
+            px, py = pixel_size
+            omega = 4.0 * math.atan(0.5 * px / distance) * math.atan(0.5 * py / distance)
+            out.append(1.0 / fourpid2 / omega / w * ((conv - 0.0) / 1e-20))
+    return np.array(out)
 
 
 def band_transmission(band, lam):
@@ -413,6 +435,8 @@ class Scene:
                        same_observer=int(meta[p + "same_observer"]), stats=int(meta[p + "record_statistics"]),
                        num_bins=int(ellv.max()) + 1, wlg_borders=L(p + "wlg_borders"), wlg_ellv=ellv,
                        kobs=(float(meta[p + "kobs_x"]), float(meta[p + "kobs_y"]), float(meta[p + "kobs_z"])))
+            if p + "distance" in meta:
+                ins["distance"] = float(meta[p + "distance"])
             if ins["kind"] == abi.INSTR_FRAME:
                 ins.update(nx=int(meta[p + "nxp"]), ny=int(meta[p + "nyp"]),
                            trig=tuple(float(meta[p + k]) for k in

@@ -74,6 +74,29 @@ def test_gpu_levels_and_bands_match_oracle(golden, gpu_backend, oracle_backend):
     check_levels_and_bands(sc, r32, 3)
 
 
+def test_gpu_calibration_matches_oracle_and_reference(golden, gpu_backend, oracle_backend):
+    """Calibration on the device: every plane scaled by its bin's factor (one multiply, as the
+    oracle), the shell's transparent SED flux equal to the reference's written Jy; a frame's total,
+    component and scattering-level planes scaled alike."""
+    from skgpu.scene import calibration_factors
+    from test_instrument_output_cpu import calibrated_shell, levels_bands_scene
+    z, f, rawg, calg = calibrated_shell(gpu_backend, golden)
+    _, _, rawo, calo = calibrated_shell(oracle_backend, golden)
+    assert np.array_equal(calg["total"], rawg["total"] * f[0])
+    assert np.array_equal(calg["components"], rawg["components"] * f[0])
+    assert calg["components"][0, 0] == pytest.approx(float(z["ref_sed_jy"][1]), rel=1e-9)
+    assert np.allclose(calg["total"], calo["total"], rtol=1e-9, atol=0)
+    sc = levels_bands_scene(golden("shell_c16.npz"), levels=3)
+    sc.upload(gpu_backend)
+    raw = sc.run(gpu_backend, 3000, seed=2)[0]
+    fr = sc.instruments[0]
+    fac = calibration_factors(fr["distance"], [0.55e-6], [1.1e-9], pixel_size=(fr["xp_size"], fr["yp_size"]))
+    gpu_backend.calibrate_instrument(0, fac)
+    cal = sc.fetch(gpu_backend)[0]
+    for key in ("total", "components", "levels"):
+        assert np.array_equal(cal[key], raw[key] * fac[0]), key
+
+
 def test_gpu_free_propagation_matches_oracle(golden, gpu_backend, oracle_backend):
     sc = Scene.from_export(golden("shell_c16.npz"))
     sc.force_scattering = False

@@ -84,3 +84,32 @@ def test_band_and_level_arguments_checked(golden, oracle_backend):
         oracle_backend.set_instrument_scattering_levels(7, 2)  # no such instrument
     with pytest.raises(SkgpuError):
         oracle_backend.set_instrument_bands(1, list_bands(ski.TEST_BANDS))  # 4 bands for a 1-bin grid
+
+
+def calibrated_shell(backend, golden):
+    """The shell's SED through the life cycle of all its packets, calibrated by the backend: the
+    transparent flux is the source luminosity over 4 pi d^2 (every packet's weight counted once), the
+    same number the reference writes, so it pins the calibration against the reference's output."""
+    from skgpu.scene import calibration_factors
+    z = golden("shell_c16.npz")
+    sc = Scene.from_export(z)
+    sc.instruments[1]["comps"] = 1
+    sc.upload(backend)
+    npp = 4000
+    raw = sc.run(backend, npp, seed=7)
+    sed = sc.instruments[1]
+    b = np.asarray(sed["wlg_borders"])
+    f = calibration_factors(sed["distance"], [float(sc.sources[0]["table_lambda"][0])], [b[1] - b[0]])
+    backend.calibrate_instrument(1, f)
+    cal = sc.fetch(backend)
+    return z, f, raw[1], cal[1]
+
+
+def test_calibration_on_oracle_matches_the_reference(golden, oracle_backend):
+    z, f, raw, cal = calibrated_shell(oracle_backend, golden)
+    assert f[0] == pytest.approx(float(z["ref_jy_per_w"]), rel=1e-9)
+    # calibration multiplies every plane by its bin's factor
+    assert np.array_equal(cal["total"], raw["total"] * f[0])
+    assert np.array_equal(cal["components"], raw["components"] * f[0])
+    # the transparent flux (Jy) equals the reference's written value (10 significant digits)
+    assert cal["components"][0, 0] == pytest.approx(float(z["ref_sed_jy"][1]), rel=1e-9)
