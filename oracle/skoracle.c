@@ -2616,8 +2616,10 @@ int or_prepare_secondary(or_ctx* c, const skgpu_secondary_options* opt, uint64_t
 {
     if (!opt || total_packets == 0) return fail(c, SKGPU_ERR_ARG, "secondary: missing options or packets");
     if (!c->hasGrid || (c->g.kind != SKGPU_GRID_CARTESIAN && c->g.kind != SKGPU_GRID_OCTREE
-                        && c->g.kind != SKGPU_GRID_ADAPTIVE_MESH))
-        return fail(c, SKGPU_ERR_UNSUPPORTED, "secondary: dust emission needs a Cartesian, octree or adaptive-mesh grid");
+                        && c->g.kind != SKGPU_GRID_ADAPTIVE_MESH && c->g.kind != SKGPU_GRID_TETRA
+                        && c->g.kind != SKGPU_GRID_SPHERE1D))
+        return fail(c, SKGPU_ERR_UNSUPPORTED, "secondary: dust emission needs a Cartesian, octree, adaptive-mesh, "
+                                              "tetrahedral or 1D spherical grid");
     if (!c->deNrf || c->deCells != c->numCells || c->deNrf != c->nrf)
         return fail(c, SKGPU_ERR_STATE, "secondary: dust emission tables do not match the medium and RF grid");
     if (!c->rf || c->rfLen != (size_t)c->numCells * c->nrf) return fail(c, SKGPU_ERR_STATE, "secondary: no radiation field");
@@ -2830,24 +2832,69 @@ static void launch_secondary(or_ctx* c, Rng* r, uint64_t hist, Packet* pk)
             w = s / ((1 - c->secXi) * s + c->secXi * b);
         }
     }
-    double b0, b1, b2, b3, b4, b5;
-    if (c->g.kind == SKGPU_GRID_CARTESIAN)
+    /* a random position in cell m (SpatialGrid::randomPositionInCell of the grid kind) */
+    if (c->g.kind == SKGPU_GRID_TETRA)
     {
-        int i = m / (c->g.nz * c->g.ny), j = (m / c->g.nz) % c->g.ny, k = m % c->g.nz;
-        b0 = c->g.xb[i]; b1 = c->g.yb[j]; b2 = c->g.zb[k];
-        b3 = c->g.xb[i + 1]; b4 = c->g.yb[j + 1]; b5 = c->g.zb[k + 1];
+        /* TetraMeshSpatialGrid::Tetra::generatePosition / generateBarycentric (TetraMeshSpatialGrid.cpp:140-173) */
+        double s = uniform(r);
+        double t = uniform(r);
+        double u = uniform(r);
+        if (s + t > 1.)
+        {
+            s = 1. - s;
+            t = 1. - t;
+        }
+        if (t + u > 1.)
+        {
+            double tmp = u;
+            u = 1. - s - t;
+            t = 1. - tmp;
+        }
+        else if (s + t + u > 1.)
+        {
+            double tmp = u;
+            u = s + t + u - 1.;
+            s = 1. - t - tmp;
+        }
+        double b = 1. - u - t - s;
+        const double *v0 = te_vertex(&c->g, m, 0), *v1 = te_vertex(&c->g, m, 1), *v2 = te_vertex(&c->g, m, 2),
+                     *v3 = te_vertex(&c->g, m, 3);
+        pk->rx = b * v0[0] + u * v1[0] + t * v2[0] + s * v3[0];
+        pk->ry = b * v0[1] + u * v1[1] + t * v2[1] + s * v3[1];
+        pk->rz = b * v0[2] + u * v1[2] + t * v2[2] + s * v3[2];
+    }
+    else if (c->g.kind == SKGPU_GRID_SPHERE1D)
+    {
+        /* Sphere1DSpatialGrid::randomPositionInCell (Sphere1DSpatialGrid.cpp:80-91) */
+        double ux, uy, uz;
+        iso_direction(r, &ux, &uy, &uz);
+        double r0 = c->g.srv[m], r1 = c->g.srv[m + 1];
+        double rad = cbrt(r0 * r0 * r0 + (r1 - r0) * (r1 * r1 + r1 * r0 + r0 * r0) * uniform(r));
+        pk->rx = rad * ux;
+        pk->ry = rad * uy;
+        pk->rz = rad * uz;
     }
     else
     {
-        const double* bb = c->g.tb + 6 * (size_t)c->secCellNode[m];
-        b0 = bb[0]; b1 = bb[1]; b2 = bb[2]; b3 = bb[3]; b4 = bb[4]; b5 = bb[5];
+        double b0, b1, b2, b3, b4, b5;
+        if (c->g.kind == SKGPU_GRID_CARTESIAN)
+        {
+            int i = m / (c->g.nz * c->g.ny), j = (m / c->g.nz) % c->g.ny, k = m % c->g.nz;
+            b0 = c->g.xb[i]; b1 = c->g.yb[j]; b2 = c->g.zb[k];
+            b3 = c->g.xb[i + 1]; b4 = c->g.yb[j + 1]; b5 = c->g.zb[k + 1];
+        }
+        else
+        {
+            const double* bb = c->g.tb + 6 * (size_t)c->secCellNode[m];
+            b0 = bb[0]; b1 = bb[1]; b2 = bb[2]; b3 = bb[3]; b4 = bb[4]; b5 = bb[5];
+        }
+        double fx = uniform(r);
+        double fy = uniform(r);
+        double fz = uniform(r);
+        pk->rx = b0 + fx * (b3 - b0);
+        pk->ry = b1 + fy * (b4 - b1);
+        pk->rz = b2 + fz * (b5 - b2);
     }
-    double fx = uniform(r);
-    double fy = uniform(r);
-    double fz = uniform(r);
-    pk->rx = b0 + fx * (b3 - b0);
-    pk->ry = b1 + fy * (b4 - b1);
-    pk->rz = b2 + fz * (b5 - b2);
     iso_direction(r, &pk->kx, &pk->ky, &pk->kz);
     pk->lambda = lambda;
     pk->L = c->secLpk * ws * w;

@@ -162,7 +162,9 @@ namespace
         }
         else
         {
-            if (!box) return (why = "secondary emission needs a Cartesian, octree or adaptive-mesh grid"), false;
+            // grids whose randomPositionInCell the library reproduces for the secondary launch
+            if (!box && !dynamic_cast<TetraMeshSpatialGrid*>(grid) && !dynamic_cast<Sphere1DSpatialGrid*>(grid))
+                return (why = "secondary emission on this grid type"), false;
             if (!config->hasDustEmission() || config->hasGasEmission() || config->hasStochasticDustEmission()
                 || config->storeEmissionRadiationField() || !config->hasPanRadiationField())
                 return (why = "secondary emission other than equilibrium dust emission"), false;

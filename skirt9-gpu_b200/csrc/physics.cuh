@@ -251,24 +251,74 @@ SKG_D Launched launchSecondary(const Scene& p, unsigned long long hist, Rng& rng
             w = s / ((1 - S.xi) * s + S.xi * b);
         }
     }
-    // the cell box: Cartesian borders, or the extent of the octree leaf
-    double b0, b1, b2, b3, b4, b5;
-    if (p.g.kind == 0)
+    // a random position in cell m (SpatialGrid::randomPositionInCell of the grid kind)
+    Launched o;
+    if (p.g.kind == 3)
     {
-        int i = m / (p.g.nz * p.g.ny), j = (m / p.g.nz) % p.g.ny, k = m % p.g.nz;
-        b0 = p.g.xb[i]; b1 = p.g.yb[j]; b2 = p.g.zb[k];
-        b3 = p.g.xb[i + 1]; b4 = p.g.yb[j + 1]; b5 = p.g.zb[k + 1];
+        // TetraMeshSpatialGrid::Tetra::generatePosition / generateBarycentric
+        // (TetraMeshSpatialGrid.cpp:140-173): the unit cube folded into the tetrahedron
+        double s = rng.uniform(), t = rng.uniform(), u = rng.uniform();
+        if (xadd(s, t) > 1.)
+        {
+            s = xsub(1., s);
+            t = xsub(1., t);
+        }
+        if (xadd(t, u) > 1.)
+        {
+            double tmp = u;
+            u = xsub(xsub(1., s), t);
+            t = xsub(1., tmp);
+        }
+        else if (xadd(xadd(s, t), u) > 1.)
+        {
+            double tmp = u;
+            u = xsub(xadd(xadd(s, t), u), 1.);
+            s = xsub(xsub(1., t), tmp);
+        }
+        double r = xsub(xsub(xsub(1., u), t), s);
+        double v[4][3];
+        for (int q = 0; q < 4; ++q) teVertex(p.g, m, q, v[q][0], v[q][1], v[q][2]);
+        double c[3];
+        for (int a = 0; a < 3; ++a)
+            c[a] = xadd(xadd(xadd(xmul(r, v[0][a]), xmul(u, v[1][a])), xmul(t, v[2][a])), xmul(s, v[3][a]));
+        o.x = c[0];
+        o.y = c[1];
+        o.z = c[2];
+    }
+    else if (p.g.kind == 4)
+    {
+        // Sphere1DSpatialGrid::randomPositionInCell (Sphere1DSpatialGrid.cpp:80-91): an isotropic
+        // direction, then r^3 uniform between the shell's borders (Cubic::pow3)
+        double ux, uy, uz;
+        isotropicDirection(rng, ux, uy, uz);
+        double r0 = p.g.sRv[m], r1 = p.g.sRv[m + 1];
+        double d3 = xmul(xsub(r1, r0), xadd(xadd(xmul(r1, r1), xmul(r1, r0)), xmul(r0, r0)));
+        double r = cbrt(xadd(xmul(xmul(r0, r0), r0), xmul(d3, rng.uniform())));
+        o.x = xmul(r, ux);
+        o.y = xmul(r, uy);
+        o.z = xmul(r, uz);
     }
     else
     {
-        const double* bb = p.g.tBounds + 6 * static_cast<size_t>(S.cellNode[m]);
-        b0 = bb[0]; b1 = bb[1]; b2 = bb[2]; b3 = bb[3]; b4 = bb[4]; b5 = bb[5];
+        // the cell box (Random::position, Box::fracPos): Cartesian borders, or the extent of the
+        // octree or adaptive-mesh leaf
+        double b0, b1, b2, b3, b4, b5;
+        if (p.g.kind == 0)
+        {
+            int i = m / (p.g.nz * p.g.ny), j = (m / p.g.nz) % p.g.ny, k = m % p.g.nz;
+            b0 = p.g.xb[i]; b1 = p.g.yb[j]; b2 = p.g.zb[k];
+            b3 = p.g.xb[i + 1]; b4 = p.g.yb[j + 1]; b5 = p.g.zb[k + 1];
+        }
+        else
+        {
+            const double* bb = p.g.tBounds + 6 * static_cast<size_t>(S.cellNode[m]);
+            b0 = bb[0]; b1 = bb[1]; b2 = bb[2]; b3 = bb[3]; b4 = bb[4]; b5 = bb[5];
+        }
+        double fx = rng.uniform(), fy = rng.uniform(), fz = rng.uniform();
+        o.x = xadd(b0, xmul(fx, xsub(b3, b0)));
+        o.y = xadd(b1, xmul(fy, xsub(b4, b1)));
+        o.z = xadd(b2, xmul(fz, xsub(b5, b2)));
     }
-    Launched o;
-    double fx = rng.uniform(), fy = rng.uniform(), fz = rng.uniform();
-    o.x = xadd(b0, xmul(fx, xsub(b3, b0)));
-    o.y = xadd(b1, xmul(fy, xsub(b4, b1)));
-    o.z = xadd(b2, xmul(fz, xsub(b5, b2)));
     isotropicDirection(rng, o.kx, o.ky, o.kz);
     o.lambda = lambda;
     o.L = xmul(xmul(S.Lpk, ws), w);

@@ -514,3 +514,14 @@ def dust_adaptive(num_packets=1e5):
     text = dust_shell(num_packets, grid="<AdaptiveMeshSpatialGrid/>",
                       medium=lambda mix: adaptive_mesh_medium("mesh.txt", 1.0, mix))
     return text, {"mesh.txt": adaptive_mesh_text(half_pc=1.0, hR=0.25, hz=0.05, rho0=500.0)}
+
+
+def dust_tetra(num_packets=1e5, num_vertices=3000):
+    """DustEmission (the dust_shell configuration) on a TetraMeshSpatialGrid of the dust shell
+    (vertices sampled from the dust density by the reference's own policy) in the +-1 pc box."""
+    return dust_shell(num_packets, grid=tetra_grid(1, "pc", num_vertices))
+
+
+def dust_sphere1d(num_packets=1e5):
+    """DustEmission (the dust_shell configuration) on a Sphere1DSpatialGrid of 24 shells 0.05-1 pc."""
+    return dust_shell(num_packets, grid=sphere1d_grid(0.05, 1, 24))

@@ -83,6 +83,19 @@ def test_bridge_dust_emission_adaptive_on_oracle(tmp_path):
 
 
 @needs_build
+@pytest.mark.parametrize("grid", ["tetra", "sphere1d"])
+def test_bridge_dust_emission_other_grids_on_oracle(tmp_path, grid):
+    """DustEmission on a tetrahedral mesh and a 1D spherical grid: secondary launches at random
+    positions in tetrahedra (barycentric fold) and spherical shells."""
+    text = ski.dust_tetra(50000) if grid == "tetra" else ski.dust_sphere1d(50000)
+    log, g, c = both(tmp_path, text, "dust")
+    assert "secondary histories on the B200" in log
+    z, _ = tb.sed_z(g, c, "dust", "sed")
+    assert len(z) > 25
+    tb.check(z, 2.0, 5.0)
+
+
+@needs_build
 @pytest.mark.parametrize("grid", sorted(tb.GRID_SCENES))
 def test_bridge_grids_on_oracle(tmp_path, grid):
     """The disk scene on the adaptive-mesh, Voronoi, tetrahedral, spherical and cylindrical grids:

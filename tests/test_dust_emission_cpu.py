@@ -20,7 +20,7 @@ import numpy as np
 import pytest
 
 from helpers import zscores
-from skgpu import Scene
+from skgpu import Scene, abi
 
 FIXTURES = ["dust_shell.npz", "dust_galaxy.npz"]
 
@@ -83,3 +83,42 @@ def test_oracle_secondary_refuses_unprepared(golden, oracle_backend):
     oracle_backend.set_options(sc.options(seed=1))
     with pytest.raises(SkgpuError):
         oracle_backend.run_secondary(0, 10)
+
+
+def secondary_on_grid(golden, grid_fixture):
+    """The dust shell's emission tables and a seeded radiation field on another grid (the tetrahedral
+    or 1D spherical path fixture): a scene whose secondary launch draws positions in tetrahedra or
+    spherical shells. Cell volumes are those of the grid's cells."""
+    dust = Scene.from_export(golden("dust_shell.npz"))
+    z = golden(grid_fixture)
+    sc = Scene.from_export(z)
+    n = len(sc.density)
+    if sc.grid["kind"] == abi.GRID_TETRA:
+        v, t = sc.grid["vertices"], sc.grid["tetra"]
+        a, b, c, d = (v[t[:, q]] for q in range(4))
+        vol = np.abs(np.einsum("ij,ij->i", b - a, np.cross(c - a, d - a))) / 6.0
+    else:
+        r = np.asarray(sc.grid["rv"])
+        vol = 4.0 / 3.0 * np.pi * (r[1:] ** 3 - r[:-1] ** 3)
+    sc.mix = dust.mix
+    sc.instruments = dust.instruments
+    sc.rf = dust.rf
+    sc.store_rf = True
+    sc.dust_emission = dict(dust.dust_emission, cell_volume=vol)
+    sc.secondary = dust.secondary
+    rng = np.random.default_rng(17)
+    rf = rng.uniform(0.5, 1.5, (n, dust.rf["num_bins"])) * np.median(golden("dust_shell.npz")["rf1"])
+    return sc, rf
+
+
+@pytest.mark.parametrize("fixture", ["paths_tetra.npz", "paths_sphere1d.npz"])
+def test_oracle_secondary_launch_in_cells(golden, oracle_backend, fixture):
+    """The oracle's secondary segment on a tetrahedral mesh and a 1D spherical grid (launch positions
+    in tetrahedra and spherical shells) runs every history and reaches the instruments; its
+    distributions are tested against the reference's runs through the bridge
+    (test_bridge_cpu.py), the GPU's launches against these (test_gpu_secondary.py)."""
+    sc, rf = secondary_on_grid(golden, fixture)
+    sc.upload(oracle_backend)
+    res, L = sc.run_secondary(oracle_backend, 4000, seed=3, rf=rf)
+    assert L > 0 and res.counters["histories"] == 4000
+    assert sum(float(ins["total"].sum()) for ins in res.instruments) > 0

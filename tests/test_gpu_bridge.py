@@ -174,6 +174,20 @@ def test_bridge_dust_emission_adaptive(tmp_path):
 
 
 @needs_build
+@pytest.mark.parametrize("grid", ["tetra", "sphere1d"])
+def test_bridge_dust_emission_other_grids(tmp_path, grid):
+    """DustEmission on a tetrahedral mesh and a 1D spherical grid through skirt_gpu -g."""
+    text = ski.dust_tetra(200000) if grid == "tetra" else ski.dust_sphere1d(200000)
+    log, g, c = both(tmp_path, text, "dust")
+    assert "secondary histories on the B200" in log
+    z, _ = sed_z(g, c, "dust", "sed")
+    assert len(z) > 25
+    check(z, 2.0, 5.0)
+    z, _ = frame_z(g, c, "dust", "i30")
+    check(z, 1.3, 6.0)
+
+
+@needs_build
 @pytest.mark.parametrize("grid", sorted(GRID_SCENES))
 def test_bridge_grids(tmp_path, grid):
     """The disk scene on the adaptive-mesh, Voronoi, tetrahedral, spherical and cylindrical grids

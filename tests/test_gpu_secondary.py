@@ -106,3 +106,25 @@ def test_gpu_primary_then_secondary_on_device(golden, gpu_backend):
     gpu_backend.clear_tallies()  # the prepared segment no longer needs the radiation field
     gpu_backend.run_secondary(0, npp)
     check_vs_reference(sc.fetch(gpu_backend, rf=False), z, sc, npp, chi2_max=1.6, zmax=6.5, tot_rel=0.03)
+
+
+@pytest.mark.parametrize("fixture", ["paths_tetra.npz", "paths_sphere1d.npz"])
+def test_gpu_secondary_other_grids_equal_oracle(golden, gpu_backend, oracle_backend, fixture):
+    """Secondary launches in tetrahedra (TetraMeshSpatialGrid::Tetra::generatePosition) and spherical
+    shells (Sphere1DSpatialGrid::randomPositionInCell): the FP64 secondary life cycle equals the
+    oracle's history by history (the shells' radii through CUDA's cbrt, to the last bit or so)."""
+    from test_dust_emission_cpu import secondary_on_grid
+    sc, rf = secondary_on_grid(golden, fixture)
+    n = 20000
+    sc.upload(gpu_backend)
+    sc.upload(oracle_backend)
+    rg, Lg = sc.run_secondary(gpu_backend, n, seed=13, rf=rf)
+    ro, Lo = sc.run_secondary(oracle_backend, n, seed=13, rf=rf)
+    assert Lg == pytest.approx(Lo, rel=1e-12)
+    assert rg.counters["histories"] == n
+    assert rg.counters["scatterings"] == pytest.approx(ro.counters["scatterings"], rel=1e-3)
+    for a, b in zip(rg.instruments, ro.instruments):
+        ta, tb = a["total"].ravel(), b["total"].ravel()
+        assert tb.sum() > 0
+        assert ta.sum() == pytest.approx(tb.sum(), rel=1e-6)
+        assert np.mean(np.isclose(ta, tb, rtol=1e-9, atol=1e-12 * np.abs(tb).max())) > 0.99
