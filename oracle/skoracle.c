@@ -2617,9 +2617,8 @@ int or_prepare_secondary(or_ctx* c, const skgpu_secondary_options* opt, uint64_t
     if (!opt || total_packets == 0) return fail(c, SKGPU_ERR_ARG, "secondary: missing options or packets");
     if (!c->hasGrid || (c->g.kind != SKGPU_GRID_CARTESIAN && c->g.kind != SKGPU_GRID_OCTREE
                         && c->g.kind != SKGPU_GRID_ADAPTIVE_MESH && c->g.kind != SKGPU_GRID_TETRA
-                        && c->g.kind != SKGPU_GRID_SPHERE1D))
-        return fail(c, SKGPU_ERR_UNSUPPORTED, "secondary: dust emission needs a Cartesian, octree, adaptive-mesh, "
-                                              "tetrahedral or 1D spherical grid");
+                        && (c->g.kind < SKGPU_GRID_SPHERE1D || c->g.kind > SKGPU_GRID_CYLINDER3D)))
+        return fail(c, SKGPU_ERR_UNSUPPORTED, "secondary: dust emission is not available on a Voronoi grid");
     if (!c->deNrf || c->deCells != c->numCells || c->deNrf != c->nrf)
         return fail(c, SKGPU_ERR_STATE, "secondary: dust emission tables do not match the medium and RF grid");
     if (!c->rf || c->rfLen != (size_t)c->numCells * c->nrf) return fail(c, SKGPU_ERR_STATE, "secondary: no radiation field");
@@ -2873,6 +2872,41 @@ static void launch_secondary(or_ctx* c, Rng* r, uint64_t hist, Packet* pk)
         pk->rx = rad * ux;
         pk->ry = rad * uy;
         pk->rz = rad * uz;
+    }
+    else if (c->g.kind == SKGPU_GRID_CYLINDER2D || c->g.kind == SKGPU_GRID_CYLINDER3D)
+    {
+        /* Cylinder2DSpatialGrid.cpp:95-106, Cylinder3DSpatialGrid.cpp:133-144; Position.cpp:21-29 */
+        const Grid* g = &c->g;
+        int i, j = 0, k;
+        const double *Rv, *zv;
+        if (g->kind == SKGPU_GRID_CYLINDER2D) { i = m / g->cnz; k = m % g->cnz; Rv = g->crv; zv = g->czv; }
+        else { i = m / (g->c3np * g->c3nz); j = (m / g->c3nz) % g->c3np; k = m % g->c3nz; Rv = g->c3r; zv = g->c3z; }
+        double R0 = Rv[i], R1 = Rv[i + 1], z0 = zv[k], z1 = zv[k + 1];
+        double R = sqrt(R0 * R0 + (R1 - R0) * (R1 + R0) * uniform(r));
+        double phi = g->kind == SKGPU_GRID_CYLINDER2D ? 2.0 * M_PI * uniform(r)
+                                                       : g->c3p[j] + (g->c3p[j + 1] - g->c3p[j]) * uniform(r);
+        double z = z0 + (z1 - z0) * uniform(r);
+        pk->rx = R * cos(phi);
+        pk->ry = R * sin(phi);
+        pk->rz = z;
+    }
+    else if (c->g.kind == SKGPU_GRID_SPHERE2D || c->g.kind == SKGPU_GRID_SPHERE3D)
+    {
+        /* Sphere2DSpatialGrid.cpp:102-113, Sphere3DSpatialGrid.cpp:146-157; Position.cpp:30-43 */
+        const Grid* g = &c->g;
+        int i, j, k = 0;
+        const double *rv, *tv;
+        if (g->kind == SKGPU_GRID_SPHERE2D) { i = m / g->s2nt; j = m % g->s2nt; rv = g->s2r; tv = g->s2t; }
+        else { i = m / (g->s3nt * g->s3np); j = (m / g->s3np) % g->s3nt; k = m % g->s3np; rv = g->s3r; tv = g->s3t; }
+        double r0 = rv[i], r1 = rv[i + 1];
+        double rad = cbrt(r0 * r0 * r0 + (r1 - r0) * (r1 * r1 + r1 * r0 + r0 * r0) * uniform(r));
+        double theta = acos(cos(tv[j]) + (cos(tv[j + 1]) - cos(tv[j])) * uniform(r));
+        double phi = g->kind == SKGPU_GRID_SPHERE2D ? 2.0 * M_PI * uniform(r)
+                                                     : g->s3p[k] + (g->s3p[k + 1] - g->s3p[k]) * uniform(r);
+        double st = sin(theta);
+        pk->rx = rad * st * cos(phi);
+        pk->ry = rad * st * sin(phi);
+        pk->rz = rad * cos(theta);
     }
     else
     {

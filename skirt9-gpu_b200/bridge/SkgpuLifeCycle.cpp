@@ -163,8 +163,7 @@ namespace
         else
         {
             // grids whose randomPositionInCell the library reproduces for the secondary launch
-            if (!box && !dynamic_cast<TetraMeshSpatialGrid*>(grid) && !dynamic_cast<Sphere1DSpatialGrid*>(grid))
-                return (why = "secondary emission on this grid type"), false;
+            if (dynamic_cast<VoronoiMeshSpatialGrid*>(grid)) return (why = "secondary emission on a Voronoi grid"), false;
             if (!config->hasDustEmission() || config->hasGasEmission() || config->hasStochasticDustEmission()
                 || config->storeEmissionRadiationField() || !config->hasPanRadiationField())
                 return (why = "secondary emission other than equilibrium dust emission"), false;

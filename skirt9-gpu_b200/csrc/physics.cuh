@@ -298,6 +298,73 @@ SKG_D Launched launchSecondary(const Scene& p, unsigned long long hist, Rng& rng
         o.y = xmul(r, uy);
         o.z = xmul(r, uz);
     }
+    else if (p.g.kind >= 5 && p.g.kind <= 8)
+    {
+        // the cylindrical and spherical grids' randomPositionInCell (Cylinder2DSpatialGrid.cpp:95-106,
+        // Sphere2DSpatialGrid.cpp:102-113, Sphere3DSpatialGrid.cpp:146-157,
+        // Cylinder3DSpatialGrid.cpp:133-144) with getCoords' bin indices and Position's cylindrical
+        // and spherical constructors (SKIRT/utils/Position.cpp:21-43)
+        const double twoPi = 2.0 * M_PI;
+        if (p.g.kind == 5 || p.g.kind == 8)
+        {
+            int i, j = 0, k;
+            const double *Rv, *zv;
+            if (p.g.kind == 5)
+            {
+                i = m / p.g.cNz;
+                k = m % p.g.cNz;
+                Rv = p.g.cRv;
+                zv = p.g.czv;
+            }
+            else
+            {
+                i = m / (p.g.c3Np * p.g.c3Nz);
+                j = (m / p.g.c3Nz) % p.g.c3Np;
+                k = m % p.g.c3Nz;
+                Rv = p.g.c3r;
+                zv = p.g.c3z;
+            }
+            double R0 = Rv[i], R1 = Rv[i + 1], z0 = zv[k], z1 = zv[k + 1];
+            double R = sqrt(xadd(xmul(R0, R0), xmul(xmul(xsub(R1, R0), xadd(R1, R0)), rng.uniform())));
+            double phi = p.g.kind == 5 ? xmul(twoPi, rng.uniform())
+                                       : xadd(p.g.c3p[j], xmul(xsub(p.g.c3p[j + 1], p.g.c3p[j]), rng.uniform()));
+            double z = xadd(z0, xmul(xsub(z1, z0), rng.uniform()));
+            o.x = xmul(R, cos(phi));
+            o.y = xmul(R, sin(phi));
+            o.z = z;
+        }
+        else
+        {
+            int i, j, k = 0;
+            const double *rv, *tv;
+            if (p.g.kind == 6)
+            {
+                i = m / p.g.s2Nt;
+                j = m % p.g.s2Nt;
+                rv = p.g.s2r;
+                tv = p.g.s2t;
+            }
+            else
+            {
+                i = m / (p.g.s3Nt * p.g.s3Np);
+                j = (m / p.g.s3Np) % p.g.s3Nt;
+                k = m % p.g.s3Np;
+                rv = p.g.s3r;
+                tv = p.g.s3t;
+            }
+            double r0 = rv[i], r1 = rv[i + 1], t0 = tv[j], t1 = tv[j + 1];
+            double d3 = xmul(xsub(r1, r0), xadd(xadd(xmul(r1, r1), xmul(r1, r0)), xmul(r0, r0)));
+            double r = cbrt(xadd(xmul(xmul(r0, r0), r0), xmul(d3, rng.uniform())));
+            double c0 = cos(t0);
+            double theta = acos(xadd(c0, xmul(xsub(cos(t1), c0), rng.uniform())));
+            double phi = p.g.kind == 6 ? xmul(twoPi, rng.uniform())
+                                       : xadd(p.g.s3p[k], xmul(xsub(p.g.s3p[k + 1], p.g.s3p[k]), rng.uniform()));
+            double st = sin(theta);
+            o.x = xmul(xmul(r, st), cos(phi));
+            o.y = xmul(xmul(r, st), sin(phi));
+            o.z = xmul(r, cos(theta));
+        }
+    }
     else
     {
         // the cell box (Random::position, Box::fracPos): Cartesian borders, or the extent of the

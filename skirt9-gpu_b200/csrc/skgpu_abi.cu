@@ -1708,9 +1708,8 @@ int skgpu_prepare_secondary(skgpu_ctx* ctx, const skgpu_secondary_options* opt, 
     if (!opt || total_packets == 0) return fail(ctx, SKGPU_ERR_ARG, "secondary: missing options or packets");
     if (!ctx->hasGrid || (ctx->g.kind != SKGPU_GRID_CARTESIAN && ctx->g.kind != SKGPU_GRID_OCTREE
                           && ctx->g.kind != SKGPU_GRID_ADAPTIVE_MESH && ctx->g.kind != SKGPU_GRID_TETRA
-                          && ctx->g.kind != SKGPU_GRID_SPHERE1D))
-        return fail(ctx, SKGPU_ERR_UNSUPPORTED, "secondary: dust emission needs a Cartesian, octree, adaptive-mesh, "
-                                                "tetrahedral or 1D spherical grid");
+                          && (ctx->g.kind < SKGPU_GRID_SPHERE1D || ctx->g.kind > SKGPU_GRID_CYLINDER3D)))
+        return fail(ctx, SKGPU_ERR_UNSUPPORTED, "secondary: dust emission is not available on a Voronoi grid");
     if (!ctx->dens || ctx->numCells != ctx->g.numCells) return fail(ctx, SKGPU_ERR_STATE, "secondary: medium does not match the grid");
     if (!ctx->de.nrf || ctx->deCells != ctx->numCells || ctx->de.nrf != ctx->nrf)
         return fail(ctx, SKGPU_ERR_STATE, "secondary: dust emission tables do not match the medium and RF grid");

@@ -525,3 +525,13 @@ def dust_tetra(num_packets=1e5, num_vertices=3000):
 def dust_sphere1d(num_packets=1e5):
     """DustEmission (the dust_shell configuration) on a Sphere1DSpatialGrid of 24 shells 0.05-1 pc."""
     return dust_shell(num_packets, grid=sphere1d_grid(0.05, 1, 24))
+
+
+def dust_curvilinear(num_packets, kind):
+    """DustEmission (the dust_shell configuration) on a spherical or cylindrical grid of the +-1 pc
+    shell: kind in sphere2d, sphere3d, cylinder2d, cylinder3d."""
+    grid = {"sphere2d": lambda: sphere2d_grid(0.05, 1, 16, 12),
+            "sphere3d": lambda: sphere3d_grid(0.05, 1, 12, 8, 8),
+            "cylinder2d": lambda: cylinder2d_grid(0.05, 1, -1, 1, 16, 16),
+            "cylinder3d": lambda: cylinder3d_grid(0.05, 1, -1, 1, 12, 8, 12)}[kind]()
+    return dust_shell(num_packets, grid=grid)

@@ -83,11 +83,11 @@ def test_bridge_dust_emission_adaptive_on_oracle(tmp_path):
 
 
 @needs_build
-@pytest.mark.parametrize("grid", ["tetra", "sphere1d"])
+@pytest.mark.parametrize("grid", ["tetra", "sphere1d", "sphere2d", "sphere3d", "cylinder2d", "cylinder3d"])
 def test_bridge_dust_emission_other_grids_on_oracle(tmp_path, grid):
-    """DustEmission on a tetrahedral mesh and a 1D spherical grid: secondary launches at random
-    positions in tetrahedra (barycentric fold) and spherical shells."""
-    text = ski.dust_tetra(50000) if grid == "tetra" else ski.dust_sphere1d(50000)
+    """DustEmission on the tetrahedral, spherical and cylindrical grids: secondary launches at random
+    positions in tetrahedra (barycentric fold) and in curvilinear cells."""
+    text = tb.dust_scene(grid, 50000)
     log, g, c = both(tmp_path, text, "dust")
     assert "secondary histories on the B200" in log
     z, _ = tb.sed_z(g, c, "dust", "sed")

@@ -97,9 +97,11 @@ def secondary_on_grid(golden, grid_fixture):
         v, t = sc.grid["vertices"], sc.grid["tetra"]
         a, b, c, d = (v[t[:, q]] for q in range(4))
         vol = np.abs(np.einsum("ij,ij->i", b - a, np.cross(c - a, d - a))) / 6.0
-    else:
+    elif sc.grid["kind"] == abi.GRID_SPHERE1D:
         r = np.asarray(sc.grid["rv"])
         vol = 4.0 / 3.0 * np.pi * (r[1:] ** 3 - r[:-1] ** 3)
+    else:
+        vol = np.full(n, 1e48)  # any positive volumes: GPU and oracle share them
     sc.mix = dust.mix
     sc.instruments = dust.instruments
     sc.rf = dust.rf
@@ -111,10 +113,14 @@ def secondary_on_grid(golden, grid_fixture):
     return sc, rf
 
 
-@pytest.mark.parametrize("fixture", ["paths_tetra.npz", "paths_sphere1d.npz"])
+OTHER_GRIDS = ["paths_tetra.npz", "paths_sphere1d.npz", "paths_cylinder2d.npz", "paths_sphere2d.npz",
+               "paths_sphere3d.npz", "paths_cylinder3d.npz"]
+
+
+@pytest.mark.parametrize("fixture", OTHER_GRIDS)
 def test_oracle_secondary_launch_in_cells(golden, oracle_backend, fixture):
-    """The oracle's secondary segment on a tetrahedral mesh and a 1D spherical grid (launch positions
-    in tetrahedra and spherical shells) runs every history and reaches the instruments; its
+    """The oracle's secondary segment on the tetrahedral, spherical and cylindrical grids (launch
+    positions in tetrahedra and in curvilinear cells) runs every history and reaches the instruments; its
     distributions are tested against the reference's runs through the bridge
     (test_bridge_cpu.py), the GPU's launches against these (test_gpu_secondary.py)."""
     sc, rf = secondary_on_grid(golden, fixture)

@@ -174,10 +174,19 @@ def test_bridge_dust_emission_adaptive(tmp_path):
 
 
 @needs_build
-@pytest.mark.parametrize("grid", ["tetra", "sphere1d"])
+def dust_scene(grid, n):
+    """The DustEmission shell on one of the non-box grids."""
+    if grid == "tetra":
+        return ski.dust_tetra(n)
+    if grid == "sphere1d":
+        return ski.dust_sphere1d(n)
+    return ski.dust_curvilinear(n, grid)
+
+
+@pytest.mark.parametrize("grid", ["tetra", "sphere1d", "sphere2d", "sphere3d", "cylinder2d", "cylinder3d"])
 def test_bridge_dust_emission_other_grids(tmp_path, grid):
-    """DustEmission on a tetrahedral mesh and a 1D spherical grid through skirt_gpu -g."""
-    text = ski.dust_tetra(200000) if grid == "tetra" else ski.dust_sphere1d(200000)
+    """DustEmission on the tetrahedral, spherical and cylindrical grids through skirt_gpu -g."""
+    text = dust_scene(grid, 200000)
     log, g, c = both(tmp_path, text, "dust")
     assert "secondary histories on the B200" in log
     z, _ = sed_z(g, c, "dust", "sed")
