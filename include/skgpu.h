@@ -175,6 +175,12 @@ int skgpu_upload_grid_adaptive_mesh(skgpu_ctx* ctx, int32_t num_nodes, const dou
  * (VoronoiMeshSnapshot.cpp:725-740); extent xmin..zmax; eps = 1e-12 * diagonal. */
 int skgpu_upload_grid_voronoi(skgpu_ctx* ctx, int32_t num_sites, const double* sites, const int32_t* nb_begin,
                               const int32_t* nb_index, int32_t num_nb_index, const double* extent, double eps);
+/* Enclosing box of every Voronoi cell (VoronoiMeshSnapshot::extent(m), VoronoiMeshSnapshot.hpp:282;
+ * xmin, ymin, zmin, xmax, ymax, zmax per cell), for the secondary launch: a position is drawn in the
+ * cell's box until it lies closer to the cell's site than to every neighbouring site
+ * (VoronoiMeshSnapshot::generatePosition / isPointClosestTo, VoronoiMeshSnapshot.cpp:879-887,
+ * 1007-1020; at most 10000 draws). Call after skgpu_upload_grid_voronoi. */
+int skgpu_upload_voronoi_cell_boxes(skgpu_ctx* ctx, int32_t num_cells, const double* boxes);
 /* Sphere1DSpatialGrid: the num_borders ascending radial border positions r_0 >= 0 .. r_N of its N
  * radial cells (Sphere1DSpatialGrid::radialBorderPositions, Sphere1DSpatialGrid.hpp:101); cell i is
  * the shell r_i <= r < r_{i+1} around the origin. */

@@ -109,6 +109,7 @@ typedef struct
     int *adiv, *acb, *ach;
     /* voronoi */
     double* vs;
+    double* vbox; /* per cell enclosing box (secondary launch) */
     int *vnbb, *vnb;
     int vn;
     /* tetra */
@@ -200,7 +201,7 @@ static void free_grid(Grid* g)
     free(g->xb); free(g->yb); free(g->zb);
     free(g->tb); free(g->tcell); free(g->tchild); free(g->tnbb); free(g->tnb);
     free(g->adiv); free(g->acb); free(g->ach);
-    free(g->vs); free(g->vnbb); free(g->vnb);
+    free(g->vs); free(g->vbox); free(g->vnbb); free(g->vnb);
     free(g->tev); free(g->ten); free(g->tebox); free(g->tet); free(g->tent); free(g->tenf);
     free(g->srv);
     free(g->crv); free(g->czv);
@@ -408,6 +409,15 @@ int or_upload_grid_adaptive_mesh(or_ctx* c, int32_t num_nodes, const double* bou
     g->eps = eps;
     g->numCells = numCells;
     c->hasGrid = 1;
+    return SKGPU_OK;
+}
+
+int or_upload_voronoi_cell_boxes(or_ctx* c, int32_t num_cells, const double* boxes)
+{
+    if (!c->hasGrid || c->g.kind != SKGPU_GRID_VORONOI) return fail(c, SKGPU_ERR_STATE, "voronoi boxes: no Voronoi grid");
+    if (num_cells != c->g.vn || !boxes) return fail(c, SKGPU_ERR_ARG, "voronoi boxes: one box per cell expected");
+    free(c->g.vbox);
+    c->g.vbox = dup(boxes, 6 * (size_t)num_cells * sizeof(double));
     return SKGPU_OK;
 }
 
@@ -2617,8 +2627,9 @@ int or_prepare_secondary(or_ctx* c, const skgpu_secondary_options* opt, uint64_t
     if (!opt || total_packets == 0) return fail(c, SKGPU_ERR_ARG, "secondary: missing options or packets");
     if (!c->hasGrid || (c->g.kind != SKGPU_GRID_CARTESIAN && c->g.kind != SKGPU_GRID_OCTREE
                         && c->g.kind != SKGPU_GRID_ADAPTIVE_MESH && c->g.kind != SKGPU_GRID_TETRA
-                        && (c->g.kind < SKGPU_GRID_SPHERE1D || c->g.kind > SKGPU_GRID_CYLINDER3D)))
-        return fail(c, SKGPU_ERR_UNSUPPORTED, "secondary: dust emission is not available on a Voronoi grid");
+                        && (c->g.kind < SKGPU_GRID_SPHERE1D || c->g.kind > SKGPU_GRID_CYLINDER3D)
+                        && !(c->g.kind == SKGPU_GRID_VORONOI && c->g.vbox)))
+        return fail(c, SKGPU_ERR_UNSUPPORTED, "secondary: a Voronoi grid needs its cell boxes (or_upload_voronoi_cell_boxes)");
     if (!c->deNrf || c->deCells != c->numCells || c->deNrf != c->nrf)
         return fail(c, SKGPU_ERR_STATE, "secondary: dust emission tables do not match the medium and RF grid");
     if (!c->rf || c->rfLen != (size_t)c->numCells * c->nrf) return fail(c, SKGPU_ERR_STATE, "secondary: no radiation field");
@@ -2872,6 +2883,34 @@ static void launch_secondary(or_ctx* c, Rng* r, uint64_t hist, Packet* pk)
         pk->rx = rad * ux;
         pk->ry = rad * uy;
         pk->rz = rad * uz;
+    }
+    else if (c->g.kind == SKGPU_GRID_VORONOI)
+    {
+        /* VoronoiMeshSnapshot::generatePosition / isPointClosestTo (VoronoiMeshSnapshot.cpp:879-887, 1007-1020) */
+        const Grid* g = &c->g;
+        const double* bb = g->vbox + 6 * (size_t)m;
+        const double* sm = g->vs + 3 * (size_t)m;
+        for (int tries = 0; tries < 10000; ++tries)
+        {
+            double fx = uniform(r);
+            double fy = uniform(r);
+            double fz = uniform(r);
+            pk->rx = bb[0] + fx * (bb[3] - bb[0]);
+            pk->ry = bb[1] + fy * (bb[4] - bb[1]);
+            pk->rz = bb[2] + fz * (bb[5] - bb[2]);
+            double dx = pk->rx - sm[0], dy = pk->ry - sm[1], dz = pk->rz - sm[2];
+            double target = dx * dx + dy * dy + dz * dz;
+            int closest = 1;
+            for (int e = g->vnbb[m]; e < g->vnbb[m + 1] && closest; ++e)
+            {
+                int id = g->vnb[e];
+                if (id < 0) continue;
+                const double* q = g->vs + 3 * (size_t)id;
+                double ex = pk->rx - q[0], ey = pk->ry - q[1], ez = pk->rz - q[2];
+                if (ex * ex + ey * ey + ez * ez < target) closest = 0;
+            }
+            if (closest) break;
+        }
     }
     else if (c->g.kind == SKGPU_GRID_CYLINDER2D || c->g.kind == SKGPU_GRID_CYLINDER3D)
     {

@@ -37,6 +37,7 @@ int or_upload_grid_octree(or_ctx* ctx, int32_t num_nodes, const double* bounds, 
 int or_upload_grid_adaptive_mesh(or_ctx* ctx, int32_t num_nodes, const double* bounds, const int32_t* cell_index,
                                  const int32_t* child_begin, const int32_t* child_count, const int32_t* child_index,
                                  int32_t num_child_index, double eps);
+int or_upload_voronoi_cell_boxes(or_ctx* ctx, int32_t num_cells, const double* boxes);
 int or_upload_grid_voronoi(or_ctx* ctx, int32_t num_sites, const double* sites, const int32_t* nb_begin,
                            const int32_t* nb_index, int32_t num_nb_index, const double* extent, double eps);
 int or_upload_grid_sphere1d(or_ctx* ctx, int32_t num_borders, const double* radial_borders);

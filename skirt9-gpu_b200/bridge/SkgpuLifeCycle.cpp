@@ -163,7 +163,6 @@ namespace
         else
         {
             // grids whose randomPositionInCell the library reproduces for the secondary launch
-            if (dynamic_cast<VoronoiMeshSpatialGrid*>(grid)) return (why = "secondary emission on a Voronoi grid"), false;
             if (!config->hasDustEmission() || config->hasGasEmission() || config->hasStochasticDustEmission()
                 || config->storeEmissionRadiationField() || !config->hasPanRadiationField())
                 return (why = "secondary emission other than equilibrium dust emission"), false;
@@ -250,6 +249,15 @@ namespace
             check(skgpu_upload_grid_voronoi(g_ctx, n, m->_traversalSiteCoordinates.data(), begin.data(), index.data(),
                                             index.size(), ext, m->_eps),
                   "Voronoi mesh");
+            // the cells' enclosing boxes, for the secondary launch (VoronoiMeshSnapshot::extent(m))
+            std::vector<double> boxes(6 * static_cast<size_t>(n));
+            for (int c = 0; c != n; ++c)
+            {
+                Box b = m->extent(c);
+                double* q = &boxes[6 * static_cast<size_t>(c)];
+                q[0] = b.xmin(); q[1] = b.ymin(); q[2] = b.zmin(); q[3] = b.xmax(); q[4] = b.ymax(); q[5] = b.zmax();
+            }
+            check(skgpu_upload_voronoi_cell_boxes(g_ctx, n, boxes.data()), "Voronoi cell boxes");
             return;
         }
         if (auto g = dynamic_cast<TetraMeshSpatialGrid*>(grid))

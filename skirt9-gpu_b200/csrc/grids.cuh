@@ -67,6 +67,7 @@ struct GridDev
     const int* vBlkBegin;  // vGridN^3 + 1
     const int* vBlkSites;  // site indices per block
     const int* vBlkRep;    // vGridN^3: a site in or near each block (start of the greedy locate)
+    const double* vBox;    // per cell its enclosing box (secondary launch), or null
 
     // tetra: vertices, vertex indices (4 per tet), face normals (12 per tet), neighbour tet and
     // face per face, tet bounding boxes, uniform tet-search grid

@@ -298,7 +298,35 @@ SKG_D Launched launchSecondary(const Scene& p, unsigned long long hist, Rng& rng
         o.y = xmul(r, uy);
         o.z = xmul(r, uz);
     }
-    else if (p.g.kind >= 5 && p.g.kind <= 8)
+    else if (p.g.kind == 2)
+    {
+        // VoronoiMeshSnapshot::generatePosition (VoronoiMeshSnapshot.cpp:1007-1020): positions in the
+        // cell's enclosing box (Random::position, x, y, z drawn in that order) until one lies at
+        // least as close to the cell's site as to every neighbouring site (isPointClosestTo,
+        // :879-887, squared distances (r - site).norm2())
+        const double* bb = p.g.vBox + 6 * static_cast<size_t>(m);
+        const double* sm = p.g.vSites + 3 * static_cast<size_t>(m);
+        auto dist2 = [](const double* q, double x, double y, double z) {
+            double dx = xsub(x, q[0]), dy = xsub(y, q[1]), dz = xsub(z, q[2]);
+            return xadd(xadd(xmul(dx, dx), xmul(dy, dy)), xmul(dz, dz));
+        };
+        for (int tries = 0; tries < 10000; ++tries)
+        {
+            double fx = rng.uniform(), fy = rng.uniform(), fz = rng.uniform();
+            o.x = xadd(bb[0], xmul(fx, xsub(bb[3], bb[0])));
+            o.y = xadd(bb[1], xmul(fy, xsub(bb[4], bb[1])));
+            o.z = xadd(bb[2], xmul(fz, xsub(bb[5], bb[2])));
+            double target = dist2(sm, o.x, o.y, o.z);
+            bool closest = true;
+            for (int e = p.g.vNbBegin[m]; e < p.g.vNbBegin[m + 1] && closest; ++e)
+            {
+                int id = p.g.vNb[e];
+                if (id >= 0 && dist2(p.g.vSites + 3 * static_cast<size_t>(id), o.x, o.y, o.z) < target) closest = false;
+            }
+            if (closest) break;
+        }
+    }
+        else if (p.g.kind >= 5 && p.g.kind <= 8)
     {
         // the cylindrical and spherical grids' randomPositionInCell (Cylinder2DSpatialGrid.cpp:95-106,
         // Sphere2DSpatialGrid.cpp:102-113, Sphere3DSpatialGrid.cpp:146-157,

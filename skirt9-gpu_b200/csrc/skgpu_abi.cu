@@ -861,6 +861,16 @@ int skgpu_upload_grid_voronoi(skgpu_ctx* ctx, int32_t num_sites, const double* s
     return SKGPU_OK;
 }
 
+int skgpu_upload_voronoi_cell_boxes(skgpu_ctx* ctx, int32_t num_cells, const double* boxes)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (!ctx->hasGrid || ctx->g.kind != SKGPU_GRID_VORONOI) return fail(ctx, SKGPU_ERR_STATE, "voronoi boxes: no Voronoi grid");
+    if (num_cells != ctx->g.vN || !boxes) return fail(ctx, SKGPU_ERR_ARG, "voronoi boxes: one box per cell expected");
+    if (!finiteAll(boxes, 6 * static_cast<size_t>(num_cells))) return fail(ctx, SKGPU_ERR_ARG, "voronoi boxes: non-finite value");
+    CK(cudaSetDevice(ctx->device));
+    return gridUpload(ctx, &ctx->g.vBox, boxes, 6 * static_cast<size_t>(num_cells));
+}
+
 int skgpu_upload_grid_sphere1d(skgpu_ctx* ctx, int32_t num_borders, const double* rv)
 {
     if (!ctx) return SKGPU_ERR_ARG;
@@ -1708,8 +1718,9 @@ int skgpu_prepare_secondary(skgpu_ctx* ctx, const skgpu_secondary_options* opt, 
     if (!opt || total_packets == 0) return fail(ctx, SKGPU_ERR_ARG, "secondary: missing options or packets");
     if (!ctx->hasGrid || (ctx->g.kind != SKGPU_GRID_CARTESIAN && ctx->g.kind != SKGPU_GRID_OCTREE
                           && ctx->g.kind != SKGPU_GRID_ADAPTIVE_MESH && ctx->g.kind != SKGPU_GRID_TETRA
-                          && (ctx->g.kind < SKGPU_GRID_SPHERE1D || ctx->g.kind > SKGPU_GRID_CYLINDER3D)))
-        return fail(ctx, SKGPU_ERR_UNSUPPORTED, "secondary: dust emission is not available on a Voronoi grid");
+                          && (ctx->g.kind < SKGPU_GRID_SPHERE1D || ctx->g.kind > SKGPU_GRID_CYLINDER3D)
+                          && !(ctx->g.kind == SKGPU_GRID_VORONOI && ctx->g.vBox)))
+        return fail(ctx, SKGPU_ERR_UNSUPPORTED, "secondary: a Voronoi grid needs its cell boxes (skgpu_upload_voronoi_cell_boxes)");
     if (!ctx->dens || ctx->numCells != ctx->g.numCells) return fail(ctx, SKGPU_ERR_STATE, "secondary: medium does not match the grid");
     if (!ctx->de.nrf || ctx->deCells != ctx->numCells || ctx->de.nrf != ctx->nrf)
         return fail(ctx, SKGPU_ERR_STATE, "secondary: dust emission tables do not match the medium and RF grid");

@@ -125,6 +125,7 @@ SIGNATURES = {
     "upload_grid_octree": [_P, _I, _P, _P, _P, _P, _P, _I, _P, _P, _I, _D],
     "upload_grid_adaptive_mesh": [_P, _I, _P, _P, _P, _P, _P, _I, _D],
     "upload_grid_voronoi": [_P, _I, _P, _P, _P, _I, _P, _D],
+    "upload_voronoi_cell_boxes": [_P, _I, _P],
     "upload_grid_tetra": [_P, _I, _P, _I, _P, _P, _P, _P, _P, _D],
     "upload_grid_sphere1d": [_P, _I, _P],
     "upload_grid_cylinder2d": [_P, _I, _P, _I, _P],
@@ -259,6 +260,10 @@ class Backend:
         b, ci, cb, cc, cx = f64(bounds), i32(cell_index), i32(child_begin), i32(child_count), i32(child_index)
         self.call("upload_grid_adaptive_mesh", len(ci), _ptr(b), _ptr(ci), _ptr(cb), _ptr(cc), _ptr(cx), len(cx),
                   float(eps))
+
+    def upload_voronoi_cell_boxes(self, boxes):
+        b = f64(boxes).reshape(-1, 6)
+        self.call("upload_voronoi_cell_boxes", len(b), _ptr(b))
 
     def upload_grid_voronoi(self, sites, nb_begin, nb_index, extent, eps):
         s, nbb, nbi, ext = f64(sites), i32(nb_begin), i32(nb_index), f64(extent)

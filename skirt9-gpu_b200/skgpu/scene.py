@@ -118,6 +118,8 @@ class Scene:
                                          g["child_index"], g["eps"])
         elif k == abi.GRID_VORONOI:
             be.upload_grid_voronoi(g["sites"], g["nb_begin"], g["nb_index"], g["extent"], g["eps"])
+            if g.get("boxes") is not None:
+                be.upload_voronoi_cell_boxes(g["boxes"])
         elif k == abi.GRID_TETRA:
             be.upload_grid_tetra(g["vertices"], g["tetra"], g["normals"], g["ntetra"], g["nface"], g["extent"], g["eps"])
         elif k == abi.GRID_SPHERE1D:

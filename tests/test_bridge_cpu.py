@@ -83,11 +83,12 @@ def test_bridge_dust_emission_adaptive_on_oracle(tmp_path):
 
 
 @needs_build
-@pytest.mark.parametrize("grid", ["tetra", "sphere1d", "sphere2d", "sphere3d", "cylinder2d", "cylinder3d"])
+@pytest.mark.parametrize("grid", ["voronoi", "tetra", "sphere1d", "sphere2d", "sphere3d", "cylinder2d", "cylinder3d"])
 def test_bridge_dust_emission_other_grids_on_oracle(tmp_path, grid):
-    """DustEmission on the tetrahedral, spherical and cylindrical grids: secondary launches at random
-    positions in tetrahedra (barycentric fold) and in curvilinear cells."""
-    text = tb.dust_scene(grid, 50000)
+    """DustEmission on the Voronoi, tetrahedral, spherical and cylindrical grids: secondary launches
+    at random positions in Voronoi cells (rejection in the cell box), tetrahedra (barycentric fold)
+    and curvilinear cells."""
+    text = ski.dust_tetra(20000, num_vertices=1000) if grid == "tetra" else tb.dust_scene(grid, 50000)
     log, g, c = both(tmp_path, text, "dust")
     assert "secondary histories on the B200" in log
     z, _ = tb.sed_z(g, c, "dust", "sed")
@@ -100,7 +101,7 @@ def test_bridge_dust_emission_other_grids_on_oracle(tmp_path, grid):
 def test_bridge_grids_on_oracle(tmp_path, grid):
     """The disk scene on the adaptive-mesh, Voronoi, tetrahedral, spherical and cylindrical grids:
     the bridge's flattening of each grid through the oracle against the reference program."""
-    text, files = tb.GRID_SCENES[grid](50000)
+    text, files = tb.GRID_SCENES[grid](20000 if grid == "tetra" else 50000)
     log, g, c = both(tmp_path, text, "disk", files)
     tb.check_disk(g, c, "disk")
 

@@ -97,6 +97,10 @@ def secondary_on_grid(golden, grid_fixture):
         v, t = sc.grid["vertices"], sc.grid["tetra"]
         a, b, c, d = (v[t[:, q]] for q in range(4))
         vol = np.abs(np.einsum("ij,ij->i", b - a, np.cross(c - a, d - a))) / 6.0
+    elif sc.grid["kind"] == abi.GRID_VORONOI:
+        # the domain as every cell's enclosing box: valid for the rejection draw (longer, same result)
+        sc.grid = dict(sc.grid, boxes=np.tile(np.asarray(sc.grid["extent"], dtype=np.float64), (n, 1)))
+        vol = np.full(n, 1e48)
     elif sc.grid["kind"] == abi.GRID_SPHERE1D:
         r = np.asarray(sc.grid["rv"])
         vol = 4.0 / 3.0 * np.pi * (r[1:] ** 3 - r[:-1] ** 3)
@@ -113,7 +117,7 @@ def secondary_on_grid(golden, grid_fixture):
     return sc, rf
 
 
-OTHER_GRIDS = ["paths_tetra.npz", "paths_sphere1d.npz", "paths_cylinder2d.npz", "paths_sphere2d.npz",
+OTHER_GRIDS = ["paths_voronoi.npz", "paths_tetra.npz", "paths_sphere1d.npz", "paths_cylinder2d.npz", "paths_sphere2d.npz",
                "paths_sphere3d.npz", "paths_cylinder3d.npz"]
 
 

@@ -180,12 +180,14 @@ def dust_scene(grid, n):
         return ski.dust_tetra(n)
     if grid == "sphere1d":
         return ski.dust_sphere1d(n)
+    if grid == "voronoi":
+        return ski.dust_shell(n, grid=ski.voronoi_grid(1, "pc", 2000))
     return ski.dust_curvilinear(n, grid)
 
 
-@pytest.mark.parametrize("grid", ["tetra", "sphere1d", "sphere2d", "sphere3d", "cylinder2d", "cylinder3d"])
+@pytest.mark.parametrize("grid", ["voronoi", "tetra", "sphere1d", "sphere2d", "sphere3d", "cylinder2d", "cylinder3d"])
 def test_bridge_dust_emission_other_grids(tmp_path, grid):
-    """DustEmission on the tetrahedral, spherical and cylindrical grids through skirt_gpu -g."""
+    """DustEmission on the Voronoi, tetrahedral, spherical and cylindrical grids through skirt_gpu -g."""
     text = dust_scene(grid, 200000)
     log, g, c = both(tmp_path, text, "dust")
     assert "secondary histories on the B200" in log

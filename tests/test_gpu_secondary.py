@@ -108,10 +108,11 @@ def test_gpu_primary_then_secondary_on_device(golden, gpu_backend):
     check_vs_reference(sc.fetch(gpu_backend, rf=False), z, sc, npp, chi2_max=1.6, zmax=6.5, tot_rel=0.03)
 
 
-@pytest.mark.parametrize("fixture", ["paths_tetra.npz", "paths_sphere1d.npz", "paths_cylinder2d.npz",
+@pytest.mark.parametrize("fixture", ["paths_voronoi.npz", "paths_tetra.npz", "paths_sphere1d.npz", "paths_cylinder2d.npz",
                                      "paths_sphere2d.npz", "paths_sphere3d.npz", "paths_cylinder3d.npz"])
 def test_gpu_secondary_other_grids_equal_oracle(golden, gpu_backend, oracle_backend, fixture):
-    """Secondary launches in tetrahedra (TetraMeshSpatialGrid::Tetra::generatePosition) and in the
+    """Secondary launches in Voronoi cells (rejection in the cell box, VoronoiMeshSnapshot::generatePosition),
+    in tetrahedra (TetraMeshSpatialGrid::Tetra::generatePosition) and in the
     cells of the spherical and cylindrical grids (their randomPositionInCell): the FP64 secondary life
     cycle equals the oracle's history by history (radii and angles through CUDA's cbrt, sqrt, acos,
     cos and sin, to the last bit or so)."""
