@@ -321,7 +321,9 @@ typedef struct skgpu_secondary_options {
  * normalised emission spectrum (emissivity, NR::cdf<NR::interpolateLogLog>); on the host, the launch
  * weights and history ranges per cell (DustSecondarySource::prepareLuminosities / preparePacketMap,
  * SecondarySourceSystem::prepareForLaunch). *luminosity receives the total dust luminosity; when it
- * is 0 there is nothing to launch and skgpu_run_secondary refuses to run. Grids: Cartesian, octree. */
+ * is 0 there is nothing to launch and skgpu_run_secondary refuses to run. The uploaded field is
+ * consumed: the radiation-field tally is empty afterwards. Grids: all kinds (a Voronoi grid with its
+ * cell boxes, skgpu_upload_voronoi_cell_boxes). */
 int skgpu_prepare_secondary(skgpu_ctx* ctx, const skgpu_secondary_options* options, uint64_t total_packets,
                             double* luminosity);
 /* Results of the last preparation: per cell the dust luminosity and temperature; *num_points the
@@ -331,8 +333,11 @@ int skgpu_fetch_dust_emission(skgpu_ctx* ctx, double* luminosity, double* temper
                               double* lambda, double* pdf, double* cdf);
 /* Runs the life cycle of histories [first, first+count) of the prepared secondary segment
  * (MonteCarloSimulation::performLifeCycle with primary = false: the dust source's launch, emission
- * peel-off, forced or free propagation, scattering peel-off and scattering; no radiation-field
- * storage), adding into the instrument tallies. */
+ * peel-off, forced or free propagation, scattering peel-off and scattering), adding into the
+ * instrument tallies. With the options' store_radiation_field the segment also tallies its own
+ * radiation field (SecondaryEmissionOptions::storeEmissionRadiationField, the secondary emission
+ * iterations: MediumSystem::storeRadiationField(false, ...), MonteCarloSimulation.cpp:391-450), and
+ * with peel_off 0 it records no detections (the iterations' performLifeCycle(.., false, false, true)). */
 int skgpu_run_secondary(skgpu_ctx* ctx, uint64_t first, uint64_t count);
 
 /* Same life cycle as skgpu_run_primary for callers that must not allocate device memory while it

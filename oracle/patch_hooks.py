@@ -3,8 +3,9 @@ reference source files that host the life-cycle hooks into oracle/_ref/patched/ 
 there (the reference tree itself is never modified):
 
 - SKIRT/core/MonteCarloSimulation.cpp: runPrimaryEmission and runSecondaryEmission hand their
-  segment to SkgpuLifeCycle::runPrimary / runSecondary and keep the Parallel::call over
-  performLifeCycle as the path taken when the bridge declines;
+  segment to SkgpuLifeCycle::runPrimary / runSecondary, and each segment of
+  runSecondaryEmissionIterations to SkgpuLifeCycle::runSecondaryIteration, keeping the
+  Parallel::call over performLifeCycle as the path taken when the bridge declines;
 - SKIRT/main/SkirtCommandLineHandler.cpp: the -g option switches the bridge on (in place of the
   reference's runtime-loaded GPU layer) and the log reports the bridge's status.
 
@@ -42,6 +43,10 @@ def main():
                 r'storeRF\); \}\);)',
                 r'\n        if (!SkgpuLifeCycle::runSecondary(this, Npp))\n        {\1\n        }',
                 "secondary segment")
+    src = patch(src,
+                r'(\n[ \t]*parallel->call\(Npp, \[this\]\(size_t i, size_t n\) \{ performLifeCycle\(i, n, false, false, true\); \}\);)',
+                r'\n            if (!SkgpuLifeCycle::runSecondaryIteration(this, Npp))\n            {\1\n            }',
+                "secondary iteration segment")
     with open(os.path.join(out, "MonteCarloSimulation.cpp"), "w") as f:
         f.write(src)
 

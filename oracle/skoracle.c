@@ -2392,7 +2392,7 @@ static void life_cycle(or_ctx* c, uint64_t hist, Path* path, Packet* pk)
         {
             path_build(c, pk, path);
             /* storeRadiationField */
-            if (c->opt.store_radiation_field && !c->secRun && pk->ellRF >= 0)
+            if (c->opt.store_radiation_field && pk->ellRF >= 0)
             {
                 double lnExtBeg = 0., extBeg = 1.;
                 for (int q = 0; q < path->n; ++q)
@@ -2763,6 +2763,8 @@ int or_prepare_secondary(or_ctx* c, const skgpu_secondary_options* opt, uint64_t
     c->secLogMin = opt->wavelength_bias > 0. ? log(c->secBmin) : 0.;
     c->secLogWidth = opt->wavelength_bias > 0. ? log(c->secBmax) - log(c->secBmin) : 0.;
     c->secPackets = N;
+    /* the uploaded radiation field is consumed: the tally starts empty for a segment storing its own */
+    if (c->rf) memset(c->rf, 0, c->rfLen * sizeof(double));
     return SKGPU_OK;
 }
 
@@ -2976,7 +2978,7 @@ static void launch_secondary(or_ctx* c, Rng* r, uint64_t hist, Packet* pk)
     pk->sext = c->mixExt[pk->ellMix];
     pk->ssca = c->mixSca[pk->ellMix];
     pk->g = c->mixG[pk->ellMix];
-    pk->ellRF = -1;
+    pk->ellRF = c->opt.store_radiation_field ? wlg_bin(c->rfB, c->rfNb, c->rfEll, lambda) : -1;
 }
 
 int or_run_secondary(or_ctx* c, uint64_t first, uint64_t count)
@@ -2985,6 +2987,16 @@ int or_run_secondary(or_ctx* c, uint64_t first, uint64_t count)
         return fail(c, SKGPU_ERR_STATE, "secondary: no prepared segment (or_prepare_secondary)");
     if (!c->nmix) return fail(c, SKGPU_ERR_STATE, "secondary: no dust mix uploaded");
     if (first + count > c->secPackets) return fail(c, SKGPU_ERR_ARG, "secondary: history range outside the segment");
+    if (c->opt.store_radiation_field && c->nrf)
+    {
+        size_t len = (size_t)c->numCells * c->nrf;
+        if (c->rfLen != len)
+        {
+            free(c->rf);
+            c->rf = (double*)calloc(len, sizeof(double));
+            c->rfLen = len;
+        }
+    }
     memset(&c->cnt, 0, sizeof c->cnt);
     c->errFlag = 0;
     c->secRun = 1;

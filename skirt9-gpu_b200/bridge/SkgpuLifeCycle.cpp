@@ -164,7 +164,7 @@ namespace
         {
             // grids whose randomPositionInCell the library reproduces for the secondary launch
             if (!config->hasDustEmission() || config->hasGasEmission() || config->hasStochasticDustEmission()
-                || config->storeEmissionRadiationField() || !config->hasPanRadiationField())
+                || !config->hasPanRadiationField())
                 return (why = "secondary emission other than equilibrium dust emission"), false;
             if (config->cellLibrary()->type() != "AllCellsLibrary") return (why = "cell library"), false;
             if (config->dustEmissionWavelengthBias() > 0
@@ -503,7 +503,10 @@ namespace
               "sources");
     }
 
-    void setOptions(MonteCarloSimulation* sim, bool storeRF)
+    // secondary segments run so far in this simulation: each draws from streams of its own
+    uint64_t g_secondarySegments = 0;
+
+    void setOptions(MonteCarloSimulation* sim, bool storeRF, bool peel = true, uint64_t stream = 0)
     {
         auto config = sim->config();
         skgpu_options o{};
@@ -512,12 +515,12 @@ namespace
         o.min_weight_reduction = config->minWeightReduction();
         o.path_length_bias = config->pathLengthBias();
         o.store_radiation_field = storeRF ? 1 : 0;
-        o.peel_off = 1;
+        o.peel_off = peel ? 1 : 0;
         const char* p = std::getenv("SKGPU_PRECISION");
         o.precision = p && std::string(p) == "fp64" ? SKGPU_PREC_FP64_EXACT : SKGPU_PREC_FP32;
         o.explicit_absorption = config->explicitAbsorption() ? 1 : 0;
         o.seed = static_cast<uint64_t>(sim->random()->seed()) * 0x9E3779B97F4A7C15ULL
-                 + static_cast<uint64_t>(ProcessManager::rank());
+                 + static_cast<uint64_t>(ProcessManager::rank()) + stream * 0xD1B54A32D192ED03ULL;
         check(skgpu_set_options(g_ctx, &o), "options");
     }
 
@@ -549,6 +552,7 @@ namespace
         uploadInstruments(sim);
         g_scene = sim;
         g_dustTables = false;
+        g_secondarySegments = 0;
     }
 
     // adds the device tallies of the last segment into the FluxRecorder arrays, then the caller
@@ -675,65 +679,89 @@ bool SkgpuLifeCycle::runPrimary(MonteCarloSimulation* sim, size_t Npp)
     return true;
 }
 
+namespace
+{
+    // a secondary-emission segment: with peel the detections go to the instruments (runSecondaryEmission),
+    // with storeRF the segment's radiation field goes to MediumSystem::_rf2c (storeEmissionRadiationField,
+    // and every secondary iteration); the dust emission follows MediumSystem::radiationField, the
+    // primary field plus the secondary field of the previous segment (_rf1 + _rf2)
+    bool runSecondarySegment(MonteCarloSimulation* sim, size_t Npp, bool peel, bool storeRF, const char* what)
+    {
+        if (!SkgpuLifeCycle::isProcessEnabled()) return false;
+        string why;
+        if (!supported(sim, true, why))
+        {
+            sim->log()->warning(string("B200 life cycle not used for the ") + what + ": " + why);
+            return false;
+        }
+        ensureScene(sim);
+        auto config = sim->config();
+        auto ms = sim->mediumSystem();
+        if (!g_dustTables)
+        {
+            const EquilibriumDustEmissionCalculator& c = dustMix(sim)->_calc;
+            auto rfw = config->radiationFieldWLG();
+            std::vector<double> sal(rfw->numBins());
+            for (int ell = 0; ell != rfw->numBins(); ++ell) sal[ell] = dustMix(sim)->sectionAbs(rfw->wavelength(ell));
+            int numCells = ms->_state._numCells;
+            std::vector<double> vol(numCells);
+            for (int m = 0; m != numCells; ++m) vol[m] = ms->_state.volume(m);
+            Range er = config->dustEmissionWLG()->wavelengthRange();
+            double range[2] = {er.min(), er.max()};
+            check(skgpu_upload_dust_emission(g_ctx, c._rflambdav.size(), &c._rfsigmaabsvv[0][0], &c._rfdlambdav[0],
+                                             &c._Bcmbv[0], sal.data(), c._Tv.size(), &c._Tv[0], &c._planckabsvv[0][0],
+                                             c._emlambdav.size(), &c._emlambdav[0], &c._emsigmaabsvv[0][0], range,
+                                             numCells, vol.data()),
+                  "dust emission tables");
+            g_dustTables = true;
+        }
+        setOptions(sim, storeRF, peel, ++g_secondarySegments);
+        // the radiation field as MediumSystem::radiationField sums it (after the communication
+        // between processes)
+        Table<2>& rf1 = ms->_rf1;
+        std::vector<double> rf(rf1.data().size());
+        for (size_t q = 0; q != rf.size(); ++q) rf[q] = rf1.data()[q];
+        if (ms->_rf2.size())
+            for (size_t q = 0; q != rf.size(); ++q) rf[q] += ms->_rf2.data()[q];
+        check(skgpu_upload_radiation_field(g_ctx, rf.data()), "radiation field upload");
+        skgpu_secondary_options so{};
+        so.spatial_bias = config->secondarySpatialBias();
+        so.source_bias = config->secondarySourceBias();
+        so.wavelength_bias = config->dustEmissionWavelengthBias();
+        if (so.wavelength_bias > 0)
+        {
+            Range r = static_cast<LogWavelengthDistribution*>(config->dustEmissionWavelengthBiasDistribution())->range();
+            so.bias_lambda_min = r.min();
+            so.bias_lambda_max = r.max();
+        }
+        double L = 0.;
+        check(skgpu_prepare_secondary(g_ctx, &so, Npp, &L), "secondary preparation");
+        if (!(L > 0)) return true;  // nothing to launch (SKIRT has already reported zero dust luminosity)
+        check(skgpu_clear_tallies(g_ctx), "clear");
+        size_t first = 0, count = Npp;
+        if (ProcessManager::isMultiProc())
+        {
+            size_t n = ProcessManager::size(), r = ProcessManager::rank();
+            first = Npp * r / n;
+            count = Npp * (r + 1) / n - first;
+        }
+        sim->log()->info("Running " + std::to_string(count) + " secondary histories on the B200");
+        check(skgpu_run_secondary(g_ctx, first, count), "secondary segment");
+        if (peel) fetchInstruments(sim, false);
+        if (storeRF) check(skgpu_fetch_radiation_field(g_ctx, &ms->_rf2c.data()[0]), "secondary radiation field");
+        check(skgpu_clear_tallies(g_ctx), "clear");
+        return true;
+    }
+}
+
 bool SkgpuLifeCycle::runSecondary(MonteCarloSimulation* sim, size_t Npp)
 {
-    if (!isProcessEnabled()) return false;
-    string why;
-    if (!supported(sim, true, why))
-    {
-        sim->log()->warning("B200 life cycle not used for the secondary emission: " + why);
-        return false;
-    }
-    ensureScene(sim);
-    auto config = sim->config();
-    auto ms = sim->mediumSystem();
-    if (!g_dustTables)
-    {
-        const EquilibriumDustEmissionCalculator& c = dustMix(sim)->_calc;
-        auto rfw = config->radiationFieldWLG();
-        std::vector<double> sal(rfw->numBins());
-        for (int ell = 0; ell != rfw->numBins(); ++ell) sal[ell] = dustMix(sim)->sectionAbs(rfw->wavelength(ell));
-        int numCells = ms->_state._numCells;
-        std::vector<double> vol(numCells);
-        for (int m = 0; m != numCells; ++m) vol[m] = ms->_state.volume(m);
-        Range er = config->dustEmissionWLG()->wavelengthRange();
-        double range[2] = {er.min(), er.max()};
-        check(skgpu_upload_dust_emission(g_ctx, c._rflambdav.size(), &c._rfsigmaabsvv[0][0], &c._rfdlambdav[0],
-                                         &c._Bcmbv[0], sal.data(), c._Tv.size(), &c._Tv[0], &c._planckabsvv[0][0],
-                                         c._emlambdav.size(), &c._emlambdav[0], &c._emsigmaabsvv[0][0], range, numCells,
-                                         vol.data()),
-              "dust emission tables");
-        g_dustTables = true;
-    }
-    setOptions(sim, false);
-    // the primary radiation field as MediumSystem holds it (summed over the processes)
-    check(skgpu_upload_radiation_field(g_ctx, &ms->_rf1.data()[0]), "radiation field upload");
-    skgpu_secondary_options so{};
-    so.spatial_bias = config->secondarySpatialBias();
-    so.source_bias = config->secondarySourceBias();
-    so.wavelength_bias = config->dustEmissionWavelengthBias();
-    if (so.wavelength_bias > 0)
-    {
-        Range r = static_cast<LogWavelengthDistribution*>(config->dustEmissionWavelengthBiasDistribution())->range();
-        so.bias_lambda_min = r.min();
-        so.bias_lambda_max = r.max();
-    }
-    double L = 0.;
-    check(skgpu_prepare_secondary(g_ctx, &so, Npp, &L), "secondary preparation");
-    if (!(L > 0)) return true;  // nothing to launch (SKIRT has already reported zero dust luminosity)
-    check(skgpu_clear_tallies(g_ctx), "clear");
-    size_t first = 0, count = Npp;
-    if (ProcessManager::isMultiProc())
-    {
-        size_t n = ProcessManager::size(), r = ProcessManager::rank();
-        first = Npp * r / n;
-        count = Npp * (r + 1) / n - first;
-    }
-    sim->log()->info("Running " + std::to_string(count) + " secondary histories on the B200");
-    check(skgpu_run_secondary(g_ctx, first, count), "secondary segment");
-    fetchInstruments(sim, false);
-    check(skgpu_clear_tallies(g_ctx), "clear");
-    return true;
+    return runSecondarySegment(sim, Npp, true, sim->config()->storeEmissionRadiationField(), "secondary emission");
+}
+
+bool SkgpuLifeCycle::runSecondaryIteration(MonteCarloSimulation* sim, size_t Npp)
+{
+    return runSecondarySegment(sim, Npp, false, true, "secondary emission iteration");
 }
 
 void SkgpuLifeCycle::release()

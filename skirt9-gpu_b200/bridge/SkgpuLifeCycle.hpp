@@ -1,8 +1,9 @@
 /* SkgpuLifeCycle: the SKIRT-side bridge of the B200 photon-packet life cycle (include/skgpu.h).
  *
  * One class added to SKIRT/core. MonteCarloSimulation::runPrimaryEmission and
- * runSecondaryEmission (SKIRT/core/MonteCarloSimulation.cpp:172-245) call runPrimary / runSecondary
- * in place of their Parallel::call over performLifeCycle; when these return false (the bridge is
+ * runSecondaryEmission (SKIRT/core/MonteCarloSimulation.cpp:172-245) call runPrimary / runSecondary,
+ * and runSecondaryEmissionIterations (:391-450) calls runSecondaryIteration, in place of their
+ * Parallel::call over performLifeCycle; when these return false (the bridge is
  * off, or the simulation uses something the library does not implement) SKIRT runs its own CPU
  * life cycle unchanged. Everything around the segment stays SKIRT's: ski parsing, setup, grid and
  * mesh construction, source normalisation and SourceSystem::prepareForLaunch, the instrument
@@ -45,6 +46,10 @@ public:
         in MediumSystem (after its communication between processes), adding the instrument tallies
         into the FluxRecorder arrays, secondary components included. Same return convention. */
     static bool runSecondary(MonteCarloSimulation* sim, size_t Npp);
+    /** Runs one segment of Npp packets of the secondary emission iterations
+        (MonteCarloSimulation::runSecondaryEmissionIterations): no detections, the segment's radiation
+        field into MediumSystem's secondary field. Same return convention. */
+    static bool runSecondaryIteration(MonteCarloSimulation* sim, size_t Npp);
 
     /** Releases the device context (end of the process). */
     static void release();

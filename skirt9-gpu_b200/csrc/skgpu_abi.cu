@@ -1833,6 +1833,9 @@ int skgpu_prepare_secondary(skgpu_ctx* ctx, const skgpu_secondary_options* opt, 
     sd.logWidth = opt->wavelength_bias > 0. ? std::log(sd.bmax) - std::log(sd.bmin) : 0.;
     CK(cudaMemcpy(ctx->secDev, &sd, sizeof sd, cudaMemcpyHostToDevice));
     ctx->secPackets = N;
+    // the uploaded radiation field has served the cells' emission: the tally starts empty for a
+    // segment that stores its own (MediumSystem::clearRadiationField(false) before it)
+    if (ctx->rf) CK(cudaMemset(ctx->rf, 0, ctx->rfLen * sizeof(double)));
     return SKGPU_OK;
 }
 
@@ -1869,11 +1872,12 @@ int skgpu_run_secondary(skgpu_ctx* ctx, uint64_t first, uint64_t count)
     if ((rc = ensureWaveBuffers(ctx, P, groups, anyStats))) return rc;
     Wave w = ctx->wave;
     w.sc = sceneOf(ctx);
-    // the secondary source replaces the primary ones; the radiation field is not stored
-    // (SecondaryEmissionOptions::storeEmissionRadiationField off); the histories draw from streams
-    // of their own (a Philox key distinct from the primary segment's)
+    // the secondary source replaces the primary ones; with store_radiation_field the segment tallies
+    // its own radiation field (SecondaryEmissionOptions::storeEmissionRadiationField, the secondary
+    // iterations: MediumSystem::storeRadiationField(false, ...) into _rf2c); the histories draw from
+    // streams of their own (a Philox key distinct from the primary segment's)
+    if ((rc = ensureRadiationField(ctx))) return rc;
     w.sc.sec = ctx->secDev;
-    w.sc.rfOn = 0;
     w.sc.seed = ctx->opt.seed ^ SKGPU_SECONDARY_KEY;
     w.traceBlocksPerSM = ctx->shapeTraceBlocks;
     w.refillMin = ctx->shapeRefill;

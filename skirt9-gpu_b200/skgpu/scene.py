@@ -265,7 +265,8 @@ class Scene:
                       rf=None):
         """One secondary (dust) emission segment of npp packets (histories [first, first+count)) from
         the radiation field on the backend (the last primary segment's, or `rf`, cells x bins);
-        returns the tallies and the total dust luminosity."""
+        returns the tallies (with store_rf the segment's own radiation field, as the secondary
+        emission iterations store it) and the total dust luminosity."""
         if clear:
             be.clear_tallies()
         be.set_options(self.options(seed, precision))
@@ -274,7 +275,7 @@ class Scene:
         s = self.secondary
         L = be.prepare_secondary(npp, s["spatial_bias"], s["source_bias"], s["wavelength_bias"], s["bias_range"])
         be.run_secondary(first, npp if count is None else count)
-        return self.fetch(be, rf=False), L
+        return self.fetch(be, rf=self.store_rf), L
 
     def fetch(self, be, rf=True):
         res = Results()

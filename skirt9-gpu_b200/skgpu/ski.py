@@ -229,13 +229,13 @@ TEST_BANDS = [([0.2, 0.35, 0.5], [0.1, 1.0, 0.1]),
 
 
 def dust_emission_options(em_min_um=1.0, em_max_um=1000.0, num_em=30, spatial_bias=0.5, source_bias=0.5,
-                          wavelength_bias=0.5, packets_multiplier=1.0):
+                          wavelength_bias=0.5, packets_multiplier=1.0, store_rf=False):
     """SecondaryEmissionOptions and DustEmissionOptions of a DustEmission simulation: equilibrium
     emission, no CMB heating, AllCellsLibrary, a logarithmic dust-emission wavelength grid and a
     log-uniform wavelength bias distribution over the same range."""
     rng = f'minWavelength="{em_min_um:g} micron" maxWavelength="{em_max_um:g} micron"'
     return (f'<secondaryEmissionOptions type="SecondaryEmissionOptions"><SecondaryEmissionOptions '
-            f'storeEmissionRadiationField="false" secondaryPacketsMultiplier="{packets_multiplier:g}" '
+            f'storeEmissionRadiationField="{"true" if store_rf else "false"}" secondaryPacketsMultiplier="{packets_multiplier:g}" '
             f'spatialBias="{spatial_bias:g}" sourceBias="{source_bias:g}"/></secondaryEmissionOptions>'
             f'<dustEmissionOptions type="DustEmissionOptions"><DustEmissionOptions dustEmissionType="Equilibrium" '
             f'includeHeatingByCMB="false" maxFractionOfPrimary="0.01" maxFractionOfPrevious="0.03" sourceWeight="1" '
@@ -249,7 +249,8 @@ def dust_emission_options(em_min_um=1.0, em_max_um=1000.0, num_em=30, spatial_bi
 def simulation(mode, num_packets, sources, media, grid, instruments, source_wavelengths="0.55 micron",
                instrument_wlg='<ListWavelengthGrid wavelengths="0.55 micron" relativeHalfWidth="0" log="false"/>',
                force_scattering=True, store_rf=False, rf_wlg="", seed=0, num_density_samples=100,
-               min_weight_reduction=1e4, path_length_bias=0.5, explicit_absorption=False, emission=""):
+               min_weight_reduction=1e4, path_length_bias=0.5, explicit_absorption=False, emission="",
+               secondary_iterations=None):
     """A complete MonteCarloSimulation ski document (`emission`: the secondary and dust emission
     options of a DustEmission simulation, see dust_emission_options)."""
     src_attr = f' wavelengths="{source_wavelengths}"' if mode.startswith("Oligo") else ' minWavelength="0.1 micron" maxWavelength="10 micron"'
@@ -260,9 +261,17 @@ def simulation(mode, num_packets, sources, media, grid, instruments, source_wave
               + (f'<radiationFieldWLG type="DisjointWavelengthGrid">{rf_wlg}</radiationFieldWLG>' if rf_wlg else "")
               + '</RadiationFieldOptions></radiationFieldOptions>')
     rf += emission
+    iterate = "false"
+    iteration_xml = ""
+    if secondary_iterations:
+        iterate = "true"
+        lo, hi = secondary_iterations
+        iteration_xml = (f'<iterationOptions type="IterationOptions"><IterationOptions minSecondaryIterations="{lo}" '
+                         f'maxSecondaryIterations="{hi}" includePrimaryEmission="false" '
+                         f'secondaryIterationPacketsMultiplier="1"/></iterationOptions>')
     return f'''<?xml version="1.0" encoding="UTF-8"?>
 <skirt-simulation-hierarchy type="MonteCarloSimulation" format="9" producer="skgpu" time="2026-01-01T00:00:00">
-<MonteCarloSimulation userLevel="Expert" simulationMode="{mode}" iteratePrimaryEmission="false" iterateSecondaryEmission="false" numPackets="{num_packets:g}">
+<MonteCarloSimulation userLevel="Expert" simulationMode="{mode}" iteratePrimaryEmission="false" iterateSecondaryEmission="{iterate}" numPackets="{num_packets:g}">
 <random type="Random"><Random seed="{seed}"/></random>
 <units type="Units"><ExtragalacticUnits wavelengthOutputStyle="Wavelength" fluxOutputStyle="Frequency"/></units>
 <cosmology type="Cosmology"><LocalUniverseCosmology/></cosmology>
@@ -270,6 +279,7 @@ def simulation(mode, num_packets, sources, media, grid, instruments, source_wave
 <sources type="Source">{sources}</sources></SourceSystem></sourceSystem>
 <mediumSystem type="MediumSystem"><MediumSystem>
 <photonPacketOptions type="PhotonPacketOptions"><PhotonPacketOptions explicitAbsorption="{"true" if explicit_absorption else "false"}" forceScattering="{"true" if force_scattering else "false"}" minWeightReduction="{min_weight_reduction:g}" minScattEvents="0" pathLengthBias="{path_length_bias:g}"/></photonPacketOptions>
+{iteration_xml}
 {rf}
 <media type="Medium">{media}</media>
 <samplingOptions type="SamplingOptions"><SamplingOptions numDensitySamples="{num_density_samples}" numPropertySamples="1" aggregateVelocity="Average"/></samplingOptions>
@@ -394,13 +404,15 @@ def shell_cartesian(num_packets=1e6, nbins=64, npix=256, stats=True, points=None
                       explicit_absorption=explicit_absorption, force_scattering=force_scattering)
 
 
-def dust_shell(num_packets=1e6, nbins=16, npix=32, stats=True, nlambda=20, num_em=30, grid=None, medium=None):
+def dust_shell(num_packets=1e6, nbins=16, npix=32, stats=True, nlambda=20, num_em=30, grid=None, medium=None,
+               self_absorption=None):
     """The dust shell of shell_cartesian with dust emission (DustEmission mode): a 5800 K black-body
     point source of 1e5 Lsun (0.1-10 micron), power-law MeanListDustMix on 40 log wavelengths 0.1-1000
     micron, radiation field on `nlambda` log bins 0.1-10 micron, equilibrium dust emission on `num_em`
     log bins 1-1000 micron, a 32^2 frame at 30 degrees and an SED instrument at 30 degrees on 30 log
     bins 0.1-1000 micron (statistics on). `grid` replaces the Cartesian grid, `medium` (a function of
-    the mix XML) the shell medium."""
+    the mix XML) the shell medium; self_absorption = (min, max) secondary iterations turns on dust
+    self-absorption (the emission radiation field stored, iterateSecondaryEmission)."""
     lam = [0.1 * (1e4 ** (i / 39)) for i in range(40)]
     kappa = [(l / 0.55) ** -1.0 for l in lam]
     albedo = [min(0.9, max(0.01, 0.5 * (l / 0.55) ** -0.5)) for l in lam]
@@ -412,7 +424,8 @@ def dust_shell(num_packets=1e6, nbins=16, npix=32, stats=True, nlambda=20, num_e
     return simulation("DustEmission", num_packets, point_source(luminosity_lsun=1e5), med,
                       grid or cartesian_grid(1, nbins), frame_instrument("i30", 30, 2, "pc", npix, stats)
                       + sed_instrument("sed", 30, stats, comps=False), instrument_wlg=iwlg, store_rf=True,
-                      rf_wlg=rf_wlg, emission=dust_emission_options(num_em=num_em))
+                      rf_wlg=rf_wlg, emission=dust_emission_options(num_em=num_em, store_rf=bool(self_absorption)),
+                      secondary_iterations=self_absorption)
 
 
 def galaxy_tetra(num_packets, vertex_filename, tau_v=1.0, npix=256, nlambda=32, half_size_kpc=25):

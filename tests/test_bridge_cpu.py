@@ -115,3 +115,17 @@ def test_bridge_off_is_the_reference(tmp_path):
     assert "on the B200" not in la
     sa, sb = (np.loadtxt(os.path.join(tmp_path / d, "s_sed_sed.dat")) for d in ("a", "b"))
     assert np.array_equal(sa, sb)
+
+
+@needs_build
+def test_bridge_dust_self_absorption_on_oracle(tmp_path):
+    """Dust self-absorption: the secondary emission iterations (MonteCarloSimulation::
+    runSecondaryEmissionIterations) and the final secondary segment store the emission radiation
+    field, and each segment's dust emission follows the primary plus the previous secondary field.
+    Every segment runs through the bridge; the SED agrees with the reference program's."""
+    text = ski.dust_shell(50000, self_absorption=(2, 3))
+    log, g, c = both(tmp_path, text, "dust")
+    assert log.count("secondary histories on the B200") >= 3  # two iterations and the final segment
+    z, (a, b) = tb.sed_z(g, c, "dust", "sed")
+    assert len(z) > 25
+    tb.check(z, 2.0, 5.0)

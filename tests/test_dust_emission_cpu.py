@@ -132,3 +132,20 @@ def test_oracle_secondary_launch_in_cells(golden, oracle_backend, fixture):
     res, L = sc.run_secondary(oracle_backend, 4000, seed=3, rf=rf)
     assert L > 0 and res.counters["histories"] == 4000
     assert sum(float(ins["total"].sum()) for ins in res.instruments) > 0
+
+
+def test_oracle_secondary_stores_its_radiation_field(golden, oracle_backend):
+    """With the radiation field stored, a secondary segment tallies its own field (the emission
+    radiation field of dust self-absorption, MediumSystem::storeRadiationField(false, ...)): the
+    uploaded primary field is consumed by the preparation and does not reappear in the tally."""
+    z = golden("dust_shell.npz")
+    sc = Scene.from_export(z)
+    sc.upload(oracle_backend)
+    res, L = sc.run_secondary(oracle_backend, 5000, seed=3, rf=z["rf1"])
+    assert L > 0 and res.rf is not None
+    assert 0 < res.rf.sum() < 0.05 * z["rf1"].sum()
+    sc.store_rf = False
+    res2, _ = sc.run_secondary(oracle_backend, 5000, seed=3, rf=z["rf1"])
+    assert res2.rf is None
+    for a, b in zip(res.instruments, res2.instruments):
+        assert np.array_equal(a["total"], b["total"])

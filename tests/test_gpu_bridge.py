@@ -225,3 +225,17 @@ def test_bridge_dust_emission(tmp_path):
     assert fa[ir].sum() == pytest.approx(fb[ir].sum(), rel=0.03)  # the dust emission itself
     z, _ = frame_z(g, c, "dust", "i30")
     check(z, 1.3, 6.0)
+
+
+@needs_build
+def test_bridge_dust_self_absorption(tmp_path):
+    """Dust self-absorption on the B200: the secondary emission iterations and the final secondary
+    segment store the emission radiation field; SED and frame against the reference program."""
+    text = ski.dust_shell(200000, self_absorption=(2, 3))
+    log, g, c = both(tmp_path, text, "dust")
+    assert log.count("secondary histories on the B200") >= 3
+    z, _ = sed_z(g, c, "dust", "sed")
+    assert len(z) > 25
+    check(z, 2.0, 5.0)
+    z, _ = frame_z(g, c, "dust", "i30")
+    check(z, 1.3, 6.0)

@@ -70,6 +70,10 @@ def test_gpu_secondary_fp64_equals_oracle(golden, gpu_backend, oracle_backend, n
         sa, sb = a["stats"].reshape(5, -1), b["stats"].reshape(5, -1)
         assert np.array_equal(sa[0], sb[0])
         assert np.allclose(sa[2], sb[2], rtol=1e-9, atol=1e-12 * np.abs(sb[2]).max())
+    # the segment's own radiation field (dust self-absorption: storeEmissionRadiationField)
+    assert ro.rf.sum() > 0
+    assert rg.rf.sum() == pytest.approx(ro.rf.sum(), rel=1e-9)
+    assert np.mean(np.isclose(rg.rf, ro.rf, rtol=1e-9, atol=1e-12 * ro.rf.max())) > 0.995
 
 
 def check_vs_reference(res, z, sc, npp, chi2_max=1.3, zmax=5.5, tot_rel=0.02):
