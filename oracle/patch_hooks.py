@@ -3,8 +3,10 @@ reference source files that host the life-cycle hooks into oracle/_ref/patched/ 
 there (the reference tree itself is never modified):
 
 - SKIRT/core/MonteCarloSimulation.cpp: runPrimaryEmission and runSecondaryEmission hand their
-  segment to SkgpuLifeCycle::runPrimary / runSecondary, and each segment of
-  runSecondaryEmissionIterations to SkgpuLifeCycle::runSecondaryIteration, keeping the
+  segment to SkgpuLifeCycle::runPrimary / runSecondary, each segment of
+  runSecondaryEmissionIterations to SkgpuLifeCycle::runSecondaryIteration, and the primary and
+  secondary segments of runMergedEmissionIterations to runPrimaryIteration / runSecondaryIteration,
+  keeping the
   Parallel::call over performLifeCycle as the path taken when the bridge declines;
 - SKIRT/main/SkirtCommandLineHandler.cpp: the -g option switches the bridge on (in place of the
   reference's runtime-loaded GPU layer) and the log reports the bridge's status.
@@ -47,6 +49,14 @@ def main():
                 r'(\n[ \t]*parallel->call\(Npp, \[this\]\(size_t i, size_t n\) \{ performLifeCycle\(i, n, false, false, true\); \}\);)',
                 r'\n            if (!SkgpuLifeCycle::runSecondaryIteration(this, Npp))\n            {\1\n            }',
                 "secondary iteration segment")
+    src = patch(src,
+                r'(\n[ \t]*parallel->call\(Npp1, \[this\]\(size_t i, size_t n\) \{ performLifeCycle\(i, n, true, false, true\); \}\);)',
+                r'\n            if (!SkgpuLifeCycle::runPrimaryIteration(this, Npp1))\n            {\1\n            }',
+                "merged primary iteration segment")
+    src = patch(src,
+                r'(\n[ \t]*parallel->call\(Npp2, \[this\]\(size_t i, size_t n\) \{ performLifeCycle\(i, n, false, false, true\); \}\);)',
+                r'\n            if (!SkgpuLifeCycle::runSecondaryIteration(this, Npp2))\n            {\1\n            }',
+                "merged secondary iteration segment")
     with open(os.path.join(out, "MonteCarloSimulation.cpp"), "w") as f:
         f.write(src)
 

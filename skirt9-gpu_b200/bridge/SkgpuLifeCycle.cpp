@@ -503,8 +503,9 @@ namespace
               "sources");
     }
 
-    // secondary segments run so far in this simulation: each draws from streams of its own
+    // secondary and iteration segments run so far in this simulation: each draws from streams of its own
     uint64_t g_secondarySegments = 0;
+    uint64_t g_iterationSegments = 0;
 
     void setOptions(MonteCarloSimulation* sim, bool storeRF, bool peel = true, uint64_t stream = 0)
     {
@@ -553,6 +554,7 @@ namespace
         g_scene = sim;
         g_dustTables = false;
         g_secondarySegments = 0;
+        g_iterationSegments = 0;
     }
 
     // adds the device tallies of the last segment into the FluxRecorder arrays, then the caller
@@ -645,38 +647,54 @@ std::string SkgpuLifeCycle::status()
            + (g_device >= 0 ? " on device " + std::to_string(g_device) : "");
 }
 
+namespace
+{
+    // a primary-emission segment: with peel the detections go to the instruments, with storeRF the
+    // radiation field to MediumSystem::_rf1; stream 0 for the primary segment, a fresh one for each
+    // segment of the merged iterations
+    bool runPrimarySegment(MonteCarloSimulation* sim, size_t Npp, bool peel, bool storeRF, uint64_t stream,
+                           const char* what)
+    {
+        if (!SkgpuLifeCycle::isProcessEnabled()) return false;
+        string why;
+        if (!supported(sim, false, why))
+        {
+            sim->log()->warning(string("B200 life cycle not used for the ") + what + ": " + why);
+            return false;
+        }
+        ensureScene(sim);
+        setOptions(sim, storeRF, peel, stream);
+        uploadSources(sim);
+        check(skgpu_clear_tallies(g_ctx), "clear");
+        // this process's share of the history indices, as Parallel::call distributes them over processes
+        size_t first = 0, count = Npp;
+        if (ProcessManager::isMultiProc())
+        {
+            size_t n = ProcessManager::size(), r = ProcessManager::rank();
+            first = Npp * r / n;
+            count = Npp * (r + 1) / n - first;
+        }
+        sim->log()->info("Running " + std::to_string(count) + " primary histories on the B200");
+        check(skgpu_run_primary(g_ctx, first, count, Npp), "primary segment");
+        if (peel) fetchInstruments(sim, true);
+        if (storeRF)
+        {
+            Table<2>& rf = sim->mediumSystem()->_rf1;
+            check(skgpu_fetch_radiation_field(g_ctx, &rf.data()[0]), "radiation field");
+        }
+        check(skgpu_clear_tallies(g_ctx), "clear");
+        return true;
+    }
+}
+
 bool SkgpuLifeCycle::runPrimary(MonteCarloSimulation* sim, size_t Npp)
 {
-    if (!isProcessEnabled()) return false;
-    string why;
-    if (!supported(sim, false, why))
-    {
-        sim->log()->warning("B200 life cycle not used for the primary emission: " + why);
-        return false;
-    }
-    ensureScene(sim);
-    bool storeRF = sim->config()->hasRadiationField();
-    setOptions(sim, storeRF);
-    uploadSources(sim);
-    check(skgpu_clear_tallies(g_ctx), "clear");
-    // this process's share of the history indices, as Parallel::call distributes them over processes
-    size_t first = 0, count = Npp;
-    if (ProcessManager::isMultiProc())
-    {
-        size_t n = ProcessManager::size(), r = ProcessManager::rank();
-        first = Npp * r / n;
-        count = Npp * (r + 1) / n - first;
-    }
-    sim->log()->info("Running " + std::to_string(count) + " primary histories on the B200");
-    check(skgpu_run_primary(g_ctx, first, count, Npp), "primary segment");
-    fetchInstruments(sim, true);
-    if (storeRF)
-    {
-        Table<2>& rf = sim->mediumSystem()->_rf1;
-        check(skgpu_fetch_radiation_field(g_ctx, &rf.data()[0]), "radiation field");
-    }
-    check(skgpu_clear_tallies(g_ctx), "clear");
-    return true;
+    return runPrimarySegment(sim, Npp, true, sim->config()->hasRadiationField(), 0, "primary emission");
+}
+
+bool SkgpuLifeCycle::runPrimaryIteration(MonteCarloSimulation* sim, size_t Npp)
+{
+    return runPrimarySegment(sim, Npp, false, true, ++g_iterationSegments, "merged primary emission iteration");
 }
 
 namespace

@@ -2,7 +2,8 @@
  *
  * One class added to SKIRT/core. MonteCarloSimulation::runPrimaryEmission and
  * runSecondaryEmission (SKIRT/core/MonteCarloSimulation.cpp:172-245) call runPrimary / runSecondary,
- * and runSecondaryEmissionIterations (:391-450) calls runSecondaryIteration, in place of their
+ * runSecondaryEmissionIterations (:391-450) calls runSecondaryIteration, and
+ * runMergedEmissionIterations runPrimaryIteration / runSecondaryIteration, in place of their
  * Parallel::call over performLifeCycle; when these return false (the bridge is
  * off, or the simulation uses something the library does not implement) SKIRT runs its own CPU
  * life cycle unchanged. Everything around the segment stays SKIRT's: ski parsing, setup, grid and
@@ -50,6 +51,10 @@ public:
         (MonteCarloSimulation::runSecondaryEmissionIterations): no detections, the segment's radiation
         field into MediumSystem's secondary field. Same return convention. */
     static bool runSecondaryIteration(MonteCarloSimulation* sim, size_t Npp);
+    /** Runs the primary segment of Npp packets of a merged primary-secondary iteration
+        (MonteCarloSimulation::runMergedEmissionIterations): no detections, the radiation field into
+        MediumSystem's primary field. Same return convention. */
+    static bool runPrimaryIteration(MonteCarloSimulation* sim, size_t Npp);
 
     /** Releases the device context (end of the process). */
     static void release();

@@ -265,9 +265,10 @@ def simulation(mode, num_packets, sources, media, grid, instruments, source_wave
     iteration_xml = ""
     if secondary_iterations:
         iterate = "true"
-        lo, hi = secondary_iterations
+        lo, hi = secondary_iterations[:2]
+        merged = "true" if len(secondary_iterations) > 2 and secondary_iterations[2] else "false"
         iteration_xml = (f'<iterationOptions type="IterationOptions"><IterationOptions minSecondaryIterations="{lo}" '
-                         f'maxSecondaryIterations="{hi}" includePrimaryEmission="false" '
+                         f'maxSecondaryIterations="{hi}" includePrimaryEmission="{merged}" '
                          f'secondaryIterationPacketsMultiplier="1"/></iterationOptions>')
     return f'''<?xml version="1.0" encoding="UTF-8"?>
 <skirt-simulation-hierarchy type="MonteCarloSimulation" format="9" producer="skgpu" time="2026-01-01T00:00:00">
@@ -412,7 +413,8 @@ def dust_shell(num_packets=1e6, nbins=16, npix=32, stats=True, nlambda=20, num_e
     log bins 1-1000 micron, a 32^2 frame at 30 degrees and an SED instrument at 30 degrees on 30 log
     bins 0.1-1000 micron (statistics on). `grid` replaces the Cartesian grid, `medium` (a function of
     the mix XML) the shell medium; self_absorption = (min, max) secondary iterations turns on dust
-    self-absorption (the emission radiation field stored, iterateSecondaryEmission)."""
+    self-absorption (the emission radiation field stored, iterateSecondaryEmission), (min, max, True)
+    with the primary emission in the iterations (includePrimaryEmission: merged iterations)."""
     lam = [0.1 * (1e4 ** (i / 39)) for i in range(40)]
     kappa = [(l / 0.55) ** -1.0 for l in lam]
     albedo = [min(0.9, max(0.01, 0.5 * (l / 0.55) ** -0.5)) for l in lam]

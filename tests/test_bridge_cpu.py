@@ -129,3 +129,17 @@ def test_bridge_dust_self_absorption_on_oracle(tmp_path):
     z, (a, b) = tb.sed_z(g, c, "dust", "sed")
     assert len(z) > 25
     tb.check(z, 2.0, 5.0)
+
+
+@needs_build
+def test_bridge_merged_iterations_on_oracle(tmp_path):
+    """Merged primary and secondary iterations (includePrimaryEmission,
+    MonteCarloSimulation::runMergedEmissionIterations): every segment of the iterations and the final
+    segments run through the bridge; the SED agrees with the reference program's."""
+    text = ski.dust_shell(50000, self_absorption=(2, 2, True))
+    log, g, c = both(tmp_path, text, "dust")
+    assert log.count("primary histories on the B200") == 3  # two iterations and the final segment
+    assert log.count("secondary histories on the B200") == 3
+    z, _ = tb.sed_z(g, c, "dust", "sed")
+    assert len(z) > 25
+    tb.check(z, 2.0, 5.0)

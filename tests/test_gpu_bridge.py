@@ -239,3 +239,17 @@ def test_bridge_dust_self_absorption(tmp_path):
     check(z, 2.0, 5.0)
     z, _ = frame_z(g, c, "dust", "i30")
     check(z, 1.3, 6.0)
+
+
+@needs_build
+def test_bridge_merged_iterations(tmp_path):
+    """Merged primary and secondary iterations on the B200: every segment through the bridge; SED
+    and frame against the reference program."""
+    text = ski.dust_shell(200000, self_absorption=(2, 2, True))
+    log, g, c = both(tmp_path, text, "dust")
+    assert log.count("primary histories on the B200") == 3
+    z, _ = sed_z(g, c, "dust", "sed")
+    assert len(z) > 25
+    check(z, 2.0, 5.0)
+    z, _ = frame_z(g, c, "dust", "i30")
+    check(z, 1.3, 6.0)
