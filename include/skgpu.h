@@ -259,6 +259,14 @@ int skgpu_set_instrument_scattering_levels(skgpu_ctx* ctx, int32_t instrument, i
  * skgpu_upload_instruments. */
 int skgpu_set_instrument_bands(skgpu_ctx* ctx, int32_t instrument, int32_t num_bands, const int32_t* band_sizes,
                                const double* lambda, const double* transmission, const double* width);
+/* Observer of a distant instrument beyond the defaults (0, 0): the observer-frame redshift z, with
+ * which FluxRecorder::detect looks the wavelength bin up at lambda * (1 + z) (FluxRecorder.cpp:377-384;
+ * DistantInstrument::setupSelfBefore passes Configuration::redshift when the distance is zero), and
+ * for an SED instrument the aperture radius R of ApertureInstrument::isInsideAperture
+ * (ApertureInstrument.cpp:25-44): a packet is recorded only when its position, projected with the
+ * instrument's inclination and azimuth (the skgpu_instrument cos/sin fields, which the caller fills
+ * for such an SED instrument too), lies within R of the centre. Call after skgpu_upload_instruments. */
+int skgpu_set_instrument_observer(skgpu_ctx* ctx, int32_t instrument, double redshift, double aperture_radius);
 
 /* ---- run ---- */
 int skgpu_set_options(skgpu_ctx* ctx, const skgpu_options* options);

@@ -207,7 +207,8 @@ BRIDGE_FNS := create destroy last_error abi_version device_count upload_grid_car
     upload_dust_emission upload_radiation_field prepare_secondary run_secondary \
     set_instrument_scattering_levels set_instrument_bands fetch_instrument_levels \
     upload_grid_sphere2d upload_grid_sphere3d upload_grid_cylinder2d upload_grid_cylinder3d \
-    upload_grid_adaptive_mesh upload_grid_voronoi upload_grid_tetra upload_voronoi_cell_boxes
+    upload_grid_adaptive_mesh upload_grid_voronoi upload_grid_tetra upload_voronoi_cell_boxes \
+    set_instrument_observer
 BRIDGE_ORACLE_DEFS := $(foreach f,$(BRIDGE_FNS),-Dskgpu_$(f)=or_$(f)) -Dskgpu_ctx=or_ctx -include $(HERE)/skoracle.h
 
 $(OBJ)/bridge/SkgpuLifeCycle_oracle.o: $(BRIDGE)/SkgpuLifeCycle.cpp $(BRIDGE)/SkgpuLifeCycle.hpp $(HERE)/skoracle.h

@@ -144,6 +144,8 @@ typedef struct
     int nband;                      /* > 0: band wavelength grid */
     int* bandBeg;                   /* nband + 1 table offsets */
     double *bandLam, *bandTr, *bandW;
+    double zfac; /* 1 + observer-frame redshift */
+    double apR2; /* SED aperture radius squared (0: none) */
 } Instr;
 
 struct or_ctx
@@ -1806,6 +1808,8 @@ int or_upload_instruments(or_ctx* c, int32_t num_instruments, const skgpu_instru
     {
         Instr* in = &c->instr[i];
         in->d = instruments[i];
+        in->zfac = 1.;
+        in->apR2 = 0.;
         size_t npix = in->d.kind == SKGPU_INSTR_FRAME ? (size_t)in->d.num_pixels_x * in->d.num_pixels_y : 1;
         in->n = npix * in->d.num_wavelength_bins;
         if (in->d.kind == SKGPU_INSTR_FRAME)
@@ -1857,6 +1861,19 @@ int or_set_instrument_bands(or_ctx* c, int32_t i, int32_t num_bands, const int32
     in->bandTr = (double*)dup(transmission, (size_t)beg[num_bands] * sizeof(double));
     in->bandW = (double*)dup(width, (size_t)num_bands * sizeof(double));
     in->nband = num_bands;
+    return SKGPU_OK;
+}
+
+/* the observer-frame redshift (FluxRecorder.cpp:377-378) and the SED aperture
+   (ApertureInstrument.cpp:25-44) */
+int or_set_instrument_observer(or_ctx* c, int32_t i, double redshift, double aperture_radius)
+{
+    if (i < 0 || i >= c->ninstr) return fail(c, SKGPU_ERR_ARG, "observer: bad instrument index");
+    if (!(redshift >= 0.) || !(aperture_radius >= 0.)) return fail(c, SKGPU_ERR_ARG, "observer: bad redshift or radius");
+    if (aperture_radius > 0. && c->instr[i].d.kind != SKGPU_INSTR_SED)
+        return fail(c, SKGPU_ERR_ARG, "observer: apertures belong to SED instruments");
+    c->instr[i].zfac = 1. + redshift;
+    c->instr[i].apR2 = aperture_radius * aperture_radius;
     return SKGPU_OK;
 }
 
@@ -2127,6 +2144,14 @@ static void peel_off(or_ctx* c, Packet* pk, int scattering)
         }
         int l = in->d.kind == SKGPU_INSTR_FRAME ? frame_pixel(&in->d, pk) : -1;
         if (in->d.kind == SKGPU_INSTR_FRAME && l < 0) continue;
+        if (in->d.kind == SKGPU_INSTR_SED && in->apR2 > 0.)
+        {
+            const skgpu_instrument* d = &in->d;
+            double xpp = -d->sin_phi * pk->rx + d->cos_phi * pk->ry;
+            double ypp = -d->cos_phi * d->cos_theta * pk->rx - d->sin_phi * d->cos_theta * pk->ry + d->sin_theta * pk->rz;
+            if (xpp * xpp + ypp * ypp > in->apR2) continue;
+        }
+        const double lambda = pk->lambda * in->zfac;
         /* WavelengthGrid::bins and ::transmission: one disjoint bin with transmission 1, or every band
            whose table range holds the wavelength (FluxRecorder.cpp:380-384) */
         int nb = in->nband ? in->nband : 1;
@@ -2136,7 +2161,7 @@ static void peel_off(or_ctx* c, Packet* pk, int scattering)
             double L = Lp;
             if (!in->nband)
             {
-                ell = wlg_bin(c->wlgB + in->d.wlg_offset, in->d.wlg_num_borders, c->wlgEll + in->d.wlg_offset, pk->lambda);
+                ell = wlg_bin(c->wlgB + in->d.wlg_offset, in->d.wlg_num_borders, c->wlgEll + in->d.wlg_offset, lambda);
                 if (ell < 0) continue;
             }
             else
@@ -2144,8 +2169,8 @@ static void peel_off(or_ctx* c, Packet* pk, int scattering)
                 ell = b;
                 const double* lv = in->bandLam + in->bandBeg[b];
                 int size = in->bandBeg[b + 1] - in->bandBeg[b];
-                if (!(pk->lambda >= lv[0] && pk->lambda <= lv[size - 1])) continue;
-                L = Lp * band_transmission(lv, in->bandTr + in->bandBeg[b], size, in->bandW[b], pk->lambda);
+                if (!(lambda >= lv[0] && lambda <= lv[size - 1])) continue;
+                L = Lp * band_transmission(lv, in->bandTr + in->bandBeg[b], size, in->bandW[b], lambda);
             }
             if (!tauKnown)
             {

@@ -68,6 +68,7 @@ int or_upload_instruments(or_ctx* ctx, int32_t num_instruments, const skgpu_inst
 int or_set_instrument_scattering_levels(or_ctx* ctx, int32_t instrument, int32_t levels);
 int or_set_instrument_bands(or_ctx* ctx, int32_t instrument, int32_t num_bands, const int32_t* band_sizes,
                             const double* lambda, const double* transmission, const double* width);
+int or_set_instrument_observer(or_ctx* ctx, int32_t instrument, double redshift, double aperture_radius);
 int or_set_options(or_ctx* ctx, const skgpu_options* options);
 int or_run_primary(or_ctx* ctx, uint64_t first, uint64_t count, uint64_t total_packets);
 int or_probe_launch(or_ctx* ctx, uint64_t first, uint64_t count, uint64_t total_packets, double* out);

@@ -135,10 +135,9 @@ namespace
         for (Instrument* instr : sim->instrumentSystem()->instruments())
         {
             auto rec = instr->instrumentFluxRecorder();
-            if (rec->_recordPolarization || rec->_redshift != 0. || rec->_local) return (why = "instrument options"), false;
+            if (rec->_recordPolarization || rec->_local) return (why = "instrument options"), false;
             auto sed = dynamic_cast<SEDInstrument*>(instr);
             if (!dynamic_cast<FrameInstrument*>(instr) && !sed) return (why = "instrument type"), false;
-            if (sed && sed->radius() > 0) return (why = "SED aperture"), false;
             if (!dynamic_cast<const DisjointWavelengthGrid*>(rec->_lambdagrid)
                 && !dynamic_cast<const BandWavelengthGrid*>(rec->_lambdagrid))
                 return (why = "instrument grid"), false;
@@ -379,6 +378,12 @@ namespace
             d.kobs[0] = k.x();
             d.kobs[1] = k.y();
             d.kobs[2] = k.z();
+            if (auto sed = dynamic_cast<SEDInstrument*>(instr))
+            {
+                // the projection of ApertureInstrument::isInsideAperture
+                d.cos_theta = sed->_costheta; d.sin_theta = sed->_sintheta;
+                d.cos_phi = sed->_cosphi; d.sin_phi = sed->_sinphi;
+            }
             if (f)
             {
                 d.num_pixels_x = f->_Nxp;
@@ -399,6 +404,11 @@ namespace
             auto rec = instr->instrumentFluxRecorder();
             if (!rec->_recordTotalOnly && rec->_numScatteringLevels > 0)
                 check(skgpu_set_instrument_scattering_levels(g_ctx, i, rec->_numScatteringLevels), "scattering levels");
+            // observer-frame redshift and SED aperture (FluxRecorder::detect, ApertureInstrument)
+            double radius = 0.;
+            if (auto sed = dynamic_cast<SEDInstrument*>(instr)) radius = sed->radius();
+            if (rec->_redshift != 0. || radius > 0.)
+                check(skgpu_set_instrument_observer(g_ctx, i, rec->_redshift, radius), "instrument observer");
             if (auto bg = dynamic_cast<const BandWavelengthGrid*>(rec->_lambdagrid))
             {
                 // the bands in the grid's (pivot wavelength) order with their normalised tables

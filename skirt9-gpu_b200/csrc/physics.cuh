@@ -44,6 +44,8 @@ struct InstrDev
     const double* bandLam;  // band tables: increasing wavelengths
     const double* bandTr;   // normalised transmissions
     const double* bandW;    // nband effective widths
+    double zfac;            // 1 + observer-frame redshift
+    double apR2;            // SED aperture radius squared (0: no aperture)
 };
 
 // The prepared secondary (dust) emission source of a segment (DustSecondarySource with the
@@ -539,14 +541,24 @@ SKG_D int framePixel(const InstrDev& in, double x, double y, double z)
     return i + in.npx * j;
 }
 
+// ApertureInstrument::isInsideAperture (ApertureInstrument.cpp:25-44): the position projected with
+// inclination and azimuth (no roll) within the aperture radius
+SKG_D bool insideAperture(const InstrDev& in, double x, double y, double z)
+{
+    if (!(in.apR2 > 0.)) return true;
+    double xpp = -in.sp * x + in.cp * y;
+    double ypp = -in.cp * in.ct * x - in.sp * in.ct * y + in.st * z;
+    return !(xpp * xpp + ypp * ypp > in.apR2);
+}
+
 // does any instrument of the observer group starting at i0 record a packet at (x,y,z)?
 SKG_D bool groupNeedsTau(const Scene& p, int i0, double x, double y, double z)
 {
     for (int i = i0; i < p.ninstr && (i == i0 || p.instr[i].same); ++i)
     {
         const InstrDev& in = p.instr[i];
-        if (in.kind == 1) return true;
-        if (framePixel(in, x, y, z) >= 0) return true;
+        if (in.kind == 1 && insideAperture(in, x, y, z)) return true;
+        if (in.kind == 0 && framePixel(in, x, y, z) >= 0) return true;
     }
     return false;
 }

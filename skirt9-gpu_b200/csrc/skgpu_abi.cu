@@ -1312,6 +1312,8 @@ int skgpu_upload_instruments(skgpu_ctx* ctx, int32_t num_instruments, const skgp
         d.xpmin = s.xp_min; d.xpsiz = s.xp_size; d.ypmin = s.yp_min; d.ypsiz = s.yp_size;
         d.ifu = d.sed = d.ifuComp = d.sedComp = d.ifuStats = d.sedStats = nullptr;
         d.levels = 0;
+        d.zfac = 1.;
+        d.apR2 = 0.;
         d.nband = 0;
         d.bandBeg = nullptr;
         d.bandLam = d.bandTr = d.bandW = nullptr;
@@ -1361,6 +1363,21 @@ int skgpu_set_instrument_scattering_levels(skgpu_ctx* ctx, int32_t instrument, i
         }
     comp = p;
     d.levels = levels;
+    CK(cudaMemcpy(ctx->instr + instrument, &d, sizeof(InstrDev), cudaMemcpyHostToDevice));
+    return SKGPU_OK;
+}
+
+int skgpu_set_instrument_observer(skgpu_ctx* ctx, int32_t instrument, double redshift, double aperture_radius)
+{
+    if (!ctx) return SKGPU_ERR_ARG;
+    if (instrument < 0 || instrument >= static_cast<int>(ctx->instrHost.size())) return fail(ctx, SKGPU_ERR_ARG, "observer: bad instrument index");
+    if (!(redshift >= 0.) || !std::isfinite(redshift)) return fail(ctx, SKGPU_ERR_ARG, "observer: redshift must be finite and >= 0");
+    if (!(aperture_radius >= 0.) || !std::isfinite(aperture_radius)) return fail(ctx, SKGPU_ERR_ARG, "observer: bad aperture radius");
+    InstrDev& d = ctx->instrHost[instrument];
+    if (aperture_radius > 0. && d.kind != SKGPU_INSTR_SED) return fail(ctx, SKGPU_ERR_ARG, "observer: apertures belong to SED instruments");
+    CK(cudaSetDevice(ctx->device));
+    d.zfac = 1. + redshift;
+    d.apR2 = aperture_radius * aperture_radius;
     CK(cudaMemcpy(ctx->instr + instrument, &d, sizeof(InstrDev), cudaMemcpyHostToDevice));
     return SKGPU_OK;
 }

@@ -572,12 +572,15 @@ static __global__ void __launch_bounds__(256) shadePeelKernel(const __grid_const
         double Lp = b.par[t];
         double ext = exp(-b.tau[t]);
         double x = b.x[t], y = b.y[t], z = b.z[t];
-        double lambda = w.pk.rec[slot].lam;
+        double lambda0 = w.pk.rec[slot].lam;
         for (int i = group; i < sc.ninstr && (i == group || sc.instr[i].same); ++i)
         {
             const InstrDev& in = sc.instr[i];
             int l = in.kind == 0 ? framePixel(in, x, y, z) : -1;
             if (in.kind == 0 && l < 0) continue;
+            if (in.kind == 1 && !insideAperture(in, x, y, z)) continue;
+            // the observer-frame wavelength (FluxRecorder.cpp:377-378)
+            const double lambda = lambda0 * in.zfac;
             if (in.nband == 0)
             {
                 // DisjointWavelengthGrid::bins: at most one bin, transmission 1

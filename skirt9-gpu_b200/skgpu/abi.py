@@ -139,6 +139,7 @@ SIGNATURES = {
     "upload_instruments": [_P, _I, _P, _I, _P, _P],
     "set_instrument_scattering_levels": [_P, _I, _I],
     "set_instrument_bands": [_P, _I, _I, _P, _P, _P, _P],
+    "set_instrument_observer": [_P, _I, _D, _D],
     "set_options": [_P, _P],
     "run_primary": [_P, _U, _U, _U],
     "probe_launch": [_P, _U, _U, _U, _P],
@@ -303,6 +304,9 @@ class Backend:
 
     def set_instrument_scattering_levels(self, i, levels):
         self.call("set_instrument_scattering_levels", int(i), int(levels))
+
+    def set_instrument_observer(self, i, redshift=0.0, aperture_radius=0.0):
+        self.call("set_instrument_observer", int(i), float(redshift), float(aperture_radius))
 
     def set_instrument_bands(self, i, bands):
         """bands: list of (wavelengths, normalised transmissions, effective width), in bin order."""

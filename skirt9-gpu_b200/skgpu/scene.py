@@ -169,9 +169,11 @@ class Scene:
             borders.extend(wb + [0.0])
             ellv.extend(we)
             s.kobs[:] = list(ins["kobs"])
+            if ins.get("trig") is not None:
+                # frames; SED instruments with an aperture (its projection)
+                (s.cos_theta, s.sin_theta, s.cos_phi, s.sin_phi, s.cos_omega, s.sin_omega) = ins["trig"]
             if s.kind == abi.INSTR_FRAME:
                 s.num_pixels_x, s.num_pixels_y = int(ins["nx"]), int(ins["ny"])
-                (s.cos_theta, s.sin_theta, s.cos_phi, s.sin_phi, s.cos_omega, s.sin_omega) = ins["trig"]
                 s.xp_min, s.xp_size, s.yp_min, s.yp_size = ins["xp_min"], ins["xp_size"], ins["yp_min"], ins["yp_size"]
             structs.append(s)
         be.upload_instruments(structs, np.array(borders), np.array(ellv, np.int32))
@@ -180,6 +182,8 @@ class Scene:
                 be.set_instrument_scattering_levels(i, ins["levels"])
             if ins.get("bands") is not None:
                 be.set_instrument_bands(i, ins["bands"])
+            if ins.get("redshift") or ins.get("aperture"):
+                be.set_instrument_observer(i, ins.get("redshift", 0.0), ins.get("aperture", 0.0))
 
     def source_structs(self, npp):
         """ABI source records for a segment of npp packets (SourceSystem::prepareForLaunch)."""

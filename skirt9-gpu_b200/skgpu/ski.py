@@ -250,7 +250,7 @@ def simulation(mode, num_packets, sources, media, grid, instruments, source_wave
                instrument_wlg='<ListWavelengthGrid wavelengths="0.55 micron" relativeHalfWidth="0" log="false"/>',
                force_scattering=True, store_rf=False, rf_wlg="", seed=0, num_density_samples=100,
                min_weight_reduction=1e4, path_length_bias=0.5, explicit_absorption=False, emission="",
-               secondary_iterations=None):
+               secondary_iterations=None, redshift=0.0):
     """A complete MonteCarloSimulation ski document (`emission`: the secondary and dust emission
     options of a DustEmission simulation, see dust_emission_options)."""
     src_attr = f' wavelengths="{source_wavelengths}"' if mode.startswith("Oligo") else ' minWavelength="0.1 micron" maxWavelength="10 micron"'
@@ -261,6 +261,9 @@ def simulation(mode, num_packets, sources, media, grid, instruments, source_wave
               + (f'<radiationFieldWLG type="DisjointWavelengthGrid">{rf_wlg}</radiationFieldWLG>' if rf_wlg else "")
               + '</RadiationFieldOptions></radiationFieldOptions>')
     rf += emission
+    cosmology = ('<cosmology type="Cosmology"><LocalUniverseCosmology/></cosmology>' if not redshift else
+                 f'<cosmology type="Cosmology"><FlatUniverseCosmology redshift="{redshift:g}" '
+                 f'reducedHubbleConstant="0.675" matterDensityFraction="0.31"/></cosmology>')
     iterate = "false"
     iteration_xml = ""
     if secondary_iterations:
@@ -275,7 +278,7 @@ def simulation(mode, num_packets, sources, media, grid, instruments, source_wave
 <MonteCarloSimulation userLevel="Expert" simulationMode="{mode}" iteratePrimaryEmission="false" iterateSecondaryEmission="{iterate}" numPackets="{num_packets:g}">
 <random type="Random"><Random seed="{seed}"/></random>
 <units type="Units"><ExtragalacticUnits wavelengthOutputStyle="Wavelength" fluxOutputStyle="Frequency"/></units>
-<cosmology type="Cosmology"><LocalUniverseCosmology/></cosmology>
+{cosmology}
 <sourceSystem type="SourceSystem"><SourceSystem{src_attr} sourceBias="0.5">
 <sources type="Source">{sources}</sources></SourceSystem></sourceSystem>
 <mediumSystem type="MediumSystem"><MediumSystem>
@@ -550,3 +553,26 @@ def dust_curvilinear(num_packets, kind):
             "cylinder2d": lambda: cylinder2d_grid(0.05, 1, -1, 1, 16, 16),
             "cylinder3d": lambda: cylinder3d_grid(0.05, 1, -1, 1, 12, 8, 12)}[kind]()
     return dust_shell(num_packets, grid=grid)
+
+
+def galaxy_observer(num_packets=30000, npix=16, nlambda=10, redshift=0.0, aperture_kpc=0.0):
+    """The galaxy on a small octree with a frame and two SED instruments at 60 degrees: at `redshift`
+    (a flat-universe cosmology, instruments at distance 0 so that they observe in the redshifted
+    frame), the second SED with an aperture of `aperture_kpc`."""
+    lam = [0.1 * (100.0 ** (i / (nlambda - 1))) for i in range(nlambda)]
+    kappa = [(l / 0.55) ** -1.0 for l in lam]
+    albedo = [min(0.9, max(0.05, 0.5 * (l / 0.55) ** -0.2)) for l in lam]
+    g = [min(0.9, max(0.0, 0.6 * (l / 0.55) ** -0.3)) for l in lam]
+    mix = mean_list_mix(lam, kappa, albedo, g)
+    sources = (geometric_source('<ExpDiskGeometry scaleLength="4 kpc" scaleHeight="0.35 kpc" minRadius="0 kpc" '
+                                'maxRadius="0 kpc" maxZ="0 kpc"/>', 6000, 8e9)
+               + geometric_source('<SersicGeometry effectiveRadius="1 kpc" index="4"/>', 4000, 2e9))
+    wlg = f'<LogWavelengthGrid minWavelength="0.1 micron" maxWavelength="10 micron" numWavelengths="{nlambda}"/>'
+    d = 0 if redshift else 10
+    aperture = sed_instrument("ap", 60, stats=True, distance_mpc=d, comps=False)
+    if aperture_kpc:
+        aperture = aperture.replace('radius="0 pc"', f'radius="{aperture_kpc} kpc"')
+    instruments = (frame_instrument("i60", 60, 50, "kpc", npix, stats=True, distance_mpc=d)
+                   + sed_instrument("sed", 60, stats=True, distance_mpc=d, comps=False) + aperture)
+    return simulation("ExtinctionOnly", num_packets, sources, expdisk_medium(6, 0.2, "kpc", 1.0, mix),
+                      octree_grid(25, "kpc", 5, 1e-3), instruments, instrument_wlg=wlg, redshift=redshift)

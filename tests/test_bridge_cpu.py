@@ -143,3 +143,11 @@ def test_bridge_merged_iterations_on_oracle(tmp_path):
     z, _ = tb.sed_z(g, c, "dust", "sed")
     assert len(z) > 25
     tb.check(z, 2.0, 5.0)
+
+
+@needs_build
+def test_bridge_redshift_and_aperture_on_oracle(tmp_path):
+    """The galaxy at redshift 0.5 (flat-universe cosmology, instruments observing in the redshifted
+    frame) with a 3 kpc SED aperture: frame and both SEDs against the reference program."""
+    log, g, c = both(tmp_path, ski.galaxy_observer(50000, redshift=0.5, aperture_kpc=3), "g")
+    tb.check_observer(g, c, "g")

@@ -101,6 +101,19 @@ def check_levels_and_bands(g, c, name):
     assert np.allclose(sa[:, 8:10].sum(axis=0), sb[:, 8:10].sum(axis=0), rtol=0.04)
 
 
+def check_observer(g, c, name):
+    """Frame and SEDs of ski.galaxy_observer: within noise, the aperture SED below the full one, and
+    nothing below 0.15 micron (the shortest source wavelength times 1 + z)."""
+    for ins in ("sed", "ap"):
+        z, _ = sed_z(g, c, name, ins)
+        assert len(z) >= 8
+        check(z, 4.0, 4.0)
+    full, ap = (np.loadtxt(os.path.join(g, f"{name}_{i}_sed.dat"))[:, 1] for i in ("sed", "ap"))
+    assert 0 < ap.sum() < full.sum() and full[0] == 0
+    z, _ = frame_z(g, c, name, "i60")
+    check(z, 1.4, 6.0)
+
+
 def check(z, chi2_max, zmax):
     """Mean square z below chi2_max; the 99.9th percentile of |z| below zmax (frame pixels see rare
     high-weight contributions, so the largest |z| of ~2e4 pixels is not a good test)."""
@@ -253,3 +266,10 @@ def test_bridge_merged_iterations(tmp_path):
     check(z, 2.0, 5.0)
     z, _ = frame_z(g, c, "dust", "i30")
     check(z, 1.3, 6.0)
+
+
+@needs_build
+def test_bridge_redshift_and_aperture(tmp_path):
+    """Redshift 0.5 and a 3 kpc SED aperture on the B200 through skirt_gpu -g."""
+    log, g, c = both(tmp_path, ski.galaxy_observer(200000, redshift=0.5, aperture_kpc=3), "g")
+    check_observer(g, c, "g")

@@ -97,6 +97,15 @@ def test_gpu_calibration_matches_oracle_and_reference(golden, gpu_backend, oracl
         assert np.array_equal(cal[key], raw[key] * fac[0]), key
 
 
+def test_gpu_observer_redshift_and_aperture_match_oracle(golden, gpu_backend, oracle_backend):
+    """Observer-frame redshift and an SED aperture: GPU FP64 equals the oracle per history."""
+    from test_instrument_output_cpu import observer_scene
+    sc = observer_scene(golden("shell_c16.npz"), 0.3 * 3.0856775814913673e16, 5e-4)
+    rg, ro = run_both(sc, gpu_backend, oracle_backend, 20000, seed=9)
+    assert_close_runs(rg, ro)
+    assert 0 < rg[2]["total"].sum() < rg[1]["total"].sum()
+
+
 def test_gpu_free_propagation_matches_oracle(golden, gpu_backend, oracle_backend):
     sc = Scene.from_export(golden("shell_c16.npz"))
     sc.force_scattering = False

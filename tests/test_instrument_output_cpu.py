@@ -113,3 +113,34 @@ def test_calibration_on_oracle_matches_the_reference(golden, oracle_backend):
     assert np.array_equal(cal["components"], raw["components"] * f[0])
     # the transparent flux (Jy) equals the reference's written value (10 significant digits)
     assert cal["components"][0, 0] == pytest.approx(float(z["ref_sed_jy"][1]), rel=1e-9)
+
+
+def observer_scene(z, radius, redshift):
+    """The shell with a second SED instrument of the same observer that has an aperture of `radius`
+    (projected with the frame's inclination and azimuth, as ApertureInstrument::isInsideAperture)
+    and an observer-frame redshift."""
+    sc = Scene.from_export(z)
+    frame, sed = sc.instruments
+    sed = dict(sed, trig=frame["trig"])
+    ap = dict(sed, same_observer=1, aperture=radius, redshift=redshift)
+    sc.instruments = [frame, sed, ap]
+    return sc
+
+
+def test_observer_redshift_and_aperture_on_oracle(golden, oracle_backend):
+    z = golden("shell_c16.npz")
+    sc = observer_scene(z, 0.3 * 3.0856775814913673e16, 5e-4)  # 0.55 micron stays in its bin
+    sc.upload(oracle_backend)
+    res = sc.run(oracle_backend, 4000, seed=9)
+    full, ap = res.instruments[1]["total"], res.instruments[2]["total"]
+    assert 0 < ap.sum() < full.sum()  # the aperture keeps the inner part of the shell
+    # an aperture larger than the domain records everything
+    sc2 = observer_scene(z, 1e30, 5e-4)
+    sc2.upload(oracle_backend)
+    res2 = sc2.run(oracle_backend, 4000, seed=9)
+    assert np.array_equal(res2.instruments[2]["total"], res2.instruments[1]["total"])
+    # a redshift that moves 0.55 micron out of the bin records nothing
+    sc3 = observer_scene(z, 0.0, 0.01)
+    sc3.upload(oracle_backend)
+    res3 = sc3.run(oracle_backend, 2000, seed=9)
+    assert res3.instruments[2]["total"].sum() == 0 and res3.instruments[1]["total"].sum() > 0
