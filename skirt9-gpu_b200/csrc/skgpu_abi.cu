@@ -799,10 +799,41 @@ int skgpu_upload_grid_voronoi(skgpu_ctx* ctx, int32_t num_sites, const double* s
     // (half the site distance for a neighbour, the distance to the domain wall for a wall), so that
     // s = (d - n . l) / (n . k) needs no squares of metre-scale coordinates, then per face the
     // neighbour's record offset (or the wall id); the faces are padded to a multiple of 4
+    // The records are laid out in the Morton order of their sites (21 bits per axis over the
+    // domain), not in cell order: a record spans several cache lines, and cells that are close in
+    // space (and so visited together) then share lines and DRAM pages. Only the layout changes;
+    // every record keeps its cell index.
+    std::vector<int> layout(num_sites);
+    {
+        auto spread = [](uint64_t v) {
+            v &= 0x1FFFFF;
+            v = (v | v << 32) & 0x1F00000000FFFFULL;
+            v = (v | v << 16) & 0x1F0000FF0000FFULL;
+            v = (v | v << 8) & 0x100F00F00F00F00FULL;
+            v = (v | v << 4) & 0x10C30C30C30C30C3ULL;
+            v = (v | v << 2) & 0x1249249249249249ULL;
+            return v;
+        };
+        std::vector<uint64_t> key(num_sites);
+        for (int c = 0; c < num_sites; ++c)
+        {
+            uint64_t q[3];
+            for (int a = 0; a < 3; ++a)
+            {
+                double f = (sites[3 * static_cast<size_t>(c) + a] - extent[a]) / (extent[a + 3] - extent[a]);
+                f = std::min(std::max(f, 0.), 1.);
+                q[a] = static_cast<uint64_t>(f * 2097151.);
+            }
+            key[c] = spread(q[0]) | spread(q[1]) << 1 | spread(q[2]) << 2;
+        }
+        for (int c = 0; c < num_sites; ++c) layout[c] = c;
+        std::stable_sort(layout.begin(), layout.end(), [&](int a, int b) { return key[a] < key[b]; });
+    }
     std::vector<int> recOff(num_sites);
     size_t units = 0;
-    for (int c = 0; c < num_sites; ++c)
+    for (int q = 0; q < num_sites; ++q)
     {
+        int c = layout[q];
         size_t n4 = (static_cast<size_t>(nb_begin[c + 1] - nb_begin[c]) + 3) & ~static_cast<size_t>(3);
         recOff[c] = static_cast<int>(units);
         units += 2 + n4 + n4 / 4;
