@@ -242,9 +242,25 @@ int skgpu_octree_build(const skgpu_octree_spec* spec, skgpu_octree** out)
             });
             t->numNb += n.nb[wall].size();
         }
+    // leaves numbered depth-first, children in OctTreeNode order (x fastest): the cells follow a
+    // Morton curve, so the walker's per-cell records of cells close in space lie close in memory
+    // (TreeSpatialGrid numbers them level by level; only the numbering differs)
     t->cellOfNode.assign(t->nodes.size(), -1);
-    for (size_t l = 0; l < t->nodes.size(); ++l)
-        if (t->nodes[l].firstChild < 0) t->cellOfNode[l] = t->numCells++;
+    {
+        std::vector<int> stack{0};
+        while (!stack.empty())
+        {
+            int l = stack.back();
+            stack.pop_back();
+            const Node& n = t->nodes[l];
+            if (n.firstChild < 0)
+            {
+                t->cellOfNode[l] = t->numCells++;
+                continue;
+            }
+            for (int q = 7; q >= 0; --q) stack.push_back(n.firstChild + q);
+        }
+    }
     t->cellDensity.resize(t->numCells);
     for (size_t l = 0; l < t->nodes.size(); ++l)
         if (t->cellOfNode[l] >= 0)
