@@ -652,6 +652,49 @@ struct TetraPlane32 : GenBase
         kzf = static_cast<float>(uz);
     }
 
+    // whether the float exit decision in tetrahedron r may differ from the exact one: the point lies
+    // within tol of the exit plane, the two nearest exits lie within the planes' error of each other
+    // (an edge or a vertex), or a face almost parallel to the path lies within tol of the point
+    SKG_D bool ambiguous(const TetRegs& r, double x, double y, double z, float tol) const
+    {
+        float best = FLT_MAX, second = FLT_MAX, nkBest = 1.f, nkSecond = 1.f;
+        float inside = FLT_MAX, graze = FLT_MAX;
+        auto face = [&](auto F) {
+            constexpr int f = decltype(F)::value;
+            if (f == ef) return;
+            float nk = r.n[3 * f] * kxf + r.n[3 * f + 1] * kyf + r.n[3 * f + 2] * kzf;
+            float me = static_cast<float>(-r.template excess<f>(x, y, z));
+            if (!(nk > 0.f))
+            {
+                if (nk > -kNk) graze = fminf(graze, me);  // may be a face ahead in exact arithmetic
+                return;
+            }
+            float s = me / nk;
+            if (s < best)
+            {
+                second = best;
+                nkSecond = nkBest;
+                best = s;
+                nkBest = nk;
+                inside = me;
+            }
+            else if (s < second)
+            {
+                second = s;
+                nkSecond = nk;
+            }
+        };
+        face(std::integral_constant<int, 0>());
+        face(std::integral_constant<int, 1>());
+        face(std::integral_constant<int, 2>());
+        face(std::integral_constant<int, 3>());
+        // second - best < tol (1/nkBest + 1/nkSecond) + 1e-6 second, multiplied through by the
+        // positive nkBest nkSecond (the bound is far coarser than the rounding of the test)
+        return inside < tol || graze < tol + 1e-6f * best ||
+               (second < FLT_MAX &&
+                (second - best) * nkBest * nkSecond < tol * (nkBest + nkSecond) + 1e-6f * second * nkBest * nkSecond);
+    }
+
     SKG_D bool next(const GridDev& g)
     {
         if (state == GS_OUTSIDE) return false;
@@ -668,84 +711,76 @@ struct TetraPlane32 : GenBase
             if (ds > 0.) return true;
         }
         // the float planes (normals rounded to FP32, offsets through a shared vertex, so neighbours
-        // agree) lie within kTilt * eps = 1.6e-7 of the domain diagonal of the exact ones; a decision
-        // closer than that to an edge, a vertex or a tie is re-taken in FP64 the reference's way
-        const double tol = kTilt * g.eps;
+        // agree) lie within kTilt * eps = 1.6e-7 of the domain diagonal of the exact ones
+        const float tol = static_cast<float>(kTilt * g.eps);
         for (int guard = 0; guard < 256; ++guard)
         {
             TetRegs r = TetRegs::load(g.teRec + mr);
-            float best = FLT_MAX, second = FLT_MAX, nkBest = 1.f, nkSecond = 1.f;
-            double inside = DBL_MAX, graze = DBL_MAX;
+            float best = FLT_MAX;
             int lf = -1;
             auto face = [&](auto F) {
                 constexpr int f = decltype(F)::value;
-                if (f == ef) return;
                 float nk = r.n[3 * f] * kxf + r.n[3 * f + 1] * kyf + r.n[3 * f + 2] * kzf;
-                double e = r.template excess<f>(rx, ry, rz);
-                if (!(nk > 0.f))
-                {
-                    if (nk > -kNk) graze = fmin(graze, -e);  // may be a face ahead in exact arithmetic
-                    return;
-                }
-                float s = static_cast<float>(-e) / nk;
+                if (f == ef || !(nk > 0.f)) return;
+                float s = static_cast<float>(-r.template excess<f>(rx, ry, rz)) / nk;
                 if (s < best)
                 {
-                    second = best;
-                    nkSecond = nkBest;
                     best = s;
-                    nkBest = nk;
-                    inside = -e;
                     lf = f;
-                }
-                else if (s < second)
-                {
-                    second = s;
-                    nkSecond = nk;
                 }
             };
             face(std::integral_constant<int, 0>());
             face(std::integral_constant<int, 1>());
             face(std::integral_constant<int, 2>());
             face(std::integral_constant<int, 3>());
-            bool exact = lf < 0 || inside < tol || graze < tol + 1e-6 * best ||
-                         (second < FLT_MAX && second - best < tol * (1. / nkBest + 1. / nkSecond) + 1e-6 * second);
-            int nt, nf;
-            if (!exact)
+            // Between two interior faces either choice continues the walk from the same point; only
+            // in a tetrahedron on the hull can a float decision end the path where the reference's
+            // goes on (or the reverse), so only there is the decision tested, in a second pass.
+            if (lf >= 0 && ((r.nb[0] | r.nb[1] | r.nb[2] | r.nb[3]) >= 0 || !ambiguous(r, rx, ry, rz, tol)))
             {
-                nt = r.neighbour(lf);
-                nf = (r.nface >> (8 * lf)) & 0xff;
-                m = mr;
-                ds = best;
-                propagater(ds);
-            }
-            else
-            {
-                double d;
-                int xf = teLeavingFace(g, mr, ef, rx, ry, rz, kx, ky, kz, d);
-                if (xf == -1 || d < g.eps)
+                int nt = r.neighbour(lf);
+                int nf = (r.nface >> (8 * lf)) & 0xff;
+                if (best > 0.f)
                 {
-                    // no exit point: the reference's eps step and its own point location
-                    propagater(g.eps);
-                    mr = tetraCellIndex(g, rx, ry, rz);
-                    ef = -1;
-                    if (mr < 0)
-                    {
-                        state = GS_OUTSIDE;
-                        return false;
-                    }
-                    continue;
+                    m = mr;
+                    ds = best;
+                    propagater(ds);
                 }
-                nt = g.teNTet[4 * static_cast<size_t>(mr) + xf];
-                nf = g.teNFace[4 * static_cast<size_t>(mr) + xf];
-                m = mr;
-                ds = d;
-                propagater(d);
+                mr = nt;
+                ef = nf;
+                if (mr < 0)
+                {
+                    // the reference drops the final in-mesh segment when the path leaves the hull
+                    state = GS_OUTSIDE;
+                    return false;
+                }
+                if (best > 0.f) return true;
+                continue;
             }
-            mr = nt;
-            ef = nf;
+            // no face ahead, or a decision within the float planes' error of an edge, a vertex or a
+            // tie: re-taken in FP64 the reference's way
+            double d;
+            int xf = teLeavingFace(g, mr, ef, rx, ry, rz, kx, ky, kz, d);
+            if (xf == -1 || d < g.eps)
+            {
+                // no exit point: the reference's eps step and its own point location
+                propagater(g.eps);
+                mr = tetraCellIndex(g, rx, ry, rz);
+                ef = -1;
+                if (mr < 0)
+                {
+                    state = GS_OUTSIDE;
+                    return false;
+                }
+                continue;
+            }
+            m = mr;
+            ds = d;
+            propagater(d);
+            ef = g.teNFace[4 * static_cast<size_t>(mr) + xf];
+            mr = g.teNTet[4 * static_cast<size_t>(mr) + xf];
             if (mr < 0)
             {
-                // the reference drops the final in-mesh segment when the path leaves the hull
                 state = GS_OUTSIDE;
                 return false;
             }
