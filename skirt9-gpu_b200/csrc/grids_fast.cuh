@@ -716,16 +716,19 @@ struct TetraPlane32 : GenBase
         for (int guard = 0; guard < 256; ++guard)
         {
             TetRegs r = TetRegs::load(g.teRec + mr);
-            float best = FLT_MAX;
+            // the nearest exit me / nk over the faces ahead (nk > 0), compared by cross-multiplication
+            // so that only the chosen face's distance takes a division
+            float meBest = 0.f, nkBest = 1.f;
             int lf = -1;
             auto face = [&](auto F) {
                 constexpr int f = decltype(F)::value;
                 float nk = r.n[3 * f] * kxf + r.n[3 * f + 1] * kyf + r.n[3 * f + 2] * kzf;
                 if (f == ef || !(nk > 0.f)) return;
-                float s = static_cast<float>(-r.template excess<f>(rx, ry, rz)) / nk;
-                if (s < best)
+                float me = static_cast<float>(-r.template excess<f>(rx, ry, rz));
+                if (lf < 0 || me * nkBest < meBest * nk)
                 {
-                    best = s;
+                    meBest = me;
+                    nkBest = nk;
                     lf = f;
                 }
             };
@@ -733,6 +736,7 @@ struct TetraPlane32 : GenBase
             face(std::integral_constant<int, 1>());
             face(std::integral_constant<int, 2>());
             face(std::integral_constant<int, 3>());
+            const float best = lf >= 0 ? meBest / nkBest : FLT_MAX;
             // Between two interior faces either choice continues the walk from the same point; only
             // in a tetrahedron on the hull can a float decision end the path where the reference's
             // goes on (or the reverse), so only there is the decision tested, in a second pass.
