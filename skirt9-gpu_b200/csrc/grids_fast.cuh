@@ -476,7 +476,9 @@ struct VoronoiRec32 : GenBase
             int n4 = (__float_as_int(h1.w) + 3) & ~3;
             const float4* E = R + 2;
             const int4* ids = reinterpret_cast<const int4*>(R + 2 + n4);
-            float best = FLT_MAX, second = FLT_MAX, scale = 0.f;
+            // the two nearest exits me / nk, compared by cross-multiplication so that only those two
+            // distances take a division
+            float meB = 0.f, nkB = 1.f, meS = 0.f, nkS = 1.f, scale = 0.f;
             int ib = kNone, is = kNone;
             for (int c = 0; c < n4; c += 4)
             {
@@ -489,19 +491,22 @@ struct VoronoiRec32 : GenBase
                 {
                     float nk = q[j].x * kxf + q[j].y * kyf + q[j].z * kzf;
                     if (!(nk > 0.f) || id[j] == prev) continue;
-                    float s = (q[j].w - (q[j].x * lx + q[j].y * ly + q[j].z * lz)) / nk;
-                    if (!(s > 0.f)) continue;
-                    if (s < best)
+                    float me = q[j].w - (q[j].x * lx + q[j].y * ly + q[j].z * lz);
+                    if (!(me > 0.f)) continue;
+                    if (ib == kNone || me * nkB < meB * nk)
                     {
-                        second = best;
+                        meS = meB;
+                        nkS = nkB;
                         is = ib;
-                        best = s;
+                        meB = me;
+                        nkB = nk;
                         ib = id[j];
                         scale = q[j].w;
                     }
-                    else if (s < second)
+                    else if (is == kNone || me * nkS < meS * nk)
                     {
-                        second = s;
+                        meS = me;
+                        nkS = nk;
                         is = id[j];
                     }
                 }
@@ -518,6 +523,7 @@ struct VoronoiRec32 : GenBase
                 }
                 continue;
             }
+            const float best = meB / nkB, second = is != kNone ? meS / nkS : FLT_MAX;
             double sq = best;
             if (is != kNone && second - best <= 2e-5f * (best + scale))
             {
